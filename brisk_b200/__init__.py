@@ -1,0 +1,12 @@
+"""brisk_b200: the SDP interior-point Newton step of BRISK on a B200 GPU.
+
+The public API mirrors the reference's Python package (``brisk``): ``solve_sdpa`` and
+``solve_file`` return a ``Result`` with the status, objectives, DIMACS errors and the solution.
+The work runs in the in-tree CUDA library ``libbrisk.so`` (sm_100a), which exports the same C
+interface as the reference's libbrisk.
+"""
+from ._core import (STATUS, Result, interrupt, library_path, load_library, options_to_argv, solve_file,
+                    solve_sdpa, version)
+
+__all__ = ["STATUS", "Result", "interrupt", "library_path", "load_library", "options_to_argv", "solve_file",
+           "solve_sdpa", "version"]

@@ -1,0 +1,97 @@
+// The step-level C ABI (include/bgpu.h): thin wrappers over the kernel launchers.
+#include "../../include/bgpu.h"
+#include "common.cuh"
+#include "kernels.h"
+#include "tf32x3.h"
+
+long long g_bgpu_launches = 0;
+static cudaStream_t S(void *s) { return (cudaStream_t)s; }
+
+extern "C" {
+
+BGPU_API int bgpu_sync(void *stream) {
+    BGPU_CHECK(cudaStreamSynchronize(S(stream)));
+    return BGPU_OK;
+}
+BGPU_API const char *bgpu_version(void) { return "brisk_b200 1.7-b200 sm_100a"; }
+BGPU_API long long bgpu_launch_count(void) { return __atomic_load_n(&g_bgpu_launches, __ATOMIC_RELAXED); }
+
+BGPU_API size_t bgpu_schur_ws_bytes(int n, int chunk, int precision) {
+    if (chunk <= 0) chunk = schur_chunk_default(n, precision);
+    return schur_ws_bytes(n, chunk, precision);
+}
+BGPU_API int bgpu_schur_chunk_default(int n, int precision) { return schur_chunk_default(n, precision); }
+
+BGPU_API int bgpu_schur_assemble(int n, int m, int ncon, const int *d_con, const long long *d_cptr,
+                                 const int *d_cpos, const double *d_cval, const double *d_X, const double *d_Zi,
+                                 double *d_M, int precision, int chunk, void *d_ws, size_t ws_bytes, void *stream) {
+    if (n <= 0 || m <= 0 || ncon < 0 || (precision != 0 && precision != 1)) return BGPU_ERR_ARG;
+    if (chunk <= 0) chunk = schur_chunk_default(n, precision);
+    DevBlock B;
+    B.n = n;
+    B.ncon = ncon;
+    B.con = (int *)d_con;
+    B.cptr = (long long *)d_cptr;
+    B.cpos = (int *)d_cpos;
+    B.cval = (double *)d_cval;
+    return schur_assemble(S(stream), B, d_X, d_Zi, d_M, m, precision, chunk, d_ws, ws_bytes);
+}
+
+BGPU_API int bgpu_potrf(int n, double *d_A, int lda, double *d_dinv, int *d_info, double *d_pmin, void *stream) {
+    if (n <= 0 || lda < n) return BGPU_ERR_ARG;
+    return potrf_f64(S(stream), n, d_A, lda, d_dinv, d_info, d_pmin);
+}
+BGPU_API int bgpu_potrf_f32(int n, float *d_A, int lda, float *d_dinv, int *d_info, double *d_pmin, void *stream) {
+    if (n <= 0 || lda < n) return BGPU_ERR_ARG;
+    return potrf_f32(S(stream), n, d_A, lda, d_dinv, d_info, d_pmin);
+}
+BGPU_API int bgpu_trsv(int n, const double *d_L, int lda, const double *d_dinv, double *d_x, int trans,
+                       int *d_flags, int epoch, int *d_err, void *stream) {
+    if (n <= 0 || lda < n) return BGPU_ERR_ARG;
+    return trsv_f64(S(stream), n, d_L, lda, d_dinv, d_x, trans, d_flags, epoch, d_err);
+}
+BGPU_API int bgpu_trsv_f32(int n, const float *d_L, int lda, const float *d_dinv, float *d_x, int trans,
+                           int *d_flags, int epoch, int *d_err, void *stream) {
+    if (n <= 0 || lda < n) return BGPU_ERR_ARG;
+    return trsv_f32(S(stream), n, d_L, lda, d_dinv, d_x, trans, d_flags, epoch, d_err);
+}
+BGPU_API int bgpu_trtri(int n, const double *d_L, int lda, const double *d_dinv, double *d_Linv, int ldi,
+                        void *stream) {
+    if (n <= 0 || lda < n || ldi < n) return BGPU_ERR_ARG;
+    return trtri_f64(S(stream), n, d_L, lda, d_dinv, d_Linv, ldi);
+}
+BGPU_API int bgpu_dgemm(int a_kmajor, int b_kmajor, int M, int N, int K, double alpha, const double *d_A,
+                        int64_t lda, const double *d_B, int64_t ldb, double beta, double *d_C, int64_t ldc,
+                        int lower, void *stream) {
+    if (M < 0 || N < 0 || K < 0) return BGPU_ERR_ARG;
+    return gemm_f64(S(stream), a_kmajor, b_kmajor, M, N, K, alpha, d_A, lda, 0, d_B, ldb, 0, beta, d_C, ldc, 0, 1,
+                    lower);
+}
+BGPU_API int bgpu_gemm_tf32x3(int M, int N, int K, const float *d_Ah, const float *d_Al, int64_t lda,
+                              const float *d_Bh, const float *d_Bl, int64_t ldb, float *d_G, int64_t ldg,
+                              void *stream) {
+    if (M < 0 || N < 0 || K < 0) return BGPU_ERR_ARG;
+    return gemm_tf32x3(S(stream), M, N, K, d_Ah, d_Al, lda, d_Bh, d_Bl, ldb, d_G, ldg);
+}
+BGPU_API int bgpu_split_tf32(int64_t n, const double *d_x, float *d_hi, float *d_lo, void *stream) {
+    return split_tf32(S(stream), n, d_x, d_hi, d_lo);
+}
+BGPU_API int bgpu_symv(int n, double alpha, const double *d_M, int ldm, const double *d_x, double beta,
+                       double *d_y, void *stream) {
+    if (n <= 0 || ldm < n) return BGPU_ERR_ARG;
+    return symv_full_f64(S(stream), n, alpha, d_M, ldm, d_x, beta, d_y);
+}
+BGPU_API int bgpu_aop(int n, int ncon, const int *d_con, const long long *d_cptr, const int *d_cpos,
+                      const double *d_cval, const double *d_D, double alpha, double beta, double *d_out,
+                      void *stream) {
+    DevBlock B;
+    B.n = n;
+    B.ncon = ncon;
+    B.con = (int *)d_con;
+    B.cptr = (long long *)d_cptr;
+    B.cpos = (int *)d_cpos;
+    B.cval = (double *)d_cval;
+    return aop_f64(S(stream), B, d_D, alpha, beta, d_out);
+}
+
+}  // extern "C"

@@ -1,0 +1,410 @@
+// The drop-in C interface: the exported brisk_* functions of the reference's libbrisk
+// (capi.c:60-201, 520-535; version script libbrisk.map) for the semidefinite path, with the
+// same argument meaning, return codes and accessor set.  Options are command-line strings
+// (main.c:5846-5960 for the ones the Newton step reads); SDPA sparse files are read here.
+#include "../../include/bgpu.h"
+#include "../../include/brisk.h"
+#include "solver.h"
+
+#include <cctype>
+#include <cerrno>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+namespace bsolve {
+void set_print_hook(int (*f)(const char *, int));
+}
+
+struct BriskResult {
+    bsolve::ResultData r;
+    std::vector<const double *> Xp, Zp;
+    std::string status_str;
+};
+
+namespace {
+int g_out_mode = 0;
+int (*g_out_cb)(const char *, int) = nullptr;
+volatile int g_stop = 0;
+int g_stop_owner = 0;
+
+int capi_print(const char *s, int is_err) {
+    if (g_out_mode == 2 && g_out_cb) return g_out_cb(s, is_err);
+    if (g_out_mode == 1 && !is_err) return 0;
+    fputs(s, is_err ? stderr : stdout);
+    return 0;
+}
+
+void fill_result(BriskResult *res) {
+    res->status_str = bsolve::status_string(res->r.status);
+    res->Xp.assign(res->r.nblk, nullptr);
+    res->Zp.assign(res->r.nblk, nullptr);
+    for (int k = 0; k < res->r.nblk && k < (int)res->r.X.size(); k++) {
+        res->Xp[k] = res->r.X[k].data();
+        res->Zp[k] = res->r.Z[k].data();
+    }
+}
+
+int run(const bsolve::InputData &in, int nopt, const char *const *opts, BriskResult *res) {
+    bsolve::Options opt;
+    std::string err;
+    bsolve::set_print_hook(capi_print);
+    if (bsolve::parse_options(nopt, opts, opt, err)) {
+        bsolve::log_printf(1, "brisk: %s\n", err.c_str());
+        fflush(stdout);
+        return 1;
+    }
+    const int rc = bsolve::solve_problem(in, opt, res->r);
+    fill_result(res);
+    fflush(stdout);
+    fflush(stderr);
+    return rc;
+}
+}  // namespace
+
+namespace bsolve {
+
+static bool parse_double(const char *s, double &v) {
+    if (!s) return false;
+    char *e = nullptr;
+    errno = 0;
+    v = strtod(s, &e);
+    return e != s && *e == 0 && errno == 0;
+}
+static bool parse_int(const char *s, int &v) {
+    double d;
+    if (!parse_double(s, d) || d != std::floor(d)) return false;
+    v = (int)d;
+    return true;
+}
+
+int parse_options(int argc, const char *const *argv, Options &opt, std::string &err) {
+    bool tol_given = false;
+    for (int i = 0; i < argc; i++) {
+        const std::string a = argv[i] ? argv[i] : "";
+        auto need = [&](const char *what) -> const char * {
+            if (i + 1 >= argc) { err = std::string("option ") + a + " needs " + what; return nullptr; }
+            return argv[++i];
+        };
+        if (a == "-tol") {
+            const char *s = need("a number");
+            if (!s || !parse_double(s, opt.tol) || !(opt.tol > 0)) { if (err.empty()) err = "bad -tol"; return 1; }
+            tol_given = true;
+        } else if (a == "-maxit") {
+            const char *s = need("a number");
+            if (!s || !parse_int(s, opt.maxit) || opt.maxit < 0) { if (err.empty()) err = "bad -maxit"; return 1; }
+        } else if (a == "-lanczos") {
+            const char *s = need("a number");
+            if (!s || !parse_int(s, opt.lanczos_k) || opt.lanczos_k < 1) { if (err.empty()) err = "bad -lanczos"; return 1; }
+        } else if (a == "-gmax") {
+            const char *s = need("a number");
+            if (!s || !parse_double(s, opt.gamma_max)) { if (err.empty()) err = "bad -gmax"; return 1; }
+        } else if (a == "-pivtol") {
+            const char *s = need("a number");
+            if (!s || !parse_double(s, opt.pivtol)) { if (err.empty()) err = "bad -pivtol"; return 1; }
+        } else if (a == "-regill") {
+            const char *s = need("a number");
+            if (!s || !parse_double(s, opt.reg_ill)) { if (err.empty()) err = "bad -regill"; return 1; }
+        } else if (a == "-mixed") {
+            const char *s = need("-1, 0 or 1");
+            if (!s || !parse_int(s, opt.mixed)) { if (err.empty()) err = "bad -mixed"; return 1; }
+        } else if (a == "-asmprec") {   // this build: the Schur assembly's precision
+            const char *s = need("fp64 or tf32x3");
+            if (!s) return 1;
+            if (!strcmp(s, "fp64")) opt.asm_prec = 0;
+            else if (!strcmp(s, "tf32x3")) opt.asm_prec = 1;
+            else { err = "bad -asmprec (fp64 or tf32x3)"; return 1; }
+        } else if (a == "-muswitch") {
+            const char *s = need("a number");
+            if (!s || !parse_double(s, opt.mu_switch)) { if (err.empty()) err = "bad -muswitch"; return 1; }
+        } else if (a == "-schurchunk") {
+            const char *s = need("8, 16, 32 or 64");
+            if (!s || !parse_int(s, opt.chunk) || (opt.chunk != 8 && opt.chunk != 16 && opt.chunk != 32 && opt.chunk != 64)) {
+                if (err.empty()) err = "bad -schurchunk";
+                return 1;
+            }
+        } else if (a == "-device") {
+            const char *s = need("a number");
+            if (!s || !parse_int(s, opt.device)) { if (err.empty()) err = "bad -device"; return 1; }
+        } else if (a == "-timelimit") {
+            const char *s = need("a number");
+            if (!s || !parse_double(s, opt.timelimit)) { if (err.empty()) err = "bad -timelimit"; return 1; }
+        } else if (a == "-sigma") {
+            const char *s = need("a number");
+            if (!s || !parse_int(s, opt.sigma_rule)) { if (err.empty()) err = "bad -sigma"; return 1; }
+        } else if (a == "-acc") {
+            const char *s = need("low, medium or high");
+            if (!s) return 1;
+            if (!strcmp(s, "low")) { opt.tol = 1e-6; opt.red_acc = 1e-4; }
+            else if (!strcmp(s, "high")) { opt.tol = 1e-10; opt.red_acc = 1e-6; }
+            else if (!strcmp(s, "medium")) { opt.tol = 1e-8; opt.red_acc = 1e-6; }
+            else { err = "bad -acc"; return 1; }
+        } else if (a == "-dir") {
+            const char *s = need("hkm, nt or auto");
+            if (!s) return 1;
+            if (strcmp(s, "hkm") && strcmp(s, "auto")) { err = "this build solves with the HKM direction only (-dir hkm)"; return 1; }
+        } else if (a == "-init") {
+            const char *s = need("0 or 1");
+            if (!s || !parse_int(s, opt.init) || opt.init < 0) { if (err.empty()) err = "bad -init"; return 1; }
+        } else if (a == "-q") {
+            opt.verbose = 0;
+        } else if (a == "-v") {
+            opt.verbose = 2;
+        } else if (a == "-vv" || a == "-vvv") {
+            opt.verbose = 3;
+        } else if (a == "-nohsd" || a == "-nofr" || a == "-feasible") {
+            if (a == "-feasible") opt.known_feasible = 1;
+        } else if (a == "-hsd" || a == "-sparse" || a == "-threads" || a == "-chordal" || a == "-sym" ||
+                   a == "-symalg" || a == "-deprows" || a == "-caller" || a == "-corr" || a == "-mixedfrac") {
+            // options of the reference that take a value and do not change this path's arithmetic
+            if (!need("a value")) return 1;
+        } else {
+            log_printf(1, "brisk: note: option %s is not used by the GPU Newton step (ignored)\n", a.c_str());
+        }
+    }
+    if (tol_given && 100.0 * opt.tol > opt.red_acc) opt.red_acc = 100.0 * opt.tol;
+    return 0;
+}
+
+// SDPA sparse reader: "m", "nblk", block sizes, c, then "mat blk i j v" lines; '"' and '*'
+// start comment lines, and ",(){}" are separators (as the reference's read_sdpa, problem.c:426).
+int read_sdpa_file(const char *path, InputData &in, std::string &err) {
+    FILE *f = fopen(path, "rb");
+    if (!f) { err = std::string("cannot open ") + path; return 2; }
+    std::string text;
+    {
+        std::vector<char> buf(1 << 20);
+        size_t n;
+        while ((n = fread(buf.data(), 1, buf.size(), f)) > 0) text.append(buf.data(), n);
+        fclose(f);
+    }
+    // drop comment lines, map separators to blanks
+    std::string clean;
+    clean.reserve(text.size());
+    size_t pos = 0;
+    while (pos < text.size()) {
+        size_t e = text.find('\n', pos);
+        if (e == std::string::npos) e = text.size();
+        size_t s = pos;
+        while (s < e && (text[s] == ' ' || text[s] == '\t' || text[s] == '\r')) s++;
+        if (s < e && text[s] != '"' && text[s] != '*') {
+            for (size_t q = pos; q < e; q++) {
+                char c = text[q];
+                if (c == ',' || c == '(' || c == ')' || c == '{' || c == '}' || c == '\r') c = ' ';
+                clean.push_back(c);
+            }
+            clean.push_back('\n');
+        }
+        pos = e + 1;
+    }
+    const char *p = clean.c_str();
+    char *endp = nullptr;
+    auto next = [&](double &v) -> bool {
+        while (*p && isspace((unsigned char)*p)) p++;
+        if (!*p) return false;
+        v = strtod(p, &endp);
+        if (endp == p) return false;
+        p = endp;
+        return true;
+    };
+    double v;
+    if (!next(v)) { err = "bad SDPA header (m)"; return 2; }
+    in.m = (int)v;
+    if (!next(v)) { err = "bad SDPA header (nblk)"; return 2; }
+    in.nblk = (int)v;
+    if (in.m < 0 || in.nblk <= 0) { err = "bad SDPA header"; return 2; }
+    in.bs.resize(in.nblk);
+    for (int k = 0; k < in.nblk; k++) {
+        if (!next(v)) { err = "bad block sizes"; return 2; }
+        in.bs[k] = (int)v;
+    }
+    in.c.resize(in.m);
+    for (int i = 0; i < in.m; i++) {
+        if (!next(v)) { err = "bad c vector"; return 2; }
+        in.c[i] = v;
+    }
+    double q[5];
+    while (true) {
+        int got = 0;
+        for (; got < 5; got++)
+            if (!next(q[got])) break;
+        if (got == 0) break;
+        if (got < 5) { err = "truncated entry line"; return 2; }
+        if (q[4] == 0) continue;
+        in.mat.push_back((int)q[0]);
+        in.blk.push_back((int)q[1]);
+        in.i.push_back((int)q[2]);
+        in.j.push_back((int)q[3]);
+        in.v.push_back(q[4]);
+    }
+    return 0;
+}
+
+}  // namespace bsolve
+
+// ---------------------------------------------------------------------------------------------
+// exported interface
+// ---------------------------------------------------------------------------------------------
+static bool make_input(int m, int nblk, const int *bs, const double *c, int64_t nnz, const int *mat, const int *blk,
+                       const int *i, const int *j, const double *v, bsolve::InputData &in) {
+    if (nnz < 0 || m < 0 || nblk <= 0 || !bs || (m > 0 && !c) || (nnz > 0 && (!mat || !blk || !i || !j || !v))) return false;
+    in.m = m;
+    in.nblk = nblk;
+    in.bs.assign(bs, bs + nblk);
+    in.c.assign(c, c + m);
+    for (int64_t q = 0; q < nnz; q++) {
+        if (v[q] == 0) continue;
+        in.mat.push_back(mat[q]);
+        in.blk.push_back(blk[q]);
+        in.i.push_back(i[q]);
+        in.j.push_back(j[q]);
+        in.v.push_back(v[q]);
+    }
+    return true;
+}
+
+extern "C" {
+
+BRISK_API void brisk_set_output(int mode, int (*cb)(const char *s, int is_err)) {
+    g_out_mode = mode;
+    g_out_cb = cb;
+}
+
+BRISK_API const char *brisk_version(void) { return "1.7-b200"; }
+
+BRISK_API BriskResult *brisk_result_new(void) {
+    BriskResult *r = new (std::nothrow) BriskResult();
+    if (r) r->r.status = -1;
+    return r;
+}
+BRISK_API void brisk_result_delete(BriskResult *r) { delete r; }
+BRISK_API int brisk_result_status(const BriskResult *r) { return r ? r->r.status : -1; }
+BRISK_API const char *brisk_result_status_str(const BriskResult *r) {
+    return r && r->r.status >= 0 ? r->status_str.c_str() : "NOT SOLVED";
+}
+BRISK_API int brisk_result_exit_code(const BriskResult *r) { return r ? r->r.exit_code : -1; }
+BRISK_API int brisk_result_iterations(const BriskResult *r) { return r ? r->r.iters : 0; }
+BRISK_API int brisk_result_m(const BriskResult *r) { return r ? r->r.m : 0; }
+BRISK_API int brisk_result_nblk(const BriskResult *r) { return r ? r->r.nblk : 0; }
+BRISK_API int brisk_result_blocksize(const BriskResult *r, int k) {
+    return r && k >= 0 && k < (int)r->r.bs.size() ? r->r.bs[k] : 0;
+}
+BRISK_API double brisk_result_pobj(const BriskResult *r) { return r ? r->r.pobj : 0; }
+BRISK_API double brisk_result_dobj(const BriskResult *r) { return r ? r->r.dobj : 0; }
+BRISK_API double brisk_result_time(const BriskResult *r) { return r ? r->r.time : 0; }
+BRISK_API int brisk_result_have_x(const BriskResult *r) { return r ? r->r.have_x : 0; }
+BRISK_API void brisk_result_dimacs(const BriskResult *r, double *err) {
+    for (int e = 0; e < 6; e++) err[e] = r ? r->r.err[e + 1] : 0;
+}
+BRISK_API const double *brisk_result_y(const BriskResult *r) { return r && !r->r.y.empty() ? r->r.y.data() : nullptr; }
+BRISK_API const double *brisk_result_X(const BriskResult *r, int k) {
+    return r && r->r.have_x && k >= 0 && k < (int)r->Xp.size() ? r->Xp[k] : nullptr;
+}
+BRISK_API const double *brisk_result_Z(const BriskResult *r, int k) {
+    return r && k >= 0 && k < (int)r->Zp.size() ? r->Zp[k] : nullptr;
+}
+BRISK_API int brisk_result_bound(const BriskResult *r, double *out) {
+    if (out) for (int q = 0; q < 6; q++) out[q] = 0;
+    return 0;
+}
+BRISK_API int brisk_result_resolves(const BriskResult *r, double *t) {
+    if (t) *t = 0;
+    return 0;
+}
+BRISK_API const char *brisk_result_cause(const BriskResult *r) { return ""; }
+
+BRISK_API void brisk_interrupt(void) { g_stop = 1; }
+BRISK_API int brisk_interrupted(void) { return g_stop != 0; }
+BRISK_API void brisk_clear_interrupt(void) { g_stop = 0; }
+BRISK_API void brisk_set_interrupt_owner(int caller) { g_stop_owner = caller != 0; }
+
+BRISK_API int brisk_solve_data(int m, int nblk, const int *bs, const double *c, int64_t nnz, const int *mat,
+                               const int *blk, const int *i, const int *j, const double *v, int nopt,
+                               const char *const *opts, BriskResult *res) {
+    if (!res) return -1;
+    res->r = bsolve::ResultData();
+    if (!g_stop_owner) g_stop = 0;
+    bsolve::InputData in;
+    if (!make_input(m, nblk, bs, c, nnz, mat, blk, i, j, v, in)) return 2;
+    return run(in, nopt, opts, res);
+}
+
+struct bgpu_session {
+    bsolve::Session *s = nullptr;
+};
+
+BGPU_API bgpu_session *bgpu_session_create(int m, int nblk, const int *bs, const double *c, int64_t nnz,
+                                           const int *mat, const int *blk, const int *i, const int *j,
+                                           const double *v, int nopt, const char *const *opts, int *rc) {
+    int code = 0;
+    bsolve::InputData in;
+    bsolve::Options opt;
+    std::string err;
+    bsolve::set_print_hook(capi_print);
+    if (!make_input(m, nblk, bs, c, nnz, mat, blk, i, j, v, in)) code = 2;
+    else if (bsolve::parse_options(nopt, opts, opt, err)) code = 1;
+    bgpu_session *h = nullptr;
+    if (!code) {
+        bsolve::Session *s = bsolve::session_create(in, opt, err, code);
+        if (s) {
+            h = new bgpu_session;
+            h->s = s;
+        }
+    }
+    if (code) bsolve::log_printf(1, "brisk: %s\n", err.c_str());
+    if (rc) *rc = code;
+    return h;
+}
+
+BGPU_API int bgpu_session_solve(bgpu_session *h, int nopt, const char *const *opts, BriskResult *res) {
+    if (!h || !res) return -1;
+    bsolve::Options opt;
+    std::string err;
+    bsolve::set_print_hook(capi_print);
+    if (bsolve::parse_options(nopt, opts, opt, err)) {
+        bsolve::log_printf(1, "brisk: %s\n", err.c_str());
+        return 1;
+    }
+    const int rc = bsolve::session_solve(h->s, opt, res->r);
+    fill_result(res);
+    fflush(stdout);
+    return rc;
+}
+
+BGPU_API void bgpu_session_destroy(bgpu_session *h) {
+    if (!h) return;
+    bsolve::session_destroy(h->s);
+    delete h;
+}
+
+BGPU_API int bgpu_result_measures(const BriskResult *r, double *out) {
+    if (!r || !out) return BGPU_ERR_ARG;
+    out[0] = r->r.device_time;
+    out[1] = r->r.schur_time;
+    out[2] = r->r.schur_flops;
+    out[3] = r->r.h2d_bytes;
+    out[4] = r->r.d2h_bytes;
+    out[5] = r->r.iters;
+    out[6] = r->r.nfloat;
+    out[7] = r->r.pcg_iters;
+    return BGPU_OK;
+}
+
+BRISK_API int brisk_solve_file(const char *fname, int nopt, const char *const *opts, BriskResult *res) {
+    if (!res) return -1;
+    res->r = bsolve::ResultData();
+    if (!g_stop_owner) g_stop = 0;
+    bsolve::InputData in;
+    std::string err;
+    bsolve::set_print_hook(capi_print);
+    if (!fname || bsolve::read_sdpa_file(fname, in, err)) {
+        bsolve::log_printf(1, "brisk: %s\n", err.c_str());
+        return 2;
+    }
+    return run(in, nopt, opts, res);
+}
+
+}  // extern "C"

@@ -1,0 +1,461 @@
+// Dense factor and solve kernels for the Schur complement M and the per-block X, Z.
+//
+// Cholesky: blocked right-looking, 64-column panels.  The diagonal block is factored in one
+// CTA, which also writes the inverse of its 64 x 64 triangle; the panel below is then solved
+// as a GEMM with that inverse and the trailing lower triangle updated by a DMMA rank-64 update
+// (gemm_f64 with lower = 1).  This is the GPU counterpart of the reference's tiled dense
+// Cholesky brisk_dpotrf / brisk_spotrf (sparsechol.c:3822-3860) and of chol_lower
+// (solver.c:679): the same factor L L' = A and the same failure report (the first
+// non-positive pivot), with the smallest squared pivot recorded for the acceptance test of
+// schur_factor_ (solver.c:5344-5353, 5400-5410).
+//
+// Triangular solves: one persistent, cooperatively launched kernel per solve.  CTA r owns block
+// row r; it subtracts L(r, c) x_c as soon as block c is published (a release/acquire flag with
+// a bounded wait) and finishes with the diagonal-block inverse.  Replaces brisk_dpotrs1 /
+// brisk_spotrs1 (sparsechol.c:4060-4180) and the dtrsv calls of the Lanczos step length.
+#include "common.cuh"
+#include "kernels.h"
+#include <cooperative_groups.h>
+
+namespace {
+constexpr int NB = TRI_NB;      // 64
+constexpr int LDS = NB + 1;     // padded smem stride
+
+// ---- diagonal-block factor + inverse ----------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) potrf_diag_kernel(int n, T *A, long long lda, int j0, T *dinv, int *info,
+                                                         double *pmin) {
+    extern __shared__ __align__(16) unsigned char dsm_raw[];
+    T *S = reinterpret_cast<T *>(dsm_raw);   // factor, then L
+    T *X = S + NB * LDS;                      // inverse of L
+    __shared__ int fail;
+    const int tid = threadIdx.x;
+    const int nb = min(NB, n - j0);
+    if (*(volatile int *)info != 0) {   // an earlier panel failed: nothing to do
+        return;
+    }
+    T *Ad = A + (long long)j0 + (long long)j0 * lda;
+    for (int idx = tid; idx < NB * NB; idx += 256) {
+        const int r = idx % NB, c = idx / NB;
+        T v = (T)0;
+        if (r < nb && c < nb && r >= c) v = Ad[r + (long long)c * lda];
+        S[r + c * LDS] = v;
+        X[r + c * LDS] = (r == c) ? (T)1 : (T)0;
+    }
+    if (tid == 0) fail = 0;
+    __syncthreads();
+    double pm = 1e300;
+    for (int c = 0; c < nb; c++) {
+        if (tid == 0) {
+            const T d = S[c + c * LDS];
+            if (!(d > (T)0) || !isfinite((double)d)) fail = j0 + c + 1;
+            else {
+                S[c + c * LDS] = sqrt(d);
+                if ((double)d < pm) pm = (double)d;
+            }
+        }
+        __syncthreads();
+        if (fail) break;
+        const T piv = S[c + c * LDS];
+        for (int r = c + 1 + tid; r < nb; r += 256) S[r + c * LDS] /= piv;
+        __syncthreads();
+        const int w = nb - c - 1;
+        for (int idx = tid; idx < w * w; idx += 256) {
+            const int r = c + 1 + idx % w, k = c + 1 + idx / w;
+            if (r >= k) S[r + k * LDS] -= S[r + c * LDS] * S[k + c * LDS];
+        }
+        __syncthreads();
+    }
+    if (fail) {
+        if (tid == 0) atomicCAS(info, 0, fail);
+        return;
+    }
+    if (tid == 0) {
+        // positive doubles order like their bit patterns
+        atomicMin((unsigned long long *)pmin, (unsigned long long)__double_as_longlong(pm));
+    }
+    // inverse of the lower triangle: forward substitution on the identity, row k at a time
+    for (int k = 0; k < nb; k++) {
+        const T lkk = S[k + k * LDS];
+        for (int j = tid; j <= k; j += 256) X[k + j * LDS] /= lkk;
+        __syncthreads();
+        const int w = nb - k - 1;
+        for (int idx = tid; idx < w * (k + 1); idx += 256) {
+            const int r = k + 1 + idx % w, j = idx / w;
+            X[r + j * LDS] -= S[r + k * LDS] * X[k + j * LDS];
+        }
+        __syncthreads();
+    }
+    for (int idx = tid; idx < NB * NB; idx += 256) {
+        const int r = idx % NB, c = idx / NB;
+        if (r < nb && c < nb && r >= c) Ad[r + (long long)c * lda] = S[r + c * LDS];
+        // identity beyond nb so a partial last block acts as a full one in the solves
+        dinv[r + c * NB] = (r < nb && c < nb) ? ((r >= c) ? X[r + c * LDS] : (T)0) : (T)(r == c ? 1 : 0);
+    }
+}
+
+__global__ void init_info_kernel(int *info, double *pmin) {
+    *info = 0;
+    *pmin = 1.0;
+}
+
+// ---- float panel solve and trailing update (SIMT FFMA; the mixed path's factor) --------------
+// A21 <- A21 * Dinv^T  (rows below the panel), in place: a CTA reads a full row block first.
+__global__ void __launch_bounds__(256) trsm_panel_f32(int rows, int nb, float *A21, long long lda, const float *dinv) {
+    __shared__ float Di[NB * NB];
+    __shared__ float R[64 * LDS];
+    const int tid = threadIdx.x;
+    const int r0 = blockIdx.x * 64;
+    for (int idx = tid; idx < NB * NB; idx += 256) Di[idx] = dinv[idx];
+    for (int idx = tid; idx < 64 * NB; idx += 256) {
+        const int r = idx % 64, c = idx / 64;
+        R[r + c * LDS] = (r0 + r < rows && c < nb) ? A21[(r0 + r) + (long long)c * lda] : 0.f;
+    }
+    __syncthreads();
+    // out(r, j) = sum_k R(r, k) Di(j, k)
+    for (int idx = tid; idx < 64 * nb; idx += 256) {
+        const int r = idx % 64, j = idx / 64;
+        float s = 0.f;
+        for (int k = 0; k <= j; k++) s += R[r + k * LDS] * Di[j + k * NB];
+        if (r0 + r < rows) A21[(r0 + r) + (long long)j * lda] = s;
+    }
+}
+
+// C(i, j) -= sum_k A(i, k) A(j, k), lower triangle, K <= 64: 64 x 64 output tiles.
+__global__ void __launch_bounds__(256) syrk_f32(int n2, int K, const float *A, long long lda, float *C, long long ldc) {
+    const int bi = blockIdx.x, bj = blockIdx.y;
+    if (bi < bj) return;
+    __shared__ float As[64 * LDS], Bs[64 * LDS];
+    const int tid = threadIdx.x;
+    for (int idx = tid; idx < 64 * 64; idx += 256) {
+        const int r = idx % 64, k = idx / 64;
+        As[r + k * LDS] = (bi * 64 + r < n2 && k < K) ? A[(bi * 64 + r) + (long long)k * lda] : 0.f;
+        Bs[r + k * LDS] = (bj * 64 + r < n2 && k < K) ? A[(bj * 64 + r) + (long long)k * lda] : 0.f;
+    }
+    __syncthreads();
+    const int tr = tid % 16, tc = tid / 16;   // 4 x 4 outputs per thread
+    float acc[4][4] = {};
+    for (int k = 0; k < K; k++) {
+        float a[4], b[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) { a[u] = As[tr + 16 * u + k * LDS]; b[u] = Bs[tc + 16 * u + k * LDS]; }
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+#pragma unroll
+            for (int v = 0; v < 4; v++) acc[u][v] += a[u] * b[v];
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+            const int i = bi * 64 + tr + 16 * u, j = bj * 64 + tc + 16 * v;
+            if (i < n2 && j < n2 && i >= j) C[i + (long long)j * ldc] -= acc[u][v];
+        }
+}
+
+// ---- persistent triangular solve -----------------------------------------------------------
+// trans = 0: solve L x = b (block rows top-down); trans = 1: solve L' x = b (bottom-up).
+template <typename T>
+__global__ void __launch_bounds__(256) trsv_kernel(int n, const T *L, long long lda, const T *dinv, T *x, int trans,
+                                                   int *flags, int epoch, int *err) {
+    __shared__ T acc[NB];
+    __shared__ T part[4][NB];
+    __shared__ T xc[NB];
+    __shared__ int bad;
+    const int tid = threadIdx.x;
+    const int nblk = (n + NB - 1) / NB;
+    const int r = trans ? (nblk - 1 - blockIdx.x) : blockIdx.x;   // the block row this CTA owns
+    const int r0 = r * NB, nr = min(NB, n - r0);
+    if (tid < NB) acc[tid] = (tid < nr) ? x[r0 + tid] : (T)0;
+    if (tid == 0) bad = 0;
+    __syncthreads();
+    const int row = tid & 63, q = tid >> 6;   // 4 threads per row, 16 columns each
+    const int ndep = trans ? (nblk - 1 - r) : r;
+    for (int d = 0; d < ndep; d++) {
+        const int c = trans ? (nblk - 1 - d) : d;   // dependencies in the order they finish
+        if (tid == 0) {
+            unsigned spins = 0;
+            while (ld_acquire(&flags[c]) != epoch) {
+                if (++spins > BGPU_SPIN_LIMIT) { bad = 1; break; }
+                __nanosleep(64);
+            }
+        }
+        __syncthreads();
+        if (bad) break;
+        const int c0 = c * NB, nc = min(NB, n - c0);
+        if (tid < NB) xc[tid] = (tid < nc) ? ((volatile T *)x)[c0 + tid] : (T)0;
+        __syncthreads();
+        T s = (T)0;
+        if (!trans) {   // acc(row) -= sum_col L(r0+row, c0+col) xc(col)
+            if (row < nr)
+                for (int k = q * 16; k < q * 16 + 16 && k < nc; k++) s += L[(r0 + row) + (long long)(c0 + k) * lda] * xc[k];
+        } else {        // acc(row) -= sum_col L(c0+col, r0+row) xc(col)
+            if (row < nr) {
+                const T *col = L + (long long)(r0 + row) * lda + c0;
+                for (int k = q * 16; k < q * 16 + 16 && k < nc; k++) s += col[k] * xc[k];
+            }
+        }
+        part[q][row] = s;
+        __syncthreads();
+        if (tid < NB) acc[tid] -= (part[0][tid] + part[1][tid]) + (part[2][tid] + part[3][tid]);
+        __syncthreads();
+    }
+    if (bad) {
+        if (tid == 0) atomicExch(err, 1);
+        return;
+    }
+    // x_r = Dinv_r acc (trans = 0) or Dinv_r' acc (trans = 1)
+    const T *D = dinv + (size_t)r * NB * NB;
+    T s = (T)0;
+    if (!trans) { for (int k = q * 16; k < q * 16 + 16; k++) s += D[row + k * NB] * acc[k]; }
+    else        { for (int k = q * 16; k < q * 16 + 16; k++) s += D[k + row * NB] * acc[k]; }
+    part[q][row] = s;
+    __syncthreads();
+    if (tid < nr) x[r0 + tid] = (part[0][tid] + part[1][tid]) + (part[2][tid] + part[3][tid]);
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) st_release(&flags[r], epoch);
+}
+
+template <typename T>
+int trsv_launch(cudaStream_t st, int n, const T *L, long long lda, const T *dinv, T *x, int trans, int *flags,
+                int epoch, int *d_err) {
+    if (n <= 0) return BGPU_OK;
+    const int nblk = (n + NB - 1) / NB;
+    static int max_coresident = -1;
+    if (max_coresident < 0) {
+        int dev = 0, nsm = 0, per = 0;
+        BGPU_CHECK(cudaGetDevice(&dev));
+        BGPU_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        BGPU_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, trsv_kernel<T>, 256, 0));
+        max_coresident = nsm * per;
+    }
+    if (nblk > max_coresident) return BGPU_ERR_TOOBIG;
+    void *args[] = {(void *)&n, (void *)&L, (void *)&lda, (void *)&dinv, (void *)&x, (void *)&trans,
+                    (void *)&flags, (void *)&epoch, (void *)&d_err};
+    BGPU_CHECK(cudaLaunchCooperativeKernel((void *)trsv_kernel<T>, dim3(nblk), dim3(256), args, 0, st));
+    BGPU_LAUNCH_CHECK();
+    return BGPU_OK;
+}
+
+// ---- element-wise helpers ---------------------------------------------------------------
+__global__ void set_identity_lower_kernel(int n, double *A, long long lda) {
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long)n * n) return;
+    const int i = (int)(idx % n), j = (int)(idx / n);
+    A[i + (long long)j * lda] = (i == j) ? 1.0 : 0.0;
+}
+
+__global__ void symv_full_kernel(int n, double alpha, const double *M, long long ldm, const double *x, double beta,
+                                 double *y) {
+    const int warps = blockDim.x >> 5;
+    const int col = blockIdx.x * warps + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (col >= n) return;
+    const double *c = M + (long long)col * ldm;
+    double s = 0.0;
+    for (int i = lane; i < n; i += 32) s += c[i] * x[i];
+    s = warp_sum(s);
+    if (lane == 0) y[col] = (beta == 0.0) ? alpha * s : alpha * s + beta * y[col];
+}
+
+__global__ void diag_scale_kernel(int m, const double *M, long long ldm, double *D) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    const double d = M[i + (long long)i * ldm];
+    D[i] = d > 0 ? 1.0 / sqrt(d) : 1.0;
+}
+
+__global__ void load_scaled_f64_kernel(int m, const double *M, long long ldm, const double *D, double reg, double *L,
+                                       long long ldl) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+    if (i >= m || i < j) return;
+    double v = M[i + (long long)j * ldm] * D[i] * D[j];
+    if (i == j) v += reg;
+    L[i + (long long)j * ldl] = v;
+}
+
+__global__ void load_scaled_f32_kernel(int m, const double *M, long long ldm, const double *D, float *F,
+                                       long long ldf) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+    if (i >= m || i < j) return;
+    const double v = M[i + (long long)j * ldm] * D[i] * D[j];
+    F[i + (long long)j * ldf] = (fabs(v) < 1e-30) ? 0.0f : (float)v;   // no subnormals in the float factor
+}
+
+__global__ void symmetrize_kernel(int n, double *A, long long lda) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+    if (i >= n || i <= j) return;
+    double *a = A + i + (long long)j * lda, *b = A + j + (long long)i * lda;
+    const double v = 0.5 * (*a + *b);
+    *a = v;
+    *b = v;
+}
+
+__global__ void lower_to_upper_kernel(int n, double *A, long long lda) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+    if (i >= n || i <= j) return;
+    A[j + (long long)i * lda] = A[i + (long long)j * lda];
+}
+
+// Deterministic two-level dot products: a fixed number of partial sums per pair.
+constexpr int DOT_PARTS = 128;
+__global__ void dots_partial_kernel(const double *const *a, const double *const *b, long long n, double *scratch) {
+    const int q = blockIdx.y, part = blockIdx.x;
+    const double *x = a[q], *y = b[q];
+    const long long chunk = (n + DOT_PARTS - 1) / DOT_PARTS;
+    const long long lo = part * chunk, hi = min(n, lo + chunk);
+    double s = 0.0;
+    for (long long i = lo + threadIdx.x; i < hi; i += blockDim.x) s += x[i] * y[i];
+    __shared__ double red[8];
+    s = warp_sum(s);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += red[w];
+        scratch[(long long)q * DOT_PARTS + part] = t;
+    }
+}
+__global__ void dots_final_kernel(const double *scratch, double *out) {
+    const int q = blockIdx.x;
+    double s = 0.0;
+    for (int i = threadIdx.x; i < DOT_PARTS; i += 32) s += scratch[(long long)q * DOT_PARTS + i];
+    s = warp_sum(s);
+    if (threadIdx.x == 0) out[q] = s;
+}
+}  // namespace
+
+// ---- host launchers -------------------------------------------------------------------------
+template <typename T>
+int diag_smem_attr() {
+    static bool done = false;
+    if (!done) {
+        BGPU_CHECK(cudaFuncSetAttribute(potrf_diag_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)(2 * NB * LDS * sizeof(T))));
+        done = true;
+    }
+    return BGPU_OK;
+}
+
+int potrf_f64(cudaStream_t st, int n, double *A, long long lda, double *dinv, int *d_info, double *d_pmin) {
+    if (int rc = diag_smem_attr<double>()) return rc;
+    init_info_kernel<<<1, 1, 0, st>>>(d_info, d_pmin);
+    BGPU_LAUNCH_CHECK();
+    for (int j0 = 0; j0 < n; j0 += NB) {
+        const int nb = (n - j0 < NB) ? n - j0 : NB;
+        potrf_diag_kernel<double><<<1, 256, 2 * NB * LDS * sizeof(double), st>>>(n, A, lda, j0, dinv + (size_t)(j0 / NB) * NB * NB, d_info, d_pmin);
+        BGPU_LAUNCH_CHECK();
+        const int rest = n - j0 - nb;
+        if (rest <= 0) break;
+        double *A21 = A + (j0 + nb) + (long long)j0 * lda;
+        double *A22 = A + (j0 + nb) + (long long)(j0 + nb) * lda;
+        const double *Di = dinv + (size_t)(j0 / NB) * NB * NB;
+        // A21 <- A21 Di'  (B(k, j) = Di(j, k) = Di[j + k*NB]: N-major); in place, N = nb <= 64
+        int rc = gemm_f64(st, 0, 0, rest, nb, nb, 1.0, A21, lda, 0, Di, NB, 0, 0.0, A21, lda, 0, 1, 0);
+        if (rc) return rc;
+        // A22 <- A22 - A21 A21'  (lower)
+        rc = gemm_f64(st, 0, 0, rest, rest, nb, -1.0, A21, lda, 0, A21, lda, 0, 1.0, A22, lda, 0, 1, 1);
+        if (rc) return rc;
+    }
+    return BGPU_OK;
+}
+
+int potrf_f32(cudaStream_t st, int n, float *A, long long lda, float *dinv, int *d_info, double *d_pmin) {
+    if (int rc = diag_smem_attr<float>()) return rc;
+    init_info_kernel<<<1, 1, 0, st>>>(d_info, d_pmin);
+    BGPU_LAUNCH_CHECK();
+    for (int j0 = 0; j0 < n; j0 += NB) {
+        const int nb = (n - j0 < NB) ? n - j0 : NB;
+        potrf_diag_kernel<float><<<1, 256, 2 * NB * LDS * sizeof(float), st>>>(n, A, lda, j0, dinv + (size_t)(j0 / NB) * NB * NB, d_info, d_pmin);
+        BGPU_LAUNCH_CHECK();
+        const int rest = n - j0 - nb;
+        if (rest <= 0) break;
+        float *A21 = A + (j0 + nb) + (long long)j0 * lda;
+        float *A22 = A + (j0 + nb) + (long long)(j0 + nb) * lda;
+        trsm_panel_f32<<<ceil_div(rest, 64), 256, 0, st>>>(rest, nb, A21, lda, dinv + (size_t)(j0 / NB) * NB * NB);
+        BGPU_LAUNCH_CHECK();
+        const int t = ceil_div(rest, 64);
+        syrk_f32<<<dim3(t, t), 256, 0, st>>>(rest, nb, A21, lda, A22, lda);
+        BGPU_LAUNCH_CHECK();
+    }
+    return BGPU_OK;
+}
+
+int trsv_f64(cudaStream_t st, int n, const double *L, long long lda, const double *dinv, double *x, int trans,
+             int *flags, int epoch, int *d_err) {
+    return trsv_launch<double>(st, n, L, lda, dinv, x, trans, flags, epoch, d_err);
+}
+int trsv_f32(cudaStream_t st, int n, const float *L, long long lda, const float *dinv, float *x, int trans,
+             int *flags, int epoch, int *d_err) {
+    return trsv_launch<float>(st, n, L, lda, dinv, x, trans, flags, epoch, d_err);
+}
+
+int trtri_f64(cudaStream_t st, int n, const double *L, long long lda, const double *dinv, double *Linv,
+              long long ldi) {
+    // Solve L X = I by block rows: X_i = Dinv_i B_i, then B_below -= L(below, i) X_i.
+    set_identity_lower_kernel<<<ceil_div((long long)n * n, 256), 256, 0, st>>>(n, Linv, ldi);
+    BGPU_LAUNCH_CHECK();
+    for (int i0 = 0; i0 < n; i0 += NB) {
+        const int nb = (n - i0 < NB) ? n - i0 : NB;
+        const int ncols = i0 + nb;   // columns 0..i0+nb-1 can be nonzero in block row i
+        double *Xi = Linv + i0;      // rows i0.., all columns (ld ldi)
+        // X_i <- Dinv_i X_i  (A = Dinv: A(r, k) = Dinv[r + k*NB], M-major; B = X_i K-major rows) in place, M <= 128
+        int rc = gemm_f64(st, 0, 1, nb, ncols, nb, 1.0, dinv + (size_t)(i0 / NB) * NB * NB, NB, 0, Xi, ldi, 0, 0.0,
+                          Xi, ldi, 0, 1, 0);
+        if (rc) return rc;
+        const int below = n - i0 - nb;
+        if (below <= 0) break;
+        // X_below -= L(below, i) X_i : A = L(i0+nb.., i0..) M-major, B(k, j) = X_i[k + j*ldi] K-major
+        rc = gemm_f64(st, 0, 1, below, ncols, nb, -1.0, L + (i0 + nb) + (long long)i0 * lda, lda, 0, Xi, ldi, 0, 1.0,
+                      Linv + (i0 + nb), ldi, 0, 1, 0);
+        if (rc) return rc;
+    }
+    return BGPU_OK;
+}
+
+int symv_full_f64(cudaStream_t st, int n, double alpha, const double *M, long long ldm, const double *x, double beta,
+                  double *y) {
+    symv_full_kernel<<<ceil_div(n, 8), 256, 0, st>>>(n, alpha, M, ldm, x, beta, y);
+    BGPU_LAUNCH_CHECK();
+    return BGPU_OK;
+}
+
+int schur_load_f64(cudaStream_t st, int m, const double *M, long long ldm, double reg, double *d_D, double *L,
+                   long long ldl) {
+    diag_scale_kernel<<<ceil_div(m, 256), 256, 0, st>>>(m, M, ldm, d_D);
+    BGPU_LAUNCH_CHECK();
+    load_scaled_f64_kernel<<<dim3(ceil_div(m, 256), m), 256, 0, st>>>(m, M, ldm, d_D, reg, L, ldl);
+    BGPU_LAUNCH_CHECK();
+    return BGPU_OK;
+}
+
+int schur_load_f32(cudaStream_t st, int m, const double *M, long long ldm, double *d_D, float *Mf, long long ldf) {
+    diag_scale_kernel<<<ceil_div(m, 256), 256, 0, st>>>(m, M, ldm, d_D);
+    BGPU_LAUNCH_CHECK();
+    load_scaled_f32_kernel<<<dim3(ceil_div(m, 256), m), 256, 0, st>>>(m, M, ldm, d_D, Mf, ldf);
+    BGPU_LAUNCH_CHECK();
+    return BGPU_OK;
+}
+
+int symmetrize_f64(cudaStream_t st, int n, double *A, long long lda) {
+    symmetrize_kernel<<<dim3(ceil_div(n, 128), n), 128, 0, st>>>(n, A, lda);
+    BGPU_LAUNCH_CHECK();
+    return BGPU_OK;
+}
+
+int copy_lower_to_upper_f64(cudaStream_t st, int n, double *A, long long lda) {
+    lower_to_upper_kernel<<<dim3(ceil_div(n, 128), n), 128, 0, st>>>(n, A, lda);
+    BGPU_LAUNCH_CHECK();
+    return BGPU_OK;
+}
+
+int dots_f64(cudaStream_t st, int nq, const double *const *a, const double *const *b, long long n, double *out,
+             double *scratch) {
+    if (nq <= 0) return BGPU_OK;
+    dots_partial_kernel<<<dim3(DOT_PARTS, nq), 256, 0, st>>>(a, b, n, scratch);
+    BGPU_LAUNCH_CHECK();
+    dots_final_kernel<<<nq, 32, 0, st>>>(scratch, out);
+    BGPU_LAUNCH_CHECK();
+    return BGPU_OK;
+}

@@ -1,0 +1,75 @@
+// Element-wise kernels over the n x n iterate arrays of a block (X, Z, dX, dZ, R0, ...).
+#include "common.cuh"
+#include "kernels.h"
+#include "elementwise.h"
+
+namespace {
+__global__ void lincomb_kernel(long long n, double a, const double *x, double b, const double *y, double c,
+                               const double *z, double *out) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double v = 0.0;
+    if (x) v += a * x[i];
+    if (y) v += b * y[i];
+    if (z) v += c * z[i];
+    out[i] = v;
+}
+__global__ void add_diag_kernel(int n, double *A, long long lda, double v) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) A[i + (long long)i * lda] += v;
+}
+__global__ void step_copy_kernel(long long n, double inc, const double *dV, double *V, double *L) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double v = V[i] + inc * dV[i];
+    V[i] = v;
+    L[i] = v;
+}
+__global__ void set_diag_matrix_kernel(int n, double *A, double v) {
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long)n * n) return;
+    const int i = (int)(idx % n), j = (int)(idx / n);
+    A[idx] = (i == j) ? v : 0.0;
+}
+// sym: out = 0.5 (G + G') + a*x + b*y  (x or y may be null)
+__global__ void sym_lincomb_kernel(int n, const double *G, double s, double a, const double *x, double b,
+                                   const double *y, double *out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+    if (i >= n) return;
+    const long long p = i + (long long)j * n, q = j + (long long)i * n;
+    double v = s * 0.5 * (G[p] + G[q]);
+    if (x) v += a * x[p];
+    if (y) v += b * y[p];
+    out[p] = v;
+}
+}  // namespace
+
+int ew_lincomb(cudaStream_t st, long long n, double a, const double *x, double b, const double *y, double c,
+               const double *z, double *out) {
+    if (n <= 0) return BGPU_OK;
+    lincomb_kernel<<<ceil_div(n, 256), 256, 0, st>>>(n, a, x, b, y, c, z, out);
+    BGPU_LAUNCH_CHECK();
+    return BGPU_OK;
+}
+int ew_add_diag(cudaStream_t st, int n, double *A, long long lda, double v) {
+    add_diag_kernel<<<ceil_div(n, 256), 256, 0, st>>>(n, A, lda, v);
+    BGPU_LAUNCH_CHECK();
+    return BGPU_OK;
+}
+int ew_step_copy(cudaStream_t st, long long n, double inc, const double *dV, double *V, double *L) {
+    step_copy_kernel<<<ceil_div(n, 256), 256, 0, st>>>(n, inc, dV, V, L);
+    BGPU_LAUNCH_CHECK();
+    return BGPU_OK;
+}
+int ew_set_scaled_identity(cudaStream_t st, int n, double *A, double v) {
+    set_diag_matrix_kernel<<<ceil_div((long long)n * n, 256), 256, 0, st>>>(n, A, v);
+    BGPU_LAUNCH_CHECK();
+    return BGPU_OK;
+}
+int ew_sym_lincomb(cudaStream_t st, int n, const double *G, double s, double a, const double *x, double b,
+                   const double *y, double *out) {
+    // out may alias x or y but not G (G is read at both (i,j) and (j,i))
+    sym_lincomb_kernel<<<dim3(ceil_div(n, 128), n), 128, 0, st>>>(n, G, s, a, x, b, y, out);
+    BGPU_LAUNCH_CHECK();
+    return BGPU_OK;
+}

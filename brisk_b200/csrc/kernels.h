@@ -1,0 +1,85 @@
+// Internal host-side launchers of the Newton-step kernels (not exported; include/bgpu.h is
+// the C ABI).  All device pointers; every launcher returns a BGPU_* status.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+// ---- GEMM (gemm_f64.cu) ----------------------------------------------------------------
+int gemm_f64(cudaStream_t st, int a_kmajor, int b_kmajor, int M, int N, int K, double alpha, const double *A,
+             long long lda, long long sA, const double *B, long long ldb, long long sB, double beta, double *C,
+             long long ldc, long long sC, int batch, int lower);
+int scale_matrix_f64(cudaStream_t st, int M, int N, double beta, double *C, long long ldc, long long sC, int batch,
+                     int lower);
+
+// ---- dense factor / solves (dense.cu) -----------------------------------------------------
+constexpr int TRI_NB = 64;   // diagonal block order of the blocked factor and solves
+
+// Blocked right-looking Cholesky of the lower triangle of A (n x n, column-major, lda), in
+// place.  Writes the inverses of the 64 x 64 diagonal blocks of L to dinv (ceil(n/64) blocks of
+// 64*64, column-major), the first failing column (1-based, 0 when none) to *d_info and the
+// smallest squared pivot to *d_pmin (both device scalars, reset here).
+int potrf_f64(cudaStream_t st, int n, double *A, long long lda, double *dinv, int *d_info, double *d_pmin);
+int potrf_f32(cudaStream_t st, int n, float *A, long long lda, float *dinv, int *d_info, double *d_pmin);
+
+// Persistent flag-chained triangular solves with the factor of potrf_*: x <- L^{-1} x (trans=0)
+// or x <- L^{-T} x (trans=1), one right-hand side.  flags: ceil(n/64) ints, epoch: a value not
+// used by an earlier call on the same flags; d_err is set to 1 when a wait gives up.
+int trsv_f64(cudaStream_t st, int n, const double *L, long long lda, const double *dinv, double *x, int trans,
+             int *flags, int epoch, int *d_err);
+int trsv_f32(cudaStream_t st, int n, const float *L, long long lda, const float *dinv, float *x, int trans,
+             int *flags, int epoch, int *d_err);
+
+// Lower triangular inverse: Linv <- L^{-1} (n x n, column-major), using the diagonal-block
+// inverses of potrf_f64.  The strict upper triangle of Linv is set to zero.
+int trtri_f64(cudaStream_t st, int n, const double *L, long long lda, const double *dinv, double *Linv,
+              long long ldi);
+
+// y = alpha M x + beta y, M symmetric and stored in full (column-major, ldm).
+int symv_full_f64(cudaStream_t st, int n, double alpha, const double *M, long long ldm, const double *x, double beta,
+                  double *y);
+
+// Equilibrated copy for the factor: L = D M D + reg I (lower triangle; D = diag(M)^{-1/2},
+// computed here into d_D), and the float variant writing Mf.
+int schur_load_f64(cudaStream_t st, int m, const double *M, long long ldm, double reg, double *d_D, double *L,
+                   long long ldl);
+int schur_load_f32(cudaStream_t st, int m, const double *M, long long ldm, double *d_D, float *Mf, long long ldf);
+
+// ---- vector and matrix element-wise helpers (dense.cu) -----------------------------------
+// Deterministic sums: out[q] = sum_i a_q[i] * b_q[i] for `nq` pairs of length n (one launch),
+// written to the device array out.
+int dots_f64(cudaStream_t st, int nq, const double *const *a, const double *const *b, long long n, double *out,
+             double *scratch);
+int symmetrize_f64(cudaStream_t st, int n, double *A, long long lda);
+int copy_lower_to_upper_f64(cudaStream_t st, int n, double *A, long long lda);
+
+// ---- Schur complement assembly (schur.cu) -------------------------------------------------
+struct DevBlock {
+    int n = 0;              // block order
+    int ncon = 0;           // constraints that touch the block
+    long long ne = 0;       // entries of the full (both triangles) expansion
+    int *con = nullptr;     // [ncon] global constraint index
+    long long *cptr = nullptr;  // [ncon+1] constraint-major offsets
+    int *cpos = nullptr;    // [ne] position p + q*n, ascending within a constraint
+    double *cval = nullptr; // [ne]
+    long long *pptr = nullptr;  // [n*n+1] position-major offsets
+    int *pcon = nullptr;    // [ne] global constraint index of each position-major entry
+    double *pval = nullptr; // [ne]
+    double *C = nullptr;    // dense n x n (scaled)
+};
+
+// out[con[t]] = beta*out[con[t]] + alpha * <A_t, D>  for every constraint of the block.
+int aop_f64(cudaStream_t st, const DevBlock &B, const double *D, double alpha, double beta, double *out);
+// F = alpha * sum_i y_i A_i + beta * F (full n x n).
+int atop_f64(cudaStream_t st, const DevBlock &B, const double *y, double alpha, double beta, double *F);
+
+// Workspace of the row-product assembly, sized by schur_ws_bytes.
+struct SchurWs {
+    void *buf = nullptr;
+    size_t bytes = 0;
+};
+size_t schur_ws_bytes(int n, int chunk, int precision);
+int schur_chunk_default(int n, int precision);
+// M (m x m, column-major, full symmetric) += the block's contribution sum over its constraints
+// of M_ab = <A_b, X A_a Zi>.  precision 0: FP64 (DMMA), 1: 3xTF32 (tcgen05).
+int schur_assemble(cudaStream_t st, const DevBlock &B, const double *X, const double *Zi, double *M, int m,
+                   int precision, int chunk, void *ws, size_t ws_bytes);

@@ -1,0 +1,232 @@
+// Schur complement assembly and the constraint operators A(.) and A'(.).
+//
+// Row-product route (the reference's route 1, schur_sdp_id, solver.c:2416-2625 / 2670-2960):
+// for each constraint a of a block, G_a = X A_a Z^-1 and M_ba = <A_b, G_a> for every b >= a.
+// B200 form, per chunk of K consecutive constraints a0..a0+K-1:
+//   1. tprod:  T[(q*K + t), k] = (Zi A_a)[q, k]          (a = a0 + t; sparse A_a, dense Zi)
+//   2. GEMM:   G[(q*K + t), p] = sum_k T[(q*K+t), k] X[k, p]  = G_a[p, q]
+//              one DMMA GEMM of (n K) x n x n, X shared by the whole chunk (L2-resident)
+//   3. gather: M[a, b] = sum_{(p,q) in A_b} A_b[p,q] G_a[p,q] for the K constraints of the chunk
+//              at once: G is stored (p, q, t) with t fastest, so an entry of A_b reads K
+//              contiguous values (one coalesced line for the warp) instead of K scattered ones.
+// Because every A_b is symmetric, sum A_b[p,q] G_a[p,q] = sum A_b[p,q] G_a[q,p]; the gather
+// indexes G by the entry's column-major position pos = p + q n directly.
+// M is written in full (both triangles): the symmetric product of the FP64 residual, the
+// equilibration and the factor copies read it without a transpose.
+#include "common.cuh"
+#include "kernels.h"
+#include "tf32x3.h"
+
+namespace {
+constexpr int TP_Q = 32, TP_K = 128, TP_LD = TP_K + 1;
+
+template <typename OutT>
+__global__ void __launch_bounds__(256) tprod_kernel(int n, int K, int a0, int ncon, const long long *__restrict__ cptr,
+                                                   const int *__restrict__ cpos, const double *__restrict__ cval,
+                                                   const double *__restrict__ Zi, OutT *__restrict__ T,
+                                                   OutT *__restrict__ Tlo) {
+    __shared__ double tile[TP_Q * TP_LD];
+    __shared__ long long rng[2];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int k0 = blockIdx.x * TP_K, q0 = blockIdx.y * TP_Q, t = blockIdx.z;
+    const int a = a0 + t;
+    for (int idx = tid; idx < TP_Q * TP_LD; idx += 256) tile[idx] = 0.0;
+    if (tid == 0) {
+        long long lo = 0, hi = 0;
+        if (a < ncon) {
+            const long long s = cptr[a], e = cptr[a + 1];
+            const long long plo = (long long)k0 * n, phi = (long long)min(k0 + TP_K, n) * n;
+            long long L = s, R = e;   // first entry with pos >= plo
+            while (L < R) { long long mid = (L + R) >> 1; if ((long long)cpos[mid] < plo) L = mid + 1; else R = mid; }
+            lo = L;
+            R = e;                    // first entry with pos >= phi
+            while (L < R) { long long mid = (L + R) >> 1; if ((long long)cpos[mid] < phi) L = mid + 1; else R = mid; }
+            hi = L;
+        }
+        rng[0] = lo;
+        rng[1] = hi;
+    }
+    __syncthreads();
+    const long long lo = rng[0], hi = rng[1];
+    const int q = q0 + lane;
+    for (long long e = lo; e < hi; e++) {
+        const int pos = cpos[e];
+        const int k = pos / n, pp = pos - k * n;
+        if (((k - k0) & 7) != warp) continue;       // one warp per column class: no smem races
+        if (q < n) tile[lane * TP_LD + (k - k0)] += cval[e] * Zi[q + (long long)pp * n];
+    }
+    __syncthreads();
+    // rows (q, t) of T, k contiguous
+    const int kw = min(TP_K, n - k0);
+    for (int idx = tid; idx < TP_Q * TP_K; idx += 256) {
+        const int r = idx / TP_K, kk = idx % TP_K;
+        if (q0 + r < n && kk < kw) {
+            const double v = tile[r * TP_LD + kk];
+            const long long o = ((long long)(q0 + r) * K + t) * n + k0 + kk;
+            if (sizeof(OutT) == 8) {
+                T[o] = (OutT)v;
+            } else {
+                const float hi_ = tf32_round((float)v);
+                T[o] = (OutT)hi_;
+                Tlo[o] = (OutT)tf32_round((float)(v - (double)hi_));
+            }
+        }
+    }
+}
+
+// One warp group of LPG lanes per constraint b; each lane holds K / LPG of the chunk's K columns.
+template <int K, typename GT>
+__global__ void __launch_bounds__(256) gather_kernel(int a0, int ncon, int m, const int *__restrict__ con,
+                                                    const long long *__restrict__ cptr, const int *__restrict__ cpos,
+                                                    const double *__restrict__ cval, const GT *__restrict__ G,
+                                                    double *M) {
+    constexpr int LPG = K < 32 ? K : 32;       // lanes per constraint group
+    constexpr int GPW = 32 / LPG;              // groups per warp (entry split)
+    constexpr int PER = K / LPG;               // columns per lane
+    const int lane = threadIdx.x & 31;
+    const int b = a0 + blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (b >= ncon) return;
+    const int sub = lane / LPG, l = lane % LPG;
+    double acc[PER];
+#pragma unroll
+    for (int u = 0; u < PER; u++) acc[u] = 0.0;
+    const long long s = cptr[b], e = cptr[b + 1];
+    for (long long base = s; base < e; base += 32) {
+        const long long my = base + lane;
+        int pos = 0;
+        double v = 0.0;
+        if (my < e) { pos = cpos[my]; v = cval[my]; }
+        const int cnt = (int)min((long long)32, e - base);
+        for (int j = 0; j < cnt; j += GPW) {   // uniform trip count: every lane shuffles together
+            const int jj = j + sub;
+            const int src = jj < cnt ? jj : 0;
+            const int pj = __shfl_sync(0xffffffffu, pos, src);
+            const double vj = __shfl_sync(0xffffffffu, v, src);
+            if (jj < cnt) {
+                const GT *g = G + (long long)pj * K;
+#pragma unroll
+                for (int u = 0; u < PER; u++) acc[u] += vj * (double)g[l + u * LPG];
+            }
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < PER; u++)
+#pragma unroll
+        for (int o = LPG; o < 32; o <<= 1) acc[u] += __shfl_xor_sync(0xffffffffu, acc[u], o);
+    if (sub != 0) return;
+    const int cb = con[b];
+#pragma unroll
+    for (int u = 0; u < PER; u++) {
+        const int a = a0 + l + u * LPG;
+        if (a < ncon && a <= b) {
+            const int ca = con[a];
+            M[(long long)ca + (long long)cb * m] += acc[u];
+            if (ca != cb) M[(long long)cb + (long long)ca * m] += acc[u];
+        }
+    }
+}
+
+template <typename GT>
+int gather_launch(cudaStream_t st, int K, int a0, int ncon, int m, const DevBlock &B, const GT *G, double *M) {
+    const int nb = ncon - a0;
+    if (nb <= 0) return BGPU_OK;
+    dim3 grid(ceil_div(nb, 8));
+    switch (K) {
+        case 8: gather_kernel<8, GT><<<grid, 256, 0, st>>>(a0, ncon, m, B.con, B.cptr, B.cpos, B.cval, G, M); break;
+        case 16: gather_kernel<16, GT><<<grid, 256, 0, st>>>(a0, ncon, m, B.con, B.cptr, B.cpos, B.cval, G, M); break;
+        case 32: gather_kernel<32, GT><<<grid, 256, 0, st>>>(a0, ncon, m, B.con, B.cptr, B.cpos, B.cval, G, M); break;
+        case 64: gather_kernel<64, GT><<<grid, 256, 0, st>>>(a0, ncon, m, B.con, B.cptr, B.cpos, B.cval, G, M); break;
+        default: return BGPU_ERR_ARG;
+    }
+    BGPU_LAUNCH_CHECK();
+    return BGPU_OK;
+}
+
+__global__ void aop_kernel(int ncon, const int *__restrict__ con, const long long *__restrict__ cptr,
+                           const int *__restrict__ cpos, const double *__restrict__ cval, const double *__restrict__ D,
+                           double alpha, double beta, double *out) {
+    const int t = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (t >= ncon) return;
+    double s = 0.0;
+    for (long long e = cptr[t] + lane; e < cptr[t + 1]; e += 32) s += cval[e] * D[cpos[e]];
+    s = warp_sum(s);
+    if (lane == 0) {
+        const int c = con[t];
+        out[c] = (beta == 0.0) ? alpha * s : alpha * s + beta * out[c];
+    }
+}
+
+__global__ void atop_kernel(long long npos, const long long *__restrict__ pptr, const int *__restrict__ pcon,
+                            const double *__restrict__ pval, const double *__restrict__ y, double alpha, double beta,
+                            double *F) {
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npos) return;
+    double s = 0.0;
+    for (long long e = pptr[p]; e < pptr[p + 1]; e++) s += pval[e] * y[pcon[e]];
+    F[p] = (beta == 0.0) ? alpha * s : alpha * s + beta * F[p];
+}
+}  // namespace
+
+int aop_f64(cudaStream_t st, const DevBlock &B, const double *D, double alpha, double beta, double *out) {
+    if (B.ncon <= 0) return BGPU_OK;
+    aop_kernel<<<ceil_div(B.ncon, 8), 256, 0, st>>>(B.ncon, B.con, B.cptr, B.cpos, B.cval, D, alpha, beta, out);
+    BGPU_LAUNCH_CHECK();
+    return BGPU_OK;
+}
+
+int atop_f64(cudaStream_t st, const DevBlock &B, const double *y, double alpha, double beta, double *F) {
+    const long long npos = (long long)B.n * B.n;
+    atop_kernel<<<ceil_div(npos, 256), 256, 0, st>>>(npos, B.pptr, B.pcon, B.pval, y, alpha, beta, F);
+    BGPU_LAUNCH_CHECK();
+    return BGPU_OK;
+}
+
+int schur_chunk_default(int n, int precision) {
+    // the chunk's G (n^2 K values) should stay L2-resident during the gather
+    const double gbytes = (double)n * n * (precision == 0 ? 8.0 : 4.0);
+    int K = 64;
+    while (K > 8 && gbytes * K > 48e6) K >>= 1;
+    return K;
+}
+
+size_t schur_ws_bytes(int n, int chunk, int precision) {
+    const size_t nn = (size_t)n * n * chunk;
+    if (precision == 0) return 2 * nn * sizeof(double);            // T, G
+    return 4 * nn * sizeof(float) + 2 * (size_t)n * n * sizeof(float);   // T hi/lo, G (float), X hi/lo
+}
+
+int schur_assemble(cudaStream_t st, const DevBlock &B, const double *X, const double *Zi, double *M, int m,
+                   int precision, int chunk, void *ws, size_t ws_bytes) {
+    const int n = B.n, K = chunk;
+    if (B.ncon <= 0) return BGPU_OK;
+    if (K != 8 && K != 16 && K != 32 && K != 64) return BGPU_ERR_ARG;
+    if (ws_bytes < schur_ws_bytes(n, K, precision)) return BGPU_ERR_ARG;
+    const size_t nnK = (size_t)n * n * K;
+    dim3 tgrid(ceil_div(n, TP_K), ceil_div(n, TP_Q), K);
+    if (precision == 0) {
+        double *T = (double *)ws, *G = T + nnK;
+        for (int a0 = 0; a0 < B.ncon; a0 += K) {
+            tprod_kernel<double><<<tgrid, 256, 0, st>>>(n, K, a0, B.ncon, B.cptr, B.cpos, B.cval, Zi, T, nullptr);
+            BGPU_LAUNCH_CHECK();
+            int rc = gemm_f64(st, 1, 1, n * K, n, n, 1.0, T, n, 0, X, n, 0, 0.0, G, (long long)n * K, 0, 1, 0);
+            if (rc) return rc;
+            rc = gather_launch<double>(st, K, a0, B.ncon, m, B, G, M);
+            if (rc) return rc;
+        }
+        return BGPU_OK;
+    }
+    // 3xTF32: T and X split into tf32 hi + lo parts; G accumulated in FP32 on the tensor cores
+    float *Th = (float *)ws, *Tl = Th + nnK, *G = Tl + nnK, *Xh = G + nnK, *Xl = Xh + (size_t)n * n;
+    int rc = split_tf32(st, (long long)n * n, X, Xh, Xl);
+    if (rc) return rc;
+    for (int a0 = 0; a0 < B.ncon; a0 += K) {
+        tprod_kernel<float><<<tgrid, 256, 0, st>>>(n, K, a0, B.ncon, B.cptr, B.cpos, B.cval, Zi, Th, Tl);
+        BGPU_LAUNCH_CHECK();
+        rc = gemm_tf32x3(st, n * K, n, n, Th, Tl, n, Xh, Xl, n, G, (long long)n * K);
+        if (rc) return rc;
+        rc = gather_launch<float>(st, K, a0, B.ncon, m, B, G, M);
+        if (rc) return rc;
+    }
+    return BGPU_OK;
+}

@@ -1,0 +1,1346 @@
+// The infeasible-start primal-dual interior-point loop (HKM direction, Mehrotra predictor-
+// corrector) with every O(n^3), O(m^2 n) and O(m^3) step on the GPU.
+//
+// The loop follows the reference's infeasible-start method, brisk_solve_body
+// (solver.c:14394-15188), step by step:
+//   Z^-1 from the factor of Z                               (solver.c:14397-14421)
+//   residuals, objectives, stopping and infeasibility tests (solver.c:14423-14612)
+//   the dual residual kept as theta R0, with a re-base      (solver.c:14317-14326, 14587-14607)
+//   Schur complement M, its factor                          (solver.c:14652-14672)
+//   rhs pieces a0 = A(Z^-1), h = A(Z^-1 theta R0 X)         (solver.c:14715-14735)
+//   predictor, step lengths, sigma, gamma                   (solver.c:14787-14873)
+//   corrector and the refinement of A(dX) = rp              (solver.c:14998-15105)
+//   step lengths, catastrophe guard, try_step, y update     (solver.c:15108-15188)
+// and the reference's problem scaling (problem_prepare, problem.c:1866-1910), starting point
+// (start_sdpt3, solver.c:6622-6661), Schur factor rules (schur_factor_, solver.c:5296-5421),
+// PCG solve (schur_solve_, solver.c:5483-5621), Lanczos step length (sdp_maxstep_lam,
+// solver.c:6083-6225), try_step (solver.c:6393-6447) and DIMACS errors on the data as given
+// (postsolve.c:2880-2897, main.c:2349-2362).  Vectors of length m live on the host (their
+// work is O(m)); the n x n block arrays and the m x m Schur complement stay in HBM.
+#include "common.cuh"
+#include "elementwise.h"
+#include "kernels.h"
+#include "solver.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstring>
+#include <map>
+
+namespace bsolve {
+
+static double wtime() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+const char *status_string(int s) {
+    switch (s) {
+        case 0: return "OPTIMAL";
+        case 1: return "PRIMAL INFEASIBLE";
+        case 2: return "DUAL INFEASIBLE";
+        case 3: return "ITERATION LIMIT";
+        case 4: return "NUMERICAL DIFFICULTIES";
+        case 5: return "REDUCED ACCURACY";
+        case 6: return "TIME LIMIT";
+        default: return "NOT SOLVED";
+    }
+}
+int exit_code_of(int s) {
+    switch (s) {
+        case 0: return 0;
+        case 5: return 10;
+        case 1: return 11;
+        case 2: return 12;
+        case 3: return 13;
+        case 4: return 14;
+        case 6: return 15;
+        default: return 14;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// host problem (scaled)
+// ---------------------------------------------------------------------------------------------
+struct HBlock {
+    int n = 0;
+    std::vector<int> con;                 // global constraint ids (ascending)
+    std::vector<long long> cptr;          // per local constraint, into cpos/cval (full expansion)
+    std::vector<int> cpos;
+    std::vector<double> cval;
+    std::vector<int> Cpos;                // C, full expansion
+    std::vector<double> Cval;
+};
+
+struct HProblem {
+    int m = 0;
+    std::vector<HBlock> blk;
+    std::vector<double> b, b0;            // scaled, as given
+    std::vector<double> d, du;
+    double bs = 1, cs = 1, normb1 = 0, normb2 = 0, normC1 = 0, normC2 = 0;
+    long long Ntot = 0;
+};
+
+static int build_problem(const InputData &in, HProblem &P, std::string &err) {
+    P.m = in.m;
+    P.b0 = in.c;
+    P.b = in.c;
+    const int nb = in.nblk;
+    P.blk.resize(nb);
+    for (int k = 0; k < nb; k++) {
+        if (in.bs[k] <= 0) { err = "LP (negative size) blocks are not supported by this build"; return 2; }
+        P.blk[k].n = in.bs[k];
+        P.Ntot += in.bs[k];
+    }
+    // entries grouped by block, then by (mat, column, row); duplicates summed
+    struct E { int mat, p, q; double v; };
+    std::vector<std::vector<E>> per(nb);
+    const size_t nnz = in.v.size();
+    for (size_t e = 0; e < nnz; e++) {
+        const int k = in.blk[e] - 1, mt = in.mat[e];
+        if (k < 0 || k >= nb || mt < 0 || mt > in.m) { err = "entry out of range"; return 2; }
+        const int n = P.blk[k].n;
+        int i = in.i[e] - 1, j = in.j[e] - 1;
+        if (i < 0 || j < 0 || i >= n || j >= n) { err = "entry index out of the block"; return 2; }
+        if (i > j) std::swap(i, j);
+        per[k].push_back({mt, i, j, in.v[e]});
+    }
+    std::vector<double> nrm2(P.m, 0.0);
+    double c2 = 0, c1 = 0;
+    for (int k = 0; k < nb; k++) {
+        HBlock &B = P.blk[k];
+        const int n = B.n;
+        auto &L = per[k];
+        std::stable_sort(L.begin(), L.end(), [](const E &a, const E &b) {
+            if (a.mat != b.mat) return a.mat < b.mat;
+            if (a.q != b.q) return a.q < b.q;
+            return a.p < b.p;
+        });
+        std::vector<E> U;   // merged
+        for (const E &e : L) {
+            if (!U.empty() && U.back().mat == e.mat && U.back().p == e.p && U.back().q == e.q) U.back().v += e.v;
+            else U.push_back(e);
+        }
+        // full expansion per matrix, sorted by position p + q n
+        size_t s = 0;
+        B.cptr.push_back(0);
+        while (s < U.size()) {
+            size_t t = s;
+            while (t < U.size() && U[t].mat == U[s].mat) t++;
+            std::vector<std::pair<int, double>> full;
+            for (size_t u = s; u < t; u++) {
+                if (U[u].v == 0.0) continue;
+                full.push_back({U[u].p + U[u].q * n, U[u].v});
+                if (U[u].p != U[u].q) full.push_back({U[u].q + U[u].p * n, U[u].v});
+            }
+            std::sort(full.begin(), full.end());
+            if (!full.empty()) {
+                if (U[s].mat == 0) {
+                    for (auto &f : full) {
+                        B.Cpos.push_back(f.first);
+                        B.Cval.push_back(-f.second);   // C = -F0
+                        c2 += f.second * f.second;
+                        c1 += std::fabs(f.second);
+                    }
+                } else {
+                    const int con = U[s].mat - 1;
+                    B.con.push_back(con);
+                    for (auto &f : full) {
+                        B.cpos.push_back(f.first);
+                        B.cval.push_back(f.second);
+                        nrm2[con] += f.second * f.second;
+                    }
+                    B.cptr.push_back((long long)B.cpos.size());
+                }
+            }
+            s = t;
+        }
+    }
+    // problem_prepare (problem.c:1866-1910): row equilibration, b and C scaling
+    P.normC2 = std::sqrt(c2);
+    P.normC1 = c1;
+    P.normb1 = P.normb2 = 0;
+    for (int i = 0; i < P.m; i++) { P.normb1 += std::fabs(P.b0[i]); P.normb2 += P.b0[i] * P.b0[i]; }
+    P.normb2 = std::sqrt(P.normb2);
+    P.d.resize(P.m);
+    for (int i = 0; i < P.m; i++) {
+        P.d[i] = nrm2[i] > 0 ? 1.0 / std::sqrt(nrm2[i]) : 1.0;
+        if (nrm2[i] == 0 && P.b[i] != 0) log_printf(1, "brisk: warning: constraint %d is empty but b != 0 (infeasible)\n", i + 1);
+    }
+    double nbv = 0;
+    for (int i = 0; i < P.m; i++) nbv += P.d[i] * P.b[i] * P.d[i] * P.b[i];
+    nbv = std::sqrt(nbv);
+    P.bs = nbv > 1 ? nbv : 1.0;
+    for (auto &B : P.blk)
+        for (size_t t = 0; t < B.con.size(); t++)
+            for (long long e = B.cptr[t]; e < B.cptr[t + 1]; e++) B.cval[e] *= P.d[B.con[t]];
+    for (int i = 0; i < P.m; i++) P.b[i] *= P.d[i];
+    P.du.resize(P.m);
+    for (int i = 0; i < P.m; i++) P.du[i] = P.bs / P.d[i];
+    P.cs = P.normC2 > 1 ? P.normC2 : 1.0;
+    for (int i = 0; i < P.m; i++) P.b[i] /= P.bs;
+    for (auto &B : P.blk)
+        for (auto &v : B.Cval) v /= P.cs;
+    return 0;
+}
+
+// ---------------------------------------------------------------------------------------------
+// small host numerics: the Ritz bound of the Lanczos step length
+// ---------------------------------------------------------------------------------------------
+// Smallest eigenvalue theta of the symmetric tridiagonal T (alpha[0..k-1], beta[0..k-2]) by
+// Sturm-count bisection, and the residual bound |beta[k-1] z[k-1]| of its unit eigenvector z by
+// inverse iteration (the quantities ritz_bound, solver.c:6030-6039, takes from dstev).
+static double sturm_below(int k, const double *a, const double *b, double x) {
+    int cnt = 0;
+    double q = a[0] - x;
+    if (q < 0) cnt++;
+    for (int i = 1; i < k; i++) {
+        if (q == 0) q = 1e-300;
+        q = (a[i] - x) - b[i - 1] * b[i - 1] / q;
+        if (q < 0) cnt++;
+    }
+    return cnt;
+}
+static double ritz_bound(int k, const double *alpha, const double *beta, double *theta) {
+    double lo = 1e300, hi = -1e300;
+    for (int i = 0; i < k; i++) {
+        const double r = (i > 0 ? std::fabs(beta[i - 1]) : 0) + (i + 1 < k ? std::fabs(beta[i]) : 0);
+        lo = std::min(lo, alpha[i] - r);
+        hi = std::max(hi, alpha[i] + r);
+    }
+    if (!std::isfinite(lo) || !std::isfinite(hi)) { *theta = 0; return 1e300; }
+    for (int it = 0; it < 200; it++) {
+        const double mid = 0.5 * (lo + hi);
+        if (mid <= lo || mid >= hi) break;
+        if (sturm_below(k, alpha, beta, mid) >= 1) hi = mid; else lo = mid;
+    }
+    const double th = 0.5 * (lo + hi);
+    *theta = th;
+    // inverse iteration on T - (th - delta) I, dense Gaussian elimination with partial pivoting
+    const double scale = std::max(std::fabs(lo), std::fabs(hi)) + 1e-300;
+    const double sh = th - 1e-10 * scale;
+    double z[64], A[64 * 64], w[64];
+    for (int i = 0; i < k; i++) z[i] = 1.0 / std::sqrt((double)k) * (1.0 + 0.01 * i);
+    for (int pass = 0; pass < 3; pass++) {
+        for (int i = 0; i < k * k; i++) A[i] = 0;
+        for (int i = 0; i < k; i++) {
+            A[i + i * k] = alpha[i] - sh;
+            if (i + 1 < k) { A[i + (i + 1) * k] = beta[i]; A[(i + 1) + i * k] = beta[i]; }
+        }
+        for (int i = 0; i < k; i++) w[i] = z[i];
+        for (int c = 0; c < k; c++) {
+            int piv = c;
+            for (int r = c + 1; r < k; r++) if (std::fabs(A[r + c * k]) > std::fabs(A[piv + c * k])) piv = r;
+            if (piv != c) {
+                for (int j = 0; j < k; j++) std::swap(A[c + j * k], A[piv + j * k]);
+                std::swap(w[c], w[piv]);
+            }
+            double d = A[c + c * k];
+            if (d == 0) d = A[c + c * k] = 1e-300;
+            for (int r = c + 1; r < k; r++) {
+                const double f = A[r + c * k] / d;
+                if (f == 0) continue;
+                for (int j = c; j < k; j++) A[r + j * k] -= f * A[c + j * k];
+                w[r] -= f * w[c];
+            }
+        }
+        for (int c = k - 1; c >= 0; c--) {
+            double s = w[c];
+            for (int j = c + 1; j < k; j++) s -= A[c + j * k] * z[j];
+            z[c] = s / A[c + c * k];
+        }
+        double nz = 0;
+        for (int i = 0; i < k; i++) nz += z[i] * z[i];
+        nz = std::sqrt(nz);
+        if (!(nz > 0) || !std::isfinite(nz)) { *theta = th; return 1e300; }
+        for (int i = 0; i < k; i++) z[i] /= nz;
+    }
+    return std::fabs(beta[k - 1] * z[k - 1]);
+}
+
+// ---------------------------------------------------------------------------------------------
+// output
+// ---------------------------------------------------------------------------------------------
+static int (*g_print)(const char *, int) = nullptr;
+void set_print_hook(int (*f)(const char *, int)) { g_print = f; }
+void log_printf(int is_err, const char *fmt, ...) {
+    char buf[2048];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (g_print) g_print(buf, is_err);
+    else fputs(buf, is_err ? stderr : stdout);
+}
+
+// ---------------------------------------------------------------------------------------------
+// the GPU solver
+// ---------------------------------------------------------------------------------------------
+namespace {
+
+struct DevArrays {   // per block
+    double *X, *Z, *Zi, *LX, *LZ, *LiX, *LiZ, *dX, *dZ, *F, *Fd, *R0, *G, *Q, *W, *T, *Xb, *Zb, *Bm;
+    double *dinvX, *dinvZ;
+    int *flags;
+};
+
+struct Gpu {
+    std::vector<void *> allocs;
+    cudaStream_t st = nullptr;
+    template <typename T>
+    T *alloc(size_t count) {
+        void *p = nullptr;
+        if (count == 0) count = 1;
+        if (cudaMalloc(&p, count * sizeof(T)) != cudaSuccess) return nullptr;
+        allocs.push_back(p);
+        return (T *)p;
+    }
+    ~Gpu() {
+        if (st) cudaStreamSynchronize(st);
+        for (void *p : allocs) cudaFree(p);
+        if (st) cudaStreamDestroy(st);
+    }
+};
+
+#define RC(call)                                   \
+    do {                                           \
+        int rc_ = (call);                          \
+        if (rc_) throw GpuFail{rc_, __LINE__};     \
+    } while (0)
+#define CU(call)                                                                  \
+    do {                                                                          \
+        cudaError_t e_ = (call);                                                  \
+        if (e_ != cudaSuccess) throw GpuFail{BGPU_ERR_CUDA, __LINE__, e_};        \
+    } while (0)
+
+struct GpuFail {
+    int rc;
+    int line;
+    cudaError_t ce = cudaSuccess;
+};
+
+class Solver {
+  public:
+    Solver(HProblem &P, const Options &opt) : P(P), opt(opt), m(P.m), nb((int)P.blk.size()) {}
+    void setup();                 // upload the scaled problem and allocate the device state
+    int run(ResultData &res);     // one solve from the resident data
+    void set_options(const Options &o) { opt = o; }
+    ~Solver() {
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (evs0) cudaEventDestroy(evs0);
+        if (evs1) cudaEventDestroy(evs1);
+        if (h_dots) cudaFreeHost(h_dots);
+    }
+    double upload_bytes = 0;
+
+  private:
+    HProblem &P;
+    Options opt;
+    int m, nb;
+    Gpu g;
+    std::vector<DevBlock> db;
+    std::vector<DevArrays> da;
+    // Schur complement
+    double *M = nullptr, *Lm = nullptr, *dinvM = nullptr, *Dsc = nullptr;
+    float *Mf = nullptr, *dinvMf = nullptr;
+    int *mflags = nullptr, *d_info = nullptr, *d_err = nullptr;
+    double *d_pmin = nullptr;
+    double *dv_in = nullptr, *dv_out = nullptr;   // m (or n) vectors
+    float *fv = nullptr;
+    double *dots_out = nullptr, *dots_scratch = nullptr;
+    const double **dots_a = nullptr, **dots_b = nullptr;
+    double *h_dots = nullptr;                     // pinned
+    void *ws = nullptr;
+    size_t ws_bytes = 0;
+    int chunk = 32, asm_prec = 0;
+    int epoch = 0;
+    // factor state (Schur in solver.c:4511-4568)
+    bool allow_float = false, want_double = false, is_float = false, reg_hint = false;
+    double reg = 0, reg_ok = 0, min_pivot = 1;
+    int nfloat = 0, nfactor = 0, pcg_iters = 0;
+    double mu_now = 1e300;
+    Timings tm;
+    double schur_flops = 0, schur_dev_time = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, evs0 = nullptr, evs1 = nullptr;
+
+    void upload_block(int k);
+    // reductions
+    void dots(int nq, const double *const *a, const double *const *b, long long n, double *out);
+    // operators
+    void aop_all(const std::vector<double *> &D, std::vector<double> &out);   // out = A(D)
+    void atop_block(int k, const std::vector<double> &y, double alpha, double beta, double *F);
+    void gemm(int akm, int bkm, int n, double alpha, const double *A, long long lda, const double *B, long long ldb,
+              double beta, double *C) {
+        RC(gemm_f64(g.st, akm, bkm, n, n, n, alpha, A, lda, 0, B, ldb, 0, beta, C, n, 0, 1, 0));
+    }
+    // C = alpha * A B with A, B column-major n x n
+    void mul(int n, double alpha, const double *A, const double *B, double *C) { gemm(0, 1, n, alpha, A, n, B, n, 0.0, C); }
+    void zinv(int k);
+    int chol(int n, double *L, double *dinv);   // returns info
+    void inv_from_chol(int n, const double *L, const double *dinv, double *Li);
+    // Schur
+    void assemble(std::vector<double> &dummy);
+    int factor();
+    void prec(const std::vector<double> &r, std::vector<double> &z);
+    void schur_mv(const std::vector<double> &x, std::vector<double> &y);
+    double schur_solve(const std::vector<double> &rhs, std::vector<double> &x, double tol_rel);
+    // step length
+    double maxstep(int primal, int K);
+    double lanczos(int n, const double *Bm, int K);
+    int try_step(int primal, double *alpha);
+    // final measures
+    void final_measures(const std::vector<double> &y, ResultData &res);
+};
+
+void Solver::dots(int nq, const double *const *a, const double *const *b, long long n, double *out) {
+    CU(cudaMemcpyAsync(dots_a, a, sizeof(double *) * nq, cudaMemcpyHostToDevice, g.st));
+    CU(cudaMemcpyAsync(dots_b, b, sizeof(double *) * nq, cudaMemcpyHostToDevice, g.st));
+    RC(dots_f64(g.st, nq, dots_a, dots_b, n, dots_out, dots_scratch));
+    CU(cudaMemcpyAsync(h_dots, dots_out, sizeof(double) * nq, cudaMemcpyDeviceToHost, g.st));
+    CU(cudaStreamSynchronize(g.st));
+    for (int q = 0; q < nq; q++) out[q] = h_dots[q];
+}
+
+void Solver::upload_block(int k) {
+    const HBlock &B = P.blk[k];
+    DevBlock &d = db[k];
+    const int n = B.n;
+    const long long nn = (long long)n * n;
+    d.n = n;
+    d.ncon = (int)B.con.size();
+    d.ne = (long long)B.cpos.size();
+    d.con = g.alloc<int>(d.ncon);
+    d.cptr = g.alloc<long long>(d.ncon + 1);
+    d.cpos = g.alloc<int>(d.ne);
+    d.cval = g.alloc<double>(d.ne);
+    d.pptr = g.alloc<long long>(nn + 1);
+    d.pcon = g.alloc<int>(d.ne);
+    d.pval = g.alloc<double>(d.ne);
+    d.C = g.alloc<double>(nn);
+    if (!d.con || !d.cptr || !d.cpos || !d.cval || !d.pptr || !d.pcon || !d.pval || !d.C) throw GpuFail{BGPU_ERR_NOMEM, __LINE__};
+    CU(cudaMemcpy(d.con, B.con.data(), sizeof(int) * d.ncon, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(d.cptr, B.cptr.data(), sizeof(long long) * (d.ncon + 1), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(d.cpos, B.cpos.data(), sizeof(int) * d.ne, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(d.cval, B.cval.data(), sizeof(double) * d.ne, cudaMemcpyHostToDevice));
+    // position-major copy (A'(y) without atomics): entries of each position in constraint order
+    std::vector<long long> pptr(nn + 1, 0);
+    for (long long e = 0; e < d.ne; e++) pptr[B.cpos[e] + 1]++;
+    for (long long p = 0; p < nn; p++) pptr[p + 1] += pptr[p];
+    std::vector<int> pcon(d.ne);
+    std::vector<double> pval(d.ne);
+    std::vector<long long> fill(pptr.begin(), pptr.end() - 1);
+    for (int t = 0; t < d.ncon; t++)
+        for (long long e = B.cptr[t]; e < B.cptr[t + 1]; e++) {
+            const long long q = fill[B.cpos[e]]++;
+            pcon[q] = B.con[t];
+            pval[q] = B.cval[e];
+        }
+    CU(cudaMemcpy(d.pptr, pptr.data(), sizeof(long long) * (nn + 1), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(d.pcon, pcon.data(), sizeof(int) * d.ne, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(d.pval, pval.data(), sizeof(double) * d.ne, cudaMemcpyHostToDevice));
+    std::vector<double> C(nn, 0.0);
+    for (size_t e = 0; e < B.Cpos.size(); e++) C[B.Cpos[e]] += B.Cval[e];
+    CU(cudaMemcpy(d.C, C.data(), sizeof(double) * nn, cudaMemcpyHostToDevice));
+    upload_bytes += (double)sizeof(int) * d.ncon + sizeof(long long) * (d.ncon + 1) + (sizeof(int) + sizeof(double)) * 2.0 * d.ne +
+                    sizeof(long long) * (nn + 1.0) + sizeof(double) * (double)nn;
+
+    DevArrays &a = da[k];
+    double **ptrs[] = {&a.X, &a.Z, &a.Zi, &a.LX, &a.LZ, &a.LiX, &a.LiZ, &a.dX, &a.dZ, &a.F, &a.Fd, &a.R0, &a.G,
+                       &a.Q, &a.W, &a.T, &a.Xb, &a.Zb, &a.Bm};
+    for (double **pp : ptrs) {
+        *pp = g.alloc<double>(nn);
+        if (!*pp) throw GpuFail{BGPU_ERR_NOMEM, __LINE__};
+    }
+    const int nblk64 = ceil_div(n, TRI_NB);
+    a.dinvX = g.alloc<double>((size_t)nblk64 * TRI_NB * TRI_NB);
+    a.dinvZ = g.alloc<double>((size_t)nblk64 * TRI_NB * TRI_NB);
+    a.flags = g.alloc<int>(nblk64);
+    if (!a.dinvX || !a.dinvZ || !a.flags) throw GpuFail{BGPU_ERR_NOMEM, __LINE__};
+    CU(cudaMemset(a.flags, 0, sizeof(int) * nblk64));
+}
+
+void Solver::setup() {
+    CU(cudaSetDevice(opt.device));
+    CU(cudaStreamCreateWithFlags(&g.st, cudaStreamNonBlocking));
+    CU(cudaEventCreate(&ev0));
+    CU(cudaEventCreate(&ev1));
+    CU(cudaEventCreate(&evs0));
+    CU(cudaEventCreate(&evs1));
+    db.resize(nb);
+    da.resize(nb);
+    int nmax = 1;
+    for (int k = 0; k < nb; k++) {
+        upload_block(k);
+        nmax = std::max(nmax, P.blk[k].n);
+    }
+    const size_t mm = (size_t)m * m;
+    M = g.alloc<double>(mm);
+    if (!M) throw GpuFail{BGPU_ERR_NOMEM, __LINE__};
+    const int mb64 = ceil_div(std::max(m, 1), TRI_NB);
+    dinvM = g.alloc<double>((size_t)mb64 * TRI_NB * TRI_NB);
+    Dsc = g.alloc<double>(m);
+    mflags = g.alloc<int>(mb64);
+    d_info = g.alloc<int>(1);
+    d_err = g.alloc<int>(1);
+    d_pmin = g.alloc<double>(1);
+    const int vlen = std::max(m, nmax);
+    dv_in = g.alloc<double>(vlen);
+    dv_out = g.alloc<double>(vlen);
+    fv = g.alloc<float>(vlen);
+    dots_out = g.alloc<double>(16);
+    dots_scratch = g.alloc<double>(16 * 128);
+    dots_a = (const double **)g.alloc<double *>(16);
+    dots_b = (const double **)g.alloc<double *>(16);
+    if (!dinvM || !Dsc || !mflags || !d_info || !d_err || !d_pmin || !dv_in || !dv_out || !fv || !dots_out ||
+        !dots_scratch || !dots_a || !dots_b)
+        throw GpuFail{BGPU_ERR_NOMEM, __LINE__};
+    CU(cudaMemset(mflags, 0, sizeof(int) * mb64));
+    CU(cudaMemset(d_err, 0, sizeof(int)));
+    CU(cudaMallocHost(&h_dots, 16 * sizeof(double)));
+    allow_float = opt.mixed > 0 || (opt.mixed < 0 && m >= 1000);
+    asm_prec = opt.asm_prec < 0 ? 0 : opt.asm_prec;
+    if (asm_prec == 1) allow_float = true;   // the 3xTF32 path factors in FP32 until mu_switch
+    if (allow_float) {
+        Mf = g.alloc<float>(mm);
+        dinvMf = g.alloc<float>((size_t)mb64 * TRI_NB * TRI_NB);
+        if (!Mf || !dinvMf) throw GpuFail{BGPU_ERR_NOMEM, __LINE__};
+    }
+    chunk = opt.chunk > 0 ? opt.chunk : schur_chunk_default(nmax, asm_prec);
+    ws_bytes = schur_ws_bytes(nmax, chunk, asm_prec);
+    ws = g.alloc<unsigned char>(ws_bytes);
+    if (!ws) throw GpuFail{BGPU_ERR_NOMEM, __LINE__};
+}
+
+void Solver::aop_all(const std::vector<double *> &D, std::vector<double> &out) {
+    CU(cudaMemsetAsync(dv_out, 0, sizeof(double) * m, g.st));
+    for (int k = 0; k < nb; k++) RC(aop_f64(g.st, db[k], D[k], 1.0, 1.0, dv_out));
+    out.resize(m);
+    CU(cudaMemcpyAsync(out.data(), dv_out, sizeof(double) * m, cudaMemcpyDeviceToHost, g.st));
+    CU(cudaStreamSynchronize(g.st));
+}
+
+void Solver::atop_block(int k, const std::vector<double> &y, double alpha, double beta, double *F) {
+    CU(cudaMemcpyAsync(dv_in, y.data(), sizeof(double) * m, cudaMemcpyHostToDevice, g.st));
+    RC(atop_f64(g.st, db[k], dv_in, alpha, beta, F));
+}
+
+int Solver::chol(int n, double *L, double *dinv) {
+    RC(potrf_f64(g.st, n, L, n, dinv, d_info, d_pmin));
+    int info = 0;
+    CU(cudaMemcpyAsync(&info, d_info, sizeof(int), cudaMemcpyDeviceToHost, g.st));
+    CU(cudaStreamSynchronize(g.st));
+    return info;
+}
+
+void Solver::inv_from_chol(int n, const double *L, const double *dinv, double *Li) { RC(trtri_f64(g.st, n, L, n, dinv, Li, n)); }
+
+void Solver::zinv(int k) {
+    // Zi = LZ^-T LZ^-1 (LZ and dinvZ from the last Cholesky of Z)
+    const int n = db[k].n;
+    DevArrays &a = da[k];
+    inv_from_chol(n, a.LZ, a.dinvZ, a.LiZ);
+    RC(gemm_f64(g.st, 1, 1, n, n, n, 1.0, a.LiZ, n, 0, a.LiZ, n, 0, 0.0, a.Zi, n, 0, 1, 0));
+    RC(symmetrize_f64(g.st, n, a.Zi, n));
+}
+
+// ---- Schur complement ----------------------------------------------------------------------
+void Solver::assemble(std::vector<double> &) {
+    CU(cudaMemsetAsync(M, 0, sizeof(double) * (size_t)m * m, g.st));
+    CU(cudaEventRecord(ev0, g.st));
+    for (int k = 0; k < nb; k++) {
+        RC(schur_assemble(g.st, db[k], da[k].X, da[k].Zi, M, m, asm_prec, chunk, ws, ws_bytes));
+        const double n = db[k].n;
+        const double ncon = db[k].ncon;
+        schur_flops += 2.0 * n * n * n * ncon;   // the row-product GEMMs: 2 n^2 r_a with r_a <= n
+    }
+    CU(cudaEventRecord(ev1, g.st));
+    CU(cudaEventSynchronize(ev1));
+    float ms = 0;
+    CU(cudaEventElapsedTime(&ms, ev0, ev1));
+    schur_dev_time += ms * 1e-3;
+}
+
+// schur_factor_ (solver.c:5296-5421), dense path
+int Solver::factor() {
+    nfactor++;
+    const double ulp = 2.220446049250313e-16;
+    const double reg_floor = opt.reg_ill > 0 ? opt.reg_ill : std::max(1e-15, (double)m * ulp);
+    const double reg_first = opt.reg_ill > 0 ? 1e-13 : std::max(1e-15, (double)m * ulp);
+    const bool float_now = allow_float && !want_double && !(asm_prec == 1 && mu_now < opt.mu_switch);
+    if (float_now) {
+        RC(schur_load_f32(g.st, m, M, m, Dsc, Mf, m));
+        RC(potrf_f32(g.st, m, Mf, m, dinvMf, d_info, d_pmin));
+        int info = 0;
+        double pmin = 0;
+        CU(cudaMemcpyAsync(&info, d_info, sizeof(int), cudaMemcpyDeviceToHost, g.st));
+        CU(cudaMemcpyAsync(&pmin, d_pmin, sizeof(double), cudaMemcpyDeviceToHost, g.st));
+        CU(cudaStreamSynchronize(g.st));
+        if (info == 0 && pmin >= 1e-6) {
+            is_float = true;
+            reg = 0;
+            nfloat++;
+            min_pivot = pmin;
+            return 0;
+        }
+        want_double = true;
+    }
+    is_float = false;
+    if (!Lm) {
+        Lm = g.alloc<double>((size_t)m * m);
+        if (!Lm) throw GpuFail{BGPU_ERR_NOMEM, __LINE__};
+    }
+    double r = reg_hint ? std::max(reg_floor, 0.01 * reg_ok) : 0.0;
+    int info = 0;
+    for (int attempt = 0; attempt < 10; attempt++) {
+        RC(schur_load_f64(g.st, m, M, m, r, Dsc, Lm, m));
+        RC(potrf_f64(g.st, m, Lm, m, dinvM, d_info, d_pmin));
+        double pmin = 0;
+        CU(cudaMemcpyAsync(&info, d_info, sizeof(int), cudaMemcpyDeviceToHost, g.st));
+        CU(cudaMemcpyAsync(&pmin, d_pmin, sizeof(double), cudaMemcpyDeviceToHost, g.st));
+        CU(cudaStreamSynchronize(g.st));
+        if (info == 0) {
+            if (pmin >= opt.pivtol || r >= reg_floor) {
+                reg = r;
+                min_pivot = pmin;
+                reg_hint = r > 0;
+                reg_ok = r;
+                return 0;
+            }
+            r = std::max(reg_floor, r * 100);
+            continue;
+        }
+        r = (r == 0) ? reg_first : r * 100;
+    }
+    return info ? info : 1;
+}
+
+void Solver::prec(const std::vector<double> &rv, std::vector<double> &z) {
+    // z = D L^-T L^-1 D r (schur_prec_, solver.c:5424-5460)
+    std::vector<double> h(m);
+    std::vector<double> Dh(m);
+    CU(cudaMemcpyAsync(Dh.data(), Dsc, sizeof(double) * m, cudaMemcpyDeviceToHost, g.st));
+    CU(cudaStreamSynchronize(g.st));
+    z.resize(m);
+    if (is_float) {
+        std::vector<float> f(m);
+        for (int i = 0; i < m; i++) f[i] = (float)(rv[i] * Dh[i]);
+        CU(cudaMemcpyAsync(fv, f.data(), sizeof(float) * m, cudaMemcpyHostToDevice, g.st));
+        RC(trsv_f32(g.st, m, Mf, m, dinvMf, fv, 0, mflags, ++epoch, d_err));
+        RC(trsv_f32(g.st, m, Mf, m, dinvMf, fv, 1, mflags, ++epoch, d_err));
+        CU(cudaMemcpyAsync(f.data(), fv, sizeof(float) * m, cudaMemcpyDeviceToHost, g.st));
+        CU(cudaStreamSynchronize(g.st));
+        for (int i = 0; i < m; i++) z[i] = (double)f[i] * Dh[i];
+    } else {
+        for (int i = 0; i < m; i++) h[i] = rv[i] * Dh[i];
+        CU(cudaMemcpyAsync(dv_in, h.data(), sizeof(double) * m, cudaMemcpyHostToDevice, g.st));
+        RC(trsv_f64(g.st, m, Lm, m, dinvM, dv_in, 0, mflags, ++epoch, d_err));
+        RC(trsv_f64(g.st, m, Lm, m, dinvM, dv_in, 1, mflags, ++epoch, d_err));
+        CU(cudaMemcpyAsync(h.data(), dv_in, sizeof(double) * m, cudaMemcpyDeviceToHost, g.st));
+        CU(cudaStreamSynchronize(g.st));
+        for (int i = 0; i < m; i++) z[i] = h[i] * Dh[i];
+    }
+    int err = 0;
+    CU(cudaMemcpy(&err, d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err) throw GpuFail{BGPU_ERR_TIMEOUT, __LINE__};
+}
+
+void Solver::schur_mv(const std::vector<double> &x, std::vector<double> &y) {
+    CU(cudaMemcpyAsync(dv_in, x.data(), sizeof(double) * m, cudaMemcpyHostToDevice, g.st));
+    RC(symv_full_f64(g.st, m, 1.0, M, m, dv_in, 0.0, dv_out));
+    y.resize(m);
+    CU(cudaMemcpyAsync(y.data(), dv_out, sizeof(double) * m, cudaMemcpyDeviceToHost, g.st));
+    CU(cudaStreamSynchronize(g.st));
+}
+
+static double dot(const std::vector<double> &a, const std::vector<double> &b) {
+    double s = 0;
+    for (size_t i = 0; i < a.size(); i++) s += a[i] * b[i];
+    return s;
+}
+static double nrm(const std::vector<double> &a) { return std::sqrt(dot(a, a)); }
+
+// schur_solve_ (solver.c:5483-5621): PCG on M x = rhs with the factor as preconditioner
+double Solver::schur_solve(const std::vector<double> &rhs, std::vector<double> &x, double tol_rel) {
+    const double nb_ = nrm(rhs);
+    x.assign(m, 0.0);
+    if (nb_ == 0) return 0;
+    prec(rhs, x);
+    std::vector<double> Mx, r(m), z, p, q, xb;
+    schur_mv(x, Mx);
+    for (int i = 0; i < m; i++) r[i] = rhs[i] - Mx[i];
+    double nr = nrm(r);
+    const double tol = std::max(tol_rel, is_float ? 1e-10 : 1e-13) * nb_;
+    if (nr <= tol) return nr / nb_;
+    double best = nr;
+    xb = x;
+    prec(r, z);
+    p = z;
+    double rz = dot(r, z);
+    const int maxit = (reg > 0 || is_float) ? 50 : 10;
+    int stall = 0, used = 0;
+    const double sgain = 0.9;
+    const int smax = 4;
+    for (int k = 0; k < maxit; k++) {
+        schur_mv(p, q);
+        const double pq = dot(p, q);
+        if (!(pq > 0)) break;
+        const double a = rz / pq;
+        for (int i = 0; i < m; i++) { x[i] += a * p[i]; r[i] -= a * q[i]; }
+        pcg_iters++;
+        used++;
+        nr = nrm(r);
+        if (nr < best) {
+            stall = (nr > sgain * best) ? stall + 1 : 0;
+            best = nr;
+            xb = x;
+        } else stall++;
+        if (nr <= tol || stall >= smax) break;
+        prec(r, z);
+        const double rz2 = dot(r, z);
+        const double beta = rz2 / rz;
+        rz = rz2;
+        for (int i = 0; i < m; i++) p[i] = z[i] + beta * p[i];
+    }
+    x = xb;
+    schur_mv(x, Mx);
+    for (int i = 0; i < m; i++) r[i] = rhs[i] - Mx[i];
+    const double rel = nrm(r) / nb_;
+    if (is_float && (used > 4 || best > tol || rel > std::max(1e-9, 10 * tol_rel))) want_double = true;
+    return rel;
+}
+
+// ---- step length ---------------------------------------------------------------------------
+// Lanczos on the explicit Bm = L^-1 D L^-T (sdp_maxstep_lam, solver.c:6083-6225, cold start):
+// returns lambda_min estimate theta - residual bound (conservative), or -1e300 on failure.
+double Solver::lanczos(int n, const double *Bm, int Kmax) {
+    int K = std::min(n, Kmax);
+    K = std::min(K, 30);
+    std::vector<double> Q((size_t)(K + 1) * n), w(n);
+    double alpha[32], beta[32];
+    double nrm0 = 0;
+    for (int i = 0; i < n; i++) { Q[i] = 1.0 + 0.5 * std::sin(1.7 * i + 0.3); nrm0 += Q[i] * Q[i]; }
+    nrm0 = 1.0 / std::sqrt(nrm0);
+    for (int i = 0; i < n; i++) Q[i] *= nrm0;
+    int kk = 0;
+    double scale = 0, theta = 0, res = 0;
+    const double lz_tol = 0.02;
+    for (int j = 0; j < K; j++) {
+        double *qj = Q.data() + (size_t)j * n;
+        CU(cudaMemcpyAsync(dv_in, qj, sizeof(double) * n, cudaMemcpyHostToDevice, g.st));
+        RC(symv_full_f64(g.st, n, 1.0, Bm, n, dv_in, 0.0, dv_out));
+        CU(cudaMemcpyAsync(w.data(), dv_out, sizeof(double) * n, cudaMemcpyDeviceToHost, g.st));
+        CU(cudaStreamSynchronize(g.st));
+        double a = 0;
+        for (int i = 0; i < n; i++) a += qj[i] * w[i];
+        alpha[j] = a;
+        for (int pass = 0; pass < 2; pass++)
+            for (int i = 0; i <= j; i++) {
+                const double *qi = Q.data() + (size_t)i * n;
+                double c = 0;
+                for (int t = 0; t < n; t++) c += qi[t] * w[t];
+                for (int t = 0; t < n; t++) w[t] -= c * qi[t];
+            }
+        double b = 0;
+        for (int t = 0; t < n; t++) b += w[t] * w[t];
+        b = std::sqrt(b);
+        beta[j] = b;
+        kk = j + 1;
+        if (std::fabs(a) > scale) scale = std::fabs(a);
+        if (b <= 1e-12 * (scale + 1e-300)) { beta[j] = 0; break; }
+        if (kk >= 6 && kk % 3 == 0) {
+            res = ritz_bound(kk, alpha, beta, &theta);
+            if (res <= lz_tol * std::fabs(theta) + 1e-14 * scale) break;
+        }
+        if (j + 1 < K) {
+            double *qn = Q.data() + (size_t)(j + 1) * n;
+            const double inv = 1.0 / b;
+            for (int t = 0; t < n; t++) qn[t] = w[t] * inv;
+        }
+    }
+    res = ritz_bound(kk, alpha, beta, &theta);
+    if (res > 1e299) return -1e300;
+    return theta - res;
+}
+
+// maxstep (solver.c:6300-6390): the largest alpha with V + alpha dV >= 0 over all blocks
+double Solver::maxstep(int primal, int K) {
+    double a = 1e30;
+    for (int k = 0; k < nb; k++) {
+        const int n = db[k].n;
+        DevArrays &d = da[k];
+        const double *Li = primal ? d.LiX : d.LiZ;
+        const double *dV = primal ? d.dX : d.dZ;
+        // Bm = Li dV Li'
+        RC(gemm_f64(g.st, 0, 1, n, n, n, 1.0, Li, n, 0, dV, n, 0, 0.0, d.T, n, 0, 1, 0));
+        RC(gemm_f64(g.st, 0, 0, n, n, n, 1.0, d.T, n, 0, Li, n, 0, 0.0, d.Bm, n, 0, 1, 0));
+        RC(symmetrize_f64(g.st, n, d.Bm, n));
+        const double lam = lanczos(n, d.Bm, K);
+        double ak;
+        if (lam <= -1e299) ak = 0.0;
+        else ak = lam >= 0 ? 1e30 : -1.0 / lam;
+        if (!std::isfinite(ak) && !(ak > 0)) ak = 0.0;
+        if (ak < a) a = ak;
+    }
+    return a;
+}
+
+// try_step (solver.c:6393-6447): V += alpha dV with a Cholesky test, alpha *= 0.8 on failure
+int Solver::try_step(int primal, double *alpha) {
+    double a = *alpha;
+    std::vector<double> stepped(nb, 0.0);
+    for (int tries = 0; tries < 40; tries++) {
+        bool ok = true;
+        for (int k = 0; k < nb; k++) {
+            const int n = db[k].n;
+            DevArrays &d = da[k];
+            double *V = primal ? d.X : d.Z, *dV = primal ? d.dX : d.dZ, *L = primal ? d.LX : d.LZ;
+            double *dinv = primal ? d.dinvX : d.dinvZ;
+            const double inc = a - stepped[k];
+            stepped[k] = a;
+            RC(ew_step_copy(g.st, (long long)n * n, inc, dV, V, L));
+            if (chol(n, L, dinv) != 0) ok = false;
+        }
+        if (ok) {
+            *alpha = a;
+            return 1;
+        }
+        a *= 0.8;
+    }
+    return 0;
+}
+
+// ---- the DIMACS errors of the returned point on the data as given ----------------------------
+void Solver::final_measures(const std::vector<double> &y, ResultData &res) {
+    // X_o = bs X, y_o = cs d y, Z_o = C - A'(y_o) = cs (C' - A'(y))   (scaled data on the device)
+    const double bs = P.bs, cs = P.cs;
+    res.y.resize(m);
+    for (int i = 0; i < m; i++) res.y[i] = cs * P.d[i] * y[i];
+    double pobj = 0, xz = 0, lamx_neg = 0, lamz_neg = 0;
+    std::vector<double *> Xs(nb);
+    res.X.resize(nb);
+    res.Z.resize(nb);
+    for (int k = 0; k < nb; k++) {
+        const int n = db[k].n;
+        const long long nn = (long long)n * n;
+        DevArrays &d = da[k];
+        // W = cs (C' - A'(y)) ; G = bs X
+        atop_block(k, y, -cs, 0.0, d.W);
+        RC(ew_lincomb(g.st, nn, 1.0, d.W, cs, db[k].C, 0.0, nullptr, d.W));
+        RC(ew_lincomb(g.st, nn, bs, d.X, 0.0, nullptr, 0.0, nullptr, d.G));
+        Xs[k] = d.G;
+        double tmp[2];
+        const double *aa[2] = {db[k].C, d.G}, *bb[2] = {d.G, d.W};
+        dots(2, aa, bb, nn, tmp);
+        pobj += cs * tmp[0];   // <C_o, X_o> = cs <C', X_o>
+        xz += tmp[1];
+        res.X[k].resize(nn);
+        res.Z[k].resize(nn);
+        CU(cudaMemcpyAsync(res.X[k].data(), d.G, sizeof(double) * nn, cudaMemcpyDeviceToHost, g.st));
+        CU(cudaMemcpyAsync(res.Z[k].data(), d.W, sizeof(double) * nn, cudaMemcpyDeviceToHost, g.st));
+        // cone errors: a Cholesky test, then lambda_min by Lanczos when it fails
+        RC(ew_lincomb(g.st, nn, 1.0, d.W, 0.0, nullptr, 0.0, nullptr, d.T));
+        if (chol(n, d.T, d.dinvZ) != 0) {
+            RC(ew_lincomb(g.st, nn, 1.0, d.W, 0.0, nullptr, 0.0, nullptr, d.Bm));
+            const double lam = lanczos(n, d.Bm, 30);
+            lamz_neg = std::max(lamz_neg, -lam);
+        }
+        RC(ew_lincomb(g.st, nn, 1.0, d.G, 0.0, nullptr, 0.0, nullptr, d.T));
+        if (chol(n, d.T, d.dinvX) != 0) {
+            RC(ew_lincomb(g.st, nn, 1.0, d.G, 0.0, nullptr, 0.0, nullptr, d.Bm));
+            const double lam = lanczos(n, d.Bm, 30);
+            lamx_neg = std::max(lamx_neg, -lam);
+        }
+    }
+    std::vector<double> AX;
+    aop_all(Xs, AX);   // scaled A' = d A: A_o(X_o) = AX / d
+    double r2 = 0, dobj = 0;
+    for (int i = 0; i < m; i++) {
+        const double v = AX[i] / P.d[i] - P.b0[i];
+        r2 += v * v;
+        dobj += P.b0[i] * res.y[i];
+    }
+    const double den = 1 + std::fabs(pobj) + std::fabs(dobj);
+    res.err[1] = std::sqrt(r2) / (1 + P.normb1);
+    res.err[2] = std::max(0.0, lamx_neg) / (1 + P.normb1);
+    res.err[3] = 0;
+    res.err[4] = std::max(0.0, lamz_neg) / (1 + P.normC1);
+    res.err[5] = (pobj - dobj) / den;
+    res.err[6] = xz / den;
+    res.pobj = pobj;
+    res.dobj = dobj;
+    res.have_x = 1;
+    res.d2h_bytes = 0;
+    for (int k = 0; k < nb; k++) res.d2h_bytes += 2.0 * sizeof(double) * (double)db[k].n * db[k].n;
+    CU(cudaStreamSynchronize(g.st));
+}
+
+struct IterRes {   // Result measures of an iterate (scaled problem), as in solver.c:14470-14484
+    double pobj = 0, dobj = 0, pinf = 0, dinf = 0, relgap = 0, relcomp = 0, err[7] = {0, 0, 0, 0, 0, 0, 0};
+};
+static double nan_inf(double v) { return v != v ? INFINITY : v; }
+static double res_score(const IterRes &R) {
+    return std::max(std::max(nan_inf(R.relgap), nan_inf(R.relcomp)), std::max(nan_inf(R.pinf), nan_inf(R.dinf)));
+}
+static double dimacs_score(const IterRes &R) {
+    return std::max(std::max(std::fabs(nan_inf(R.err[1])), std::fabs(nan_inf(R.err[3]))),
+                    std::max(std::fabs(nan_inf(R.err[5])), std::fabs(nan_inf(R.err[6]))));
+}
+
+int Solver::run(ResultData &res) {
+    const double t0 = wtime();
+    tm = Timings();
+    want_double = is_float = reg_hint = false;
+    reg = reg_ok = 0;
+    min_pivot = 1;
+    nfloat = nfactor = pcg_iters = 0;
+    mu_now = 1e300;
+    schur_flops = schur_dev_time = 0;
+    CU(cudaEventRecord(evs0, g.st));
+    std::vector<double> y(m, 0.0), ybest(m, 0.0), dy, rp(m), a0, h(m, 0.0), rhs(m), qv, ev(m), wv;
+    std::vector<double> tmpv;
+    // start_sdpt3 (solver.c:6622-6661)
+    for (int k = 0; k < nb; k++) {
+        const HBlock &B = P.blk[k];
+        const int n = B.n;
+        double nC = 0, maxA = 0, ratio = 0;
+        for (double v : B.Cval) nC += v * v;
+        nC = std::sqrt(nC);
+        for (size_t t = 0; t < B.con.size(); t++) {
+            double a = 0;
+            for (long long e = B.cptr[t]; e < B.cptr[t + 1]; e++) a += B.cval[e] * B.cval[e];
+            a = std::sqrt(a);
+            maxA = std::max(maxA, a);
+            ratio = std::max(ratio, (1 + std::fabs(P.b[B.con[t]])) / (1 + a));
+        }
+        const double xi = std::max(10.0, std::max(std::sqrt((double)n), n * ratio));
+        const double eta = std::max(10.0, std::max(std::sqrt((double)n), std::max(maxA, nC)));
+        DevArrays &d = da[k];
+        RC(ew_set_scaled_identity(g.st, n, d.X, xi));
+        RC(ew_set_scaled_identity(g.st, n, d.Z, eta));
+        RC(ew_set_scaled_identity(g.st, n, d.LX, std::sqrt(xi)));
+        RC(ew_set_scaled_identity(g.st, n, d.LZ, std::sqrt(eta)));
+        // the factors' diagonal-block inverses: a Cholesky of the diagonal starts
+        RC(ew_set_scaled_identity(g.st, n, d.T, xi));
+        if (chol(n, d.T, d.dinvX)) throw GpuFail{BGPU_ERR_NOTPD, __LINE__};
+        RC(ew_set_scaled_identity(g.st, n, d.T, eta));
+        if (chol(n, d.T, d.dinvZ)) throw GpuFail{BGPU_ERR_NOTPD, __LINE__};
+        inv_from_chol(n, d.LX, d.dinvX, d.LiX);
+    }
+    // R0 = C - Z - A'y (y = 0), theta = 1
+    double theta = 1.0, r0norm = 0;
+    for (int k = 0; k < nb; k++) {
+        const long long nn = (long long)db[k].n * db[k].n;
+        RC(ew_lincomb(g.st, nn, 1.0, db[k].C, -1.0, da[k].Z, 0.0, nullptr, da[k].R0));
+        double t;
+        const double *aa[1] = {da[k].R0};
+        dots(1, aa, aa, nn, &t);
+        r0norm += t;
+    }
+    r0norm = std::sqrt(r0norm);
+    double nbs = nrm(P.b);
+    int status = -1, it = 0, it_best = 0, stall = 0;
+    double alp = 0, ald = 0, sigma = 0, best_score = INFINITY;
+    IterRes R, best;
+    const bool keep_best = true;
+    const double Ntot = (double)P.Ntot;
+    if (opt.verbose > 0)
+        log_printf(0, " it   pobj            dobj            pinf     dinf     gap      mu       alp   ald   sigma  time\n");
+    for (it = 0; it <= opt.maxit; it++) {
+        double td = wtime();
+        for (int k = 0; k < nb; k++) zinv(k);
+        // residuals and objectives
+        std::vector<double *> Xs(nb);
+        for (int k = 0; k < nb; k++) Xs[k] = da[k].X;
+        std::vector<double> AX;
+        aop_all(Xs, AX);
+        for (int i = 0; i < m; i++) rp[i] = P.b[i] - AX[i];
+        double pobj = 0, xz = 0, rdn2 = 0, nCR2 = 0, dev2 = 0;
+        for (int k = 0; k < nb; k++) {
+            const long long nn = (long long)db[k].n * db[k].n;
+            DevArrays &d = da[k];
+            atop_block(k, y, 1.0, 0.0, d.F);                                                   // A'y
+            RC(ew_lincomb(g.st, nn, 1.0, d.F, 1.0, d.Z, 0.0, nullptr, d.F));                  // A'y + Z
+            RC(ew_lincomb(g.st, nn, 1.0, d.F, -1.0, db[k].C, 0.0, nullptr, d.Fd));            // -Rd
+            RC(ew_lincomb(g.st, nn, 1.0, d.Fd, theta, d.R0, 0.0, nullptr, d.T));              // -Rd + theta R0
+            double part[5];
+            const double *aa[5] = {d.F, db[k].C, d.X, d.Fd, d.T}, *bb[5] = {d.F, d.X, d.Z, d.Fd, d.T};
+            dots(5, aa, bb, nn, part);
+            nCR2 += part[0]; pobj += part[1]; xz += part[2]; rdn2 += part[3]; dev2 += part[4];
+        }
+        double dobj = dot(P.b, y);
+        double mu = xz / Ntot;
+        mu_now = P.bs * P.cs * mu;
+        double rpo = 0;
+        for (int i = 0; i < m; i++) { const double v = rp[i] * P.du[i]; rpo += v * v; }
+        rpo = std::sqrt(rpo);
+        const double rdo = P.cs * std::sqrt(rdn2);
+        const double sc = P.bs * P.cs;
+        const double po = sc * pobj, dob = sc * dobj;
+        R.pobj = po; R.dobj = dob;
+        R.pinf = rpo / (1 + P.normb2);
+        R.dinf = rdo / (1 + P.normC2);
+        const double oden = 1 + std::fabs(po) + std::fabs(dob);
+        R.relgap = std::fabs(po - dob) / oden;
+        R.relcomp = sc * xz / oden;
+        R.err[1] = rpo / (1 + P.normb1);
+        R.err[3] = rdo / (1 + P.normC1);
+        R.err[5] = (po - dob) / oden;
+        R.err[6] = sc * xz / oden;
+        tm.dense += wtime() - td;
+        if (opt.verbose > 0)
+            log_printf(0, "%3d %+.8e %+.8e %.2e %.2e %.2e %.2e %.3f %.3f %.3f %6.2f\n", it, -po, -dob, R.pinf, R.dinf,
+                       R.relgap, sc * mu, alp, ald, sigma, wtime() - t0);
+        if (!std::isfinite(po) || !std::isfinite(dob)) { status = 4; break; }
+        const double score = res_score(R);
+        if (score < best_score) {
+            best_score = score;
+            it_best = it;
+            best = R;
+            ybest = y;
+            if (keep_best)
+                for (int k = 0; k < nb; k++) {
+                    const size_t nn = (size_t)db[k].n * db[k].n;
+                    CU(cudaMemcpyAsync(da[k].Xb, da[k].X, sizeof(double) * nn, cudaMemcpyDeviceToDevice, g.st));
+                    CU(cudaMemcpyAsync(da[k].Zb, da[k].Z, sizeof(double) * nn, cudaMemcpyDeviceToDevice, g.st));
+                }
+        }
+        if (score < opt.tol) { status = 0; break; }
+        if (keep_best && it > it_best && dimacs_score(best) <= 0.5 * opt.tol) { status = 4; break; }
+        if (opt.timelimit > 0 && wtime() - t0 > opt.timelimit) { status = 6; break; }
+        const double nCR = std::sqrt(nCR2);
+        if (!opt.known_feasible && dobj > 0 && nCR / dobj < 1e-8 && it > 5) { status = 1; break; }
+        double nAX = 0;
+        for (int i = 0; i < m; i++) { const double v = P.b[i] - rp[i]; nAX += v * v; }
+        nAX = std::sqrt(nAX);
+        if (!opt.known_feasible && pobj < 0 && nAX / (-pobj) < 1e-8 && it > 5) { status = 2; break; }
+        if (it == opt.maxit) { status = 3; break; }
+        if (stall >= 3) { status = 4; break; }
+        if (it - it_best >= opt.stall_win && best_score < 1e-6) { status = 4; break; }
+        if (it - it_best >= 8 && best_score < 1e-4) { status = 4; break; }
+        if (it - it_best >= 12) { status = 4; break; }
+        // re-base the dual residual when the recurrence has drifted
+        {
+            const double dev = std::sqrt(dev2);
+            if (dev > 1e-10 * (1.0 + theta * r0norm) && dev > 1e-12) {
+                theta = 1.0;
+                r0norm = std::sqrt(rdn2);
+                for (int k = 0; k < nb; k++)
+                    RC(ew_lincomb(g.st, (long long)db[k].n * db[k].n, -1.0, da[k].Fd, 0.0, nullptr, 0.0, nullptr, da[k].R0));
+            }
+            if (theta * r0norm <= 1e-13) theta = 0.0;
+        }
+        // ---- Schur complement ----
+        double ts = wtime();
+        assemble(tmpv);
+        double tc = wtime();
+        tm.schur += tc - ts;
+        if (factor() != 0) { status = 4; tm.chol += wtime() - tc; break; }
+        tm.chol += wtime() - tc;
+        // ---- rhs pieces ----
+        td = wtime();
+        const bool hasH = theta > 0;
+        {
+            std::vector<double *> Zis(nb), Gs(nb);
+            for (int k = 0; k < nb; k++) Zis[k] = da[k].Zi;
+            aop_all(Zis, a0);
+            if (hasH) {
+                for (int k = 0; k < nb; k++) {
+                    const int n = db[k].n;
+                    DevArrays &d = da[k];
+                    mul(n, theta, d.Zi, d.R0, d.T);   // theta Zi R0
+                    mul(n, 1.0, d.T, d.X, d.G);       // theta Zi R0 X
+                    Gs[k] = d.G;
+                }
+                aop_all(Gs, h);
+            } else h.assign(m, 0.0);
+        }
+        tm.dense += wtime() - td;
+        // ---- predictor ----
+        for (int i = 0; i < m; i++) rhs[i] = P.b[i] + h[i];
+        tc = wtime();
+        schur_solve(rhs, dy, 1e-7);
+        tm.chol += wtime() - tc;
+        td = wtime();
+        for (int k = 0; k < nb; k++) {
+            const int n = db[k].n;
+            const long long nn = (long long)n * n;
+            DevArrays &d = da[k];
+            atop_block(k, dy, -1.0, 0.0, d.dZ);
+            RC(ew_lincomb(g.st, nn, 1.0, d.dZ, theta, d.R0, 0.0, nullptr, d.dZ));   // dZ = -A'dy + theta R0
+            mul(n, 1.0, d.Zi, d.dZ, d.T);
+            mul(n, 1.0, d.T, d.X, d.G);                                            // Zi dZ X
+            RC(ew_sym_lincomb(g.st, n, d.G, -1.0, -1.0, d.X, 0.0, nullptr, d.dX)); // dX = -sym(G) - X
+        }
+        tm.dense += wtime() - td;
+        double tst = wtime();
+        const double ap = std::min(1.0, maxstep(1, opt.lanczos_k));
+        const double ad = std::min(1.0, maxstep(0, opt.lanczos_k));
+        tm.step += wtime() - tst;
+        double xdz = 0, dxz = 0, dxdz = 0;
+        for (int k = 0; k < nb; k++) {
+            const long long nn = (long long)db[k].n * db[k].n;
+            double t3[3];
+            const double *aa[3] = {da[k].X, da[k].dX, da[k].dX}, *bb[3] = {da[k].dZ, da[k].Z, da[k].dZ};
+            dots(3, aa, bb, nn, t3);
+            xdz += t3[0]; dxz += t3[1]; dxdz += t3[2];
+        }
+        const double mu_a = (xz + ap * dxz + ad * xdz + ap * ad * dxdz) / Ntot;
+        const double frac = std::max(0.0, mu_a / mu);
+        const double mina = std::min(ap, ad);
+        int rule = opt.sigma_rule < 0 ? 0 : opt.sigma_rule;   // SDP blocks present: the adaptive rule
+        double expon;
+        if (rule == 1) expon = 3.0;
+        else if (rule == 2) expon = (mina < 0.1) ? 1.0 : 3.0;
+        else expon = (R.relgap > 1e-6) ? std::max(1.0, 3 * mina * mina) : 3.0;
+        sigma = std::min(1.0, std::pow(frac, expon));
+        if (sigma < opt.sigma_min) sigma = opt.sigma_min;
+        {
+            const double infeas = std::max(R.pinf, R.dinf), bal = opt.balance;
+            if (bal > 0 && infeas > bal * R.relcomp && R.relcomp > 0) {
+                const double s_min = std::min(1.0, infeas / (bal * R.relcomp) * 0.1);
+                if (sigma < s_min) sigma = s_min;
+            }
+        }
+        const double gamma = 0.9 + (opt.gamma_max - 0.9) * mina;
+        // ---- corrector ----
+        const double smu = sigma * mu;
+        td = wtime();
+        {
+            std::vector<double *> Qs(nb);
+            for (int k = 0; k < nb; k++) {
+                const int n = db[k].n;
+                DevArrays &d = da[k];
+                mul(n, 1.0, d.Zi, d.dZ, d.T);
+                mul(n, 1.0, d.T, d.dX, d.Q);   // Q = Zi dZp dXp
+                Qs[k] = d.Q;
+            }
+            aop_all(Qs, qv);
+        }
+        for (int i = 0; i < m; i++) rhs[i] = P.b[i] - smu * a0[i] + qv[i] + h[i];
+        tm.dense += wtime() - td;
+        tc = wtime();
+        schur_solve(rhs, dy, 0);
+        tm.chol += wtime() - tc;
+        td = wtime();
+        for (int k = 0; k < nb; k++) {
+            const int n = db[k].n;
+            const long long nn = (long long)n * n;
+            DevArrays &d = da[k];
+            atop_block(k, dy, -1.0, 0.0, d.dZ);
+            RC(ew_lincomb(g.st, nn, 1.0, d.dZ, theta, d.R0, 0.0, nullptr, d.dZ));
+            mul(n, 1.0, d.Zi, d.dZ, d.T);
+            mul(n, 1.0, d.T, d.X, d.G);
+            RC(ew_lincomb(g.st, nn, 1.0, d.G, 1.0, d.Q, 0.0, nullptr, d.G));          // Zi dZ X + Q
+            RC(ew_sym_lincomb(g.st, n, d.G, -1.0, smu, d.Zi, -1.0, d.X, d.dX));      // -sym(.) + smu Zi - X
+        }
+        tm.dense += wtime() - td;
+        // ---- refinement of A(dX) = rp ----
+        for (int pass = 0; pass < 3; pass++) {
+            td = wtime();
+            std::vector<double *> dXs(nb);
+            for (int k = 0; k < nb; k++) dXs[k] = da[k].dX;
+            std::vector<double> AdX;
+            aop_all(dXs, AdX);
+            for (int i = 0; i < m; i++) ev[i] = rp[i] - AdX[i];
+            const double ne = nrm(ev), nrp = nrm(rp);
+            tm.dense += wtime() - td;
+            if (!(ne > 1e-2 * nrp && ne > 1e-3 * opt.tol * (1 + nbs))) break;
+            tc = wtime();
+            schur_solve(ev, wv, 0);
+            tm.chol += wtime() - tc;
+            td = wtime();
+            std::vector<double *> Gs(nb);
+            for (int k = 0; k < nb; k++) {
+                const int n = db[k].n;
+                DevArrays &d = da[k];
+                atop_block(k, wv, 1.0, 0.0, d.W);            // A'w
+                mul(n, 1.0, d.Zi, d.W, d.T);
+                mul(n, 1.0, d.T, d.X, d.F);                  // Zi A'w X  (F is free here)
+                RC(ew_sym_lincomb(g.st, n, d.F, 1.0, 0.0, nullptr, 0.0, nullptr, d.G));
+                Gs[k] = d.G;
+            }
+            std::vector<double> AG;
+            aop_all(Gs, AG);
+            for (int i = 0; i < m; i++) qv[i] = ev[i] - AG[i];
+            const double ne2 = nrm(qv);
+            tm.dense += wtime() - td;
+            if (!(ne2 < 0.5 * ne)) break;
+            for (int i = 0; i < m; i++) dy[i] += wv[i];
+            for (int k = 0; k < nb; k++) {
+                const long long nn = (long long)db[k].n * db[k].n;
+                RC(ew_lincomb(g.st, nn, 1.0, da[k].dZ, -1.0, da[k].W, 0.0, nullptr, da[k].dZ));
+                RC(ew_lincomb(g.st, nn, 1.0, da[k].dX, 1.0, da[k].G, 0.0, nullptr, da[k].dX));
+            }
+        }
+        tst = wtime();
+        const double apr = std::min(1.0, maxstep(1, opt.lanczos_k));
+        const double adr = std::min(1.0, maxstep(0, opt.lanczos_k));
+        tm.step += wtime() - tst;
+        double apn = std::min(1.0, gamma * apr), adn = std::min(1.0, gamma * adr);
+        // catastrophe guard (solver.c:15138-15158)
+        if (R.pinf < 1e-6) {
+            td = wtime();
+            std::vector<double *> dXs(nb);
+            for (int k = 0; k < nb; k++) dXs[k] = da[k].dX;
+            std::vector<double> AdX;
+            aop_all(dXs, AdX);
+            for (int i = 0; i < m; i++) ev[i] = rp[i] - AdX[i];
+            const double nrp = nrm(rp), nev = nrm(ev);
+            tm.dense += wtime() - td;
+            const double gg = std::max(1e3, 1e-6 / std::max(R.pinf, 1e-300));
+            const double lim = gg * nrp;
+            if (nev > lim && nrp > 0) {
+                const double cap = lim / nev;
+                if (cap < apn) apn = cap;
+                if (allow_float) want_double = true;
+            }
+        }
+        tst = wtime();
+        const int okp = try_step(1, &apn);
+        const int okd = try_step(0, &adn);
+        for (int k = 0; k < nb; k++) inv_from_chol(db[k].n, da[k].LX, da[k].dinvX, da[k].LiX);
+        tm.step += wtime() - tst;
+        if (!okp || !okd) { status = 4; break; }
+        for (int i = 0; i < m; i++) y[i] += adn * dy[i];
+        theta *= (1.0 - adn);
+        alp = apn;
+        ald = adn;
+        stall = (apn < 1e-6 && adn < 1e-6) ? stall + 1 : 0;
+    }
+    res.iters = it;
+    // fall back to the best iterate seen
+    if (status != 0 && status != 1 && status != 2 && best_score < res_score(R)) {
+        R = best;
+        y = ybest;
+        for (int k = 0; k < nb; k++) {
+            const size_t nn = (size_t)db[k].n * db[k].n;
+            CU(cudaMemcpyAsync(da[k].X, da[k].Xb, sizeof(double) * nn, cudaMemcpyDeviceToDevice, g.st));
+            CU(cudaMemcpyAsync(da[k].Z, da[k].Zb, sizeof(double) * nn, cudaMemcpyDeviceToDevice, g.st));
+        }
+        if (opt.verbose > 1) log_printf(0, "   returning best iterate (iteration %d)\n", it_best);
+    }
+    final_measures(y, res);
+    // the status of the returned point as measured on the data as given (main.c:2349-2362)
+    const double acc = std::max(std::max(res.err[1], res.err[2]),
+                                std::max(res.err[4], std::max(std::fabs(res.err[5]), std::fabs(res.err[6]))));
+    if (status == 0 || status == 5 || status == 3 || status == 4 || status == 6) {
+        if (acc <= opt.tol) status = 0;
+        else if (acc <= opt.red_acc) status = 5;
+        else if (status == 0 || status == 5) status = 4;
+    }
+    res.status = status;
+    res.exit_code = exit_code_of(status);
+    res.nfloat = nfloat;
+    res.nfactor = nfactor;
+    res.pcg_iters = pcg_iters;
+    res.schur_flops = schur_flops;
+    res.schur_time = schur_dev_time;
+    CU(cudaEventRecord(evs1, g.st));
+    CU(cudaEventSynchronize(evs1));
+    float dms = 0;
+    CU(cudaEventElapsedTime(&dms, evs0, evs1));
+    res.device_time = dms * 1e-3;
+    tm.total = wtime() - t0;
+    res.t = tm;
+    res.time = tm.total;
+    return res.exit_code;
+}
+
+}  // namespace
+
+int solve_problem(const InputData &in, const Options &opt, ResultData &res) {
+    HProblem P;
+    std::string err;
+    const double t0 = wtime();
+    res = ResultData();
+    res.m = in.m;
+    res.nblk = in.nblk;
+    res.bs = in.bs;
+    if (int rc = build_problem(in, P, err)) {
+        log_printf(1, "brisk: %s\n", err.c_str());
+        return rc;
+    }
+    if (opt.verbose > 0) {
+        int nmax = 0;
+        for (auto &B : P.blk) nmax = std::max(nmax, B.n);
+        log_printf(0, "BRISK-B200 %s interior-point SDP solver (Newton step on the GPU)\n", "1.7");
+        log_printf(0, "problem: m = %d, %d SDP blocks (max n = %d)\n", in.m, in.nblk, nmax);
+    }
+    try {
+        Solver S(P, opt);
+        S.setup();
+        const double t1 = wtime();
+        int rc = S.run(res);
+        res.t.setup = t1 - t0;
+        res.h2d_bytes = S.upload_bytes;
+        res.time = wtime() - t0;
+        if (opt.verbose > 0) {
+            log_printf(0, "status: %s   iterations: %d\n", status_string(res.status), res.iters);
+            log_printf(0, "  primal obj <C,X> = %.10e   dual obj b'y = %.10e\n", res.pobj, res.dobj);
+            log_printf(0, "  DIMACS errors: %.1e %.1e %.1e %.1e %.1e %.1e\n", res.err[1], res.err[2], res.err[3],
+                       res.err[4], res.err[5], res.err[6]);
+            log_printf(0, "time: total %.3fs | schur %.3f  chol/solve %.3f  dense %.3f  step %.3f  setup %.3f\n",
+                       res.t.total, res.t.schur, res.t.chol, res.t.dense, res.t.step, res.t.setup);
+        }
+        return rc;
+    } catch (const GpuFail &f) {
+        log_printf(1, "brisk: GPU failure (code %d at solver.cu:%d%s%s)\n", f.rc, f.line,
+                   f.ce != cudaSuccess ? ": " : "", f.ce != cudaSuccess ? cudaGetErrorString(f.ce) : "");
+        res.status = 4;
+        res.exit_code = -3;
+        return -3;
+    }
+}
+
+}  // namespace bsolve
+
+namespace bsolve {
+
+struct Session {
+    HProblem P;
+    Solver *S = nullptr;
+    int m = 0, nblk = 0;
+    std::vector<int> bs;
+    ~Session() { delete S; }
+};
+
+Session *session_create(const InputData &in, const Options &opt, std::string &err, int &rc) {
+    Session *s = new Session;
+    s->m = in.m;
+    s->nblk = in.nblk;
+    s->bs = in.bs;
+    rc = build_problem(in, s->P, err);
+    if (rc) { delete s; return nullptr; }
+    try {
+        s->S = new Solver(s->P, opt);
+        s->S->setup();
+    } catch (const GpuFail &f) {
+        err = "GPU failure during setup (code " + std::to_string(f.rc) + ")";
+        rc = -3;
+        delete s;
+        return nullptr;
+    }
+    return s;
+}
+
+int session_solve(Session *s, const Options &opt, ResultData &res) {
+    res = ResultData();
+    res.m = s->m;
+    res.nblk = s->nblk;
+    res.bs = s->bs;
+    s->S->set_options(opt);
+    try {
+        return s->S->run(res);
+    } catch (const GpuFail &f) {
+        log_printf(1, "brisk: GPU failure (code %d at solver.cu:%d)\n", f.rc, f.line);
+        res.status = 4;
+        res.exit_code = -3;
+        return -3;
+    }
+}
+
+void session_destroy(Session *s) { delete s; }
+
+}  // namespace bsolve

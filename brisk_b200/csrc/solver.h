@@ -1,0 +1,89 @@
+// Host-side solver of the B200 SDP Newton step: the problem as given, the options, the result.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace bsolve {
+
+// The numbers of an SDPA sparse problem (brisk.h:128-140), already checked and with zero
+// values dropped.  mat 0 = F0 = -C; 1..m = A_i; i, j are 1-based within the block.
+struct InputData {
+    int m = 0, nblk = 0;
+    std::vector<int> bs;
+    std::vector<double> c;
+    std::vector<int> mat, blk, i, j;
+    std::vector<double> v;
+};
+
+struct Options {
+    double tol = 1e-8;
+    int maxit = 100;
+    int verbose = 1;            // 0 quiet, 1 default log, 2.. diagnosis
+    int lanczos_k = 30;
+    double gamma_max = 0.99;
+    double pivtol = 1e-14;
+    double sigma_min = 0.0;
+    double balance = 0.0;
+    int sigma_rule = -1;
+    int mixed = -1;             // FP32 Schur factor: -1 auto (m >= 1000), 0 never, 1 always
+    int asm_prec = -1;          // Schur assembly: -1 auto (FP64), 0 FP64, 1 3xTF32
+    double mu_switch = 1e-4;    // 3xTF32 path: the factor goes to FP64 once scaled mu < mu_switch
+    int chunk = 0;              // constraints per assembly chunk (0: chosen by the block order)
+    double timelimit = 0.0;
+    double reg_ill = 0.0;
+    int stall_win = 5;
+    double red_acc = 1e-6;
+    int known_feasible = 0;
+    int device = 0;
+    int sparse = -1;            // accepted for compatibility (dense Schur complement only)
+    int init = 1;               // 0: SDPT3 start (start_sdpt3); 1: least-squares start (solver.c:13939-14198)
+};
+
+struct Timings {
+    double setup = 0, schur = 0, chol = 0, dense = 0, step = 0, total = 0, read = 0;
+};
+
+struct ResultData {
+    int status = -1;            // 0 optimal, 1 primal infeasible, 2 dual infeasible, 3 iteration limit,
+                                // 4 numerical difficulties, 5 reduced accuracy, 6 time limit
+    int exit_code = 0;
+    int iters = 0;
+    int have_x = 0;
+    int m = 0, nblk = 0;
+    std::vector<int> bs;
+    double pobj = 0, dobj = 0;  // <C,X>, b'y on the data as given
+    double err[7] = {0, 0, 0, 0, 0, 0, 0};
+    double time = 0;
+    std::vector<double> y;
+    std::vector<std::vector<double>> X, Z;
+    Timings t;
+    int nfloat = 0, nfactor = 0, pcg_iters = 0;
+    double schur_flops = 0;     // algorithmic flops of the assembly GEMMs, summed over iterations
+    double schur_time = 0;      // device time of the assemblies (s)
+    double device_time = 0;     // CUDA-event time of the solve on the library's stream (s)
+    double h2d_bytes = 0, d2h_bytes = 0;   // problem upload and result download
+};
+
+const char *status_string(int status);
+int exit_code_of(int status);
+
+// Parses command-line options (argv strings).  Returns 0 on success, 1 on a bad option.
+int parse_options(int argc, const char *const *argv, Options &opt, std::string &err);
+
+// Solves on the GPU; fills res.  Returns the exit code (0, 10-15) or a negative abort code.
+int solve_problem(const InputData &in, const Options &opt, ResultData &res);
+
+// A problem kept resident in HBM between solves (the benchmark's device-resident timing).
+struct Session;
+Session *session_create(const InputData &in, const Options &opt, std::string &err, int &rc);
+int session_solve(Session *s, const Options &opt, ResultData &res);
+void session_destroy(Session *s);
+
+// Reads an SDPA sparse file.  Returns 0 or an error message in err.
+int read_sdpa_file(const char *path, InputData &in, std::string &err);
+
+// Output (the C API's brisk_set_output routes it).
+void log_printf(int is_err, const char *fmt, ...);
+
+}  // namespace bsolve

@@ -1,0 +1,251 @@
+"""Seeded synthetic SDP instances in the numbers of an SDPA sparse file.
+
+A problem is what BRISK's C interface takes (``brisk_solve_data``, capi.c:175): block sizes
+``bs`` (LP blocks negative), the right-hand side ``c`` (m entries) and the entries
+``(mat, blk, i, j, v)``, 1-based as in the file, ``mat`` 0 being F0 = -C and 1..m the A_i
+(brisk.h:128-140).  BRISK solves (P) min <C,X> s.t. <A_i,X> = b_i, X >= 0 with C = -F0,
+A_i = F_i, b = c.
+
+The generators follow the workload descriptions the solver is measured on:
+
+* ``theta_problem``     Lovasz theta of a seeded G(n, p): one n x n block, C = -J,
+                        tr(X) = 1 and X_ij = 0 per edge (the SDPA form of the reference's
+                        tools/timelimit_test.sh:16-27, with n = 50, p = 0.5).
+* ``random_sdp``        one n x n block, m constraints, each A_i symmetric with
+                        round(density * n(n+1)/2) upper entries at uniform distinct positions
+                        and N(0,1) values, b_i = <A_i, I> (X0 = I is feasible),
+                        C = G G'/n + I with G ~ N(0,1) (n=400, m=2000, 1 %; n=1000, m=8000,
+                        0.5 %).
+* ``random_dense_batch`` independent small instances: n ~ U{8..64},
+                        m ~ U{n..floor(n(n+1)/4)}, dense N(0,1) symmetric A_i, b = A(I),
+                        C = G G'/n + I.
+
+All randomness comes from ``numpy.random.default_rng(seed)`` (or Python's ``random`` for the
+graph, as the reference's generator does), so the same seed gives the same bits everywhere.
+"""
+from __future__ import annotations
+
+import random as _pyrandom
+from dataclasses import dataclass, field
+from typing import List, Optional
+
+import numpy as np
+
+
+@dataclass
+class SdpaData:
+    """An SDP in SDPA sparse numbers (1-based entries; mat 0 is F0 = -C)."""
+    bs: np.ndarray          # int32 block sizes
+    c: np.ndarray           # float64, m
+    mat: np.ndarray         # int32
+    blk: np.ndarray         # int32
+    i: np.ndarray           # int32 (1-based, i <= j after normalisation)
+    j: np.ndarray           # int32
+    v: np.ndarray           # float64
+    name: str = ""
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def m(self) -> int:
+        return int(self.c.size)
+
+    @property
+    def nblk(self) -> int:
+        return int(self.bs.size)
+
+    @property
+    def nnz(self) -> int:
+        return int(self.v.size)
+
+    def args(self):
+        """The positional arguments of ``solve_sdpa`` (blocksizes, c, mat, blk, i, j, v)."""
+        return (self.bs, self.c, self.mat, self.blk, self.i, self.j, self.v)
+
+    # ---- dense views (small problems only: tests and the oracle) ----
+    def dense_blocks(self):
+        """C and A_1..A_m as dense symmetric matrices, one list per block:
+        returns (C[k], A[k][t]) with A[k] a (m, n, n) array for SDP block k."""
+        Cs, As = [], []
+        for k, n in enumerate(self.bs):
+            n = abs(int(n))
+            Ck = np.zeros((n, n))
+            Ak = np.zeros((self.m, n, n))
+            sel = self.blk == k + 1
+            for mt, ii, jj, vv in zip(self.mat[sel], self.i[sel] - 1, self.j[sel] - 1, self.v[sel]):
+                if mt == 0:
+                    Ck[ii, jj] = -vv
+                    Ck[jj, ii] = -vv
+                else:
+                    Ak[mt - 1, ii, jj] = vv
+                    Ak[mt - 1, jj, ii] = vv
+            Cs.append(Ck)
+            As.append(Ak)
+        return Cs, As
+
+
+def _normalise(mat, blk, i, j, v):
+    i = np.asarray(i, dtype=np.int32)
+    j = np.asarray(j, dtype=np.int32)
+    lo, hi = np.minimum(i, j), np.maximum(i, j)
+    return (np.asarray(mat, dtype=np.int32), np.asarray(blk, dtype=np.int32), lo, hi,
+            np.asarray(v, dtype=np.float64))
+
+
+def theta_problem(n: int = 50, p: float = 0.5, seed: int = 1) -> SdpaData:
+    """Lovasz theta SDP of a seeded Erdos-Renyi graph G(n, p).
+
+    max <J, X> s.t. tr X = 1, X_ij = 0 for each edge ij, X >= 0; in BRISK form
+    C = -J (F0 = J), A_1 = I (b_1 = 1), A_k = E_ij + E_ji (b_k = 0).  The edge list is
+    drawn with Python's ``random.Random(seed)`` in the order of the reference's generator.
+    """
+    rng = _pyrandom.Random(seed)
+    E = [(a, b) for a in range(1, n + 1) for b in range(a + 1, n + 1) if rng.random() < p]
+    m = 1 + len(E)
+    iu, ju = np.triu_indices(n)
+    mats = [np.zeros(iu.size, np.int32), np.ones(n, np.int32), np.arange(2, m + 1, dtype=np.int32)]
+    ii = [iu + 1, np.arange(1, n + 1), np.array([e[0] for e in E], np.int32)]
+    jj = [ju + 1, np.arange(1, n + 1), np.array([e[1] for e in E], np.int32)]
+    vv = [np.ones(iu.size), np.ones(n), np.ones(len(E))]
+    mat = np.concatenate(mats)
+    d = _normalise(mat, np.ones(mat.size, np.int32), np.concatenate(ii), np.concatenate(jj), np.concatenate(vv))
+    c = np.zeros(m)
+    c[0] = 1.0
+    return SdpaData(np.array([n], np.int32), c, *d, name=f"theta_G({n},{p})_seed{seed}",
+                    meta=dict(kind="theta", n=n, p=p, seed=seed, edges=len(E)))
+
+
+def _random_upper_positions(rng, n, k):
+    """k distinct uniform positions of the upper triangle (with diagonal) of an n x n matrix."""
+    tot = n * (n + 1) // 2
+    lin = rng.choice(tot, size=k, replace=False)
+    lin.sort()
+    # invert the column-major upper packing: column j holds rows 0..j, starting at j(j+1)/2
+    jcol = ((np.sqrt(8.0 * lin + 1.0) - 1.0) / 2.0).astype(np.int64)
+    jcol -= (jcol * (jcol + 1) // 2 > lin)
+    jcol += ((jcol + 1) * (jcol + 2) // 2 <= lin)
+    irow = lin - jcol * (jcol + 1) // 2
+    return irow, jcol
+
+
+def random_sdp(n: int = 400, m: int = 2000, density: float = 0.01, seed: int = 0) -> SdpaData:
+    """Dense-C random SDP with sparse N(0,1) constraints (one n x n block).
+
+    Each A_i has round(density * n(n+1)/2) upper-triangle entries at distinct uniform
+    positions with N(0,1) values; b_i = <A_i, I> so X0 = I is feasible; C = G G'/n + I.
+    """
+    rng = np.random.default_rng(seed)
+    k = int(round(density * n * (n + 1) / 2))
+    G = rng.standard_normal((n, n))
+    C = G @ G.T / n + np.eye(n)
+    mats, ii, jj, vv = [], [], [], []
+    iu, ju = np.triu_indices(n)
+    mats.append(np.zeros(iu.size, np.int32))
+    ii.append(iu + 1)
+    jj.append(ju + 1)
+    vv.append(-C[iu, ju])
+    b = np.zeros(m)
+    for t in range(m):
+        r, cc = _random_upper_positions(rng, n, k)
+        val = rng.standard_normal(k)
+        mats.append(np.full(k, t + 1, np.int32))
+        ii.append(r + 1)
+        jj.append(cc + 1)
+        vv.append(val)
+        b[t] = val[r == cc].sum()
+    mat = np.concatenate(mats)
+    d = _normalise(mat, np.ones(mat.size, np.int32), np.concatenate(ii), np.concatenate(jj), np.concatenate(vv))
+    return SdpaData(np.array([n], np.int32), b, *d, name=f"random_sdp_n{n}_m{m}_d{density}_seed{seed}",
+                    meta=dict(kind="random", n=n, m=m, density=density, seed=seed, upper_per_con=k))
+
+
+def random_dense_instance(rng, n: int, m: int, name: str = "") -> SdpaData:
+    """One small dense instance: A_i dense N(0,1) symmetric, b = A(I), C = G G'/n + I."""
+    iu, ju = np.triu_indices(n)
+    G = rng.standard_normal((n, n))
+    C = G @ G.T / n + np.eye(n)
+    U = rng.standard_normal((m, iu.size))             # upper entries of each A_i
+    b = U[:, iu == ju].sum(axis=1)
+    mat = np.concatenate([np.zeros(iu.size, np.int32), np.repeat(np.arange(1, m + 1, dtype=np.int32), iu.size)])
+    i = np.concatenate([iu + 1, np.tile(iu + 1, m)])
+    j = np.concatenate([ju + 1, np.tile(ju + 1, m)])
+    v = np.concatenate([-C[iu, ju], U.ravel()])
+    d = _normalise(mat, np.ones(mat.size, np.int32), i, j, v)
+    return SdpaData(np.array([n], np.int32), b, *d, name=name, meta=dict(kind="dense", n=n, m=m))
+
+
+def random_dense_batch(count: int = 4096, nmin: int = 8, nmax: int = 64, seed: int = 0,
+                       sizes_only: bool = False):
+    """The uneven batch: n ~ U{nmin..nmax}, m ~ U{n..floor(n(n+1)/4)} per instance.
+
+    Returns the list of (n, m) when ``sizes_only``; else the list of SdpaData instances."""
+    rng = np.random.default_rng(seed)
+    ns = rng.integers(nmin, nmax + 1, size=count)
+    ms = np.array([rng.integers(n, n * (n + 1) // 4 + 1) for n in ns])
+    if sizes_only:
+        return list(zip(ns.tolist(), ms.tolist()))
+    out = []
+    for q, (n, m) in enumerate(zip(ns, ms)):
+        sub = np.random.default_rng([seed, q])
+        out.append(random_dense_instance(sub, int(n), int(m), name=f"batch{seed}_{q}"))
+    return out
+
+
+# ---------------------------------------------------------------------------------------
+# SDPA sparse files
+# ---------------------------------------------------------------------------------------
+def write_sdpa(d: SdpaData, path: str) -> None:
+    """Write an SDPA sparse file (values with 17 significant digits: reading it back gives
+    the same doubles)."""
+    with open(path, "w") as f:
+        f.write(f'"{d.name}"\n{d.m}\n{d.nblk}\n')
+        f.write(" ".join(str(int(b)) for b in d.bs) + "\n")
+        f.write(" ".join(repr(float(x)) for x in d.c) + "\n")
+        arr = np.empty(d.nnz, dtype=[("mat", "i4"), ("blk", "i4"), ("i", "i4"), ("j", "i4"), ("v", "f8")])
+        arr["mat"], arr["blk"], arr["i"], arr["j"], arr["v"] = d.mat, d.blk, d.i, d.j, d.v
+        np.savetxt(f, arr, fmt=["%d", "%d", "%d", "%d", "%.17g"])
+
+
+def read_sdpa(path: str) -> SdpaData:
+    """Read an SDPA sparse file (comments '"' / '*' lines, separators , ( ) { })."""
+    with open(path) as f:
+        toks = []
+        body = []
+        header_done = False
+        for line in f:
+            s = line.strip()
+            if not s or s[0] in '"*':
+                continue
+            s = s.translate(str.maketrans(",(){}", "     "))
+            if not header_done:
+                toks.extend(s.split())
+                if len(toks) >= 2:
+                    m, nb = int(float(toks[0])), int(float(toks[1]))
+                    if len(toks) >= 2 + nb + m:
+                        header_done = True
+                        rest = toks[2 + nb + m:]
+                        if rest:
+                            body.append(" ".join(rest))
+                continue
+            body.append(s)
+    m, nb = int(float(toks[0])), int(float(toks[1]))
+    bs = np.array([int(float(x)) for x in toks[2:2 + nb]], np.int32)
+    c = np.array([float(x) for x in toks[2 + nb:2 + nb + m]])
+    vals = np.array(" ".join(body).split(), dtype=np.float64).reshape(-1, 5) if body else np.zeros((0, 5))
+    d = _normalise(vals[:, 0].astype(np.int32), vals[:, 1].astype(np.int32), vals[:, 2].astype(np.int32),
+                   vals[:, 3].astype(np.int32), vals[:, 4])
+    keep = d[4] != 0
+    return SdpaData(bs, c, *(a[keep] for a in d), name=path)
+
+
+WORKLOADS = {
+    "theta50": dict(fn=theta_problem, kw=dict(n=50, p=0.5, seed=1)),
+    "rand400": dict(fn=random_sdp, kw=dict(n=400, m=2000, density=0.01, seed=0)),
+    "rand1000": dict(fn=random_sdp, kw=dict(n=1000, m=8000, density=0.005, seed=0)),
+}
+
+
+def workload(name: str, **over) -> SdpaData:
+    w = WORKLOADS[name]
+    kw = dict(w["kw"])
+    kw.update(over)
+    return w["fn"](**kw)

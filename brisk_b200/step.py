@@ -1,0 +1,69 @@
+"""ctypes binding of the step-level C ABI (include/bgpu.h) for callers holding device memory.
+
+Device buffers are passed as integer addresses (``torch.Tensor.data_ptr()`` in the tests and the
+benchmark; PyTorch only allocates).  Every call checks the returned status and raises
+``BgpuError`` on failure; nothing falls back to the CPU.
+"""
+from __future__ import annotations
+
+import ctypes
+
+from ._core import load_library
+
+STATUS = {0: "OK", -1: "CUDA error", -2: "bad argument", -3: "not positive definite", -4: "device wait timed out",
+          -5: "out of device memory", -6: "unsupported", -7: "size above the maximum"}
+
+
+class BgpuError(RuntimeError):
+    def __init__(self, name, rc):
+        super().__init__(f"{name} failed: {STATUS.get(rc, rc)} ({rc})")
+        self.rc = rc
+
+
+_sig_done = False
+
+
+def lib():
+    global _sig_done
+    L = load_library()
+    if _sig_done:
+        return L
+    P, I, D, I64, SZ = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int64, ctypes.c_size_t
+    sigs = {
+        "bgpu_sync": ([P], I),
+        "bgpu_schur_ws_bytes": ([I, I, I], SZ),
+        "bgpu_schur_chunk_default": ([I, I], I),
+        "bgpu_schur_assemble": ([I, I, I, P, P, P, P, P, P, P, I, I, P, SZ, P], I),
+        "bgpu_potrf": ([I, P, I, P, P, P, P], I),
+        "bgpu_potrf_f32": ([I, P, I, P, P, P, P], I),
+        "bgpu_trsv": ([I, P, I, P, P, I, P, I, P, P], I),
+        "bgpu_trsv_f32": ([I, P, I, P, P, I, P, I, P, P], I),
+        "bgpu_trtri": ([I, P, I, P, P, I, P], I),
+        "bgpu_dgemm": ([I, I, I, I, I, D, P, I64, P, I64, D, P, I64, I, P], I),
+        "bgpu_gemm_tf32x3": ([I, I, I, P, P, I64, P, P, I64, P, I64, P], I),
+        "bgpu_split_tf32": ([I64, P, P, P, P], I),
+        "bgpu_symv": ([I, D, P, I, P, D, P, P], I),
+        "bgpu_aop": ([I, I, P, P, P, P, P, D, D, P, P], I),
+    }
+    for name, (args, res) in sigs.items():
+        f = getattr(L, name)
+        f.argtypes, f.restype = args, res
+    L.bgpu_version.restype = ctypes.c_char_p
+    _sig_done = True
+    return L
+
+
+def call(name, *args):
+    """Call bgpu_<name>(*args) and raise BgpuError on a nonzero status."""
+    rc = getattr(lib(), "bgpu_" + name)(*args)
+    if rc != 0:
+        raise BgpuError(name, rc)
+    return rc
+
+
+def ws_bytes(n, chunk, precision):
+    return int(lib().bgpu_schur_ws_bytes(n, chunk, precision))
+
+
+def chunk_default(n, precision):
+    return int(lib().bgpu_schur_chunk_default(n, precision))

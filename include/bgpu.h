@@ -1,0 +1,121 @@
+/*
+ * bgpu.h - step-level C ABI of the B200 Newton-step kernels.
+ *
+ * The reference's hot functions are static inside solver.c and sparsechol.c, so this
+ * interface is the framework's own; each entry mirrors the contract of the reference
+ * function it replaces (cited per entry).  Every pointer argument named d_* is device memory
+ * (allocated by the caller: cudaMalloc, or torch tensors in the tests); stream is a
+ * cudaStream_t (NULL for the default stream).  Every call returns a status: 0 on success,
+ * BGPU_ERR_* (< 0) otherwise; no exception crosses the ABI.  Calls are asynchronous on the
+ * stream unless stated; bgpu_sync waits for it.
+ */
+#ifndef BGPU_H
+#define BGPU_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define BGPU_API __attribute__((visibility("default")))
+#else
+#define BGPU_API
+#endif
+
+#define BGPU_OK 0
+#define BGPU_ERR_CUDA (-1)
+#define BGPU_ERR_ARG (-2)
+#define BGPU_ERR_NOTPD (-3)
+#define BGPU_ERR_TIMEOUT (-4)
+#define BGPU_ERR_NOMEM (-5)
+#define BGPU_ERR_UNSUPPORTED (-6)
+#define BGPU_ERR_TOOBIG (-7)
+
+BGPU_API int bgpu_sync(void *stream);
+BGPU_API const char *bgpu_version(void);
+/* Number of kernels this library has launched since it was loaded (all entry points). */
+BGPU_API long long bgpu_launch_count(void);
+
+/* A problem kept resident in device memory between solves: bgpu_session_create takes the
+ * numbers of brisk_solve_data (capi.c:175) and the options, uploads the scaled problem and
+ * returns a handle (NULL on failure, *rc the exit code: 1 bad options, 2 bad problem, < 0 GPU
+ * failure); bgpu_session_solve runs one interior-point solve from the resident data into res
+ * (a brisk_result_new handle) and returns the exit code as brisk_solve_data.  Extension of
+ * this build: the reference re-reads the problem on every call. */
+struct BriskResult;
+typedef struct bgpu_session bgpu_session;
+BGPU_API bgpu_session *bgpu_session_create(int m, int nblk, const int *bs, const double *c, int64_t nnz,
+                                           const int *mat, const int *blk, const int *i, const int *j,
+                                           const double *v, int nopt, const char *const *opts, int *rc);
+BGPU_API int bgpu_session_solve(bgpu_session *s, int nopt, const char *const *opts, struct BriskResult *res);
+BGPU_API void bgpu_session_destroy(bgpu_session *s);
+/* Measures of the last solve of res: [0] device time (s, CUDA events on the library's
+ * stream), [1] assembly device time (s), [2] assembly algorithmic flops, [3] host-to-device
+ * bytes, [4] device-to-host bytes, [5] iterations, [6] float factorizations, [7] PCG steps. */
+BGPU_API int bgpu_result_measures(const struct BriskResult *res, double *out8);
+
+/* Workspace bytes of bgpu_schur_assemble for a block of order n, chunk constraints per GEMM
+ * (8, 16, 32 or 64; 0 picks the default) and precision (0 FP64, 1 3xTF32). */
+BGPU_API size_t bgpu_schur_ws_bytes(int n, int chunk, int precision);
+BGPU_API int bgpu_schur_chunk_default(int n, int precision);
+
+/* Schur complement of one SDP block, accumulated into the full symmetric d_M (m x m,
+ * column-major): M[con_a, con_b] += <A_b, X A_a Zi> for all constraint pairs of the block.
+ * Constraints are given constraint-major: local constraint t has global index d_con[t] and
+ * entries d_cpos/d_cval[d_cptr[t] .. d_cptr[t+1]) of the full (both triangles) expansion, with
+ * positions p + q n ascending.  Replaces schur_sdp / schur_sdp_id (solver.c:1969, 2339-3021)
+ * for the row-product route. */
+BGPU_API int bgpu_schur_assemble(int n, int m, int ncon, const int *d_con, const long long *d_cptr,
+                                 const int *d_cpos, const double *d_cval, const double *d_X, const double *d_Zi,
+                                 double *d_M, int precision, int chunk, void *d_ws, size_t ws_bytes, void *stream);
+
+/* In-place Cholesky L L' = A of the lower triangle (column-major, lda); d_dinv receives the
+ * inverses of the 64 x 64 diagonal blocks (ceil(n/64)*4096 entries), *d_info the first failing
+ * column (1-based) or 0, *d_pmin the smallest squared pivot.  Replaces brisk_dpotrf
+ * (sparsechol.c:3822) / chol_lower (solver.c:679); the float form replaces brisk_spotrf
+ * (sparsechol.c:3841). */
+BGPU_API int bgpu_potrf(int n, double *d_A, int lda, double *d_dinv, int *d_info, double *d_pmin, void *stream);
+BGPU_API int bgpu_potrf_f32(int n, float *d_A, int lda, float *d_dinv, int *d_info, double *d_pmin, void *stream);
+
+/* x <- L^-1 x (trans 0) or L^-T x (trans 1) with the factor of bgpu_potrf.  d_flags holds
+ * ceil(n/64) ints; epoch must differ from the value of every earlier call on the same flags;
+ * *d_err is set to 1 when a bounded device wait gives up.  Replaces brisk_dpotrs1 /
+ * brisk_spotrs1 (sparsechol.c:4060-4180). */
+BGPU_API int bgpu_trsv(int n, const double *d_L, int lda, const double *d_dinv, double *d_x, int trans,
+                       int *d_flags, int epoch, int *d_err, void *stream);
+BGPU_API int bgpu_trsv_f32(int n, const float *d_L, int lda, const float *d_dinv, float *d_x, int trans,
+                           int *d_flags, int epoch, int *d_err, void *stream);
+
+/* Linv = L^-1 from the factor of bgpu_potrf (the first half of brisk_dpotri_full,
+ * sparsechol.c:4190). */
+BGPU_API int bgpu_trtri(int n, const double *d_L, int lda, const double *d_dinv, double *d_Linv, int ldi,
+                        void *stream);
+
+/* C = alpha op(A) op(B) + beta C in FP64 on the DMMA tensor path (a_kmajor: A(i,k) =
+ * A[i*lda+k], else A[i+k*lda]; b_kmajor: B(k,j) = B[k+j*ldb], else B[k*ldb+j]; C column-
+ * major; lower: only i >= j).  The BLAS dgemm/dsyrk calls of the reference's dense routes. */
+BGPU_API int bgpu_dgemm(int a_kmajor, int b_kmajor, int M, int N, int K, double alpha, const double *d_A,
+                        int64_t lda, const double *d_B, int64_t ldb, double beta, double *d_C, int64_t ldc,
+                        int lower, void *stream);
+
+/* G = (Ah+Al)(Bh+Bl) by 3xTF32 on tcgen05 (A K-major rows, B K-major columns, G column-major). */
+BGPU_API int bgpu_gemm_tf32x3(int M, int N, int K, const float *d_Ah, const float *d_Al, int64_t lda,
+                              const float *d_Bh, const float *d_Bl, int64_t ldb, float *d_G, int64_t ldg,
+                              void *stream);
+BGPU_API int bgpu_split_tf32(int64_t n, const double *d_x, float *d_hi, float *d_lo, void *stream);
+
+/* y = alpha M x + beta y for a full symmetric M (schur_mv_, solver.c:4815). */
+BGPU_API int bgpu_symv(int n, double alpha, const double *d_M, int ldm, const double *d_x, double beta,
+                       double *d_y, void *stream);
+
+/* out[con[t]] = beta out[con[t]] + alpha <A_t, D> (blk_Aop, solver.c:884-994). */
+BGPU_API int bgpu_aop(int n, int ncon, const int *d_con, const long long *d_cptr, const int *d_cpos,
+                      const double *d_cval, const double *d_D, double alpha, double beta, double *d_out,
+                      void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,333 @@
+"""Oracle: a CPU (numpy, FP64) restatement of the reference's SDP interior-point Newton step.
+
+TEST INFRASTRUCTURE ONLY.  Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline
+leg may import this module, and only as the checker; the product (brisk_b200/libbrisk.so) never
+calls it and has no CPU path.
+
+It restates, on dense matrices (small sizes: tests), the reference BRISK 1.7 algorithm:
+
+* problem_prepare        row equilibration and b/C scaling         problem.c:1866-1910
+* start_sdpt3            X0 = xi I, Z0 = eta I, y = 0               solver.c:6622-6661
+* schur (HKM)            M_ij = <A_i, X A_j Z^-1>                    solver.c:1969, 2339-3021
+* the infeasible-start HKM predictor-corrector loop                   solver.c:14394-15188
+  (residuals 14423-14484, theta R0 recurrence 14317-14326 / 14587-14607, rhs pieces
+  14715-14735, predictor 14787-14818, sigma rule 14829-14873, corrector 14998-15050,
+  refinement of A(dX) = rp 15058-15105, try_step 6393-6447)
+* maxstep                the largest alpha with V + alpha dV >= 0     solver.c:6300-6390
+  (exact eigenvalues here; the reference's Lanczos estimate theta - residual is <= it)
+* DIMACS errors on the data as given                                  postsolve.c:2880-2897
+* the final status rule                                               main.c:2349-2362
+
+Pinned against the reference's own runs on the same seeded inputs (tests/golden/, made by
+tests/golden/make_golden.py from oracle/_ref/brisk_ref, the reference compiled by
+oracle/Makefile), and against the reference's published golden value for theta1
+(INSTALL.md:44-45).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+
+@dataclass
+class Scaled:
+    """The scaled problem (problem_prepare): dense blocks, one list entry per block."""
+    m: int
+    C: list                 # scaled C per block (n x n)
+    A: list                 # per block: (m, n, n) scaled A_i (zero for constraints not in the block)
+    b: np.ndarray           # scaled b
+    b0: np.ndarray          # b as given
+    d: np.ndarray
+    du: np.ndarray
+    bs: float
+    cs: float
+    normb1: float
+    normb2: float
+    normC1: float
+    normC2: float
+    C0: list = field(default_factory=list)   # C as given
+    A0: list = field(default_factory=list)   # A as given
+
+
+def scale_problem(data) -> Scaled:
+    """problem_prepare (problem.c:1866-1910) on dense blocks."""
+    C0, A0 = data.dense_blocks()
+    m = data.m
+    b0 = np.array(data.c, dtype=np.float64)
+    nrm2 = np.zeros(m)
+    c2 = c1 = 0.0
+    for Ck, Ak in zip(C0, A0):
+        nrm2 += np.einsum("tij,tij->t", Ak, Ak)            # sum of squares of the full expansion
+        c2 += float(np.sum(Ck * Ck))
+        c1 += float(np.sum(np.abs(Ck)))
+    normC2, normC1 = np.sqrt(c2), c1
+    normb1, normb2 = float(np.sum(np.abs(b0))), float(np.sqrt(np.sum(b0 * b0)))
+    d = np.where(nrm2 > 0, 1.0 / np.sqrt(np.where(nrm2 > 0, nrm2, 1.0)), 1.0)
+    nb = float(np.sqrt(np.sum((d * b0) ** 2)))
+    bs = nb if nb > 1 else 1.0
+    A = [Ak * d[:, None, None] for Ak in A0]
+    b = b0 * d
+    du = bs / d
+    cs = normC2 if normC2 > 1 else 1.0
+    b = b / bs
+    C = [Ck / cs for Ck in C0]
+    return Scaled(m, C, A, b, b0, d, du, bs, cs, normb1, normb2, normC1, normC2, C0, A0)
+
+
+def start_point(S: Scaled):
+    """start_sdpt3 (solver.c:6622-6661): per block xi, eta; X0 = xi I, Z0 = eta I, y0 = 0."""
+    X, Z, xis, etas = [], [], [], []
+    for Ck, Ak in zip(S.C, S.A):
+        n = Ck.shape[0]
+        nC = float(np.sqrt(np.sum(Ck * Ck)))
+        a = np.sqrt(np.einsum("tij,tij->t", Ak, Ak))
+        inb = a > 0                                            # constraints touching the block
+        maxA = float(a[inb].max()) if inb.any() else 0.0
+        ratio = float(((1 + np.abs(S.b[inb])) / (1 + a[inb])).max()) if inb.any() else 0.0
+        xi = max(10.0, max(np.sqrt(n), n * ratio))
+        eta = max(10.0, max(np.sqrt(n), max(maxA, nC)))
+        X.append(xi * np.eye(n))
+        Z.append(eta * np.eye(n))
+        xis.append(xi)
+        etas.append(eta)
+    return X, Z, np.zeros(S.m), xis, etas
+
+
+def schur(A_blocks, X_blocks, Zi_blocks):
+    """M_ij = sum_blocks <A_i, X A_j Zi> (the HKM Schur complement, dense formula)."""
+    m = A_blocks[0].shape[0]
+    M = np.zeros((m, m))
+    for Ak, Xk, Zik in zip(A_blocks, X_blocks, Zi_blocks):
+        G = np.einsum("pq,tqr,rs->tps", Xk, Ak, Zik)        # G_j = X A_j Zi
+        M += np.einsum("ipq,jpq->ij", Ak, G)
+    return M
+
+
+def aop(A_blocks, D_blocks):
+    return sum(np.einsum("tij,ij->t", Ak, Dk) for Ak, Dk in zip(A_blocks, D_blocks))
+
+
+def atop(A_blocks, y):
+    return [np.einsum("t,tij->ij", y, Ak) for Ak in A_blocks]
+
+
+def lam_min(L, D):
+    """lambda_min(L^-1 D L^-T) (exact)."""
+    Li = np.linalg.inv(L)
+    B = Li @ D @ Li.T
+    return float(np.linalg.eigvalsh(0.5 * (B + B.T))[0])
+
+
+def maxstep(Ls, dVs):
+    """maxstep (solver.c:6300-6390) with exact eigenvalues: 1e30 when unbounded."""
+    a = 1e30
+    for L, dV in zip(Ls, dVs):
+        lam = lam_min(L, dV)
+        ak = 1e30 if lam >= 0 else -1.0 / lam
+        a = min(a, ak)
+    return a
+
+
+def try_step(Vs, dVs, alpha):
+    """try_step (solver.c:6393-6447): alpha *= 0.8 until every V + alpha dV is Cholesky-definite."""
+    a = alpha
+    for _ in range(40):
+        new = [V + a * dV for V, dV in zip(Vs, dVs)]
+        try:
+            Ls = [np.linalg.cholesky(V) for V in new]
+            return True, a, new, Ls
+        except np.linalg.LinAlgError:
+            a *= 0.8
+    return False, a, Vs, None
+
+
+def dimacs(S: Scaled, Xs, y):
+    """DIMACS errors 1..6 of (X, y) on the data as given, with Z = C - A'y
+    (postsolve.c:2880-2897); X, y in the scaled problem's units."""
+    Xo = [S.bs * X for X in Xs]
+    yo = S.cs * S.d * y
+    Zo = [Ck - Ak_y for Ck, Ak_y in zip(S.C0, atop(S.A0, yo))]
+    pobj = sum(float(np.sum(Ck * Xk)) for Ck, Xk in zip(S.C0, Xo))
+    dobj = float(S.b0 @ yo)
+    r = aop(S.A0, Xo) - S.b0
+    xz = sum(float(np.sum(Xk * Zk)) for Xk, Zk in zip(Xo, Zo))
+    lamx = min(float(np.linalg.eigvalsh(Xk)[0]) for Xk in Xo)
+    lamz = min(float(np.linalg.eigvalsh(Zk)[0]) for Zk in Zo)
+    den = 1 + abs(pobj) + abs(dobj)
+    err = np.array([np.linalg.norm(r) / (1 + S.normb1), max(0.0, -lamx) / (1 + S.normb1), 0.0,
+                    max(0.0, -lamz) / (1 + S.normC1), (pobj - dobj) / den, xz / den])
+    return err, pobj, dobj, Xo, yo, Zo
+
+
+STATUS = {0: "OPTIMAL", 1: "PRIMAL INFEASIBLE", 2: "DUAL INFEASIBLE", 3: "ITERATION LIMIT",
+          4: "NUMERICAL DIFFICULTIES", 5: "REDUCED ACCURACY", 6: "TIME LIMIT"}
+
+
+def solve(data, tol=1e-8, maxit=100, gamma_max=0.99, red_acc=None, log=None):
+    """The infeasible-start HKM predictor-corrector loop (solver.c:14394-15188), FP64, dense.
+
+    Returns a dict with status, iterations, pobj, dobj, dimacs (errors 1..6), the iteration-0
+    measures (it0: pobj, dobj, pinf, dinf, gap, mu in the reference's -v table convention) and
+    the first Schur complement M0 (scaled problem)."""
+    if red_acc is None:
+        red_acc = max(1e-6, 100 * tol)
+    S = scale_problem(data)
+    Xs, Zs, y, xis, etas = start_point(S)
+    LX = [np.linalg.cholesky(X) for X in Xs]
+    LZ = [np.linalg.cholesky(Z) for Z in Zs]
+    m = S.m
+    Ntot = sum(X.shape[0] for X in Xs)
+    R0 = [Ck - Zk - Ak for Ck, Zk, Ak in zip(S.C, Zs, atop(S.A, y))]
+    theta = 1.0
+    r0norm = float(np.sqrt(sum(np.sum(R * R) for R in R0)))
+    nbs = float(np.linalg.norm(S.b))
+    best_score, it_best, best, ybest, XZbest = np.inf, 0, None, y.copy(), None
+    status, stall, alp, ald, sigma = -1, 0, 0.0, 0.0, 0.0
+    out = {"M0": None, "it0": None, "table": []}
+    it = 0
+    for it in range(maxit + 1):
+        Zi = [np.linalg.inv(L).T @ np.linalg.inv(L) for L in LZ]
+        Zi = [0.5 * (Q + Q.T) for Q in Zi]
+        rp = S.b - aop(S.A, Xs)
+        ATy = atop(S.A, y)
+        Fs = [a + Zk for a, Zk in zip(ATy, Zs)]
+        nCR2 = sum(float(np.sum(F * F)) for F in Fs)
+        Fd = [F - Ck for F, Ck in zip(Fs, S.C)]
+        pobj = sum(float(np.sum(Ck * Xk)) for Ck, Xk in zip(S.C, Xs))
+        xz = sum(float(np.sum(Xk * Zk)) for Xk, Zk in zip(Xs, Zs))
+        rdn2 = sum(float(np.sum(F * F)) for F in Fd)
+        dev2 = sum(float(np.sum((F + theta * R) ** 2)) for F, R in zip(Fd, R0))
+        dobj = float(S.b @ y)
+        mu = xz / Ntot
+        rpo = float(np.linalg.norm(rp * S.du))
+        rdo = S.cs * np.sqrt(rdn2)
+        sc = S.bs * S.cs
+        po, dob = sc * pobj, sc * dobj
+        pinf = rpo / (1 + S.normb2)
+        dinf = rdo / (1 + S.normC2)
+        oden = 1 + abs(po) + abs(dob)
+        relgap = abs(po - dob) / oden
+        relcomp = sc * xz / oden
+        row = dict(it=it, pobj=-po, dobj=-dob, pinf=pinf, dinf=dinf, gap=relgap, mu=sc * mu)
+        out["table"].append(row)
+        if it == 0:
+            out["it0"] = row
+        if log:
+            log(f"{it:3d} {-po:+.8e} {-dob:+.8e} {pinf:.2e} {dinf:.2e} {relgap:.2e} {sc * mu:.2e} "
+                f"{alp:.3f} {ald:.3f} {sigma:.3f}")
+        score = max(relgap, relcomp, pinf, dinf)
+        err_it = (rpo / (1 + S.normb1), rdo / (1 + S.normC1), (po - dob) / oden, sc * xz / oden)
+        if score < best_score:
+            best_score, it_best, ybest = score, it, y.copy()
+            best = err_it
+            XZbest = ([X.copy() for X in Xs], [Z.copy() for Z in Zs])
+        if score < tol:
+            status = 0
+            break
+        if it > it_best and max(abs(e) for e in best) <= 0.5 * tol:
+            status = 4
+            break
+        if dobj > 0 and np.sqrt(nCR2) / dobj < 1e-8 and it > 5:
+            status = 1
+            break
+        nAX = float(np.linalg.norm(S.b - rp))
+        if pobj < 0 and nAX / (-pobj) < 1e-8 and it > 5:
+            status = 2
+            break
+        if it == maxit:
+            status = 3
+            break
+        if stall >= 3 or (it - it_best >= 5 and best_score < 1e-6) or (it - it_best >= 8 and best_score < 1e-4) \
+                or it - it_best >= 12:
+            status = 4
+            break
+        dev = np.sqrt(dev2)
+        if dev > 1e-10 * (1.0 + theta * r0norm) and dev > 1e-12:
+            theta, r0norm = 1.0, float(np.sqrt(rdn2))
+            R0 = [-F for F in Fd]
+        if theta * r0norm <= 1e-13:
+            theta = 0.0
+        M = schur(S.A, Xs, Zi)
+        if out["M0"] is None:
+            out["M0"] = M.copy()
+        Minv = np.linalg.inv(M)
+        a0 = aop(S.A, Zi)
+        h = aop(S.A, [theta * Zk @ R @ Xk for Zk, R, Xk in zip(Zi, R0, Xs)]) if theta > 0 else np.zeros(m)
+        dy = Minv @ (S.b + h)
+        dZ = [-a + theta * R for a, R in zip(atop(S.A, dy), R0)]
+        dX = []
+        for Zk, dZk, Xk in zip(Zi, dZ, Xs):
+            G = Zk @ dZk @ Xk
+            dX.append(-0.5 * (G + G.T) - Xk)
+        ap = min(1.0, maxstep(LX, dX))
+        ad = min(1.0, maxstep(LZ, dZ))
+        xdz = sum(float(np.sum(a * b)) for a, b in zip(Xs, dZ))
+        dxz = sum(float(np.sum(a * b)) for a, b in zip(dX, Zs))
+        dxdz = sum(float(np.sum(a * b)) for a, b in zip(dX, dZ))
+        mu_a = (xz + ap * dxz + ad * xdz + ap * ad * dxdz) / Ntot
+        frac = max(0.0, mu_a / mu)
+        mina = min(ap, ad)
+        expon = max(1.0, 3 * mina * mina) if relgap > 1e-6 else 3.0
+        sigma = min(1.0, frac ** expon)
+        gamma = 0.9 + (gamma_max - 0.9) * mina
+        smu = sigma * mu
+        Q = [Zk @ dZk @ dXk for Zk, dZk, dXk in zip(Zi, dZ, dX)]
+        rhs = S.b - smu * a0 + aop(S.A, Q) + h
+        dy = Minv @ rhs
+        dZ = [-a + theta * R for a, R in zip(atop(S.A, dy), R0)]
+        dX = []
+        for Zk, dZk, Xk, Qk in zip(Zi, dZ, Xs, Q):
+            G = Zk @ dZk @ Xk + Qk
+            dX.append(-0.5 * (G + G.T) + smu * Zk - Xk)
+        for _ in range(3):
+            ev = rp - aop(S.A, dX)
+            ne, nrp = np.linalg.norm(ev), np.linalg.norm(rp)
+            if not (ne > 1e-2 * nrp and ne > 1e-3 * tol * (1 + nbs)):
+                break
+            wv = Minv @ ev
+            Qd = atop(S.A, wv)
+            Gs = []
+            for Zk, Qk, Xk in zip(Zi, Qd, Xs):
+                G = Zk @ Qk @ Xk
+                Gs.append(0.5 * (G + G.T))
+            ne2 = np.linalg.norm(ev - aop(S.A, Gs))
+            if not (ne2 < 0.5 * ne):
+                break
+            dy = dy + wv
+            dZ = [a - b for a, b in zip(dZ, Qd)]
+            dX = [a + b for a, b in zip(dX, Gs)]
+        apr = min(1.0, maxstep(LX, dX))
+        adr = min(1.0, maxstep(LZ, dZ))
+        apn, adn = min(1.0, gamma * apr), min(1.0, gamma * adr)
+        if pinf < 1e-6:
+            ev = rp - aop(S.A, dX)
+            nrp, nev = np.linalg.norm(rp), np.linalg.norm(ev)
+            lim = max(1e3, 1e-6 / max(pinf, 1e-300)) * nrp
+            if nev > lim and nrp > 0:
+                apn = min(apn, lim / nev)
+        okp, apn, Xs, LXn = try_step(Xs, dX, apn)
+        okd, adn, Zs, LZn = try_step(Zs, dZ, adn)
+        if not okp or not okd:
+            status = 4
+            break
+        LX, LZ = LXn, LZn
+        y = y + adn * dy
+        theta *= (1.0 - adn)
+        alp, ald = apn, adn
+        stall = stall + 1 if (apn < 1e-6 and adn < 1e-6) else 0
+    if status not in (0, 1, 2) and XZbest is not None and best_score < score:
+        y = ybest
+        Xs, Zs = XZbest
+    err, pobj_o, dobj_o, Xo, yo, Zo = dimacs(S, Xs, y)
+    acc = max(err[0], err[1], err[3], abs(err[4]), abs(err[5]))
+    if status in (0, 3, 4, 5, 6):
+        if acc <= tol:
+            status = 0
+        elif acc <= red_acc:
+            status = 5
+        elif status in (0, 5):
+            status = 4
+    out.update(status=status, status_str=STATUS.get(status, "?"), iterations=it, pobj=pobj_o, dobj=dobj_o,
+               dimacs=err, X=Xo, y=yo, Z=Zo, xi=xis, eta=etas, scaled=S)
+    return out

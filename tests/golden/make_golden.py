@@ -1,0 +1,89 @@
+"""Generate tests/golden/ref_runs.json: the reference BRISK solver's own results on seeded
+instances of the workloads, for the parity tests.
+
+Runs oracle/_ref/brisk_ref (the reference compiled from its sources by oracle/Makefile) on SDPA
+files written by brisk_b200.problems, with the reference's presolves off so that it solves the
+problem as given, and records per run: status, iterations, objectives, the six DIMACS errors,
+the iteration table of -v (pobj, dobj, pinf, dinf, gap, mu per iteration) and the time.
+
+usage: python tests/golden/make_golden.py [--big]    (--big adds the n=400, m=2000 instance)
+"""
+from __future__ import annotations
+
+import json
+import os
+import re
+import subprocess
+import sys
+import tempfile
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+from brisk_b200.problems import random_sdp, theta_problem, write_sdpa  # noqa: E402
+
+REF = os.path.join(ROOT, "oracle", "_ref", "brisk_ref")
+OUT = os.path.join(ROOT, "tests", "golden", "ref_runs.json")
+AS_GIVEN = ["-sym", "none", "-symalg", "0", "-chordal", "0", "-nofr", "-deprows", "0"]
+
+INSTANCES = {
+    "theta50": (theta_problem, dict(n=50, p=0.5, seed=1)),
+    "theta30": (theta_problem, dict(n=30, p=0.3, seed=7)),
+    "rand30": (random_sdp, dict(n=30, m=60, density=0.1, seed=1)),
+    "rand60": (random_sdp, dict(n=60, m=200, density=0.05, seed=2)),
+    "rand100": (random_sdp, dict(n=100, m=300, density=0.02, seed=3)),
+}
+BIG = {"rand400": (random_sdp, dict(n=400, m=2000, density=0.01, seed=0))}
+
+ROW = re.compile(r"^\s*(\d+)\s+([+-]\S+)\s+([+-]\S+)\s+(\S+)\s+(\S+)\s+(\S+)\s+(\S+)\s+(\S+)\s+(\S+)\s+(\S+)\s+(\S+)\s*$")
+
+
+def run(path, opts):
+    cmd = [REF, path] + opts + ["-v", "-threads", "8"]
+    env = dict(os.environ, BRISK_NOBUSY="1")
+    p = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=3600)
+    out = p.stdout + p.stderr
+    rows = []
+    for line in out.splitlines():
+        mm = ROW.match(line)
+        if mm:
+            it, po, do, pinf, dinf, gap, mu = mm.groups()[:7]
+            rows.append(dict(it=int(it), pobj=float(po), dobj=float(do), pinf=float(pinf), dinf=float(dinf),
+                             gap=float(gap), mu=float(mu)))
+    st = re.search(r"^status: (.+?)\s+iterations: (\d+)", out, re.M)
+    ob = re.search(r"primal obj <C,X> = (\S+)\s+dual obj b'y = (\S+)", out)
+    de = re.search(r"^\s*DIMACS errors: (\S+) (\S+) (\S+) (\S+) (\S+) (\S+)", out, re.M)
+    tt = re.search(r"^time: total (\S+)s \(read (\S+),", out, re.M)
+    return dict(cmd=" ".join(["brisk_ref", os.path.basename(path)] + opts), exit_code=p.returncode,
+                status=st.group(1).strip() if st else None, iterations=int(st.group(2)) if st else None,
+                pobj=float(ob.group(1)) if ob else None, dobj=float(ob.group(2)) if ob else None,
+                dimacs=[float(x) for x in de.groups()] if de else None,
+                time_total=float(tt.group(1)) if tt else None, time_read=float(tt.group(2)) if tt else None,
+                rows=rows)
+
+
+def main():
+    inst = dict(INSTANCES)
+    if "--big" in sys.argv:
+        inst.update(BIG)
+    res = {}
+    if os.path.exists(OUT):
+        with open(OUT) as f:
+            res = json.load(f)
+    with tempfile.TemporaryDirectory() as td:
+        for name, (fn, kw) in inst.items():
+            d = fn(**kw)
+            path = os.path.join(td, name + ".dat-s")
+            write_sdpa(d, path)
+            entry = dict(generator=fn.__name__, kwargs=kw, m=d.m, n=int(d.bs[0]), runs={})
+            base = ["-nohsd", "-dir", "hkm", "-mixed", "0", "-tol", "1e-7"] + AS_GIVEN
+            entry["runs"]["init0"] = run(path, base + ["-init", "0"])
+            entry["runs"]["default"] = run(path, base)
+            res[name] = entry
+            r = entry["runs"]["init0"]
+            print(name, d.m, r["status"], r["iterations"], r["pobj"], r["dobj"], flush=True)
+    with open(OUT, "w") as f:
+        json.dump(res, f, indent=1)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,64 @@
+"""The C-ABI library loads without a GPU and exports every function include/*.h declares."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    names = set()
+    for h in ("brisk.h", "bgpu.h"):
+        with open(os.path.join(ROOT, "include", h)) as f:
+            text = f.read()
+        names |= set(re.findall(r"(?:BRISK_API|BGPU_API)[^;(]*?\b((?:brisk|bgpu)_\w+)\s*\(", text))
+    return sorted(names)
+
+
+def test_headers_declare_the_reference_interface():
+    names = declared_symbols()
+    for must in ("brisk_solve_data", "brisk_solve_file", "brisk_result_new", "brisk_result_delete",
+                 "brisk_result_status", "brisk_result_dimacs", "brisk_result_y", "brisk_result_X",
+                 "brisk_result_Z", "brisk_set_output", "brisk_version", "brisk_interrupt",
+                 "bgpu_schur_assemble", "bgpu_potrf", "bgpu_trsv", "bgpu_dgemm", "bgpu_gemm_tf32x3"):
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol(libpath):
+    L = ctypes.CDLL(libpath, mode=os.RTLD_LOCAL)
+    missing = [n for n in declared_symbols() if not hasattr(L, n)]
+    assert not missing, missing
+
+
+def test_version_and_result_handle_without_gpu(libpath):
+    from brisk_b200 import _core
+    L = _core.load_library(libpath)
+    assert L.brisk_version().decode().startswith("1.7")
+    r = L.brisk_result_new()
+    assert L.brisk_result_status(r) == -1
+    assert L.brisk_result_status_str(r).decode() == "NOT SOLVED"
+    L.brisk_result_delete(r)
+
+
+def test_bad_input_is_rejected_before_any_gpu_work(libpath):
+    from brisk_b200 import _core
+    with pytest.raises(ValueError):
+        _core.solve_sdpa([3], [1.0], [1], [1], [1], [1], [np.nan], verbose=False)
+    with pytest.raises(ValueError):
+        _core.solve_sdpa([3], [1.0], [1, 1], [1], [1], [1], [1.0], verbose=False)
+    # a bad option returns exit code 1 without touching the device
+    res = _core.solve_sdpa([2], [1.0], [1], [1], [1], [1], [1.0], options=["-tol", "x"], verbose=False)
+    assert res.exit_code == 1
+    # LP blocks are outside this build: input error 2
+    res = _core.solve_sdpa([-2], [1.0], [1], [1], [1], [1], [1.0], verbose=False)
+    assert res.exit_code == 2
+
+
+def test_options_to_argv_matches_reference_forms():
+    from brisk_b200 import options_to_argv
+    assert options_to_argv({"tol": 1e-7, "nohsd": True, "dir": "hkm", "x": None}) == ["-tol", "1e-07", "-nohsd", "-dir", "hkm"]
+    assert options_to_argv("-tol 1e-7 -mixed 0") == ["-tol", "1e-7", "-mixed", "0"]
+    assert options_to_argv(["-q"]) == ["-q"]

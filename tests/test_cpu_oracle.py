@@ -1,0 +1,102 @@
+"""The oracle (oracle/restate.py) against the reference's own runs (tests/golden/ref_runs.json)
+and the reference's published golden value, plus the host-side problem plumbing."""
+import os
+
+import numpy as np
+import pytest
+
+from brisk_b200 import problems
+from oracle import restate
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+SMALL = ["theta30", "rand30", "rand60"]
+
+
+def make(entry):
+    fn = getattr(problems, entry["generator"])
+    return fn(**entry["kwargs"])
+
+
+@pytest.mark.parametrize("name", ["theta30", "theta50", "rand30", "rand60", "rand100"])
+def test_oracle_scaling_and_start_match_reference_iteration0(golden, name):
+    """Scaling (problem_prepare) and the SDPT3 start pinned: the reference's iteration-0 row
+    (printed to 9 significant digits in pobj/dobj, 3 in the rest) is reproduced."""
+    if name not in golden:
+        pytest.skip("instance not in the fixtures")
+    e = golden[name]
+    d = make(e)
+    S = restate.scale_problem(d)
+    X, Z, y, xi, eta = restate.start_point(S)
+    sc = S.bs * S.cs
+    n = X[0].shape[0]
+    pobj = sc * sum(float(np.sum(C * Xk)) for C, Xk in zip(S.C, X))
+    mu = sc * sum(float(np.sum(Xk * Zk)) for Xk, Zk in zip(X, Z)) / n
+    rp = S.b - restate.aop(S.A, X)
+    pinf = np.linalg.norm(rp * S.du) / (1 + S.normb2)
+    row = e["runs"]["init0"]["rows"][0]
+    assert -pobj == pytest.approx(row["pobj"], rel=1e-8, abs=1e-8)
+    assert mu == pytest.approx(row["mu"], rel=6e-3)
+    assert pinf == pytest.approx(row["pinf"], rel=6e-3, abs=1e-15)
+
+
+def test_oracle_first_schur_is_gram_at_the_start(golden):
+    """M0 = (xi/eta) <A_i, A_j> on the scaled data (X0 = xi I, Z0 = eta I)."""
+    d = make(golden["rand30"])
+    S = restate.scale_problem(d)
+    X, Z, y, xi, eta = restate.start_point(S)
+    M0 = restate.schur(S.A, X, [np.linalg.inv(Zk) for Zk in Z])
+    G = np.einsum("ipq,jpq->ij", S.A[0], S.A[0])
+    np.testing.assert_allclose(M0, xi[0] / eta[0] * G, rtol=1e-12, atol=1e-14)
+
+
+@pytest.mark.parametrize("name", SMALL)
+def test_oracle_solve_matches_reference(golden, name):
+    """Same status, objectives within 1e-7 relative, DIMACS errors <= 1e-7 (the reference's
+    -init 0 run: the oracle restates the SDPT3 start).  "Relative" uses the DIMACS gap's
+    denominator 1 + |<C,X>| + |b'y|: each solve is only that accurate."""
+    e = golden[name]
+    ref = e["runs"]["init0"]
+    out = restate.solve(make(e), tol=1e-7)
+    assert out["status_str"] == ref["status"] == "OPTIMAL"
+    den = 1 + abs(ref["pobj"]) + abs(ref["dobj"])
+    assert abs(out["pobj"] - ref["pobj"]) <= 1e-7 * den
+    assert abs(out["dobj"] - ref["dobj"]) <= 1e-7 * den
+    assert np.max(np.abs(out["dimacs"])) <= 1e-7
+    assert max(abs(x) for x in ref["dimacs"]) <= 1e-7
+
+
+@pytest.mark.skipif(not os.path.exists("/root/reference/examples/theta1.dat-s"), reason="reference tree absent")
+def test_oracle_theta1_published_value():
+    """theta1 -> 2.2999999997e+01 (the reference's INSTALL.md:44-45)."""
+    d = problems.read_sdpa("/root/reference/examples/theta1.dat-s")
+    out = restate.solve(d, tol=1e-8)
+    assert out["status_str"] == "OPTIMAL"
+    assert -out["pobj"] == pytest.approx(23.0, rel=1e-7)
+
+
+def test_sdpa_roundtrip(tmp_path):
+    d = problems.random_sdp(n=12, m=20, density=0.2, seed=5)
+    p = tmp_path / "x.dat-s"
+    problems.write_sdpa(d, str(p))
+    e = problems.read_sdpa(str(p))
+    assert e.m == d.m and list(e.bs) == list(d.bs)
+    np.testing.assert_array_equal(e.c, d.c)
+    np.testing.assert_array_equal(e.v, d.v)
+    np.testing.assert_array_equal(e.i, d.i)
+    np.testing.assert_array_equal(e.mat, d.mat)
+
+
+def test_generators_match_workload_shapes():
+    d = problems.theta_problem(n=50, p=0.5, seed=1)
+    assert d.m == 588 and int(d.bs[0]) == 50
+    d = problems.random_sdp(n=40, m=30, density=0.01 * 20, seed=0)
+    k = int(round(0.2 * 40 * 41 / 2))
+    assert d.meta["upper_per_con"] == k
+    # b_i = <A_i, I>
+    C, A = d.dense_blocks()
+    np.testing.assert_allclose(np.trace(A[0], axis1=1, axis2=2), d.c, rtol=1e-12, atol=1e-12)
+    # C = G G'/n + I is positive definite
+    assert np.linalg.eigvalsh(C[0]).min() > 0.99
+    sizes = problems.random_dense_batch(count=64, seed=0, sizes_only=True)
+    for n, m in sizes:
+        assert 8 <= n <= 64 and n <= m <= n * (n + 1) // 4

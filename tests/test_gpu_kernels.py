@@ -1,0 +1,222 @@
+"""Kernel parity through the C ABI (include/bgpu.h) on a B200: each kernel against the oracle
+(oracle/restate.py) or a plain FP64 reference of the same operation.  Device memory comes from
+torch (allocation only); every compute call goes through libbrisk.so."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+from brisk_b200 import problems, step  # noqa: E402
+from oracle import restate  # noqa: E402
+
+
+def dev(a, cuda, dtype=None):
+    t = torch.as_tensor(np.ascontiguousarray(a))
+    if dtype is not None:
+        t = t.to(dtype)
+    return t.to(cuda).contiguous()
+
+
+def colmajor(A, cuda):
+    """A column-major copy (the transpose's row-major buffer)."""
+    return dev(np.asarray(A).T, cuda)
+
+
+def from_colmajor(t, n, m=None):
+    m = n if m is None else m
+    return t.cpu().numpy().reshape(m, n).T
+
+
+@pytest.mark.parametrize("akm,bkm", [(0, 0), (0, 1), (1, 0), (1, 1)])
+@pytest.mark.parametrize("M,N,K", [(1, 1, 1), (130, 70, 33), (257, 200, 64), (64, 513, 129)])
+def test_dgemm_layouts(cuda, akm, bkm, M, N, K):
+    rng = np.random.default_rng(M * 7 + N + K)
+    A = rng.standard_normal((M, K))
+    B = rng.standard_normal((K, N))
+    C0 = rng.standard_normal((M, N))
+    # device buffers in the requested layouts
+    dA = dev(A if akm else A.T, cuda)            # KMAJOR: A[i*lda+k] (row-major); MMAJOR: column-major
+    dB = dev(B.T if bkm else B, cuda)            # KMAJOR: B[k+j*ldb] (column-major); NMAJOR: row-major
+    dC = colmajor(C0, cuda)
+    lda = K if akm else M
+    ldb = K if bkm else N
+    step.call("dgemm", akm, bkm, M, N, K, 1.5, dA.data_ptr(), lda, dB.data_ptr(), ldb, -0.5, dC.data_ptr(), M, 0, None)
+    step.call("sync", None)
+    got = from_colmajor(dC, M, N) if False else dC.cpu().numpy().reshape(N, M).T
+    want = 1.5 * A @ B - 0.5 * C0
+    np.testing.assert_allclose(got, want, rtol=1e-12, atol=1e-12 * np.abs(want).max())
+
+
+def test_dgemm_lower_only(cuda):
+    rng = np.random.default_rng(1)
+    n, K = 150, 40
+    A = rng.standard_normal((n, K))
+    C0 = rng.standard_normal((n, n))
+    dA = dev(A.T, cuda)                          # column-major n x K (MMAJOR), also N-major for B
+    dC = colmajor(C0, cuda)
+    step.call("dgemm", 0, 0, n, n, K, -1.0, dA.data_ptr(), n, dA.data_ptr(), n, 1.0, dC.data_ptr(), n, 1, None)
+    step.call("sync", None)
+    got = dC.cpu().numpy().reshape(n, n).T
+    want = C0 - A @ A.T
+    low = np.tril_indices(n)
+    np.testing.assert_allclose(got[low], want[low], rtol=1e-12, atol=1e-11)
+    up = np.triu_indices(n, 1)
+    np.testing.assert_array_equal(got[up], C0[up])
+
+
+def spd(n, seed, cond=1e3):
+    rng = np.random.default_rng(seed)
+    Q, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    ev = np.logspace(0, np.log10(cond), n)
+    return (Q * ev) @ Q.T
+
+
+@pytest.mark.parametrize("n", [1, 63, 64, 65, 200, 700])
+def test_potrf_trsv_trtri(cuda, n):
+    A = spd(n, n)
+    L_ref = np.linalg.cholesky(A)
+    dA = colmajor(A, cuda)
+    nb = (n + 63) // 64
+    dinv = torch.zeros(nb * 4096, dtype=torch.float64, device=cuda)
+    info = torch.zeros(1, dtype=torch.int32, device=cuda)
+    pmin = torch.zeros(1, dtype=torch.float64, device=cuda)
+    step.call("potrf", n, dA.data_ptr(), n, dinv.data_ptr(), info.data_ptr(), pmin.data_ptr(), None)
+    step.call("sync", None)
+    assert int(info.item()) == 0
+    L = np.tril(dA.cpu().numpy().reshape(n, n).T)
+    np.testing.assert_allclose(L, L_ref, rtol=1e-10, atol=1e-12 * np.abs(L_ref).max())
+    assert pmin.item() == pytest.approx(np.min(np.diag(L_ref)) ** 2, rel=1e-10)
+    # triangular solves
+    rng = np.random.default_rng(n + 1)
+    b = rng.standard_normal(n)
+    flags = torch.zeros(nb, dtype=torch.int32, device=cuda)
+    err = torch.zeros(1, dtype=torch.int32, device=cuda)
+    x = dev(b, cuda)
+    step.call("trsv", n, dA.data_ptr(), n, dinv.data_ptr(), x.data_ptr(), 0, flags.data_ptr(), 1, err.data_ptr(), None)
+    step.call("trsv", n, dA.data_ptr(), n, dinv.data_ptr(), x.data_ptr(), 1, flags.data_ptr(), 2, err.data_ptr(), None)
+    step.call("sync", None)
+    assert int(err.item()) == 0
+    np.testing.assert_allclose(x.cpu().numpy(), np.linalg.solve(A, b), rtol=1e-8, atol=1e-10)
+    # inverse of the factor
+    Li = torch.zeros(n * n, dtype=torch.float64, device=cuda)
+    step.call("trtri", n, dA.data_ptr(), n, dinv.data_ptr(), Li.data_ptr(), n, None)
+    step.call("sync", None)
+    got = Li.cpu().numpy().reshape(n, n).T
+    np.testing.assert_allclose(got @ L_ref, np.eye(n), atol=1e-9)
+
+
+def test_potrf_reports_first_nonpositive_pivot(cuda):
+    n = 130
+    A = spd(n, 3)
+    A[100, 100] = -1.0           # leading minors up to 100 stay definite
+    dA = colmajor(A, cuda)
+    dinv = torch.zeros(3 * 4096, dtype=torch.float64, device=cuda)
+    info = torch.zeros(1, dtype=torch.int32, device=cuda)
+    pmin = torch.zeros(1, dtype=torch.float64, device=cuda)
+    step.call("potrf", n, dA.data_ptr(), n, dinv.data_ptr(), info.data_ptr(), pmin.data_ptr(), None)
+    step.call("sync", None)
+    want = next(k + 1 for k in range(n) if np.linalg.eigvalsh(A[:k + 1, :k + 1])[0] <= 0)
+    assert int(info.item()) == want
+
+
+@pytest.mark.parametrize("n", [64, 300])
+def test_potrf_f32_and_trsv_f32(cuda, n):
+    A = spd(n, 11, cond=50)
+    dA = colmajor(A, cuda).float()
+    nb = (n + 63) // 64
+    dinv = torch.zeros(nb * 4096, dtype=torch.float32, device=cuda)
+    info = torch.zeros(1, dtype=torch.int32, device=cuda)
+    pmin = torch.zeros(1, dtype=torch.float64, device=cuda)
+    step.call("potrf_f32", n, dA.data_ptr(), n, dinv.data_ptr(), info.data_ptr(), pmin.data_ptr(), None)
+    b = np.random.default_rng(2).standard_normal(n)
+    x = dev(b, cuda).float()
+    flags = torch.zeros(nb, dtype=torch.int32, device=cuda)
+    err = torch.zeros(1, dtype=torch.int32, device=cuda)
+    step.call("trsv_f32", n, dA.data_ptr(), n, dinv.data_ptr(), x.data_ptr(), 0, flags.data_ptr(), 5, err.data_ptr(), None)
+    step.call("trsv_f32", n, dA.data_ptr(), n, dinv.data_ptr(), x.data_ptr(), 1, flags.data_ptr(), 6, err.data_ptr(), None)
+    step.call("sync", None)
+    assert int(info.item()) == 0 and int(err.item()) == 0
+    np.testing.assert_allclose(x.cpu().numpy(), np.linalg.solve(A, b), rtol=1e-4, atol=1e-4)
+
+
+def block_arrays(d, cuda):
+    """Constraint-major device arrays of block 1 of an SdpaData, as the solver lays them out:
+    scaled entries (problem_prepare), full expansion sorted by position p + q n."""
+    S = restate.scale_problem(d)
+    n = int(d.bs[0])
+    A = S.A[0]
+    con, cptr, cpos, cval = [], [0], [], []
+    for t in range(d.m):
+        iq = np.nonzero(A[t].T.ravel())[0]          # column-major positions
+        if iq.size == 0:
+            continue
+        con.append(t)
+        cpos.extend(iq.tolist())
+        cval.extend(A[t].T.ravel()[iq].tolist())
+        cptr.append(len(cpos))
+    arrs = dict(con=torch.tensor(con, dtype=torch.int32, device=cuda),
+                cptr=torch.tensor(cptr, dtype=torch.int64, device=cuda),
+                cpos=torch.tensor(cpos, dtype=torch.int32, device=cuda),
+                cval=torch.tensor(cval, dtype=torch.float64, device=cuda))
+    return S, n, arrs
+
+
+@pytest.mark.parametrize("name,kw,chunk", [
+    ("rand30", dict(n=30, m=60, density=0.1, seed=1), 8),
+    ("rand60", dict(n=60, m=200, density=0.05, seed=2), 32),
+    ("rand100", dict(n=100, m=300, density=0.02, seed=3), 64),
+    ("theta50", None, 16),
+])
+def test_schur_fp64_matches_oracle(cuda, name, kw, chunk):
+    d = problems.theta_problem() if kw is None else problems.random_sdp(**kw)
+    S, n, a = block_arrays(d, cuda)
+    rng = np.random.default_rng(4)
+    X = spd(n, 5, cond=100)
+    Zi = spd(n, 6, cond=100)
+    want = restate.schur(S.A, [X], [Zi])
+    M = torch.zeros(d.m * d.m, dtype=torch.float64, device=cuda)
+    ws = torch.empty(step.ws_bytes(n, chunk, 0), dtype=torch.uint8, device=cuda)
+    dX, dZi = colmajor(X, cuda), colmajor(Zi, cuda)
+    step.call("schur_assemble", n, d.m, int(a["con"].numel()), a["con"].data_ptr(), a["cptr"].data_ptr(),
+              a["cpos"].data_ptr(), a["cval"].data_ptr(), dX.data_ptr(), dZi.data_ptr(), M.data_ptr(), 0, chunk,
+              ws.data_ptr(), ws.numel(), None)
+    step.call("sync", None)
+    got = M.cpu().numpy().reshape(d.m, d.m).T
+    np.testing.assert_allclose(got, want, rtol=1e-10, atol=1e-12 * np.abs(want).max())
+
+
+def test_first_schur_matches_oracle_at_start(cuda, golden):
+    """M at the first iteration (the SDPT3 start on the scaled problem), FP64: 1e-10 relative."""
+    d = problems.random_sdp(**golden["rand60"]["kwargs"])
+    S, n, a = block_arrays(d, cuda)
+    X, Z, y, xi, eta = restate.start_point(S)
+    Zi = np.linalg.inv(Z[0])
+    want = restate.schur(S.A, X, [Zi])
+    M = torch.zeros(d.m * d.m, dtype=torch.float64, device=cuda)
+    ws = torch.empty(step.ws_bytes(n, 0, 0), dtype=torch.uint8, device=cuda)
+    step.call("schur_assemble", n, d.m, int(a["con"].numel()), a["con"].data_ptr(), a["cptr"].data_ptr(),
+              a["cpos"].data_ptr(), a["cval"].data_ptr(), colmajor(X[0], cuda).data_ptr(),
+              colmajor(Zi, cuda).data_ptr(), M.data_ptr(), 0, 0, ws.data_ptr(), ws.numel(), None)
+    step.call("sync", None)
+    got = M.cpu().numpy().reshape(d.m, d.m).T
+    rel = np.abs(got - want).max() / np.abs(want).max()
+    assert rel <= 1e-10
+
+
+def test_aop_and_symv(cuda):
+    d = problems.random_sdp(n=40, m=50, density=0.1, seed=9)
+    S, n, a = block_arrays(d, cuda)
+    D = spd(n, 7)
+    out = torch.zeros(d.m, dtype=torch.float64, device=cuda)
+    step.call("aop", n, int(a["con"].numel()), a["con"].data_ptr(), a["cptr"].data_ptr(), a["cpos"].data_ptr(),
+              a["cval"].data_ptr(), colmajor(D, cuda).data_ptr(), 1.0, 0.0, out.data_ptr(), None)
+    step.call("sync", None)
+    np.testing.assert_allclose(out.cpu().numpy(), restate.aop(S.A, [D]), rtol=1e-12, atol=1e-12)
+    M = spd(300, 8)
+    x = np.random.default_rng(3).standard_normal(300)
+    y = torch.zeros(300, dtype=torch.float64, device=cuda)
+    step.call("symv", 300, 2.0, colmajor(M, cuda).data_ptr(), 300, dev(x, cuda).data_ptr(), 0.0, y.data_ptr(), None)
+    step.call("sync", None)
+    np.testing.assert_allclose(y.cpu().numpy(), 2.0 * M @ x, rtol=1e-12, atol=1e-10)

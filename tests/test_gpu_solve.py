@@ -1,0 +1,74 @@
+"""End-to-end parity on a B200 through the reference-compatible C interface: the reference's
+own CPU solve (tests/golden/ref_runs.json, made from oracle/_ref) and this library must give
+the same status, objectives within 1e-7 relative and DIMACS errors of at most 1e-7."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+import brisk_b200  # noqa: E402
+from brisk_b200 import problems  # noqa: E402
+
+FP64 = ["-nohsd", "-dir", "hkm", "-mixed", "0", "-tol", "1e-7"]
+
+
+def make(entry):
+    return getattr(problems, entry["generator"])(**entry["kwargs"])
+
+
+def check(res, ref):
+    """Same status; objectives within 1e-7 relative to the DIMACS denominator
+    1 + |<C,X>| + |b'y| (the accuracy either solve has at DIMACS error 1e-7); DIMACS <= 1e-7."""
+    assert res.status_str == ref["status"], res.log
+    den = 1 + abs(ref["pobj"]) + abs(ref["dobj"])
+    assert abs(res.pobj - ref["pobj"]) <= 1e-7 * den, (res.pobj, ref["pobj"])
+    assert abs(res.dobj - ref["dobj"]) <= 1e-7 * den, (res.dobj, ref["dobj"])
+    assert np.max(np.abs(res.dimacs)) <= 1e-7, res.dimacs
+
+
+@pytest.mark.parametrize("name", ["theta30", "theta50", "rand30", "rand60", "rand100"])
+def test_solve_matches_reference_init0(golden, name):
+    e = golden[name]
+    res = brisk_b200.solve_sdpa(*make(e).args(), options=FP64 + ["-init", "0"], verbose=False)
+    check(res, e["runs"]["init0"])
+    # the iteration-0 row (same scaling and start): pobj/dobj printed to 9 digits
+    row0 = e["runs"]["init0"]["rows"][0]
+    line = [ln for ln in res.log.splitlines() if ln.strip().startswith("0 ")][0].split()
+    assert float(line[1]) == pytest.approx(row0["pobj"], rel=1e-8, abs=1e-8)
+    assert float(line[2]) == pytest.approx(row0["dobj"], rel=1e-8, abs=1e-8)
+
+
+@pytest.mark.parametrize("name", ["theta50", "rand60", "rand100"])
+def test_solve_matches_reference_default_start(golden, name):
+    e = golden[name]
+    res = brisk_b200.solve_sdpa(*make(e).args(), options=FP64, verbose=False)
+    check(res, e["runs"]["default"])
+
+
+def test_solve_full_size_fp64(golden):
+    """The n = 400, m = 2000 workload, FP64 on the GPU, against the reference's solve."""
+    e = golden["rand400"]
+    res = brisk_b200.solve_sdpa(*make(e).args(), options=FP64, verbose=False)
+    check(res, e["runs"]["default"])
+
+
+def test_solve_file_equals_solve_data(tmp_path, golden):
+    """brisk_solve_file on the SDPA file and brisk_solve_data on the same numbers give the same
+    result bits (the reference's tools/capi_test.c:134-140 check)."""
+    d = make(golden["rand30"])
+    p = tmp_path / "p.dat-s"
+    problems.write_sdpa(d, str(p))
+    r1 = brisk_b200.solve_file(str(p), options=FP64, verbose=False)
+    r2 = brisk_b200.solve_sdpa(*d.args(), options=FP64, verbose=False)
+    assert r1.status == r2.status and r1.iterations == r2.iterations
+    assert r1.pobj == r2.pobj and r1.dobj == r2.dobj
+    np.testing.assert_array_equal(r1.y, r2.y)
+    np.testing.assert_array_equal(r1.X[0], r2.X[0])
+
+
+def test_repeated_solves_are_bitwise_identical(golden):
+    d = make(golden["rand60"])
+    a = brisk_b200.solve_sdpa(*d.args(), options=FP64, verbose=False)
+    b = brisk_b200.solve_sdpa(*d.args(), options=FP64, verbose=False)
+    assert a.pobj == b.pobj and a.iterations == b.iterations
+    np.testing.assert_array_equal(a.y, b.y)
