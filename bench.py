@@ -168,12 +168,12 @@ def cpu_reference_sample(d, workload, threads, opts_extra):
     with tempfile.TemporaryDirectory() as td:
         path = os.path.join(td, workload + ".dat-s")
         write_sdpa(d, path)
-        cmd = [ref, path, "-nohsd", "-dir", "hkm", "-tol", "1e-7", "-threads", str(threads)] + opts_extra
+        cmd = [ref, path, "-nohsd", "-dir", "hkm", "-tol", "1e-7", "-v", "-threads", str(threads)] + opts_extra
         env = dict(os.environ, BRISK_NOBUSY="1")
         t0 = time.time()
         p = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=3600)
         wall = time.time() - t0
-    out = p.stdout + p.stderr
+    out = p.stdout + p.stderr + f" [exit {p.returncode}]"
     tt = re.search(r"time: total (\S+)s \(read (\S+),", out)
     st = re.search(r"^status: (.+?)\s+iterations: (\d+)", out, re.M)
     if not tt:
@@ -322,6 +322,8 @@ def run_ours(args):
             if r and "error" not in r:
                 cpu = {"value": r["time"], "unit": "s", "cores": threads, "kind": "reference",
                        "sample": f"one full reference solve to 1e-7 ({r['status']}, {r['iterations']} iterations)"}
+            else:
+                cpu = {"value": None, "error": (r or {}).get("error", "oracle/_ref/brisk_ref absent")[-300:]}
     if world > 1:
         torch.distributed.barrier()
     if rank == 0:

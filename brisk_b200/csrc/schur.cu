@@ -21,7 +21,7 @@ namespace {
 constexpr int TP_Q = 32, TP_K = 128, TP_LD = TP_K + 1;
 
 template <typename OutT>
-__global__ void __launch_bounds__(256) tprod_kernel(int n, int K, int a0, int ncon, const long long *__restrict__ cptr,
+__global__ void __launch_bounds__(256) tprod_kernel(int n, int ldt, int K, int a0, int ncon, const long long *__restrict__ cptr,
                                                    const int *__restrict__ cpos, const double *__restrict__ cval,
                                                    const double *__restrict__ Zi, OutT *__restrict__ T,
                                                    OutT *__restrict__ Tlo) {
@@ -62,7 +62,7 @@ __global__ void __launch_bounds__(256) tprod_kernel(int n, int K, int a0, int nc
         const int r = idx / TP_K, kk = idx % TP_K;
         if (q0 + r < n && kk < kw) {
             const double v = tile[r * TP_LD + kk];
-            const long long o = ((long long)(q0 + r) * K + t) * n + k0 + kk;
+            const long long o = ((long long)(q0 + r) * K + t) * ldt + k0 + kk;
             if (sizeof(OutT) == 8) {
                 T[o] = (OutT)v;
             } else {
@@ -142,6 +142,16 @@ int gather_launch(cudaStream_t st, int K, int a0, int ncon, int m, const DevBloc
     return BGPU_OK;
 }
 
+// hi/lo tf32 parts of a column-major n x n double matrix into rows of stride ld (ld >= n)
+__global__ void split2d_kernel(int n, const double *__restrict__ X, int ld, float *__restrict__ hi, float *__restrict__ lo) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+    if (i >= ld) return;
+    const double v = i < n ? X[i + (long long)j * n] : 0.0;
+    const float h = tf32_round((float)v);
+    hi[i + (long long)j * ld] = h;
+    lo[i + (long long)j * ld] = tf32_round((float)(v - (double)h));
+}
+
 __global__ void aop_kernel(int ncon, const int *__restrict__ con, const long long *__restrict__ cptr,
                            const int *__restrict__ cpos, const double *__restrict__ cval, const double *__restrict__ D,
                            double alpha, double beta, double *out) {
@@ -190,10 +200,15 @@ int schur_chunk_default(int n, int precision) {
     return K;
 }
 
+// tf32 operand rows padded to a multiple of 4 floats: the tensor maps need 16-byte strides
+static inline int tf32_ld(int n) { return (n + 3) / 4 * 4; }
+
 size_t schur_ws_bytes(int n, int chunk, int precision) {
     const size_t nn = (size_t)n * n * chunk;
     if (precision == 0) return 2 * nn * sizeof(double);            // T, G
-    return 4 * nn * sizeof(float) + 2 * (size_t)n * n * sizeof(float);   // T hi/lo, G (float), X hi/lo
+    const size_t ld = tf32_ld(n);
+    // T hi/lo (n K rows of ld), G (float, n K x n), X hi/lo (n rows of ld), plus 256 B alignment slack each
+    return (2 * (size_t)n * chunk * ld + nn + 2 * (size_t)n * ld) * sizeof(float) + 5 * 256;
 }
 
 int schur_assemble(cudaStream_t st, const DevBlock &B, const double *X, const double *Zi, double *M, int m,
@@ -207,7 +222,7 @@ int schur_assemble(cudaStream_t st, const DevBlock &B, const double *X, const do
     if (precision == 0) {
         double *T = (double *)ws, *G = T + nnK;
         for (int a0 = 0; a0 < B.ncon; a0 += K) {
-            tprod_kernel<double><<<tgrid, 256, 0, st>>>(n, K, a0, B.ncon, B.cptr, B.cpos, B.cval, Zi, T, nullptr);
+            tprod_kernel<double><<<tgrid, 256, 0, st>>>(n, n, K, a0, B.ncon, B.cptr, B.cpos, B.cval, Zi, T, nullptr);
             BGPU_LAUNCH_CHECK();
             int rc = gemm_f64(st, 1, 1, n * K, n, n, 1.0, T, n, 0, X, n, 0, 0.0, G, (long long)n * K, 0, 1, 0);
             if (rc) return rc;
@@ -217,13 +232,22 @@ int schur_assemble(cudaStream_t st, const DevBlock &B, const double *X, const do
         return BGPU_OK;
     }
     // 3xTF32: T and X split into tf32 hi + lo parts; G accumulated in FP32 on the tensor cores
-    float *Th = (float *)ws, *Tl = Th + nnK, *G = Tl + nnK, *Xh = G + nnK, *Xl = Xh + (size_t)n * n;
-    int rc = split_tf32(st, (long long)n * n, X, Xh, Xl);
-    if (rc) return rc;
+    const int ld = tf32_ld(n);
+    auto carve = [&](size_t count) {   // 256-byte aligned sub-buffers of the workspace
+        static_assert(sizeof(float) == 4, "");
+        uintptr_t p = ((uintptr_t)ws + 255) & ~(uintptr_t)255;
+        float *r = (float *)p;
+        ws = (void *)(p + count * sizeof(float));
+        return r;
+    };
+    float *Th = carve((size_t)n * K * ld), *Tl = carve((size_t)n * K * ld), *G = carve(nnK);
+    float *Xh = carve((size_t)n * ld), *Xl = carve((size_t)n * ld);
+    split2d_kernel<<<dim3(ceil_div(ld, 256), n), 256, 0, st>>>(n, X, ld, Xh, Xl);
+    BGPU_LAUNCH_CHECK();
     for (int a0 = 0; a0 < B.ncon; a0 += K) {
-        tprod_kernel<float><<<tgrid, 256, 0, st>>>(n, K, a0, B.ncon, B.cptr, B.cpos, B.cval, Zi, Th, Tl);
+        tprod_kernel<float><<<tgrid, 256, 0, st>>>(n, ld, K, a0, B.ncon, B.cptr, B.cpos, B.cval, Zi, Th, Tl);
         BGPU_LAUNCH_CHECK();
-        rc = gemm_tf32x3(st, n * K, n, n, Th, Tl, n, Xh, Xl, n, G, (long long)n * K);
+        int rc = gemm_tf32x3(st, n * K, n, n, Th, Tl, ld, Xh, Xl, ld, G, (long long)n * K);
         if (rc) return rc;
         rc = gather_launch<float>(st, K, a0, B.ncon, m, B, G, M);
         if (rc) return rc;

@@ -354,7 +354,8 @@ class Solver {
     double *h_dots = nullptr;                     // pinned
     void *ws = nullptr;
     size_t ws_bytes = 0;
-    int chunk = 32, asm_prec = 0;
+    int chunk = 32, chunk64 = 32, asm_prec = 0;
+    int chunk_fp64(int) const { return chunk64; }
     int epoch = 0;
     // factor state (Schur in solver.c:4511-4568)
     bool allow_float = false, want_double = false, is_float = false, reg_hint = false;
@@ -390,6 +391,7 @@ class Solver {
     double maxstep(int primal, int K);
     double lanczos(int n, const double *Bm, int K);
     int try_step(int primal, double *alpha);
+    void least_squares_start(std::vector<double> &y);
     // final measures
     void final_measures(const std::vector<double> &y, ResultData &res);
 };
@@ -508,7 +510,8 @@ void Solver::setup() {
         if (!Mf || !dinvMf) throw GpuFail{BGPU_ERR_NOMEM, __LINE__};
     }
     chunk = opt.chunk > 0 ? opt.chunk : schur_chunk_default(nmax, asm_prec);
-    ws_bytes = schur_ws_bytes(nmax, chunk, asm_prec);
+    chunk64 = opt.chunk > 0 ? opt.chunk : schur_chunk_default(nmax, 0);
+    ws_bytes = std::max(schur_ws_bytes(nmax, chunk, asm_prec), schur_ws_bytes(nmax, chunk64, 0));
     ws = g.alloc<unsigned char>(ws_bytes);
     if (!ws) throw GpuFail{BGPU_ERR_NOMEM, __LINE__};
 }
@@ -811,6 +814,70 @@ int Solver::try_step(int primal, double *alpha) {
     return 0;
 }
 
+// The least-squares start (the default init = 1, solver.c:13939-14198), in its factored form:
+// dy = (A A')^-1 b and y = (A A')^-1 A(C) with A A' the Schur complement at X = Zi = I, then
+// X0 = A'dy and Z0 = C - A'y shifted into the cone by their smallest eigenvalues (X: 1 + |lmin|
+// when not positive definite; Z: max(0, 1 - lmin)) and raised until a Cholesky test passes.
+void Solver::least_squares_start(std::vector<double> &y) {
+    const bool af = allow_float;
+    allow_float = false;   // the start's Gram solves in FP64
+    CU(cudaMemsetAsync(M, 0, sizeof(double) * (size_t)m * m, g.st));
+    for (int k = 0; k < nb; k++) {
+        RC(ew_set_scaled_identity(g.st, db[k].n, da[k].T, 1.0));
+        RC(schur_assemble(g.st, db[k], da[k].T, da[k].T, M, m, 0, chunk_fp64(k), ws, ws_bytes));
+    }
+    const int frc = factor();
+    allow_float = af;
+    if (frc != 0) return;   // keep the SDPT3 start (the reference's init_ok = 0 path)
+    std::vector<double> dy, AC;
+    schur_solve(P.b, dy, 1e-8);
+    std::vector<double *> Cs(nb);
+    for (int k = 0; k < nb; k++) Cs[k] = db[k].C;
+    aop_all(Cs, AC);
+    schur_solve(AC, y, 1e-8);
+    double ax = -1e300, az = -1e300;
+    for (int k = 0; k < nb; k++) {
+        const int n = db[k].n;
+        const long long nn = (long long)n * n;
+        DevArrays &d = da[k];
+        atop_block(k, dy, 1.0, 0.0, d.X);                                          // X = A'dy
+        atop_block(k, y, -1.0, 0.0, d.Z);
+        RC(ew_lincomb(g.st, nn, 1.0, d.Z, 1.0, db[k].C, 0.0, nullptr, d.Z));      // Z = C - A'y
+        RC(ew_lincomb(g.st, nn, 1.0, d.X, 0.0, nullptr, 0.0, nullptr, d.Bm));
+        const double lx = lanczos(n, d.Bm, opt.lanczos_k);
+        RC(ew_lincomb(g.st, nn, 1.0, d.Z, 0.0, nullptr, 0.0, nullptr, d.Bm));
+        const double lz = lanczos(n, d.Bm, opt.lanczos_k);
+        ax = std::max(ax, -lx);
+        az = std::max(az, -lz);
+    }
+    const double shx = ax >= -1e-8 ? 1.0 + ax : 0.0;
+    const double shz = std::max(0.0, 1.0 + az);
+    for (int k = 0; k < nb; k++) {
+        const int n = db[k].n;
+        const long long nn = (long long)n * n;
+        DevArrays &d = da[k];
+        RC(ew_add_diag(g.st, n, d.X, n, shx));
+        RC(ew_add_diag(g.st, n, d.Z, n, shz));
+        for (double extra = 1e-8;; extra *= 10) {
+            RC(ew_lincomb(g.st, nn, 1.0, d.X, 0.0, nullptr, 0.0, nullptr, d.LX));
+            if (chol(n, d.LX, d.dinvX) == 0) break;
+            RC(ew_add_diag(g.st, n, d.X, n, extra));
+            if (extra > 1e30) throw GpuFail{BGPU_ERR_NOTPD, __LINE__};
+        }
+        for (double extra = 1e-8;; extra *= 10) {
+            RC(ew_lincomb(g.st, nn, 1.0, d.Z, 0.0, nullptr, 0.0, nullptr, d.LZ));
+            if (chol(n, d.LZ, d.dinvZ) == 0) break;
+            RC(ew_add_diag(g.st, n, d.Z, n, extra));
+            if (extra > 1e30) throw GpuFail{BGPU_ERR_NOTPD, __LINE__};
+        }
+        inv_from_chol(n, d.LX, d.dinvX, d.LiX);
+    }
+    // the factor state starts afresh for the loop
+    want_double = is_float = reg_hint = false;
+    reg = reg_ok = 0;
+    nfactor = nfloat = 0;
+}
+
 // ---- the DIMACS errors of the returned point on the data as given ----------------------------
 void Solver::final_measures(const std::vector<double> &y, ResultData &res) {
     // X_o = bs X, y_o = cs d y, Z_o = C - A'(y_o) = cs (C' - A'(y))   (scaled data on the device)
@@ -928,11 +995,13 @@ int Solver::run(ResultData &res) {
         if (chol(n, d.T, d.dinvZ)) throw GpuFail{BGPU_ERR_NOTPD, __LINE__};
         inv_from_chol(n, d.LX, d.dinvX, d.LiX);
     }
-    // R0 = C - Z - A'y (y = 0), theta = 1
+    if (opt.init >= 1 && m > 0) least_squares_start(y);
+    // R0 = C - Z - A'y, theta = 1 (solver.c:14317-14326)
     double theta = 1.0, r0norm = 0;
     for (int k = 0; k < nb; k++) {
         const long long nn = (long long)db[k].n * db[k].n;
-        RC(ew_lincomb(g.st, nn, 1.0, db[k].C, -1.0, da[k].Z, 0.0, nullptr, da[k].R0));
+        atop_block(k, y, -1.0, 0.0, da[k].R0);
+        RC(ew_lincomb(g.st, nn, 1.0, db[k].C, -1.0, da[k].Z, 1.0, da[k].R0, da[k].R0));
         double t;
         const double *aa[1] = {da[k].R0};
         dots(1, aa, aa, nn, &t);

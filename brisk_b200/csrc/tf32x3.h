@@ -18,3 +18,6 @@ int split_tf32(cudaStream_t st, long long n, const double *x, float *hi, float *
 // accumulation; G column-major (G[i + j*ldg]).
 int gemm_tf32x3(cudaStream_t st, int M, int N, int K, const float *Ah, const float *Al, long long lda,
                 const float *Bh, const float *Bl, long long ldb, float *G, long long ldg);
+
+// The sticky device flag of the tcgen05 GEMM: 1 once a bounded wait ran out (read, not reset).
+int tf32x3_error_flag(int *host_value);

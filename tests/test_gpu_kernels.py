@@ -87,7 +87,8 @@ def test_potrf_trsv_trtri(cuda, n):
     assert int(info.item()) == 0
     L = np.tril(dA.cpu().numpy().reshape(n, n).T)
     np.testing.assert_allclose(L, L_ref, rtol=1e-10, atol=1e-12 * np.abs(L_ref).max())
-    assert pmin.item() == pytest.approx(np.min(np.diag(L_ref)) ** 2, rel=1e-10)
+    # the smallest squared pivot, capped at 1 (schur_factor_'s pmin starts at 1.0, solver.c:5346)
+    assert pmin.item() == pytest.approx(min(1.0, np.min(np.diag(L_ref)) ** 2), rel=1e-10)
     # triangular solves
     rng = np.random.default_rng(n + 1)
     b = rng.standard_normal(n)
@@ -196,9 +197,10 @@ def test_first_schur_matches_oracle_at_start(cuda, golden):
     want = restate.schur(S.A, X, [Zi])
     M = torch.zeros(d.m * d.m, dtype=torch.float64, device=cuda)
     ws = torch.empty(step.ws_bytes(n, 0, 0), dtype=torch.uint8, device=cuda)
+    dX, dZi = colmajor(X[0], cuda), colmajor(Zi, cuda)   # kept alive across the call
     step.call("schur_assemble", n, d.m, int(a["con"].numel()), a["con"].data_ptr(), a["cptr"].data_ptr(),
-              a["cpos"].data_ptr(), a["cval"].data_ptr(), colmajor(X[0], cuda).data_ptr(),
-              colmajor(Zi, cuda).data_ptr(), M.data_ptr(), 0, 0, ws.data_ptr(), ws.numel(), None)
+              a["cpos"].data_ptr(), a["cval"].data_ptr(), dX.data_ptr(), dZi.data_ptr(), M.data_ptr(), 0, 0,
+              ws.data_ptr(), ws.numel(), None)
     step.call("sync", None)
     got = M.cpu().numpy().reshape(d.m, d.m).T
     rel = np.abs(got - want).max() / np.abs(want).max()
@@ -210,13 +212,63 @@ def test_aop_and_symv(cuda):
     S, n, a = block_arrays(d, cuda)
     D = spd(n, 7)
     out = torch.zeros(d.m, dtype=torch.float64, device=cuda)
+    dD = colmajor(D, cuda)
     step.call("aop", n, int(a["con"].numel()), a["con"].data_ptr(), a["cptr"].data_ptr(), a["cpos"].data_ptr(),
-              a["cval"].data_ptr(), colmajor(D, cuda).data_ptr(), 1.0, 0.0, out.data_ptr(), None)
+              a["cval"].data_ptr(), dD.data_ptr(), 1.0, 0.0, out.data_ptr(), None)
     step.call("sync", None)
     np.testing.assert_allclose(out.cpu().numpy(), restate.aop(S.A, [D]), rtol=1e-12, atol=1e-12)
     M = spd(300, 8)
     x = np.random.default_rng(3).standard_normal(300)
     y = torch.zeros(300, dtype=torch.float64, device=cuda)
-    step.call("symv", 300, 2.0, colmajor(M, cuda).data_ptr(), 300, dev(x, cuda).data_ptr(), 0.0, y.data_ptr(), None)
+    dM, dx = colmajor(M, cuda), dev(x, cuda)
+    step.call("symv", 300, 2.0, dM.data_ptr(), 300, dx.data_ptr(), 0.0, y.data_ptr(), None)
     step.call("sync", None)
     np.testing.assert_allclose(y.cpu().numpy(), 2.0 * M @ x, rtol=1e-12, atol=1e-10)
+
+
+@pytest.mark.parametrize("M,N,K", [(128, 208, 32), (300, 400, 400), (1000, 1000, 1000), (16000, 256, 100), (130, 129, 37)])
+def test_gemm_tf32x3_accuracy(cuda, M, N, K):
+    """3xTF32 on tcgen05 reaches FP32-level accuracy: |G - A B| <= 2e-6 |A||B| entrywise bound
+    against the FP64 product of the unsplit inputs."""
+    rng = np.random.default_rng(M + N + K)
+    A = rng.standard_normal((M, K))
+    B = rng.standard_normal((K, N))
+    Kp = (K + 3) // 4 * 4                          # 16-byte row stride for the tensor maps
+    dA = torch.zeros((M, Kp), dtype=torch.float64, device=cuda)
+    dA[:, :K] = torch.as_tensor(A, device=cuda)
+    dBt = torch.zeros((N, Kp), dtype=torch.float64, device=cuda)
+    dBt[:, :K] = torch.as_tensor(B.T, device=cuda)
+    Ah = torch.empty((M, Kp), dtype=torch.float32, device=cuda)
+    Al = torch.empty_like(Ah)
+    Bh = torch.empty((N, Kp), dtype=torch.float32, device=cuda)
+    Bl = torch.empty_like(Bh)
+    step.call("split_tf32", M * Kp, dA.data_ptr(), Ah.data_ptr(), Al.data_ptr(), None)
+    step.call("split_tf32", N * Kp, dBt.data_ptr(), Bh.data_ptr(), Bl.data_ptr(), None)
+    G = torch.zeros(M * N, dtype=torch.float32, device=cuda)
+    step.call("gemm_tf32x3", M, N, K, Ah.data_ptr(), Al.data_ptr(), Kp, Bh.data_ptr(), Bl.data_ptr(), Kp,
+              G.data_ptr(), M, None)
+    step.call("sync", None)
+    got = G.cpu().numpy().reshape(N, M).T.astype(np.float64)
+    want = A @ B
+    bound = np.abs(A) @ np.abs(B)
+    assert np.max(np.abs(got - want) / bound) <= 2e-6
+
+
+def test_schur_tf32x3_matches_fp64(cuda):
+    """The mixed-precision assembly (3xTF32 GEMM, FP32 G, FP64 gather) against the FP64 one."""
+    d = problems.random_sdp(n=100, m=300, density=0.02, seed=3)
+    S, n, a = block_arrays(d, cuda)
+    X = spd(n, 5, cond=100)
+    Zi = spd(n, 6, cond=100)
+    dX, dZi = colmajor(X, cuda), colmajor(Zi, cuda)
+    out = []
+    for prec in (0, 1):
+        M = torch.zeros(d.m * d.m, dtype=torch.float64, device=cuda)
+        ws = torch.empty(step.ws_bytes(n, 16, prec), dtype=torch.uint8, device=cuda)
+        step.call("schur_assemble", n, d.m, int(a["con"].numel()), a["con"].data_ptr(), a["cptr"].data_ptr(),
+                  a["cpos"].data_ptr(), a["cval"].data_ptr(), dX.data_ptr(), dZi.data_ptr(), M.data_ptr(), prec, 16,
+                  ws.data_ptr(), ws.numel(), None)
+        step.call("sync", None)
+        out.append(M.cpu().numpy().reshape(d.m, d.m).T)
+    rel = np.abs(out[1] - out[0]).max() / np.abs(out[0]).max()
+    assert rel <= 1e-5
