@@ -22,9 +22,20 @@ BGPU_API size_t bgpu_schur_ws_bytes(int n, int chunk, int precision) {
 }
 BGPU_API int bgpu_schur_chunk_default(int n, int precision) { return schur_chunk_default(n, precision); }
 
+BGPU_API int bgpu_schur_colptr(int n, int ncon, const long long *d_cptr, const int *d_cpos, int *d_ccol, void *stream) {
+    DevBlock B;
+    B.n = n;
+    B.ncon = ncon;
+    B.cptr = (long long *)d_cptr;
+    B.cpos = (int *)d_cpos;
+    B.ccol = d_ccol;
+    return schur_colptr(S(stream), B);
+}
+
 BGPU_API int bgpu_schur_assemble(int n, int m, int ncon, const int *d_con, const long long *d_cptr,
-                                 const int *d_cpos, const double *d_cval, const double *d_X, const double *d_Zi,
-                                 double *d_M, int precision, int chunk, void *d_ws, size_t ws_bytes, void *stream) {
+                                 const int *d_ccol, const int *d_cpos, const double *d_cval, const double *d_X,
+                                 const double *d_Zi, double *d_M, int precision, int chunk, void *d_ws,
+                                 size_t ws_bytes, void *stream) {
     if (n <= 0 || m <= 0 || ncon < 0 || (precision != 0 && precision != 1)) return BGPU_ERR_ARG;
     if (chunk <= 0) chunk = schur_chunk_default(n, precision);
     DevBlock B;
@@ -32,6 +43,7 @@ BGPU_API int bgpu_schur_assemble(int n, int m, int ncon, const int *d_con, const
     B.ncon = ncon;
     B.con = (int *)d_con;
     B.cptr = (long long *)d_cptr;
+    B.ccol = (int *)d_ccol;
     B.cpos = (int *)d_cpos;
     B.cval = (double *)d_cval;
     return schur_assemble(S(stream), B, d_X, d_Zi, d_M, m, precision, chunk, d_ws, ws_bytes);

@@ -60,6 +60,7 @@ struct DevBlock {
     int *con = nullptr;     // [ncon] global constraint index
     long long *cptr = nullptr;  // [ncon+1] constraint-major offsets
     int *cpos = nullptr;    // [ne] position p + q*n, ascending within a constraint
+    int *ccol = nullptr;    // [ncon*(n+1)] first entry of each column k, relative to cptr[t]
     double *cval = nullptr; // [ne]
     long long *pptr = nullptr;  // [n*n+1] position-major offsets
     int *pcon = nullptr;    // [ne] global constraint index of each position-major entry
@@ -78,6 +79,8 @@ struct SchurWs {
     size_t bytes = 0;
 };
 size_t schur_ws_bytes(int n, int chunk, int precision);
+// Fills B.ccol (device, ncon*(n+1) ints) from cptr/cpos: the column pointers of each constraint.
+int schur_colptr(cudaStream_t st, const DevBlock &B);
 int schur_chunk_default(int n, int precision);
 // M (m x m, column-major, full symmetric) += the block's contribution sum over its constraints
 // of M_ab = <A_b, X A_a Zi>.  precision 0: FP64 (DMMA), 1: 3xTF32 (tcgen05).

@@ -18,58 +18,56 @@
 #include "tf32x3.h"
 
 namespace {
-constexpr int TP_Q = 32, TP_K = 128, TP_LD = TP_K + 1;
+constexpr int TP_Q = 128, TP_K = 32, TP_LD = TP_K + 1;   // CTA tile: 128 rows q x 32 columns k
 
+// T[(q K + t) ldt + k] = sum_{p'} Zi[q, p'] A_a[p', k]  (a = a0 + t): column k of Zi A_a is the
+// combination of the Zi columns p' that column k of A_a holds (Zi is symmetric: Zi[q, p'] =
+// Zi[q + p' n]).  Warp w owns columns k0 + w, k0 + w + 8, ...; a lane owns rows q0 + lane + 32 u.
+// The column's entries come from the per-constraint column pointers ccol, so no entry is read
+// by a warp that does not use it and the sums stay in registers in a fixed order.
 template <typename OutT>
-__global__ void __launch_bounds__(256) tprod_kernel(int n, int ldt, int K, int a0, int ncon, const long long *__restrict__ cptr,
+__global__ void __launch_bounds__(256) tprod_kernel(int n, int ldt, int K, int a0, int ncon,
+                                                   const long long *__restrict__ cptr, const int *__restrict__ ccol,
                                                    const int *__restrict__ cpos, const double *__restrict__ cval,
                                                    const double *__restrict__ Zi, OutT *__restrict__ T,
                                                    OutT *__restrict__ Tlo) {
     __shared__ double tile[TP_Q * TP_LD];
-    __shared__ long long rng[2];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int k0 = blockIdx.x * TP_K, q0 = blockIdx.y * TP_Q, t = blockIdx.z;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int q0 = blockIdx.x * TP_Q, k0 = blockIdx.y * TP_K, t = blockIdx.z;
     const int a = a0 + t;
-    for (int idx = tid; idx < TP_Q * TP_LD; idx += 256) tile[idx] = 0.0;
-    if (tid == 0) {
-        long long lo = 0, hi = 0;
-        if (a < ncon) {
-            const long long s = cptr[a], e = cptr[a + 1];
-            const long long plo = (long long)k0 * n, phi = (long long)min(k0 + TP_K, n) * n;
-            long long L = s, R = e;   // first entry with pos >= plo
-            while (L < R) { long long mid = (L + R) >> 1; if ((long long)cpos[mid] < plo) L = mid + 1; else R = mid; }
-            lo = L;
-            R = e;                    // first entry with pos >= phi
-            while (L < R) { long long mid = (L + R) >> 1; if ((long long)cpos[mid] < phi) L = mid + 1; else R = mid; }
-            hi = L;
-        }
-        rng[0] = lo;
-        rng[1] = hi;
-    }
-    __syncthreads();
-    const long long lo = rng[0], hi = rng[1];
-    const int q = q0 + lane;
-    for (long long e = lo; e < hi; e++) {
-        const int pos = cpos[e];
-        const int k = pos / n, pp = pos - k * n;
-        if (((k - k0) & 7) != warp) continue;       // one warp per column class: no smem races
-        if (q < n) tile[lane * TP_LD + (k - k0)] += cval[e] * Zi[q + (long long)pp * n];
-    }
-    __syncthreads();
-    // rows (q, t) of T, k contiguous
-    const int kw = min(TP_K, n - k0);
-    for (int idx = tid; idx < TP_Q * TP_K; idx += 256) {
-        const int r = idx / TP_K, kk = idx % TP_K;
-        if (q0 + r < n && kk < kw) {
-            const double v = tile[r * TP_LD + kk];
-            const long long o = ((long long)(q0 + r) * K + t) * ldt + k0 + kk;
-            if (sizeof(OutT) == 8) {
-                T[o] = (OutT)v;
-            } else {
-                const float hi_ = tf32_round((float)v);
-                T[o] = (OutT)hi_;
-                Tlo[o] = (OutT)tf32_round((float)(v - (double)hi_));
+    for (int kk = warp; kk < TP_K; kk += 8) {
+        const int k = k0 + kk;
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        if (a < ncon && k < n) {
+            const long long base = cptr[a];
+            const int *cc = ccol + (long long)a * (n + 1);
+            const long long e0 = base + cc[k], e1 = base + cc[k + 1];
+            for (long long e = e0; e < e1; e++) {
+                const int pp = cpos[e] - k * n;   // the row p' of the entry (p', k)
+                const double v = cval[e];
+                const double *z = Zi + (long long)pp * n + q0 + lane;
+#pragma unroll
+                for (int u = 0; u < 4; u++)
+                    if (q0 + lane + 32 * u < n) acc[u] += v * z[32 * u];
             }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) tile[(lane + 32 * u) * TP_LD + kk] = acc[u];
+    }
+    __syncthreads();
+    // rows (q, t) of T, k contiguous: a warp writes one row of 32 values per step
+    const int kw = min(TP_K, n - k0);
+    for (int r = warp; r < TP_Q; r += 8) {
+        const int q = q0 + r;
+        if (q >= n || lane >= kw) continue;
+        const double v = tile[r * TP_LD + lane];
+        const long long o = ((long long)q * K + t) * ldt + k0 + lane;
+        if (sizeof(OutT) == 8) {
+            T[o] = (OutT)v;
+        } else {
+            const float hi_ = tf32_round((float)v);
+            T[o] = (OutT)hi_;
+            Tlo[o] = (OutT)tf32_round((float)(v - (double)hi_));
         }
     }
 }
@@ -91,24 +89,50 @@ __global__ void __launch_bounds__(256) gather_kernel(int a0, int ncon, int m, co
 #pragma unroll
     for (int u = 0; u < PER; u++) acc[u] = 0.0;
     const long long s = cptr[b], e = cptr[b + 1];
-    for (long long base = s; base < e; base += 32) {
+    // two accumulators per column (even and odd entry slots) break the FMA chain; full 32-entry
+    // groups run fully unrolled so their G loads are all in flight together
+    double acc2[PER];
+#pragma unroll
+    for (int u = 0; u < PER; u++) acc2[u] = 0.0;
+    long long base = s;
+    for (; base + 32 <= e; base += 32) {
+        const int pos = cpos[base + lane];
+        const double v = cval[base + lane];
+        const GT *gp = G + l;
+#pragma unroll
+        for (int j = 0; j < 32; j += GPW) {
+            const int pj = __shfl_sync(0xffffffffu, pos, j + sub);
+            const double vj = __shfl_sync(0xffffffffu, v, j + sub);
+            const GT *g = gp + (long long)pj * K;
+            if ((j / GPW) & 1) {
+#pragma unroll
+                for (int u = 0; u < PER; u++) acc2[u] += vj * (double)g[u * LPG];
+            } else {
+#pragma unroll
+                for (int u = 0; u < PER; u++) acc[u] += vj * (double)g[u * LPG];
+            }
+        }
+    }
+    if (base < e) {   // the ragged last group
         const long long my = base + lane;
         int pos = 0;
         double v = 0.0;
         if (my < e) { pos = cpos[my]; v = cval[my]; }
-        const int cnt = (int)min((long long)32, e - base);
+        const int cnt = (int)(e - base);
         for (int j = 0; j < cnt; j += GPW) {   // uniform trip count: every lane shuffles together
             const int jj = j + sub;
             const int src = jj < cnt ? jj : 0;
             const int pj = __shfl_sync(0xffffffffu, pos, src);
             const double vj = __shfl_sync(0xffffffffu, v, src);
             if (jj < cnt) {
-                const GT *g = G + (long long)pj * K;
+                const GT *g = G + (long long)pj * K + l;
 #pragma unroll
-                for (int u = 0; u < PER; u++) acc[u] += vj * (double)g[l + u * LPG];
+                for (int u = 0; u < PER; u++) acc[u] += vj * (double)g[u * LPG];
             }
         }
     }
+#pragma unroll
+    for (int u = 0; u < PER; u++) acc[u] += acc2[u];
 #pragma unroll
     for (int u = 0; u < PER; u++)
 #pragma unroll
@@ -178,6 +202,31 @@ __global__ void atop_kernel(long long npos, const long long *__restrict__ pptr, 
 }
 }  // namespace
 
+namespace {
+__global__ void colptr_kernel(int n, int ncon, const long long *__restrict__ cptr, const int *__restrict__ cpos,
+                              int *__restrict__ ccol) {
+    const int t = blockIdx.x;
+    if (t >= ncon) return;
+    const long long s = cptr[t], e = cptr[t + 1];
+    for (int k = threadIdx.x; k <= n; k += blockDim.x) {
+        const long long key = (long long)k * n;   // first position of column k
+        long long L = s, R = e;
+        while (L < R) {
+            const long long mid = (L + R) >> 1;
+            if ((long long)cpos[mid] < key) L = mid + 1; else R = mid;
+        }
+        ccol[(long long)t * (n + 1) + k] = (int)(L - s);
+    }
+}
+}  // namespace
+
+int schur_colptr(cudaStream_t st, const DevBlock &B) {
+    if (B.ncon <= 0) return BGPU_OK;
+    colptr_kernel<<<B.ncon, 128, 0, st>>>(B.n, B.ncon, B.cptr, B.cpos, B.ccol);
+    BGPU_LAUNCH_CHECK();
+    return BGPU_OK;
+}
+
 int aop_f64(cudaStream_t st, const DevBlock &B, const double *D, double alpha, double beta, double *out) {
     if (B.ncon <= 0) return BGPU_OK;
     aop_kernel<<<ceil_div(B.ncon, 8), 256, 0, st>>>(B.ncon, B.con, B.cptr, B.cpos, B.cval, D, alpha, beta, out);
@@ -216,13 +265,14 @@ int schur_assemble(cudaStream_t st, const DevBlock &B, const double *X, const do
     const int n = B.n, K = chunk;
     if (B.ncon <= 0) return BGPU_OK;
     if (K != 8 && K != 16 && K != 32 && K != 64) return BGPU_ERR_ARG;
+    if (!B.ccol) return BGPU_ERR_ARG;
     if (ws_bytes < schur_ws_bytes(n, K, precision)) return BGPU_ERR_ARG;
     const size_t nnK = (size_t)n * n * K;
-    dim3 tgrid(ceil_div(n, TP_K), ceil_div(n, TP_Q), K);
+    dim3 tgrid(ceil_div(n, TP_Q), ceil_div(n, TP_K), K);
     if (precision == 0) {
         double *T = (double *)ws, *G = T + nnK;
         for (int a0 = 0; a0 < B.ncon; a0 += K) {
-            tprod_kernel<double><<<tgrid, 256, 0, st>>>(n, n, K, a0, B.ncon, B.cptr, B.cpos, B.cval, Zi, T, nullptr);
+            tprod_kernel<double><<<tgrid, 256, 0, st>>>(n, n, K, a0, B.ncon, B.cptr, B.ccol, B.cpos, B.cval, Zi, T, nullptr);
             BGPU_LAUNCH_CHECK();
             int rc = gemm_f64(st, 1, 1, n * K, n, n, 1.0, T, n, 0, X, n, 0, 0.0, G, (long long)n * K, 0, 1, 0);
             if (rc) return rc;
@@ -245,7 +295,7 @@ int schur_assemble(cudaStream_t st, const DevBlock &B, const double *X, const do
     split2d_kernel<<<dim3(ceil_div(ld, 256), n), 256, 0, st>>>(n, X, ld, Xh, Xl);
     BGPU_LAUNCH_CHECK();
     for (int a0 = 0; a0 < B.ncon; a0 += K) {
-        tprod_kernel<float><<<tgrid, 256, 0, st>>>(n, ld, K, a0, B.ncon, B.cptr, B.cpos, B.cval, Zi, Th, Tl);
+        tprod_kernel<float><<<tgrid, 256, 0, st>>>(n, ld, K, a0, B.ncon, B.cptr, B.ccol, B.cpos, B.cval, Zi, Th, Tl);
         BGPU_LAUNCH_CHECK();
         int rc = gemm_tf32x3(st, n * K, n, n, Th, Tl, ld, Xh, Xl, ld, G, (long long)n * K);
         if (rc) return rc;

@@ -417,15 +417,18 @@ void Solver::upload_block(int k) {
     d.cptr = g.alloc<long long>(d.ncon + 1);
     d.cpos = g.alloc<int>(d.ne);
     d.cval = g.alloc<double>(d.ne);
+    d.ccol = g.alloc<int>((size_t)d.ncon * (n + 1));
     d.pptr = g.alloc<long long>(nn + 1);
     d.pcon = g.alloc<int>(d.ne);
     d.pval = g.alloc<double>(d.ne);
     d.C = g.alloc<double>(nn);
-    if (!d.con || !d.cptr || !d.cpos || !d.cval || !d.pptr || !d.pcon || !d.pval || !d.C) throw GpuFail{BGPU_ERR_NOMEM, __LINE__};
+    if (!d.con || !d.cptr || !d.cpos || !d.cval || !d.ccol || !d.pptr || !d.pcon || !d.pval || !d.C)
+        throw GpuFail{BGPU_ERR_NOMEM, __LINE__};
     CU(cudaMemcpy(d.con, B.con.data(), sizeof(int) * d.ncon, cudaMemcpyHostToDevice));
     CU(cudaMemcpy(d.cptr, B.cptr.data(), sizeof(long long) * (d.ncon + 1), cudaMemcpyHostToDevice));
     CU(cudaMemcpy(d.cpos, B.cpos.data(), sizeof(int) * d.ne, cudaMemcpyHostToDevice));
     CU(cudaMemcpy(d.cval, B.cval.data(), sizeof(double) * d.ne, cudaMemcpyHostToDevice));
+    RC(schur_colptr(g.st, d));
     // position-major copy (A'(y) without atomics): entries of each position in constraint order
     std::vector<long long> pptr(nn + 1, 0);
     for (long long e = 0; e < d.ne; e++) pptr[B.cpos[e] + 1]++;

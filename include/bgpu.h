@@ -65,11 +65,14 @@ BGPU_API int bgpu_schur_chunk_default(int n, int precision);
  * column-major): M[con_a, con_b] += <A_b, X A_a Zi> for all constraint pairs of the block.
  * Constraints are given constraint-major: local constraint t has global index d_con[t] and
  * entries d_cpos/d_cval[d_cptr[t] .. d_cptr[t+1]) of the full (both triangles) expansion, with
- * positions p + q n ascending.  Replaces schur_sdp / schur_sdp_id (solver.c:1969, 2339-3021)
- * for the row-product route. */
+ * positions p + q n ascending.  d_ccol (ncon*(n+1) ints) receives/holds the per-constraint
+ * column pointers: bgpu_schur_colptr fills it once per problem.  Replaces schur_sdp /
+ * schur_sdp_id (solver.c:1969, 2339-3021) for the row-product route. */
+BGPU_API int bgpu_schur_colptr(int n, int ncon, const long long *d_cptr, const int *d_cpos, int *d_ccol, void *stream);
 BGPU_API int bgpu_schur_assemble(int n, int m, int ncon, const int *d_con, const long long *d_cptr,
-                                 const int *d_cpos, const double *d_cval, const double *d_X, const double *d_Zi,
-                                 double *d_M, int precision, int chunk, void *d_ws, size_t ws_bytes, void *stream);
+                                 const int *d_ccol, const int *d_cpos, const double *d_cval, const double *d_X,
+                                 const double *d_Zi, double *d_M, int precision, int chunk, void *d_ws,
+                                 size_t ws_bytes, void *stream);
 
 /* In-place Cholesky L L' = A of the lower triangle (column-major, lda); d_dinv receives the
  * inverses of the 64 x 64 diagonal blocks (ceil(n/64)*4096 entries), *d_info the first failing

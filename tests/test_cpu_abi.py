@@ -62,3 +62,36 @@ def test_options_to_argv_matches_reference_forms():
     assert options_to_argv({"tol": 1e-7, "nohsd": True, "dir": "hkm", "x": None}) == ["-tol", "1e-07", "-nohsd", "-dir", "hkm"]
     assert options_to_argv("-tol 1e-7 -mixed 0") == ["-tol", "1e-7", "-mixed", "0"]
     assert options_to_argv(["-q"]) == ["-q"]
+
+
+# The entry points the reference's ctypes loader (python/brisk/_core.py:61-102) binds without a
+# hasattr guard: a drop-in must export every one of them.
+REFERENCE_LOADER_SYMBOLS = [
+    "brisk_version", "brisk_set_output", "brisk_result_new", "brisk_result_delete", "brisk_result_status",
+    "brisk_result_exit_code", "brisk_result_iterations", "brisk_result_m", "brisk_result_nblk",
+    "brisk_result_have_x", "brisk_result_pobj", "brisk_result_dobj", "brisk_result_time",
+    "brisk_result_status_str", "brisk_result_blocksize", "brisk_result_dimacs", "brisk_result_y", "brisk_result_X",
+    "brisk_result_Z", "brisk_solve_data", "brisk_solve_file", "brisk_result_bound", "brisk_result_resolves",
+    "brisk_result_cause", "brisk_interrupt", "brisk_interrupted",
+]
+
+
+def test_exports_what_the_reference_loader_binds(libpath):
+    L = ctypes.CDLL(libpath, mode=os.RTLD_LOCAL)
+    assert [s for s in REFERENCE_LOADER_SYMBOLS if not hasattr(L, s)] == []
+
+
+@pytest.mark.skipif(not os.path.isdir("/root/reference/python/brisk"), reason="reference tree absent")
+def test_reference_python_package_loads_this_library(libpath, monkeypatch):
+    """The reference's own binding loads libbrisk (B200 build) through BRISK_LIBRARY."""
+    import importlib
+    import sys
+    monkeypatch.setenv("BRISK_LIBRARY", libpath)
+    monkeypatch.syspath_prepend("/root/reference/python")
+    sys.modules.pop("brisk", None)
+    sys.modules.pop("brisk._core", None)
+    brisk = importlib.import_module("brisk")
+    assert brisk.version().startswith("1.7")
+    assert os.path.samefile(brisk.library_path(), libpath)
+    sys.modules.pop("brisk", None)
+    sys.modules.pop("brisk._core", None)

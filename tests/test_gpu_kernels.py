@@ -161,6 +161,9 @@ def block_arrays(d, cuda):
                 cptr=torch.tensor(cptr, dtype=torch.int64, device=cuda),
                 cpos=torch.tensor(cpos, dtype=torch.int32, device=cuda),
                 cval=torch.tensor(cval, dtype=torch.float64, device=cuda))
+    arrs["ccol"] = torch.zeros(len(con) * (n + 1), dtype=torch.int32, device=cuda)
+    step.call("schur_colptr", n, len(con), arrs["cptr"].data_ptr(), arrs["cpos"].data_ptr(), arrs["ccol"].data_ptr(),
+              None)
     return S, n, arrs
 
 
@@ -181,7 +184,7 @@ def test_schur_fp64_matches_oracle(cuda, name, kw, chunk):
     ws = torch.empty(step.ws_bytes(n, chunk, 0), dtype=torch.uint8, device=cuda)
     dX, dZi = colmajor(X, cuda), colmajor(Zi, cuda)
     step.call("schur_assemble", n, d.m, int(a["con"].numel()), a["con"].data_ptr(), a["cptr"].data_ptr(),
-              a["cpos"].data_ptr(), a["cval"].data_ptr(), dX.data_ptr(), dZi.data_ptr(), M.data_ptr(), 0, chunk,
+              a["ccol"].data_ptr(), a["cpos"].data_ptr(), a["cval"].data_ptr(), dX.data_ptr(), dZi.data_ptr(), M.data_ptr(), 0, chunk,
               ws.data_ptr(), ws.numel(), None)
     step.call("sync", None)
     got = M.cpu().numpy().reshape(d.m, d.m).T
@@ -199,7 +202,7 @@ def test_first_schur_matches_oracle_at_start(cuda, golden):
     ws = torch.empty(step.ws_bytes(n, 0, 0), dtype=torch.uint8, device=cuda)
     dX, dZi = colmajor(X[0], cuda), colmajor(Zi, cuda)   # kept alive across the call
     step.call("schur_assemble", n, d.m, int(a["con"].numel()), a["con"].data_ptr(), a["cptr"].data_ptr(),
-              a["cpos"].data_ptr(), a["cval"].data_ptr(), dX.data_ptr(), dZi.data_ptr(), M.data_ptr(), 0, 0,
+              a["ccol"].data_ptr(), a["cpos"].data_ptr(), a["cval"].data_ptr(), dX.data_ptr(), dZi.data_ptr(), M.data_ptr(), 0, 0,
               ws.data_ptr(), ws.numel(), None)
     step.call("sync", None)
     got = M.cpu().numpy().reshape(d.m, d.m).T
@@ -266,7 +269,7 @@ def test_schur_tf32x3_matches_fp64(cuda):
         M = torch.zeros(d.m * d.m, dtype=torch.float64, device=cuda)
         ws = torch.empty(step.ws_bytes(n, 16, prec), dtype=torch.uint8, device=cuda)
         step.call("schur_assemble", n, d.m, int(a["con"].numel()), a["con"].data_ptr(), a["cptr"].data_ptr(),
-                  a["cpos"].data_ptr(), a["cval"].data_ptr(), dX.data_ptr(), dZi.data_ptr(), M.data_ptr(), prec, 16,
+                  a["ccol"].data_ptr(), a["cpos"].data_ptr(), a["cval"].data_ptr(), dX.data_ptr(), dZi.data_ptr(), M.data_ptr(), prec, 16,
                   ws.data_ptr(), ws.numel(), None)
         step.call("sync", None)
         out.append(M.cpu().numpy().reshape(d.m, d.m).T)
