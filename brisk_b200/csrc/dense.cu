@@ -458,3 +458,66 @@ int dots_f64(cudaStream_t st, int nq, const double *const *a, const double *cons
     BGPU_LAUNCH_CHECK();
     return BGPU_OK;
 }
+
+// ---- the triangular solve without caller-provided scratch ----------------------------------
+// Some callers cannot allocate device memory where they solve: code between the steps of a loop
+// where cudaMalloc / cudaFree would synchronize the device, or a process whose device memory is
+// owned by another allocator (a framework's caching pool, a fixed budget).  For them,
+// bgpu_trsv_noalloc keeps the block-row flags and the wait-error flag of the solve in this
+// file-scope array instead of buffers the caller passes.  Every GPU that loads the library holds
+// the array (16 KB) until the process exits.
+#include <mutex>
+#define BGPU_NOALLOC_TRSV_MAXBLK 4096   // block rows of 64: n <= 262144
+static __device__ __align__(256) int g_trsv_noalloc_scratch[BGPU_NOALLOC_TRSV_MAXBLK + 1];
+
+namespace {
+struct NoallocDev {
+    int *ptr = nullptr;   // device address of g_trsv_noalloc_scratch on this device
+    int epoch = 0;
+};
+constexpr int NOALLOC_MAXDEV = 64;
+NoallocDev g_noalloc[NOALLOC_MAXDEV];
+std::mutex g_noalloc_mu;
+}  // namespace
+
+extern "C" BGPU_API int bgpu_trsv_noalloc(int n, const double *d_L, int lda, const double *d_dinv, double *d_x,
+                                          int trans, void *stream) {
+    if (n <= 0 || lda < n || !d_L || !d_dinv || !d_x) return BGPU_ERR_ARG;
+    const int nblk = (n + NB - 1) / NB;
+    if (nblk > BGPU_NOALLOC_TRSV_MAXBLK) {
+        fprintf(stderr, "bgpu_trsv_noalloc: n = %d is above this entry point's maximum of %d\n", n,
+                BGPU_NOALLOC_TRSV_MAXBLK * NB);
+        return BGPU_ERR_TOOBIG;
+    }
+    int dev = 0;
+    BGPU_CHECK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= NOALLOC_MAXDEV) return BGPU_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    int *scratch = nullptr, epoch = 0;
+    {
+        std::lock_guard<std::mutex> lock(g_noalloc_mu);
+        NoallocDev &d = g_noalloc[dev];
+        if (!d.ptr) {
+            // set-up on the first call on this device: the array's device address (the host-side
+            // symbol is only a stand-in) and its flags cleared to 0 (every epoch below is > 0)
+            void *p = nullptr;
+            BGPU_CHECK(cudaGetSymbolAddress(&p, g_trsv_noalloc_scratch));
+            BGPU_CHECK(cudaMemset(p, 0, sizeof(int) * (BGPU_NOALLOC_TRSV_MAXBLK + 1)));
+            d.ptr = (int *)p;
+        }
+        if (d.epoch == 0x7fffffff) {   // epochs exhausted: start over from cleared flags
+            BGPU_CHECK(cudaMemsetAsync(d.ptr, 0, sizeof(int) * BGPU_NOALLOC_TRSV_MAXBLK, st));
+            d.epoch = 0;
+        }
+        epoch = ++d.epoch;
+        scratch = d.ptr;
+    }
+    int *err = scratch + BGPU_NOALLOC_TRSV_MAXBLK;
+    BGPU_CHECK(cudaMemsetAsync(err, 0, sizeof(int), st));   // the error flag starts each call at 0
+    int rc = trsv_launch<double>(st, n, d_L, lda, d_dinv, d_x, trans, scratch, epoch, err);
+    if (rc) return rc;
+    int h_err = 0;
+    BGPU_CHECK(cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    BGPU_CHECK(cudaStreamSynchronize(st));
+    return h_err ? BGPU_ERR_TIMEOUT : BGPU_OK;
+}

@@ -39,6 +39,7 @@ def lib():
         "bgpu_potrf_f32": ([I, P, I, P, P, P, P], I),
         "bgpu_trsv": ([I, P, I, P, P, I, P, I, P, P], I),
         "bgpu_trsv_f32": ([I, P, I, P, P, I, P, I, P, P], I),
+        "bgpu_trsv_noalloc": ([I, P, I, P, P, I, P], I),
         "bgpu_trtri": ([I, P, I, P, P, I, P], I),
         "bgpu_dgemm": ([I, I, I, I, I, D, P, I64, P, I64, D, P, I64, I, P], I),
         "bgpu_gemm_tf32x3": ([I, I, I, P, P, I64, P, P, I64, P, I64, P], I),

@@ -91,6 +91,18 @@ BGPU_API int bgpu_trsv(int n, const double *d_L, int lda, const double *d_dinv, 
 BGPU_API int bgpu_trsv_f32(int n, const float *d_L, int lda, const float *d_dinv, float *d_x, int trans,
                            int *d_flags, int epoch, int *d_err, void *stream);
 
+/* bgpu_trsv without caller-provided scratch, for callers that cannot allocate device memory
+ * where they solve (between loop steps where cudaMalloc/cudaFree would synchronize the device,
+ * or under another allocator that owns the device memory).  It has no counterpart in the
+ * reference.  The block-row flags and the wait-error flag live in a static 16 KB device array of
+ * the library, so n <= 262144 (64 x 4096 block rows); a larger n returns BGPU_ERR_TOOBIG with a
+ * message.  The first call on each device sets the array up (its device address and cleared
+ * flags); make that first call before any stream capture.  The call waits for the stream and
+ * returns BGPU_ERR_TIMEOUT when a bounded device wait gave up.  Every call on a device shares the
+ * array: calls that overlap on the GPU (other streams, other threads) race. */
+BGPU_API int bgpu_trsv_noalloc(int n, const double *d_L, int lda, const double *d_dinv, double *d_x, int trans,
+                               void *stream);
+
 /* Linv = L^-1 from the factor of bgpu_potrf (the first half of brisk_dpotri_full,
  * sparsechol.c:4190). */
 BGPU_API int bgpu_trtri(int n, const double *d_L, int lda, const double *d_dinv, double *d_Linv, int ldi,
