@@ -1,0 +1,36 @@
+"""Command line: solve an SDPA file or a seeded workload on the GPU, options as for BRISK.
+
+    python -m brisk_b200 problem.dat-s -tol 1e-7 -v
+    python -m brisk_b200 --workload rand1000 -asmprec tf32x3 -v
+
+The file form mirrors the reference's command line (`brisk <file> <options>`, main.c:3571); the
+workload form solves one of the seeded instances of brisk_b200.problems.
+"""
+import sys
+
+from . import problems, solve_file, solve_sdpa
+
+WORKLOADS = {
+    "theta50": lambda: problems.theta_problem(n=50, p=0.5, seed=1),
+    "rand400": lambda: problems.random_sdp(n=400, m=2000, density=0.01, seed=0),
+    "rand1000": lambda: problems.random_sdp(n=1000, m=8000, density=0.005, seed=0),
+}
+
+
+def main(argv):
+    if not argv:
+        print(__doc__)
+        return 1
+    if argv[0] == "--workload":
+        if len(argv) < 2 or argv[1] not in WORKLOADS:
+            print("workloads: " + ", ".join(sorted(WORKLOADS)))
+            return 1
+        d = WORKLOADS[argv[1]]()
+        r = solve_sdpa(*d.args(), options=argv[2:], verbose=True)
+    else:
+        r = solve_file(argv[0], options=argv[1:], verbose=True)
+    return r.exit_code
+
+
+if __name__ == "__main__":
+    sys.exit(main(sys.argv[1:]))

@@ -21,6 +21,7 @@
 #include "elementwise.h"
 #include "kernels.h"
 #include "solver.h"
+#include "tf32x3.h"
 
 #include <algorithm>
 #include <chrono>
@@ -386,6 +387,15 @@ class Solver {
     int factor();
     void prec(const std::vector<double> &r, std::vector<double> &z);
     void schur_mv(const std::vector<double> &x, std::vector<double> &y);
+    // y = A(Z^-1 A'(x) X): the Newton system's operator in FP64 without the assembled M (the
+    // residual of the mixed path, whose M is FP32-accurate)
+    void newton_mv(const std::vector<double> &x, std::vector<double> &y);
+    void mv(const std::vector<double> &x, std::vector<double> &y) {
+        if (m_exact) schur_mv(x, y);
+        else newton_mv(x, y);
+    }
+    bool m_exact = true;      // M was assembled in FP64 (the residual may use it)
+    bool asm_fp64 = false;    // the mixed path fell back to FP64 assembly
     double schur_solve(const std::vector<double> &rhs, std::vector<double> &x, double tol_rel);
     // step length
     double maxstep(int primal, int K);
@@ -555,8 +565,10 @@ void Solver::zinv(int k) {
 void Solver::assemble(std::vector<double> &) {
     CU(cudaMemsetAsync(M, 0, sizeof(double) * (size_t)m * m, g.st));
     CU(cudaEventRecord(ev0, g.st));
+    const int prec = (asm_prec == 1 && !asm_fp64) ? 1 : 0;
+    m_exact = prec == 0;
     for (int k = 0; k < nb; k++) {
-        RC(schur_assemble(g.st, db[k], da[k].X, da[k].Zi, M, m, asm_prec, chunk, ws, ws_bytes));
+        RC(schur_assemble(g.st, db[k], da[k].X, da[k].Zi, M, m, prec, prec ? chunk : chunk64, ws, ws_bytes));
         const double n = db[k].n;
         const double ncon = db[k].ncon;
         schur_flops += 2.0 * n * n * n * ncon;   // the row-product GEMMs: 2 n^2 r_a with r_a <= n
@@ -566,6 +578,11 @@ void Solver::assemble(std::vector<double> &) {
     float ms = 0;
     CU(cudaEventElapsedTime(&ms, ev0, ev1));
     schur_dev_time += ms * 1e-3;
+    if (prec == 1) {
+        int bad = 0;
+        RC(tf32x3_error_flag(&bad));
+        if (bad) throw GpuFail{BGPU_ERR_TIMEOUT, __LINE__};
+    }
 }
 
 // schur_factor_ (solver.c:5296-5421), dense path
@@ -660,6 +677,19 @@ void Solver::schur_mv(const std::vector<double> &x, std::vector<double> &y) {
     CU(cudaStreamSynchronize(g.st));
 }
 
+void Solver::newton_mv(const std::vector<double> &x, std::vector<double> &y) {
+    std::vector<double *> Fs(nb);
+    for (int k = 0; k < nb; k++) {
+        const int n = db[k].n;
+        DevArrays &d = da[k];
+        atop_block(k, x, 1.0, 0.0, d.W);   // A'(x)
+        mul(n, 1.0, d.Zi, d.W, d.T);
+        mul(n, 1.0, d.T, d.X, d.F);        // Z^-1 A'(x) X
+        Fs[k] = d.F;
+    }
+    aop_all(Fs, y);
+}
+
 static double dot(const std::vector<double> &a, const std::vector<double> &b) {
     double s = 0;
     for (size_t i = 0; i < a.size(); i++) s += a[i] * b[i];
@@ -674,7 +704,7 @@ double Solver::schur_solve(const std::vector<double> &rhs, std::vector<double> &
     if (nb_ == 0) return 0;
     prec(rhs, x);
     std::vector<double> Mx, r(m), z, p, q, xb;
-    schur_mv(x, Mx);
+    mv(x, Mx);
     for (int i = 0; i < m; i++) r[i] = rhs[i] - Mx[i];
     double nr = nrm(r);
     const double tol = std::max(tol_rel, is_float ? 1e-10 : 1e-13) * nb_;
@@ -689,7 +719,7 @@ double Solver::schur_solve(const std::vector<double> &rhs, std::vector<double> &
     const double sgain = 0.9;
     const int smax = 4;
     for (int k = 0; k < maxit; k++) {
-        schur_mv(p, q);
+        mv(p, q);
         const double pq = dot(p, q);
         if (!(pq > 0)) break;
         const double a = rz / pq;
@@ -710,10 +740,16 @@ double Solver::schur_solve(const std::vector<double> &rhs, std::vector<double> &
         for (int i = 0; i < m; i++) p[i] = z[i] + beta * p[i];
     }
     x = xb;
-    schur_mv(x, Mx);
+    mv(x, Mx);
     for (int i = 0; i < m; i++) r[i] = rhs[i] - Mx[i];
     const double rel = nrm(r) / nb_;
     if (is_float && (used > 4 || best > tol || rel > std::max(1e-9, 10 * tol_rel))) want_double = true;
+    // the mixed path: when PCG cannot reach the tolerance against the FP64 operator with the
+    // factor of the FP32-accurate M, the following iterations assemble M in FP64
+    if (!m_exact && (best > tol || rel > std::max(1e-9, 10 * tol_rel)) && !asm_fp64) {
+        asm_fp64 = true;
+        if (opt.verbose > 1) log_printf(0, "   mixed path: PCG missed %.1e (rel %.1e): FP64 assembly from here on\n", tol / nb_, rel);
+    }
     return rel;
 }
 
@@ -824,6 +860,7 @@ int Solver::try_step(int primal, double *alpha) {
 void Solver::least_squares_start(std::vector<double> &y) {
     const bool af = allow_float;
     allow_float = false;   // the start's Gram solves in FP64
+    m_exact = true;        // A A' is assembled in FP64 here
     CU(cudaMemsetAsync(M, 0, sizeof(double) * (size_t)m * m, g.st));
     for (int k = 0; k < nb; k++) {
         RC(ew_set_scaled_identity(g.st, db[k].n, da[k].T, 1.0));
@@ -966,6 +1003,8 @@ int Solver::run(ResultData &res) {
     min_pivot = 1;
     nfloat = nfactor = pcg_iters = 0;
     mu_now = 1e300;
+    m_exact = true;
+    asm_fp64 = false;
     schur_flops = schur_dev_time = 0;
     CU(cudaEventRecord(evs0, g.st));
     std::vector<double> y(m, 0.0), ybest(m, 0.0), dy, rp(m), a0, h(m, 0.0), rhs(m), qv, ev(m), wv;
@@ -1104,6 +1143,7 @@ int Solver::run(ResultData &res) {
             if (theta * r0norm <= 1e-13) theta = 0.0;
         }
         // ---- Schur complement ----
+        const double ts_before = tm.schur, tstep_before = tm.step;
         double ts = wtime();
         assemble(tmpv);
         double tc = wtime();
@@ -1277,6 +1317,9 @@ int Solver::run(ResultData &res) {
         if (!okp || !okd) { status = 4; break; }
         for (int i = 0; i < m; i++) y[i] += adn * dy[i];
         theta *= (1.0 - adn);
+        if (opt.verbose > 1)
+            log_printf(0, "     [schur %.3fs %s, factor %s reg %.0e pmin %.1e, pcg %d, step %.3fs]\n", tm.schur - ts_before,
+                       m_exact ? "fp64" : "tf32x3", is_float ? "fp32" : "fp64", reg, min_pivot, pcg_iters, tm.step - tstep_before);
         alp = apn;
         ald = adn;
         stall = (apn < 1e-6 && adn < 1e-6) ? stall + 1 : 0;
