@@ -3,6 +3,7 @@
 #include "common.cuh"
 #include "kernels.h"
 #include "tf32x3.h"
+#include "small.h"
 
 long long g_bgpu_launches = 0;
 static cudaStream_t S(void *s) { return (cudaStream_t)s; }
@@ -104,6 +105,22 @@ BGPU_API int bgpu_aop(int n, int ncon, const int *d_con, const long long *d_cptr
     B.cpos = (int *)d_cpos;
     B.cval = (double *)d_cval;
     return aop_f64(S(stream), B, d_D, alpha, beta, d_out);
+}
+
+BGPU_API int bgpu_small_chol_inv(int nb, const int *d_n, double *const *d_A, double *const *d_L,
+                                 double *const *d_Li, int *d_info, void *stream) {
+    if (nb < 0) return BGPU_ERR_ARG;
+    return small_chol_inv(S(stream), nb, d_n, d_A, d_L, d_Li, d_info);
+}
+BGPU_API int bgpu_small_lammin(int nb, const int *d_n, const double *const *d_Li, const double *const *d_D,
+                               double *d_lam, void *stream) {
+    if (nb < 0) return BGPU_ERR_ARG;
+    return small_lammin(S(stream), nb, d_n, d_Li, d_D, d_lam);
+}
+BGPU_API int bgpu_small_gemm(int nb, const int *d_n, int ta, int tb, double alpha, const double *const *d_A,
+                             const double *const *d_B, double beta, double *const *d_C, int sym, void *stream) {
+    if (nb < 0) return BGPU_ERR_ARG;
+    return small_gemm(S(stream), nb, d_n, ta, tb, alpha, d_A, d_B, beta, d_C, sym);
 }
 
 }  // extern "C"

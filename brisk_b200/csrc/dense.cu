@@ -22,75 +22,67 @@ constexpr int NB = TRI_NB;      // 64
 constexpr int LDS = NB + 1;     // padded smem stride
 
 // ---- diagonal-block factor + inverse ----------------------------------------------------
-// One CTA of 64 threads: thread i owns row i of the 64 x 64 block in shared memory.  Column c:
-// the pivot, then every row below scales its entry and updates its own row (two barriers a
-// column); the inverse of the factor is formed the same way, one row of X per thread.
+// One CTA of 256 threads (a 16 x 16 grid tx, ty) on the 64 x 64 block in shared memory.  Column
+// c: every thread reads the pivot (a broadcast), the column below is scaled, then the trailing
+// lower triangle is updated with the 2-D thread grid (two barriers a column, no integer
+// division in the loops).  The inverse of the factor follows the same pattern: row k of X is
+// final once divided by L(k,k); the rows below subtract L(r,k) X(k,:).
 template <typename T>
-__global__ void __launch_bounds__(64) potrf_diag_kernel(int n, T *A, long long lda, int j0, T *dinv, int *info,
-                                                        double *pmin) {
+__global__ void __launch_bounds__(256) potrf_diag_kernel(int n, T *A, long long lda, int j0, T *dinv, int *info,
+                                                         double *pmin) {
     extern __shared__ __align__(16) unsigned char dsm_raw[];
     T *S = reinterpret_cast<T *>(dsm_raw);   // S[r + c*LDS]: factor, then L
     T *X = S + NB * LDS;                      // inverse of L
-    __shared__ int fail;
-    __shared__ double pm_s;
-    const int i = threadIdx.x;
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
     const int nb = min(NB, n - j0);
     if (*(volatile int *)info != 0) return;   // an earlier panel failed: nothing to do
     T *Ad = A + (long long)j0 + (long long)j0 * lda;
-    for (int c = 0; c < NB; c++) {            // column c, row i: coalesced over i
-        T v = (T)0;
-        if (i < nb && c < nb && i >= c) v = Ad[i + (long long)c * lda];
-        S[i + c * LDS] = v;
-        X[i + c * LDS] = (i == c) ? (T)1 : (T)0;
-    }
-    if (i == 0) { fail = 0; pm_s = 1e300; }
+    for (int c = ty; c < NB; c += 16)
+        for (int r = tx; r < NB; r += 16) {   // column c: rows r coalesced over tx
+            T v = (T)0;
+            if (r < nb && c < nb && r >= c) v = Ad[r + (long long)c * lda];
+            S[r + c * LDS] = v;
+            X[r + c * LDS] = (r == c) ? (T)1 : (T)0;
+        }
     __syncthreads();
+    double pm = 1e300;
+    int fail = 0;
     for (int c = 0; c < nb; c++) {
-        if (i == c) {
-            const T d = S[c + c * LDS];
-            if (!(d > (T)0) || !isfinite((double)d)) fail = j0 + c + 1;
-            else {
-                S[c + c * LDS] = sqrt(d);
-                if ((double)d < pm_s) pm_s = (double)d;
-            }
+        const T d = S[c + c * LDS];            // every thread reads the same pivot
+        if (!(d > (T)0) || !isfinite((double)d)) { fail = j0 + c + 1; break; }
+        if ((double)d < pm) pm = (double)d;
+        const T piv = sqrt(d);
+        __syncthreads();                       // all have read S(c,c) before it is overwritten
+        if (tid == 0) S[c + c * LDS] = piv;
+        for (int r = c + 1 + tid; r < nb; r += 256) S[r + c * LDS] /= piv;
+        __syncthreads();
+        for (int k = c + 1 + tx; k < nb; k += 16) {
+            const T lkc = S[k + c * LDS];
+            for (int r = k + ty; r < nb; r += 16) S[r + k * LDS] -= S[r + c * LDS] * lkc;
         }
         __syncthreads();
-        if (fail) break;
-        T lic = (T)0;
-        if (i > c && i < nb) {
-            lic = S[i + c * LDS] / S[c + c * LDS];
-            S[i + c * LDS] = lic;
-        }
-        __syncthreads();
-        if (i > c && i < nb)
-            for (int k = c + 1; k <= i; k++) S[i + k * LDS] -= lic * S[k + c * LDS];
     }
-    __syncthreads();
     if (fail) {
-        if (i == 0) atomicCAS(info, 0, fail);
+        if (tid == 0) atomicCAS(info, 0, fail);
         return;
     }
-    if (i == 0) atomicMin((unsigned long long *)pmin, (unsigned long long)__double_as_longlong(pm_s));
-    // X = L^-1 by forward substitution: row r of X needs rows < r (thread r computes row r
-    // after the rows above it): X(r, j) = (delta_rj - sum_{k<r} L(r,k) X(k,j)) / L(r,r).
-    // Column-oriented instead: for k = 0.., row k of X is final; rows below subtract L(r,k) X(k,:).
+    if (tid == 0) atomicMin((unsigned long long *)pmin, (unsigned long long)__double_as_longlong(pm));
     for (int k = 0; k < nb; k++) {
-        if (i == k) {
-            const T lkk = S[k + k * LDS];
-            for (int j = 0; j <= k; j++) X[k + j * LDS] /= lkk;
+        const T lkk = S[k + k * LDS];
+        for (int j = tid; j <= k; j += 256) X[k + j * LDS] /= lkk;
+        __syncthreads();
+        for (int j = tx; j <= k; j += 16) {
+            const T xkj = X[k + j * LDS];
+            for (int r = k + 1 + ty; r < nb; r += 16) X[r + j * LDS] -= S[r + k * LDS] * xkj;
         }
         __syncthreads();
-        if (i > k && i < nb) {
-            const T lik = S[i + k * LDS];
-            for (int j = 0; j <= k; j++) X[i + j * LDS] -= lik * X[k + j * LDS];
+    }
+    for (int c = ty; c < NB; c += 16)
+        for (int r = tx; r < NB; r += 16) {
+            if (r < nb && c < nb && r >= c) Ad[r + (long long)c * lda] = S[r + c * LDS];
+            // identity beyond nb so a partial last block acts as a full one in the solves
+            dinv[r + c * NB] = (r < nb && c < nb) ? ((r >= c) ? X[r + c * LDS] : (T)0) : (T)(r == c ? 1 : 0);
         }
-    }
-    __syncthreads();
-    for (int c = 0; c < NB; c++) {
-        if (i < nb && c < nb && i >= c) Ad[i + (long long)c * lda] = S[i + c * LDS];
-        // identity beyond nb so a partial last block acts as a full one in the solves
-        dinv[i + c * NB] = (i < nb && c < nb) ? ((i >= c) ? X[i + c * LDS] : (T)0) : (T)(i == c ? 1 : 0);
-    }
 }
 
 __global__ void init_info_kernel(int *info, double *pmin) {
@@ -343,7 +335,7 @@ int potrf_f64(cudaStream_t st, int n, double *A, long long lda, double *dinv, in
     BGPU_LAUNCH_CHECK();
     for (int j0 = 0; j0 < n; j0 += NB) {
         const int nb = (n - j0 < NB) ? n - j0 : NB;
-        potrf_diag_kernel<double><<<1, 64, 2 * NB * LDS * sizeof(double), st>>>(n, A, lda, j0, dinv + (size_t)(j0 / NB) * NB * NB, d_info, d_pmin);
+        potrf_diag_kernel<double><<<1, 256, 2 * NB * LDS * sizeof(double), st>>>(n, A, lda, j0, dinv + (size_t)(j0 / NB) * NB * NB, d_info, d_pmin);
         BGPU_LAUNCH_CHECK();
         const int rest = n - j0 - nb;
         if (rest <= 0) break;
@@ -366,7 +358,7 @@ int potrf_f32(cudaStream_t st, int n, float *A, long long lda, float *dinv, int 
     BGPU_LAUNCH_CHECK();
     for (int j0 = 0; j0 < n; j0 += NB) {
         const int nb = (n - j0 < NB) ? n - j0 : NB;
-        potrf_diag_kernel<float><<<1, 64, 2 * NB * LDS * sizeof(float), st>>>(n, A, lda, j0, dinv + (size_t)(j0 / NB) * NB * NB, d_info, d_pmin);
+        potrf_diag_kernel<float><<<1, 256, 2 * NB * LDS * sizeof(float), st>>>(n, A, lda, j0, dinv + (size_t)(j0 / NB) * NB * NB, d_info, d_pmin);
         BGPU_LAUNCH_CHECK();
         const int rest = n - j0 - nb;
         if (rest <= 0) break;

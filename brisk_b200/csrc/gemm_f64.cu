@@ -6,7 +6,8 @@
 // `lower` restricts the update to i >= j (a symmetric rank-k update of a lower triangle).
 // Batched over blockIdx.z with element strides sA, sB, sC.  C may alias A or B when every
 // CTA reads only the rows it writes (N <= 64 with A == C, or M <= 128 with B == C): all loads of
-// a tile complete before its epilogue stores.
+// a tile complete before its epilogue stores.  Tiles are 128 x BN with BN in {64, 80, 112, 128},
+// chosen per call to pad N least (N = 400 -> 80, N = 1000 -> 112).
 //
 // Used for: the row-product Schur GEMM G = X (A_a Z^-1) (FP64 mode), the trailing updates
 // of the blocked Cholesky of M and of X/Z, the HKM products Z^-1 dZ X, and the blocked
@@ -15,14 +16,19 @@
 #include "kernels.h"
 
 namespace {
-constexpr int BM = 128, BN = 64, BK = 16, STAGES = 3, NT = 256;
+constexpr int BM = 128, BK = 16, STAGES = 3, NT = 256;
 constexpr int LDA_M = BM + 8;   // smem stride for an MMAJOR A tile  [BK][BM+8]
 constexpr int LDA_K = BK + 4;   // smem stride for a  KMAJOR A tile  [BM][BK+4]
 constexpr int LDB_K = BK + 4;   // smem stride for a  KMAJOR B tile  [BN][BK+4]
-constexpr int LDB_N = BN + 8;   // smem stride for an NMAJOR B tile  [BK][BN+8]
 constexpr int A_STAGE = (BK * LDA_M > BM * LDA_K) ? BK * LDA_M : BM * LDA_K;
-constexpr int B_STAGE = (BN * LDB_K > BK * LDB_N) ? BN * LDB_K : BK * LDB_N;
-constexpr size_t SMEM_BYTES = (size_t)STAGES * (A_STAGE + B_STAGE) * sizeof(double);
+// the N tile (64, 80, 112 or 128 columns): the launcher picks the one that pads N least
+template <int BN>
+struct TileN {
+    static constexpr int LDB_N = BN + 8;   // smem stride for an NMAJOR B tile  [BK][BN+8]
+    static constexpr int B_STAGE = (BN * LDB_K > BK * LDB_N) ? BN * LDB_K : BK * LDB_N;
+    static constexpr int NT8 = BN / 16;     // n8 tiles per warp (warps are 4 x 2)
+    static constexpr size_t SMEM = (size_t)STAGES * (A_STAGE + B_STAGE) * sizeof(double);
+};
 
 __device__ __forceinline__ void dmma16(double (&c)[4], double a0, double a1, double b0) {
     asm volatile("mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};"
@@ -30,12 +36,13 @@ __device__ __forceinline__ void dmma16(double (&c)[4], double a0, double a1, dou
                  : "d"(a0), "d"(a1), "d"(b0));
 }
 
-template <bool A_KM, bool B_KM>
-__global__ void __launch_bounds__(NT) dgemm_kernel(int M, int N, int K, double alpha,
+template <bool A_KM, bool B_KM, int BN>
+__global__ void __launch_bounds__(NT, (BN <= 64) ? 2 : 1) dgemm_kernel(int M, int N, int K, double alpha,
                                                    const double *A, long long lda, long long sA,
                                                    const double *B, long long ldb, long long sB,
                                                    double beta, double *C, long long ldc, long long sC,
                                                    int lower) {
+    constexpr int LDB_N = TileN<BN>::LDB_N, B_STAGE = TileN<BN>::B_STAGE, NT8 = TileN<BN>::NT8;
     extern __shared__ __align__(16) double smem[];
     double *As = smem;
     double *Bs = smem + STAGES * A_STAGE;
@@ -45,7 +52,7 @@ __global__ void __launch_bounds__(NT) dgemm_kernel(int M, int N, int K, double a
     B += (long long)blockIdx.z * sB;
     C += (long long)blockIdx.z * sC;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int wm = warp & 3, wn = warp >> 2;          // 4 x 2 warps, 32 x 32 each
+    const int wm = warp & 3, wn = warp >> 2;          // 4 x 2 warps, 32 x BN/2 each
     const int g = lane >> 2, tig = lane & 3;
     const int nk = (K + BK - 1) / BK;
 
@@ -85,11 +92,11 @@ __global__ void __launch_bounds__(NT) dgemm_kernel(int M, int N, int K, double a
         }
     };
 
-    double acc[2][4][4];
+    double acc[2][NT8][4];
 #pragma unroll
     for (int a = 0; a < 2; a++)
 #pragma unroll
-        for (int b = 0; b < 4; b++)
+        for (int b = 0; b < NT8; b++)
 #pragma unroll
             for (int c = 0; c < 4; c++) acc[a][b][c] = 0.0;
 
@@ -111,7 +118,7 @@ __global__ void __launch_bounds__(NT) dgemm_kernel(int M, int N, int K, double a
 #pragma unroll
         for (int kk = 0; kk < BK / 4; kk++) {
             const int k = kk * 4 + tig;
-            double af[2][2], bf[4];
+            double af[2][2], bf[NT8];
 #pragma unroll
             for (int mt = 0; mt < 2; mt++) {
                 const int r = wm * 32 + mt * 16 + g;
@@ -119,14 +126,14 @@ __global__ void __launch_bounds__(NT) dgemm_kernel(int M, int N, int K, double a
                 else      { af[mt][0] = as[k * LDA_M + r]; af[mt][1] = as[k * LDA_M + r + 8]; }
             }
 #pragma unroll
-            for (int nt = 0; nt < 4; nt++) {
-                const int c = wn * 32 + nt * 8 + g;
+            for (int nt = 0; nt < NT8; nt++) {
+                const int c = wn * (BN / 2) + nt * 8 + g;
                 bf[nt] = B_KM ? bs[c * LDB_K + k] : bs[k * LDB_N + c];
             }
 #pragma unroll
             for (int mt = 0; mt < 2; mt++)
 #pragma unroll
-                for (int nt = 0; nt < 4; nt++) dmma16(acc[mt][nt], af[mt][0], af[mt][1], bf[nt]);
+                for (int nt = 0; nt < NT8; nt++) dmma16(acc[mt][nt], af[mt][0], af[mt][1], bf[nt]);
         }
     }
     cp_async_wait<0>();
@@ -134,11 +141,11 @@ __global__ void __launch_bounds__(NT) dgemm_kernel(int M, int N, int K, double a
 #pragma unroll
     for (int mt = 0; mt < 2; mt++)
 #pragma unroll
-        for (int nt = 0; nt < 4; nt++)
+        for (int nt = 0; nt < NT8; nt++)
 #pragma unroll
             for (int q = 0; q < 4; q++) {
                 const int i = i0 + wm * 32 + mt * 16 + g + (q >> 1) * 8;
-                const int j = j0 + wn * 32 + nt * 8 + 2 * tig + (q & 1);
+                const int j = j0 + wn * (BN / 2) + nt * 8 + 2 * tig + (q & 1);
                 if (i < M && j < N && (!lower || i >= j)) {
                     double *p = C + (long long)i + (long long)j * ldc;
                     const double v = alpha * acc[mt][nt][q];
@@ -147,21 +154,41 @@ __global__ void __launch_bounds__(NT) dgemm_kernel(int M, int N, int K, double a
             }
 }
 
-template <bool A_KM, bool B_KM>
+template <bool A_KM, bool B_KM, int BN>
 int launch(cudaStream_t st, int M, int N, int K, double alpha, const double *A, long long lda, long long sA,
            const double *B, long long ldb, long long sB, double beta, double *C, long long ldc, long long sC,
            int batch, int lower) {
     static bool attr_set = false;
     if (!attr_set) {
-        BGPU_CHECK(cudaFuncSetAttribute(dgemm_kernel<A_KM, B_KM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)SMEM_BYTES));
+        BGPU_CHECK(cudaFuncSetAttribute(dgemm_kernel<A_KM, B_KM, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)TileN<BN>::SMEM));
         attr_set = true;
     }
     dim3 grid(ceil_div(M, BM), ceil_div(N, BN), batch);
-    dgemm_kernel<A_KM, B_KM><<<grid, NT, SMEM_BYTES, st>>>(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc,
-                                                           sC, lower);
+    dgemm_kernel<A_KM, B_KM, BN><<<grid, NT, TileN<BN>::SMEM, st>>>(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C,
+                                                                    ldc, sC, lower);
     BGPU_LAUNCH_CHECK();
     return BGPU_OK;
+}
+
+template <bool A_KM, bool B_KM>
+int launch_bn(cudaStream_t st, int M, int N, int K, double alpha, const double *A, long long lda, long long sA,
+              const double *B, long long ldb, long long sB, double beta, double *C, long long ldc, long long sC,
+              int batch, int lower) {
+    // the N tile that pads N least (ties to the wider); N <= 64 always takes 64
+    const int cand[4] = {128, 112, 80, 64};
+    int best = 64;
+    long long pad = 1LL << 60;
+    for (int c : cand) {
+        const long long p = (long long)ceil_div(N, c) * c;
+        if (p < pad) { pad = p; best = c; }
+    }
+    switch (best) {
+        case 128: return launch<A_KM, B_KM, 128>(st, M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, batch, lower);
+        case 112: return launch<A_KM, B_KM, 112>(st, M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, batch, lower);
+        case 80: return launch<A_KM, B_KM, 80>(st, M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, batch, lower);
+        default: return launch<A_KM, B_KM, 64>(st, M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, batch, lower);
+    }
 }
 }  // namespace
 
@@ -174,11 +201,11 @@ int gemm_f64(cudaStream_t st, int a_kmajor, int b_kmajor, int M, int N, int K, d
         return scale_matrix_f64(st, M, N, beta, C, ldc, sC, batch, lower);
     }
     if (a_kmajor) {
-        if (b_kmajor) return launch<true, true>(st, M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, batch, lower);
-        return launch<true, false>(st, M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, batch, lower);
+        if (b_kmajor) return launch_bn<true, true>(st, M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, batch, lower);
+        return launch_bn<true, false>(st, M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, batch, lower);
     }
-    if (b_kmajor) return launch<false, true>(st, M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, batch, lower);
-    return launch<false, false>(st, M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, batch, lower);
+    if (b_kmajor) return launch_bn<false, true>(st, M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, batch, lower);
+    return launch_bn<false, false>(st, M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, batch, lower);
 }
 
 namespace {

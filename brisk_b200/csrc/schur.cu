@@ -72,28 +72,29 @@ __global__ void __launch_bounds__(256) tprod_kernel(int n, int ldt, int K, int a
     }
 }
 
-// One warp group of LPG lanes per constraint b; each lane holds K / LPG of the chunk's K columns.
+// One CTA of GW warps per constraint b (b >= a0): warp w sums a fixed slice of b's entries
+// with LPG lanes per entry group, each lane holding K / LPG of the chunk's K columns; the slices
+// are added in warp order (a fixed order: the same bits on every run).
+constexpr int GW = 8;
 template <int K, typename GT>
-__global__ void __launch_bounds__(256) gather_kernel(int a0, int ncon, int m, const int *__restrict__ con,
-                                                    const long long *__restrict__ cptr, const int *__restrict__ cpos,
-                                                    const double *__restrict__ cval, const GT *__restrict__ G,
-                                                    double *M) {
-    constexpr int LPG = K < 32 ? K : 32;       // lanes per constraint group
-    constexpr int GPW = 32 / LPG;              // groups per warp (entry split)
+__global__ void __launch_bounds__(GW * 32) gather_kernel(int a0, int ncon, int m, const int *__restrict__ con,
+                                                        const long long *__restrict__ cptr, const int *__restrict__ cpos,
+                                                        const double *__restrict__ cval, const GT *__restrict__ G,
+                                                        double *M) {
+    constexpr int LPG = K < 32 ? K : 32;       // lanes per entry group
+    constexpr int GPW = 32 / LPG;              // entry groups per warp
     constexpr int PER = K / LPG;               // columns per lane
-    const int lane = threadIdx.x & 31;
-    const int b = a0 + blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    __shared__ double part[GW][K];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int b = a0 + blockIdx.x;
     if (b >= ncon) return;
     const int sub = lane / LPG, l = lane % LPG;
-    double acc[PER];
+    double acc[PER], acc2[PER];
 #pragma unroll
-    for (int u = 0; u < PER; u++) acc[u] = 0.0;
-    const long long s = cptr[b], e = cptr[b + 1];
-    // two accumulators per column (even and odd entry slots) break the FMA chain; full 32-entry
-    // groups run fully unrolled so their G loads are all in flight together
-    double acc2[PER];
-#pragma unroll
-    for (int u = 0; u < PER; u++) acc2[u] = 0.0;
+    for (int u = 0; u < PER; u++) acc[u] = acc2[u] = 0.0;
+    const long long s0 = cptr[b], e0 = cptr[b + 1];
+    const long long len = e0 - s0, per_w = (len + GW - 1) / GW;
+    const long long s = s0 + warp * per_w, e = min(e0, s + per_w);
     long long base = s;
     for (; base + 32 <= e; base += 32) {
         const int pos = cpos[base + lane];
@@ -113,7 +114,7 @@ __global__ void __launch_bounds__(256) gather_kernel(int a0, int ncon, int m, co
             }
         }
     }
-    if (base < e) {   // the ragged last group
+    if (base < e) {   // the ragged last group of the slice
         const long long my = base + lane;
         int pos = 0;
         double v = 0.0;
@@ -132,20 +133,25 @@ __global__ void __launch_bounds__(256) gather_kernel(int a0, int ncon, int m, co
         }
     }
 #pragma unroll
-    for (int u = 0; u < PER; u++) acc[u] += acc2[u];
-#pragma unroll
-    for (int u = 0; u < PER; u++)
+    for (int u = 0; u < PER; u++) {
+        acc[u] += acc2[u];
 #pragma unroll
         for (int o = LPG; o < 32; o <<= 1) acc[u] += __shfl_xor_sync(0xffffffffu, acc[u], o);
-    if (sub != 0) return;
-    const int cb = con[b];
+    }
+    if (sub == 0)
 #pragma unroll
-    for (int u = 0; u < PER; u++) {
-        const int a = a0 + l + u * LPG;
+        for (int u = 0; u < PER; u++) part[warp][l + u * LPG] = acc[u];
+    __syncthreads();
+    if (threadIdx.x < K) {
+        const int t = threadIdx.x;
+        double v = 0.0;
+#pragma unroll
+        for (int w = 0; w < GW; w++) v += part[w][t];
+        const int a = a0 + t;
         if (a < ncon && a <= b) {
-            const int ca = con[a];
-            M[(long long)ca + (long long)cb * m] += acc[u];
-            if (ca != cb) M[(long long)cb + (long long)ca * m] += acc[u];
+            const int ca = con[a], cb = con[b];
+            M[(long long)ca + (long long)cb * m] += v;
+            if (ca != cb) M[(long long)cb + (long long)ca * m] += v;
         }
     }
 }
@@ -154,12 +160,12 @@ template <typename GT>
 int gather_launch(cudaStream_t st, int K, int a0, int ncon, int m, const DevBlock &B, const GT *G, double *M) {
     const int nb = ncon - a0;
     if (nb <= 0) return BGPU_OK;
-    dim3 grid(ceil_div(nb, 8));
+    dim3 grid(nb);
     switch (K) {
-        case 8: gather_kernel<8, GT><<<grid, 256, 0, st>>>(a0, ncon, m, B.con, B.cptr, B.cpos, B.cval, G, M); break;
-        case 16: gather_kernel<16, GT><<<grid, 256, 0, st>>>(a0, ncon, m, B.con, B.cptr, B.cpos, B.cval, G, M); break;
-        case 32: gather_kernel<32, GT><<<grid, 256, 0, st>>>(a0, ncon, m, B.con, B.cptr, B.cpos, B.cval, G, M); break;
-        case 64: gather_kernel<64, GT><<<grid, 256, 0, st>>>(a0, ncon, m, B.con, B.cptr, B.cpos, B.cval, G, M); break;
+        case 8: gather_kernel<8, GT><<<grid, GW * 32, 0, st>>>(a0, ncon, m, B.con, B.cptr, B.cpos, B.cval, G, M); break;
+        case 16: gather_kernel<16, GT><<<grid, GW * 32, 0, st>>>(a0, ncon, m, B.con, B.cptr, B.cpos, B.cval, G, M); break;
+        case 32: gather_kernel<32, GT><<<grid, GW * 32, 0, st>>>(a0, ncon, m, B.con, B.cptr, B.cpos, B.cval, G, M); break;
+        case 64: gather_kernel<64, GT><<<grid, GW * 32, 0, st>>>(a0, ncon, m, B.con, B.cptr, B.cpos, B.cval, G, M); break;
         default: return BGPU_ERR_ARG;
     }
     BGPU_LAUNCH_CHECK();

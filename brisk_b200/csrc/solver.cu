@@ -20,6 +20,7 @@
 #include "common.cuh"
 #include "elementwise.h"
 #include "kernels.h"
+#include "small.h"
 #include "solver.h"
 #include "tf32x3.h"
 
@@ -333,6 +334,8 @@ class Solver {
         if (evs0) cudaEventDestroy(evs0);
         if (evs1) cudaEventDestroy(evs1);
         if (h_dots) cudaFreeHost(h_dots);
+        if (h_sinfo) cudaFreeHost(h_sinfo);
+        if (h_slam) cudaFreeHost(h_slam);
     }
     double upload_bytes = 0;
 
@@ -355,6 +358,15 @@ class Solver {
     double *h_dots = nullptr;                     // pinned
     void *ws = nullptr;
     size_t ws_bytes = 0;
+    // blocks of order <= SMALL_N_MAX run through the batched one-CTA-per-block kernels (small.cu)
+    std::vector<int> small_ids, big_ids;
+    int *d_sns = nullptr, *d_sinfo = nullptr, *h_sinfo = nullptr;
+    double *d_slam = nullptr, *h_slam = nullptr;
+    std::vector<std::pair<double *DevArrays::*, double **>> stab;   // device pointer tables per array kind
+    double **tab(double *DevArrays::*mem);
+    // C = alpha A B (column-major n x n) on every block: per-block DMMA GEMMs for the large
+    // blocks, one batched launch for the small ones
+    void mul_all(double alpha, double *DevArrays::*A, double *DevArrays::*B, double *DevArrays::*C);
     int chunk = 32, chunk64 = 32, asm_prec = 0;
     int chunk_fp64(int) const { return chunk64; }
     int epoch = 0;
@@ -490,6 +502,19 @@ void Solver::setup() {
         upload_block(k);
         nmax = std::max(nmax, P.blk[k].n);
     }
+    for (int k = 0; k < nb; k++) (P.blk[k].n <= SMALL_N_MAX ? small_ids : big_ids).push_back(k);
+    if (!small_ids.empty()) {
+        const int ns = (int)small_ids.size();
+        std::vector<int> nsz(ns);
+        for (int i = 0; i < ns; i++) nsz[i] = P.blk[small_ids[i]].n;
+        d_sns = g.alloc<int>(ns);
+        d_sinfo = g.alloc<int>(ns);
+        d_slam = g.alloc<double>(ns);
+        if (!d_sns || !d_sinfo || !d_slam) throw GpuFail{BGPU_ERR_NOMEM, __LINE__};
+        CU(cudaMemcpy(d_sns, nsz.data(), sizeof(int) * ns, cudaMemcpyHostToDevice));
+        CU(cudaMallocHost(&h_sinfo, sizeof(int) * ns));
+        CU(cudaMallocHost(&h_slam, sizeof(double) * ns));
+    }
     const size_t mm = (size_t)m * m;
     M = g.alloc<double>(mm);
     if (!M) throw GpuFail{BGPU_ERR_NOMEM, __LINE__};
@@ -551,6 +576,25 @@ int Solver::chol(int n, double *L, double *dinv) {
 }
 
 void Solver::inv_from_chol(int n, const double *L, const double *dinv, double *Li) { RC(trtri_f64(g.st, n, L, n, dinv, Li, n)); }
+
+double **Solver::tab(double *DevArrays::*mem) {
+    for (auto &e : stab)
+        if (e.first == mem) return e.second;
+    std::vector<double *> ptrs;
+    for (int k : small_ids) ptrs.push_back(da[k].*mem);
+    double **d = g.alloc<double *>(ptrs.size());
+    if (!d) throw GpuFail{BGPU_ERR_NOMEM, __LINE__};
+    CU(cudaMemcpy(d, ptrs.data(), sizeof(double *) * ptrs.size(), cudaMemcpyHostToDevice));
+    stab.push_back({mem, d});
+    return d;
+}
+
+void Solver::mul_all(double alpha, double *DevArrays::*A, double *DevArrays::*B, double *DevArrays::*C) {
+    for (int k : big_ids) mul(db[k].n, alpha, da[k].*A, da[k].*B, da[k].*C);
+    if (!small_ids.empty())
+        RC(small_gemm(g.st, (int)small_ids.size(), d_sns, 0, 0, alpha, (const double *const *)tab(A),
+                      (const double *const *)tab(B), 0.0, tab(C), 0));
+}
 
 void Solver::zinv(int k) {
     // Zi = LZ^-T LZ^-1 (LZ and dinvZ from the last Cholesky of Z)
@@ -680,13 +724,11 @@ void Solver::schur_mv(const std::vector<double> &x, std::vector<double> &y) {
 void Solver::newton_mv(const std::vector<double> &x, std::vector<double> &y) {
     std::vector<double *> Fs(nb);
     for (int k = 0; k < nb; k++) {
-        const int n = db[k].n;
-        DevArrays &d = da[k];
-        atop_block(k, x, 1.0, 0.0, d.W);   // A'(x)
-        mul(n, 1.0, d.Zi, d.W, d.T);
-        mul(n, 1.0, d.T, d.X, d.F);        // Z^-1 A'(x) X
-        Fs[k] = d.F;
+        atop_block(k, x, 1.0, 0.0, da[k].W);   // A'(x)
+        Fs[k] = da[k].F;
     }
+    mul_all(1.0, &DevArrays::Zi, &DevArrays::W, &DevArrays::T);
+    mul_all(1.0, &DevArrays::T, &DevArrays::X, &DevArrays::F);   // Z^-1 A'(x) X
     aop_all(Fs, y);
 }
 
@@ -809,7 +851,7 @@ double Solver::lanczos(int n, const double *Bm, int Kmax) {
 // maxstep (solver.c:6300-6390): the largest alpha with V + alpha dV >= 0 over all blocks
 double Solver::maxstep(int primal, int K) {
     double a = 1e30;
-    for (int k = 0; k < nb; k++) {
+    for (int k : big_ids) {
         const int n = db[k].n;
         DevArrays &d = da[k];
         const double *Li = primal ? d.LiX : d.LiZ;
@@ -825,24 +867,48 @@ double Solver::maxstep(int primal, int K) {
         if (!std::isfinite(ak) && !(ak > 0)) ak = 0.0;
         if (ak < a) a = ak;
     }
+    if (!small_ids.empty()) {   // exact lambda_min per small block, one launch (small_lammin, solver.c:5947)
+        const int ns = (int)small_ids.size();
+        RC(small_lammin(g.st, ns, d_sns, (const double *const *)tab(primal ? &DevArrays::LiX : &DevArrays::LiZ),
+                        (const double *const *)tab(primal ? &DevArrays::dX : &DevArrays::dZ), d_slam));
+        CU(cudaMemcpyAsync(h_slam, d_slam, sizeof(double) * ns, cudaMemcpyDeviceToHost, g.st));
+        CU(cudaStreamSynchronize(g.st));
+        for (int i = 0; i < ns; i++) {
+            const double lam = h_slam[i];
+            double ak = (lam <= -1e299) ? 0.0 : (lam >= 0 ? 1e30 : -1.0 / lam);
+            if (!std::isfinite(ak) && !(ak > 0)) ak = 0.0;
+            if (ak < a) a = ak;
+        }
+    }
     return a;
 }
 
 // try_step (solver.c:6393-6447): V += alpha dV with a Cholesky test, alpha *= 0.8 on failure
 int Solver::try_step(int primal, double *alpha) {
     double a = *alpha;
-    std::vector<double> stepped(nb, 0.0);
+    double stepped = 0.0;   // all blocks stay at the same step
+    const int ns = (int)small_ids.size();
     for (int tries = 0; tries < 40; tries++) {
         bool ok = true;
-        for (int k = 0; k < nb; k++) {
+        const double inc = a - stepped;
+        stepped = a;
+        for (int k : big_ids) {
             const int n = db[k].n;
             DevArrays &d = da[k];
             double *V = primal ? d.X : d.Z, *dV = primal ? d.dX : d.dZ, *L = primal ? d.LX : d.LZ;
             double *dinv = primal ? d.dinvX : d.dinvZ;
-            const double inc = a - stepped[k];
-            stepped[k] = a;
             RC(ew_step_copy(g.st, (long long)n * n, inc, dV, V, L));
             if (chol(n, L, dinv) != 0) ok = false;
+        }
+        if (ns > 0) {
+            double **V = tab(primal ? &DevArrays::X : &DevArrays::Z), **L = tab(primal ? &DevArrays::LX : &DevArrays::LZ);
+            RC(small_step_copy(g.st, ns, d_sns, inc, (const double *const *)tab(primal ? &DevArrays::dX : &DevArrays::dZ),
+                               V, L));
+            RC(small_chol_inv(g.st, ns, d_sns, L, L, tab(primal ? &DevArrays::LiX : &DevArrays::LiZ), d_sinfo));
+            CU(cudaMemcpyAsync(h_sinfo, d_sinfo, sizeof(int) * ns, cudaMemcpyDeviceToHost, g.st));
+            CU(cudaStreamSynchronize(g.st));
+            for (int i = 0; i < ns; i++)
+                if (h_sinfo[i]) ok = false;
         }
         if (ok) {
             *alpha = a;
@@ -911,6 +977,7 @@ void Solver::least_squares_start(std::vector<double> &y) {
             if (extra > 1e30) throw GpuFail{BGPU_ERR_NOTPD, __LINE__};
         }
         inv_from_chol(n, d.LX, d.dinvX, d.LiX);
+        inv_from_chol(n, d.LZ, d.dinvZ, d.LiZ);   // the small blocks' Z^-1 comes from LiZ
     }
     // the factor state starts afresh for the loop
     want_double = is_float = reg_hint = false;
@@ -1036,6 +1103,7 @@ int Solver::run(ResultData &res) {
         RC(ew_set_scaled_identity(g.st, n, d.T, eta));
         if (chol(n, d.T, d.dinvZ)) throw GpuFail{BGPU_ERR_NOTPD, __LINE__};
         inv_from_chol(n, d.LX, d.dinvX, d.LiX);
+        inv_from_chol(n, d.LZ, d.dinvZ, d.LiZ);   // the small blocks' Z^-1 comes from LiZ
     }
     if (opt.init >= 1 && m > 0) least_squares_start(y);
     // R0 = C - Z - A'y, theta = 1 (solver.c:14317-14326)
@@ -1060,7 +1128,10 @@ int Solver::run(ResultData &res) {
         log_printf(0, " it   pobj            dobj            pinf     dinf     gap      mu       alp   ald   sigma  time\n");
     for (it = 0; it <= opt.maxit; it++) {
         double td = wtime();
-        for (int k = 0; k < nb; k++) zinv(k);
+        for (int k : big_ids) zinv(k);
+        if (!small_ids.empty())   // Zi = LiZ' LiZ (symmetric part), LiZ from the last small Cholesky of Z
+            RC(small_gemm(g.st, (int)small_ids.size(), d_sns, 1, 0, 1.0, (const double *const *)tab(&DevArrays::LiZ),
+                          (const double *const *)tab(&DevArrays::LiZ), 0.0, tab(&DevArrays::Zi), 1));
         // residuals and objectives
         std::vector<double *> Xs(nb);
         for (int k = 0; k < nb; k++) Xs[k] = da[k].X;
@@ -1158,13 +1229,9 @@ int Solver::run(ResultData &res) {
             for (int k = 0; k < nb; k++) Zis[k] = da[k].Zi;
             aop_all(Zis, a0);
             if (hasH) {
-                for (int k = 0; k < nb; k++) {
-                    const int n = db[k].n;
-                    DevArrays &d = da[k];
-                    mul(n, theta, d.Zi, d.R0, d.T);   // theta Zi R0
-                    mul(n, 1.0, d.T, d.X, d.G);       // theta Zi R0 X
-                    Gs[k] = d.G;
-                }
+                mul_all(theta, &DevArrays::Zi, &DevArrays::R0, &DevArrays::T);   // theta Zi R0
+                mul_all(1.0, &DevArrays::T, &DevArrays::X, &DevArrays::G);       // theta Zi R0 X
+                for (int k = 0; k < nb; k++) Gs[k] = da[k].G;
                 aop_all(Gs, h);
             } else h.assign(m, 0.0);
         }
@@ -1176,15 +1243,14 @@ int Solver::run(ResultData &res) {
         tm.chol += wtime() - tc;
         td = wtime();
         for (int k = 0; k < nb; k++) {
-            const int n = db[k].n;
-            const long long nn = (long long)n * n;
-            DevArrays &d = da[k];
-            atop_block(k, dy, -1.0, 0.0, d.dZ);
-            RC(ew_lincomb(g.st, nn, 1.0, d.dZ, theta, d.R0, 0.0, nullptr, d.dZ));   // dZ = -A'dy + theta R0
-            mul(n, 1.0, d.Zi, d.dZ, d.T);
-            mul(n, 1.0, d.T, d.X, d.G);                                            // Zi dZ X
-            RC(ew_sym_lincomb(g.st, n, d.G, -1.0, -1.0, d.X, 0.0, nullptr, d.dX)); // dX = -sym(G) - X
+            const long long nn = (long long)db[k].n * db[k].n;
+            atop_block(k, dy, -1.0, 0.0, da[k].dZ);
+            RC(ew_lincomb(g.st, nn, 1.0, da[k].dZ, theta, da[k].R0, 0.0, nullptr, da[k].dZ));   // dZ = -A'dy + theta R0
         }
+        mul_all(1.0, &DevArrays::Zi, &DevArrays::dZ, &DevArrays::T);
+        mul_all(1.0, &DevArrays::T, &DevArrays::X, &DevArrays::G);                                 // Zi dZ X
+        for (int k = 0; k < nb; k++)
+            RC(ew_sym_lincomb(g.st, db[k].n, da[k].G, -1.0, -1.0, da[k].X, 0.0, nullptr, da[k].dX)); // dX = -sym(G) - X
         tm.dense += wtime() - td;
         double tst = wtime();
         const double ap = std::min(1.0, maxstep(1, opt.lanczos_k));
@@ -1221,13 +1287,9 @@ int Solver::run(ResultData &res) {
         td = wtime();
         {
             std::vector<double *> Qs(nb);
-            for (int k = 0; k < nb; k++) {
-                const int n = db[k].n;
-                DevArrays &d = da[k];
-                mul(n, 1.0, d.Zi, d.dZ, d.T);
-                mul(n, 1.0, d.T, d.dX, d.Q);   // Q = Zi dZp dXp
-                Qs[k] = d.Q;
-            }
+            mul_all(1.0, &DevArrays::Zi, &DevArrays::dZ, &DevArrays::T);
+            mul_all(1.0, &DevArrays::T, &DevArrays::dX, &DevArrays::Q);   // Q = Zi dZp dXp
+            for (int k = 0; k < nb; k++) Qs[k] = da[k].Q;
             aop_all(Qs, qv);
         }
         for (int i = 0; i < m; i++) rhs[i] = P.b[i] - smu * a0[i] + qv[i] + h[i];
@@ -1237,13 +1299,16 @@ int Solver::run(ResultData &res) {
         tm.chol += wtime() - tc;
         td = wtime();
         for (int k = 0; k < nb; k++) {
+            const long long nn = (long long)db[k].n * db[k].n;
+            atop_block(k, dy, -1.0, 0.0, da[k].dZ);
+            RC(ew_lincomb(g.st, nn, 1.0, da[k].dZ, theta, da[k].R0, 0.0, nullptr, da[k].dZ));
+        }
+        mul_all(1.0, &DevArrays::Zi, &DevArrays::dZ, &DevArrays::T);
+        mul_all(1.0, &DevArrays::T, &DevArrays::X, &DevArrays::G);
+        for (int k = 0; k < nb; k++) {
             const int n = db[k].n;
             const long long nn = (long long)n * n;
             DevArrays &d = da[k];
-            atop_block(k, dy, -1.0, 0.0, d.dZ);
-            RC(ew_lincomb(g.st, nn, 1.0, d.dZ, theta, d.R0, 0.0, nullptr, d.dZ));
-            mul(n, 1.0, d.Zi, d.dZ, d.T);
-            mul(n, 1.0, d.T, d.X, d.G);
             RC(ew_lincomb(g.st, nn, 1.0, d.G, 1.0, d.Q, 0.0, nullptr, d.G));          // Zi dZ X + Q
             RC(ew_sym_lincomb(g.st, n, d.G, -1.0, smu, d.Zi, -1.0, d.X, d.dX));      // -sym(.) + smu Zi - X
         }
@@ -1264,14 +1329,12 @@ int Solver::run(ResultData &res) {
             tm.chol += wtime() - tc;
             td = wtime();
             std::vector<double *> Gs(nb);
+            for (int k = 0; k < nb; k++) atop_block(k, wv, 1.0, 0.0, da[k].W);   // A'w
+            mul_all(1.0, &DevArrays::Zi, &DevArrays::W, &DevArrays::T);
+            mul_all(1.0, &DevArrays::T, &DevArrays::X, &DevArrays::F);           // Zi A'w X  (F is free here)
             for (int k = 0; k < nb; k++) {
-                const int n = db[k].n;
-                DevArrays &d = da[k];
-                atop_block(k, wv, 1.0, 0.0, d.W);            // A'w
-                mul(n, 1.0, d.Zi, d.W, d.T);
-                mul(n, 1.0, d.T, d.X, d.F);                  // Zi A'w X  (F is free here)
-                RC(ew_sym_lincomb(g.st, n, d.F, 1.0, 0.0, nullptr, 0.0, nullptr, d.G));
-                Gs[k] = d.G;
+                RC(ew_sym_lincomb(g.st, db[k].n, da[k].F, 1.0, 0.0, nullptr, 0.0, nullptr, da[k].G));
+                Gs[k] = da[k].G;
             }
             std::vector<double> AG;
             aop_all(Gs, AG);
@@ -1312,7 +1375,7 @@ int Solver::run(ResultData &res) {
         tst = wtime();
         const int okp = try_step(1, &apn);
         const int okd = try_step(0, &adn);
-        for (int k = 0; k < nb; k++) inv_from_chol(db[k].n, da[k].LX, da[k].dinvX, da[k].LiX);
+        for (int k : big_ids) inv_from_chol(db[k].n, da[k].LX, da[k].dinvX, da[k].LiX);
         tm.step += wtime() - tst;
         if (!okp || !okd) { status = 4; break; }
         for (int i = 0; i < m; i++) y[i] += adn * dy[i];

@@ -249,3 +249,74 @@ def workload(name: str, **over) -> SdpaData:
     kw = dict(w["kw"])
     kw.update(over)
     return w["fn"](**kw)
+
+
+def _monomials_upto(vars_, deg):
+    """Monomials of degree <= deg in the given variables, as sorted tuples (graded order)."""
+    out = [()]
+    frontier = [()]
+    for _ in range(deg):
+        nxt = []
+        for mono in frontier:
+            start = vars_.index(mono[-1]) if mono else 0
+            for v in vars_[start:]:
+                nxt.append(mono + (v,))
+        out.extend(nxt)
+        frontier = nxt
+    return out
+
+
+def moment_relaxation(nvars: int = 60, clique: int = 4, seed: int = 0) -> SdpaData:
+    """Degree-2 (order-2) sparse moment relaxation of a seeded random quartic with chain cliques.
+
+    f(x) = sum of c_alpha x^alpha over every monomial of degree <= 4 supported on one of the
+    cliques {i, ..., i+clique-1} (i = 0..nvars-clique), c_alpha ~ N(0,1), except that each x_i^4
+    gets 1 + the sum of |c| of the other quartic monomials containing x_i, so f is bounded
+    below and the relaxation has an optimum.  The relaxation
+    min sum c_alpha y_alpha  s.t.  M_2(y, I_k) >= 0 for every clique, y_0 = 1
+    has one moment block per clique, indexed by the monomials of degree <= 2 in its variables
+    (15 x 15 for cliques of 4), and one free moment y_alpha per monomial alpha != 0.  In BRISK's
+    form max b'y s.t. C - sum y_i A_i = Z >= 0: C = B_0, A_i = -B_alpha_i, b_i = -c_alpha_i, where
+    B_alpha has a 1 at (u, v) of block k whenever u + v = alpha.  The optimal value is
+    c_0 - (the SDP's b'y)."""
+    rng = np.random.default_rng(seed)
+    cliques = [tuple(range(i, i + clique)) for i in range(nvars - clique + 1)]
+    index = {}
+
+    def mono_id(mono):
+        if mono not in index:
+            index[mono] = len(index)
+        return index[mono]
+
+    mono_id(())
+    for cl in cliques:
+        for mono in _monomials_upto(list(cl), 4):
+            mono_id(mono)
+    coef = rng.standard_normal(len(index))
+    # bounded below: each x_i^4 gets 1 + the absolute sum of the other quartic coefficients
+    # whose monomial contains x_i (the random quartic would otherwise be unbounded)
+    for mono, t in index.items():
+        if len(mono) == 4 and len(set(mono)) == 1:
+            i = mono[0]
+            coef[t] = 1.0 + sum(abs(coef[u]) for mo, u in index.items()
+                                if len(mo) == 4 and i in mo and len(set(mo)) > 1)
+    m = len(index) - 1                        # every moment but y_0
+    mats, blks, ii, jj, vv = [], [], [], [], []
+    for k, cl in enumerate(cliques):
+        basis = _monomials_upto(list(cl), 2)
+        for a in range(len(basis)):
+            for b in range(a, len(basis)):
+                alpha = tuple(sorted(basis[a] + basis[b]))
+                t = index[alpha]
+                # F0 = -C = -B_0 at t = 0; F_t = A_t = -B_alpha otherwise
+                mats.append(t)
+                blks.append(k + 1)
+                ii.append(a + 1)
+                jj.append(b + 1)
+                vv.append(-1.0)
+    c = -coef[1:]
+    d = _normalise(np.array(mats), np.array(blks), np.array(ii), np.array(jj), np.array(vv))
+    nb = len(cliques)
+    bsz = len(_monomials_upto(list(cliques[0]), 2))
+    return SdpaData(np.full(nb, bsz, np.int32), c, *d, name=f"moment_chain_n{nvars}_c{clique}_seed{seed}",
+                    meta=dict(kind="moment", nvars=nvars, clique=clique, seed=seed, offset=float(coef[0]), m=m))

@@ -46,6 +46,9 @@ def lib():
         "bgpu_split_tf32": ([I64, P, P, P, P], I),
         "bgpu_symv": ([I, D, P, I, P, D, P, P], I),
         "bgpu_aop": ([I, I, P, P, P, P, P, D, D, P, P], I),
+        "bgpu_small_chol_inv": ([I, P, P, P, P, P, P], I),
+        "bgpu_small_lammin": ([I, P, P, P, P, P], I),
+        "bgpu_small_gemm": ([I, P, I, I, D, P, P, D, P, I, P], I),
     }
     for name, (args, res) in sigs.items():
         f = getattr(L, name)

@@ -121,6 +121,18 @@ BGPU_API int bgpu_gemm_tf32x3(int M, int N, int K, const float *d_Ah, const floa
                               void *stream);
 BGPU_API int bgpu_split_tf32(int64_t n, const double *d_x, float *d_hi, float *d_lo, void *stream);
 
+/* Batched small blocks (order n[k] <= 64, one CTA each; d_* arrays of nb device pointers to
+ * n x n column-major matrices).  bgpu_small_chol_inv: L = chol(A), Li = L^-1 (lower), info[k]
+ * the first failing column or 0 (chol_lower, solver.c:679).  bgpu_small_lammin: lam[k] =
+ * lambda_min(Li D Li') by Householder tridiagonalization and Sturm bisection (small_lammin,
+ * solver.c:5947-6027).  bgpu_small_gemm: C = alpha op(A) op(B) + beta C, or its symmetric part. */
+BGPU_API int bgpu_small_chol_inv(int nb, const int *d_n, double *const *d_A, double *const *d_L,
+                                 double *const *d_Li, int *d_info, void *stream);
+BGPU_API int bgpu_small_lammin(int nb, const int *d_n, const double *const *d_Li, const double *const *d_D,
+                               double *d_lam, void *stream);
+BGPU_API int bgpu_small_gemm(int nb, const int *d_n, int ta, int tb, double alpha, const double *const *d_A,
+                             const double *const *d_B, double beta, double *const *d_C, int sym, void *stream);
+
 /* y = alpha M x + beta y for a full symmetric M (schur_mv_, solver.c:4815). */
 BGPU_API int bgpu_symv(int n, double alpha, const double *d_M, int ldm, const double *d_x, double beta,
                        double *d_y, void *stream);

@@ -19,7 +19,7 @@ import tempfile
 
 ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 sys.path.insert(0, ROOT)
-from brisk_b200.problems import random_sdp, theta_problem, write_sdpa  # noqa: E402
+from brisk_b200.problems import moment_relaxation, random_sdp, theta_problem, write_sdpa  # noqa: E402
 
 REF = os.path.join(ROOT, "oracle", "_ref", "brisk_ref")
 OUT = os.path.join(ROOT, "tests", "golden", "ref_runs.json")
@@ -31,6 +31,8 @@ INSTANCES = {
     "rand30": (random_sdp, dict(n=30, m=60, density=0.1, seed=1)),
     "rand60": (random_sdp, dict(n=60, m=200, density=0.05, seed=2)),
     "rand100": (random_sdp, dict(n=100, m=300, density=0.02, seed=3)),
+    "mom8": (moment_relaxation, dict(nvars=8, clique=4, seed=1)),
+    "mom60": (moment_relaxation, dict(nvars=60, clique=4, seed=0)),
 }
 BIG = {"rand400": (random_sdp, dict(n=400, m=2000, density=0.01, seed=0))}
 
@@ -69,12 +71,15 @@ def main():
     if os.path.exists(OUT):
         with open(OUT) as f:
             res = json.load(f)
+    only = [a for a in sys.argv[1:] if not a.startswith("--")]
     with tempfile.TemporaryDirectory() as td:
         for name, (fn, kw) in inst.items():
+            if only and name not in only:
+                continue
             d = fn(**kw)
             path = os.path.join(td, name + ".dat-s")
             write_sdpa(d, path)
-            entry = dict(generator=fn.__name__, kwargs=kw, m=d.m, n=int(d.bs[0]), runs={})
+            entry = dict(generator=fn.__name__, kwargs=kw, m=d.m, n=int(d.bs[0]), nblk=d.nblk, runs={})
             base = ["-nohsd", "-dir", "hkm", "-mixed", "0", "-tol", "1e-7"] + AS_GIVEN
             entry["runs"]["init0"] = run(path, base + ["-init", "0"])
             entry["runs"]["default"] = run(path, base)

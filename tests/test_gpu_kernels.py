@@ -275,3 +275,63 @@ def test_schur_tf32x3_matches_fp64(cuda):
         out.append(M.cpu().numpy().reshape(d.m, d.m).T)
     rel = np.abs(out[1] - out[0]).max() / np.abs(out[0]).max()
     assert rel <= 1e-5
+
+
+def _ptr_table(tensors, cuda):
+    return torch.tensor([t.data_ptr() for t in tensors], dtype=torch.int64, device=cuda)
+
+
+def test_small_batched_chol_gemm_lammin(cuda):
+    """The one-CTA-per-block kernels on blocks of uneven order (1..64) against numpy FP64."""
+    rng = np.random.default_rng(21)
+    sizes = [1, 2, 7, 15, 15, 31, 32, 33, 63, 64]
+    A = [spd(n, 100 + n) for n in sizes]
+    D = []
+    for n in sizes:
+        R = rng.standard_normal((n, n))
+        D.append(R + R.T)
+    dA = [colmajor(a, cuda) for a in A]
+    dL = [torch.zeros(n * n, dtype=torch.float64, device=cuda) for n in sizes]
+    dLi = [torch.zeros(n * n, dtype=torch.float64, device=cuda) for n in sizes]
+    dD = [colmajor(d, cuda) for d in D]
+    ns = torch.tensor(sizes, dtype=torch.int32, device=cuda)
+    info = torch.full((len(sizes),), -1, dtype=torch.int32, device=cuda)
+    tA, tL, tLi, tD = (_ptr_table(x, cuda) for x in (dA, dL, dLi, dD))
+    step.call("small_chol_inv", len(sizes), ns.data_ptr(), tA.data_ptr(), tL.data_ptr(), tLi.data_ptr(),
+              info.data_ptr(), None)
+    lam = torch.zeros(len(sizes), dtype=torch.float64, device=cuda)
+    step.call("small_lammin", len(sizes), ns.data_ptr(), tLi.data_ptr(), tD.data_ptr(), lam.data_ptr(), None)
+    C = [torch.zeros(n * n, dtype=torch.float64, device=cuda) for n in sizes]
+    tC = _ptr_table(C, cuda)
+    step.call("small_gemm", len(sizes), ns.data_ptr(), 1, 0, 2.0, tLi.data_ptr(), tD.data_ptr(), 0.0, tC.data_ptr(), 0,
+              None)
+    step.call("sync", None)
+    assert info.cpu().numpy().tolist() == [0] * len(sizes)
+    for k, n in enumerate(sizes):
+        Lr = np.linalg.cholesky(A[k])
+        L = dL[k].cpu().numpy().reshape(n, n).T
+        Li = dLi[k].cpu().numpy().reshape(n, n).T
+        np.testing.assert_allclose(L, Lr, rtol=1e-10, atol=1e-12 * np.abs(Lr).max())
+        np.testing.assert_allclose(Li @ Lr, np.eye(n), atol=1e-9)
+        Lir = np.linalg.inv(Lr)
+        B = Lir @ D[k] @ Lir.T
+        want = np.linalg.eigvalsh(0.5 * (B + B.T))[0]
+        assert lam[k].item() <= want + 1e-10 * max(1.0, abs(want))
+        assert lam[k].item() == pytest.approx(want, rel=1e-9, abs=1e-10)
+        got = C[k].cpu().numpy().reshape(n, n).T
+        np.testing.assert_allclose(got, 2.0 * Lir.T @ D[k], rtol=1e-10, atol=1e-10 * np.abs(got).max())
+
+
+def test_small_chol_reports_failure(cuda):
+    n = 20
+    A = spd(n, 4)
+    A[12, 12] = -5.0
+    dA = colmajor(A, cuda)
+    dL = torch.zeros(n * n, dtype=torch.float64, device=cuda)
+    ns = torch.tensor([n], dtype=torch.int32, device=cuda)
+    info = torch.zeros(1, dtype=torch.int32, device=cuda)
+    tA, tL = _ptr_table([dA], cuda), _ptr_table([dL], cuda)
+    step.call("small_chol_inv", 1, ns.data_ptr(), tA.data_ptr(), tL.data_ptr(), 0, info.data_ptr(), None)
+    step.call("sync", None)
+    want = next(k + 1 for k in range(n) if np.linalg.eigvalsh(A[:k + 1, :k + 1])[0] <= 0)
+    assert int(info.item()) == want

@@ -72,3 +72,14 @@ def test_repeated_solves_are_bitwise_identical(golden):
     b = brisk_b200.solve_sdpa(*d.args(), options=FP64, verbose=False)
     assert a.pobj == b.pobj and a.iterations == b.iterations
     np.testing.assert_array_equal(a.y, b.y)
+
+
+@pytest.mark.parametrize("name", ["mom8", "mom60"])
+def test_moment_relaxation_matches_reference(golden, name):
+    """Many small blocks (chain moment relaxation: 15 x 15 moment blocks, batched small-block
+    kernels) against the reference's solve of the same instance."""
+    if name not in golden:
+        pytest.skip("instance not in the fixtures")
+    e = golden[name]
+    res = brisk_b200.solve_sdpa(*make(e).args(), options=FP64, verbose=False)
+    check(res, e["runs"]["default"])
