@@ -749,14 +749,17 @@ double Solver::schur_solve(const std::vector<double> &rhs, std::vector<double> &
     mv(x, Mx);
     for (int i = 0; i < m; i++) r[i] = rhs[i] - Mx[i];
     double nr = nrm(r);
-    const double tol = std::max(tol_rel, is_float ? 1e-10 : 1e-13) * nb_;
+    // a preconditioner of FP32 accuracy (the float factor, or any factor of the 3xTF32 M) is
+    // refined to 1e-10 as the reference's float factor (solver.c:5547); the exact one to 1e-13
+    const bool approx = is_float || !m_exact;
+    const double tol = std::max(tol_rel, approx ? 1e-10 : 1e-13) * nb_;
     if (nr <= tol) return nr / nb_;
     double best = nr;
     xb = x;
     prec(r, z);
     p = z;
     double rz = dot(r, z);
-    const int maxit = (reg > 0 || is_float) ? 50 : 10;
+    const int maxit = (reg > 0 || approx) ? 50 : 10;
     int stall = 0, used = 0;
     const double sgain = 0.9;
     const int smax = 4;
