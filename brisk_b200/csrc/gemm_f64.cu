@@ -46,7 +46,8 @@ __global__ void __launch_bounds__(NT, (BN <= 64) ? 2 : 1) dgemm_kernel(int M, in
     extern __shared__ __align__(16) double smem[];
     double *As = smem;
     double *Bs = smem + STAGES * A_STAGE;
-    const int i0 = blockIdx.x * BM, j0 = blockIdx.y * BN;
+    // N tiles vary fastest: the CTAs that share an A row panel run together and reuse it from L2
+    const int i0 = blockIdx.y * BM, j0 = blockIdx.x * BN;
     if (lower && i0 + BM - 1 < j0) return;   // tile entirely above the diagonal
     A += (long long)blockIdx.z * sA;
     B += (long long)blockIdx.z * sB;
@@ -164,7 +165,8 @@ int launch(cudaStream_t st, int M, int N, int K, double alpha, const double *A, 
                                         (int)TileN<BN>::SMEM));
         attr_set = true;
     }
-    dim3 grid(ceil_div(M, BM), ceil_div(N, BN), batch);
+    if (ceil_div(M, BM) > 65535) return BGPU_ERR_TOOBIG;
+    dim3 grid(ceil_div(N, BN), ceil_div(M, BM), batch);
     dgemm_kernel<A_KM, B_KM, BN><<<grid, NT, TileN<BN>::SMEM, st>>>(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C,
                                                                     ldc, sC, lower);
     BGPU_LAUNCH_CHECK();

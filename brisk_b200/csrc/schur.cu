@@ -248,10 +248,11 @@ int atop_f64(cudaStream_t st, const DevBlock &B, const double *y, double alpha, 
 }
 
 int schur_chunk_default(int n, int precision) {
-    // the chunk's G (n^2 K values) should stay L2-resident during the gather
+    // the chunk's G (n^2 K values) should stay L2-resident during the gather (<= 64 MB of the
+    // 126 MB L2); a wider chunk reads each constraint's entry list fewer times
     const double gbytes = (double)n * n * (precision == 0 ? 8.0 : 4.0);
     int K = 64;
-    while (K > 8 && gbytes * K > 48e6) K >>= 1;
+    while (K > 8 && gbytes * K > 64e6) K >>= 1;
     return K;
 }
 

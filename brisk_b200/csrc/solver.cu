@@ -30,6 +30,7 @@
 #include <cstdarg>
 #include <cstring>
 #include <map>
+#include <thread>
 
 namespace bsolve {
 
@@ -84,80 +85,126 @@ struct HProblem {
     long long Ntot = 0;
 };
 
+// Runs f(i) for i in [0, count) on the host's threads (contiguous chunks, joined before return).
+template <typename F>
+static void parallel_for(long long count, F f) {
+    unsigned nt = std::thread::hardware_concurrency();
+    nt = std::max(1u, std::min(nt, 32u));
+    if (count < 64 || nt == 1) {
+        for (long long i = 0; i < count; i++) f(i);
+        return;
+    }
+    std::vector<std::thread> th;
+    const long long chunk = (count + nt - 1) / nt;
+    for (unsigned t = 0; t < nt; t++) {
+        const long long lo = t * chunk, hi = std::min(count, lo + chunk);
+        if (lo >= hi) break;
+        th.emplace_back([lo, hi, &f] { for (long long i = lo; i < hi; i++) f(i); });
+    }
+    for (auto &t : th) t.join();
+}
+
 static int build_problem(const InputData &in, HProblem &P, std::string &err) {
     P.m = in.m;
     P.b0 = in.c;
     P.b = in.c;
-    const int nb = in.nblk;
+    const int nb = in.nblk, m = in.m;
     P.blk.resize(nb);
     for (int k = 0; k < nb; k++) {
         if (in.bs[k] <= 0) { err = "LP (negative size) blocks are not supported by this build"; return 2; }
         P.blk[k].n = in.bs[k];
         P.Ntot += in.bs[k];
     }
-    // entries grouped by block, then by (mat, column, row); duplicates summed
-    struct E { int mat, p, q; double v; };
-    std::vector<std::vector<E>> per(nb);
+    // entries bucketed by (block, matrix) with a counting sort (stable: input order within a bucket)
     const size_t nnz = in.v.size();
+    const long long nkey = (long long)nb * (m + 1);
+    std::vector<long long> start(nkey + 1, 0);
     for (size_t e = 0; e < nnz; e++) {
         const int k = in.blk[e] - 1, mt = in.mat[e];
-        if (k < 0 || k >= nb || mt < 0 || mt > in.m) { err = "entry out of range"; return 2; }
+        if (k < 0 || k >= nb || mt < 0 || mt > m) { err = "entry out of range"; return 2; }
         const int n = P.blk[k].n;
-        int i = in.i[e] - 1, j = in.j[e] - 1;
-        if (i < 0 || j < 0 || i >= n || j >= n) { err = "entry index out of the block"; return 2; }
-        if (i > j) std::swap(i, j);
-        per[k].push_back({mt, i, j, in.v[e]});
+        const int i = in.i[e], j = in.j[e];
+        if (i < 1 || j < 1 || i > n || j > n) { err = "entry index out of the block"; return 2; }
+        start[(long long)k * (m + 1) + mt + 1]++;
     }
+    for (long long q = 0; q < nkey; q++) start[q + 1] += start[q];
+    std::vector<long long> order(nnz);
+    {
+        std::vector<long long> fill(start.begin(), start.end() - 1);
+        for (size_t e = 0; e < nnz; e++) order[fill[(long long)(in.blk[e] - 1) * (m + 1) + in.mat[e]]++] = (long long)e;
+    }
+    // per (block, matrix): merge duplicates, expand to both triangles, sort by position p + q n
+    struct Bucket { std::vector<int> pos; std::vector<double> val; double ss = 0, sa = 0; };
+    std::vector<Bucket> bk(nkey);
+    parallel_for(nkey, [&](long long key) {
+        const long long s0 = start[key], s1 = start[key + 1];
+        if (s0 == s1) return;
+        const int k = (int)(key / (m + 1));
+        const int n = P.blk[k].n;
+        std::vector<std::pair<long long, double>> up;   // (upper position q*n + p with p <= q, value)
+        up.reserve(s1 - s0);
+        for (long long u = s0; u < s1; u++) {
+            const long long e = order[u];
+            int i = in.i[e] - 1, j = in.j[e] - 1;
+            if (i > j) std::swap(i, j);
+            up.push_back({(long long)j * n + i, in.v[e]});
+        }
+        std::stable_sort(up.begin(), up.end(),
+                         [](const std::pair<long long, double> &a, const std::pair<long long, double> &b) {
+                             return a.first < b.first;
+                         });
+        std::vector<std::pair<int, double>> full;
+        full.reserve(2 * up.size());
+        for (size_t u = 0; u < up.size();) {
+            size_t w = u;
+            double v = 0;
+            while (w < up.size() && up[w].first == up[u].first) v += up[w++].second;   // duplicates summed
+            if (v != 0.0) {
+                const int q = (int)(up[u].first / n), pp = (int)(up[u].first % n);
+                full.push_back({pp + q * n, v});
+                if (pp != q) full.push_back({q + pp * n, v});
+            }
+            u = w;
+        }
+        std::sort(full.begin(), full.end());
+        Bucket &b = bk[key];
+        b.pos.resize(full.size());
+        b.val.resize(full.size());
+        for (size_t u = 0; u < full.size(); u++) {
+            b.pos[u] = full[u].first;
+            b.val[u] = full[u].second;
+            b.ss += full[u].second * full[u].second;
+            b.sa += std::fabs(full[u].second);
+        }
+    });
     std::vector<double> nrm2(P.m, 0.0);
     double c2 = 0, c1 = 0;
     for (int k = 0; k < nb; k++) {
         HBlock &B = P.blk[k];
-        const int n = B.n;
-        auto &L = per[k];
-        std::stable_sort(L.begin(), L.end(), [](const E &a, const E &b) {
-            if (a.mat != b.mat) return a.mat < b.mat;
-            if (a.q != b.q) return a.q < b.q;
-            return a.p < b.p;
+        const long long k0 = (long long)k * (m + 1);
+        Bucket &C0 = bk[k0];
+        B.Cpos = std::move(C0.pos);
+        B.Cval = std::move(C0.val);
+        for (auto &v : B.Cval) v = -v;   // C = -F0
+        c2 += C0.ss;
+        c1 += C0.sa;
+        long long total = 0;
+        B.cptr.assign(1, 0);
+        for (int mt = 1; mt <= m; mt++) {
+            Bucket &b = bk[k0 + mt];
+            if (b.pos.empty()) continue;
+            B.con.push_back(mt - 1);
+            nrm2[mt - 1] += b.ss;
+            total += (long long)b.pos.size();
+            B.cptr.push_back(total);
+        }
+        B.cpos.resize(total);
+        B.cval.resize(total);
+        parallel_for((long long)B.con.size(), [&](long long t) {
+            Bucket &b = bk[k0 + B.con[t] + 1];
+            std::copy(b.pos.begin(), b.pos.end(), B.cpos.begin() + B.cptr[t]);
+            std::copy(b.val.begin(), b.val.end(), B.cval.begin() + B.cptr[t]);
         });
-        std::vector<E> U;   // merged
-        for (const E &e : L) {
-            if (!U.empty() && U.back().mat == e.mat && U.back().p == e.p && U.back().q == e.q) U.back().v += e.v;
-            else U.push_back(e);
-        }
-        // full expansion per matrix, sorted by position p + q n
-        size_t s = 0;
-        B.cptr.push_back(0);
-        while (s < U.size()) {
-            size_t t = s;
-            while (t < U.size() && U[t].mat == U[s].mat) t++;
-            std::vector<std::pair<int, double>> full;
-            for (size_t u = s; u < t; u++) {
-                if (U[u].v == 0.0) continue;
-                full.push_back({U[u].p + U[u].q * n, U[u].v});
-                if (U[u].p != U[u].q) full.push_back({U[u].q + U[u].p * n, U[u].v});
-            }
-            std::sort(full.begin(), full.end());
-            if (!full.empty()) {
-                if (U[s].mat == 0) {
-                    for (auto &f : full) {
-                        B.Cpos.push_back(f.first);
-                        B.Cval.push_back(-f.second);   // C = -F0
-                        c2 += f.second * f.second;
-                        c1 += std::fabs(f.second);
-                    }
-                } else {
-                    const int con = U[s].mat - 1;
-                    B.con.push_back(con);
-                    for (auto &f : full) {
-                        B.cpos.push_back(f.first);
-                        B.cval.push_back(f.second);
-                        nrm2[con] += f.second * f.second;
-                    }
-                    B.cptr.push_back((long long)B.cpos.size());
-                }
-            }
-            s = t;
-        }
     }
     // problem_prepare (problem.c:1866-1910): row equilibration, b and C scaling
     P.normC2 = std::sqrt(c2);
@@ -219,8 +266,9 @@ static double ritz_bound(int k, const double *alpha, const double *beta, double 
     }
     const double th = 0.5 * (lo + hi);
     *theta = th;
+    const double scale = std::max(std::fabs(lo), std::fabs(hi));
+    if (!(scale > 1e-280)) return std::fabs(beta[k - 1]);   // a zero operator: theta = 0, |z_k| <= 1
     // inverse iteration on T - (th - delta) I, dense Gaussian elimination with partial pivoting
-    const double scale = std::max(std::fabs(lo), std::fabs(hi)) + 1e-300;
     const double sh = th - 1e-10 * scale;
     double z[64], A[64 * 64], w[64];
     for (int i = 0; i < k; i++) z[i] = 1.0 / std::sqrt((double)k) * (1.0 + 0.01 * i);
@@ -252,10 +300,12 @@ static double ritz_bound(int k, const double *alpha, const double *beta, double 
             for (int j = c + 1; j < k; j++) s -= A[c + j * k] * z[j];
             z[c] = s / A[c + c * k];
         }
+        double zmax = 0;
+        for (int i = 0; i < k; i++) zmax = std::max(zmax, std::fabs(z[i]));
+        if (!(zmax > 0) || !std::isfinite(zmax)) return std::fabs(beta[k - 1]);   // the trivial bound |z_k| <= 1
         double nz = 0;
-        for (int i = 0; i < k; i++) nz += z[i] * z[i];
+        for (int i = 0; i < k; i++) { z[i] /= zmax; nz += z[i] * z[i]; }
         nz = std::sqrt(nz);
-        if (!(nz > 0) || !std::isfinite(nz)) { *theta = th; return 1e300; }
         for (int i = 0; i < k; i++) z[i] /= nz;
     }
     return std::fabs(beta[k - 1] * z[k - 1]);
@@ -1443,6 +1493,7 @@ int solve_problem(const InputData &in, const Options &opt, ResultData &res) {
         log_printf(1, "brisk: %s\n", err.c_str());
         return rc;
     }
+    if (opt.verbose > 1) log_printf(0, "   [host problem build %.3fs]\n", wtime() - t0);
     if (opt.verbose > 0) {
         int nmax = 0;
         for (auto &B : P.blk) nmax = std::max(nmax, B.n);
@@ -1451,8 +1502,10 @@ int solve_problem(const InputData &in, const Options &opt, ResultData &res) {
     }
     try {
         Solver S(P, opt);
+        const double tsu = wtime();
         S.setup();
         const double t1 = wtime();
+        if (opt.verbose > 1) log_printf(0, "   [device setup and upload %.3fs]\n", t1 - tsu);
         int rc = S.run(res);
         res.t.setup = t1 - t0;
         res.h2d_bytes = S.upload_bytes;

@@ -117,7 +117,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     uint32_t *tslot = (uint32_t *)(done + 1);
     int *bad = (int *)(tslot + 1);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+    // N tiles vary fastest: the CTAs that share an A row panel run together and reuse it from L2
+    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
     const int nkb = (K + BK - 1) / BK;
 
     if (threadIdx.x == 0) {
@@ -275,7 +276,7 @@ int launch(cudaStream_t st, int M, int N, int K, const float *Ah, const float *A
     }
     int *err = err_flag();
     if (!err) return BGPU_ERR_NOMEM;
-    dim3 grid(ceil_div(M, BM), ceil_div(N, BN));
+    dim3 grid(ceil_div(N, BN), ceil_div(M, BM));
     tf32x3_kernel<BN><<<grid, NTHREADS, Cfg<BN>::SMEM, st>>>(mAh, mAl, mBh, mBl, G, ldg, M, N, K, err);
     BGPU_LAUNCH_CHECK();
     return BGPU_OK;
