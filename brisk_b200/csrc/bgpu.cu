@@ -50,6 +50,39 @@ BGPU_API int bgpu_schur_assemble(int n, int m, int ncon, const int *d_con, const
     return schur_assemble(S(stream), B, d_X, d_Zi, d_M, m, precision, chunk, d_ws, ws_bytes);
 }
 
+BGPU_API size_t bgpu_schur_dense_ws_bytes(int n, int ncon, int chunk, int precision) {
+    if (chunk <= 0) chunk = schur_chunk_default(n, precision);
+    return schur_dense_ws_bytes(n, ncon, chunk, precision);
+}
+BGPU_API int bgpu_schur_densify(int n, int ncon, const long long *d_cptr, const int *d_cpos, const double *d_cval,
+                                double *d_Ad, void *stream) {
+    DevBlock B;
+    B.n = n;
+    B.ncon = ncon;
+    B.cptr = (long long *)d_cptr;
+    B.cpos = (int *)d_cpos;
+    B.cval = (double *)d_cval;
+    B.Ad = d_Ad;
+    return schur_densify(S(stream), B);
+}
+BGPU_API int bgpu_schur_assemble_dense(int n, int m, int ncon, const int *d_con, const long long *d_cptr,
+                                       const int *d_ccol, const int *d_cpos, const double *d_cval, const double *d_Ad,
+                                       const double *d_X, const double *d_Zi, double *d_M, int precision, int chunk,
+                                       void *d_ws, size_t ws_bytes, void *stream) {
+    if (n <= 0 || m <= 0 || ncon < 0 || (precision != 0 && precision != 1)) return BGPU_ERR_ARG;
+    if (chunk <= 0) chunk = schur_chunk_default(n, precision);
+    DevBlock B;
+    B.n = n;
+    B.ncon = ncon;
+    B.con = (int *)d_con;
+    B.cptr = (long long *)d_cptr;
+    B.ccol = (int *)d_ccol;
+    B.cpos = (int *)d_cpos;
+    B.cval = (double *)d_cval;
+    B.Ad = (double *)d_Ad;
+    return schur_assemble_dense(S(stream), B, d_X, d_Zi, d_M, m, precision, chunk, d_ws, ws_bytes);
+}
+
 BGPU_API int bgpu_potrf(int n, double *d_A, int lda, double *d_dinv, int *d_info, double *d_pmin, void *stream) {
     if (n <= 0 || lda < n) return BGPU_ERR_ARG;
     return potrf_f64(S(stream), n, d_A, lda, d_dinv, d_info, d_pmin);

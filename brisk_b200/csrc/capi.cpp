@@ -149,6 +149,13 @@ int parse_options(int argc, const char *const *argv, Options &opt, std::string &
         } else if (a == "-init") {
             const char *s = need("0 or 1");
             if (!s || !parse_int(s, opt.init) || opt.init < 0) { if (err.empty()) err = "bad -init"; return 1; }
+        } else if (a == "-schurroute") {   // this build: the assembly route of every block
+            const char *s = need("auto, row or dense");
+            if (!s) return 1;
+            if (!strcmp(s, "auto")) opt.route = -1;
+            else if (!strcmp(s, "row")) opt.route = 0;
+            else if (!strcmp(s, "dense")) opt.route = 1;
+            else { err = "bad -schurroute (auto, row or dense)"; return 1; }
         } else if (a == "-q") {
             opt.verbose = 0;
         } else if (a == "-v") {

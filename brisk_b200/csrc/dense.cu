@@ -45,21 +45,32 @@ __global__ void __launch_bounds__(256) potrf_diag_kernel(int n, T *A, long long 
             X[r + c * LDS] = (r == c) ? (T)1 : (T)0;
         }
     __syncthreads();
+    // Column c (one barrier a column): every thread reads d = S(c,c); the trailing update uses the
+    // unscaled column, S(r,q) -= S(r,c) S(q,c) / d, and column c is scaled by 1/sqrt(d) one phase
+    // later, when nothing reads it any more.
     double pm = 1e300;
     int fail = 0;
+    T prev_inv = (T)0, prev_piv = (T)0;
     for (int c = 0; c < nb; c++) {
-        const T d = S[c + c * LDS];            // every thread reads the same pivot
+        const T d = S[c + c * LDS];
         if (!(d > (T)0) || !isfinite((double)d)) { fail = j0 + c + 1; break; }
         if ((double)d < pm) pm = (double)d;
-        const T piv = sqrt(d);
-        __syncthreads();                       // all have read S(c,c) before it is overwritten
-        if (tid == 0) S[c + c * LDS] = piv;
-        for (int r = c + 1 + tid; r < nb; r += 256) S[r + c * LDS] /= piv;
-        __syncthreads();
-        for (int k = c + 1 + tx; k < nb; k += 16) {
-            const T lkc = S[k + c * LDS];
-            for (int r = k + ty; r < nb; r += 16) S[r + k * LDS] -= S[r + c * LDS] * lkc;
+        const T inv_d = (T)1 / d;
+        if (c > 0) {   // scale column c-1 (its pivot was d_{c-1})
+            for (int r = c - 1 + tid; r < nb; r += 256)
+                S[r + (c - 1) * LDS] = (r == c - 1) ? prev_piv : S[r + (c - 1) * LDS] * prev_inv;
         }
+        for (int q = c + 1 + tx; q < nb; q += 16) {
+            const T sqc = S[q + c * LDS] * inv_d;
+            for (int r = q + ty; r < nb; r += 16) S[r + q * LDS] -= S[r + c * LDS] * sqc;
+        }
+        prev_piv = sqrt(d);
+        prev_inv = (T)1 / prev_piv;
+        __syncthreads();
+    }
+    if (!fail && nb > 0) {   // scale the last column
+        for (int r = nb - 1 + tid; r < nb; r += 256)
+            S[r + (nb - 1) * LDS] = (r == nb - 1) ? prev_piv : S[r + (nb - 1) * LDS] * prev_inv;
         __syncthreads();
     }
     if (fail) {
@@ -67,14 +78,22 @@ __global__ void __launch_bounds__(256) potrf_diag_kernel(int n, T *A, long long 
         return;
     }
     if (tid == 0) atomicMin((unsigned long long *)pmin, (unsigned long long)__double_as_longlong(pm));
+    // X = L^-1, one barrier a row: row k of X is final after its division by L(k,k); the rows below
+    // subtract L(r,k)/L(k,k) times the undivided row k, and row k is divided one phase later.
+    T prev_dinv = (T)0;
     for (int k = 0; k < nb; k++) {
-        const T lkk = S[k + k * LDS];
-        for (int j = tid; j <= k; j += 256) X[k + j * LDS] /= lkk;
-        __syncthreads();
+        const T rk = (T)1 / S[k + k * LDS];
+        if (k > 0)
+            for (int j = tid; j <= k - 1; j += 256) X[(k - 1) + j * LDS] *= prev_dinv;
         for (int j = tx; j <= k; j += 16) {
-            const T xkj = X[k + j * LDS];
+            const T xkj = X[k + j * LDS] * rk;
             for (int r = k + 1 + ty; r < nb; r += 16) X[r + j * LDS] -= S[r + k * LDS] * xkj;
         }
+        prev_dinv = rk;
+        __syncthreads();
+    }
+    if (nb > 0) {
+        for (int j = tid; j <= nb - 1; j += 256) X[(nb - 1) + j * LDS] *= prev_dinv;
         __syncthreads();
     }
     for (int c = ty; c < NB; c += 16)

@@ -16,7 +16,7 @@
 #include "kernels.h"
 
 namespace {
-constexpr int BM = 128, BK = 16, STAGES = 3, NT = 256;
+constexpr int BM = 128, BK = 16, NT = 256;
 constexpr int LDA_M = BM + 8;   // smem stride for an MMAJOR A tile  [BK][BM+8]
 constexpr int LDA_K = BK + 4;   // smem stride for a  KMAJOR A tile  [BM][BK+4]
 constexpr int LDB_K = BK + 4;   // smem stride for a  KMAJOR B tile  [BN][BK+4]
@@ -24,6 +24,8 @@ constexpr int A_STAGE = (BK * LDA_M > BM * LDA_K) ? BK * LDA_M : BM * LDA_K;
 // the N tile (64, 80, 112 or 128 columns): the launcher picks the one that pads N least
 template <int BN>
 struct TileN {
+    // 3 stages keep two 64-wide CTAs per SM; the wider tiles (one CTA per SM) pipeline 4 deep
+    static constexpr int STAGES = BN <= 64 ? 3 : 4;
     static constexpr int LDB_N = BN + 8;   // smem stride for an NMAJOR B tile  [BK][BN+8]
     static constexpr int B_STAGE = (BN * LDB_K > BK * LDB_N) ? BN * LDB_K : BK * LDB_N;
     static constexpr int NT8 = BN / 16;     // n8 tiles per warp (warps are 4 x 2)
@@ -43,6 +45,7 @@ __global__ void __launch_bounds__(NT, (BN <= 64) ? 2 : 1) dgemm_kernel(int M, in
                                                    double beta, double *C, long long ldc, long long sC,
                                                    int lower) {
     constexpr int LDB_N = TileN<BN>::LDB_N, B_STAGE = TileN<BN>::B_STAGE, NT8 = TileN<BN>::NT8;
+    constexpr int STAGES = TileN<BN>::STAGES;
     extern __shared__ __align__(16) double smem[];
     double *As = smem;
     double *Bs = smem + STAGES * A_STAGE;

@@ -66,6 +66,7 @@ struct DevBlock {
     int *pcon = nullptr;    // [ne] global constraint index of each position-major entry
     double *pval = nullptr; // [ne]
     double *C = nullptr;    // dense n x n (scaled)
+    double *Ad = nullptr;   // [ncon * n*n] the constraints as dense matrices (dense route only)
 };
 
 // out[con[t]] = beta*out[con[t]] + alpha * <A_t, D>  for every constraint of the block.
@@ -79,6 +80,16 @@ struct SchurWs {
     size_t bytes = 0;
 };
 size_t schur_ws_bytes(int n, int chunk, int precision);
+// Workspace of the dense route: schur_ws_bytes plus the chunk's output columns (and an FP64 copy
+// of G in the mixed path).
+size_t schur_dense_ws_bytes(int n, int ncon, int chunk, int precision);
+// Fills B.Ad (device, ncon * n*n doubles) from the constraint-major entries.
+int schur_densify(cudaStream_t st, const DevBlock &B);
+// The dense route (the reference's route 2, solver.c:2972-3021): G_a = X A_a Zi as in the
+// row-product route, then M[:, a] = Ad vec(G_a) for the chunk's constraints as one DMMA GEMM
+// (ncon x K x n^2) instead of the entry gather.
+int schur_assemble_dense(cudaStream_t st, const DevBlock &B, const double *X, const double *Zi, double *M, int m,
+                         int precision, int chunk, void *ws, size_t ws_bytes);
 // Fills B.ccol (device, ncon*(n+1) ints) from cptr/cpos: the column pointers of each constraint.
 int schur_colptr(cudaStream_t st, const DevBlock &B);
 int schur_chunk_default(int n, int precision);

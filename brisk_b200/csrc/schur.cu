@@ -311,3 +311,97 @@ int schur_assemble(cudaStream_t st, const DevBlock &B, const double *X, const do
     }
     return BGPU_OK;
 }
+
+// ---- the dense route -------------------------------------------------------------------------
+namespace {
+__global__ void densify_kernel(int n, int ncon, const long long *__restrict__ cptr, const int *__restrict__ cpos,
+                               const double *__restrict__ cval, double *__restrict__ Ad) {
+    const int t = blockIdx.x;
+    if (t >= ncon) return;
+    double *row = Ad + (long long)t * n * n;
+    for (long long e = cptr[t] + threadIdx.x; e < cptr[t + 1]; e += blockDim.x) row[cpos[e]] = cval[e];
+}
+__global__ void f2d_kernel(long long count, const float *__restrict__ src, double *__restrict__ dst) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count) dst[i] = (double)src[i];
+}
+// M[con[b], con[a0 + j]] += Mloc[b + j ncon] for every local b and the chunk's columns j
+__global__ void scatter_cols_kernel(int ncon, int a0, int kw, int m, const int *__restrict__ con,
+                                    const double *__restrict__ Mloc, double *M) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+    if (b >= ncon || j >= kw) return;
+    M[(long long)con[b] + (long long)con[a0 + j] * m] += Mloc[b + (long long)j * ncon];
+}
+}  // namespace
+
+size_t schur_dense_ws_bytes(int n, int ncon, int chunk, int precision) {
+    size_t b = schur_ws_bytes(n, chunk, precision) + (size_t)ncon * chunk * sizeof(double) + 256;
+    if (precision == 1) b += (size_t)n * n * chunk * sizeof(double) + 256;
+    return b;
+}
+
+int schur_densify(cudaStream_t st, const DevBlock &B) {
+    if (B.ncon <= 0) return BGPU_OK;
+    BGPU_CHECK(cudaMemsetAsync(B.Ad, 0, sizeof(double) * (size_t)B.ncon * B.n * B.n, st));
+    densify_kernel<<<B.ncon, 256, 0, st>>>(B.n, B.ncon, B.cptr, B.cpos, B.cval, B.Ad);
+    BGPU_LAUNCH_CHECK();
+    return BGPU_OK;
+}
+
+int schur_assemble_dense(cudaStream_t st, const DevBlock &B, const double *X, const double *Zi, double *M, int m,
+                         int precision, int chunk, void *ws, size_t ws_bytes) {
+    const int n = B.n, K = chunk, ncon = B.ncon;
+    if (ncon <= 0) return BGPU_OK;
+    if (!B.Ad || !B.ccol) return BGPU_ERR_ARG;
+    if (ws_bytes < schur_dense_ws_bytes(n, ncon, K, precision)) return BGPU_ERR_ARG;
+    const size_t nnK = (size_t)n * n * K;
+    const size_t base_bytes = schur_ws_bytes(n, K, precision);
+    uintptr_t tail = ((uintptr_t)ws + base_bytes + 255) & ~(uintptr_t)255;
+    double *Mloc = (double *)tail;
+    double *G64 = nullptr;
+    if (precision == 1) G64 = (double *)((((uintptr_t)(Mloc + (size_t)ncon * K)) + 255) & ~(uintptr_t)255);
+    dim3 tgrid(ceil_div(n, TP_Q), ceil_div(n, TP_K), K);
+    double *T64 = (double *)ws, *Gd = T64 + nnK;   // FP64 layout of the workspace
+    float *Th = nullptr, *Tl = nullptr, *Gf = nullptr, *Xh = nullptr, *Xl = nullptr;
+    const int ld = tf32_ld(n);
+    if (precision == 1) {
+        void *w = ws;
+        auto carve = [&](size_t count) {
+            uintptr_t p = ((uintptr_t)w + 255) & ~(uintptr_t)255;
+            w = (void *)(p + count * sizeof(float));
+            return (float *)p;
+        };
+        Th = carve((size_t)n * K * ld);
+        Tl = carve((size_t)n * K * ld);
+        Gf = carve(nnK);
+        Xh = carve((size_t)n * ld);
+        Xl = carve((size_t)n * ld);
+        split2d_kernel<<<dim3(ceil_div(ld, 256), n), 256, 0, st>>>(n, X, ld, Xh, Xl);
+        BGPU_LAUNCH_CHECK();
+    }
+    for (int a0 = 0; a0 < ncon; a0 += K) {
+        const int kw = min(K, ncon - a0);
+        const double *G = nullptr;
+        if (precision == 0) {
+            tprod_kernel<double><<<tgrid, 256, 0, st>>>(n, n, K, a0, ncon, B.cptr, B.ccol, B.cpos, B.cval, Zi, T64, nullptr);
+            BGPU_LAUNCH_CHECK();
+            int rc = gemm_f64(st, 1, 1, n * K, n, n, 1.0, T64, n, 0, X, n, 0, 0.0, Gd, (long long)n * K, 0, 1, 0);
+            if (rc) return rc;
+            G = Gd;
+        } else {
+            tprod_kernel<float><<<tgrid, 256, 0, st>>>(n, ld, K, a0, ncon, B.cptr, B.ccol, B.cpos, B.cval, Zi, Th, Tl);
+            BGPU_LAUNCH_CHECK();
+            int rc = gemm_tf32x3(st, n * K, n, n, Th, Tl, ld, Xh, Xl, ld, Gf, (long long)n * K);
+            if (rc) return rc;
+            f2d_kernel<<<ceil_div((long long)nnK, 256), 256, 0, st>>>((long long)nnK, Gf, G64);
+            BGPU_LAUNCH_CHECK();
+            G = G64;
+        }
+        // Mloc (ncon x K) = Ad (ncon x n^2, K-major rows) * G (n^2 x K, column index fastest)
+        int rc = gemm_f64(st, 1, 0, ncon, kw, n * n, 1.0, B.Ad, (long long)n * n, 0, G, K, 0, 0.0, Mloc, ncon, 0, 1, 0);
+        if (rc) return rc;
+        scatter_cols_kernel<<<dim3(ceil_div(ncon, 256), kw), 256, 0, st>>>(ncon, a0, kw, m, B.con, Mloc, M);
+        BGPU_LAUNCH_CHECK();
+    }
+    return BGPU_OK;
+}

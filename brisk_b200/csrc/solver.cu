@@ -396,6 +396,7 @@ class Solver {
     Gpu g;
     std::vector<DevBlock> db;
     std::vector<DevArrays> da;
+    std::vector<char> dense_route;   // per block: the dense Schur route (Ad resident)
     // Schur complement
     double *M = nullptr, *Lm = nullptr, *dinvM = nullptr, *Dsc = nullptr;
     float *Mf = nullptr, *dinvMf = nullptr;
@@ -501,6 +502,20 @@ void Solver::upload_block(int k) {
     CU(cudaMemcpy(d.cpos, B.cpos.data(), sizeof(int) * d.ne, cudaMemcpyHostToDevice));
     CU(cudaMemcpy(d.cval, B.cval.data(), sizeof(double) * d.ne, cudaMemcpyHostToDevice));
     RC(schur_colptr(g.st, d));
+    // the dense route: constraints averaging >= 2 % of the n^2 entries (the reference's dense
+    // candidates, problem.c:1299), n >= 8, and their dense copies within 8 GB
+    {
+        const double avg = d.ncon > 0 ? (double)d.ne / d.ncon : 0.0;
+        const double bytes = (double)d.ncon * n * n * sizeof(double);
+        bool dense = opt.route == 1 || (opt.route < 0 && n >= 8 && avg >= 0.02 * (double)n * n);
+        if (dense && bytes > 8e9) dense = false;
+        dense_route[k] = dense;
+        if (dense && d.ncon > 0) {
+            d.Ad = g.alloc<double>((size_t)d.ncon * n * n);
+            if (!d.Ad) throw GpuFail{BGPU_ERR_NOMEM, __LINE__};
+            RC(schur_densify(g.st, d));
+        }
+    }
     // position-major copy (A'(y) without atomics): entries of each position in constraint order
     std::vector<long long> pptr(nn + 1, 0);
     for (long long e = 0; e < d.ne; e++) pptr[B.cpos[e] + 1]++;
@@ -547,6 +562,7 @@ void Solver::setup() {
     CU(cudaEventCreate(&evs1));
     db.resize(nb);
     da.resize(nb);
+    dense_route.assign(nb, 0);
     int nmax = 1;
     for (int k = 0; k < nb; k++) {
         upload_block(k);
@@ -600,6 +616,10 @@ void Solver::setup() {
     chunk = opt.chunk > 0 ? opt.chunk : schur_chunk_default(nmax, asm_prec);
     chunk64 = opt.chunk > 0 ? opt.chunk : schur_chunk_default(nmax, 0);
     ws_bytes = std::max(schur_ws_bytes(nmax, chunk, asm_prec), schur_ws_bytes(nmax, chunk64, 0));
+    for (int k = 0; k < nb; k++)
+        if (dense_route[k])
+            ws_bytes = std::max(ws_bytes, std::max(schur_dense_ws_bytes(db[k].n, db[k].ncon, chunk, asm_prec),
+                                                   schur_dense_ws_bytes(db[k].n, db[k].ncon, chunk64, 0)));
     ws = g.alloc<unsigned char>(ws_bytes);
     if (!ws) throw GpuFail{BGPU_ERR_NOMEM, __LINE__};
 }
@@ -662,7 +682,10 @@ void Solver::assemble(std::vector<double> &) {
     const int prec = (asm_prec == 1 && !asm_fp64) ? 1 : 0;
     m_exact = prec == 0;
     for (int k = 0; k < nb; k++) {
-        RC(schur_assemble(g.st, db[k], da[k].X, da[k].Zi, M, m, prec, prec ? chunk : chunk64, ws, ws_bytes));
+        if (dense_route[k])
+            RC(schur_assemble_dense(g.st, db[k], da[k].X, da[k].Zi, M, m, prec, prec ? chunk : chunk64, ws, ws_bytes));
+        else
+            RC(schur_assemble(g.st, db[k], da[k].X, da[k].Zi, M, m, prec, prec ? chunk : chunk64, ws, ws_bytes));
         const double n = db[k].n;
         const double ncon = db[k].ncon;
         schur_flops += 2.0 * n * n * n * ncon;   // the row-product GEMMs: 2 n^2 r_a with r_a <= n
@@ -983,7 +1006,8 @@ void Solver::least_squares_start(std::vector<double> &y) {
     CU(cudaMemsetAsync(M, 0, sizeof(double) * (size_t)m * m, g.st));
     for (int k = 0; k < nb; k++) {
         RC(ew_set_scaled_identity(g.st, db[k].n, da[k].T, 1.0));
-        RC(schur_assemble(g.st, db[k], da[k].T, da[k].T, M, m, 0, chunk_fp64(k), ws, ws_bytes));
+        if (dense_route[k]) RC(schur_assemble_dense(g.st, db[k], da[k].T, da[k].T, M, m, 0, chunk_fp64(k), ws, ws_bytes));
+        else RC(schur_assemble(g.st, db[k], da[k].T, da[k].T, M, m, 0, chunk_fp64(k), ws, ws_bytes));
     }
     const int frc = factor();
     allow_float = af;

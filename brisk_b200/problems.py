@@ -173,6 +173,11 @@ def random_dense_instance(rng, n: int, m: int, name: str = "") -> SdpaData:
     return SdpaData(np.array([n], np.int32), b, *d, name=name, meta=dict(kind="dense", n=n, m=m))
 
 
+def dense_instance(n: int, m: int, seed: int = 0) -> SdpaData:
+    """One seeded small dense instance (random_dense_instance with default_rng(seed))."""
+    return random_dense_instance(np.random.default_rng(seed), n, m, name=f"dense_n{n}_m{m}_seed{seed}")
+
+
 def random_dense_batch(count: int = 4096, nmin: int = 8, nmax: int = 64, seed: int = 0,
                        sizes_only: bool = False):
     """The uneven batch: n ~ U{nmin..nmax}, m ~ U{n..floor(n(n+1)/4)} per instance.

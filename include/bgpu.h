@@ -74,6 +74,19 @@ BGPU_API int bgpu_schur_assemble(int n, int m, int ncon, const int *d_con, const
                                  const double *d_Zi, double *d_M, int precision, int chunk, void *d_ws,
                                  size_t ws_bytes, void *stream);
 
+/* The dense route (the reference's route 2, solver.c:2972-3021) for blocks of dense constraints:
+ * bgpu_schur_densify writes the constraints as dense matrices (d_Ad: ncon * n*n doubles, row t
+ * the column-major A_t); bgpu_schur_assemble_dense then forms G_a = X A_a Zi per chunk of
+ * constraints and M[:, a] = Ad vec(G_a) by one DMMA GEMM per chunk (full columns of M).  The
+ * workspace is bgpu_schur_dense_ws_bytes. */
+BGPU_API size_t bgpu_schur_dense_ws_bytes(int n, int ncon, int chunk, int precision);
+BGPU_API int bgpu_schur_densify(int n, int ncon, const long long *d_cptr, const int *d_cpos, const double *d_cval,
+                                double *d_Ad, void *stream);
+BGPU_API int bgpu_schur_assemble_dense(int n, int m, int ncon, const int *d_con, const long long *d_cptr,
+                                       const int *d_ccol, const int *d_cpos, const double *d_cval, const double *d_Ad,
+                                       const double *d_X, const double *d_Zi, double *d_M, int precision, int chunk,
+                                       void *d_ws, size_t ws_bytes, void *stream);
+
 /* In-place Cholesky L L' = A of the lower triangle (column-major, lda); d_dinv receives the
  * inverses of the 64 x 64 diagonal blocks (ceil(n/64)*4096 entries), *d_info the first failing
  * column (1-based) or 0, *d_pmin the smallest squared pivot.  Replaces brisk_dpotrf

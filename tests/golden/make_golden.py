@@ -19,7 +19,7 @@ import tempfile
 
 ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 sys.path.insert(0, ROOT)
-from brisk_b200.problems import moment_relaxation, random_sdp, theta_problem, write_sdpa  # noqa: E402
+from brisk_b200.problems import dense_instance, moment_relaxation, random_sdp, theta_problem, write_sdpa  # noqa: E402
 
 REF = os.path.join(ROOT, "oracle", "_ref", "brisk_ref")
 OUT = os.path.join(ROOT, "tests", "golden", "ref_runs.json")
@@ -33,6 +33,8 @@ INSTANCES = {
     "rand100": (random_sdp, dict(n=100, m=300, density=0.02, seed=3)),
     "mom8": (moment_relaxation, dict(nvars=8, clique=4, seed=1)),
     "mom60": (moment_relaxation, dict(nvars=60, clique=4, seed=0)),
+    "dense24": (dense_instance, dict(n=24, m=100, seed=11)),
+    "dense48": (dense_instance, dict(n=48, m=500, seed=12)),
 }
 BIG = {"rand400": (random_sdp, dict(n=400, m=2000, density=0.01, seed=0))}
 

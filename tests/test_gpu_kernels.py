@@ -335,3 +335,28 @@ def test_small_chol_reports_failure(cuda):
     step.call("sync", None)
     want = next(k + 1 for k in range(n) if np.linalg.eigvalsh(A[:k + 1, :k + 1])[0] <= 0)
     assert int(info.item()) == want
+
+
+@pytest.mark.parametrize("prec,tol", [(0, 1e-10), (1, 1e-5)])
+def test_schur_dense_route_matches_oracle(cuda, prec, tol):
+    """The dense route (M[:, a] = Ad vec(X A_a Zi) by GEMM) on a dense-constraint block."""
+    rng = np.random.default_rng(5)
+    d = problems.random_dense_instance(rng, 24, 100)
+    S, n, a = block_arrays(d, cuda)
+    X = spd(n, 8, cond=50)
+    Zi = spd(n, 9, cond=50)
+    want = restate.schur(S.A, [X], [Zi])
+    ncon = int(a["con"].numel())
+    Ad = torch.zeros(ncon * n * n, dtype=torch.float64, device=cuda)
+    step.call("schur_densify", n, ncon, a["cptr"].data_ptr(), a["cpos"].data_ptr(), a["cval"].data_ptr(),
+              Ad.data_ptr(), None)
+    M = torch.zeros(d.m * d.m, dtype=torch.float64, device=cuda)
+    chunk = 16
+    ws = torch.empty(int(step.lib().bgpu_schur_dense_ws_bytes(n, ncon, chunk, prec)), dtype=torch.uint8, device=cuda)
+    dX, dZi = colmajor(X, cuda), colmajor(Zi, cuda)
+    step.call("schur_assemble_dense", n, d.m, ncon, a["con"].data_ptr(), a["cptr"].data_ptr(), a["ccol"].data_ptr(),
+              a["cpos"].data_ptr(), a["cval"].data_ptr(), Ad.data_ptr(), dX.data_ptr(), dZi.data_ptr(), M.data_ptr(),
+              prec, chunk, ws.data_ptr(), ws.numel(), None)
+    step.call("sync", None)
+    got = M.cpu().numpy().reshape(d.m, d.m).T
+    assert np.abs(got - want).max() / np.abs(want).max() <= tol

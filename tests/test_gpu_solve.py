@@ -83,3 +83,13 @@ def test_moment_relaxation_matches_reference(golden, name):
     e = golden[name]
     res = brisk_b200.solve_sdpa(*make(e).args(), options=FP64, verbose=False)
     check(res, e["runs"]["default"])
+
+
+@pytest.mark.parametrize("name", ["dense24", "dense48"])
+@pytest.mark.parametrize("route", ["dense", "row"])
+def test_dense_constraints_match_reference(golden, name, route):
+    """Dense N(0,1) constraints (the batch workload's instances): the dense route (Ad times G by
+    GEMM) and the row-product route both reach the reference's solution."""
+    e = golden[name]
+    res = brisk_b200.solve_sdpa(*make(e).args(), options=FP64 + ["-schurroute", route], verbose=False)
+    check(res, e["runs"]["default"])
