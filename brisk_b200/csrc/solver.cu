@@ -1296,7 +1296,22 @@ int Solver::run(ResultData &res) {
         assemble(tmpv);
         double tc = wtime();
         tm.schur += tc - ts;
-        if (factor() != 0) { status = 4; tm.chol += wtime() - tc; break; }
+        int frc = factor();
+        if (!m_exact && (frc != 0 || reg > 0)) {
+            // the 3xTF32 M is FP32-accurate: once its factor needs a regularization it no longer
+            // preconditions the FP64 system; this and the later iterations assemble in FP64
+            asm_fp64 = true;
+            reg_hint = false;
+            reg_ok = 0;
+            if (opt.verbose > 1) log_printf(0, "   mixed path: the FP32-accurate M needed a shift: FP64 assembly from here on\n");
+            tm.chol += wtime() - tc;
+            ts = wtime();
+            assemble(tmpv);
+            tc = wtime();
+            tm.schur += tc - ts;
+            frc = factor();
+        }
+        if (frc != 0) { status = 4; tm.chol += wtime() - tc; break; }
         tm.chol += wtime() - tc;
         // ---- rhs pieces ----
         td = wtime();
