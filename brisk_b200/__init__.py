@@ -1,12 +1,13 @@
 """brisk_b200: the SDP interior-point Newton step of BRISK on a B200 GPU.
 
 The public API mirrors the reference's Python package (``brisk``): ``solve_sdpa`` and
-``solve_file`` return a ``Result`` with the status, objectives, DIMACS errors and the solution.
+``solve_file`` return a ``Result`` with the status, objectives, DIMACS errors and the solution;
+``solve_batch`` solves many independent problems in one call (bgpu_batch_solve).
 The work runs in the in-tree CUDA library ``libbrisk.so`` (sm_100a), which exports the same C
 interface as the reference's libbrisk.
 """
-from ._core import (STATUS, Result, interrupt, library_path, load_library, options_to_argv, solve_file,
-                    solve_sdpa, version)
+from ._core import (STATUS, Result, concat_problems, interrupt, library_path, load_library, options_to_argv,
+                    solve_batch, solve_batch_arrays, solve_file, solve_sdpa, version)
 
-__all__ = ["STATUS", "Result", "interrupt", "library_path", "load_library", "options_to_argv", "solve_file",
-           "solve_sdpa", "version"]
+__all__ = ["STATUS", "Result", "concat_problems", "interrupt", "library_path", "load_library", "options_to_argv",
+           "solve_batch", "solve_batch_arrays", "solve_file", "solve_sdpa", "version"]

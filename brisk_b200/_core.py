@@ -70,6 +70,9 @@ def load_library(path=None):
     L.brisk_solve_data.restype = I
     L.brisk_solve_file.argtypes = [ctypes.c_char_p, I, ppc, P]
     L.brisk_solve_file.restype = I
+    L.bgpu_batch_solve.argtypes = [I, pi, pi, pi, pd, ctypes.POINTER(ctypes.c_int64), pi, pi, pi, pi, pd, I, ppc, I,
+                                   ctypes.POINTER(P), pi]
+    L.bgpu_batch_solve.restype = I
     L.brisk_interrupt.argtypes, L.brisk_interrupt.restype = [], None
     L.brisk_interrupted.argtypes, L.brisk_interrupted.restype = [], I
     _lib, _lib_path = L, path
@@ -219,6 +222,63 @@ def solve_sdpa(blocksizes, c, mat, blk, i, j, v, options=None, verbose=True):
 def solve_file(path, options=None, verbose=True):
     """Solve an SDPA sparse file."""
     return _run(lambda L, n, a, r: L.brisk_solve_file(os.fsencode(path), n, a, r), options, verbose)
+
+
+def solve_batch_arrays(m, nblk, bs, c, nnz, mat, blk, i, j, v, options=None, workers=0):
+    """Solve independent problems given as concatenated brisk_solve_data arrays (problem p: m[p]
+    constraints, nblk[p] block sizes, nnz[p] entries, in problem order) with one call of
+    bgpu_batch_solve.  Returns the list of Results (no log: the batch runs quiet)."""
+    L = load_library()
+    m, nblk, bs = _ints(m, "m"), _ints(nblk, "nblk"), _ints(bs, "bs")
+    nnz = np.ascontiguousarray(nnz, dtype=np.int64)
+    count = int(m.size)
+    if nblk.size != count or nnz.size != count:
+        raise ValueError("m, nblk and nnz must have one entry per problem")
+    if int(nblk.sum()) != bs.size or int(m.sum()) != np.asarray(c).size:
+        raise ValueError("bs and c must hold the block sizes and right-hand sides of every problem")
+    c = _finite(c, "c")
+    arrs = [np.ascontiguousarray(a, dtype=np.intc) for a in (mat, blk, i, j)]
+    v = np.ascontiguousarray(v, dtype=np.float64)
+    if any(a.size != int(nnz.sum()) for a in arrs) or v.size != int(nnz.sum()):
+        raise ValueError("mat, blk, i, j and v must hold the entries of every problem")
+    av = options_to_argv(options)
+    arr = (ctypes.c_char_p * max(len(av), 1))(*[a.encode() for a in av])
+    pi = ctypes.POINTER(ctypes.c_int)
+    pd = ctypes.POINTER(ctypes.c_double)
+    P = lambda a, t: a.ctypes.data_as(t)   # noqa: E731
+    with _lock:
+        L.brisk_set_output(1, _PRINT(0))
+        handles = (ctypes.c_void_p * max(count, 1))(*[L.brisk_result_new() for _ in range(count)])
+        rcs = np.zeros(max(count, 1), dtype=np.intc)
+        try:
+            rc = L.bgpu_batch_solve(count, P(m, pi), P(nblk, pi), P(bs, pi), P(c, pd),
+                                    nnz.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), P(arrs[0], pi),
+                                    P(arrs[1], pi), P(arrs[2], pi), P(arrs[3], pi), P(v, pd), len(av), arr,
+                                    int(workers), handles, P(rcs, pi))
+            if rc != 0:
+                raise RuntimeError(f"brisk: bgpu_batch_solve returned {rc}")
+            return [_collect(L, handles[p], int(rcs[p]), "") for p in range(count)]
+        finally:
+            for p in range(count):
+                L.brisk_result_delete(handles[p])
+            L.brisk_set_output(0, _PRINT(0))
+
+
+def concat_problems(problems):
+    """The concatenated arrays of solve_batch_arrays for objects with the fields bs, c, mat,
+    blk, i, j, v (brisk_b200.problems.SdpaData)."""
+    cat = lambda k, t: np.concatenate([np.asarray(getattr(d, k), dtype=t) for d in problems])  # noqa: E731
+    return dict(m=np.array([len(d.c) for d in problems], np.intc),
+                nblk=np.array([len(d.bs) for d in problems], np.intc),
+                bs=cat("bs", np.intc), c=cat("c", np.float64),
+                nnz=np.array([len(d.v) for d in problems], np.int64),
+                mat=cat("mat", np.intc), blk=cat("blk", np.intc), i=cat("i", np.intc), j=cat("j", np.intc),
+                v=cat("v", np.float64))
+
+
+def solve_batch(problems, options=None, workers=0):
+    """Solve a list of problems (SdpaData-like objects) with one bgpu_batch_solve call."""
+    return solve_batch_arrays(**concat_problems(problems), options=options, workers=workers)
 
 
 def interrupt():

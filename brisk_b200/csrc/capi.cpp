@@ -120,6 +120,12 @@ int parse_options(int argc, const char *const *argv, Options &opt, std::string &
         } else if (a == "-muswitch") {
             const char *s = need("a number");
             if (!s || !parse_double(s, opt.mu_switch)) { if (err.empty()) err = "bad -muswitch"; return 1; }
+        } else if (a == "-mixedshift") {
+            const char *s = need("0 or 1");
+            if (!s || !parse_int(s, opt.mixed_shift) || opt.mixed_shift < 0 || opt.mixed_shift > 1) {
+                if (err.empty()) err = "bad -mixedshift (0 or 1)";
+                return 1;
+            }
         } else if (a == "-schurchunk") {
             const char *s = need("8, 16, 32 or 64");
             if (!s || !parse_int(s, opt.chunk) || (opt.chunk != 8 && opt.chunk != 16 && opt.chunk != 32 && opt.chunk != 64)) {
@@ -337,6 +343,48 @@ BRISK_API int brisk_solve_data(int m, int nblk, const int *bs, const double *c, 
     bsolve::InputData in;
     if (!make_input(m, nblk, bs, c, nnz, mat, blk, i, j, v, in)) return 2;
     return run(in, nopt, opts, res);
+}
+
+BGPU_API int bgpu_batch_solve(int count, const int *m, const int *nblk, const int *bs, const double *c,
+                              const int64_t *nnz, const int *mat, const int *blk, const int *i, const int *j,
+                              const double *v, int nopt, const char *const *opts, int workers,
+                              BriskResult *const *res, int *rc) {
+    if (count < 0 || (count > 0 && (!m || !nblk || !bs || !nnz || !res || !rc))) return -1;
+    std::vector<int64_t> boff(count + 1, 0), coff(count + 1, 0), eoff(count + 1, 0);
+    std::vector<double> work(count, 0.0);
+    for (int p = 0; p < count; p++) {
+        if (!res[p] || nblk[p] < 0 || m[p] < 0 || nnz[p] < 0) return -1;
+        boff[p + 1] = boff[p] + nblk[p];
+        coff[p + 1] = coff[p] + m[p];
+        eoff[p + 1] = eoff[p] + nnz[p];
+        // assembly m (4 n^3 + 2 n^2 m) per block plus the factor m^3 / 3: the largest go first
+        const double mm = m[p];
+        double w = mm * mm * mm / 3.0;
+        for (int k = 0; k < nblk[p]; k++) {
+            const double n = std::fabs((double)bs[boff[p] + k]);
+            w += mm * (4.0 * n * n * n + 2.0 * n * n * mm);
+        }
+        work[p] = w;
+    }
+    bsolve::Options opt;
+    std::string err;
+    bsolve::set_print_hook(capi_print);
+    if (bsolve::parse_options(nopt, opts, opt, err)) {
+        bsolve::log_printf(1, "brisk: %s\n", err.c_str());
+        fflush(stdout);
+        return 1;
+    }
+    auto get = [&](int p, bsolve::InputData &in) {
+        const int64_t e = eoff[p];
+        return make_input(m[p], nblk[p], bs + boff[p], c ? c + coff[p] : nullptr, nnz[p], mat ? mat + e : nullptr,
+                          blk ? blk + e : nullptr, i ? i + e : nullptr, j ? j + e : nullptr, v ? v + e : nullptr, in);
+    };
+    auto put = [&](int p, bsolve::ResultData &r, int code) {
+        res[p]->r = std::move(r);
+        fill_result(res[p]);
+        rc[p] = code;
+    };
+    return bsolve::solve_batch(count, work, get, put, opt, workers, err);
 }
 
 struct bgpu_session {

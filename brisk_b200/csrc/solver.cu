@@ -29,7 +29,9 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstring>
+#include <atomic>
 #include <map>
+#include <numeric>
 #include <thread>
 
 namespace bsolve {
@@ -86,11 +88,15 @@ struct HProblem {
 };
 
 // Runs f(i) for i in [0, count) on the host's threads (contiguous chunks, joined before return).
+// Set in batch workers: the host problem build of one instance then runs on the calling thread
+// (the batch already keeps every host core busy with other instances).
+static thread_local bool tl_serial = false;
+
 template <typename F>
 static void parallel_for(long long count, F f) {
     unsigned nt = std::thread::hardware_concurrency();
     nt = std::max(1u, std::min(nt, 32u));
-    if (count < 64 || nt == 1) {
+    if (count < 64 || nt == 1 || tl_serial) {
         for (long long i = 0; i < count; i++) f(i);
         return;
     }
@@ -337,21 +343,53 @@ struct DevArrays {   // per block
     int *flags;
 };
 
+// Device memory of one solve.  Stand-alone solves allocate with cudaMalloc and own a stream; the
+// batch workers hand in an arena (one allocation and one stream per worker, reused by every
+// instance it solves) so that no cudaMalloc / cudaFree runs between instances.
 struct Gpu {
     std::vector<void *> allocs;
     cudaStream_t st = nullptr;
+    Arena *arena = nullptr;
     template <typename T>
     T *alloc(size_t count) {
-        void *p = nullptr;
         if (count == 0) count = 1;
+        if (arena) {
+            const size_t off = (arena->used + 255) & ~(size_t)255;
+            if (off + count * sizeof(T) > arena->cap) {
+                arena->need = std::max(arena->need, off + count * sizeof(T));
+                return nullptr;
+            }
+            arena->used = off + count * sizeof(T);
+            return (T *)(arena->base + off);
+        }
+        void *p = nullptr;
         if (cudaMalloc(&p, count * sizeof(T)) != cudaSuccess) return nullptr;
         allocs.push_back(p);
         return (T *)p;
     }
+    // Pinned host memory for the small device-to-host reads of the loop (from the arena's
+    // pinned buffer in a batch worker, where it fits).
+    std::vector<void *> hallocs;
+    template <typename T>
+    T *host_alloc(size_t count) {
+        if (count == 0) count = 1;
+        if (arena && arena->hbase) {
+            const size_t off = (arena->hused + 63) & ~(size_t)63;
+            if (off + count * sizeof(T) <= arena->hcap) {
+                arena->hused = off + count * sizeof(T);
+                return (T *)(arena->hbase + off);
+            }
+        }
+        void *p = nullptr;
+        if (cudaMallocHost(&p, count * sizeof(T)) != cudaSuccess) return nullptr;
+        hallocs.push_back(p);
+        return (T *)p;
+    }
     ~Gpu() {
         if (st) cudaStreamSynchronize(st);
+        for (void *p : hallocs) cudaFreeHost(p);
         for (void *p : allocs) cudaFree(p);
-        if (st) cudaStreamDestroy(st);
+        if (st && !arena) cudaStreamDestroy(st);
     }
 };
 
@@ -374,7 +412,9 @@ struct GpuFail {
 
 class Solver {
   public:
-    Solver(HProblem &P, const Options &opt) : P(P), opt(opt), m(P.m), nb((int)P.blk.size()) {}
+    Solver(HProblem &P, const Options &opt, Arena *arena = nullptr) : P(P), opt(opt), m(P.m), nb((int)P.blk.size()) {
+        g.arena = arena;
+    }
     void setup();                 // upload the scaled problem and allocate the device state
     int run(ResultData &res);     // one solve from the resident data
     void set_options(const Options &o) { opt = o; }
@@ -383,9 +423,6 @@ class Solver {
         if (ev1) cudaEventDestroy(ev1);
         if (evs0) cudaEventDestroy(evs0);
         if (evs1) cudaEventDestroy(evs1);
-        if (h_dots) cudaFreeHost(h_dots);
-        if (h_sinfo) cudaFreeHost(h_sinfo);
-        if (h_slam) cudaFreeHost(h_slam);
     }
     double upload_bytes = 0;
 
@@ -406,7 +443,7 @@ class Solver {
     float *fv = nullptr;
     double *dots_out = nullptr, *dots_scratch = nullptr;
     const double **dots_a = nullptr, **dots_b = nullptr;
-    double *h_dots = nullptr;                     // pinned
+    double *h_dots = nullptr;
     void *ws = nullptr;
     size_t ws_bytes = 0;
     // blocks of order <= SMALL_N_MAX run through the batched one-CTA-per-block kernels (small.cu)
@@ -497,10 +534,10 @@ void Solver::upload_block(int k) {
     d.C = g.alloc<double>(nn);
     if (!d.con || !d.cptr || !d.cpos || !d.cval || !d.ccol || !d.pptr || !d.pcon || !d.pval || !d.C)
         throw GpuFail{BGPU_ERR_NOMEM, __LINE__};
-    CU(cudaMemcpy(d.con, B.con.data(), sizeof(int) * d.ncon, cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(d.cptr, B.cptr.data(), sizeof(long long) * (d.ncon + 1), cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(d.cpos, B.cpos.data(), sizeof(int) * d.ne, cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(d.cval, B.cval.data(), sizeof(double) * d.ne, cudaMemcpyHostToDevice));
+    CU(cudaMemcpyAsync(d.con, B.con.data(), sizeof(int) * d.ncon, cudaMemcpyHostToDevice, g.st));
+    CU(cudaMemcpyAsync(d.cptr, B.cptr.data(), sizeof(long long) * (d.ncon + 1), cudaMemcpyHostToDevice, g.st));
+    CU(cudaMemcpyAsync(d.cpos, B.cpos.data(), sizeof(int) * d.ne, cudaMemcpyHostToDevice, g.st));
+    CU(cudaMemcpyAsync(d.cval, B.cval.data(), sizeof(double) * d.ne, cudaMemcpyHostToDevice, g.st));
     RC(schur_colptr(g.st, d));
     // the dense route: constraints averaging >= 2 % of the n^2 entries (the reference's dense
     // candidates, problem.c:1299), n >= 8, and their dense copies within 8 GB
@@ -529,12 +566,12 @@ void Solver::upload_block(int k) {
             pcon[q] = B.con[t];
             pval[q] = B.cval[e];
         }
-    CU(cudaMemcpy(d.pptr, pptr.data(), sizeof(long long) * (nn + 1), cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(d.pcon, pcon.data(), sizeof(int) * d.ne, cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(d.pval, pval.data(), sizeof(double) * d.ne, cudaMemcpyHostToDevice));
+    CU(cudaMemcpyAsync(d.pptr, pptr.data(), sizeof(long long) * (nn + 1), cudaMemcpyHostToDevice, g.st));
+    CU(cudaMemcpyAsync(d.pcon, pcon.data(), sizeof(int) * d.ne, cudaMemcpyHostToDevice, g.st));
+    CU(cudaMemcpyAsync(d.pval, pval.data(), sizeof(double) * d.ne, cudaMemcpyHostToDevice, g.st));
     std::vector<double> C(nn, 0.0);
     for (size_t e = 0; e < B.Cpos.size(); e++) C[B.Cpos[e]] += B.Cval[e];
-    CU(cudaMemcpy(d.C, C.data(), sizeof(double) * nn, cudaMemcpyHostToDevice));
+    CU(cudaMemcpyAsync(d.C, C.data(), sizeof(double) * nn, cudaMemcpyHostToDevice, g.st));
     upload_bytes += (double)sizeof(int) * d.ncon + sizeof(long long) * (d.ncon + 1) + (sizeof(int) + sizeof(double)) * 2.0 * d.ne +
                     sizeof(long long) * (nn + 1.0) + sizeof(double) * (double)nn;
 
@@ -550,12 +587,20 @@ void Solver::upload_block(int k) {
     a.dinvZ = g.alloc<double>((size_t)nblk64 * TRI_NB * TRI_NB);
     a.flags = g.alloc<int>(nblk64);
     if (!a.dinvX || !a.dinvZ || !a.flags) throw GpuFail{BGPU_ERR_NOMEM, __LINE__};
-    CU(cudaMemset(a.flags, 0, sizeof(int) * nblk64));
+    CU(cudaMemsetAsync(a.flags, 0, sizeof(int) * nblk64, g.st));
+    CU(cudaStreamSynchronize(g.st));   // the host staging vectors above go out of scope
 }
 
 void Solver::setup() {
+    const double t0 = wtime();
     CU(cudaSetDevice(opt.device));
-    CU(cudaStreamCreateWithFlags(&g.st, cudaStreamNonBlocking));
+    if (g.arena) {
+        g.st = (cudaStream_t)g.arena->st;
+        g.arena->used = 0;
+        g.arena->hused = 0;
+    } else {
+        CU(cudaStreamCreateWithFlags(&g.st, cudaStreamNonBlocking));
+    }
     CU(cudaEventCreate(&ev0));
     CU(cudaEventCreate(&ev1));
     CU(cudaEventCreate(&evs0));
@@ -564,10 +609,12 @@ void Solver::setup() {
     da.resize(nb);
     dense_route.assign(nb, 0);
     int nmax = 1;
+    const double t1 = wtime();
     for (int k = 0; k < nb; k++) {
         upload_block(k);
         nmax = std::max(nmax, P.blk[k].n);
     }
+    if (opt.verbose > 1) log_printf(0, "   [device context %.3fs, block upload %.3fs]\n", t1 - t0, wtime() - t1);
     for (int k = 0; k < nb; k++) (P.blk[k].n <= SMALL_N_MAX ? small_ids : big_ids).push_back(k);
     if (!small_ids.empty()) {
         const int ns = (int)small_ids.size();
@@ -577,9 +624,11 @@ void Solver::setup() {
         d_sinfo = g.alloc<int>(ns);
         d_slam = g.alloc<double>(ns);
         if (!d_sns || !d_sinfo || !d_slam) throw GpuFail{BGPU_ERR_NOMEM, __LINE__};
-        CU(cudaMemcpy(d_sns, nsz.data(), sizeof(int) * ns, cudaMemcpyHostToDevice));
-        CU(cudaMallocHost(&h_sinfo, sizeof(int) * ns));
-        CU(cudaMallocHost(&h_slam, sizeof(double) * ns));
+        CU(cudaMemcpyAsync(d_sns, nsz.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, g.st));
+        CU(cudaStreamSynchronize(g.st));
+        h_sinfo = g.host_alloc<int>(ns);
+        h_slam = g.host_alloc<double>(ns);
+        if (!h_sinfo || !h_slam) throw GpuFail{BGPU_ERR_NOMEM, __LINE__};
     }
     const size_t mm = (size_t)m * m;
     M = g.alloc<double>(mm);
@@ -602,9 +651,10 @@ void Solver::setup() {
     if (!dinvM || !Dsc || !mflags || !d_info || !d_err || !d_pmin || !dv_in || !dv_out || !fv || !dots_out ||
         !dots_scratch || !dots_a || !dots_b)
         throw GpuFail{BGPU_ERR_NOMEM, __LINE__};
-    CU(cudaMemset(mflags, 0, sizeof(int) * mb64));
-    CU(cudaMemset(d_err, 0, sizeof(int)));
-    CU(cudaMallocHost(&h_dots, 16 * sizeof(double)));
+    CU(cudaMemsetAsync(mflags, 0, sizeof(int) * mb64, g.st));
+    CU(cudaMemsetAsync(d_err, 0, sizeof(int), g.st));
+    h_dots = g.host_alloc<double>(16);
+    if (!h_dots) throw GpuFail{BGPU_ERR_NOMEM, __LINE__};
     allow_float = opt.mixed > 0 || (opt.mixed < 0 && m >= 1000);
     asm_prec = opt.asm_prec < 0 ? 0 : opt.asm_prec;
     if (asm_prec == 1) allow_float = true;   // the 3xTF32 path factors in FP32 until mu_switch
@@ -654,7 +704,8 @@ double **Solver::tab(double *DevArrays::*mem) {
     for (int k : small_ids) ptrs.push_back(da[k].*mem);
     double **d = g.alloc<double *>(ptrs.size());
     if (!d) throw GpuFail{BGPU_ERR_NOMEM, __LINE__};
-    CU(cudaMemcpy(d, ptrs.data(), sizeof(double *) * ptrs.size(), cudaMemcpyHostToDevice));
+    CU(cudaMemcpyAsync(d, ptrs.data(), sizeof(double *) * ptrs.size(), cudaMemcpyHostToDevice, g.st));
+    CU(cudaStreamSynchronize(g.st));
     stab.push_back({mem, d});
     return d;
 }
@@ -782,7 +833,8 @@ void Solver::prec(const std::vector<double> &rv, std::vector<double> &z) {
         for (int i = 0; i < m; i++) z[i] = h[i] * Dh[i];
     }
     int err = 0;
-    CU(cudaMemcpy(&err, d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    CU(cudaMemcpyAsync(&err, d_err, sizeof(int), cudaMemcpyDeviceToHost, g.st));
+    CU(cudaStreamSynchronize(g.st));
     if (err) throw GpuFail{BGPU_ERR_TIMEOUT, __LINE__};
 }
 
@@ -832,10 +884,12 @@ double Solver::schur_solve(const std::vector<double> &rhs, std::vector<double> &
     prec(r, z);
     p = z;
     double rz = dot(r, z);
-    const int maxit = (reg > 0 || approx) ? 50 : 10;
+    // the factor of a shifted 3xTF32 M preconditions the FP64 operator less well: more steps
+    const bool shifted = !m_exact && reg > 0;
+    const int maxit = shifted ? 150 : (reg > 0 || approx) ? 50 : 10;
     int stall = 0, used = 0;
     const double sgain = 0.9;
-    const int smax = 4;
+    const int smax = shifted ? 10 : 4;
     for (int k = 0; k < maxit; k++) {
         mv(p, q);
         const double pq = dot(p, q);
@@ -1297,7 +1351,11 @@ int Solver::run(ResultData &res) {
         double tc = wtime();
         tm.schur += tc - ts;
         int frc = factor();
-        if (!m_exact && (frc != 0 || reg > 0)) {
+        if (!m_exact && frc == 0 && reg > 0 && opt.mixed_shift) {
+            // the 3xTF32 M is FP32-accurate and its factor needed a shift: PCG against the FP64
+            // operator with the shifted factor (schur_solve turns to FP64 assembly if it misses)
+            if (opt.verbose > 1) log_printf(0, "   mixed path: the 3xTF32 M factored with shift %.1e\n", reg);
+        } else if (!m_exact && (frc != 0 || reg > 0)) {
             // the 3xTF32 M is FP32-accurate: once its factor needs a regularization it no longer
             // preconditions the FP64 system; this and the later iterations assemble in FP64
             asm_fp64 = true;
@@ -1520,7 +1578,7 @@ int Solver::run(ResultData &res) {
 
 }  // namespace
 
-int solve_problem(const InputData &in, const Options &opt, ResultData &res) {
+static int solve_impl(const InputData &in, const Options &opt, ResultData &res, Arena *arena) {
     HProblem P;
     std::string err;
     const double t0 = wtime();
@@ -1540,7 +1598,7 @@ int solve_problem(const InputData &in, const Options &opt, ResultData &res) {
         log_printf(0, "problem: m = %d, %d SDP blocks (max n = %d)\n", in.m, in.nblk, nmax);
     }
     try {
-        Solver S(P, opt);
+        Solver S(P, opt, arena);
         const double tsu = wtime();
         S.setup();
         const double t1 = wtime();
@@ -1559,12 +1617,99 @@ int solve_problem(const InputData &in, const Options &opt, ResultData &res) {
         }
         return rc;
     } catch (const GpuFail &f) {
+        if (arena && f.rc == BGPU_ERR_NOMEM) {   // the batch worker grows its arena and retries
+            res.status = 4;
+            res.exit_code = BGPU_ERR_NOMEM;
+            return BGPU_ERR_NOMEM;
+        }
         log_printf(1, "brisk: GPU failure (code %d at solver.cu:%d%s%s)\n", f.rc, f.line,
                    f.ce != cudaSuccess ? ": " : "", f.ce != cudaSuccess ? cudaGetErrorString(f.ce) : "");
         res.status = 4;
         res.exit_code = -3;
         return -3;
     }
+}
+
+int solve_problem(const InputData &in, const Options &opt, ResultData &res) { return solve_impl(in, opt, res, nullptr); }
+
+int solve_problem_arena(const InputData &in, const Options &opt, ResultData &res, Arena *arena) {
+    tl_serial = true;
+    const int rc = solve_impl(in, opt, res, arena);
+    tl_serial = false;
+    return rc;
+}
+
+int solve_batch(int count, const std::vector<double> &work, const std::function<bool(int, InputData &)> &get,
+                const std::function<void(int, ResultData &, int)> &put, const Options &opt, int workers,
+                std::string &err) {
+    if (count <= 0) return 0;
+    if (workers <= 0) workers = (int)std::max(2u, std::thread::hardware_concurrency());
+    workers = std::min(workers, count);
+    std::vector<int> order(count);
+    std::iota(order.begin(), order.end(), 0);
+    if ((int)work.size() == count)
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return work[a] > work[b]; });
+    std::atomic<int> next{0};
+    Options o = opt;
+    o.verbose = 0;
+    auto body = [&]() {
+        cudaStream_t st = nullptr;
+        Arena a;
+        const bool ok = cudaSetDevice(o.device) == cudaSuccess &&
+                        cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) == cudaSuccess;
+        a.st = st;
+        if (ok && cudaMallocHost((void **)&a.hbase, (size_t)1 << 20) == cudaSuccess) a.hcap = (size_t)1 << 20;
+        else a.hbase = nullptr;
+        for (;;) {
+            const int q = next.fetch_add(1);
+            if (q >= count) break;
+            const int p = order[q];
+            InputData in;
+            ResultData r;
+            int rc = -3;
+            try {
+                if (!ok) {
+                    r.status = 4;
+                } else if (!get(p, in)) {
+                    rc = 2;
+                } else {
+                    for (int grow = 0; grow < 8; grow++) {
+                        rc = solve_problem_arena(in, o, r, &a);
+                        if (rc != BGPU_ERR_NOMEM) break;
+                        // The arena grows to the instance's need (with headroom); instances run
+                        // largest first, so this happens a few times per worker at most.
+                        const size_t want = std::max(std::max(a.cap * 2, a.need + a.need / 4), (size_t)64 << 20);
+                        cudaStreamSynchronize(st);
+                        if (a.base) cudaFree(a.base);
+                        a.base = nullptr;
+                        a.cap = a.need = 0;
+                        if (cudaMalloc(&a.base, want) != cudaSuccess) {
+                            a.base = nullptr;
+                            rc = -3;
+                            r.status = 4;
+                            break;
+                        }
+                        a.cap = want;
+                    }
+                    if (rc == BGPU_ERR_NOMEM) rc = -3;
+                }
+            } catch (...) {
+                rc = -3;
+                r.status = 4;
+            }
+            r.exit_code = rc;
+            put(p, r, rc);
+        }
+        if (st) cudaStreamSynchronize(st);
+        if (a.base) cudaFree(a.base);
+        if (a.hbase) cudaFreeHost(a.hbase);
+        if (st) cudaStreamDestroy(st);
+    };
+    (void)err;
+    std::vector<std::thread> th;
+    for (int w = 0; w < workers; w++) th.emplace_back(body);
+    for (auto &t : th) t.join();
+    return 0;
 }
 
 }  // namespace bsolve

@@ -1,6 +1,7 @@
 // Host-side solver of the B200 SDP Newton step: the problem as given, the options, the result.
 #pragma once
 #include <cstdint>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -29,6 +30,7 @@ struct Options {
     int mixed = -1;             // FP32 Schur factor: -1 auto (m >= 1000), 0 never, 1 always
     int asm_prec = -1;          // Schur assembly: -1 auto (FP64), 0 FP64, 1 3xTF32
     double mu_switch = 1e-4;    // 3xTF32 path: the factor goes to FP64 once scaled mu < mu_switch
+    int mixed_shift = 1;        // 3xTF32 path: a shifted factor of M still preconditions PCG (0: FP64 assembly)
     int chunk = 0;              // constraints per assembly chunk (0: chosen by the block order)
     double timelimit = 0.0;
     double reg_ill = 0.0;
@@ -75,6 +77,29 @@ int parse_options(int argc, const char *const *argv, Options &opt, std::string &
 
 // Solves on the GPU; fills res.  Returns the exit code (0, 10-15) or a negative abort code.
 int solve_problem(const InputData &in, const Options &opt, ResultData &res);
+
+// A device arena for a batch worker: one allocation and one stream reused by every instance.
+struct Arena {
+    char *base = nullptr;
+    size_t cap = 0, used = 0;
+    size_t need = 0;      // set when an allocation did not fit: a lower bound of the bytes needed
+    void *st = nullptr;   // cudaStream_t
+    char *hbase = nullptr;   // pinned host memory for the loop's small reads
+    size_t hcap = 0, hused = 0;
+};
+// Solves with the device memory and stream of the arena (no cudaMalloc / cudaFree, no device-wide
+// synchronisation) and builds the host problem on the calling thread.  Returns BGPU_ERR_NOMEM
+// (arena->need set) when the arena is too small; the caller grows it and calls again.
+int solve_problem_arena(const InputData &in, const Options &opt, ResultData &res, Arena *arena);
+
+// Solves `count` independent problems on `workers` host threads (0: one per host core), each
+// with its own stream and arena, largest estimated work first.  get(p, in) fills problem p
+// (false: bad problem, exit code 2); put(p, res, rc) receives its result.  Every instance runs
+// the same code as solve_problem (quiet), so its result equals the stand-alone solve's.
+// Returns 0, or 1 on bad options (err set).
+int solve_batch(int count, const std::vector<double> &work, const std::function<bool(int, InputData &)> &get,
+                const std::function<void(int, ResultData &, int)> &put, const Options &opt, int workers,
+                std::string &err);
 
 // A problem kept resident in HBM between solves (the benchmark's device-resident timing).
 struct Session;

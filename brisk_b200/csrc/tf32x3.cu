@@ -254,10 +254,14 @@ int make_map(CUtensorMap *map, const float *ptr, long long rows, long long K, lo
     return r == CUDA_SUCCESS ? BGPU_OK : BGPU_ERR_ARG;
 }
 
+// The sticky error flag of the bounded mbarrier waits: a device variable (one per device, zero at
+// module load), so the first use needs no allocation and no lock.
+__device__ int g_tf32x3_err = 0;
+
 int *err_flag() {
-    static int *d = nullptr;
-    if (!d && cudaMalloc(&d, sizeof(int)) == cudaSuccess) cudaMemset(d, 0, sizeof(int));
-    return d;
+    void *d = nullptr;
+    if (cudaGetSymbolAddress(&d, g_tf32x3_err) != cudaSuccess) return nullptr;
+    return (int *)d;
 }
 
 template <int BN>

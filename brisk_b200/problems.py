@@ -195,6 +195,12 @@ def random_dense_batch(count: int = 4096, nmin: int = 8, nmax: int = 64, seed: i
     return out
 
 
+def batch_instance(q: int, count: int = 4096, nmin: int = 8, nmax: int = 64, seed: int = 0) -> SdpaData:
+    """Instance q of random_dense_batch(count, nmin, nmax, seed), made without the others."""
+    n, m = random_dense_batch(count, nmin, nmax, seed, sizes_only=True)[q]
+    return random_dense_instance(np.random.default_rng([seed, q]), int(n), int(m), name=f"batch{seed}_{q}")
+
+
 # ---------------------------------------------------------------------------------------
 # SDPA sparse files
 # ---------------------------------------------------------------------------------------

@@ -51,6 +51,20 @@ BGPU_API bgpu_session *bgpu_session_create(int m, int nblk, const int *bs, const
                                            const double *v, int nopt, const char *const *opts, int *rc);
 BGPU_API int bgpu_session_solve(bgpu_session *s, int nopt, const char *const *opts, struct BriskResult *res);
 BGPU_API void bgpu_session_destroy(bgpu_session *s);
+/* Solves `count` independent problems in one call: the arrays of brisk_solve_data (capi.c:175)
+ * for every problem, concatenated in problem order.  Problem p has m[p] constraints, nblk[p]
+ * blocks (its sizes follow those of problems 0..p-1 in bs), m[p] right-hand sides in c and
+ * nnz[p] entries in mat/blk/i/j/v.  Every problem takes the same options; res[p] (a
+ * brisk_result_new handle each) receives its result and rc[p] its exit code as brisk_solve_data
+ * returns it.  The problems run concurrently on `workers` host threads (0: one per host core),
+ * each with its own CUDA stream and one device arena reused from problem to problem, so no
+ * device allocation or device-wide synchronisation runs between problems; each problem's result
+ * is the result of brisk_solve_data on it.  Returns 0, 1 on bad options, -1 on bad arguments.
+ * Replaces a loop of brisk_solve_data calls (capi.c:175), which is not reentrant. */
+BGPU_API int bgpu_batch_solve(int count, const int *m, const int *nblk, const int *bs, const double *c,
+                              const int64_t *nnz, const int *mat, const int *blk, const int *i, const int *j,
+                              const double *v, int nopt, const char *const *opts, int workers,
+                              struct BriskResult *const *res, int *rc);
 /* Measures of the last solve of res: [0] device time (s, CUDA events on the library's
  * stream), [1] assembly device time (s), [2] assembly algorithmic flops, [3] host-to-device
  * bytes, [4] device-to-host bytes, [5] iterations, [6] float factorizations, [7] PCG steps. */

@@ -19,7 +19,8 @@ import tempfile
 
 ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 sys.path.insert(0, ROOT)
-from brisk_b200.problems import dense_instance, moment_relaxation, random_sdp, theta_problem, write_sdpa  # noqa: E402
+from brisk_b200.problems import (batch_instance, dense_instance, moment_relaxation, random_sdp, theta_problem,  # noqa: E402
+                                 write_sdpa)
 
 REF = os.path.join(ROOT, "oracle", "_ref", "brisk_ref")
 OUT = os.path.join(ROOT, "tests", "golden", "ref_runs.json")
@@ -36,6 +37,10 @@ INSTANCES = {
     "dense24": (dense_instance, dict(n=24, m=100, seed=11)),
     "dense48": (dense_instance, dict(n=48, m=500, seed=12)),
 }
+# instances of the 4096-instance uneven batch (n ~ U{8..64}, m ~ U{n..n(n+1)/4}, seed 0): the
+# first twelve and the largest (q = 3339: n = 64, m = 1038)
+for _q in list(range(12)) + [3339]:
+    INSTANCES[f"batch_q{_q}"] = (batch_instance, dict(q=_q))
 BIG = {"rand400": (random_sdp, dict(n=400, m=2000, density=0.01, seed=0))}
 
 ROW = re.compile(r"^\s*(\d+)\s+([+-]\S+)\s+([+-]\S+)\s+(\S+)\s+(\S+)\s+(\S+)\s+(\S+)\s+(\S+)\s+(\S+)\s+(\S+)\s+(\S+)\s*$")

@@ -95,3 +95,18 @@ def test_reference_python_package_loads_this_library(libpath, monkeypatch):
     assert os.path.samefile(brisk.library_path(), libpath)
     sys.modules.pop("brisk", None)
     sys.modules.pop("brisk._core", None)
+
+
+def test_batch_entry_checks_before_any_gpu_work(libpath):
+    """bgpu_batch_solve: an empty batch returns nothing, mismatched arrays and bad options are
+    rejected on the host."""
+    import brisk_b200
+    from brisk_b200 import problems
+    assert brisk_b200.solve_batch_arrays([], [], [], [], [], [], [], [], [], []) == []
+    arrs = brisk_b200.concat_problems([problems.batch_instance(5), problems.batch_instance(6)])
+    bad = dict(arrs, v=arrs["v"][:-1])
+    with pytest.raises(ValueError):
+        brisk_b200.solve_batch_arrays(**bad)
+    with pytest.raises(RuntimeError):
+        brisk_b200.solve_batch_arrays(**arrs, options=["-tol", "abc"])
+    assert int(arrs["nnz"].sum()) == arrs["v"].size and list(arrs["m"]) == [11, 15]

@@ -1,0 +1,66 @@
+"""The batch entry point (bgpu_batch_solve) on a B200: instances of the uneven 4096-instance
+batch (n ~ U{8..64}, m ~ U{n..n(n+1)/4}, dense N(0,1) A_i, b = A(I), C = G G'/n + I) solved
+in one call, each checked against the reference's own solve of that instance and against its
+own stand-alone solve through brisk_solve_data."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+import brisk_b200  # noqa: E402
+from brisk_b200 import problems  # noqa: E402
+
+FP64 = ["-nohsd", "-dir", "hkm", "-mixed", "0", "-tol", "1e-7"]
+GOLDEN_Q = list(range(12)) + [3339]
+
+
+def check(res, ref):
+    """Same status; objectives within 1e-7 relative to 1 + |<C,X>| + |b'y|; DIMACS <= 1e-7."""
+    assert res.status_str == ref["status"]
+    den = 1 + abs(ref["pobj"]) + abs(ref["dobj"])
+    assert abs(res.pobj - ref["pobj"]) <= 1e-7 * den, (res.pobj, ref["pobj"])
+    assert abs(res.dobj - ref["dobj"]) <= 1e-7 * den, (res.dobj, ref["dobj"])
+    assert np.max(np.abs(res.dimacs)) <= 1e-7, res.dimacs
+
+
+def test_batch_matches_reference(golden):
+    """Thirteen instances (the first twelve and the largest, n = 64, m = 1038) in one call."""
+    insts = [problems.batch_instance(q) for q in GOLDEN_Q]
+    out = brisk_b200.solve_batch(insts, options=FP64, workers=6)
+    assert len(out) == len(insts)
+    for q, res in zip(GOLDEN_Q, out):
+        assert res.exit_code == 0, (q, res.exit_code)
+        check(res, golden[f"batch_q{q}"]["runs"]["default"])
+
+
+def test_batch_equals_standalone_solves():
+    """Each instance's result in a concurrent batch is bit for bit its stand-alone solve's:
+    the workers run the same kernels in the same order on their own streams."""
+    insts = [problems.batch_instance(q) for q in range(12, 44)]
+    out = brisk_b200.solve_batch(insts, options=FP64, workers=8)
+    for d, res in zip(insts, out):
+        ref = brisk_b200.solve_sdpa(*d.args(), options=FP64, verbose=False)
+        assert res.exit_code == ref.exit_code and res.status == ref.status
+        assert res.iterations == ref.iterations
+        assert res.pobj == ref.pobj and res.dobj == ref.dobj
+        np.testing.assert_array_equal(res.y, ref.y)
+        np.testing.assert_array_equal(res.X[0], ref.X[0])
+        np.testing.assert_array_equal(res.dimacs, ref.dimacs)
+
+
+def test_batch_bad_instance_does_not_stop_the_others():
+    """A problem with a bad block size gets exit code 2; the rest of the batch solves."""
+    good = [problems.batch_instance(q) for q in (5, 6, 7)]
+    arrs = brisk_b200.concat_problems(good)
+    arrs["bs"] = arrs["bs"].copy()
+    arrs["bs"][1] = 0                        # instance 1: a block of order 0
+    out = brisk_b200.solve_batch_arrays(**arrs, options=FP64, workers=2)
+    assert out[1].exit_code == 2
+    assert out[0].exit_code == 0 and out[2].exit_code == 0
+    assert out[0].status_str == "OPTIMAL" and out[2].status_str == "OPTIMAL"
+
+
+def test_batch_rejects_bad_options():
+    d = problems.batch_instance(5)
+    with pytest.raises(RuntimeError):
+        brisk_b200.solve_batch([d], options=["-tol", "abc"])
