@@ -50,6 +50,64 @@ BGPU_API int bgpu_schur_assemble(int n, int m, int ncon, const int *d_con, const
     return schur_assemble(S(stream), B, d_X, d_Zi, d_M, m, precision, chunk, d_ws, ws_bytes);
 }
 
+BGPU_API int bgpu_schur_upper(int n, int ncon, const long long *d_cptr, const int *d_cpos, const double *d_cval,
+                              int *d_counts, long long *d_uptr, int *d_upos, double *d_uval, long long *nu,
+                              void *stream) {
+    if (n <= 0 || ncon < 0 || !d_uptr || !d_counts || !nu) return BGPU_ERR_ARG;
+    DevBlock B;
+    B.n = n;
+    B.ncon = ncon;
+    B.cptr = (long long *)d_cptr;
+    B.cpos = (int *)d_cpos;
+    B.cval = (double *)d_cval;
+    B.uptr = d_uptr;
+    B.upos = d_upos;
+    B.uval = d_uval;
+    *nu = 0;
+    if (ncon == 0) return BGPU_OK;
+    int rc = schur_upper_ptr(S(stream), B, d_counts);
+    if (rc) return rc;
+    BGPU_CHECK(cudaMemcpyAsync(nu, d_uptr + ncon, sizeof(long long), cudaMemcpyDeviceToHost, S(stream)));
+    BGPU_CHECK(cudaStreamSynchronize(S(stream)));
+    if (!d_upos || !d_uval) return BGPU_OK;
+    return schur_upper(S(stream), B);
+}
+
+BGPU_API int bgpu_schur_assemble_sym(int n, int m, int ncon, const int *d_con, const long long *d_cptr,
+                                     const int *d_ccol, const int *d_cpos, const double *d_cval,
+                                     const long long *d_uptr, const int *d_upos, const double *d_uval,
+                                     const double *d_X, const double *d_Zi, double *d_M, int precision, int chunk,
+                                     void *d_ws, size_t ws_bytes, void *stream) {
+    if (n <= 0 || m <= 0 || ncon < 0 || (precision != 0 && precision != 1)) return BGPU_ERR_ARG;
+    if (ncon > 0 && (!d_uptr || !d_upos || !d_uval)) return BGPU_ERR_ARG;
+    if (chunk <= 0) chunk = schur_chunk_default(n, precision);
+    DevBlock B;
+    B.n = n;
+    B.ncon = ncon;
+    B.con = (int *)d_con;
+    B.cptr = (long long *)d_cptr;
+    B.ccol = (int *)d_ccol;
+    B.cpos = (int *)d_cpos;
+    B.cval = (double *)d_cval;
+    B.uptr = (long long *)d_uptr;
+    B.upos = (int *)d_upos;
+    B.uval = (double *)d_uval;
+    return schur_assemble(S(stream), B, d_X, d_Zi, d_M, m, precision, chunk, d_ws, ws_bytes);
+}
+
+BGPU_API int bgpu_schur_gram(int n, int m, int ncon, const int *d_con, const long long *d_uptr, const int *d_upos,
+                             const double *d_uval, double *d_M, void *d_ws, size_t ws_bytes, void *stream) {
+    if (n <= 0 || m <= 0 || ncon < 0) return BGPU_ERR_ARG;
+    DevBlock B;
+    B.n = n;
+    B.ncon = ncon;
+    B.con = (int *)d_con;
+    B.uptr = (long long *)d_uptr;
+    B.upos = (int *)d_upos;
+    B.uval = (double *)d_uval;
+    return schur_assemble_gram(S(stream), B, d_M, m, d_ws, ws_bytes);
+}
+
 BGPU_API size_t bgpu_schur_dense_ws_bytes(int n, int ncon, int chunk, int precision) {
     if (chunk <= 0) chunk = schur_chunk_default(n, precision);
     return schur_dense_ws_bytes(n, ncon, chunk, precision);

@@ -67,6 +67,13 @@ struct DevBlock {
     double *pval = nullptr; // [ne]
     double *C = nullptr;    // dense n x n (scaled)
     double *Ad = nullptr;   // [ncon * n*n] the constraints as dense matrices (dense route only)
+    // upper-triangle lists (optional): entries p <= q of each constraint, packed index
+    // u = q (q + 1) / 2 + p (ascending), value A[p, q]; the assembly then gathers from the packed
+    // symmetric sum G_a + G_a' and reads half the entries and half the G values
+    long long nu = 0;            // upper entries in all
+    long long *uptr = nullptr;   // [ncon+1]
+    int *upos = nullptr;         // [nu]
+    double *uval = nullptr;      // [nu]
 };
 
 // out[con[t]] = beta*out[con[t]] + alpha * <A_t, D>  for every constraint of the block.
@@ -92,6 +99,13 @@ int schur_assemble_dense(cudaStream_t st, const DevBlock &B, const double *X, co
                          int precision, int chunk, void *ws, size_t ws_bytes);
 // Fills B.ccol (device, ncon*(n+1) ints) from cptr/cpos: the column pointers of each constraint.
 int schur_colptr(cudaStream_t st, const DevBlock &B);
+// Upper-triangle lists from the full ones: schur_upper_ptr fills B.uptr (ncon+1; uptr[ncon] is
+// the total) using counts (device scratch, ncon ints); schur_upper then fills B.upos / B.uval.
+int schur_upper_ptr(cudaStream_t st, const DevBlock &B, int *counts);
+int schur_upper(cudaStream_t st, const DevBlock &B);
+// M += the Gram matrix <A_b, A_a> of the block's constraints (the assembly at X = Zi = I, with no
+// products): needs the upper lists.
+int schur_assemble_gram(cudaStream_t st, const DevBlock &B, double *M, int m, void *ws, size_t ws_bytes);
 int schur_chunk_default(int n, int precision);
 // M (m x m, column-major, full symmetric) += the block's contribution sum over its constraints
 // of M_ab = <A_b, X A_a Zi>.  precision 0: FP64 (DMMA), 1: 3xTF32 (tcgen05).

@@ -156,6 +156,245 @@ __global__ void __launch_bounds__(GW * 32) gather_kernel(int a0, int ncon, int m
     }
 }
 
+// ---- the packed symmetric gather ---------------------------------------------------------
+// Every A_b is symmetric, so <A_b, G_a> = sum_{p<=q} A_b[p,q] S_a[p,q] with S_a = G_a + G_a' off
+// the diagonal and S_a[p,p] = G_a[p,p]: sym_pack_kernel folds the chunk's G into S (packed upper,
+// index u = q (q+1)/2 + p, K values per position, t fastest) and gather_sym_kernel reads each
+// constraint's upper entries only: half the entries and half the G values of the full gather.
+__device__ __forceinline__ long long upk(int p, int q) { return (long long)q * (q + 1) / 2 + p; }
+
+template <typename GT> struct Vec16;
+template <> struct Vec16<float> { using T = float4; static constexpr int N = 4; };
+template <> struct Vec16<double> { using T = double2; static constexpr int N = 2; };
+__device__ __forceinline__ void vget(const float4 &v, double *o) { o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w; }
+__device__ __forceinline__ void vget(const double2 &v, double *o) { o[0] = v.x; o[1] = v.y; }
+__device__ __forceinline__ float4 vadd(const float4 &a, const float4 &b) { return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w); }
+__device__ __forceinline__ double2 vadd(const double2 &a, const double2 &b) { return make_double2(a.x + b.x, a.y + b.y); }
+
+// S[(upk(i, j)) K + t] = G_a[i, j] + G_a[j, i] (i < j) or G_a[i, i]; G holds G_a[p, q] at
+// ((p n + q) K + t).  Column j = blockIdx.y; a thread owns 16 bytes of one position.
+template <typename GT, int K>
+__global__ void sym_pack_kernel(int n, const GT *__restrict__ G, GT *__restrict__ S) {
+    using V = typename Vec16<GT>::T;
+    constexpr int NV = K / Vec16<GT>::N;
+    const int j = blockIdx.y;
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = (int)(idx / NV), v = (int)(idx % NV);
+    if (i > j) return;
+    const V a = reinterpret_cast<const V *>(G + ((long long)i * n + j) * K)[v];
+    V r = a;
+    if (i < j) r = vadd(a, reinterpret_cast<const V *>(G + ((long long)j * n + i) * K)[v]);
+    reinterpret_cast<V *>(S + upk(i, j) * K)[v] = r;
+}
+
+// One CTA of GW warps per constraint b >= a0 over b's upper entries; LPG lanes per entry, each
+// loading 16 contiguous bytes of S (VEC columns); fixed summation order as gather_kernel.
+template <int K, typename GT>
+__global__ void __launch_bounds__(GW * 32) gather_sym_kernel(int a0, int ncon, int m, const int *__restrict__ con,
+                                                            const long long *__restrict__ uptr,
+                                                            const int *__restrict__ upos,
+                                                            const double *__restrict__ uval,
+                                                            const GT *__restrict__ S, double *M) {
+    using V = typename Vec16<GT>::T;
+    constexpr int VEC = Vec16<GT>::N;
+    constexpr int LPG = K / VEC;               // lanes per entry
+    constexpr int GPW = 32 / LPG;              // entries per warp step
+    __shared__ double part[GW][K];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int b = a0 + blockIdx.x;
+    if (b >= ncon) return;
+    const int sub = lane / LPG, l = lane % LPG;
+    double acc[VEC], acc2[VEC], g[VEC];
+#pragma unroll
+    for (int u = 0; u < VEC; u++) acc[u] = acc2[u] = 0.0;
+    const long long s0 = uptr[b], e0 = uptr[b + 1];
+    const long long len = e0 - s0, per_w = (len + GW - 1) / GW;
+    const long long s = s0 + warp * per_w, e = min(e0, s + per_w);
+    long long base = s;
+    for (; base + 32 <= e; base += 32) {
+        const int pos = upos[base + lane];
+        const double v = uval[base + lane];
+#pragma unroll
+        for (int j = 0; j < 32; j += GPW) {
+            const int pj = __shfl_sync(0xffffffffu, pos, j + sub);
+            const double vj = __shfl_sync(0xffffffffu, v, j + sub);
+            vget(__ldg(reinterpret_cast<const V *>(S + (long long)pj * K) + l), g);
+            if ((j / GPW) & 1) {
+#pragma unroll
+                for (int u = 0; u < VEC; u++) acc2[u] += vj * g[u];
+            } else {
+#pragma unroll
+                for (int u = 0; u < VEC; u++) acc[u] += vj * g[u];
+            }
+        }
+    }
+    if (base < e) {   // the ragged last group of the slice
+        const long long my = base + lane;
+        int pos = 0;
+        double v = 0.0;
+        if (my < e) { pos = upos[my]; v = uval[my]; }
+        const int cnt = (int)(e - base);
+        for (int j = 0; j < cnt; j += GPW) {   // uniform trip count: every lane shuffles together
+            const int jj = j + sub;
+            const int src = jj < cnt ? jj : 0;
+            const int pj = __shfl_sync(0xffffffffu, pos, src);
+            const double vj = __shfl_sync(0xffffffffu, v, src);
+            if (jj < cnt) {
+                vget(__ldg(reinterpret_cast<const V *>(S + (long long)pj * K) + l), g);
+#pragma unroll
+                for (int u = 0; u < VEC; u++) acc[u] += vj * g[u];
+            }
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < VEC; u++) {
+        acc[u] += acc2[u];
+#pragma unroll
+        for (int o = LPG; o < 32; o <<= 1) acc[u] += __shfl_xor_sync(0xffffffffu, acc[u], o);
+    }
+    if (sub == 0)
+#pragma unroll
+        for (int u = 0; u < VEC; u++) part[warp][l * VEC + u] = acc[u];
+    __syncthreads();
+    if (threadIdx.x < K) {
+        const int t = threadIdx.x;
+        double v = 0.0;
+#pragma unroll
+        for (int w = 0; w < GW; w++) v += part[w][t];
+        const int a = a0 + t;
+        if (a < ncon && a <= b) {
+            const int ca = con[a], cb = con[b];
+            M[(long long)ca + (long long)cb * m] += v;
+            if (ca != cb) M[(long long)cb + (long long)ca * m] += v;
+        }
+    }
+}
+
+// S[(u K) + t] = A_a[p, q] + A_a[q, p] for the upper entries of constraint a = a0 + t (the Gram
+// matrix's "G_a" is A_a itself)
+__global__ void gram_scatter_kernel(int K, int a0, int ncon, const long long *__restrict__ uptr,
+                                    const int *__restrict__ upos, const double *__restrict__ uval, double *S) {
+    const int t = blockIdx.y, a = a0 + t;
+    if (a >= ncon) return;
+    for (long long e = uptr[a] + (long long)blockIdx.x * blockDim.x + threadIdx.x; e < uptr[a + 1];
+         e += (long long)gridDim.x * blockDim.x) {
+        const long long u = upos[e];
+        long long q = (long long)((sqrt(8.0 * (double)u + 1.0) - 1.0) * 0.5);
+        while (q * (q + 1) / 2 > u) q--;
+        while ((q + 1) * (q + 2) / 2 <= u) q++;
+        const long long p = u - q * (q + 1) / 2;
+        S[u * K + t] = (p == q) ? uval[e] : 2.0 * uval[e];
+    }
+}
+
+__global__ void upper_count_kernel(int n, int ncon, const long long *__restrict__ cptr, const int *__restrict__ cpos,
+                                   int *counts) {
+    __shared__ int wsum[8];
+    const int t = blockIdx.x;
+    if (t >= ncon) return;
+    int c = 0;
+    for (long long e = cptr[t] + threadIdx.x; e < cptr[t + 1]; e += blockDim.x) {
+        const int pos = cpos[e], q = pos / n, p = pos - q * n;
+        c += p <= q;
+    }
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int tot = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) tot += wsum[w];
+        counts[t] = tot;
+    }
+}
+
+// uptr = exclusive scan of counts (one CTA of 1024 threads, each a contiguous range)
+__global__ void __launch_bounds__(1024) upper_scan_kernel(int ncon, const int *__restrict__ counts, long long *uptr) {
+    __shared__ long long part[1024];
+    const int tid = threadIdx.x;
+    const int per = (ncon + 1023) / 1024;
+    const int lo = min(ncon, tid * per), hi = min(ncon, lo + per);
+    long long s = 0;
+    for (int i = lo; i < hi; i++) s += counts[i];
+    part[tid] = s;
+    __syncthreads();
+    if (tid == 0) {
+        long long run = 0;
+        for (int w = 0; w < 1024; w++) { const long long v = part[w]; part[w] = run; run += v; }
+        uptr[ncon] = run;
+    }
+    __syncthreads();
+    long long run = part[tid];
+    for (int i = lo; i < hi; i++) { uptr[i] = run; run += counts[i]; }
+}
+
+// order-preserving compaction of each constraint's entries p <= q (one CTA of 256 per constraint)
+__global__ void __launch_bounds__(256) upper_fill_kernel(int n, int ncon, const long long *__restrict__ cptr,
+                                                         const int *__restrict__ cpos,
+                                                         const double *__restrict__ cval,
+                                                         const long long *__restrict__ uptr, int *upos, double *uval) {
+    __shared__ int wcount[8];
+    __shared__ long long base_s;
+    const int t = blockIdx.x;
+    if (t >= ncon) return;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) base_s = uptr[t];
+    __syncthreads();
+    for (long long e0 = cptr[t]; e0 < cptr[t + 1]; e0 += 256) {
+        const long long e = e0 + threadIdx.x;
+        int p = 1, q = 0, pos = 0;
+        if (e < cptr[t + 1]) { pos = cpos[e]; q = pos / n; p = pos - q * n; }
+        const bool keep = e < cptr[t + 1] && p <= q;
+        const unsigned mask = __ballot_sync(0xffffffffu, keep);
+        if (lane == 0) wcount[warp] = __popc(mask);
+        __syncthreads();
+        long long off = base_s;
+        for (int w = 0; w < warp; w++) off += wcount[w];
+        off += __popc(mask & ((1u << lane) - 1u));
+        if (keep) {
+            upos[off] = (int)upk(p, q);
+            uval[off] = cval[e];
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            long long tot = 0;
+            for (int w = 0; w < 8; w++) tot += wcount[w];
+            base_s += tot;
+        }
+        __syncthreads();
+    }
+}
+
+template <typename GT>
+int sym_pack_launch(cudaStream_t st, int K, int n, const GT *G, GT *S) {
+    const int NV = K / Vec16<GT>::N;
+    dim3 grid(ceil_div((long long)n * NV, 256), n);
+    switch (K) {
+        case 8: sym_pack_kernel<GT, 8><<<grid, 256, 0, st>>>(n, G, S); break;
+        case 16: sym_pack_kernel<GT, 16><<<grid, 256, 0, st>>>(n, G, S); break;
+        case 32: sym_pack_kernel<GT, 32><<<grid, 256, 0, st>>>(n, G, S); break;
+        case 64: sym_pack_kernel<GT, 64><<<grid, 256, 0, st>>>(n, G, S); break;
+        default: return BGPU_ERR_ARG;
+    }
+    BGPU_LAUNCH_CHECK();
+    return BGPU_OK;
+}
+
+template <typename GT>
+int gather_sym_launch(cudaStream_t st, int K, int a0, int ncon, int m, const DevBlock &B, const GT *S, double *M) {
+    const int nb = ncon - a0;
+    if (nb <= 0) return BGPU_OK;
+    dim3 grid(nb);
+    switch (K) {
+        case 8: gather_sym_kernel<8, GT><<<grid, GW * 32, 0, st>>>(a0, ncon, m, B.con, B.uptr, B.upos, B.uval, S, M); break;
+        case 16: gather_sym_kernel<16, GT><<<grid, GW * 32, 0, st>>>(a0, ncon, m, B.con, B.uptr, B.upos, B.uval, S, M); break;
+        case 32: gather_sym_kernel<32, GT><<<grid, GW * 32, 0, st>>>(a0, ncon, m, B.con, B.uptr, B.upos, B.uval, S, M); break;
+        case 64: gather_sym_kernel<64, GT><<<grid, GW * 32, 0, st>>>(a0, ncon, m, B.con, B.uptr, B.upos, B.uval, S, M); break;
+        default: return BGPU_ERR_ARG;
+    }
+    BGPU_LAUNCH_CHECK();
+    return BGPU_OK;
+}
+
 template <typename GT>
 int gather_launch(cudaStream_t st, int K, int a0, int ncon, int m, const DevBlock &B, const GT *G, double *M) {
     const int nb = ncon - a0;
@@ -283,7 +522,12 @@ int schur_assemble(cudaStream_t st, const DevBlock &B, const double *X, const do
             BGPU_LAUNCH_CHECK();
             int rc = gemm_f64(st, 1, 1, n * K, n, n, 1.0, T, n, 0, X, n, 0, 0.0, G, (long long)n * K, 0, 1, 0);
             if (rc) return rc;
-            rc = gather_launch<double>(st, K, a0, B.ncon, m, B, G, M);
+            if (B.upos) {   // T is free again: it takes the packed symmetric sum
+                if ((rc = sym_pack_launch<double>(st, K, n, G, T))) return rc;
+                rc = gather_sym_launch<double>(st, K, a0, B.ncon, m, B, T, M);
+            } else {
+                rc = gather_launch<double>(st, K, a0, B.ncon, m, B, G, M);
+            }
             if (rc) return rc;
         }
         return BGPU_OK;
@@ -306,7 +550,50 @@ int schur_assemble(cudaStream_t st, const DevBlock &B, const double *X, const do
         BGPU_LAUNCH_CHECK();
         int rc = gemm_tf32x3(st, n * K, n, n, Th, Tl, ld, Xh, Xl, ld, G, (long long)n * K);
         if (rc) return rc;
-        rc = gather_launch<float>(st, K, a0, B.ncon, m, B, G, M);
+        if (B.upos) {
+            if ((rc = sym_pack_launch<float>(st, K, n, G, Th))) return rc;
+            rc = gather_sym_launch<float>(st, K, a0, B.ncon, m, B, Th, M);
+        } else {
+            rc = gather_launch<float>(st, K, a0, B.ncon, m, B, G, M);
+        }
+        if (rc) return rc;
+    }
+    return BGPU_OK;
+}
+
+int schur_upper_ptr(cudaStream_t st, const DevBlock &B, int *counts) {
+    if (B.ncon <= 0) return BGPU_OK;
+    if (!B.uptr || !counts) return BGPU_ERR_ARG;
+    upper_count_kernel<<<B.ncon, 256, 0, st>>>(B.n, B.ncon, B.cptr, B.cpos, counts);
+    BGPU_LAUNCH_CHECK();
+    upper_scan_kernel<<<1, 1024, 0, st>>>(B.ncon, counts, B.uptr);
+    BGPU_LAUNCH_CHECK();
+    return BGPU_OK;
+}
+
+int schur_upper(cudaStream_t st, const DevBlock &B) {
+    if (B.ncon <= 0) return BGPU_OK;
+    if (!B.uptr || !B.upos || !B.uval) return BGPU_ERR_ARG;
+    upper_fill_kernel<<<B.ncon, 256, 0, st>>>(B.n, B.ncon, B.cptr, B.cpos, B.cval, B.uptr, B.upos, B.uval);
+    BGPU_LAUNCH_CHECK();
+    return BGPU_OK;
+}
+
+int schur_assemble_gram(cudaStream_t st, const DevBlock &B, double *M, int m, void *ws, size_t ws_bytes) {
+    const int n = B.n, ncon = B.ncon;
+    if (ncon <= 0) return BGPU_OK;
+    if (!B.upos || !B.uptr || !B.uval) return BGPU_ERR_ARG;
+    if (((uintptr_t)ws & 15) != 0) return BGPU_ERR_ARG;
+    const size_t npk = (size_t)n * (n + 1) / 2;
+    int K = 64;   // the widest chunk whose packed S fits the workspace and stays L2-resident (64 MB)
+    while (K > 8 && (npk * K * sizeof(double) > ws_bytes || npk * K * sizeof(double) > 64e6)) K >>= 1;
+    if (npk * K * sizeof(double) > ws_bytes) return BGPU_ERR_ARG;
+    double *S = (double *)ws;
+    for (int a0 = 0; a0 < ncon; a0 += K) {
+        BGPU_CHECK(cudaMemsetAsync(S, 0, npk * K * sizeof(double), st));
+        gram_scatter_kernel<<<dim3(16, K), 256, 0, st>>>(K, a0, ncon, B.uptr, B.upos, B.uval, S);
+        BGPU_LAUNCH_CHECK();
+        int rc = gather_sym_launch<double>(st, K, a0, ncon, m, B, S, M);
         if (rc) return rc;
     }
     return BGPU_OK;

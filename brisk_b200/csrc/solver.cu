@@ -539,6 +539,19 @@ void Solver::upload_block(int k) {
     CU(cudaMemcpyAsync(d.cpos, B.cpos.data(), sizeof(int) * d.ne, cudaMemcpyHostToDevice, g.st));
     CU(cudaMemcpyAsync(d.cval, B.cval.data(), sizeof(double) * d.ne, cudaMemcpyHostToDevice, g.st));
     RC(schur_colptr(g.st, d));
+    // upper-triangle lists for the packed symmetric gather and the Gram matrix
+    if (d.ncon > 0) {
+        d.uptr = g.alloc<long long>(d.ncon + 1);
+        int *cnt = g.alloc<int>(d.ncon);
+        if (!d.uptr || !cnt) throw GpuFail{BGPU_ERR_NOMEM, __LINE__};
+        RC(schur_upper_ptr(g.st, d, cnt));
+        CU(cudaMemcpyAsync(&d.nu, d.uptr + d.ncon, sizeof(long long), cudaMemcpyDeviceToHost, g.st));
+        CU(cudaStreamSynchronize(g.st));
+        d.upos = g.alloc<int>(d.nu);
+        d.uval = g.alloc<double>(d.nu);
+        if (!d.upos || !d.uval) throw GpuFail{BGPU_ERR_NOMEM, __LINE__};
+        RC(schur_upper(g.st, d));
+    }
     // the dense route: constraints averaging >= 2 % of the n^2 entries (the reference's dense
     // candidates, problem.c:1299), n >= 8, and their dense copies within 8 GB
     {
@@ -1061,7 +1074,7 @@ void Solver::least_squares_start(std::vector<double> &y) {
     for (int k = 0; k < nb; k++) {
         RC(ew_set_scaled_identity(g.st, db[k].n, da[k].T, 1.0));
         if (dense_route[k]) RC(schur_assemble_dense(g.st, db[k], da[k].T, da[k].T, M, m, 0, chunk_fp64(k), ws, ws_bytes));
-        else RC(schur_assemble(g.st, db[k], da[k].T, da[k].T, M, m, 0, chunk_fp64(k), ws, ws_bytes));
+        else RC(schur_assemble_gram(g.st, db[k], M, m, ws, ws_bytes));
     }
     const int frc = factor();
     allow_float = af;

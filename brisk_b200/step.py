@@ -35,6 +35,9 @@ def lib():
         "bgpu_schur_chunk_default": ([I, I], I),
         "bgpu_schur_colptr": ([I, I, P, P, P, P], I),
         "bgpu_schur_assemble": ([I, I, I, P, P, P, P, P, P, P, P, I, I, P, SZ, P], I),
+        "bgpu_schur_upper": ([I, I, P, P, P, P, P, P, P, P, P], I),
+        "bgpu_schur_assemble_sym": ([I, I, I, P, P, P, P, P, P, P, P, P, P, P, I, I, P, SZ, P], I),
+        "bgpu_schur_gram": ([I, I, I, P, P, P, P, P, P, SZ, P], I),
         "bgpu_schur_dense_ws_bytes": ([I, I, I, I], SZ),
         "bgpu_schur_densify": ([I, I, P, P, P, P, P], I),
         "bgpu_schur_assemble_dense": ([I, I, I, P, P, P, P, P, P, P, P, P, I, I, P, SZ, P], I),

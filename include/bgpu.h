@@ -88,6 +88,30 @@ BGPU_API int bgpu_schur_assemble(int n, int m, int ncon, const int *d_con, const
                                  const double *d_Zi, double *d_M, int precision, int chunk, void *d_ws,
                                  size_t ws_bytes, void *stream);
 
+/* Upper-triangle entry lists of the block's constraints for the packed symmetric gather:
+ * entries p <= q of each constraint's full list, packed index u = q (q+1)/2 + p (ascending),
+ * value A[p, q].  Fills d_uptr (ncon+1 offsets; d_counts is ncon ints of scratch) and *nu (the
+ * total; the call synchronises on the stream); with d_upos and d_uval (nu each) non-NULL it
+ * also fills them.  The reference keeps both triangles of each constraint (problem.c:1570-1610);
+ * these lists are this build's own layout. */
+BGPU_API int bgpu_schur_upper(int n, int ncon, const long long *d_cptr, const int *d_cpos, const double *d_cval,
+                              int *d_counts, long long *d_uptr, int *d_upos, double *d_uval, long long *nu,
+                              void *stream);
+/* bgpu_schur_assemble with the packed symmetric gather: each chunk's G is folded into
+ * G + G' on the upper triangle and every constraint's upper entries are read once (half the
+ * entries and G values of the full gather; the same M up to rounding). */
+BGPU_API int bgpu_schur_assemble_sym(int n, int m, int ncon, const int *d_con, const long long *d_cptr,
+                                     const int *d_ccol, const int *d_cpos, const double *d_cval,
+                                     const long long *d_uptr, const int *d_upos, const double *d_uval,
+                                     const double *d_X, const double *d_Zi, double *d_M, int precision, int chunk,
+                                     void *d_ws, size_t ws_bytes, void *stream);
+/* M[con_a, con_b] += <A_a, A_b> for the block's constraints (the Gram matrix A A' of the
+ * least-squares start, solver.c:13939-14198, which the reference assembles as the Schur
+ * complement at X = Z = I): no products, the constraints' entries are scattered and gathered.
+ * d_ws holds the packed chunk (n(n+1)/2 x K doubles, K the widest of 64..8 that fits). */
+BGPU_API int bgpu_schur_gram(int n, int m, int ncon, const int *d_con, const long long *d_uptr, const int *d_upos,
+                             const double *d_uval, double *d_M, void *d_ws, size_t ws_bytes, void *stream);
+
 /* The dense route (the reference's route 2, solver.c:2972-3021) for blocks of dense constraints:
  * bgpu_schur_densify writes the constraints as dense matrices (d_Ad: ncon * n*n doubles, row t
  * the column-major A_t); bgpu_schur_assemble_dense then forms G_a = X A_a Zi per chunk of

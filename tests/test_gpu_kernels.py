@@ -1,6 +1,8 @@
 """Kernel parity through the C ABI (include/bgpu.h) on a B200: each kernel against the oracle
 (oracle/restate.py) or a plain FP64 reference of the same operation.  Device memory comes from
 torch (allocation only); every compute call goes through libbrisk.so."""
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -208,6 +210,90 @@ def test_first_schur_matches_oracle_at_start(cuda, golden):
     got = M.cpu().numpy().reshape(d.m, d.m).T
     rel = np.abs(got - want).max() / np.abs(want).max()
     assert rel <= 1e-10
+
+
+def upper_arrays(a, n, cuda):
+    """The upper-triangle lists of bgpu_schur_upper (count call, then fill call)."""
+    ncon = int(a["con"].numel())
+    counts = torch.zeros(max(ncon, 1), dtype=torch.int32, device=cuda)
+    uptr = torch.zeros(ncon + 1, dtype=torch.int64, device=cuda)
+    nu = ctypes.c_longlong(0)
+    step.call("schur_upper", n, ncon, a["cptr"].data_ptr(), a["cpos"].data_ptr(), a["cval"].data_ptr(),
+              counts.data_ptr(), uptr.data_ptr(), None, None, ctypes.addressof(nu), None)
+    upos = torch.zeros(max(nu.value, 1), dtype=torch.int32, device=cuda)
+    uval = torch.zeros(max(nu.value, 1), dtype=torch.float64, device=cuda)
+    step.call("schur_upper", n, ncon, a["cptr"].data_ptr(), a["cpos"].data_ptr(), a["cval"].data_ptr(),
+              counts.data_ptr(), uptr.data_ptr(), upos.data_ptr(), uval.data_ptr(), ctypes.addressof(nu), None)
+    step.call("sync", None)
+    return dict(uptr=uptr, upos=upos, uval=uval, nu=nu.value)
+
+
+def test_upper_lists_match_numpy(cuda):
+    """Entries p <= q of each constraint, packed index q (q+1)/2 + p ascending, same values."""
+    d = problems.random_sdp(n=60, m=200, density=0.05, seed=2)
+    S, n, a = block_arrays(d, cuda)
+    u = upper_arrays(a, n, cuda)
+    cptr, cpos, cval = (a[k].cpu().numpy() for k in ("cptr", "cpos", "cval"))
+    uptr, upos, uval = u["uptr"].cpu().numpy(), u["upos"].cpu().numpy()[:u["nu"]], u["uval"].cpu().numpy()[:u["nu"]]
+    want_ptr, want_pos, want_val = [0], [], []
+    for t in range(len(cptr) - 1):
+        pos = cpos[cptr[t]:cptr[t + 1]]
+        q, p = pos // n, pos % n
+        keep = p <= q
+        want_pos.extend((q[keep] * (q[keep] + 1) // 2 + p[keep]).tolist())
+        want_val.extend(cval[cptr[t]:cptr[t + 1]][keep].tolist())
+        want_ptr.append(len(want_pos))
+    np.testing.assert_array_equal(uptr, want_ptr)
+    np.testing.assert_array_equal(upos, want_pos)
+    np.testing.assert_array_equal(uval, want_val)
+    assert all(np.all(np.diff(upos[uptr[t]:uptr[t + 1]]) > 0) for t in range(len(uptr) - 1))
+
+
+@pytest.mark.parametrize("name,kw,chunk", [
+    ("rand30", dict(n=30, m=60, density=0.1, seed=1), 8),
+    ("rand60", dict(n=60, m=200, density=0.05, seed=2), 32),
+    ("rand100", dict(n=100, m=300, density=0.02, seed=3), 64),
+    ("theta50", None, 16),
+])
+def test_schur_sym_gather_matches_oracle(cuda, name, kw, chunk):
+    """The packed symmetric gather (G + G' on the upper triangle, upper entries only): FP64 M to
+    1e-10 of the oracle; the 3xTF32 one to 1e-5 of the FP64 one."""
+    d = problems.theta_problem() if kw is None else problems.random_sdp(**kw)
+    S, n, a = block_arrays(d, cuda)
+    u = upper_arrays(a, n, cuda)
+    X = spd(n, 5, cond=100)
+    Zi = spd(n, 6, cond=100)
+    want = restate.schur(S.A, [X], [Zi])
+    dX, dZi = colmajor(X, cuda), colmajor(Zi, cuda)
+    got = []
+    for prec in (0, 1):
+        M = torch.zeros(d.m * d.m, dtype=torch.float64, device=cuda)
+        ws = torch.empty(step.ws_bytes(n, chunk, prec), dtype=torch.uint8, device=cuda)
+        step.call("schur_assemble_sym", n, d.m, int(a["con"].numel()), a["con"].data_ptr(), a["cptr"].data_ptr(),
+                  a["ccol"].data_ptr(), a["cpos"].data_ptr(), a["cval"].data_ptr(), u["uptr"].data_ptr(),
+                  u["upos"].data_ptr(), u["uval"].data_ptr(), dX.data_ptr(), dZi.data_ptr(), M.data_ptr(), prec,
+                  chunk, ws.data_ptr(), ws.numel(), None)
+        step.call("sync", None)
+        got.append(M.cpu().numpy().reshape(d.m, d.m).T)
+    np.testing.assert_allclose(got[0], want, rtol=1e-10, atol=1e-12 * np.abs(want).max())
+    assert np.abs(got[1] - got[0]).max() / np.abs(got[0]).max() <= 1e-5
+
+
+@pytest.mark.parametrize("kw", [dict(n=60, m=200, density=0.05, seed=2), dict(n=100, m=300, density=0.02, seed=3)])
+def test_gram_matches_numpy(cuda, kw):
+    """bgpu_schur_gram: <A_a, A_b> of the scaled constraints, to 1e-13 relative."""
+    d = problems.random_sdp(**kw)
+    S, n, a = block_arrays(d, cuda)
+    u = upper_arrays(a, n, cuda)
+    Af = np.stack([A.ravel() for A in S.A[0]])
+    want = Af @ Af.T
+    M = torch.zeros(d.m * d.m, dtype=torch.float64, device=cuda)
+    ws = torch.empty(step.ws_bytes(n, 0, 0), dtype=torch.uint8, device=cuda)
+    step.call("schur_gram", n, d.m, int(a["con"].numel()), a["con"].data_ptr(), u["uptr"].data_ptr(),
+              u["upos"].data_ptr(), u["uval"].data_ptr(), M.data_ptr(), ws.data_ptr(), ws.numel(), None)
+    step.call("sync", None)
+    got = M.cpu().numpy().reshape(d.m, d.m).T
+    np.testing.assert_allclose(got, want, rtol=1e-13, atol=1e-13 * np.abs(want).max())
 
 
 def test_aop_and_symv(cuda):
