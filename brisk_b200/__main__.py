@@ -14,6 +14,8 @@ WORKLOADS = {
     "theta50": lambda: problems.theta_problem(n=50, p=0.5, seed=1),
     "rand400": lambda: problems.random_sdp(n=400, m=2000, density=0.01, seed=0),
     "rand1000": lambda: problems.random_sdp(n=1000, m=8000, density=0.005, seed=0),
+    "mom60": lambda: problems.moment_relaxation(nvars=60, clique=4, seed=0),
+    "mom700": lambda: problems.moment_relaxation(nvars=700, clique=4, seed=0),
 }
 
 

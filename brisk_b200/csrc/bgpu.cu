@@ -4,6 +4,7 @@
 #include "kernels.h"
 #include "tf32x3.h"
 #include "small.h"
+#include "sparse.h"
 
 long long g_bgpu_launches = 0;
 static cudaStream_t S(void *s) { return (cudaStream_t)s; }
@@ -212,6 +213,100 @@ BGPU_API int bgpu_small_gemm(int nb, const int *d_n, int ta, int tb, double alph
                              const double *const *d_B, double beta, double *const *d_C, int sym, void *stream) {
     if (nb < 0) return BGPU_ERR_ARG;
     return small_gemm(S(stream), nb, d_n, ta, tb, alpha, d_A, d_B, beta, d_C, sym);
+}
+
+struct bgpu_schol {
+    schol::Analysis A;
+    schol::Factor F;
+    void *buf = nullptr;
+    bool bound = false;
+};
+
+BGPU_API bgpu_schol *bgpu_schol_analyze(int m, int ncliques, const int64_t *clq_ptr, const int *clq_idx, int *rc) {
+    int code = BGPU_OK;
+    bgpu_schol *h = nullptr;
+    if (m < 0 || ncliques < 0 || (ncliques > 0 && (!clq_ptr || !clq_idx))) code = BGPU_ERR_ARG;
+    if (!code) {
+        std::vector<std::vector<int>> cl(ncliques);
+        for (int c = 0; c < ncliques; c++) {
+            if (clq_ptr[c + 1] < clq_ptr[c]) { code = BGPU_ERR_ARG; break; }
+            cl[c].assign(clq_idx + clq_ptr[c], clq_idx + clq_ptr[c + 1]);
+        }
+        if (!code) {
+            h = new (std::nothrow) bgpu_schol;
+            if (!h) code = BGPU_ERR_NOMEM;
+            else if (schol::analyze(m, cl, h->A)) { delete h; h = nullptr; code = BGPU_ERR_ARG; }
+        }
+    }
+    if (rc) *rc = code;
+    return h;
+}
+
+BGPU_API int bgpu_schol_info(const bgpu_schol *h, double *out8) {
+    if (!h || !out8) return BGPU_ERR_ARG;
+    out8[0] = h->A.nsup;
+    out8[1] = h->A.nnz;
+    out8[2] = h->A.flops;
+    out8[3] = h->A.fmax;
+    out8[4] = h->A.lvptr.empty() ? 0 : (double)(h->A.lvptr.size() - 1);
+    out8[5] = (double)h->A.pattern;
+    out8[6] = h->A.m;
+    out8[7] = (double)schol::factor_bytes(h->A);
+    return BGPU_OK;
+}
+
+BGPU_API int bgpu_schol_perm(const bgpu_schol *h, int *perm) {
+    if (!h || !perm) return BGPU_ERR_ARG;
+    std::copy(h->A.perm.begin(), h->A.perm.end(), perm);
+    return BGPU_OK;
+}
+
+BGPU_API int bgpu_schol_supernodes(const bgpu_schol *h, int *sfirst, int *parent, int64_t *rptr, int *rows) {
+    if (!h) return BGPU_ERR_ARG;
+    const auto &A = h->A;
+    if (sfirst) std::copy(A.sfirst.begin(), A.sfirst.end(), sfirst);
+    if (parent) std::copy(A.parent.begin(), A.parent.end(), parent);
+    if (rptr) for (size_t s = 0; s < A.rptr.size(); s++) rptr[s] = A.rptr[s];
+    if (rows) std::copy(A.rows.begin(), A.rows.end(), rows);
+    return BGPU_OK;
+}
+
+BGPU_API int bgpu_schol_factor(bgpu_schol *h, const double *d_M, int64_t ldm, const double *d_D, double reg,
+                               int *info, double *pmin, void *stream) {
+    if (!h || !d_M || !d_D || ldm < h->A.m) return BGPU_ERR_ARG;
+    if (!h->bound) {
+        const size_t b = schol::factor_bytes(h->A);
+        if (cudaMalloc(&h->buf, b) != cudaSuccess) { h->buf = nullptr; return BGPU_ERR_NOMEM; }
+        int rc = schol::factor_bind(S(stream), h->A, h->buf, h->F);
+        if (rc) return rc;
+        h->bound = true;
+    }
+    int rc = schol::factor(S(stream), h->F, d_M, ldm, d_D, reg);
+    if (rc) return rc;
+    if (info || pmin) {
+        int i = 0;
+        double p = 0;
+        BGPU_CHECK(cudaMemcpyAsync(&i, h->F.info, sizeof(int), cudaMemcpyDeviceToHost, S(stream)));
+        BGPU_CHECK(cudaMemcpyAsync(&p, h->F.pmin, sizeof(double), cudaMemcpyDeviceToHost, S(stream)));
+        BGPU_CHECK(cudaStreamSynchronize(S(stream)));
+        if (info) *info = i;
+        if (pmin) *pmin = p;
+    }
+    return BGPU_OK;
+}
+
+BGPU_API int bgpu_schol_solve(bgpu_schol *h, const double *d_D, double *d_x, void *stream) {
+    if (!h || !h->bound || !d_D || !d_x) return BGPU_ERR_ARG;
+    return schol::solve(S(stream), h->F, d_D, d_x);
+}
+
+BGPU_API void bgpu_schol_destroy(bgpu_schol *h) {
+    if (!h) return;
+    if (h->buf) {
+        cudaDeviceSynchronize();
+        cudaFree(h->buf);
+    }
+    delete h;
 }
 
 }  // extern "C"

@@ -170,7 +170,13 @@ int parse_options(int argc, const char *const *argv, Options &opt, std::string &
             opt.verbose = 3;
         } else if (a == "-nohsd" || a == "-nofr" || a == "-feasible") {
             if (a == "-feasible") opt.known_feasible = 1;
-        } else if (a == "-hsd" || a == "-sparse" || a == "-threads" || a == "-chordal" || a == "-sym" ||
+        } else if (a == "-sparse") {
+            const char *s = need("-1, 0 or 1");
+            if (!s || !parse_int(s, opt.sparse) || opt.sparse < -1 || opt.sparse > 1) {
+                if (err.empty()) err = "bad -sparse (-1 auto, 0 dense, 1 sparse)";
+                return 1;
+            }
+        } else if (a == "-hsd" || a == "-threads" || a == "-chordal" || a == "-sym" ||
                    a == "-symalg" || a == "-deprows" || a == "-caller" || a == "-corr" || a == "-mixedfrac") {
             // options of the reference that take a value and do not change this path's arithmetic
             if (!need("a value")) return 1;

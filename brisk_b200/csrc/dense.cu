@@ -440,6 +440,12 @@ int schur_load_f64(cudaStream_t st, int m, const double *M, long long ldm, doubl
     return BGPU_OK;
 }
 
+int schur_diag_scale(cudaStream_t st, int m, const double *M, long long ldm, double *d_D) {
+    diag_scale_kernel<<<ceil_div(m, 256), 256, 0, st>>>(m, M, ldm, d_D);
+    BGPU_LAUNCH_CHECK();
+    return BGPU_OK;
+}
+
 int schur_load_f32(cudaStream_t st, int m, const double *M, long long ldm, double *d_D, float *Mf, long long ldf) {
     diag_scale_kernel<<<ceil_div(m, 256), 256, 0, st>>>(m, M, ldm, d_D);
     BGPU_LAUNCH_CHECK();

@@ -40,6 +40,8 @@ int symv_full_f64(cudaStream_t st, int n, double alpha, const double *M, long lo
 
 // Equilibrated copy for the factor: L = D M D + reg I (lower triangle; D = diag(M)^{-1/2},
 // computed here into d_D), and the float variant writing Mf.
+// d_D = diag(M)^-1/2 (1 where the diagonal is not positive).
+int schur_diag_scale(cudaStream_t st, int m, const double *M, long long ldm, double *d_D);
 int schur_load_f64(cudaStream_t st, int m, const double *M, long long ldm, double reg, double *d_D, double *L,
                    long long ldl);
 int schur_load_f32(cudaStream_t st, int m, const double *M, long long ldm, double *d_D, float *Mf, long long ldf);

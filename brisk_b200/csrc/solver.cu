@@ -22,6 +22,7 @@
 #include "kernels.h"
 #include "small.h"
 #include "solver.h"
+#include "sparse.h"
 #include "tf32x3.h"
 
 #include <algorithm>
@@ -436,6 +437,11 @@ class Solver {
     std::vector<char> dense_route;   // per block: the dense Schur route (Ad resident)
     // Schur complement
     double *M = nullptr, *Lm = nullptr, *dinvM = nullptr, *Dsc = nullptr;
+    // the supernodal sparse factor of M (use_sparse): symbolic analysis and device factor
+    bool use_sparse = false;
+    schol::Analysis sp_an;
+    schol::Factor sp_f;
+    void choose_sparse();
     float *Mf = nullptr, *dinvMf = nullptr;
     int *mflags = nullptr, *d_info = nullptr, *d_err = nullptr;
     double *d_pmin = nullptr;
@@ -668,9 +674,10 @@ void Solver::setup() {
     CU(cudaMemsetAsync(d_err, 0, sizeof(int), g.st));
     h_dots = g.host_alloc<double>(16);
     if (!h_dots) throw GpuFail{BGPU_ERR_NOMEM, __LINE__};
-    allow_float = opt.mixed > 0 || (opt.mixed < 0 && m >= 1000);
+    choose_sparse();
+    allow_float = !use_sparse && (opt.mixed > 0 || (opt.mixed < 0 && m >= 1000));
     asm_prec = opt.asm_prec < 0 ? 0 : opt.asm_prec;
-    if (asm_prec == 1) allow_float = true;   // the 3xTF32 path factors in FP32 until mu_switch
+    if (asm_prec == 1 && !use_sparse) allow_float = true;   // the 3xTF32 path factors in FP32 until mu_switch
     if (allow_float) {
         Mf = g.alloc<float>(mm);
         dinvMf = g.alloc<float>((size_t)mb64 * TRI_NB * TRI_NB);
@@ -685,6 +692,44 @@ void Solver::setup() {
                                                    schur_dense_ws_bytes(db[k].n, db[k].ncon, chunk64, 0)));
     ws = g.alloc<unsigned char>(ws_bytes);
     if (!ws) throw GpuFail{BGPU_ERR_NOMEM, __LINE__};
+}
+
+// sparse_build (solver.c:4014-4100): the pattern of M is the union of the blocks' constraint
+// cliques.  -sparse 1 takes the sparse factor whenever the analysis succeeds; the automatic choice
+// (-sparse -1) keeps the reference's caps: m >= 200, the largest clique and the pattern within
+// 0.45 m^2 (0.30 m^2 above m = 8000) of the lower triangle, and the factor's flops within
+// m^3/3 x 0.75 / 1.3.
+void Solver::choose_sparse() {
+    use_sparse = false;
+    if (opt.sparse == 0 || m <= 0 || (opt.sparse < 0 && m < 200)) return;
+    const double md = m;
+    const double cap = (m <= 8000 ? 0.45 : 0.30) * md * md + 1000;
+    std::vector<std::vector<int>> cl;
+    double cmax = 0;
+    for (auto &B : P.blk) {
+        cl.push_back(B.con);
+        cmax = std::max(cmax, (double)B.con.size());
+    }
+    if (opt.sparse < 0 && 0.5 * cmax * (cmax + 1) > cap) return;
+    const double t0 = wtime();
+    if (schol::analyze(m, cl, sp_an)) return;
+    const double fcap = md * md * md / 3.0 * 0.75 / 1.3;
+    if (opt.sparse < 0 && ((double)sp_an.pattern > cap || sp_an.flops > fcap)) {
+        if (opt.verbose > 1)
+            log_printf(0, "   [Schur pattern: %.3g entries below the diagonal, sparse factor %.3g flops: dense factor]\n",
+                       (double)sp_an.pattern, sp_an.flops);
+        sp_an = schol::Analysis();
+        return;
+    }
+    void *buf = g.alloc<unsigned char>(schol::factor_bytes(sp_an));
+    if (!buf) throw GpuFail{BGPU_ERR_NOMEM, __LINE__};
+    RC(schol::factor_bind(g.st, sp_an, buf, sp_f));
+    CU(cudaStreamSynchronize(g.st));
+    use_sparse = true;
+    if (opt.verbose > 1)
+        log_printf(0, "   [Schur pattern: sparse Cholesky, %.0f nonzeros in L, %.1e flops, %d supernodes, largest front %d, "
+                   "%d levels (%.3fs)]\n", sp_an.nnz, sp_an.flops, sp_an.nsup, sp_an.fmax,
+                   (int)sp_an.lvptr.size() - 1, wtime() - t0);
 }
 
 void Solver::aop_all(const std::vector<double *> &D, std::vector<double> &out) {
@@ -791,6 +836,32 @@ int Solver::factor() {
         want_double = true;
     }
     is_float = false;
+    if (use_sparse) {
+        RC(schur_diag_scale(g.st, m, M, m, Dsc));
+        double r = reg_hint ? std::max(reg_floor, 0.01 * reg_ok) : 0.0;
+        int info = 0;
+        for (int attempt = 0; attempt < 10; attempt++) {
+            RC(schol::factor(g.st, sp_f, M, m, Dsc, r));
+            double pmin = 0;
+            CU(cudaMemcpyAsync(&info, sp_f.info, sizeof(int), cudaMemcpyDeviceToHost, g.st));
+            CU(cudaMemcpyAsync(&pmin, sp_f.pmin, sizeof(double), cudaMemcpyDeviceToHost, g.st));
+            CU(cudaStreamSynchronize(g.st));
+            if (info == 0) {
+                pmin = std::min(pmin, 1.0);
+                if (pmin >= opt.pivtol || r >= reg_floor) {
+                    reg = r;
+                    min_pivot = pmin;
+                    reg_hint = r > 0;
+                    reg_ok = r;
+                    return 0;
+                }
+                r = std::max(reg_floor, r * 100);
+                continue;
+            }
+            r = (r == 0) ? reg_first : r * 100;
+        }
+        return info ? info : 1;
+    }
     if (!Lm) {
         Lm = g.alloc<double>((size_t)m * m);
         if (!Lm) throw GpuFail{BGPU_ERR_NOMEM, __LINE__};
@@ -836,6 +907,11 @@ void Solver::prec(const std::vector<double> &rv, std::vector<double> &z) {
         CU(cudaMemcpyAsync(f.data(), fv, sizeof(float) * m, cudaMemcpyDeviceToHost, g.st));
         CU(cudaStreamSynchronize(g.st));
         for (int i = 0; i < m; i++) z[i] = (double)f[i] * Dh[i];
+    } else if (use_sparse) {
+        CU(cudaMemcpyAsync(dv_in, rv.data(), sizeof(double) * m, cudaMemcpyHostToDevice, g.st));
+        RC(schol::solve(g.st, sp_f, Dsc, dv_in));
+        CU(cudaMemcpyAsync(z.data(), dv_in, sizeof(double) * m, cudaMemcpyDeviceToHost, g.st));
+        CU(cudaStreamSynchronize(g.st));
     } else {
         for (int i = 0; i < m; i++) h[i] = rv[i] * Dh[i];
         CU(cudaMemcpyAsync(dv_in, h.data(), sizeof(double) * m, cudaMemcpyHostToDevice, g.st));

@@ -39,7 +39,8 @@ struct Options {
     double red_acc = 1e-6;
     int known_feasible = 0;
     int device = 0;
-    int sparse = -1;            // accepted for compatibility (dense Schur complement only)
+    int sparse = -1;            // Schur factor: -1 auto (the reference's caps, solver.c:4014-4100), 0 dense,
+                                // 1 supernodal sparse
     int init = 1;               // 0: SDPT3 start (start_sdpt3); 1: least-squares start (solver.c:13939-14198)
     int route = -1;             // Schur route per block: -1 auto (dense when the constraints average >= 2 % of
                                 // n^2 entries, problem.c:1299), 0 row-product, 1 dense

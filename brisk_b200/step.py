@@ -39,6 +39,13 @@ def lib():
         "bgpu_schur_assemble_sym": ([I, I, I, P, P, P, P, P, P, P, P, P, P, P, I, I, P, SZ, P], I),
         "bgpu_schur_gram": ([I, I, I, P, P, P, P, P, P, SZ, P], I),
         "bgpu_schur_dense_ws_bytes": ([I, I, I, I], SZ),
+        "bgpu_schol_analyze": ([I, I, P, P, P], P),
+        "bgpu_schol_info": ([P, P], I),
+        "bgpu_schol_perm": ([P, P], I),
+        "bgpu_schol_supernodes": ([P, P, P, P, P], I),
+        "bgpu_schol_factor": ([P, P, I64, P, D, P, P, P], I),
+        "bgpu_schol_solve": ([P, P, P, P], I),
+        "bgpu_schol_destroy": ([P], None),
         "bgpu_schur_densify": ([I, I, P, P, P, P, P], I),
         "bgpu_schur_assemble_dense": ([I, I, I, P, P, P, P, P, P, P, P, P, I, I, P, SZ, P], I),
         "bgpu_potrf": ([I, P, I, P, P, P, P], I),
@@ -78,3 +85,57 @@ def ws_bytes(n, chunk, precision):
 
 def chunk_default(n, precision):
     return int(lib().bgpu_schur_chunk_default(n, precision))
+
+
+class SparseCholesky:
+    """Handle of bgpu_schol_analyze (the symbolic phase runs on the host, no GPU needed)."""
+
+    def __init__(self, m, cliques):
+        import numpy as np
+        L = lib()
+        ptr = np.zeros(len(cliques) + 1, dtype=np.int64)
+        for c, cl in enumerate(cliques):
+            ptr[c + 1] = ptr[c] + len(cl)
+        idx = np.ascontiguousarray(np.concatenate([np.asarray(c, dtype=np.int32) for c in cliques])
+                                   if cliques else np.zeros(1, np.int32), dtype=np.int32)
+        rc = ctypes.c_int(0)
+        self.h = L.bgpu_schol_analyze(int(m), len(cliques), ptr.ctypes.data, idx.ctypes.data, ctypes.addressof(rc))
+        if not self.h:
+            raise BgpuError("schol_analyze", rc.value)
+        self.m = int(m)
+
+    def info(self):
+        import numpy as np
+        out = np.zeros(8)
+        call("schol_info", self.h, out.ctypes.data)
+        keys = ("nsup", "nnz", "flops", "fmax", "levels", "pattern", "m", "bytes")
+        return dict(zip(keys, out.tolist()))
+
+    def perm(self):
+        import numpy as np
+        p = np.zeros(self.m, dtype=np.int32)
+        call("schol_perm", self.h, p.ctypes.data)
+        return p
+
+    def supernodes(self):
+        """(sfirst, parent, rptr, rows) as numpy arrays."""
+        import numpy as np
+        ns = int(self.info()["nsup"])
+        sfirst = np.zeros(ns + 1, np.int32)
+        parent = np.zeros(max(ns, 1), np.int32)
+        rptr = np.zeros(ns + 1, np.int64)
+        call("schol_supernodes", self.h, sfirst.ctypes.data, parent.ctypes.data, rptr.ctypes.data, None)
+        rows = np.zeros(max(int(rptr[-1]), 1), np.int32)
+        call("schol_supernodes", self.h, None, None, None, rows.ctypes.data)
+        return sfirst, parent[:ns], rptr, rows[:int(rptr[-1])]
+
+    def close(self):
+        if self.h:
+            lib().bgpu_schol_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -193,6 +193,31 @@ BGPU_API int bgpu_aop(int n, int ncon, const int *d_con, const long long *d_cptr
                       const double *d_cval, const double *d_D, double alpha, double beta, double *d_out,
                       void *stream);
 
+/* Supernodal sparse Cholesky of the Schur complement (replaces sparse_build, solver.c:4014, and
+ * schol_analyze / schol_factor / schol_solve, sparsechol.c).  The pattern of M is the union of
+ * the cliques (the constraint sets of the blocks, clique c = clq_idx[clq_ptr[c] .. clq_ptr[c+1])).
+ * bgpu_schol_analyze orders it (minimum degree on the clique quotient graph) and finds the
+ * supernodes on the host (no GPU needed); *rc is 0 or a BGPU_ERR_ code.  bgpu_schol_info gives
+ * [0] supernodes [1] entries of L [2] factor flops [3] largest front [4] tree levels [5] pattern
+ * entries below the diagonal [6] m [7] device bytes of the factor.  bgpu_schol_perm gives the
+ * elimination order (perm[k] = constraint eliminated k-th); bgpu_schol_supernodes gives the
+ * supernodes' first positions (nsup+1), parents (-1 at a root), and the front rows (rptr nsup+1,
+ * rows: elimination positions), any of them NULL to skip.
+ * bgpu_schol_factor computes L L' = D M D + reg I on the pattern from the dense device M
+ * (m x m, both triangles, leading dimension ldm) and the scaling d_D (m), on the device; the
+ * first call allocates the factor's memory.  *info: 0 or the failing elimination position + 1;
+ * *pmin: the smallest pivot (either pointer may be NULL; the call then does not synchronise).
+ * bgpu_schol_solve: d_x := D (L L')^-1 D d_x. */
+typedef struct bgpu_schol bgpu_schol;
+BGPU_API bgpu_schol *bgpu_schol_analyze(int m, int ncliques, const int64_t *clq_ptr, const int *clq_idx, int *rc);
+BGPU_API int bgpu_schol_info(const bgpu_schol *h, double *out8);
+BGPU_API int bgpu_schol_perm(const bgpu_schol *h, int *perm);
+BGPU_API int bgpu_schol_supernodes(const bgpu_schol *h, int *sfirst, int *parent, int64_t *rptr, int *rows);
+BGPU_API int bgpu_schol_factor(bgpu_schol *h, const double *d_M, int64_t ldm, const double *d_D, double reg,
+                               int *info, double *pmin, void *stream);
+BGPU_API int bgpu_schol_solve(bgpu_schol *h, const double *d_D, double *d_x, void *stream);
+BGPU_API void bgpu_schol_destroy(bgpu_schol *h);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,95 @@
+"""The supernodal sparse Schur factor on a B200 (bgpu_schol_factor / bgpu_schol_solve): the
+factor of D M D + reg I on the clique pattern solves like numpy's dense solve, a matrix that is
+not positive definite is reported (no fault), and the moment relaxation solves to the
+reference's result with the sparse factor."""
+import ctypes
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+import brisk_b200  # noqa: E402
+from brisk_b200 import problems, step  # noqa: E402
+
+FP64 = ["-nohsd", "-dir", "hkm", "-mixed", "0", "-tol", "1e-7"]
+
+
+def cliques_of(d):
+    return [np.unique(d.mat[(d.blk == k) & (d.mat >= 1)] - 1).tolist() for k in range(1, d.nblk + 1)]
+
+
+def pattern_spd(m, cliques, seed, shift=1e-3):
+    """A symmetric positive definite matrix whose pattern is the union of the cliques."""
+    rng = np.random.default_rng(seed)
+    M = np.zeros((m, m))
+    for cl in cliques:
+        B = rng.standard_normal((len(cl), len(cl)))
+        M[np.ix_(cl, cl)] += B @ B.T / len(cl)
+    M += shift * np.eye(m)
+    return M
+
+
+def factor_solve(S, M, cuda, reg=0.0):
+    m = M.shape[0]
+    dM = torch.as_tensor(M.T.copy().ravel(), device=cuda)
+    D = 1.0 / np.sqrt(np.abs(np.diag(M)))
+    dD = torch.as_tensor(D, device=cuda)
+    info, pmin = ctypes.c_int(0), ctypes.c_double(0)
+    step.call("schol_factor", S.h, dM.data_ptr(), m, dD.data_ptr(), reg, ctypes.addressof(info),
+              ctypes.addressof(pmin), None)
+    return dM, dD, D, info.value, pmin.value
+
+
+@pytest.mark.parametrize("name,nv", [("mom8", 8), ("mom60", 60)])
+def test_sparse_factor_solves_like_dense(cuda, name, nv):
+    d = problems.moment_relaxation(nvars=nv, clique=4, seed=1 if nv == 8 else 0)
+    cl = cliques_of(d)
+    S = step.SparseCholesky(d.m, cl)
+    M = pattern_spd(d.m, cl, 3)
+    dM, dD, D, info, pmin = factor_solve(S, M, cuda)
+    assert info == 0 and 0 < pmin <= 1
+    b = np.random.default_rng(4).standard_normal(d.m)
+    x = torch.as_tensor(b, device=cuda)
+    step.call("schol_solve", S.h, dD.data_ptr(), x.data_ptr(), None)
+    step.call("sync", None)
+    want = np.linalg.solve(M, b)
+    got = x.cpu().numpy()
+    assert np.linalg.norm(got - want) <= 1e-12 * np.linalg.cond(M) * np.linalg.norm(want)
+    # the smallest pivot of the scaled matrix: the dense Cholesky's, to rounding
+    Ms = D[:, None] * M * D[None, :]
+    perm = S.perm()
+    Lp = np.linalg.cholesky(Ms[np.ix_(perm, perm)])
+    assert pmin == pytest.approx(np.min(np.diag(Lp)) ** 2, rel=1e-8)
+    S.close()
+
+
+def test_sparse_factor_reports_indefinite(cuda):
+    d = problems.moment_relaxation(nvars=8, clique=4, seed=1)
+    cl = cliques_of(d)
+    S = step.SparseCholesky(d.m, cl)
+    M = pattern_spd(d.m, cl, 5)
+    M[np.ix_(cl[2], cl[2])] -= 3.0 * np.eye(len(cl[2]))   # indefinite on one clique
+    _, _, _, info, _ = factor_solve(S, M, cuda)
+    assert info > 0
+    # the same handle factors a positive definite matrix again
+    _, _, _, info2, _ = factor_solve(S, pattern_spd(d.m, cl, 6), cuda)
+    assert info2 == 0
+    S.close()
+
+
+@pytest.mark.parametrize("sparse", ["1", "-1"])
+def test_moment_relaxation_sparse_factor_matches_reference(golden, sparse):
+    """mom60 (57 moment blocks of 15, m = 2029) with the sparse Schur factor (forced, and the
+    automatic choice, which takes it) against the reference's solve."""
+    e = golden["mom60"]
+    d = problems.moment_relaxation(**e["kwargs"])
+    res = brisk_b200.solve_sdpa(*d.args(), options=FP64 + ["-sparse", sparse, "-v"], verbose=False)
+    assert "sparse Cholesky" in res.log
+    ref = e["runs"]["default"]
+    assert res.status_str == ref["status"]
+    den = 1 + abs(ref["pobj"]) + abs(ref["dobj"])
+    assert abs(res.pobj - ref["pobj"]) <= 1e-7 * den and abs(res.dobj - ref["dobj"]) <= 1e-7 * den
+    assert np.max(np.abs(res.dimacs)) <= 1e-7
