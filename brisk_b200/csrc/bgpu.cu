@@ -242,6 +242,8 @@ BGPU_API bgpu_schol *bgpu_schol_analyze(int m, int ncliques, const int64_t *clq_
     return h;
 }
 
+BGPU_API void bgpu_schol_set_delta(double delta) { schol::g_mmd_delta = delta < 0 ? 0 : delta; }
+
 BGPU_API int bgpu_schol_info(const bgpu_schol *h, double *out8) {
     if (!h || !out8) return BGPU_ERR_ARG;
     out8[0] = h->A.nsup;

@@ -25,6 +25,8 @@
 
 namespace schol {
 
+double g_mmd_delta = 1.0;
+
 int analyze(int m, const std::vector<std::vector<int>> &cliques, Analysis &A) {
     A = Analysis();
     A.m = m;
@@ -97,74 +99,93 @@ int analyze(int m, const std::vector<std::vector<int>> &cliques, Analysis &A) {
         if (w[v] > 0) { deg[v] = degree(v); pq.insert({deg[v], v}); }
     estamp.assign(L.size(), 0);
     std::vector<std::vector<int>> sup_cols, sup_off;   // constraint ids
+    // Multiple elimination (rounds): every supervariable whose degree is within
+    // dmin (1 + g_mmd_delta) and that is not adjacent to one already eliminated in the round goes
+    // in the round; degrees are updated once per round.  Independent eliminations give a bushy
+    // supernode tree (on a chain of cliques, alternate groups at each round: a tree of
+    // logarithmic height, so the fronts of a level fill the GPU).
+    std::vector<int> touched(m, 0), upd;
+    int round = 0;
     while (!pq.empty()) {
-        const int p = pq.begin()->second;
-        pq.erase(pq.begin());
-        ++cur;
-        stamp[p] = cur;
-        const int mk = cur;
-        std::vector<int> Ln;
-        for (int e : E[p]) {
-            if (!alive[e]) continue;
-            for (int u : L[e])
-                if (w[u] > 0 && stamp[u] != mk) { stamp[u] = mk; Ln.push_back(u); }
-            alive[e] = 0;
-        }
-        std::sort(Ln.begin(), Ln.end());
-        sup_cols.push_back(mem[p]);
-        std::vector<int> off;
-        for (int u : Ln) off.insert(off.end(), mem[u].begin(), mem[u].end());
-        sup_off.push_back(std::move(off));
-        w[p] = 0;
-        done[p] = 1;
-        E[p].clear();
-        if (Ln.empty()) continue;
-        const int en = (int)L.size();
-        L.push_back(Ln);
-        alive.push_back(1);
-        estamp.push_back(0);
-        // element lists of the new element's variables: the dead ones out, the new one in; an
-        // element whose live variables all lie in the new one is absorbed
-        for (int u : Ln) {
-            auto &eu = E[u];
-            size_t k = 0;
-            for (int e : eu) if (alive[e]) eu[k++] = e;
-            eu.resize(k);
-        }
-        for (int u : Ln)
-            for (int e : E[u]) {
-                if (estamp[e] == mk) continue;
-                estamp[e] = mk;
-                bool sub = true;
-                for (int x : L[e])
-                    if (w[x] > 0 && stamp[x] != mk) { sub = false; break; }
-                if (sub) alive[e] = 0;
+        ++round;
+        const long long dmin = pq.begin()->first;
+        const long long dlim = dmin + (long long)(g_mmd_delta * (double)dmin);
+        std::vector<int> cand;
+        for (auto it = pq.begin(); it != pq.end() && it->first <= dlim; ++it) cand.push_back(it->second);
+        upd.clear();
+        for (const int p : cand) {
+            if (w[p] <= 0 || touched[p] == round) continue;
+            pq.erase({deg[p], p});
+            ++cur;
+            stamp[p] = cur;
+            const int mk = cur;
+            std::vector<int> Ln;
+            for (int e : E[p]) {
+                if (!alive[e]) continue;
+                for (int u : L[e])
+                    if (w[u] > 0 && stamp[u] != mk) { stamp[u] = mk; Ln.push_back(u); }
+                alive[e] = 0;
             }
-        for (int u : Ln) {
-            auto &eu = E[u];
-            size_t k = 0;
-            for (int e : eu) if (alive[e]) eu[k++] = e;
-            eu.resize(k);
-            eu.push_back(en);
-        }
-        // indistinguishable variables of the new element merge
-        {
-            std::map<std::vector<int>, int> first;
+            std::sort(Ln.begin(), Ln.end());
+            sup_cols.push_back(mem[p]);
+            std::vector<int> off;
+            for (int u : Ln) off.insert(off.end(), mem[u].begin(), mem[u].end());
+            sup_off.push_back(std::move(off));
+            w[p] = 0;
+            done[p] = 1;
+            E[p].clear();
+            if (Ln.empty()) continue;
+            const int en = (int)L.size();
+            L.push_back(Ln);
+            alive.push_back(1);
+            estamp.push_back(0);
+            // element lists of the new element's variables: the dead ones out, the new one in; an
+            // element whose live variables all lie in the new one is absorbed
             for (int u : Ln) {
-                std::vector<int> key = E[u];
-                std::sort(key.begin(), key.end());
-                auto it = first.find(key);
-                if (it == first.end()) { first.emplace(std::move(key), u); continue; }
-                const int f = it->second;
-                pq.erase({deg[u], u});
-                w[f] += w[u];
-                mem[f].insert(mem[f].end(), mem[u].begin(), mem[u].end());
-                w[u] = 0;
-                done[u] = 1;
-                E[u].clear();
+                auto &eu = E[u];
+                size_t k = 0;
+                for (int e : eu) if (alive[e]) eu[k++] = e;
+                eu.resize(k);
             }
+            for (int u : Ln)
+                for (int e : E[u]) {
+                    if (estamp[e] == mk) continue;
+                    estamp[e] = mk;
+                    bool sub = true;
+                    for (int x : L[e])
+                        if (w[x] > 0 && stamp[x] != mk) { sub = false; break; }
+                    if (sub) alive[e] = 0;
+                }
+            for (int u : Ln) {
+                auto &eu = E[u];
+                size_t k = 0;
+                for (int e : eu) if (alive[e]) eu[k++] = e;
+                eu.resize(k);
+                eu.push_back(en);
+                touched[u] = round;
+            }
+            // indistinguishable variables of the new element merge
+            {
+                std::map<std::vector<int>, int> first;
+                for (int u : Ln) {
+                    std::vector<int> key = E[u];
+                    std::sort(key.begin(), key.end());
+                    auto it = first.find(key);
+                    if (it == first.end()) { first.emplace(std::move(key), u); continue; }
+                    const int f = it->second;
+                    pq.erase({deg[u], u});
+                    w[f] += w[u];
+                    mem[f].insert(mem[f].end(), mem[u].begin(), mem[u].end());
+                    w[u] = 0;
+                    done[u] = 1;
+                    E[u].clear();
+                }
+            }
+            upd.insert(upd.end(), Ln.begin(), Ln.end());
         }
-        for (int u : Ln) {
+        std::sort(upd.begin(), upd.end());
+        upd.erase(std::unique(upd.begin(), upd.end()), upd.end());
+        for (int u : upd) {
             if (w[u] <= 0) continue;
             pq.erase({deg[u], u});
             deg[u] = degree(u);

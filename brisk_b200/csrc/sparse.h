@@ -31,6 +31,8 @@ struct Analysis {
     int fmax = 0;                    // the largest front
 };
 
+// Minimum-degree rounds take every supervariable of degree <= dmin (1 + g_mmd_delta) (default 1).
+extern double g_mmd_delta;
 // cliques: constraint index sets (each block's constraints).  Returns 0, or 1 on bad input.
 int analyze(int m, const std::vector<std::vector<int>> &cliques, Analysis &A);
 

@@ -46,6 +46,7 @@ def lib():
         "bgpu_schol_factor": ([P, P, I64, P, D, P, P, P], I),
         "bgpu_schol_solve": ([P, P, P, P], I),
         "bgpu_schol_destroy": ([P], None),
+        "bgpu_schol_set_delta": ([D], None),
         "bgpu_schur_densify": ([I, I, P, P, P, P, P], I),
         "bgpu_schur_assemble_dense": ([I, I, I, P, P, P, P, P, P, P, P, P, I, I, P, SZ, P], I),
         "bgpu_potrf": ([I, P, I, P, P, P, P], I),

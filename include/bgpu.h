@@ -217,6 +217,10 @@ BGPU_API int bgpu_schol_factor(bgpu_schol *h, const double *d_M, int64_t ldm, co
                                int *info, double *pmin, void *stream);
 BGPU_API int bgpu_schol_solve(bgpu_schol *h, const double *d_D, double *d_x, void *stream);
 BGPU_API void bgpu_schol_destroy(bgpu_schol *h);
+/* The ordering's tolerance for later analyses: each minimum-degree round eliminates the
+ * independent supervariables of degree <= dmin (1 + delta) (default 1; 0: strict minimum degree,
+ * the least fill, a taller tree).  No counterpart in the reference (its AMD has none). */
+BGPU_API void bgpu_schol_set_delta(double delta);
 
 #ifdef __cplusplus
 }

@@ -6,7 +6,7 @@ files written by brisk_b200.problems, with the reference's presolves off so that
 problem as given, and records per run: status, iterations, objectives, the six DIMACS errors,
 the iteration table of -v (pobj, dobj, pinf, dinf, gap, mu per iteration) and the time.
 
-usage: python tests/golden/make_golden.py [--big]    (--big adds the n=400, m=2000 instance)
+usage: python tests/golden/make_golden.py [--big] [names]   (--big adds rand400 and mom700)
 """
 from __future__ import annotations
 
@@ -41,7 +41,8 @@ INSTANCES = {
 # first twelve and the largest (q = 3339: n = 64, m = 1038)
 for _q in list(range(12)) + [3339]:
     INSTANCES[f"batch_q{_q}"] = (batch_instance, dict(q=_q))
-BIG = {"rand400": (random_sdp, dict(n=400, m=2000, density=0.01, seed=0))}
+BIG = {"rand400": (random_sdp, dict(n=400, m=2000, density=0.01, seed=0)),
+       "mom700": (moment_relaxation, dict(nvars=700, clique=4, seed=0))}
 
 ROW = re.compile(r"^\s*(\d+)\s+([+-]\S+)\s+([+-]\S+)\s+(\S+)\s+(\S+)\s+(\S+)\s+(\S+)\s+(\S+)\s+(\S+)\s+(\S+)\s+(\S+)\s*$")
 

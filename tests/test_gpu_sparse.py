@@ -93,3 +93,17 @@ def test_moment_relaxation_sparse_factor_matches_reference(golden, sparse):
     den = 1 + abs(ref["pobj"]) + abs(ref["dobj"])
     assert abs(res.pobj - ref["pobj"]) <= 1e-7 * den and abs(res.dobj - ref["dobj"]) <= 1e-7 * den
     assert np.max(np.abs(res.dimacs)) <= 1e-7
+
+
+def test_large_moment_relaxation_sparse_matches_reference(golden):
+    """The chain moment relaxation in 700 variables (697 blocks of 15, m = 24429): the automatic
+    choice takes the sparse factor; the result matches the reference's."""
+    e = golden["mom700"]
+    d = problems.moment_relaxation(**e["kwargs"])
+    res = brisk_b200.solve_sdpa(*d.args(), options=FP64 + ["-v"], verbose=False)
+    assert "sparse Cholesky" in res.log
+    ref = e["runs"]["default"]
+    assert res.status_str == ref["status"]
+    den = 1 + abs(ref["pobj"]) + abs(ref["dobj"])
+    assert abs(res.pobj - ref["pobj"]) <= 1e-7 * den and abs(res.dobj - ref["dobj"]) <= 1e-7 * den
+    assert np.max(np.abs(res.dimacs)) <= 1e-7
