@@ -500,78 +500,98 @@ __global__ void __launch_bounds__(FT) front_kernel(const int *__restrict__ sups,
     }
 }
 
-// Forward and backward substitution over the supernodes in one CTA (x in elimination order):
-// forward: x_s = L_ss^-1 x_s, x_rows -= L_rs x_s; backward: x_s -= L_rs' x_rows, x_s = L_ss^-T x_s.
-constexpr int ST = 512;
-__global__ void __launch_bounds__(ST) solve_kernel(int nsup, const int *__restrict__ fsz, const int *__restrict__ nsz,
-                                                   const long long *__restrict__ rptr, const int *__restrict__ rows,
-                                                   const long long *__restrict__ lptr, const double *__restrict__ L,
-                                                   const int *__restrict__ perm, const double *__restrict__ D, int m,
-                                                   double *x, double *xe) {
-    __shared__ double xs[256];
-    __shared__ double red[ST / 32];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (int k = tid; k < m; k += ST) { const int c = perm[k]; xe[k] = D[c] * x[c]; }
+// Triangular solves by tree levels, one CTA per supernode (the multifrontal solve).  Forward
+// (leaves first): y_s = L_ss^-1 (b_s - the children's contributions to s's columns), and s passes
+// up V_s = L_off,s y_s + the children's contributions to s's off-diagonal rows (added through the
+// relative indices, children in a fixed order).  Backward (root first): x_s = L_ss^-T (y_s -
+// L_off,s' x_off), x_off already final.  xe holds the permuted, scaled vector.
+constexpr int ST = 256;
+constexpr int SX = 512;   // own columns held in shared memory (larger supernodes use the global xe)
+
+__global__ void perm_in_kernel(int m, const int *__restrict__ perm, const double *__restrict__ D,
+                               const double *__restrict__ x, double *xe) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < m) { const int c = perm[k]; xe[k] = D[c] * x[c]; }
+}
+__global__ void perm_out_kernel(int m, const int *__restrict__ perm, const double *__restrict__ D,
+                                const double *__restrict__ xe, double *x) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < m) { const int c = perm[k]; x[c] = D[c] * xe[k]; }
+}
+
+__global__ void __launch_bounds__(ST) fwd_kernel(const int *__restrict__ sups, const int *__restrict__ fsz,
+                                                 const int *__restrict__ nsz, const long long *__restrict__ rptr,
+                                                 const int *__restrict__ rows, const long long *__restrict__ lptr,
+                                                 const double *__restrict__ L, const int *__restrict__ cptr,
+                                                 const int *__restrict__ child, const long long *__restrict__ relptr,
+                                                 const int *__restrict__ rel, double *xe, double *V) {
+    __shared__ double xs[SX];
+    __shared__ double yj;
+    const int s = sups[blockIdx.x], tid = threadIdx.x;
+    const int f = fsz[s], ns = nsz[s], rs = f - ns;
+    const int k0 = rows[rptr[s]];
+    const double *P = L + lptr[s];
+    double *vo = V + relptr[s];   // rs values (none at a root)
+    const bool sm = ns <= SX;
+    double *y = sm ? xs : xe + k0;
+    if (sm) for (int j = tid; j < ns; j += ST) xs[j] = xe[k0 + j];
+    for (int i = tid; i < rs; i += ST) vo[i] = 0.0;
     __syncthreads();
-    // forward
-    for (int s = 0; s < nsup; s++) {
-        const int f = fsz[s], ns = nsz[s];
-        const int *rw = rows + rptr[s];
-        const double *P = L + lptr[s];
-        const int k0 = rw[0];
-        for (int c0 = 0; c0 < ns; c0 += 256) {   // the diagonal block in panels of 256 columns
-            const int cw = min(256, ns - c0);
-            if (tid < cw) xs[tid] = xe[k0 + c0 + tid];
-            __syncthreads();
-            for (int j = 0; j < cw; j++) {   // column c0 + j of the diagonal block
-                const int jc = c0 + j;
-                if (tid == 0) xs[j] /= P[jc + (long long)jc * f];
-                __syncthreads();
-                const double xj = xs[j];
-                for (int i = j + 1 + tid; i < cw; i += ST) xs[i] -= P[(c0 + i) + (long long)jc * f] * xj;
-                __syncthreads();
-            }
-            if (tid < cw) xe[k0 + c0 + tid] = xs[tid];
-            __syncthreads();
-            // rows below this column panel: the rest of the diagonal block and the off rows
-            for (int i = c0 + cw + tid; i < f; i += ST) {
-                double a = 0.0;
-                for (int j = 0; j < cw; j++) a += P[i + (long long)(c0 + j) * f] * xs[j];
-                xe[rw[i]] -= a;
-            }
-            __syncthreads();
-        }
-    }
-    // backward
-    for (int s = nsup - 1; s >= 0; s--) {
-        const int f = fsz[s], ns = nsz[s];
-        const int *rw = rows + rptr[s];
-        const double *P = L + lptr[s];
-        const int k0 = rw[0];
-        // x_s -= L_rs' x_rows: one warp per column
-        for (int j = warp; j < ns; j += ST / 32) {
-            double a = 0.0;
-            for (int i = ns + lane; i < f; i += 32) a += P[i + (long long)j * f] * xe[rw[i]];
-            a = warp_sum(a);
-            if (lane == 0) xe[k0 + j] -= a;
+    for (int c = cptr[s]; c < cptr[s + 1]; c++) {
+        const int k = child[c];
+        const int rc = fsz[k] - nsz[k];
+        const int *rl = rel + relptr[k];
+        const double *vc = V + relptr[k];
+        for (int i = tid; i < rc; i += ST) {
+            const int r = rl[i];
+            if (r < ns) y[r] -= vc[i]; else vo[r - ns] += vc[i];
         }
         __syncthreads();
-        // L_ss' x_s = rhs, columns from the last
-        for (int j = ns - 1; j >= 0; j--) {
-            double a = 0.0;
-            for (int i = j + 1 + tid; i < ns; i += ST) a += P[i + (long long)j * f] * xe[k0 + i];
-            for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
-            if (lane == 0) red[warp] = a;
-            __syncthreads();
-            if (tid == 0) {
-                double t = 0.0;
-                for (int w = 0; w < ST / 32; w++) t += red[w];
-                xe[k0 + j] = (xe[k0 + j] - t) / P[j + (long long)j * f];
-            }
-            __syncthreads();
-        }
     }
-    for (int k = tid; k < m; k += ST) { const int c = perm[k]; x[c] = D[c] * xe[k]; }
+    for (int j = 0; j < ns; j++) {
+        if (tid == 0) { yj = y[j] / P[j + (long long)j * f]; y[j] = yj; }
+        __syncthreads();
+        const double v = yj;
+        for (int i = j + 1 + tid; i < ns; i += ST) y[i] -= P[i + (long long)j * f] * v;
+        __syncthreads();
+    }
+    for (int i = tid; i < rs; i += ST) {
+        double a = 0.0;
+        for (int j = 0; j < ns; j++) a += P[(ns + i) + (long long)j * f] * y[j];
+        vo[i] += a;
+    }
+    if (sm) for (int j = tid; j < ns; j += ST) xe[k0 + j] = xs[j];
+}
+
+__global__ void __launch_bounds__(ST) bwd_kernel(const int *__restrict__ sups, const int *__restrict__ fsz,
+                                                 const int *__restrict__ nsz, const long long *__restrict__ rptr,
+                                                 const int *__restrict__ rows, const long long *__restrict__ lptr,
+                                                 const double *__restrict__ L, double *xe) {
+    __shared__ double xs[SX];
+    __shared__ double xj_s;
+    const int s = sups[blockIdx.x], tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int f = fsz[s], ns = nsz[s];
+    const int *rw = rows + rptr[s];
+    const int k0 = rw[0];
+    const double *P = L + lptr[s];
+    const bool sm = ns <= SX;
+    double *x = sm ? xs : xe + k0;
+    // x_s = y_s - L_off,s' x_off: a warp per column
+    for (int j = warp; j < ns; j += ST / 32) {
+        double a = 0.0;
+        for (int i = ns + lane; i < f; i += 32) a += P[i + (long long)j * f] * xe[rw[i]];
+        a = warp_sum(a);
+        if (lane == 0) x[j] = xe[k0 + j] - a;
+    }
+    __syncthreads();
+    for (int j = ns - 1; j >= 0; j--) {
+        if (tid == 0) { xj_s = x[j] / P[j + (long long)j * f]; x[j] = xj_s; }
+        __syncthreads();
+        const double v = xj_s;
+        for (int i = tid; i < j; i += ST) x[i] -= P[j + (long long)i * f] * v;
+        __syncthreads();
+    }
+    if (sm) for (int j = tid; j < ns; j += ST) xe[k0 + j] = xs[j];
 }
 }  // namespace
 
@@ -590,6 +610,7 @@ size_t factor_bytes(const Analysis &A) {
     b += al(sizeof(double) * (A.lptr.empty() ? 1 : A.lptr[n] + 1));
     b += al(sizeof(double) * (A.uptr.empty() ? 1 : A.uptr[n] + 1));
     b += al(sizeof(double) * (A.m + 1));          // xe
+    b += al(sizeof(double) * (A.rel.size() + 1)); // V (the solve's passed-up vectors)
     b += al(sizeof(int)) + al(sizeof(double));    // info, pmin
     return b + 256;
 }
@@ -619,6 +640,7 @@ int factor_bind(cudaStream_t st, const Analysis &A, void *buf, Factor &F) {
     F.L = (double *)take(sizeof(double) * (A.lptr[n] + 1));
     F.U = (double *)take(sizeof(double) * (A.uptr[n] + 1));
     F.x = (double *)take(sizeof(double) * (A.m + 1));
+    F.V = (double *)take(sizeof(double) * (A.rel.size() + 1));
     F.info = (int *)take(sizeof(int));
     F.pmin = (double *)take(sizeof(double));
     F.bytes = factor_bytes(A);
@@ -691,7 +713,21 @@ int factor(cudaStream_t st, Factor &F, const double *M, long long ldm, const dou
 
 int solve(cudaStream_t st, Factor &F, const double *d_D, double *x) {
     const Analysis &A = *F.A;
-    solve_kernel<<<1, ST, 0, st>>>(A.nsup, F.f, F.ns, F.rptr, F.rows, F.lptr, F.L, F.perm, d_D, A.m, x, F.x);
+    const int m = A.m, nlev = (int)A.lvptr.size() - 1;
+    perm_in_kernel<<<ceil_div(m, 256), 256, 0, st>>>(m, F.perm, d_D, x, F.x);
+    BGPU_LAUNCH_CHECK();
+    for (int l = 0; l < nlev; l++) {
+        const int lo = A.lvptr[l], cnt = A.lvptr[l + 1] - lo;
+        fwd_kernel<<<cnt, ST, 0, st>>>(F.lvsup + lo, F.f, F.ns, F.rptr, F.rows, F.lptr, F.L, F.cptr, F.child, F.relptr,
+                                       F.rel, F.x, F.V);
+        BGPU_LAUNCH_CHECK();
+    }
+    for (int l = nlev - 1; l >= 0; l--) {
+        const int lo = A.lvptr[l], cnt = A.lvptr[l + 1] - lo;
+        bwd_kernel<<<cnt, ST, 0, st>>>(F.lvsup + lo, F.f, F.ns, F.rptr, F.rows, F.lptr, F.L, F.x);
+        BGPU_LAUNCH_CHECK();
+    }
+    perm_out_kernel<<<ceil_div(m, 256), 256, 0, st>>>(m, F.perm, d_D, F.x, x);
     BGPU_LAUNCH_CHECK();
     return BGPU_OK;
 }

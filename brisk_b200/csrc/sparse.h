@@ -43,7 +43,7 @@ struct Factor {
     int *perm = nullptr, *f = nullptr, *ns = nullptr, *rows = nullptr, *cptr = nullptr, *child = nullptr,
         *rel = nullptr, *lvsup = nullptr;
     long long *rptr = nullptr, *relptr = nullptr, *lptr = nullptr, *uptr = nullptr;
-    double *L = nullptr, *U = nullptr, *x = nullptr;
+    double *L = nullptr, *U = nullptr, *x = nullptr, *V = nullptr;
     int *info = nullptr;
     double *pmin = nullptr;
     size_t bytes = 0;
