@@ -42,7 +42,59 @@ __global__ void sym_lincomb_kernel(int n, const double *G, double s, double a, c
     if (y) v += b * y[p];
     out[p] = v;
 }
+// the block of concatenated element g: off (nb+1 offsets) is ascending, off[0] = 0
+__device__ __forceinline__ int block_of(long long g, int nb, const long long *__restrict__ off) {
+    int lo = 0, hi = nb - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (off[mid] <= g) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+__global__ void sym_lincomb_blocks_kernel(int nb, const int *__restrict__ ns, const long long *__restrict__ off,
+                                          long long total, const double *G, double s, double a, const double *x,
+                                          double b, const double *y, double *out) {
+    const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= total) return;
+    const int k = block_of(g, nb, off), n = ns[k];
+    const long long l = g - off[k];
+    const int j = (int)(l / n), i = (int)(l - (long long)j * n);
+    const long long q = off[k] + j + (long long)i * n;
+    double v = s * 0.5 * (G[g] + G[q]);
+    if (x) v += a * x[g];
+    if (y) v += b * y[g];
+    out[g] = v;
+}
+
+__global__ void scaled_identity_blocks_kernel(int nb, const int *__restrict__ ns, const long long *__restrict__ off,
+                                              long long total, const double *__restrict__ v,
+                                              const int *__restrict__ only, double *out) {
+    const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= total) return;
+    const int k = block_of(g, nb, off), n = ns[k];
+    if (only && !only[k]) return;
+    const long long l = g - off[k];
+    out[g] = (l % (n + 1) == 0) ? v[k] : 0.0;
+}
 }  // namespace
+
+int ew_sym_lincomb_blocks(cudaStream_t st, int nb, const int *d_n, const long long *d_off, long long total,
+                          const double *G, double s, double a, const double *x, double b, const double *y,
+                          double *out) {
+    if (total <= 0 || nb <= 0) return BGPU_OK;
+    sym_lincomb_blocks_kernel<<<ceil_div(total, 256), 256, 0, st>>>(nb, d_n, d_off, total, G, s, a, x, b, y, out);
+    BGPU_LAUNCH_CHECK();
+    return BGPU_OK;
+}
+
+int ew_scaled_identity_blocks(cudaStream_t st, int nb, const int *d_n, const long long *d_off, long long total,
+                              const double *d_v, const int *d_only, double *out) {
+    if (total <= 0 || nb <= 0) return BGPU_OK;
+    scaled_identity_blocks_kernel<<<ceil_div(total, 256), 256, 0, st>>>(nb, d_n, d_off, total, d_v, d_only, out);
+    BGPU_LAUNCH_CHECK();
+    return BGPU_OK;
+}
 
 int ew_lincomb(cudaStream_t st, long long n, double a, const double *x, double b, const double *y, double c,
                const double *z, double *out) {

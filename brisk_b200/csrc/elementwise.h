@@ -12,3 +12,12 @@ int ew_set_scaled_identity(cudaStream_t st, int n, double *A, double v);
 // out = s sym(G) + a x + b y, sym(G) = (G + G')/2; out must not alias G
 int ew_sym_lincomb(cudaStream_t st, int n, const double *G, double s, double a, const double *x, double b,
                    const double *y, double *out);
+
+// Over blocks stored one after another (block k: order d_n[k], elements d_off[k] .. d_off[k+1] of
+// the concatenation, column-major; d_off has nb+1 entries): the same as ew_sym_lincomb per block,
+// and out_k = v_k I (only the blocks with d_only[k] != 0 when d_only is not null), in one launch each.
+int ew_sym_lincomb_blocks(cudaStream_t st, int nb, const int *d_n, const long long *d_off, long long total,
+                          const double *G, double s, double a, const double *x, double b, const double *y,
+                          double *out);
+int ew_scaled_identity_blocks(cudaStream_t st, int nb, const int *d_n, const long long *d_off, long long total,
+                              const double *d_v, const int *d_only, double *out);

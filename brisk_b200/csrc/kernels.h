@@ -82,6 +82,11 @@ struct DevBlock {
 int aop_f64(cudaStream_t st, const DevBlock &B, const double *D, double alpha, double beta, double *out);
 // F = alpha * sum_i y_i A_i + beta * F (full n x n).
 int atop_f64(cudaStream_t st, const DevBlock &B, const double *y, double alpha, double beta, double *F);
+// The same for nb blocks stored one after another in F (block k at d_off[k], d_off has nb+1
+// entries, total = d_off[nb]); the blocks' position-major lists as device pointer tables.
+int atop_blocks_f64(cudaStream_t st, int nb, const long long *d_off, long long total, const long long *const *pptr,
+                    const int *const *pcon, const double *const *pval, const double *y, double alpha, double beta,
+                    double *F);
 
 // Workspace of the row-product assembly, sized by schur_ws_bytes.
 struct SchurWs {

@@ -445,6 +445,27 @@ __global__ void atop_kernel(long long npos, const long long *__restrict__ pptr, 
     for (long long e = pptr[p]; e < pptr[p + 1]; e++) s += pval[e] * y[pcon[e]];
     F[p] = (beta == 0.0) ? alpha * s : alpha * s + beta * F[p];
 }
+// A'(y) for blocks stored one after another: position g of the concatenation lies in block k
+// (off ascending); the block's position-major lists come from pointer tables.
+__global__ void atop_blocks_kernel(int nb, const long long *__restrict__ off, long long total,
+                                   const long long *const *__restrict__ pptr, const int *const *__restrict__ pcon,
+                                   const double *const *__restrict__ pval, const double *__restrict__ y, double alpha,
+                                   double beta, double *F) {
+    const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= total) return;
+    int lo = 0, hi = nb - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (off[mid] <= g) lo = mid; else hi = mid - 1;
+    }
+    const long long p = g - off[lo];
+    const long long *pp = pptr[lo];
+    const int *pc = pcon[lo];
+    const double *pv = pval[lo];
+    double s = 0.0;
+    for (long long e = pp[p]; e < pp[p + 1]; e++) s += pv[e] * y[pc[e]];
+    F[g] = (beta == 0.0) ? alpha * s : alpha * s + beta * F[g];
+}
 }  // namespace
 
 namespace {
@@ -475,6 +496,15 @@ int schur_colptr(cudaStream_t st, const DevBlock &B) {
 int aop_f64(cudaStream_t st, const DevBlock &B, const double *D, double alpha, double beta, double *out) {
     if (B.ncon <= 0) return BGPU_OK;
     aop_kernel<<<ceil_div(B.ncon, 8), 256, 0, st>>>(B.ncon, B.con, B.cptr, B.cpos, B.cval, D, alpha, beta, out);
+    BGPU_LAUNCH_CHECK();
+    return BGPU_OK;
+}
+
+int atop_blocks_f64(cudaStream_t st, int nb, const long long *d_off, long long total, const long long *const *pptr,
+                    const int *const *pcon, const double *const *pval, const double *y, double alpha, double beta,
+                    double *F) {
+    if (total <= 0 || nb <= 0) return BGPU_OK;
+    atop_blocks_kernel<<<ceil_div(total, 256), 256, 0, st>>>(nb, d_off, total, pptr, pcon, pval, y, alpha, beta, F);
     BGPU_LAUNCH_CHECK();
     return BGPU_OK;
 }

@@ -343,6 +343,11 @@ struct DevArrays {   // per block
     double *dinvX, *dinvZ;
     int *flags;
 };
+// the n x n members, each one concatenation over the blocks
+static double *DevArrays::*const kCatMembers[] = {
+    &DevArrays::X,  &DevArrays::Z,  &DevArrays::Zi, &DevArrays::LX, &DevArrays::LZ, &DevArrays::LiX, &DevArrays::LiZ,
+    &DevArrays::dX, &DevArrays::dZ, &DevArrays::F,  &DevArrays::Fd, &DevArrays::R0, &DevArrays::G,   &DevArrays::Q,
+    &DevArrays::W,  &DevArrays::T,  &DevArrays::Xb, &DevArrays::Zb, &DevArrays::Bm};
 
 // Device memory of one solve.  Stand-alone solves allocate with cudaMalloc and own a stream; the
 // batch workers hand in an arena (one allocation and one stream per worker, reused by every
@@ -477,8 +482,29 @@ class Solver {
     // reductions
     void dots(int nq, const double *const *a, const double *const *b, long long n, double *out);
     // operators
-    void aop_all(const std::vector<double *> &D, std::vector<double> &out);   // out = A(D)
-    void atop_block(int k, const std::vector<double> &y, double alpha, double beta, double *F);
+    // The blocks' n x n arrays are stored one after another: block k's at boff[k] of each
+    // concatenation (cat.X, cat.Z, ..., Ccat, Icat = I), so element-wise work and inner products
+    // over all blocks are one launch each; gall holds every constraint's entries at concatenated
+    // positions (the block's own arrays when there is one block).
+    std::vector<long long> boff;
+    long long Ntot2 = 0;
+    DevArrays cat{};
+    double *Ccat = nullptr, *Icat = nullptr;
+    long long *d_boff = nullptr;
+    int *d_bn = nullptr, *d_bsmall = nullptr;   // block orders; 1 for the blocks of order <= SMALL_N_MAX
+    double *d_bval = nullptr;                   // one value per block (scratch)
+    const long long **d_ppt = nullptr;
+    const int **d_pct = nullptr;
+    const double **d_pvt = nullptr;
+    DevBlock gall;
+    void build_gall();
+    void aop_cat(const double *D, std::vector<double> &out);                                    // out = A(D)
+    void atop_cat(const std::vector<double> &y, double alpha, double beta, double *F);         // F = a A'y + b F
+    void sym_cat(const double *G, double s, double a, const double *x, double b, const double *y, double *out);
+    void dots_cat(int nq, const double *const *a, const double *const *b, double *out) { dots(nq, a, b, Ntot2, out); }
+    void lincomb_cat(double a, const double *x, double b, const double *y, double c, const double *z, double *out) {
+        RC(ew_lincomb(g.st, Ntot2, a, x, b, y, c, z, out));
+    }
     void gemm(int akm, int bkm, int n, double alpha, const double *A, long long lda, const double *B, long long ldb,
               double beta, double *C) {
         RC(gemm_f64(g.st, akm, bkm, n, n, n, alpha, A, lda, 0, B, ldb, 0, beta, C, n, 0, 1, 0));
@@ -537,7 +563,7 @@ void Solver::upload_block(int k) {
     d.pptr = g.alloc<long long>(nn + 1);
     d.pcon = g.alloc<int>(d.ne);
     d.pval = g.alloc<double>(d.ne);
-    d.C = g.alloc<double>(nn);
+    d.C = Ccat + boff[k];
     if (!d.con || !d.cptr || !d.cpos || !d.cval || !d.ccol || !d.pptr || !d.pcon || !d.pval || !d.C)
         throw GpuFail{BGPU_ERR_NOMEM, __LINE__};
     CU(cudaMemcpyAsync(d.con, B.con.data(), sizeof(int) * d.ncon, cudaMemcpyHostToDevice, g.st));
@@ -595,12 +621,7 @@ void Solver::upload_block(int k) {
                     sizeof(long long) * (nn + 1.0) + sizeof(double) * (double)nn;
 
     DevArrays &a = da[k];
-    double **ptrs[] = {&a.X, &a.Z, &a.Zi, &a.LX, &a.LZ, &a.LiX, &a.LiZ, &a.dX, &a.dZ, &a.F, &a.Fd, &a.R0, &a.G,
-                       &a.Q, &a.W, &a.T, &a.Xb, &a.Zb, &a.Bm};
-    for (double **pp : ptrs) {
-        *pp = g.alloc<double>(nn);
-        if (!*pp) throw GpuFail{BGPU_ERR_NOMEM, __LINE__};
-    }
+    for (double *DevArrays::*mem : kCatMembers) a.*mem = cat.*mem + boff[k];
     const int nblk64 = ceil_div(n, TRI_NB);
     a.dinvX = g.alloc<double>((size_t)nblk64 * TRI_NB * TRI_NB);
     a.dinvZ = g.alloc<double>((size_t)nblk64 * TRI_NB * TRI_NB);
@@ -629,10 +650,37 @@ void Solver::setup() {
     dense_route.assign(nb, 0);
     int nmax = 1;
     const double t1 = wtime();
+    boff.assign(nb + 1, 0);
+    for (int k = 0; k < nb; k++) boff[k + 1] = boff[k] + (long long)P.blk[k].n * P.blk[k].n;
+    Ntot2 = boff[nb];
+    for (double *DevArrays::*mem : kCatMembers) {
+        cat.*mem = g.alloc<double>(Ntot2);
+        if (!(cat.*mem)) throw GpuFail{BGPU_ERR_NOMEM, __LINE__};
+    }
+    Ccat = g.alloc<double>(Ntot2);
+    Icat = g.alloc<double>(Ntot2);
+    d_boff = g.alloc<long long>(nb + 1);
+    d_bn = g.alloc<int>(nb);
+    d_bval = g.alloc<double>(nb);
+    d_bsmall = g.alloc<int>(nb);
+    if (!Ccat || !Icat || !d_boff || !d_bn || !d_bval || !d_bsmall) throw GpuFail{BGPU_ERR_NOMEM, __LINE__};
+    {
+        std::vector<int> bn(nb), bsm(nb);
+        std::vector<double> ones(nb, 1.0);
+        for (int k = 0; k < nb; k++) bn[k] = P.blk[k].n;
+        for (int k = 0; k < nb; k++) bsm[k] = P.blk[k].n <= SMALL_N_MAX;
+        CU(cudaMemcpyAsync(d_bsmall, bsm.data(), sizeof(int) * nb, cudaMemcpyHostToDevice, g.st));
+        CU(cudaMemcpyAsync(d_boff, boff.data(), sizeof(long long) * (nb + 1), cudaMemcpyHostToDevice, g.st));
+        CU(cudaMemcpyAsync(d_bn, bn.data(), sizeof(int) * nb, cudaMemcpyHostToDevice, g.st));
+        CU(cudaMemcpyAsync(d_bval, ones.data(), sizeof(double) * nb, cudaMemcpyHostToDevice, g.st));
+        RC(ew_scaled_identity_blocks(g.st, nb, d_bn, d_boff, Ntot2, d_bval, nullptr, Icat));
+        CU(cudaStreamSynchronize(g.st));
+    }
     for (int k = 0; k < nb; k++) {
         upload_block(k);
         nmax = std::max(nmax, P.blk[k].n);
     }
+    build_gall();
     if (opt.verbose > 1) log_printf(0, "   [device context %.3fs, block upload %.3fs]\n", t1 - t0, wtime() - t1);
     for (int k = 0; k < nb; k++) (P.blk[k].n <= SMALL_N_MAX ? small_ids : big_ids).push_back(k);
     if (!small_ids.empty()) {
@@ -732,17 +780,76 @@ void Solver::choose_sparse() {
                    (int)sp_an.lvptr.size() - 1, wtime() - t0);
 }
 
-void Solver::aop_all(const std::vector<double *> &D, std::vector<double> &out) {
+void Solver::build_gall() {
+    if (nb == 1) {
+        gall = db[0];
+        return;
+    }
+    // every constraint's entries over all blocks (block order, then position) at concatenated
+    // positions boff[k] + p + q n
+    long long ne = 0;
+    for (auto &B : P.blk) ne += (long long)B.cpos.size();
+    std::vector<long long> cptr(m + 1, 0);
+    for (auto &B : P.blk)
+        for (size_t t = 0; t < B.con.size(); t++) cptr[B.con[t] + 1] += B.cptr[t + 1] - B.cptr[t];
+    for (int i = 0; i < m; i++) cptr[i + 1] += cptr[i];
+    std::vector<int> cpos(ne), con(m);
+    std::vector<double> cval(ne);
+    std::vector<long long> fill(cptr.begin(), cptr.end() - 1);
+    for (int k = 0; k < nb; k++) {
+        const HBlock &B = P.blk[k];
+        for (size_t t = 0; t < B.con.size(); t++)
+            for (long long e = B.cptr[t]; e < B.cptr[t + 1]; e++) {
+                const long long q = fill[B.con[t]]++;
+                cpos[q] = (int)(boff[k] + B.cpos[e]);
+                cval[q] = B.cval[e];
+            }
+    }
+    for (int i = 0; i < m; i++) con[i] = i;
+    if (Ntot2 >= (1LL << 31)) throw GpuFail{BGPU_ERR_TOOBIG, __LINE__};
+    gall = DevBlock();
+    gall.ncon = m;
+    gall.ne = ne;
+    gall.con = g.alloc<int>(m);
+    gall.cptr = g.alloc<long long>(m + 1);
+    gall.cpos = g.alloc<int>(ne);
+    gall.cval = g.alloc<double>(ne);
+    d_ppt = (const long long **)g.alloc<long long *>(nb);
+    d_pct = (const int **)g.alloc<int *>(nb);
+    d_pvt = (const double **)g.alloc<double *>(nb);
+    if (!gall.con || !gall.cptr || !gall.cpos || !gall.cval || !d_ppt || !d_pct || !d_pvt)
+        throw GpuFail{BGPU_ERR_NOMEM, __LINE__};
+    std::vector<const long long *> ppt(nb);
+    std::vector<const int *> pct(nb);
+    std::vector<const double *> pvt(nb);
+    for (int k = 0; k < nb; k++) { ppt[k] = db[k].pptr; pct[k] = db[k].pcon; pvt[k] = db[k].pval; }
+    CU(cudaMemcpyAsync(gall.con, con.data(), sizeof(int) * m, cudaMemcpyHostToDevice, g.st));
+    CU(cudaMemcpyAsync(gall.cptr, cptr.data(), sizeof(long long) * (m + 1), cudaMemcpyHostToDevice, g.st));
+    CU(cudaMemcpyAsync(gall.cpos, cpos.data(), sizeof(int) * ne, cudaMemcpyHostToDevice, g.st));
+    CU(cudaMemcpyAsync(gall.cval, cval.data(), sizeof(double) * ne, cudaMemcpyHostToDevice, g.st));
+    CU(cudaMemcpyAsync(d_ppt, ppt.data(), sizeof(void *) * nb, cudaMemcpyHostToDevice, g.st));
+    CU(cudaMemcpyAsync(d_pct, pct.data(), sizeof(void *) * nb, cudaMemcpyHostToDevice, g.st));
+    CU(cudaMemcpyAsync(d_pvt, pvt.data(), sizeof(void *) * nb, cudaMemcpyHostToDevice, g.st));
+    CU(cudaStreamSynchronize(g.st));
+    upload_bytes += (double)ne * 12 + (double)m * 12;
+}
+
+void Solver::aop_cat(const double *D, std::vector<double> &out) {
     CU(cudaMemsetAsync(dv_out, 0, sizeof(double) * m, g.st));
-    for (int k = 0; k < nb; k++) RC(aop_f64(g.st, db[k], D[k], 1.0, 1.0, dv_out));
+    RC(aop_f64(g.st, gall, D, 1.0, 1.0, dv_out));
     out.resize(m);
     CU(cudaMemcpyAsync(out.data(), dv_out, sizeof(double) * m, cudaMemcpyDeviceToHost, g.st));
     CU(cudaStreamSynchronize(g.st));
 }
 
-void Solver::atop_block(int k, const std::vector<double> &y, double alpha, double beta, double *F) {
+void Solver::atop_cat(const std::vector<double> &y, double alpha, double beta, double *F) {
     CU(cudaMemcpyAsync(dv_in, y.data(), sizeof(double) * m, cudaMemcpyHostToDevice, g.st));
-    RC(atop_f64(g.st, db[k], dv_in, alpha, beta, F));
+    if (nb == 1) RC(atop_f64(g.st, db[0], dv_in, alpha, beta, F));
+    else RC(atop_blocks_f64(g.st, nb, d_boff, Ntot2, d_ppt, d_pct, d_pvt, dv_in, alpha, beta, F));
+}
+
+void Solver::sym_cat(const double *G, double s, double a, const double *x, double b, const double *y, double *out) {
+    RC(ew_sym_lincomb_blocks(g.st, nb, d_bn, d_boff, Ntot2, G, s, a, x, b, y, out));
 }
 
 int Solver::chol(int n, double *L, double *dinv) {
@@ -936,14 +1043,10 @@ void Solver::schur_mv(const std::vector<double> &x, std::vector<double> &y) {
 }
 
 void Solver::newton_mv(const std::vector<double> &x, std::vector<double> &y) {
-    std::vector<double *> Fs(nb);
-    for (int k = 0; k < nb; k++) {
-        atop_block(k, x, 1.0, 0.0, da[k].W);   // A'(x)
-        Fs[k] = da[k].F;
-    }
+    atop_cat(x, 1.0, 0.0, cat.W);   // A'(x)
     mul_all(1.0, &DevArrays::Zi, &DevArrays::W, &DevArrays::T);
     mul_all(1.0, &DevArrays::T, &DevArrays::X, &DevArrays::F);   // Z^-1 A'(x) X
-    aop_all(Fs, y);
+    aop_cat(cat.F, y);
 }
 
 static double dot(const std::vector<double> &a, const std::vector<double> &b) {
@@ -1157,18 +1260,16 @@ void Solver::least_squares_start(std::vector<double> &y) {
     if (frc != 0) return;   // keep the SDPT3 start (the reference's init_ok = 0 path)
     std::vector<double> dy, AC;
     schur_solve(P.b, dy, 1e-8);
-    std::vector<double *> Cs(nb);
-    for (int k = 0; k < nb; k++) Cs[k] = db[k].C;
-    aop_all(Cs, AC);
+    aop_cat(Ccat, AC);
     schur_solve(AC, y, 1e-8);
     double ax = -1e300, az = -1e300;
-    for (int k = 0; k < nb; k++) {
+    atop_cat(dy, 1.0, 0.0, cat.X);                               // X = A'dy
+    atop_cat(y, -1.0, 0.0, cat.Z);
+    lincomb_cat(1.0, cat.Z, 1.0, Ccat, 0.0, nullptr, cat.Z);     // Z = C - A'y
+    for (int k : big_ids) {
         const int n = db[k].n;
         const long long nn = (long long)n * n;
         DevArrays &d = da[k];
-        atop_block(k, dy, 1.0, 0.0, d.X);                                          // X = A'dy
-        atop_block(k, y, -1.0, 0.0, d.Z);
-        RC(ew_lincomb(g.st, nn, 1.0, d.Z, 1.0, db[k].C, 0.0, nullptr, d.Z));      // Z = C - A'y
         RC(ew_lincomb(g.st, nn, 1.0, d.X, 0.0, nullptr, 0.0, nullptr, d.Bm));
         const double lx = lanczos(n, d.Bm, opt.lanczos_k);
         RC(ew_lincomb(g.st, nn, 1.0, d.Z, 0.0, nullptr, 0.0, nullptr, d.Bm));
@@ -1176,14 +1277,47 @@ void Solver::least_squares_start(std::vector<double> &y) {
         ax = std::max(ax, -lx);
         az = std::max(az, -lz);
     }
+    const int nsm = (int)small_ids.size();
+    if (nsm > 0) {   // the small blocks' exact smallest eigenvalues, all at once
+        CU(cudaMemcpyAsync(cat.LiX, Icat, sizeof(double) * Ntot2, cudaMemcpyDeviceToDevice, g.st));
+        for (int pass = 0; pass < 2; pass++) {
+            RC(small_lammin(g.st, nsm, d_sns, (const double *const *)tab(&DevArrays::LiX),
+                            (const double *const *)tab(pass == 0 ? &DevArrays::X : &DevArrays::Z), d_slam));
+            CU(cudaMemcpyAsync(h_slam, d_slam, sizeof(double) * nsm, cudaMemcpyDeviceToHost, g.st));
+            CU(cudaStreamSynchronize(g.st));
+            double &a = pass == 0 ? ax : az;
+            for (int i = 0; i < nsm; i++) a = std::max(a, -h_slam[i]);
+        }
+    }
     const double shx = ax >= -1e-8 ? 1.0 + ax : 0.0;
     const double shz = std::max(0.0, 1.0 + az);
-    for (int k = 0; k < nb; k++) {
+    lincomb_cat(1.0, cat.X, shx, Icat, 0.0, nullptr, cat.X);
+    lincomb_cat(1.0, cat.Z, shz, Icat, 0.0, nullptr, cat.Z);
+    if (nsm > 0) {   // Cholesky tests of the small blocks, raised where they fail
+        for (int pass = 0; pass < 2; pass++) {
+            double *DevArrays::*V = pass == 0 ? &DevArrays::X : &DevArrays::Z;
+            double *DevArrays::*Lv = pass == 0 ? &DevArrays::LX : &DevArrays::LZ;
+            double *DevArrays::*Li = pass == 0 ? &DevArrays::LiX : &DevArrays::LiZ;
+            for (double extra = 1e-8;; extra *= 10) {
+                RC(small_chol_inv(g.st, nsm, d_sns, tab(V), tab(Lv), tab(Li), d_sinfo));
+                CU(cudaMemcpyAsync(h_sinfo, d_sinfo, sizeof(int) * nsm, cudaMemcpyDeviceToHost, g.st));
+                CU(cudaStreamSynchronize(g.st));
+                bool all = true;
+                for (int i = 0; i < nsm; i++)
+                    if (h_sinfo[i]) {
+                        all = false;
+                        const int k = small_ids[i];
+                        RC(ew_add_diag(g.st, db[k].n, da[k].*V, db[k].n, extra));
+                    }
+                if (all) break;
+                if (extra > 1e30) throw GpuFail{BGPU_ERR_NOTPD, __LINE__};
+            }
+        }
+    }
+    for (int k : big_ids) {
         const int n = db[k].n;
         const long long nn = (long long)n * n;
         DevArrays &d = da[k];
-        RC(ew_add_diag(g.st, n, d.X, n, shx));
-        RC(ew_add_diag(g.st, n, d.Z, n, shz));
         for (double extra = 1e-8;; extra *= 10) {
             RC(ew_lincomb(g.st, nn, 1.0, d.X, 0.0, nullptr, 0.0, nullptr, d.LX));
             if (chol(n, d.LX, d.dinvX) == 0) break;
@@ -1212,27 +1346,46 @@ void Solver::final_measures(const std::vector<double> &y, ResultData &res) {
     res.y.resize(m);
     for (int i = 0; i < m; i++) res.y[i] = cs * P.d[i] * y[i];
     double pobj = 0, xz = 0, lamx_neg = 0, lamz_neg = 0;
-    std::vector<double *> Xs(nb);
     res.X.resize(nb);
     res.Z.resize(nb);
+    // W = cs (C' - A'(y)) ; G = bs X
+    atop_cat(y, -cs, 0.0, cat.W);
+    lincomb_cat(1.0, cat.W, cs, Ccat, 0.0, nullptr, cat.W);
+    lincomb_cat(bs, cat.X, 0.0, nullptr, 0.0, nullptr, cat.G);
+    {
+        double tmp[2];
+        const double *aa[2] = {Ccat, cat.G}, *bb[2] = {cat.G, cat.W};
+        dots_cat(2, aa, bb, tmp);
+        pobj = cs * tmp[0];   // <C_o, X_o> = cs <C', X_o>
+        xz = tmp[1];
+    }
     for (int k = 0; k < nb; k++) {
+        const long long nn = (long long)db[k].n * db[k].n;
+        res.X[k].resize(nn);
+        res.Z[k].resize(nn);
+        CU(cudaMemcpyAsync(res.X[k].data(), da[k].G, sizeof(double) * nn, cudaMemcpyDeviceToHost, g.st));
+        CU(cudaMemcpyAsync(res.Z[k].data(), da[k].W, sizeof(double) * nn, cudaMemcpyDeviceToHost, g.st));
+    }
+    const int nsm = (int)small_ids.size();
+    if (nsm > 0) {   // the small blocks' cone errors: Cholesky tests, exact lambda_min where they fail
+        CU(cudaMemcpyAsync(cat.LiX, Icat, sizeof(double) * Ntot2, cudaMemcpyDeviceToDevice, g.st));
+        for (int pass = 0; pass < 2; pass++) {
+            double *DevArrays::*V = pass == 0 ? &DevArrays::W : &DevArrays::G;
+            RC(small_chol_inv(g.st, nsm, d_sns, tab(V), tab(&DevArrays::T), nullptr, d_sinfo));
+            RC(small_lammin(g.st, nsm, d_sns, (const double *const *)tab(&DevArrays::LiX),
+                            (const double *const *)tab(V), d_slam));
+            CU(cudaMemcpyAsync(h_sinfo, d_sinfo, sizeof(int) * nsm, cudaMemcpyDeviceToHost, g.st));
+            CU(cudaMemcpyAsync(h_slam, d_slam, sizeof(double) * nsm, cudaMemcpyDeviceToHost, g.st));
+            CU(cudaStreamSynchronize(g.st));
+            double &neg = pass == 0 ? lamz_neg : lamx_neg;
+            for (int i = 0; i < nsm; i++)
+                if (h_sinfo[i]) neg = std::max(neg, -h_slam[i]);
+        }
+    }
+    for (int k : big_ids) {
         const int n = db[k].n;
         const long long nn = (long long)n * n;
         DevArrays &d = da[k];
-        // W = cs (C' - A'(y)) ; G = bs X
-        atop_block(k, y, -cs, 0.0, d.W);
-        RC(ew_lincomb(g.st, nn, 1.0, d.W, cs, db[k].C, 0.0, nullptr, d.W));
-        RC(ew_lincomb(g.st, nn, bs, d.X, 0.0, nullptr, 0.0, nullptr, d.G));
-        Xs[k] = d.G;
-        double tmp[2];
-        const double *aa[2] = {db[k].C, d.G}, *bb[2] = {d.G, d.W};
-        dots(2, aa, bb, nn, tmp);
-        pobj += cs * tmp[0];   // <C_o, X_o> = cs <C', X_o>
-        xz += tmp[1];
-        res.X[k].resize(nn);
-        res.Z[k].resize(nn);
-        CU(cudaMemcpyAsync(res.X[k].data(), d.G, sizeof(double) * nn, cudaMemcpyDeviceToHost, g.st));
-        CU(cudaMemcpyAsync(res.Z[k].data(), d.W, sizeof(double) * nn, cudaMemcpyDeviceToHost, g.st));
         // cone errors: a Cholesky test, then lambda_min by Lanczos when it fails
         RC(ew_lincomb(g.st, nn, 1.0, d.W, 0.0, nullptr, 0.0, nullptr, d.T));
         if (chol(n, d.T, d.dinvZ) != 0) {
@@ -1248,7 +1401,7 @@ void Solver::final_measures(const std::vector<double> &y, ResultData &res) {
         }
     }
     std::vector<double> AX;
-    aop_all(Xs, AX);   // scaled A' = d A: A_o(X_o) = AX / d
+    aop_cat(cat.G, AX);   // scaled A' = d A: A_o(X_o) = AX / d
     double r2 = 0, dobj = 0;
     for (int i = 0; i < m; i++) {
         const double v = AX[i] / P.d[i] - P.b0[i];
@@ -1297,6 +1450,7 @@ int Solver::run(ResultData &res) {
     std::vector<double> y(m, 0.0), ybest(m, 0.0), dy, rp(m), a0, h(m, 0.0), rhs(m), qv, ev(m), wv;
     std::vector<double> tmpv;
     // start_sdpt3 (solver.c:6622-6661)
+    std::vector<std::vector<double>> sval(6, std::vector<double>(nb, 0.0));
     for (int k = 0; k < nb; k++) {
         const HBlock &B = P.blk[k];
         const int n = B.n;
@@ -1313,6 +1467,15 @@ int Solver::run(ResultData &res) {
         const double xi = std::max(10.0, std::max(std::sqrt((double)n), n * ratio));
         const double eta = std::max(10.0, std::max(std::sqrt((double)n), std::max(maxA, nC)));
         DevArrays &d = da[k];
+        if (n <= SMALL_N_MAX) {   // set below for all small blocks at once (closed form)
+            sval[0][k] = xi;
+            sval[1][k] = eta;
+            sval[2][k] = std::sqrt(xi);
+            sval[3][k] = std::sqrt(eta);
+            sval[4][k] = 1.0 / std::sqrt(xi);
+            sval[5][k] = 1.0 / std::sqrt(eta);
+            continue;
+        }
         RC(ew_set_scaled_identity(g.st, n, d.X, xi));
         RC(ew_set_scaled_identity(g.st, n, d.Z, eta));
         RC(ew_set_scaled_identity(g.st, n, d.LX, std::sqrt(xi)));
@@ -1325,17 +1488,23 @@ int Solver::run(ResultData &res) {
         inv_from_chol(n, d.LX, d.dinvX, d.LiX);
         inv_from_chol(n, d.LZ, d.dinvZ, d.LiZ);   // the small blocks' Z^-1 comes from LiZ
     }
+    if (!small_ids.empty()) {   // X = xi I, Z = eta I, their factors and inverses (big blocks: kept)
+        double *DevArrays::*mems[6] = {&DevArrays::X, &DevArrays::Z, &DevArrays::LX, &DevArrays::LZ, &DevArrays::LiX,
+                                       &DevArrays::LiZ};
+        for (int q = 0; q < 6; q++) {
+            CU(cudaMemcpyAsync(d_bval, sval[q].data(), sizeof(double) * nb, cudaMemcpyHostToDevice, g.st));
+            RC(ew_scaled_identity_blocks(g.st, nb, d_bn, d_boff, Ntot2, d_bval, d_bsmall, cat.*mems[q]));
+            CU(cudaStreamSynchronize(g.st));   // d_bval is reused by the next member
+        }
+    }
     if (opt.init >= 1 && m > 0) least_squares_start(y);
     // R0 = C - Z - A'y, theta = 1 (solver.c:14317-14326)
     double theta = 1.0, r0norm = 0;
-    for (int k = 0; k < nb; k++) {
-        const long long nn = (long long)db[k].n * db[k].n;
-        atop_block(k, y, -1.0, 0.0, da[k].R0);
-        RC(ew_lincomb(g.st, nn, 1.0, db[k].C, -1.0, da[k].Z, 1.0, da[k].R0, da[k].R0));
-        double t;
-        const double *aa[1] = {da[k].R0};
-        dots(1, aa, aa, nn, &t);
-        r0norm += t;
+    {
+        atop_cat(y, -1.0, 0.0, cat.R0);
+        lincomb_cat(1.0, Ccat, -1.0, cat.Z, 1.0, cat.R0, cat.R0);
+        const double *aa[1] = {cat.R0};
+        dots_cat(1, aa, aa, &r0norm);
     }
     r0norm = std::sqrt(r0norm);
     double nbs = nrm(P.b);
@@ -1353,23 +1522,19 @@ int Solver::run(ResultData &res) {
             RC(small_gemm(g.st, (int)small_ids.size(), d_sns, 1, 0, 1.0, (const double *const *)tab(&DevArrays::LiZ),
                           (const double *const *)tab(&DevArrays::LiZ), 0.0, tab(&DevArrays::Zi), 1));
         // residuals and objectives
-        std::vector<double *> Xs(nb);
-        for (int k = 0; k < nb; k++) Xs[k] = da[k].X;
         std::vector<double> AX;
-        aop_all(Xs, AX);
+        aop_cat(cat.X, AX);
         for (int i = 0; i < m; i++) rp[i] = P.b[i] - AX[i];
         double pobj = 0, xz = 0, rdn2 = 0, nCR2 = 0, dev2 = 0;
-        for (int k = 0; k < nb; k++) {
-            const long long nn = (long long)db[k].n * db[k].n;
-            DevArrays &d = da[k];
-            atop_block(k, y, 1.0, 0.0, d.F);                                                   // A'y
-            RC(ew_lincomb(g.st, nn, 1.0, d.F, 1.0, d.Z, 0.0, nullptr, d.F));                  // A'y + Z
-            RC(ew_lincomb(g.st, nn, 1.0, d.F, -1.0, db[k].C, 0.0, nullptr, d.Fd));            // -Rd
-            RC(ew_lincomb(g.st, nn, 1.0, d.Fd, theta, d.R0, 0.0, nullptr, d.T));              // -Rd + theta R0
+        {
+            atop_cat(y, 1.0, 0.0, cat.F);                                  // A'y
+            lincomb_cat(1.0, cat.F, 1.0, cat.Z, 0.0, nullptr, cat.F);      // A'y + Z
+            lincomb_cat(1.0, cat.F, -1.0, Ccat, 0.0, nullptr, cat.Fd);     // -Rd
+            lincomb_cat(1.0, cat.Fd, theta, cat.R0, 0.0, nullptr, cat.T);  // -Rd + theta R0
             double part[5];
-            const double *aa[5] = {d.F, db[k].C, d.X, d.Fd, d.T}, *bb[5] = {d.F, d.X, d.Z, d.Fd, d.T};
-            dots(5, aa, bb, nn, part);
-            nCR2 += part[0]; pobj += part[1]; xz += part[2]; rdn2 += part[3]; dev2 += part[4];
+            const double *aa[5] = {cat.F, Ccat, cat.X, cat.Fd, cat.T}, *bb[5] = {cat.F, cat.X, cat.Z, cat.Fd, cat.T};
+            dots_cat(5, aa, bb, part);
+            nCR2 = part[0]; pobj = part[1]; xz = part[2]; rdn2 = part[3]; dev2 = part[4];
         }
         double dobj = dot(P.b, y);
         double mu = xz / Ntot;
@@ -1401,12 +1566,10 @@ int Solver::run(ResultData &res) {
             it_best = it;
             best = R;
             ybest = y;
-            if (keep_best)
-                for (int k = 0; k < nb; k++) {
-                    const size_t nn = (size_t)db[k].n * db[k].n;
-                    CU(cudaMemcpyAsync(da[k].Xb, da[k].X, sizeof(double) * nn, cudaMemcpyDeviceToDevice, g.st));
-                    CU(cudaMemcpyAsync(da[k].Zb, da[k].Z, sizeof(double) * nn, cudaMemcpyDeviceToDevice, g.st));
-                }
+            if (keep_best) {
+                CU(cudaMemcpyAsync(cat.Xb, cat.X, sizeof(double) * Ntot2, cudaMemcpyDeviceToDevice, g.st));
+                CU(cudaMemcpyAsync(cat.Zb, cat.Z, sizeof(double) * Ntot2, cudaMemcpyDeviceToDevice, g.st));
+            }
         }
         if (score < opt.tol) { status = 0; break; }
         if (keep_best && it > it_best && dimacs_score(best) <= 0.5 * opt.tol) { status = 4; break; }
@@ -1428,8 +1591,7 @@ int Solver::run(ResultData &res) {
             if (dev > 1e-10 * (1.0 + theta * r0norm) && dev > 1e-12) {
                 theta = 1.0;
                 r0norm = std::sqrt(rdn2);
-                for (int k = 0; k < nb; k++)
-                    RC(ew_lincomb(g.st, (long long)db[k].n * db[k].n, -1.0, da[k].Fd, 0.0, nullptr, 0.0, nullptr, da[k].R0));
+                lincomb_cat(-1.0, cat.Fd, 0.0, nullptr, 0.0, nullptr, cat.R0);
             }
             if (theta * r0norm <= 1e-13) theta = 0.0;
         }
@@ -1464,14 +1626,11 @@ int Solver::run(ResultData &res) {
         td = wtime();
         const bool hasH = theta > 0;
         {
-            std::vector<double *> Zis(nb), Gs(nb);
-            for (int k = 0; k < nb; k++) Zis[k] = da[k].Zi;
-            aop_all(Zis, a0);
+            aop_cat(cat.Zi, a0);
             if (hasH) {
                 mul_all(theta, &DevArrays::Zi, &DevArrays::R0, &DevArrays::T);   // theta Zi R0
                 mul_all(1.0, &DevArrays::T, &DevArrays::X, &DevArrays::G);       // theta Zi R0 X
-                for (int k = 0; k < nb; k++) Gs[k] = da[k].G;
-                aop_all(Gs, h);
+                aop_cat(cat.G, h);
             } else h.assign(m, 0.0);
         }
         tm.dense += wtime() - td;
@@ -1481,27 +1640,22 @@ int Solver::run(ResultData &res) {
         schur_solve(rhs, dy, 1e-7);
         tm.chol += wtime() - tc;
         td = wtime();
-        for (int k = 0; k < nb; k++) {
-            const long long nn = (long long)db[k].n * db[k].n;
-            atop_block(k, dy, -1.0, 0.0, da[k].dZ);
-            RC(ew_lincomb(g.st, nn, 1.0, da[k].dZ, theta, da[k].R0, 0.0, nullptr, da[k].dZ));   // dZ = -A'dy + theta R0
-        }
+        atop_cat(dy, -1.0, 0.0, cat.dZ);
+        lincomb_cat(1.0, cat.dZ, theta, cat.R0, 0.0, nullptr, cat.dZ);   // dZ = -A'dy + theta R0
         mul_all(1.0, &DevArrays::Zi, &DevArrays::dZ, &DevArrays::T);
-        mul_all(1.0, &DevArrays::T, &DevArrays::X, &DevArrays::G);                                 // Zi dZ X
-        for (int k = 0; k < nb; k++)
-            RC(ew_sym_lincomb(g.st, db[k].n, da[k].G, -1.0, -1.0, da[k].X, 0.0, nullptr, da[k].dX)); // dX = -sym(G) - X
+        mul_all(1.0, &DevArrays::T, &DevArrays::X, &DevArrays::G);        // Zi dZ X
+        sym_cat(cat.G, -1.0, -1.0, cat.X, 0.0, nullptr, cat.dX);          // dX = -sym(G) - X
         tm.dense += wtime() - td;
         double tst = wtime();
         const double ap = std::min(1.0, maxstep(1, opt.lanczos_k));
         const double ad = std::min(1.0, maxstep(0, opt.lanczos_k));
         tm.step += wtime() - tst;
         double xdz = 0, dxz = 0, dxdz = 0;
-        for (int k = 0; k < nb; k++) {
-            const long long nn = (long long)db[k].n * db[k].n;
+        {
             double t3[3];
-            const double *aa[3] = {da[k].X, da[k].dX, da[k].dX}, *bb[3] = {da[k].dZ, da[k].Z, da[k].dZ};
-            dots(3, aa, bb, nn, t3);
-            xdz += t3[0]; dxz += t3[1]; dxdz += t3[2];
+            const double *aa[3] = {cat.X, cat.dX, cat.dX}, *bb[3] = {cat.dZ, cat.Z, cat.dZ};
+            dots_cat(3, aa, bb, t3);
+            xdz = t3[0]; dxz = t3[1]; dxdz = t3[2];
         }
         const double mu_a = (xz + ap * dxz + ad * xdz + ap * ad * dxdz) / Ntot;
         const double frac = std::max(0.0, mu_a / mu);
@@ -1524,41 +1678,27 @@ int Solver::run(ResultData &res) {
         // ---- corrector ----
         const double smu = sigma * mu;
         td = wtime();
-        {
-            std::vector<double *> Qs(nb);
-            mul_all(1.0, &DevArrays::Zi, &DevArrays::dZ, &DevArrays::T);
-            mul_all(1.0, &DevArrays::T, &DevArrays::dX, &DevArrays::Q);   // Q = Zi dZp dXp
-            for (int k = 0; k < nb; k++) Qs[k] = da[k].Q;
-            aop_all(Qs, qv);
-        }
+        mul_all(1.0, &DevArrays::Zi, &DevArrays::dZ, &DevArrays::T);
+        mul_all(1.0, &DevArrays::T, &DevArrays::dX, &DevArrays::Q);   // Q = Zi dZp dXp
+        aop_cat(cat.Q, qv);
         for (int i = 0; i < m; i++) rhs[i] = P.b[i] - smu * a0[i] + qv[i] + h[i];
         tm.dense += wtime() - td;
         tc = wtime();
         schur_solve(rhs, dy, 0);
         tm.chol += wtime() - tc;
         td = wtime();
-        for (int k = 0; k < nb; k++) {
-            const long long nn = (long long)db[k].n * db[k].n;
-            atop_block(k, dy, -1.0, 0.0, da[k].dZ);
-            RC(ew_lincomb(g.st, nn, 1.0, da[k].dZ, theta, da[k].R0, 0.0, nullptr, da[k].dZ));
-        }
+        atop_cat(dy, -1.0, 0.0, cat.dZ);
+        lincomb_cat(1.0, cat.dZ, theta, cat.R0, 0.0, nullptr, cat.dZ);
         mul_all(1.0, &DevArrays::Zi, &DevArrays::dZ, &DevArrays::T);
         mul_all(1.0, &DevArrays::T, &DevArrays::X, &DevArrays::G);
-        for (int k = 0; k < nb; k++) {
-            const int n = db[k].n;
-            const long long nn = (long long)n * n;
-            DevArrays &d = da[k];
-            RC(ew_lincomb(g.st, nn, 1.0, d.G, 1.0, d.Q, 0.0, nullptr, d.G));          // Zi dZ X + Q
-            RC(ew_sym_lincomb(g.st, n, d.G, -1.0, smu, d.Zi, -1.0, d.X, d.dX));      // -sym(.) + smu Zi - X
-        }
+        lincomb_cat(1.0, cat.G, 1.0, cat.Q, 0.0, nullptr, cat.G);          // Zi dZ X + Q
+        sym_cat(cat.G, -1.0, smu, cat.Zi, -1.0, cat.X, cat.dX);            // -sym(.) + smu Zi - X
         tm.dense += wtime() - td;
         // ---- refinement of A(dX) = rp ----
         for (int pass = 0; pass < 3; pass++) {
             td = wtime();
-            std::vector<double *> dXs(nb);
-            for (int k = 0; k < nb; k++) dXs[k] = da[k].dX;
             std::vector<double> AdX;
-            aop_all(dXs, AdX);
+            aop_cat(cat.dX, AdX);
             for (int i = 0; i < m; i++) ev[i] = rp[i] - AdX[i];
             const double ne = nrm(ev), nrp = nrm(rp);
             tm.dense += wtime() - td;
@@ -1567,26 +1707,19 @@ int Solver::run(ResultData &res) {
             schur_solve(ev, wv, 0);
             tm.chol += wtime() - tc;
             td = wtime();
-            std::vector<double *> Gs(nb);
-            for (int k = 0; k < nb; k++) atop_block(k, wv, 1.0, 0.0, da[k].W);   // A'w
+            atop_cat(wv, 1.0, 0.0, cat.W);                                       // A'w
             mul_all(1.0, &DevArrays::Zi, &DevArrays::W, &DevArrays::T);
             mul_all(1.0, &DevArrays::T, &DevArrays::X, &DevArrays::F);           // Zi A'w X  (F is free here)
-            for (int k = 0; k < nb; k++) {
-                RC(ew_sym_lincomb(g.st, db[k].n, da[k].F, 1.0, 0.0, nullptr, 0.0, nullptr, da[k].G));
-                Gs[k] = da[k].G;
-            }
+            sym_cat(cat.F, 1.0, 0.0, nullptr, 0.0, nullptr, cat.G);
             std::vector<double> AG;
-            aop_all(Gs, AG);
+            aop_cat(cat.G, AG);
             for (int i = 0; i < m; i++) qv[i] = ev[i] - AG[i];
             const double ne2 = nrm(qv);
             tm.dense += wtime() - td;
             if (!(ne2 < 0.5 * ne)) break;
             for (int i = 0; i < m; i++) dy[i] += wv[i];
-            for (int k = 0; k < nb; k++) {
-                const long long nn = (long long)db[k].n * db[k].n;
-                RC(ew_lincomb(g.st, nn, 1.0, da[k].dZ, -1.0, da[k].W, 0.0, nullptr, da[k].dZ));
-                RC(ew_lincomb(g.st, nn, 1.0, da[k].dX, 1.0, da[k].G, 0.0, nullptr, da[k].dX));
-            }
+            lincomb_cat(1.0, cat.dZ, -1.0, cat.W, 0.0, nullptr, cat.dZ);
+            lincomb_cat(1.0, cat.dX, 1.0, cat.G, 0.0, nullptr, cat.dX);
         }
         tst = wtime();
         const double apr = std::min(1.0, maxstep(1, opt.lanczos_k));
@@ -1596,10 +1729,8 @@ int Solver::run(ResultData &res) {
         // catastrophe guard (solver.c:15138-15158)
         if (R.pinf < 1e-6) {
             td = wtime();
-            std::vector<double *> dXs(nb);
-            for (int k = 0; k < nb; k++) dXs[k] = da[k].dX;
             std::vector<double> AdX;
-            aop_all(dXs, AdX);
+            aop_cat(cat.dX, AdX);
             for (int i = 0; i < m; i++) ev[i] = rp[i] - AdX[i];
             const double nrp = nrm(rp), nev = nrm(ev);
             tm.dense += wtime() - td;
@@ -1631,11 +1762,8 @@ int Solver::run(ResultData &res) {
     if (status != 0 && status != 1 && status != 2 && best_score < res_score(R)) {
         R = best;
         y = ybest;
-        for (int k = 0; k < nb; k++) {
-            const size_t nn = (size_t)db[k].n * db[k].n;
-            CU(cudaMemcpyAsync(da[k].X, da[k].Xb, sizeof(double) * nn, cudaMemcpyDeviceToDevice, g.st));
-            CU(cudaMemcpyAsync(da[k].Z, da[k].Zb, sizeof(double) * nn, cudaMemcpyDeviceToDevice, g.st));
-        }
+        CU(cudaMemcpyAsync(cat.X, cat.Xb, sizeof(double) * Ntot2, cudaMemcpyDeviceToDevice, g.st));
+        CU(cudaMemcpyAsync(cat.Z, cat.Zb, sizeof(double) * Ntot2, cudaMemcpyDeviceToDevice, g.st));
         if (opt.verbose > 1) log_printf(0, "   returning best iterate (iteration %d)\n", it_best);
     }
     final_measures(y, res);
