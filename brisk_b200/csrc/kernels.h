@@ -104,6 +104,16 @@ int schur_densify(cudaStream_t st, const DevBlock &B);
 // (ncon x K x n^2) instead of the entry gather.
 int schur_assemble_dense(cudaStream_t st, const DevBlock &B, const double *X, const double *Zi, double *M, int m,
                          int precision, int chunk, void *ws, size_t ws_bytes);
+// Many small blocks (n <= SB_NMAX) at once: M += each listed block's contribution (FP64), one CTA
+// per block.  The listed blocks must share no constraint.  Per-block data by block id: order d_n,
+// constraint count d_ncon, and device pointer tables of con / cptr / cpos / cval (the full
+// expansion); X and Zi are the concatenations (block k at d_boff[k]); nmax = the largest listed n.
+constexpr int SB_NMAX = 32;
+size_t schur_small_smem(int nmax);
+int schur_assemble_small(cudaStream_t st, int count, const int *d_blocks, int nmax, const int *d_n,
+                         const int *d_ncon, const int *const *con_tab, const long long *const *cptr_tab,
+                         const int *const *cpos_tab, const double *const *cval_tab, const long long *d_boff,
+                         const double *Xcat, const double *Zicat, double *M, int m);
 // Fills B.ccol (device, ncon*(n+1) ints) from cptr/cpos: the column pointers of each constraint.
 int schur_colptr(cudaStream_t st, const DevBlock &B);
 // Upper-triangle lists from the full ones: schur_upper_ptr fills B.uptr (ncon+1; uptr[ncon] is

@@ -629,6 +629,90 @@ int schur_assemble_gram(cudaStream_t st, const DevBlock &B, double *M, int m, vo
     return BGPU_OK;
 }
 
+// ---- many small blocks at once ----------------------------------------------------------------
+// One CTA per block (n <= SB_NMAX), one warp per constraint a of the block: W = A_a Zi row by row
+// from a's entries (W[p, :] += v Zi[q, :]), G = X W over the rows A_a touches, then
+// M[a, b] = <A_b, G> for the block's b >= a, a warp sum per b.  The blocks of one launch share no
+// constraint (the caller colours them), so every M entry has one writer per launch and the
+// launches add in a fixed order.
+namespace {
+constexpr int SB_W = 8;   // warps per CTA
+__global__ void __launch_bounds__(SB_W * 32) small_schur_kernel(
+    const int *__restrict__ blocks, const int *__restrict__ bn, const int *__restrict__ bncon,
+    const int *const *__restrict__ con_tab, const long long *const *__restrict__ cptr_tab,
+    const int *const *__restrict__ cpos_tab, const double *const *__restrict__ cval_tab,
+    const long long *__restrict__ boff, const double *__restrict__ Xcat, const double *__restrict__ Zcat, double *M,
+    int m) {
+    extern __shared__ __align__(16) double sb_sm[];
+    const int k = blocks[blockIdx.x];
+    const int n = bn[k], ncon = bncon[k], nn = n * n;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double *Xs = sb_sm, *Zs = sb_sm + nn;
+    double *W = sb_sm + 2 * nn + (size_t)warp * 2 * nn, *G = W + nn;
+    const double *X = Xcat + boff[k], *Zi = Zcat + boff[k];
+    for (int i = threadIdx.x; i < nn; i += SB_W * 32) { Xs[i] = X[i]; Zs[i] = Zi[i]; }
+    __syncthreads();
+    const int *con = con_tab[k];
+    const long long *cptr = cptr_tab[k];
+    const int *cpos = cpos_tab[k];
+    const double *cval = cval_tab[k];
+    for (int a = warp; a < ncon; a += SB_W) {
+        for (int i = lane; i < nn; i += 32) W[i] = 0.0;
+        __syncwarp();
+        unsigned long long rows = 0;
+        for (long long e = cptr[a]; e < cptr[a + 1]; e++) {   // every lane walks the entries in order
+            const int pos = cpos[e], q = pos / n, p = pos - q * n;
+            const double v = cval[e];
+            rows |= 1ull << p;
+            for (int j = lane; j < n; j += 32) W[p + j * n] += v * Zs[q + j * n];   // Zi symmetric
+            __syncwarp();
+        }
+        for (int i = lane; i < nn; i += 32) {   // G = X W over the touched rows
+            const int r = i % n, c = i / n;
+            double acc = 0.0;
+            for (unsigned long long b = rows; b; b &= b - 1) {
+                const int p = __ffsll((long long)b) - 1;
+                acc += Xs[r + p * n] * W[p + c * n];
+            }
+            G[i] = acc;
+        }
+        __syncwarp();
+        const int ca = con[a];
+        for (int b = a; b < ncon; b++) {
+            double sum = 0.0;
+            for (long long e = cptr[b] + lane; e < cptr[b + 1]; e += 32) sum += cval[e] * G[cpos[e]];
+            sum = warp_sum(sum);
+            if (lane == 0) {
+                const int cb = con[b];
+                M[(long long)ca + (long long)cb * m] += sum;
+                if (ca != cb) M[(long long)cb + (long long)ca * m] += sum;
+            }
+        }
+        __syncwarp();
+    }
+}
+}  // namespace
+
+size_t schur_small_smem(int nmax) { return (size_t)(2 + 2 * SB_W) * nmax * nmax * sizeof(double); }
+
+int schur_assemble_small(cudaStream_t st, int count, const int *d_blocks, int nmax, const int *d_n,
+                         const int *d_ncon, const int *const *con_tab, const long long *const *cptr_tab,
+                         const int *const *cpos_tab, const double *const *cval_tab, const long long *d_boff,
+                         const double *Xcat, const double *Zicat, double *M, int m) {
+    if (count <= 0) return BGPU_OK;
+    if (nmax <= 0 || nmax > SB_NMAX) return BGPU_ERR_ARG;
+    static bool attr = false;
+    if (!attr) {
+        BGPU_CHECK(cudaFuncSetAttribute(small_schur_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)schur_small_smem(SB_NMAX)));
+        attr = true;
+    }
+    small_schur_kernel<<<count, SB_W * 32, schur_small_smem(nmax), st>>>(d_blocks, d_n, d_ncon, con_tab, cptr_tab,
+                                                                         cpos_tab, cval_tab, d_boff, Xcat, Zicat, M, m);
+    BGPU_LAUNCH_CHECK();
+    return BGPU_OK;
+}
+
 // ---- the dense route -------------------------------------------------------------------------
 namespace {
 __global__ void densify_kernel(int n, int ncon, const long long *__restrict__ cptr, const int *__restrict__ cpos,

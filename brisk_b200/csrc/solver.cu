@@ -498,6 +498,16 @@ class Solver {
     const double **d_pvt = nullptr;
     DevBlock gall;
     void build_gall();
+    // many small blocks (n <= SB_NMAX, two or more): assembled by one kernel per colour class of
+    // blocks that share no constraint
+    std::vector<char> in_sb;
+    std::vector<int> sb_coff, sb_nmax;   // colour c: d_sb_list[sb_coff[c] .. sb_coff[c+1]), its largest n
+    int *d_sb_list = nullptr, *d_sb_ncon = nullptr;
+    const int **d_sb_con = nullptr, **d_sb_cpos = nullptr;
+    const long long **d_sb_cptr = nullptr;
+    const double **d_sb_cval = nullptr;
+    void setup_small_schur();
+    void assemble_small(const double *Xc, const double *Zc);
     void aop_cat(const double *D, std::vector<double> &out);                                    // out = A(D)
     void atop_cat(const std::vector<double> &y, double alpha, double beta, double *F);         // F = a A'y + b F
     void sym_cat(const double *G, double s, double a, const double *x, double b, const double *y, double *out);
@@ -683,6 +693,7 @@ void Solver::setup() {
     build_gall();
     if (opt.verbose > 1) log_printf(0, "   [device context %.3fs, block upload %.3fs]\n", t1 - t0, wtime() - t1);
     for (int k = 0; k < nb; k++) (P.blk[k].n <= SMALL_N_MAX ? small_ids : big_ids).push_back(k);
+    setup_small_schur();
     if (!small_ids.empty()) {
         const int ns = (int)small_ids.size();
         std::vector<int> nsz(ns);
@@ -834,6 +845,75 @@ void Solver::build_gall() {
     upload_bytes += (double)ne * 12 + (double)m * 12;
 }
 
+void Solver::setup_small_schur() {
+    in_sb.assign(nb, 0);
+    std::vector<int> ids;
+    for (int k : small_ids)
+        if (db[k].n <= SB_NMAX && db[k].ncon > 0) ids.push_back(k);
+    if (ids.size() < 2) return;
+    // greedy colouring: the first colour none of whose blocks shares a constraint with k
+    std::vector<std::vector<char>> used;
+    std::vector<std::vector<int>> cls;
+    for (int k : ids) {
+        const auto &con = P.blk[k].con;
+        size_t c = 0;
+        for (; c < used.size(); c++) {
+            bool clash = false;
+            for (int x : con)
+                if (used[c][x]) { clash = true; break; }
+            if (!clash) break;
+        }
+        if (c == used.size()) { used.emplace_back(m, 0); cls.emplace_back(); }
+        for (int x : con) used[c][x] = 1;
+        cls[c].push_back(k);
+    }
+    std::vector<int> list;
+    sb_coff.assign(1, 0);
+    sb_nmax.clear();
+    for (auto &cl : cls) {
+        int nm = 1;
+        for (int k : cl) { list.push_back(k); nm = std::max(nm, db[k].n); }
+        sb_coff.push_back((int)list.size());
+        sb_nmax.push_back(nm);
+    }
+    std::vector<int> ncon(nb, 0);
+    std::vector<const int *> con(nb, nullptr), cpos(nb, nullptr);
+    std::vector<const long long *> cptr(nb, nullptr);
+    std::vector<const double *> cval(nb, nullptr);
+    for (int k = 0; k < nb; k++) {
+        ncon[k] = db[k].ncon;
+        con[k] = db[k].con;
+        cptr[k] = db[k].cptr;
+        cpos[k] = db[k].cpos;
+        cval[k] = db[k].cval;
+    }
+    d_sb_list = g.alloc<int>(list.size());
+    d_sb_ncon = g.alloc<int>(nb);
+    d_sb_con = (const int **)g.alloc<int *>(nb);
+    d_sb_cpos = (const int **)g.alloc<int *>(nb);
+    d_sb_cptr = (const long long **)g.alloc<long long *>(nb);
+    d_sb_cval = (const double **)g.alloc<double *>(nb);
+    if (!d_sb_list || !d_sb_ncon || !d_sb_con || !d_sb_cpos || !d_sb_cptr || !d_sb_cval)
+        throw GpuFail{BGPU_ERR_NOMEM, __LINE__};
+    CU(cudaMemcpyAsync(d_sb_list, list.data(), sizeof(int) * list.size(), cudaMemcpyHostToDevice, g.st));
+    CU(cudaMemcpyAsync(d_sb_ncon, ncon.data(), sizeof(int) * nb, cudaMemcpyHostToDevice, g.st));
+    CU(cudaMemcpyAsync(d_sb_con, con.data(), sizeof(void *) * nb, cudaMemcpyHostToDevice, g.st));
+    CU(cudaMemcpyAsync(d_sb_cpos, cpos.data(), sizeof(void *) * nb, cudaMemcpyHostToDevice, g.st));
+    CU(cudaMemcpyAsync(d_sb_cptr, cptr.data(), sizeof(void *) * nb, cudaMemcpyHostToDevice, g.st));
+    CU(cudaMemcpyAsync(d_sb_cval, cval.data(), sizeof(void *) * nb, cudaMemcpyHostToDevice, g.st));
+    CU(cudaStreamSynchronize(g.st));
+    for (int k : ids) in_sb[k] = 1;
+    if (opt.verbose > 1)
+        log_printf(0, "   [small blocks: %d assembled in %d launches of blocks sharing no constraint]\n", (int)ids.size(),
+                   (int)cls.size());
+}
+
+void Solver::assemble_small(const double *Xc, const double *Zc) {
+    for (size_t c = 0; c + 1 < sb_coff.size(); c++)
+        RC(schur_assemble_small(g.st, sb_coff[c + 1] - sb_coff[c], d_sb_list + sb_coff[c], sb_nmax[c], d_bn, d_sb_ncon,
+                                d_sb_con, d_sb_cptr, d_sb_cpos, d_sb_cval, d_boff, Xc, Zc, M, m));
+}
+
 void Solver::aop_cat(const double *D, std::vector<double> &out) {
     CU(cudaMemsetAsync(dv_out, 0, sizeof(double) * m, g.st));
     RC(aop_f64(g.st, gall, D, 1.0, 1.0, dv_out));
@@ -897,7 +977,12 @@ void Solver::assemble(std::vector<double> &) {
     CU(cudaEventRecord(ev0, g.st));
     const int prec = (asm_prec == 1 && !asm_fp64) ? 1 : 0;
     m_exact = prec == 0;
+    assemble_small(cat.X, cat.Zi);
     for (int k = 0; k < nb; k++) {
+        if (in_sb[k]) {
+            schur_flops += 2.0 * db[k].n * db[k].n * db[k].n * db[k].ncon;
+            continue;
+        }
         if (dense_route[k])
             RC(schur_assemble_dense(g.st, db[k], da[k].X, da[k].Zi, M, m, prec, prec ? chunk : chunk64, ws, ws_bytes));
         else
@@ -1250,7 +1335,9 @@ void Solver::least_squares_start(std::vector<double> &y) {
     allow_float = false;   // the start's Gram solves in FP64
     m_exact = true;        // A A' is assembled in FP64 here
     CU(cudaMemsetAsync(M, 0, sizeof(double) * (size_t)m * m, g.st));
+    assemble_small(Icat, Icat);   // the Gram matrix of the small blocks: X = Zi = I
     for (int k = 0; k < nb; k++) {
+        if (in_sb[k]) continue;
         RC(ew_set_scaled_identity(g.st, db[k].n, da[k].T, 1.0));
         if (dense_route[k]) RC(schur_assemble_dense(g.st, db[k], da[k].T, da[k].T, M, m, 0, chunk_fp64(k), ws, ws_bytes));
         else RC(schur_assemble_gram(g.st, db[k], M, m, ws, ws_bytes));
