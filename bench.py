@@ -36,13 +36,32 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 WORKLOADS = {
-    "rand400": dict(gen=dict(n=400, m=2000, density=0.01, seed=0),
+    "rand400": dict(kind="random", gen=dict(n=400, m=2000, density=0.01, seed=0),
                     desc="random SDP: one 400x400 block, m=2000, A_i 1% dense N(0,1), b=A(I), C=GG'/n+I, seed 0",
                     paths={"fp64": ["-mixed", "0"]}, primary="fp64"),
-    "rand1000": dict(gen=dict(n=1000, m=8000, density=0.005, seed=0),
+    "rand1000": dict(kind="random", gen=dict(n=1000, m=8000, density=0.005, seed=0),
                      desc="random SDP: one 1000x1000 block, m=8000, A_i 0.5% dense N(0,1), b=A(I), C=GG'/n+I, seed 0",
-                     paths={"mixed": ["-asmprec", "tf32x3"], "fp64": ["-mixed", "0"]}, primary="mixed"),
+                     paths={"mixed": ["-asmprec", "tf32x3"], "fp64": ["-mixed", "0"]}, primary="mixed",
+                     ref_maxit=1),
+    "mom60": dict(kind="moment", gen=dict(nvars=60, clique=4, seed=0),
+                  desc="degree-2 moment relaxation of a seeded quartic in 60 variables, cliques of 4 consecutive "
+                       "variables: 57 blocks of 15, m=2029, sparse Schur factor",
+                  paths={"fp64": ["-mixed", "0"]}, primary="fp64"),
+    "mom700": dict(kind="moment", gen=dict(nvars=700, clique=4, seed=0),
+                   desc="the same moment relaxation in 700 variables: 697 blocks of 15, m=24429, sparse Schur factor",
+                   paths={"fp64": ["-mixed", "0"]}, primary="fp64"),
+    "batch": dict(kind="batch", gen=dict(nmin=8, nmax=64, seed=0),
+                  desc="batch of independent dense random SDPs: n ~ U{8..64}, m ~ U{n..n(n+1)/4}, A_i dense N(0,1) "
+                       "symmetric, b=A(I), C=GG'/n+I, seed 0",
+                  paths={"fp64": ["-mixed", "0"]}, primary="fp64"),
 }
+
+
+def make_instance(w):
+    from brisk_b200 import problems
+    if w["kind"] == "moment":
+        return problems.moment_relaxation(**w["gen"])
+    return problems.random_sdp(**w["gen"])
 BASE_OPTS = ["-nohsd", "-dir", "hkm", "-tol", "1e-7", "-q"]
 
 
@@ -183,13 +202,169 @@ def cpu_reference_sample(d, workload, threads, opts_extra):
             "cmd": " ".join(["brisk_ref", workload + ".dat-s"] + cmd[2:])}
 
 
+def _ref_batch_one(q):
+    """One batch instance solved by the reference on one thread: (solve time, status)."""
+    from brisk_b200 import problems
+    from brisk_b200.problems import write_sdpa
+    ref = os.path.join(ROOT, "oracle", "_ref", "brisk_ref")
+    d = problems.batch_instance(q)
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, f"b{q}.dat-s")
+        write_sdpa(d, path)
+        cmd = [ref, path, "-nohsd", "-dir", "hkm", "-tol", "1e-7", "-mixed", "0", "-v", "-threads", "1"]
+        p = subprocess.run(cmd, capture_output=True, text=True, env=dict(os.environ, BRISK_NOBUSY="1"), timeout=3600)
+    out = p.stdout + p.stderr
+    tt = re.search(r"time: total (\S+)s \(read (\S+),", out)
+    st = re.search(r"^status: (.+?)\s+iterations", out, re.M)
+    if not tt:
+        return None
+    return float(tt.group(1)) - float(tt.group(2)), (st.group(1).strip() if st else None)
+
+
+def cpu_reference_batch(count, sample):
+    """The reference on a bounded sample of the batch: `sample` instances spread over the batch,
+    each solved on one thread, one process per host core (the batch's natural CPU form: its
+    instances are independent).  Scaled to the whole batch: sum of the sample's solve times x
+    count / sample / cores."""
+    import multiprocessing as mp
+    if not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "brisk_ref")):
+        return None
+    qs = [int(round(k * count / sample)) for k in range(sample)]
+    cores = os.cpu_count() or 1
+    t0 = time.time()
+    with mp.get_context("spawn").Pool(cores) as pool:
+        res = pool.map(_ref_batch_one, qs)
+    wall = time.time() - t0
+    if any(r is None for r in res):
+        return {"error": "a reference solve failed"}
+    tsum = sum(r[0] for r in res)
+    nopt = sum(1 for r in res if r[1] == "OPTIMAL")
+    return {"value": tsum * count / sample / cores, "cores": cores, "sum": tsum, "wall": wall,
+            "sample": f"{sample} instances spread over the {count} (every {count // sample}-th), one thread each, "
+                      f"{nopt}/{sample} OPTIMAL, sum of solve times {tsum:.1f} s; scaled: sum x {count}/{sample} / "
+                      f"{cores} cores"}
+
+
+def run_reference_batch(args, w):
+    r = cpu_reference_batch(args.batch_count, min(args.batch_count, args.batch_sample))
+    if r is None or "error" in r:
+        print(json.dumps({"impl": "reference", "unavailable": (r or {}).get("error", "oracle/_ref/brisk_ref absent")}))
+        return
+    v = r["value"]
+    print(json.dumps({"impl": "reference", "metric": "time_to_1e-7_dimacs_s", "value": v, "unit": "s",
+                      "n_gpus": args.gpus, "steps": 1, "warmup": 0, "ms_per_step": v * 1e3, "higher_is_better": False,
+                      "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
+                      "config": {"workload": "batch", "count": args.batch_count, "desc": w["desc"],
+                                 "parallelism": "one process per host core"},
+                      "cpu_baseline": {"value": v, "unit": "s", "cores": r["cores"], "kind": "reference",
+                                       "sample": r["sample"]},
+                      "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
+          flush=True)
+
+
+def run_ours_batch(args, w, torch):
+    """The batch through bgpu_batch_solve (host arrays in, results out: the call a user makes).
+    A step is the whole batch; the warm-up steps solve its first 64 instances."""
+    from brisk_b200 import _core, problems, step
+    rank, world, local = dist_info()
+    L = _core.load_library()
+    S = step.lib()
+    S.bgpu_launch_count.restype = ctypes.c_longlong
+    S.bgpu_result_measures.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+    count = args.batch_count
+    t0 = time.time()
+    full = problems.batch_arrays(count, **w["gen"])
+    gen_s = time.time() - t0
+    warm = problems.batch_arrays(min(64, count), **w["gen"])
+    opts = BASE_OPTS + w["paths"]["fp64"] + ["-device", str(local)]
+    av = (ctypes.c_char_p * len(opts))(*[o.encode() for o in opts])
+    pi = ctypes.POINTER(ctypes.c_int)
+    pd = ctypes.POINTER(ctypes.c_double)
+
+    def solve(a):
+        cnt = int(a["m"].size)
+        handles = (ctypes.c_void_p * cnt)(*[L.brisk_result_new() for _ in range(cnt)])
+        rcs = np.zeros(cnt, np.intc)
+        P = lambda x, t: x.ctypes.data_as(t)   # noqa: E731
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        rc = L.bgpu_batch_solve(cnt, P(a["m"], pi), P(a["nblk"], pi), P(a["bs"], pi), P(a["c"], pd),
+                                a["nnz"].ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), P(a["mat"], pi),
+                                P(a["blk"], pi), P(a["i"], pi), P(a["j"], pi), P(a["v"], pd), len(opts), av,
+                                args.batch_workers, handles, P(rcs, pi))
+        e1.record()
+        torch.cuda.synchronize()
+        if rc != 0:
+            raise RuntimeError(f"bgpu_batch_solve returned {rc}")
+        t = e0.elapsed_time(e1) * 1e-3
+        st = {}
+        meas = (ctypes.c_double * 8)()
+        h2d = d2h = its = 0.0
+        worst = 0.0
+        for q in range(cnt):
+            s_ = L.brisk_result_status_str(handles[q]).decode()
+            st[s_] = st.get(s_, 0) + 1
+            S.bgpu_result_measures(handles[q], meas)
+            h2d += meas[3]
+            d2h += meas[4]
+            its += meas[5]
+            dm = (ctypes.c_double * 6)()
+            L.brisk_result_dimacs(handles[q], dm)
+            worst = max(worst, max(abs(x) for x in dm))
+            L.brisk_result_delete(handles[q])
+        return t, st, h2d, d2h, its, worst
+
+    for _ in range(args.warmup):
+        solve(warm)
+    times = []
+    l0 = S.bgpu_launch_count()
+    with Clocks(local) as clk:
+        for _ in range(args.steps):
+            t, st, h2d, d2h, its, worst = solve(full)
+            times.append(t)
+    launches = (S.bgpu_launch_count() - l0) / args.steps
+    v = statistics.mean(times)
+    if world > 1:
+        tt = torch.tensor([v], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        v = float(tt.item())
+    sizes = list(zip(full["bs"].tolist(), full["m"].tolist()))
+    asm_flops = sum(m * (4.0 * n ** 3 + 2.0 * n * n * m) for n, m in sizes)
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline and world == 1:
+        r = cpu_reference_batch(count, min(count, args.batch_sample))
+        if r and "error" not in r:
+            cpu = {"value": r["value"], "unit": "s", "cores": r["cores"], "kind": "reference", "sample": r["sample"]}
+        else:
+            cpu = {"value": None, "error": (r or {}).get("error", "oracle/_ref/brisk_ref absent")}
+    if rank == 0:
+        print(json.dumps({
+            "metric": "time_to_1e-7_dimacs_s", "value": v, "unit": "s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
+            "config": {"workload": "batch", "count": count, "desc": w["desc"], "workers": args.batch_workers,
+                       "l2": "inputs (host arrays) larger than L2", "parallelism": f"replicas x{world}",
+                       "warmup_note": "warm-up steps solve the first 64 instances", "generation_s": round(gen_s, 1)},
+            "status": st, "dimacs_max": worst, "iterations_total": int(its),
+            "instances_per_s": count / v, "assembly_flops_per_iteration": asm_flops,
+            "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                    "note": "the batch API takes host arrays: value and e2e are the same call"},
+            "gpu_launches": int(launches), "clocks": clk.summary(), "roofline": None,
+            "roofline_note": "many small independent solves: latency-bound, no dominant kernel",
+            "cpu_baseline": cpu}), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
 def run_reference(args):
     rank, world, local = dist_info()
     if rank != 0:
         return
-    from brisk_b200 import problems
     w = WORKLOADS[args.workload]
-    d = problems.random_sdp(**w["gen"])
+    if w["kind"] == "batch":
+        return run_reference_batch(args, w)
+    d = make_instance(w)
     threads = os.cpu_count() or 1
     opts = w["paths"]["fp64"] if w["primary"] == "fp64" else []
     times = []
@@ -234,7 +409,9 @@ def run_ours(args):
     S.bgpu_result_measures.argtypes = [P, P]
     S.bgpu_launch_count.restype = ctypes.c_longlong
     w = WORKLOADS[args.workload]
-    d = problems.random_sdp(**w["gen"])
+    if w["kind"] == "batch":
+        return run_ours_batch(args, w, torch)
+    d = make_instance(w)
     bs, c, mat, blk, ii, jj, v = [np.ascontiguousarray(a) for a in d.args()]
     bs = bs.astype(np.intc); mat = mat.astype(np.intc); blk = blk.astype(np.intc)
     ii = ii.astype(np.intc); jj = jj.astype(np.intc)
@@ -309,19 +486,27 @@ def run_ours(args):
             results[pname]["e2e"] = dict(value=statistics.mean(e2e_times), h2d=meas[3], d2h=meas[4])
         L.brisk_result_delete(res)
     prim = results[w["primary"]]
-    n = w["gen"]["n"]
     roof = None
     cpu = None
     if rank == 0:
-        peak64 = measure_fp64_peak(torch)
-        roof = gemm_roofline(torch, step, n, step.chunk_default(n, 0), peak64)
+        if w["kind"] == "random":
+            peak64 = measure_fp64_peak(torch)
+            roof = gemm_roofline(torch, step, w["gen"]["n"], step.chunk_default(w["gen"]["n"], 0), peak64)
         if not args.no_cpu_baseline and world == 1:
             threads = os.cpu_count() or 1
             opts_ref = w["paths"]["fp64"] if w["primary"] == "fp64" else []
-            r = cpu_reference_sample(d, args.workload, threads, opts_ref)
-            if r and "error" not in r:
+            maxit = w.get("ref_maxit")
+            r = cpu_reference_sample(d, args.workload, threads, opts_ref + (["-maxit", str(maxit)] if maxit else []))
+            if r and "error" not in r and not maxit:
                 cpu = {"value": r["time"], "unit": "s", "cores": threads, "kind": "reference",
                        "sample": f"one full reference solve to 1e-7 ({r['status']}, {r['iterations']} iterations)"}
+            elif r and "error" not in r:
+                # the full reference solve takes tens of minutes: a bounded sample of `maxit` iterations
+                # (start included), scaled to the iterations this build's solve took
+                per_it = r["time"] / max(1, maxit)
+                cpu = {"value": per_it * prim["iterations"], "unit": "s", "cores": threads, "kind": "reference",
+                       "sample": f"reference solve stopped after {maxit} iteration(s) ({r['time']:.1f} s, start "
+                                 f"included), scaled to {prim['iterations']} iterations"}
             else:
                 cpu = {"value": None, "error": (r or {}).get("error", "oracle/_ref/brisk_ref absent")[-300:]}
     if world > 1:
@@ -339,6 +524,7 @@ def run_ours(args):
                         "d2h_bytes_per_step": int(prim["e2e"]["d2h"])},
                 "gpu_launches": int(prim["launches_per_step"] * prim["steps"]),
                 "clocks": prim["clocks"], "roofline": roof, "cpu_baseline": cpu,
+                "roofline_note": None if roof else "no dominant GEMM on this workload (small blocks, sparse factor)",
                 "paths": {k: {kk: vv for kk, vv in r.items() if kk in ("value", "status", "iterations", "schur_tflops")}
                           for k, r in results.items()}}
         print(json.dumps(line), flush=True)
@@ -354,6 +540,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="rand400", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch-count", type=int, default=4096, help="instances of the batch workload")
+    ap.add_argument("--batch-workers", type=int, default=16, help="host workers of bgpu_batch_solve")
+    ap.add_argument("--batch-sample", type=int, default=64, help="instances the reference solves for its sample")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

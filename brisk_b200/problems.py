@@ -195,6 +195,35 @@ def random_dense_batch(count: int = 4096, nmin: int = 8, nmax: int = 64, seed: i
     return out
 
 
+def batch_arrays(count: int = 4096, nmin: int = 8, nmax: int = 64, seed: int = 0, first: int = 0,
+                 total: int = 4096):
+    """Instances first .. first+count-1 of random_dense_batch(total, ...) (batch_instance(q)) as
+    the concatenated arrays of solve_batch_arrays, filled one instance at a time (peak memory:
+    the arrays plus one instance)."""
+    sizes = random_dense_batch(max(total, first + count), nmin, nmax, seed, sizes_only=True)[first:first + count]
+    tri = [n * (n + 1) // 2 for n, _ in sizes]
+    nnz = np.array([t * (m + 1) for t, (_, m) in zip(tri, sizes)], np.int64)
+    tot = int(nnz.sum())
+    out = dict(m=np.array([m for _, m in sizes], np.intc), nblk=np.ones(count, np.intc),
+               bs=np.array([n for n, _ in sizes], np.intc), c=np.empty(sum(m for _, m in sizes)),
+               nnz=nnz, mat=np.empty(tot, np.intc), blk=np.ones(tot, np.intc), i=np.empty(tot, np.intc),
+               j=np.empty(tot, np.intc), v=np.empty(tot))
+    e = cc = 0
+    for q, (n, m) in enumerate(sizes):
+        d = random_dense_instance(np.random.default_rng([seed, first + q]), int(n), int(m))
+        k = d.v.size
+        if k != nnz[q]:
+            raise RuntimeError("batch instance size mismatch")
+        out["mat"][e:e + k] = d.mat
+        out["i"][e:e + k] = d.i
+        out["j"][e:e + k] = d.j
+        out["v"][e:e + k] = d.v
+        out["c"][cc:cc + m] = d.c
+        e += k
+        cc += m
+    return out
+
+
 def batch_instance(q: int, count: int = 4096, nmin: int = 8, nmax: int = 64, seed: int = 0) -> SdpaData:
     """Instance q of random_dense_batch(count, nmin, nmax, seed), made without the others."""
     n, m = random_dense_batch(count, nmin, nmax, seed, sizes_only=True)[q]
