@@ -170,6 +170,12 @@ int parse_options(int argc, const char *const *argv, Options &opt, std::string &
             opt.verbose = 3;
         } else if (a == "-nohsd" || a == "-nofr" || a == "-feasible") {
             if (a == "-feasible") opt.known_feasible = 1;
+        } else if (a == "-batchmode") {
+            const char *s = need("lockstep or concurrent");
+            if (!s) return 1;
+            if (!strcmp(s, "lockstep")) opt.batch_mode = 1;
+            else if (!strcmp(s, "concurrent")) opt.batch_mode = 0;
+            else { err = "bad -batchmode (lockstep or concurrent)"; return 1; }
         } else if (a == "-sparse") {
             const char *s = need("-1, 0 or 1");
             if (!s || !parse_int(s, opt.sparse) || opt.sparse < -1 || opt.sparse > 1) {

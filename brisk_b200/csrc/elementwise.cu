@@ -77,7 +77,90 @@ __global__ void scaled_identity_blocks_kernel(int nb, const int *__restrict__ ns
     const long long l = g - off[k];
     out[g] = (l % (n + 1) == 0) ? v[k] : 0.0;
 }
+// per-block coefficients: out = ca[k] x + cb[k] y + cc[k] z on block k (a null coefficient array
+// or operand counts as zero)
+__global__ void lincomb_coef_kernel(int nb, const long long *__restrict__ off, long long total,
+                                    const double *__restrict__ ca, const double *x, const double *__restrict__ cb,
+                                    const double *y, const double *__restrict__ cc, const double *z, double *out) {
+    const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= total) return;
+    const int k = block_of(g, nb, off);
+    double v = 0.0;
+    if (ca && x) v += ca[k] * x[g];
+    if (cb && y) v += cb[k] * y[g];
+    if (cc && z) v += cc[k] * z[g];
+    out[g] = v;
+}
+
+// out = cs[k] sym(G) + ca[k] x + cb[k] y on block k
+__global__ void sym_coef_kernel(int nb, const int *__restrict__ ns, const long long *__restrict__ off, long long total,
+                                const double *G, const double *__restrict__ cs, const double *__restrict__ ca,
+                                const double *x, const double *__restrict__ cb, const double *y, double *out) {
+    const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= total) return;
+    const int k = block_of(g, nb, off), n = ns[k];
+    const long long l = g - off[k];
+    const int j = (int)(l / n), i = (int)(l - (long long)j * n);
+    const long long q = off[k] + j + (long long)i * n;
+    double v = cs[k] * 0.5 * (G[g] + G[q]);
+    if (ca && x) v += ca[k] * x[g];
+    if (cb && y) v += cb[k] * y[g];
+    out[g] = v;
+}
+
+// V += inc[k] dV and L = V on block k
+__global__ void step_copy_coef_kernel(int nb, const long long *__restrict__ off, long long total,
+                                      const double *__restrict__ inc, const double *__restrict__ dV, double *V,
+                                      double *L) {
+    const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= total) return;
+    const int k = block_of(g, nb, off);
+    const double v = V[g] + inc[k] * dV[g];
+    V[g] = v;
+    L[g] = v;
+}
+
+// dst = src on the blocks with flag[k] != 0
+__global__ void copy_masked_kernel(int nb, const long long *__restrict__ off, long long total, const int *__restrict__ flag,
+                                   const double *__restrict__ src, double *dst) {
+    const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= total) return;
+    if (flag[block_of(g, nb, off)]) dst[g] = src[g];
+}
 }  // namespace
+
+int ew_lincomb_coef(cudaStream_t st, int nb, const long long *d_off, long long total, const double *ca,
+                    const double *x, const double *cb, const double *y, const double *cc, const double *z,
+                    double *out) {
+    if (total <= 0 || nb <= 0) return BGPU_OK;
+    lincomb_coef_kernel<<<ceil_div(total, 256), 256, 0, st>>>(nb, d_off, total, ca, x, cb, y, cc, z, out);
+    BGPU_LAUNCH_CHECK();
+    return BGPU_OK;
+}
+
+int ew_sym_coef(cudaStream_t st, int nb, const int *d_n, const long long *d_off, long long total, const double *G,
+                const double *cs, const double *ca, const double *x, const double *cb, const double *y, double *out) {
+    if (total <= 0 || nb <= 0) return BGPU_OK;
+    sym_coef_kernel<<<ceil_div(total, 256), 256, 0, st>>>(nb, d_n, d_off, total, G, cs, ca, x, cb, y, out);
+    BGPU_LAUNCH_CHECK();
+    return BGPU_OK;
+}
+
+int ew_step_copy_coef(cudaStream_t st, int nb, const long long *d_off, long long total, const double *inc,
+                      const double *dV, double *V, double *L) {
+    if (total <= 0 || nb <= 0) return BGPU_OK;
+    step_copy_coef_kernel<<<ceil_div(total, 256), 256, 0, st>>>(nb, d_off, total, inc, dV, V, L);
+    BGPU_LAUNCH_CHECK();
+    return BGPU_OK;
+}
+
+int ew_copy_masked(cudaStream_t st, int nb, const long long *d_off, long long total, const int *flag,
+                   const double *src, double *dst) {
+    if (total <= 0 || nb <= 0) return BGPU_OK;
+    copy_masked_kernel<<<ceil_div(total, 256), 256, 0, st>>>(nb, d_off, total, flag, src, dst);
+    BGPU_LAUNCH_CHECK();
+    return BGPU_OK;
+}
 
 int ew_sym_lincomb_blocks(cudaStream_t st, int nb, const int *d_n, const long long *d_off, long long total,
                           const double *G, double s, double a, const double *x, double b, const double *y,

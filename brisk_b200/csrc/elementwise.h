@@ -21,3 +21,15 @@ int ew_sym_lincomb_blocks(cudaStream_t st, int nb, const int *d_n, const long lo
                           double *out);
 int ew_scaled_identity_blocks(cudaStream_t st, int nb, const int *d_n, const long long *d_off, long long total,
                               const double *d_v, const int *d_only, double *out);
+// Per-block coefficients (device arrays of nb values; a null array or operand counts as zero):
+// out = ca x + cb y + cc z;  out = cs sym(G) + ca x + cb y;  V += inc dV, L = V;  dst = src on the
+// blocks whose flag is set.
+int ew_lincomb_coef(cudaStream_t st, int nb, const long long *d_off, long long total, const double *ca,
+                    const double *x, const double *cb, const double *y, const double *cc, const double *z,
+                    double *out);
+int ew_sym_coef(cudaStream_t st, int nb, const int *d_n, const long long *d_off, long long total, const double *G,
+                const double *cs, const double *ca, const double *x, const double *cb, const double *y, double *out);
+int ew_step_copy_coef(cudaStream_t st, int nb, const long long *d_off, long long total, const double *inc,
+                      const double *dV, double *V, double *L);
+int ew_copy_masked(cudaStream_t st, int nb, const long long *d_off, long long total, const int *flag,
+                   const double *src, double *dst);

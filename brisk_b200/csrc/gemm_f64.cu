@@ -38,23 +38,15 @@ __device__ __forceinline__ void dmma16(double (&c)[4], double a0, double a1, dou
                  : "d"(a0), "d"(a1), "d"(b0));
 }
 
+// One BM x BN tile of C at (i0, j0).
 template <bool A_KM, bool B_KM, int BN>
-__global__ void __launch_bounds__(NT, (BN <= 64) ? 2 : 1) dgemm_kernel(int M, int N, int K, double alpha,
-                                                   const double *A, long long lda, long long sA,
-                                                   const double *B, long long ldb, long long sB,
-                                                   double beta, double *C, long long ldc, long long sC,
-                                                   int lower) {
+__device__ __forceinline__ void gemm_tile(int i0, int j0, int M, int N, int K, double alpha, const double *A,
+                                          long long lda, const double *B, long long ldb, double beta, double *C,
+                                          long long ldc, int lower, double *smem) {
     constexpr int LDB_N = TileN<BN>::LDB_N, B_STAGE = TileN<BN>::B_STAGE, NT8 = TileN<BN>::NT8;
     constexpr int STAGES = TileN<BN>::STAGES;
-    extern __shared__ __align__(16) double smem[];
     double *As = smem;
     double *Bs = smem + STAGES * A_STAGE;
-    // N tiles vary fastest: the CTAs that share an A row panel run together and reuse it from L2
-    const int i0 = blockIdx.y * BM, j0 = blockIdx.x * BN;
-    if (lower && i0 + BM - 1 < j0) return;   // tile entirely above the diagonal
-    A += (long long)blockIdx.z * sA;
-    B += (long long)blockIdx.z * sB;
-    C += (long long)blockIdx.z * sC;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int wm = warp & 3, wn = warp >> 2;          // 4 x 2 warps, 32 x BN/2 each
     const int g = lane >> 2, tig = lane & 3;
@@ -159,6 +151,33 @@ __global__ void __launch_bounds__(NT, (BN <= 64) ? 2 : 1) dgemm_kernel(int M, in
 }
 
 template <bool A_KM, bool B_KM, int BN>
+__global__ void __launch_bounds__(NT, (BN <= 64) ? 2 : 1) dgemm_kernel(int M, int N, int K, double alpha,
+                                                   const double *A, long long lda, long long sA,
+                                                   const double *B, long long ldb, long long sB,
+                                                   double beta, double *C, long long ldc, long long sC,
+                                                   int lower) {
+    extern __shared__ __align__(16) double smem[];
+    // N tiles vary fastest: the CTAs that share an A row panel run together and reuse it from L2
+    const int i0 = blockIdx.y * BM, j0 = blockIdx.x * BN;
+    if (lower && i0 + BM - 1 < j0) return;   // tile entirely above the diagonal
+    gemm_tile<A_KM, B_KM, BN>(i0, j0, M, N, K, alpha, A + (long long)blockIdx.z * sA, lda,
+                              B + (long long)blockIdx.z * sB, ldb, beta, C + (long long)blockIdx.z * sC, ldc, lower,
+                              smem);
+}
+
+// Grouped: CTA t computes tile (tiles[t].y, tiles[t].z) (row, column tile index) of group
+// tiles[t].x, each group with its own sizes and operands (A K-major, B K-major, C lower).
+__global__ void __launch_bounds__(NT, 2) dgemm_grouped_kernel(const int4 *__restrict__ tiles,
+                                                              const GemmGroup *__restrict__ groups, double alpha,
+                                                              double beta) {
+    extern __shared__ __align__(16) double smem[];
+    const int4 t = tiles[blockIdx.x];
+    const GemmGroup gr = groups[t.x];
+    gemm_tile<true, true, 64>(t.y * BM, t.z * 64, gr.M, gr.N, gr.K, alpha, gr.A, gr.lda, gr.B, gr.ldb, beta, gr.C,
+                              gr.ldc, 1, smem);
+}
+
+template <bool A_KM, bool B_KM, int BN>
 int launch(cudaStream_t st, int M, int N, int K, double alpha, const double *A, long long lda, long long sA,
            const double *B, long long ldb, long long sB, double beta, double *C, long long ldc, long long sC,
            int batch, int lower) {
@@ -220,6 +239,22 @@ __global__ void scale_kernel(int M, int N, double beta, double *C, long long ldc
     if (i < M && j < N && (!lower || i >= j)) C[i + (long long)j * ldc] *= beta;
 }
 }  // namespace
+
+int gemm_f64_grouped(cudaStream_t st, int ntiles, const int4 *d_tiles, const GemmGroup *d_groups, double alpha,
+                     double beta) {
+    if (ntiles <= 0) return BGPU_OK;
+    static bool attr_set = false;
+    if (!attr_set) {
+        BGPU_CHECK(cudaFuncSetAttribute(dgemm_grouped_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)TileN<64>::SMEM));
+        attr_set = true;
+    }
+    dgemm_grouped_kernel<<<ntiles, NT, TileN<64>::SMEM, st>>>(d_tiles, d_groups, alpha, beta);
+    BGPU_LAUNCH_CHECK();
+    return BGPU_OK;
+}
+
+int gemm_grouped_tile_rows() { return BM; }
 
 int scale_matrix_f64(cudaStream_t st, int M, int N, double beta, double *C, long long ldc, long long sC, int batch,
                      int lower) {

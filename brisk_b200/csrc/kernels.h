@@ -8,6 +8,18 @@
 int gemm_f64(cudaStream_t st, int a_kmajor, int b_kmajor, int M, int N, int K, double alpha, const double *A,
              long long lda, long long sA, const double *B, long long ldb, long long sB, double beta, double *C,
              long long ldc, long long sC, int batch, int lower);
+// Grouped lower-triangle GEMMs: C_g(i, j) = alpha sum_k A_g(i, k) B_g(k, j) + beta C_g(i, j) for
+// i >= j, A_g K-major (A(i,k) = A[i lda + k]), B_g K-major (B(k,j) = B[k + j ldb]); CTA t computes
+// the 128 x 64 tile (tiles[t].y, tiles[t].z) of group tiles[t].x.
+struct GemmGroup {
+    const double *A, *B;
+    double *C;
+    int M, N, K;
+    long long lda, ldb, ldc;
+};
+int gemm_f64_grouped(cudaStream_t st, int ntiles, const int4 *d_tiles, const GemmGroup *d_groups, double alpha,
+                     double beta);
+int gemm_grouped_tile_rows();   // 128 (the tile is 128 x 64)
 int scale_matrix_f64(cudaStream_t st, int M, int N, double beta, double *C, long long ldc, long long sC, int batch,
                      int lower);
 

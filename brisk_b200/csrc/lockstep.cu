@@ -1,0 +1,399 @@
+// Kernels of the lockstep batch (lockstep.h).  Every kernel covers all listed instances in one
+// launch, one CTA per instance (or per work item), and sums in a fixed order.
+#include "common.cuh"
+#include "lockstep.h"
+
+#include <algorithm>
+
+namespace lockstep {
+namespace {
+
+__device__ __forceinline__ long long upk(int p, int q) { return (long long)q * (q + 1) / 2 + p; }
+
+// one work item: ITEM constraints of one instance; shared: X, Z, A, W (n x n each)
+__global__ void __launch_bounds__(256) form_q_kernel(const int2 *__restrict__ items, const int *__restrict__ nv,
+                                                     const int *__restrict__ mv, const long long *__restrict__ boff,
+                                                     const long long *__restrict__ poff, const double *__restrict__ P,
+                                                     const double *__restrict__ Xc, const double *__restrict__ Zc,
+                                                     double *Q) {
+    extern __shared__ __align__(16) double fq[];
+    const int2 it = items[blockIdx.x];
+    const int k = it.x, a0 = it.y;
+    const int n = nv[k], m = mv[k], nn = n * n, t = n * (n + 1) / 2;
+    double *Xs = fq, *Zs = fq + nn, *As = fq + 2 * nn, *Ws = fq + 3 * nn;
+    const double *X = Xc + boff[k], *Z = Zc + boff[k];
+    for (int i = threadIdx.x; i < nn; i += blockDim.x) { Xs[i] = X[i]; Zs[i] = Z[i]; }
+    const double *Pk = P + poff[k];
+    double *Qk = Q + poff[k];
+    const int a1 = min(m, a0 + ITEM);
+    for (int a = a0; a < a1; a++) {
+        const double *prow = Pk + (long long)a * t;
+        __syncthreads();   // the previous constraint's A and W are no longer read
+        for (int idx = threadIdx.x; idx < nn; idx += blockDim.x) {
+            const int i = idx % n, j = idx / n;
+            As[idx] = prow[i <= j ? upk(i, j) : upk(j, i)];
+        }
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < nn; idx += blockDim.x) {   // W = A Zi
+            const int i = idx % n, j = idx / n;
+            double s = 0.0;
+            for (int q = 0; q < n; q++) s += As[q + i * n] * Zs[q + j * n];   // A symmetric: A[i, q] = A[q, i]
+            Ws[idx] = s;
+        }
+        __syncthreads();
+        double *qrow = Qk + (long long)a * t;
+        for (int idx = threadIdx.x; idx < nn; idx += blockDim.x) {   // Q = packed (G + G'), G = X W
+            const int i = idx % n, j = idx / n;
+            if (i > j) continue;
+            double s = 0.0;
+            for (int q = 0; q < n; q++) s += Xs[i + q * n] * Ws[q + j * n];
+            if (i < j)
+                for (int q = 0; q < n; q++) s += Xs[j + q * n] * Ws[q + i * n];
+            qrow[upk(i, j)] = s;
+        }
+    }
+}
+
+__global__ void mirror_kernel(const int *__restrict__ list, const int *__restrict__ mv, const long long *__restrict__ moff,
+                              double *M) {
+    const int k = list[blockIdx.x], m = mv[k];
+    double *Mk = M + moff[k];
+    for (long long idx = threadIdx.x; idx < (long long)m * m; idx += blockDim.x) {
+        const int i = (int)(idx % m), j = (int)(idx / m);
+        if (i < j) Mk[idx] = Mk[j + (long long)i * m];
+    }
+}
+
+constexpr int CB = 32;   // panel width of the batched Cholesky
+constexpr int CT = 64;   // tile of its trailing update
+
+__global__ void __launch_bounds__(256) chol_kernel(const int *__restrict__ list, const int *__restrict__ mv,
+                                                   const long long *__restrict__ moff, const long long *__restrict__ coff,
+                                                   const double *__restrict__ M, const double *__restrict__ reg,
+                                                   double *D, double *Lf, int *info, double *pmin) {
+    __shared__ double S[CB][CB + 1];
+    __shared__ double PI[CT][CB + 1], PJ[CT][CB + 1];
+    __shared__ int fail_s;
+    __shared__ double pm_s;
+    const int k = list[blockIdx.x], m = mv[k];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const double *Mk = M + moff[k];
+    double *Lk = Lf + moff[k];
+    double *Dk = D + coff[k];
+    const double r = reg[k];
+    for (int i = tid; i < m; i += 256) {
+        const double d = Mk[i + (long long)i * m];
+        Dk[i] = d > 0 ? 1.0 / sqrt(d) : 1.0;
+    }
+    if (tid == 0) { fail_s = 0; pm_s = 1e300; }
+    __syncthreads();
+    for (long long idx = tid; idx < (long long)m * m; idx += 256) {
+        const int i = (int)(idx % m), j = (int)(idx / m);
+        Lk[idx] = (i >= j) ? Dk[i] * Mk[idx] * Dk[j] + (i == j ? r : 0.0) : 0.0;
+    }
+    __syncthreads();
+    for (int k0 = 0; k0 < m; k0 += CB) {
+        const int nb = min(CB, m - k0);
+        for (int idx = tid; idx < CB * CB; idx += 256) {
+            const int i = idx % CB, j = idx / CB;
+            S[i][j] = (i < nb && j < nb && i >= j) ? Lk[(k0 + i) + (long long)(k0 + j) * m] : 0.0;
+        }
+        __syncthreads();
+        if (warp == 0) {   // the diagonal block, one warp (lane r owns row r)
+            for (int c = 0; c < nb; c++) {
+                __syncwarp();
+                const double d = S[c][c];
+                if (!(d > 0.0) || !isfinite(d)) {
+                    if (lane == 0) fail_s = k0 + c + 1;
+                    break;
+                }
+                if (lane == 0) pm_s = fmin(pm_s, d);
+                const double sd = sqrt(d);
+                __syncwarp();
+                if (lane > c && lane < nb) S[lane][c] /= sd;
+                __syncwarp();
+                if (lane == c) S[c][c] = sd;
+                if (lane > c && lane < nb)
+                    for (int q = c + 1; q <= lane; q++) S[lane][q] -= S[lane][c] * S[q][c];
+            }
+        }
+        __syncthreads();
+        if (fail_s) break;
+        for (int idx = tid; idx < CB * CB; idx += 256) {
+            const int i = idx % CB, j = idx / CB;
+            if (i < nb && j < nb && i >= j) Lk[(k0 + i) + (long long)(k0 + j) * m] = S[i][j];
+        }
+        // the panel below: L(i, k0..k0+nb) = A(i, .) L_kk^-T
+        for (int i = k0 + nb + tid; i < m; i += 256) {
+            for (int c = 0; c < nb; c++) {
+                double v = Lk[i + (long long)(k0 + c) * m];
+                for (int q = 0; q < c; q++) v -= Lk[i + (long long)(k0 + q) * m] * S[c][q];
+                Lk[i + (long long)(k0 + c) * m] = v / S[c][c];
+            }
+        }
+        __syncthreads();
+        // the trailing lower triangle: L(i, j) -= L(i, panel) L(j, panel)', i >= j >= k0 + nb
+        const int base = k0 + nb, rem = m - base, T = (rem + CT - 1) / CT;
+        for (int ti = 0; ti < T; ti++) {
+            for (int idx = tid; idx < CT * CB; idx += 256) {
+                const int ii = idx % CT, c = idx / CT;
+                const int i = base + ti * CT + ii;
+                PI[ii][c] = (i < m && c < nb) ? Lk[i + (long long)(k0 + c) * m] : 0.0;
+            }
+            for (int tj = 0; tj <= ti; tj++) {
+                for (int idx = tid; idx < CT * CB; idx += 256) {
+                    const int jj = idx % CT, c = idx / CT;
+                    const int j = base + tj * CT + jj;
+                    PJ[jj][c] = (j < m && c < nb) ? Lk[j + (long long)(k0 + c) * m] : 0.0;
+                }
+                __syncthreads();
+                for (int e = tid; e < CT * CT; e += 256) {
+                    const int ii = e % CT, jj = e / CT;
+                    const int i = base + ti * CT + ii, j = base + tj * CT + jj;
+                    if (i < m && j < m && i >= j) {
+                        double s = 0.0;
+                        for (int c = 0; c < nb; c++) s += PI[ii][c] * PJ[jj][c];
+                        Lk[i + (long long)j * m] -= s;
+                    }
+                }
+                __syncthreads();
+            }
+        }
+    }
+    if (tid == 0) {
+        info[k] = fail_s;
+        pmin[k] = fail_s ? 0.0 : pm_s;
+    }
+}
+
+__global__ void __launch_bounds__(256) prec_kernel(const int *__restrict__ list, const int *__restrict__ mv,
+                                                   const long long *__restrict__ moff, const long long *__restrict__ coff,
+                                                   const double *__restrict__ Lf, const double *__restrict__ D,
+                                                   double *x) {
+    extern __shared__ __align__(16) double xs[];
+    const int k = list[blockIdx.x], m = mv[k];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const double *Lk = Lf + moff[k];
+    const double *Dk = D + coff[k];
+    double *xk = x + coff[k];
+    for (int i = tid; i < m; i += 256) xs[i] = Dk[i] * xk[i];
+    __syncthreads();
+    for (int k0 = 0; k0 < m; k0 += 32) {   // forward: L y = x
+        const int nb = min(32, m - k0);
+        if (warp == 0) {
+            double v = lane < nb ? xs[k0 + lane] : 0.0;
+            for (int c = 0; c < nb; c++) {
+                const double xc = __shfl_sync(0xffffffffu, v, c) / Lk[(k0 + c) + (long long)(k0 + c) * m];
+                if (lane == c) v = xc;
+                else if (lane > c && lane < nb) v -= Lk[(k0 + lane) + (long long)(k0 + c) * m] * xc;
+            }
+            if (lane < nb) xs[k0 + lane] = v;
+        }
+        __syncthreads();
+        for (int i = k0 + nb + tid; i < m; i += 256) {
+            double s = 0.0;
+            for (int c = 0; c < nb; c++) s += Lk[i + (long long)(k0 + c) * m] * xs[k0 + c];
+            xs[i] -= s;
+        }
+        __syncthreads();
+    }
+    for (int k0 = ((m - 1) / 32) * 32; k0 >= 0; k0 -= 32) {   // backward: L' z = y
+        const int nb = min(32, m - k0);
+        for (int c = warp; c < nb; c += 8) {
+            double s = 0.0;
+            for (int i = k0 + nb + lane; i < m; i += 32) s += Lk[i + (long long)(k0 + c) * m] * xs[i];
+            s = warp_sum(s);
+            if (lane == 0) xs[k0 + c] -= s;
+        }
+        __syncthreads();
+        if (warp == 0) {
+            double v = lane < nb ? xs[k0 + lane] : 0.0;
+            for (int c = nb - 1; c >= 0; c--) {
+                const double xc = __shfl_sync(0xffffffffu, v, c) / Lk[(k0 + c) + (long long)(k0 + c) * m];
+                if (lane == c) v = xc;
+                else if (lane < c) v -= Lk[(k0 + c) + (long long)(k0 + lane) * m] * xc;
+            }
+            if (lane < nb) xs[k0 + lane] = v;
+        }
+        __syncthreads();
+    }
+    for (int i = tid; i < m; i += 256) xk[i] = Dk[i] * xs[i];
+}
+
+__global__ void __launch_bounds__(256) symv_kernel(const int *__restrict__ list, const int *__restrict__ mv,
+                                                   const long long *__restrict__ moff, const long long *__restrict__ coff,
+                                                   const double *__restrict__ M, const double *__restrict__ x, double *y) {
+    const int k = list[blockIdx.x], m = mv[k];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const double *Mk = M + moff[k];
+    const double *xk = x + coff[k];
+    double *yk = y + coff[k];
+    for (int i = warp; i < m; i += 8) {   // column i of the symmetric M
+        double s = 0.0;
+        for (int j = lane; j < m; j += 32) s += Mk[j + (long long)i * m] * xk[j];
+        s = warp_sum(s);
+        if (lane == 0) yk[i] = s;
+    }
+}
+
+// y[a] = <A_a, D> = sum_u P[a, u] Dp[u], Dp = packed (D + D') off the diagonal, D on it
+__global__ void __launch_bounds__(256) aop_packed_kernel(const int *__restrict__ list, const int *__restrict__ nv,
+                                                         const int *__restrict__ mv, const long long *__restrict__ boff,
+                                                         const long long *__restrict__ coff,
+                                                         const long long *__restrict__ poff, const double *__restrict__ P,
+                                                         const double *__restrict__ Dc, double *y) {
+    extern __shared__ __align__(16) double dp[];
+    const int k = list[blockIdx.x], n = nv[k], m = mv[k], t = n * (n + 1) / 2;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const double *D = Dc + boff[k];
+    for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+        const int i = idx % n, j = idx / n;
+        if (i < j) dp[upk(i, j)] = D[idx] + D[j + i * n];
+        else if (i == j) dp[upk(i, i)] = D[idx];
+    }
+    __syncthreads();
+    const double *Pk = P + poff[k];
+    double *yk = y + coff[k];
+    for (int a = warp; a < m; a += 8) {
+        const double *row = Pk + (long long)a * t;
+        double s = 0.0;
+        for (int u = lane; u < t; u += 32) s += row[u] * dp[u];
+        s = warp_sum(s);
+        if (lane == 0) yk[a] = s;
+    }
+}
+
+// F = alpha unpack(P' y) + beta F
+__global__ void __launch_bounds__(256) atop_packed_kernel(const int *__restrict__ list, const int *__restrict__ nv,
+                                                          const int *__restrict__ mv, const long long *__restrict__ boff,
+                                                          const long long *__restrict__ coff,
+                                                          const long long *__restrict__ poff,
+                                                          const double *__restrict__ P, const double *__restrict__ y,
+                                                          double alpha, double beta, double *Fc) {
+    extern __shared__ __align__(16) double fp[];
+    const int k = list[blockIdx.x], n = nv[k], m = mv[k], t = n * (n + 1) / 2;
+    const double *Pk = P + poff[k];
+    const double *yk = y + coff[k];
+    for (int u = threadIdx.x; u < t; u += blockDim.x) {
+        double s = 0.0;
+        for (int a = 0; a < m; a++) s += Pk[(long long)a * t + u] * yk[a];
+        fp[u] = s;
+    }
+    __syncthreads();
+    double *F = Fc + boff[k];
+    for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+        const int i = idx % n, j = idx / n;
+        const double v = alpha * fp[i <= j ? upk(i, j) : upk(j, i)];
+        F[idx] = beta == 0.0 ? v : v + beta * F[idx];
+    }
+}
+
+constexpr int DQ = 8;
+__global__ void __launch_bounds__(256) seg_dots_kernel(const long long *__restrict__ off, int nq,
+                                                       const double *const *__restrict__ a,
+                                                       const double *const *__restrict__ b, double *out) {
+    __shared__ double part[DQ][8];
+    const int k = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    double acc[DQ];
+#pragma unroll
+    for (int q = 0; q < DQ; q++) acc[q] = 0.0;
+    for (long long i = off[k] + tid; i < off[k + 1]; i += 256)
+#pragma unroll
+        for (int q = 0; q < DQ; q++)
+            if (q < nq) acc[q] += a[q][i] * b[q][i];
+#pragma unroll
+    for (int q = 0; q < DQ; q++) {
+        const double v = warp_sum(acc[q]);
+        if (lane == 0) part[q][warp] = v;
+    }
+    __syncthreads();
+    if (tid < nq) {
+        double s = 0.0;
+        for (int w = 0; w < 8; w++) s += part[tid][w];
+        out[(long long)k * nq + tid] = s;
+    }
+}
+}  // namespace
+
+size_t form_q_smem(int nmax) { return 4 * (size_t)nmax * nmax * sizeof(double); }
+
+int form_q(cudaStream_t st, const Layout &L, const int2 *items, int nitems, int nmax, const double *P,
+           const double *Xc, const double *Zc, double *Q) {
+    if (nitems <= 0) return BGPU_OK;
+    if (nmax <= 0 || nmax > NMAX) return BGPU_ERR_ARG;
+    static bool attr = false;
+    if (!attr) {
+        BGPU_CHECK(cudaFuncSetAttribute(form_q_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)form_q_smem(NMAX)));
+        attr = true;
+    }
+    form_q_kernel<<<nitems, 256, form_q_smem(nmax), st>>>(items, L.n, L.m, L.boff, L.poff, P, Xc, Zc, Q);
+    BGPU_LAUNCH_CHECK();
+    return BGPU_OK;
+}
+
+int mirror(cudaStream_t st, const Layout &L, const int *list, int cnt, double *M) {
+    if (cnt <= 0) return BGPU_OK;
+    mirror_kernel<<<cnt, 256, 0, st>>>(list, L.m, L.moff, M);
+    BGPU_LAUNCH_CHECK();
+    return BGPU_OK;
+}
+
+int chol(cudaStream_t st, const Layout &L, const int *list, int cnt, const double *M, const double *reg, double *D,
+         double *Lf, int *info, double *pmin) {
+    if (cnt <= 0) return BGPU_OK;
+    chol_kernel<<<cnt, 256, 0, st>>>(list, L.m, L.moff, L.coff, M, reg, D, Lf, info, pmin);
+    BGPU_LAUNCH_CHECK();
+    return BGPU_OK;
+}
+
+int prec(cudaStream_t st, const Layout &L, const int *list, int cnt, int mmax, const double *Lf, const double *D,
+         double *x) {
+    if (cnt <= 0) return BGPU_OK;
+    const size_t smem = (size_t)std::max(mmax, 1) * sizeof(double);
+    if (smem > 200 * 1024) return BGPU_ERR_TOOBIG;
+    static bool attr = false;
+    if (!attr) {
+        BGPU_CHECK(cudaFuncSetAttribute(prec_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        attr = true;
+    }
+    prec_kernel<<<cnt, 256, smem, st>>>(list, L.m, L.moff, L.coff, Lf, D, x);
+    BGPU_LAUNCH_CHECK();
+    return BGPU_OK;
+}
+
+int symv(cudaStream_t st, const Layout &L, const int *list, int cnt, const double *M, const double *x, double *y) {
+    if (cnt <= 0) return BGPU_OK;
+    symv_kernel<<<cnt, 256, 0, st>>>(list, L.m, L.moff, L.coff, M, x, y);
+    BGPU_LAUNCH_CHECK();
+    return BGPU_OK;
+}
+
+int aop_packed(cudaStream_t st, const Layout &L, const int *list, int cnt, int nmax, const double *P,
+               const double *Dc, double *y) {
+    if (cnt <= 0) return BGPU_OK;
+    aop_packed_kernel<<<cnt, 256, (size_t)nmax * (nmax + 1) / 2 * sizeof(double), st>>>(list, L.n, L.m, L.boff, L.coff,
+                                                                                       L.poff, P, Dc, y);
+    BGPU_LAUNCH_CHECK();
+    return BGPU_OK;
+}
+
+int atop_packed(cudaStream_t st, const Layout &L, const int *list, int cnt, int nmax, const double *P, const double *y,
+                double alpha, double beta, double *Fc) {
+    if (cnt <= 0) return BGPU_OK;
+    atop_packed_kernel<<<cnt, 256, (size_t)nmax * (nmax + 1) / 2 * sizeof(double), st>>>(list, L.n, L.m, L.boff, L.coff,
+                                                                                        L.poff, P, y, alpha, beta, Fc);
+    BGPU_LAUNCH_CHECK();
+    return BGPU_OK;
+}
+
+int seg_dots(cudaStream_t st, int B, const long long *off, int nq, const double *const *a, const double *const *b,
+             double *out) {
+    if (B <= 0) return BGPU_OK;
+    if (nq <= 0 || nq > DQ) return BGPU_ERR_ARG;
+    seg_dots_kernel<<<B, 256, 0, st>>>(off, nq, a, b, out);
+    BGPU_LAUNCH_CHECK();
+    return BGPU_OK;
+}
+
+}  // namespace lockstep

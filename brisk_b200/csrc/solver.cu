@@ -23,6 +23,7 @@
 #include "small.h"
 #include "solver.h"
 #include "sparse.h"
+#include "lockstep.h"
 #include "tf32x3.h"
 
 #include <algorithm>
@@ -1880,6 +1881,8 @@ int Solver::run(ResultData &res) {
     return res.exit_code;
 }
 
+#include "lockstep_solver.cuh"
+
 }  // namespace
 
 static int solve_impl(const InputData &in, const Options &opt, ResultData &res, Arena *arena) {
@@ -1943,12 +1946,69 @@ int solve_problem_arena(const InputData &in, const Options &opt, ResultData &res
     return rc;
 }
 
+// The lockstep form of the batch when every problem has one SDP block of order <= 64: builds the
+// problems on the host threads and solves them together (Lockstep).  Returns false (nothing
+// solved, nothing reported) when a problem does not have that shape.
+static bool lockstep_batch(int count, const std::function<bool(int, InputData &)> &get,
+                           const std::function<void(int, ResultData &, int)> &put, const Options &opt) {
+    std::vector<HProblem> Ps(count);
+    std::vector<int> rc(count, 0);
+    std::vector<char> shape_ok(count, 1);
+    parallel_for(count, [&](long long pp) {
+        const int p = (int)pp;
+        tl_serial = true;
+        InputData in;
+        std::string err;
+        if (!get(p, in)) { rc[p] = 2; return; }
+        if (in.nblk != 1 || in.bs.empty() || in.bs[0] < 1 || in.bs[0] > lockstep::NMAX || in.m < 1) {
+            shape_ok[p] = 0;
+            return;
+        }
+        if (build_problem(in, Ps[p], err)) rc[p] = 2;
+    });
+    for (int p = 0; p < count; p++)
+        if (!shape_ok[p]) return false;
+    std::vector<int> idx;
+    std::vector<HProblem> good;
+    for (int p = 0; p < count; p++)
+        if (rc[p] == 0) { idx.push_back(p); good.push_back(std::move(Ps[p])); }
+    Ps.clear();
+    std::vector<ResultData> res;
+    int code = 0;
+    if (!good.empty()) {
+        Options o = opt;
+        o.verbose = 0;
+        try {
+            Lockstep L(good, o);
+            L.setup();
+            L.run(res);
+        } catch (const GpuFail &f) {
+            log_printf(1, "brisk: GPU failure in the lockstep batch (code %d at line %d)\n", f.rc, f.line);
+            code = -3;
+        }
+    }
+    for (size_t q = 0; q < idx.size(); q++) {
+        ResultData r = code ? ResultData() : std::move(res[q]);
+        if (code) r.status = 4;
+        r.exit_code = code ? code : r.exit_code;
+        put(idx[q], r, code ? code : r.exit_code);
+    }
+    for (int p = 0; p < count; p++)
+        if (rc[p]) {
+            ResultData r;
+            r.exit_code = rc[p];
+            put(p, r, rc[p]);
+        }
+    return true;
+}
+
 int solve_batch(int count, const std::vector<double> &work, const std::function<bool(int, InputData &)> &get,
                 const std::function<void(int, ResultData &, int)> &put, const Options &opt, int workers,
                 std::string &err) {
     if (count <= 0) return 0;
     if (workers <= 0) workers = (int)std::max(2u, std::thread::hardware_concurrency());
     workers = std::min(workers, count);
+    if (opt.batch_mode != 0 && lockstep_batch(count, get, put, opt)) return 0;
     std::vector<int> order(count);
     std::iota(order.begin(), order.end(), 0);
     if ((int)work.size() == count)

@@ -42,6 +42,8 @@ struct Options {
     int sparse = -1;            // Schur factor: -1 auto (the reference's caps, solver.c:4014-4100), 0 dense,
                                 // 1 supernodal sparse
     int init = 1;               // 0: SDPT3 start (start_sdpt3); 1: least-squares start (solver.c:13939-14198)
+    int batch_mode = -1;        // bgpu_batch_solve: -1/1 lockstep when every problem has one block of order
+                                // <= 64 (else concurrent), 0 concurrent per-problem solves
     int route = -1;             // Schur route per block: -1 auto (dense when the constraints average >= 2 % of
                                 // n^2 entries, problem.c:1299), 0 row-product, 1 dense
 };

@@ -1,7 +1,9 @@
 """The batch entry point (bgpu_batch_solve) on a B200: instances of the uneven 4096-instance
 batch (n ~ U{8..64}, m ~ U{n..n(n+1)/4}, dense N(0,1) A_i, b = A(I), C = G G'/n + I) solved
 in one call, each checked against the reference's own solve of that instance and against its
-own stand-alone solve through brisk_solve_data."""
+own stand-alone solve through brisk_solve_data.  The default (lockstep) form advances every
+instance together with batched kernels; the concurrent form runs the stand-alone solver per
+instance on worker streams and gives its bits."""
 import numpy as np
 import pytest
 
@@ -23,21 +25,48 @@ def check(res, ref):
     assert np.max(np.abs(res.dimacs)) <= 1e-7, res.dimacs
 
 
-def test_batch_matches_reference(golden):
+@pytest.mark.parametrize("mode", ["lockstep", "concurrent"])
+def test_batch_matches_reference(golden, mode):
     """Thirteen instances (the first twelve and the largest, n = 64, m = 1038) in one call."""
     insts = [problems.batch_instance(q) for q in GOLDEN_Q]
-    out = brisk_b200.solve_batch(insts, options=FP64, workers=6)
+    out = brisk_b200.solve_batch(insts, options=FP64 + ["-batchmode", mode], workers=6)
     assert len(out) == len(insts)
     for q, res in zip(GOLDEN_Q, out):
         assert res.exit_code == 0, (q, res.exit_code)
         check(res, golden[f"batch_q{q}"]["runs"]["default"])
 
 
+def test_lockstep_batch_matches_standalone_solves():
+    """96 instances in lockstep: each has its stand-alone solve's status, DIMACS errors <= 1e-7
+    and objectives within 1e-7 of it (relative to 1 + |<C,X>| + |b'y|)."""
+    insts = [problems.batch_instance(q) for q in range(100, 196)]
+    out = brisk_b200.solve_batch(insts, options=FP64)
+    for d, res in zip(insts, out):
+        ref = brisk_b200.solve_sdpa(*d.args(), options=FP64, verbose=False)
+        assert res.status == ref.status and res.exit_code == 0
+        den = 1 + abs(ref.pobj) + abs(ref.dobj)
+        assert abs(res.pobj - ref.pobj) <= 1e-7 * den and abs(res.dobj - ref.dobj) <= 1e-7 * den
+        assert np.max(np.abs(res.dimacs)) <= 1e-7
+        assert abs(res.iterations - ref.iterations) <= 2
+
+
+def test_lockstep_bad_instance_does_not_stop_the_others():
+    """An entry outside its block gives that problem exit code 2; the lockstep batch solves the rest."""
+    good = [problems.batch_instance(q) for q in (5, 6, 7)]
+    arrs = brisk_b200.concat_problems(good)
+    arrs["i"] = arrs["i"].copy()
+    first1 = int(arrs["nnz"][0])
+    arrs["i"][first1 + 3] = 99                 # instance 1: row 99 of a 12 x 12 block
+    out = brisk_b200.solve_batch_arrays(**arrs, options=FP64)
+    assert out[1].exit_code == 2
+    assert out[0].status_str == "OPTIMAL" and out[2].status_str == "OPTIMAL"
+
+
 def test_batch_equals_standalone_solves():
     """Each instance's result in a concurrent batch is bit for bit its stand-alone solve's:
     the workers run the same kernels in the same order on their own streams."""
     insts = [problems.batch_instance(q) for q in range(12, 44)]
-    out = brisk_b200.solve_batch(insts, options=FP64, workers=8)
+    out = brisk_b200.solve_batch(insts, options=FP64 + ["-batchmode", "concurrent"], workers=8)
     for d, res in zip(insts, out):
         ref = brisk_b200.solve_sdpa(*d.args(), options=FP64, verbose=False)
         assert res.exit_code == ref.exit_code and res.status == ref.status
