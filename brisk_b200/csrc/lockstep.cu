@@ -9,6 +9,14 @@ namespace lockstep {
 namespace {
 
 __device__ __forceinline__ long long upk(int p, int q) { return (long long)q * (q + 1) / 2 + p; }
+// the (p, q), p <= q, of packed index u
+__device__ __forceinline__ void unpk(int u, int &p, int &q) {
+    int c = (int)((sqrt(8.0 * (double)u + 1.0) - 1.0) * 0.5);
+    while (c * (c + 1) / 2 > u) c--;
+    while ((c + 1) * (c + 2) / 2 <= u) c++;
+    q = c;
+    p = u - c * (c + 1) / 2;
+}
 
 // one work item: ITEM constraints of one instance; shared: X, Z, A, W (n x n each)
 __global__ void __launch_bounds__(256) form_q_kernel(const int2 *__restrict__ items, const int *__restrict__ nv,
@@ -37,19 +45,22 @@ __global__ void __launch_bounds__(256) form_q_kernel(const int2 *__restrict__ it
         for (int idx = threadIdx.x; idx < nn; idx += blockDim.x) {   // W = A Zi
             const int i = idx % n, j = idx / n;
             double s = 0.0;
-            for (int q = 0; q < n; q++) s += As[q + i * n] * Zs[q + j * n];   // A symmetric: A[i, q] = A[q, i]
+            for (int q = 0; q < n; q++) s += As[i + q * n] * Zs[q + j * n];   // consecutive i: no bank conflicts
             Ws[idx] = s;
         }
         __syncthreads();
-        double *qrow = Qk + (long long)a * t;
-        for (int idx = threadIdx.x; idx < nn; idx += blockDim.x) {   // Q = packed (G + G'), G = X W
+        for (int idx = threadIdx.x; idx < nn; idx += blockDim.x) {   // G = X W, into A's buffer
             const int i = idx % n, j = idx / n;
-            if (i > j) continue;
             double s = 0.0;
             for (int q = 0; q < n; q++) s += Xs[i + q * n] * Ws[q + j * n];
-            if (i < j)
-                for (int q = 0; q < n; q++) s += Xs[j + q * n] * Ws[q + i * n];
-            qrow[upk(i, j)] = s;
+            As[idx] = s;
+        }
+        __syncthreads();
+        double *qrow = Qk + (long long)a * t;
+        for (int u = threadIdx.x; u < t; u += blockDim.x) {   // Q = packed (G + G')
+            int j, i;
+            unpk(u, i, j);
+            qrow[u] = (i < j) ? As[i + j * n] + As[j + i * n] : As[i + i * n];
         }
     }
 }
@@ -220,15 +231,17 @@ __global__ void __launch_bounds__(256) prec_kernel(const int *__restrict__ list,
     for (int i = tid; i < m; i += 256) xk[i] = Dk[i] * xs[i];
 }
 
-__global__ void __launch_bounds__(256) symv_kernel(const int *__restrict__ list, const int *__restrict__ mv,
+__global__ void __launch_bounds__(256) symv_kernel(const int2 *__restrict__ items, const int *__restrict__ mv,
                                                    const long long *__restrict__ moff, const long long *__restrict__ coff,
                                                    const double *__restrict__ M, const double *__restrict__ x, double *y) {
-    const int k = list[blockIdx.x], m = mv[k];
+    const int2 it = items[blockIdx.x];
+    const int k = it.x, m = mv[k];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const double *Mk = M + moff[k];
     const double *xk = x + coff[k];
     double *yk = y + coff[k];
-    for (int i = warp; i < m; i += 8) {   // column i of the symmetric M
+    const int i1 = min(m, it.y + RI);
+    for (int i = it.y + warp; i < i1; i += 8) {   // column i of the symmetric M
         double s = 0.0;
         for (int j = lane; j < m; j += 32) s += Mk[j + (long long)i * m] * xk[j];
         s = warp_sum(s);
@@ -236,25 +249,28 @@ __global__ void __launch_bounds__(256) symv_kernel(const int *__restrict__ list,
     }
 }
 
-// y[a] = <A_a, D> = sum_u P[a, u] Dp[u], Dp = packed (D + D') off the diagonal, D on it
-__global__ void __launch_bounds__(256) aop_packed_kernel(const int *__restrict__ list, const int *__restrict__ nv,
+// y[a] = <A_a, D> = sum_u P[a, u] Dp[u], Dp = packed (D + D') off the diagonal, D on it; a work
+// item is (instance, first row) with RI rows
+__global__ void __launch_bounds__(256) aop_packed_kernel(const int2 *__restrict__ items, const int *__restrict__ nv,
                                                          const int *__restrict__ mv, const long long *__restrict__ boff,
                                                          const long long *__restrict__ coff,
                                                          const long long *__restrict__ poff, const double *__restrict__ P,
                                                          const double *__restrict__ Dc, double *y) {
     extern __shared__ __align__(16) double dp[];
-    const int k = list[blockIdx.x], n = nv[k], m = mv[k], t = n * (n + 1) / 2;
+    const int2 it = items[blockIdx.x];
+    const int k = it.x, r0 = it.y, n = nv[k], m = mv[k], t = n * (n + 1) / 2;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const double *D = Dc + boff[k];
-    for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
-        const int i = idx % n, j = idx / n;
-        if (i < j) dp[upk(i, j)] = D[idx] + D[j + i * n];
-        else if (i == j) dp[upk(i, i)] = D[idx];
+    for (int u = threadIdx.x; u < t; u += blockDim.x) {
+        int i, j;
+        unpk(u, i, j);
+        dp[u] = (i < j) ? D[i + j * n] + D[j + i * n] : D[i + i * n];
     }
     __syncthreads();
     const double *Pk = P + poff[k];
     double *yk = y + coff[k];
-    for (int a = warp; a < m; a += 8) {
+    const int r1 = min(m, r0 + RI);
+    for (int a = r0 + warp; a < r1; a += 8) {
         const double *row = Pk + (long long)a * t;
         double s = 0.0;
         for (int u = lane; u < t; u += 32) s += row[u] * dp[u];
@@ -263,29 +279,27 @@ __global__ void __launch_bounds__(256) aop_packed_kernel(const int *__restrict__
     }
 }
 
-// F = alpha unpack(P' y) + beta F
-__global__ void __launch_bounds__(256) atop_packed_kernel(const int *__restrict__ list, const int *__restrict__ nv,
+// F = alpha unpack(P' y) + beta F; a work item is (instance, first packed index) with 256 of them
+__global__ void __launch_bounds__(256) atop_packed_kernel(const int2 *__restrict__ items, const int *__restrict__ nv,
                                                           const int *__restrict__ mv, const long long *__restrict__ boff,
                                                           const long long *__restrict__ coff,
                                                           const long long *__restrict__ poff,
                                                           const double *__restrict__ P, const double *__restrict__ y,
                                                           double alpha, double beta, double *Fc) {
-    extern __shared__ __align__(16) double fp[];
-    const int k = list[blockIdx.x], n = nv[k], m = mv[k], t = n * (n + 1) / 2;
+    const int2 it = items[blockIdx.x];
+    const int k = it.x, n = nv[k], m = mv[k], t = n * (n + 1) / 2;
+    const int u = it.y + threadIdx.x;
+    if (u >= t) return;
     const double *Pk = P + poff[k];
     const double *yk = y + coff[k];
-    for (int u = threadIdx.x; u < t; u += blockDim.x) {
-        double s = 0.0;
-        for (int a = 0; a < m; a++) s += Pk[(long long)a * t + u] * yk[a];
-        fp[u] = s;
-    }
-    __syncthreads();
+    double s = 0.0;
+    for (int a = 0; a < m; a++) s += Pk[(long long)a * t + u] * yk[a];
+    int i, j;
+    unpk(u, i, j);
     double *F = Fc + boff[k];
-    for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
-        const int i = idx % n, j = idx / n;
-        const double v = alpha * fp[i <= j ? upk(i, j) : upk(j, i)];
-        F[idx] = beta == 0.0 ? v : v + beta * F[idx];
-    }
+    const double v = alpha * s;
+    F[i + j * n] = beta == 0.0 ? v : v + beta * F[i + j * n];
+    if (i != j) F[j + i * n] = beta == 0.0 ? v : v + beta * F[j + i * n];
 }
 
 constexpr int DQ = 8;
@@ -362,27 +376,26 @@ int prec(cudaStream_t st, const Layout &L, const int *list, int cnt, int mmax, c
     return BGPU_OK;
 }
 
-int symv(cudaStream_t st, const Layout &L, const int *list, int cnt, const double *M, const double *x, double *y) {
+int symv(cudaStream_t st, const Layout &L, const int2 *items, int cnt, const double *M, const double *x, double *y) {
     if (cnt <= 0) return BGPU_OK;
-    symv_kernel<<<cnt, 256, 0, st>>>(list, L.m, L.moff, L.coff, M, x, y);
+    symv_kernel<<<cnt, 256, 0, st>>>(items, L.m, L.moff, L.coff, M, x, y);
     BGPU_LAUNCH_CHECK();
     return BGPU_OK;
 }
 
-int aop_packed(cudaStream_t st, const Layout &L, const int *list, int cnt, int nmax, const double *P,
+int aop_packed(cudaStream_t st, const Layout &L, const int2 *items, int cnt, int nmax, const double *P,
                const double *Dc, double *y) {
     if (cnt <= 0) return BGPU_OK;
-    aop_packed_kernel<<<cnt, 256, (size_t)nmax * (nmax + 1) / 2 * sizeof(double), st>>>(list, L.n, L.m, L.boff, L.coff,
+    aop_packed_kernel<<<cnt, 256, (size_t)nmax * (nmax + 1) / 2 * sizeof(double), st>>>(items, L.n, L.m, L.boff, L.coff,
                                                                                        L.poff, P, Dc, y);
     BGPU_LAUNCH_CHECK();
     return BGPU_OK;
 }
 
-int atop_packed(cudaStream_t st, const Layout &L, const int *list, int cnt, int nmax, const double *P, const double *y,
+int atop_packed(cudaStream_t st, const Layout &L, const int2 *items, int cnt, const double *P, const double *y,
                 double alpha, double beta, double *Fc) {
     if (cnt <= 0) return BGPU_OK;
-    atop_packed_kernel<<<cnt, 256, (size_t)nmax * (nmax + 1) / 2 * sizeof(double), st>>>(list, L.n, L.m, L.boff, L.coff,
-                                                                                        L.poff, P, y, alpha, beta, Fc);
+    atop_packed_kernel<<<cnt, 256, 0, st>>>(items, L.n, L.m, L.boff, L.coff, L.poff, P, y, alpha, beta, Fc);
     BGPU_LAUNCH_CHECK();
     return BGPU_OK;
 }

@@ -35,13 +35,17 @@ int chol(cudaStream_t st, const Layout &L, const int *list, int cnt, const doubl
 // x := D Lf^-T Lf^-1 D x for the listed instances (x concatenated by coff; mmax: the largest m).
 int prec(cudaStream_t st, const Layout &L, const int *list, int cnt, int mmax, const double *Lf, const double *D,
          double *x);
-// y = M x for the listed instances (M full, both triangles).
-int symv(cudaStream_t st, const Layout &L, const int *list, int cnt, const double *M, const double *x, double *y);
+// Work items (instance, first row / column / packed index) split the larger instances over
+// several CTAs: RI rows or columns per item for aop_packed and symv, 256 packed entries for
+// atop_packed.
+constexpr int RI = 64;
+// y = M x for the listed items (M full, both triangles).
+int symv(cudaStream_t st, const Layout &L, const int2 *items, int cnt, const double *M, const double *x, double *y);
 // y[coff + a] = <A_a, D_k> from the packed rows (D: the n x n concatenation), and
-// F_k = alpha sum_a y_a A_a + beta F_k, for the listed instances (nmax: the largest n listed).
-int aop_packed(cudaStream_t st, const Layout &L, const int *list, int cnt, int nmax, const double *P,
+// F_k = alpha sum_a y_a A_a + beta F_k, for the work items (nmax: the largest n).
+int aop_packed(cudaStream_t st, const Layout &L, const int2 *items, int cnt, int nmax, const double *P,
                const double *Dc, double *y);
-int atop_packed(cudaStream_t st, const Layout &L, const int *list, int cnt, int nmax, const double *P, const double *y,
+int atop_packed(cudaStream_t st, const Layout &L, const int2 *items, int cnt, const double *P, const double *y,
                 double alpha, double beta, double *Fc);
 // out[k nq + q] = <a_q, b_q> over instance k's segment [off[k], off[k+1]) for all k < B (a and b
 // device pointer tables of nq entries; fixed summation order).

@@ -45,6 +45,8 @@ class Lockstep {
     std::vector<std::pair<double *DevArrays::*, double **>> stab;
     std::vector<int> all;
     int *d_all = nullptr;   // 0 .. B-1
+    int2 *d_aitems = nullptr, *d_titems = nullptr, *d_sitems = nullptr;   // A(.), A'(.), symv work items
+    int n_aitems = 0, n_titems = 0;
     // per-instance factor state (schur_factor_)
     std::vector<double> reg, reg_ok, min_pivot;
     std::vector<char> reg_hint;
@@ -137,6 +139,22 @@ void Lockstep::setup() {
     for (int k = 0; k < B; k++) max_items += (m[k] + lockstep::ITEM - 1) / lockstep::ITEM;
     const int TR = gemm_grouped_tile_rows();
     for (int k = 0; k < B; k++) max_tiles += (long long)ceil_div(m[k], TR) * ceil_div(m[k], 64);
+    {   // the work items of A(.) (RI rows) and A'(.) (256 packed entries) over all instances
+        std::vector<int2> ai, ti;
+        for (int k = 0; k < B; k++) {
+            for (int r0 = 0; r0 < m[k]; r0 += lockstep::RI) ai.push_back(make_int2(k, r0));
+            for (int u0 = 0; u0 < t[k]; u0 += 256) ti.push_back(make_int2(k, u0));
+        }
+        n_aitems = (int)ai.size();
+        n_titems = (int)ti.size();
+        d_aitems = g.alloc<int2>(ai.size());
+        d_titems = g.alloc<int2>(ti.size());
+        d_sitems = g.alloc<int2>(ai.size());
+        need(d_aitems); need(d_titems); need(d_sitems);
+        CU(cudaMemcpyAsync(d_aitems, ai.data(), sizeof(int2) * ai.size(), cudaMemcpyHostToDevice, g.st));
+        CU(cudaMemcpyAsync(d_titems, ti.data(), sizeof(int2) * ti.size(), cudaMemcpyHostToDevice, g.st));
+        CU(cudaStreamSynchronize(g.st));
+    }
     d_items = g.alloc<int2>(max_items);
     d_tiles = g.alloc<int4>(max_tiles);
     d_groups = g.alloc<GemmGroup>(B);
@@ -243,7 +261,7 @@ void Lockstep::mul(double *DevArrays::*A, double *DevArrays::*Bm, double *DevArr
 }
 
 void Lockstep::aop(const double *D, std::vector<double> &out) {
-    RC(lockstep::aop_packed(g.st, Ld, d_all, B, nmax, Pp, D, dv_a));
+    RC(lockstep::aop_packed(g.st, Ld, d_aitems, n_aitems, nmax, Pp, D, dv_a));
     CU(cudaMemcpyAsync(h_a, dv_a, sizeof(double) * mT, cudaMemcpyDeviceToHost, g.st));
     CU(cudaStreamSynchronize(g.st));
     out.assign(h_a, h_a + mT);
@@ -252,7 +270,7 @@ void Lockstep::aop(const double *D, std::vector<double> &out) {
 void Lockstep::atop(const std::vector<double> &y, double alpha, double beta, double *F) {
     std::copy(y.begin(), y.end(), h_a);
     CU(cudaMemcpyAsync(dv_a, h_a, sizeof(double) * mT, cudaMemcpyHostToDevice, g.st));
-    RC(lockstep::atop_packed(g.st, Ld, d_all, B, nmax, Pp, dv_a, alpha, beta, F));
+    RC(lockstep::atop_packed(g.st, Ld, d_titems, n_titems, Pp, dv_a, alpha, beta, F));
     CU(cudaStreamSynchronize(g.st));   // h_a is reused by the next call
 }
 
@@ -343,8 +361,11 @@ void Lockstep::prec(const std::vector<int> &L, std::vector<double> &v) {
 void Lockstep::symv(const std::vector<int> &L, const std::vector<double> &x, std::vector<double> &y) {
     std::copy(x.begin(), x.end(), h_b);
     CU(cudaMemcpyAsync(dv_b, h_b, sizeof(double) * mT, cudaMemcpyHostToDevice, g.st));
-    upload_list(L);
-    RC(lockstep::symv(g.st, Ld, d_list, (int)L.size(), Mm, dv_b, dv_a));
+    std::vector<int2> si;
+    for (int k : L)
+        for (int c0 = 0; c0 < m[k]; c0 += lockstep::RI) si.push_back(make_int2(k, c0));
+    CU(cudaMemcpyAsync(d_sitems, si.data(), sizeof(int2) * si.size(), cudaMemcpyHostToDevice, g.st));
+    RC(lockstep::symv(g.st, Ld, d_sitems, (int)si.size(), Mm, dv_b, dv_a));
     CU(cudaMemcpyAsync(h_a, dv_a, sizeof(double) * mT, cudaMemcpyDeviceToHost, g.st));
     CU(cudaStreamSynchronize(g.st));
     y.resize(mT);
