@@ -280,6 +280,11 @@ static bool make_input(int m, int nblk, const int *bs, const double *c, int64_t 
     in.nblk = nblk;
     in.bs.assign(bs, bs + nblk);
     in.c.assign(c, c + m);
+    in.mat.reserve(nnz);
+    in.blk.reserve(nnz);
+    in.i.reserve(nnz);
+    in.j.reserve(nnz);
+    in.v.reserve(nnz);
     for (int64_t q = 0; q < nnz; q++) {
         if (v[q] == 0) continue;
         in.mat.push_back(mat[q]);

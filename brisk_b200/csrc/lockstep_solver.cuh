@@ -53,6 +53,12 @@ class Lockstep {
     std::vector<int> pcg_iters, nfactor;
     double schur_flops = 0;
 
+  public:
+    // wall time of the phases (s): start, assembly, factor, PCG, the rest of the loop, final measures
+    double t_start = 0, t_asm = 0, t_fac = 0, t_pcg = 0, t_loop = 0, t_final = 0;
+
+  private:
+
     double **tab(double *DevArrays::*mem);
     void upload_list(const std::vector<int> &L);
     void set_coef(int i, const std::vector<double> &v);
@@ -196,28 +202,17 @@ void Lockstep::setup() {
         CU(cudaMemcpyAsync(d_groups, gr.data(), sizeof(GemmGroup) * B, cudaMemcpyHostToDevice, g.st));
         CU(cudaStreamSynchronize(g.st));
     }
-    // P (packed constraints) and C, per instance, built on the host in parallel and uploaded
-    CU(cudaMemsetAsync(Pp, 0, sizeof(double) * PT, g.st));
+    // P (the packed constraints, built with the problems) and C, uploaded
     std::vector<double> Ch(Ntot2, 0.0);
     {
-        std::vector<std::vector<double>> Ph(B);
-        parallel_for(B, [&](long long kk) {
-            const int k = (int)kk;
+        for (int k = 0; k < B; k++) {
             const HBlock &Bl = Pb[k].blk[0];
-            const int nk = n[k], tk = t[k];
-            auto &row = Ph[k];
-            row.assign((size_t)m[k] * tk, 0.0);
-            for (size_t a = 0; a < Bl.con.size(); a++)
-                for (long long e = Bl.cptr[a]; e < Bl.cptr[a + 1]; e++) {
-                    const int pos = Bl.cpos[e], q = pos / nk, p = pos - q * nk;
-                    if (p <= q) row[(size_t)Bl.con[a] * tk + (size_t)q * (q + 1) / 2 + p] = Bl.cval[e];
-                }
             for (size_t e = 0; e < Bl.Cpos.size(); e++) Ch[boff[k] + Bl.Cpos[e]] += Bl.Cval[e];
-        });
-        for (int k = 0; k < B; k++)
-            if (!Ph[k].empty())
-                CU(cudaMemcpyAsync(Pp + poff[k], Ph[k].data(), sizeof(double) * Ph[k].size(), cudaMemcpyHostToDevice,
-                                   g.st));
+            if ((long long)Pb[k].packed.size() != (long long)m[k] * t[k]) throw GpuFail{BGPU_ERR_ARG, __LINE__};
+            if (!Pb[k].packed.empty())
+                CU(cudaMemcpyAsync(Pp + poff[k], Pb[k].packed.data(), sizeof(double) * Pb[k].packed.size(),
+                                   cudaMemcpyHostToDevice, g.st));
+        }
         CU(cudaMemcpyAsync(Ccat, Ch.data(), sizeof(double) * Ntot2, cudaMemcpyHostToDevice, g.st));
         std::vector<double> ones(B, 1.0);
         CU(cudaMemcpyAsync(d_coef[0], ones.data(), sizeof(double) * B, cudaMemcpyHostToDevice, g.st));
@@ -285,6 +280,7 @@ void Lockstep::segdots(int nq, const double *const *a, const double *const *b, s
 
 void Lockstep::assemble(const std::vector<int> &L, const double *X, const double *Zi) {
     if (L.empty()) return;
+    const double t0 = wtime();
     std::vector<int2> items;
     std::vector<int4> tiles;
     const int TR = gemm_grouped_tile_rows();
@@ -304,10 +300,12 @@ void Lockstep::assemble(const std::vector<int> &L, const double *X, const double
     upload_list(L);
     RC(lockstep::mirror(g.st, Ld, d_list, (int)L.size(), Mm));
     CU(cudaStreamSynchronize(g.st));
+    t_asm += wtime() - t0;
 }
 
 // schur_factor_ (solver.c:5296-5421), FP64, per instance: the regularization ladder of Solver::factor
 void Lockstep::factor(const std::vector<int> &L, std::vector<int> &failed) {
+    const double t0 = wtime();
     const double ulp = 2.220446049250313e-16;
     std::vector<int> todo = L;
     std::vector<double> r(B, 0.0);
@@ -346,6 +344,7 @@ void Lockstep::factor(const std::vector<int> &L, std::vector<int> &failed) {
         todo.swap(again);
     }
     failed = todo;
+    t_fac += wtime() - t0;
 }
 
 void Lockstep::prec(const std::vector<int> &L, std::vector<double> &v) {
@@ -374,6 +373,11 @@ void Lockstep::symv(const std::vector<int> &L, const std::vector<double> &x, std
 
 // schur_solve_ (solver.c:5483-5621) per instance: PCG on M x = rhs with the exact FP64 factor
 void Lockstep::pcg(const std::vector<int> &L, const std::vector<double> &rhs, std::vector<double> &x, double tol_rel) {
+    const double t0 = wtime();
+    struct Acc {
+        double &t, t0;
+        ~Acc() { t += wtime() - t0; }
+    } acc{t_pcg, t0};
     x.assign(mT, 0.0);
     std::vector<int> run;
     std::vector<double> nb(B, 0.0), tol(B, 0.0), best(B, 0.0), rz(B, 0.0), nr(B, 0.0);
@@ -663,20 +667,7 @@ void Lockstep::run(std::vector<ResultData> &res) {
     {
         std::vector<std::vector<double>> sv(6, std::vector<double>(B, 0.0));
         for (int k = 0; k < B; k++) {
-            const HBlock &Bl = Pb[k].blk[0];
-            const int nk = Bl.n;
-            double nC = 0, maxA = 0, ratio = 0;
-            for (double v : Bl.Cval) nC += v * v;
-            nC = std::sqrt(nC);
-            for (size_t a = 0; a < Bl.con.size(); a++) {
-                double s = 0;
-                for (long long e = Bl.cptr[a]; e < Bl.cptr[a + 1]; e++) s += Bl.cval[e] * Bl.cval[e];
-                s = std::sqrt(s);
-                maxA = std::max(maxA, s);
-                ratio = std::max(ratio, (1 + std::fabs(Pb[k].b[Bl.con[a]])) / (1 + s));
-            }
-            const double xi = std::max(10.0, std::max(std::sqrt((double)nk), nk * ratio));
-            const double eta = std::max(10.0, std::max(std::sqrt((double)nk), std::max(maxA, nC)));
+            const double xi = Pb[k].xi0, eta = Pb[k].eta0;
             sv[0][k] = xi;
             sv[1][k] = eta;
             sv[2][k] = std::sqrt(xi);
@@ -694,6 +685,8 @@ void Lockstep::run(std::vector<ResultData> &res) {
     }
     std::vector<char> started;
     if (opt.init >= 1) least_squares_start(y, started);
+    t_start = wtime() - t0;
+    const double t_a0 = t_asm, t_f0 = t_fac, t_p0 = t_pcg;
     // R0 = C - Z - A'y, theta = 1
     std::vector<double> theta(B, 1.0), r0norm(B, 0.0);
     atop(y, -1.0, 0.0, cat.R0);
@@ -1010,7 +1003,10 @@ void Lockstep::run(std::vector<ResultData> &res) {
         RC(ew_copy_masked(g.st, B, d_boff, Ntot2, d_flag, cat.Zb, cat.Z));
         CU(cudaStreamSynchronize(g.st));
     }
+    const double tl = wtime();
+    t_loop = tl - t0 - t_start - (t_asm - t_a0) - (t_fac - t_f0) - (t_pcg - t_p0);
     final_measures(y, res);
+    t_final = wtime() - tl;
     const double tt = wtime() - t0;
     for (int k = 0; k < B; k++) {
         ResultData &r = res[k];

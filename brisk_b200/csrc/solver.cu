@@ -87,7 +87,28 @@ struct HProblem {
     std::vector<double> d, du;
     double bs = 1, cs = 1, normb1 = 0, normb2 = 0, normC1 = 0, normC2 = 0;
     long long Ntot = 0;
+    // the lockstep batch keeps, instead of its one block's entry lists: the constraints as packed
+    // upper rows (m x n(n+1)/2) and the start's scalings xi, eta
+    std::vector<double> packed;
+    double xi0 = 0, eta0 = 0;
 };
+
+// start_sdpt3's scalings of a one-block problem (solver.c:6622-6661)
+static void sdpt3_scalings(const HProblem &P, const HBlock &Bl, double &xi, double &eta) {
+    const int nk = Bl.n;
+    double nC = 0, maxA = 0, ratio = 0;
+    for (double v : Bl.Cval) nC += v * v;
+    nC = std::sqrt(nC);
+    for (size_t a = 0; a < Bl.con.size(); a++) {
+        double s = 0;
+        for (long long e = Bl.cptr[a]; e < Bl.cptr[a + 1]; e++) s += Bl.cval[e] * Bl.cval[e];
+        s = std::sqrt(s);
+        maxA = std::max(maxA, s);
+        ratio = std::max(ratio, (1 + std::fabs(P.b[Bl.con[a]])) / (1 + s));
+    }
+    xi = std::max(10.0, std::max(std::sqrt((double)nk), nk * ratio));
+    eta = std::max(10.0, std::max(std::sqrt((double)nk), std::max(maxA, nC)));
+}
 
 // Runs f(i) for i in [0, count) on the host's threads (contiguous chunks, joined before return).
 // Set in batch workers: the host problem build of one instance then runs on the calling thread
@@ -149,6 +170,44 @@ static int build_problem(const InputData &in, HProblem &P, std::string &err) {
         if (s0 == s1) return;
         const int k = (int)(key / (m + 1));
         const int n = P.blk[k].n;
+        const long long nn = (long long)n * n;
+        if (nn <= 16 * (s1 - s0) + 4096) {
+            // dense enough: scatter the upper entries into a per-thread n x n scratch (duplicates
+            // summed in input order), then read both triangles out in position order (no sort)
+            thread_local std::vector<double> acc;
+            thread_local std::vector<char> mark;
+            if ((long long)acc.size() < nn) { acc.assign(nn, 0.0); mark.assign(nn, 0); }
+            for (long long u = s0; u < s1; u++) {
+                const long long e = order[u];
+                int i = in.i[e] - 1, j = in.j[e] - 1;
+                if (i > j) std::swap(i, j);
+                const long long q = (long long)j * n + i;
+                acc[q] += in.v[e];
+                mark[q] = 1;
+            }
+            Bucket &b = bk[key];
+            b.pos.reserve(2 * (s1 - s0));
+            b.val.reserve(2 * (s1 - s0));
+            for (int q = 0; q < n; q++)
+                for (int pp = 0; pp < n; pp++) {   // position pp + q n of the full matrix
+                    const long long uk = pp <= q ? (long long)q * n + pp : (long long)pp * n + q;
+                    if (!mark[uk] || acc[uk] == 0.0) continue;
+                    const double v = acc[uk];
+                    b.pos.push_back(pp + q * n);
+                    b.val.push_back(v);
+                    b.ss += v * v;
+                    b.sa += std::fabs(v);
+                }
+            for (long long u = s0; u < s1; u++) {   // clear the scratch for the next bucket
+                const long long e = order[u];
+                int i = in.i[e] - 1, j = in.j[e] - 1;
+                if (i > j) std::swap(i, j);
+                const long long q = (long long)j * n + i;
+                acc[q] = 0.0;
+                mark[q] = 0;
+            }
+            return;
+        }
         std::vector<std::pair<long long, double>> up;   // (upper position q*n + p with p <= q, value)
         up.reserve(s1 - s0);
         for (long long u = s0; u < s1; u++) {
@@ -1951,6 +2010,7 @@ int solve_problem_arena(const InputData &in, const Options &opt, ResultData &res
 // solved, nothing reported) when a problem does not have that shape.
 static bool lockstep_batch(int count, const std::function<bool(int, InputData &)> &get,
                            const std::function<void(int, ResultData &, int)> &put, const Options &opt) {
+    const double t0 = wtime();
     std::vector<HProblem> Ps(count);
     std::vector<int> rc(count, 0);
     std::vector<char> shape_ok(count, 1);
@@ -1964,10 +2024,26 @@ static bool lockstep_batch(int count, const std::function<bool(int, InputData &)
             shape_ok[p] = 0;
             return;
         }
-        if (build_problem(in, Ps[p], err)) rc[p] = 2;
+        if (build_problem(in, Ps[p], err)) { rc[p] = 2; return; }
+        in = InputData();
+        HProblem &P = Ps[p];
+        HBlock &Bl = P.blk[0];
+        sdpt3_scalings(P, Bl, P.xi0, P.eta0);
+        const int nk = Bl.n, tk = nk * (nk + 1) / 2;
+        P.packed.assign((size_t)P.m * tk, 0.0);
+        for (size_t a = 0; a < Bl.con.size(); a++)
+            for (long long e = Bl.cptr[a]; e < Bl.cptr[a + 1]; e++) {
+                const int pos = Bl.cpos[e], q = pos / nk, pp = pos - q * nk;
+                if (pp <= q) P.packed[(size_t)Bl.con[a] * tk + (size_t)q * (q + 1) / 2 + pp] = Bl.cval[e];
+            }
+        std::vector<int>().swap(Bl.cpos);   // the entry lists are not needed any more
+        std::vector<double>().swap(Bl.cval);
+        std::vector<long long>().swap(Bl.cptr);
+        std::vector<int>().swap(Bl.con);
     });
     for (int p = 0; p < count; p++)
         if (!shape_ok[p]) return false;
+    if (opt.verbose > 2) log_printf(1, "lockstep batch: %d problems built on the host in %.3fs\n", count, wtime() - t0);
     std::vector<int> idx;
     std::vector<HProblem> good;
     for (int p = 0; p < count; p++)
@@ -1979,9 +2055,15 @@ static bool lockstep_batch(int count, const std::function<bool(int, InputData &)
         Options o = opt;
         o.verbose = 0;
         try {
+            const double t1 = wtime();
             Lockstep L(good, o);
             L.setup();
+            const double t2 = wtime();
             L.run(res);
+            if (opt.verbose > 2)   // -vv: the phases of the batch (on the error channel: the batch runs quiet)
+                log_printf(1, "lockstep batch of %d: host build %.3fs, device setup %.3fs, start %.3fs, assembly %.3fs, "
+                           "factor %.3fs, PCG %.3fs, rest of the loop %.3fs, final %.3fs\n", (int)good.size(), t1 - t0,
+                           t2 - t1, L.t_start, L.t_asm, L.t_fac, L.t_pcg, L.t_loop, L.t_final);
         } catch (const GpuFail &f) {
             log_printf(1, "brisk: GPU failure in the lockstep batch (code %d at line %d)\n", f.rc, f.line);
             code = -3;
