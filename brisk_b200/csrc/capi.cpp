@@ -401,7 +401,22 @@ BGPU_API int bgpu_batch_solve(int count, const int *m, const int *nblk, const in
         fill_result(res[p]);
         rc[p] = code;
     };
-    return bsolve::solve_batch(count, work, get, put, opt, workers, err);
+    auto view = [&](int p, bsolve::InputView &in) {
+        const int64_t e = eoff[p];
+        in.m = m[p];
+        in.nblk = nblk[p];
+        in.bs = bs + boff[p];
+        in.c = c ? c + coff[p] : nullptr;
+        in.nnz = nnz[p];
+        in.mat = mat ? mat + e : nullptr;
+        in.blk = blk ? blk + e : nullptr;
+        in.i = i ? i + e : nullptr;
+        in.j = j ? j + e : nullptr;
+        in.v = v ? v + e : nullptr;
+        return !(in.m < 0 || in.nblk <= 0 || (in.m > 0 && !in.c) ||
+                 (in.nnz > 0 && (!in.mat || !in.blk || !in.i || !in.j || !in.v)));
+    };
+    return bsolve::solve_batch(count, work, get, put, opt, workers, err, view);
 }
 
 struct bgpu_session {

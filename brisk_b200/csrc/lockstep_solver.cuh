@@ -206,8 +206,8 @@ void Lockstep::setup() {
     std::vector<double> Ch(Ntot2, 0.0);
     {
         for (int k = 0; k < B; k++) {
-            const HBlock &Bl = Pb[k].blk[0];
-            for (size_t e = 0; e < Bl.Cpos.size(); e++) Ch[boff[k] + Bl.Cpos[e]] += Bl.Cval[e];
+            if ((long long)Pb[k].Cdense.size() != (long long)n[k] * n[k]) throw GpuFail{BGPU_ERR_ARG, __LINE__};
+            std::copy(Pb[k].Cdense.begin(), Pb[k].Cdense.end(), Ch.begin() + boff[k]);
             if ((long long)Pb[k].packed.size() != (long long)m[k] * t[k]) throw GpuFail{BGPU_ERR_ARG, __LINE__};
             if (!Pb[k].packed.empty())
                 CU(cudaMemcpyAsync(Pp + poff[k], Pb[k].packed.data(), sizeof(double) * Pb[k].packed.size(),

@@ -90,31 +90,108 @@ struct HProblem {
     // the lockstep batch keeps, instead of its one block's entry lists: the constraints as packed
     // upper rows (m x n(n+1)/2) and the start's scalings xi, eta
     std::vector<double> packed;
+    std::vector<double> Cdense;   // C (scaled), n x n
     double xi0 = 0, eta0 = 0;
 };
 
-// start_sdpt3's scalings of a one-block problem (solver.c:6622-6661)
-static void sdpt3_scalings(const HProblem &P, const HBlock &Bl, double &xi, double &eta) {
-    const int nk = Bl.n;
-    double nC = 0, maxA = 0, ratio = 0;
-    for (double v : Bl.Cval) nC += v * v;
-    nC = std::sqrt(nC);
-    for (size_t a = 0; a < Bl.con.size(); a++) {
+// build_problem for a problem of one SDP block, straight from the caller's arrays into the packed
+// rows of the lockstep batch (the same checks, duplicate sums in input order, problem_prepare
+// scaling and start_sdpt3 scalings; the row norms are summed over the packed upper entries).
+static int build_packed(const InputView &in, HProblem &P, std::string &err) {
+    const int m = in.m, n = in.bs[0];
+    if (in.nblk != 1 || n <= 0) { err = "not a one-block problem"; return 2; }
+    const int t = n * (n + 1) / 2;
+    P = HProblem();
+    P.m = m;
+    P.b0.assign(in.c, in.c + m);
+    P.b = P.b0;
+    P.blk.resize(1);
+    P.blk[0].n = n;
+    P.Ntot = n;
+    P.packed.assign((size_t)m * t, 0.0);
+    std::vector<double> Cu(t, 0.0);
+    for (long long e = 0; e < in.nnz; e++) {
+        const double v = in.v[e];
+        if (v == 0) continue;
+        const int k = in.blk[e] - 1, mt = in.mat[e];
+        if (k != 0 || mt < 0 || mt > m) { err = "entry out of range"; return 2; }
+        int i = in.i[e], j = in.j[e];
+        if (i < 1 || j < 1 || i > n || j > n) { err = "entry index out of the block"; return 2; }
+        if (i > j) std::swap(i, j);
+        const size_t u = (size_t)(j - 1) * j / 2 + (i - 1);
+        if (mt == 0) Cu[u] += v;
+        else P.packed[(size_t)(mt - 1) * t + u] += v;
+    }
+    auto w = [](int u) {   // 2 off the diagonal: both triangles count
+        int c = (int)((std::sqrt(8.0 * u + 1.0) - 1.0) * 0.5);
+        while (c * (c + 1) / 2 > u) c--;
+        while ((c + 1) * (c + 2) / 2 <= u) c++;
+        return (u - c * (c + 1) / 2 == c) ? 1.0 : 2.0;
+    };
+    std::vector<double> wt(t);
+    for (int u = 0; u < t; u++) wt[u] = w(u);
+    std::vector<double> nrm2(m, 0.0);
+    for (int a = 0; a < m; a++) {
+        const double *row = P.packed.data() + (size_t)a * t;
         double s = 0;
-        for (long long e = Bl.cptr[a]; e < Bl.cptr[a + 1]; e++) s += Bl.cval[e] * Bl.cval[e];
+        for (int u = 0; u < t; u++) s += wt[u] * row[u] * row[u];
+        nrm2[a] = s;
+    }
+    double c2 = 0, c1 = 0;
+    for (int u = 0; u < t; u++) { c2 += wt[u] * Cu[u] * Cu[u]; c1 += wt[u] * std::fabs(Cu[u]); }
+    P.normC2 = std::sqrt(c2);
+    P.normC1 = c1;
+    for (int i = 0; i < m; i++) { P.normb1 += std::fabs(P.b0[i]); P.normb2 += P.b0[i] * P.b0[i]; }
+    P.normb2 = std::sqrt(P.normb2);
+    P.d.resize(m);
+    for (int i = 0; i < m; i++) {
+        P.d[i] = nrm2[i] > 0 ? 1.0 / std::sqrt(nrm2[i]) : 1.0;
+        if (nrm2[i] == 0 && P.b[i] != 0) log_printf(1, "brisk: warning: constraint %d is empty but b != 0 (infeasible)\n", i + 1);
+    }
+    double nbv = 0;
+    for (int i = 0; i < m; i++) nbv += P.d[i] * P.b[i] * P.d[i] * P.b[i];
+    nbv = std::sqrt(nbv);
+    P.bs = nbv > 1 ? nbv : 1.0;
+    for (int a = 0; a < m; a++) {
+        double *row = P.packed.data() + (size_t)a * t;
+        for (int u = 0; u < t; u++) row[u] *= P.d[a];
+    }
+    for (int i = 0; i < m; i++) P.b[i] *= P.d[i];
+    P.du.resize(m);
+    for (int i = 0; i < m; i++) P.du[i] = P.bs / P.d[i];
+    P.cs = P.normC2 > 1 ? P.normC2 : 1.0;
+    for (int i = 0; i < m; i++) P.b[i] /= P.bs;
+    // C = -F0 (scaled) in full, and the start's scalings (start_sdpt3, solver.c:6622-6661)
+    P.Cdense.assign((size_t)n * n, 0.0);
+    double nC = 0;
+    for (int q = 0; q < n; q++)
+        for (int p = 0; p <= q; p++) {
+            const double v = -Cu[(size_t)q * (q + 1) / 2 + p] / P.cs;
+            P.Cdense[p + (size_t)q * n] = v;
+            P.Cdense[q + (size_t)p * n] = v;
+            nC += (p == q ? 1.0 : 2.0) * v * v;
+        }
+    nC = std::sqrt(nC);
+    double maxA = 0, ratio = 0;
+    for (int a = 0; a < m; a++) {
+        if (nrm2[a] == 0) continue;   // not a constraint of the block
+        const double *row = P.packed.data() + (size_t)a * t;
+        double s = 0;
+        for (int u = 0; u < t; u++) s += wt[u] * row[u] * row[u];
         s = std::sqrt(s);
         maxA = std::max(maxA, s);
-        ratio = std::max(ratio, (1 + std::fabs(P.b[Bl.con[a]])) / (1 + s));
+        ratio = std::max(ratio, (1 + std::fabs(P.b[a])) / (1 + s));
     }
-    xi = std::max(10.0, std::max(std::sqrt((double)nk), nk * ratio));
-    eta = std::max(10.0, std::max(std::sqrt((double)nk), std::max(maxA, nC)));
+    P.xi0 = std::max(10.0, std::max(std::sqrt((double)n), n * ratio));
+    P.eta0 = std::max(10.0, std::max(std::sqrt((double)n), std::max(maxA, nC)));
+    return 0;
 }
 
-// Runs f(i) for i in [0, count) on the host's threads (contiguous chunks, joined before return).
 // Set in batch workers: the host problem build of one instance then runs on the calling thread
 // (the batch already keeps every host core busy with other instances).
 static thread_local bool tl_serial = false;
 
+// Runs f(i) for i in [0, count) on the host's threads (contiguous chunks, joined before return).
 template <typename F>
 static void parallel_for(long long count, F f) {
     unsigned nt = std::thread::hardware_concurrency();
@@ -2009,6 +2086,7 @@ int solve_problem_arena(const InputData &in, const Options &opt, ResultData &res
 // problems on the host threads and solves them together (Lockstep).  Returns false (nothing
 // solved, nothing reported) when a problem does not have that shape.
 static bool lockstep_batch(int count, const std::function<bool(int, InputData &)> &get,
+                           const std::function<bool(int, InputView &)> &view,
                            const std::function<void(int, ResultData &, int)> &put, const Options &opt) {
     const double t0 = wtime();
     std::vector<HProblem> Ps(count);
@@ -2017,29 +2095,29 @@ static bool lockstep_batch(int count, const std::function<bool(int, InputData &)
     parallel_for(count, [&](long long pp) {
         const int p = (int)pp;
         tl_serial = true;
-        InputData in;
         std::string err;
-        if (!get(p, in)) { rc[p] = 2; return; }
-        if (in.nblk != 1 || in.bs.empty() || in.bs[0] < 1 || in.bs[0] > lockstep::NMAX || in.m < 1) {
+        InputData inD;
+        InputView in;
+        if (view) {
+            if (!view(p, in)) { rc[p] = 2; return; }
+        } else {
+            if (!get(p, inD)) { rc[p] = 2; return; }
+            in.m = inD.m;
+            in.nblk = inD.nblk;
+            in.bs = inD.bs.data();
+            in.c = inD.c.data();
+            in.nnz = (long long)inD.v.size();
+            in.mat = inD.mat.data();
+            in.blk = inD.blk.data();
+            in.i = inD.i.data();
+            in.j = inD.j.data();
+            in.v = inD.v.data();
+        }
+        if (in.nblk != 1 || !in.bs || in.bs[0] < 1 || in.bs[0] > lockstep::NMAX || in.m < 1) {
             shape_ok[p] = 0;
             return;
         }
-        if (build_problem(in, Ps[p], err)) { rc[p] = 2; return; }
-        in = InputData();
-        HProblem &P = Ps[p];
-        HBlock &Bl = P.blk[0];
-        sdpt3_scalings(P, Bl, P.xi0, P.eta0);
-        const int nk = Bl.n, tk = nk * (nk + 1) / 2;
-        P.packed.assign((size_t)P.m * tk, 0.0);
-        for (size_t a = 0; a < Bl.con.size(); a++)
-            for (long long e = Bl.cptr[a]; e < Bl.cptr[a + 1]; e++) {
-                const int pos = Bl.cpos[e], q = pos / nk, pp = pos - q * nk;
-                if (pp <= q) P.packed[(size_t)Bl.con[a] * tk + (size_t)q * (q + 1) / 2 + pp] = Bl.cval[e];
-            }
-        std::vector<int>().swap(Bl.cpos);   // the entry lists are not needed any more
-        std::vector<double>().swap(Bl.cval);
-        std::vector<long long>().swap(Bl.cptr);
-        std::vector<int>().swap(Bl.con);
+        if (build_packed(in, Ps[p], err)) rc[p] = 2;
     });
     for (int p = 0; p < count; p++)
         if (!shape_ok[p]) return false;
@@ -2086,11 +2164,11 @@ static bool lockstep_batch(int count, const std::function<bool(int, InputData &)
 
 int solve_batch(int count, const std::vector<double> &work, const std::function<bool(int, InputData &)> &get,
                 const std::function<void(int, ResultData &, int)> &put, const Options &opt, int workers,
-                std::string &err) {
+                std::string &err, const std::function<bool(int, InputView &)> &view) {
     if (count <= 0) return 0;
     if (workers <= 0) workers = (int)std::max(2u, std::thread::hardware_concurrency());
     workers = std::min(workers, count);
-    if (opt.batch_mode != 0 && lockstep_batch(count, get, put, opt)) return 0;
+    if (opt.batch_mode != 0 && lockstep_batch(count, get, view, put, opt)) return 0;
     std::vector<int> order(count);
     std::iota(order.begin(), order.end(), 0);
     if ((int)work.size() == count)

@@ -17,6 +17,17 @@ struct InputData {
     std::vector<double> v;
 };
 
+// The same numbers seen in place (the caller's arrays; nothing copied; zero values are skipped
+// as make_input does).
+struct InputView {
+    int m = 0, nblk = 0;
+    const int *bs = nullptr;
+    const double *c = nullptr;
+    long long nnz = 0;
+    const int *mat = nullptr, *blk = nullptr, *i = nullptr, *j = nullptr;
+    const double *v = nullptr;
+};
+
 struct Options {
     double tol = 1e-8;
     int maxit = 100;
@@ -101,9 +112,10 @@ int solve_problem_arena(const InputData &in, const Options &opt, ResultData &res
 // (false: bad problem, exit code 2); put(p, res, rc) receives its result.  Every instance runs
 // the same code as solve_problem (quiet), so its result equals the stand-alone solve's.
 // Returns 0, or 1 on bad options (err set).
+// view(p, v) (optional) gives problem p in place, for the lockstep form's host build.
 int solve_batch(int count, const std::vector<double> &work, const std::function<bool(int, InputData &)> &get,
                 const std::function<void(int, ResultData &, int)> &put, const Options &opt, int workers,
-                std::string &err);
+                std::string &err, const std::function<bool(int, InputView &)> &view = nullptr);
 
 // A problem kept resident in HBM between solves (the benchmark's device-resident timing).
 struct Session;
