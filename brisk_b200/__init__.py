@@ -6,8 +6,8 @@ The public API mirrors the reference's Python package (``brisk``): ``solve_sdpa`
 The work runs in the in-tree CUDA library ``libbrisk.so`` (sm_100a), which exports the same C
 interface as the reference's libbrisk.
 """
-from ._core import (STATUS, Result, concat_problems, interrupt, library_path, load_library, options_to_argv,
+from ._core import (STATUS, BatchSession, Result, concat_problems, interrupt, library_path, load_library, options_to_argv,
                     solve_batch, solve_batch_arrays, solve_file, solve_sdpa, version)
 
-__all__ = ["STATUS", "Result", "concat_problems", "interrupt", "library_path", "load_library", "options_to_argv",
+__all__ = ["STATUS", "BatchSession", "Result", "concat_problems", "interrupt", "library_path", "load_library", "options_to_argv",
            "solve_batch", "solve_batch_arrays", "solve_file", "solve_sdpa", "version"]

@@ -264,6 +264,65 @@ def solve_batch_arrays(m, nblk, bs, c, nnz, mat, blk, i, j, v, options=None, wor
             L.brisk_set_output(0, _PRINT(0))
 
 
+class BatchSession:
+    """A batch of one-block problems (order <= 64) kept resident in device memory
+    (bgpu_batch_create / bgpu_batch_run): build once, solve many times."""
+
+    def __init__(self, m, nblk, bs, c, nnz, mat, blk, i, j, v, options=None):
+        L = load_library()
+        L.bgpu_batch_create.restype = ctypes.c_void_p
+        L.bgpu_batch_create.argtypes = [ctypes.c_int] + [ctypes.c_void_p] * 10 + [ctypes.c_int, ctypes.c_void_p,
+                                                                                 ctypes.c_void_p]
+        L.bgpu_batch_run.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.bgpu_batch_run.restype = ctypes.c_int
+        L.bgpu_batch_destroy.argtypes = [ctypes.c_void_p]
+        L.bgpu_batch_destroy.restype = None
+        self._keep = [np.ascontiguousarray(a, dtype=t) for a, t in
+                      ((m, np.intc), (nblk, np.intc), (bs, np.intc), (c, np.float64), (nnz, np.int64),
+                       (mat, np.intc), (blk, np.intc), (i, np.intc), (j, np.intc), (v, np.float64))]
+        self.count = int(self._keep[0].size)
+        av = options_to_argv(options)
+        arr = (ctypes.c_char_p * max(len(av), 1))(*[a.encode() for a in av])
+        rc = ctypes.c_int(0)
+        with _lock:
+            L.brisk_set_output(1, _PRINT(0))
+            self.h = L.bgpu_batch_create(self.count, *[a.ctypes.data for a in self._keep], len(av), arr,
+                                         ctypes.addressof(rc))
+            L.brisk_set_output(0, _PRINT(0))
+        if not self.h:
+            raise RuntimeError(f"brisk: bgpu_batch_create failed ({rc.value})")
+
+    def run(self, collect=True):
+        """Solve every problem; the list of Results (or, collect=False, the exit codes only)."""
+        L = load_library()
+        handles = (ctypes.c_void_p * self.count)(*[L.brisk_result_new() for _ in range(self.count)])
+        rcs = np.zeros(self.count, dtype=np.intc)
+        try:
+            with _lock:
+                L.brisk_set_output(1, _PRINT(0))
+                rc = L.bgpu_batch_run(self.h, handles, rcs.ctypes.data)
+                L.brisk_set_output(0, _PRINT(0))
+            if rc != 0:
+                raise RuntimeError(f"brisk: bgpu_batch_run returned {rc}")
+            if not collect:
+                return rcs.copy()
+            return [_collect(L, handles[p], int(rcs[p]), "") for p in range(self.count)]
+        finally:
+            for p in range(self.count):
+                L.brisk_result_delete(handles[p])
+
+    def close(self):
+        if getattr(self, "h", None):
+            load_library().bgpu_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def concat_problems(problems):
     """The concatenated arrays of solve_batch_arrays for objects with the fields bs, c, mat,
     blk, i, j, v (brisk_b200.problems.SdpaData)."""

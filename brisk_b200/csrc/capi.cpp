@@ -419,6 +419,87 @@ BGPU_API int bgpu_batch_solve(int count, const int *m, const int *nblk, const in
     return bsolve::solve_batch(count, work, get, put, opt, workers, err, view);
 }
 
+struct bgpu_batch {
+    bsolve::BatchSession *s = nullptr;
+    int count = 0;
+    int verbose = 0;
+};
+
+BGPU_API bgpu_batch *bgpu_batch_create(int count, const int *m, const int *nblk, const int *bs, const double *c,
+                                       const int64_t *nnz, const int *mat, const int *blk, const int *i, const int *j,
+                                       const double *v, int nopt, const char *const *opts, int *rc) {
+    int code = 0;
+    if (count <= 0 || !m || !nblk || !bs || !nnz) code = -1;
+    std::vector<int64_t> boff(count > 0 ? count + 1 : 1, 0), coff(boff), eoff(boff);
+    for (int p = 0; !code && p < count; p++) {
+        if (nblk[p] < 0 || m[p] < 0 || nnz[p] < 0) { code = -1; break; }
+        boff[p + 1] = boff[p] + nblk[p];
+        coff[p + 1] = coff[p] + m[p];
+        eoff[p + 1] = eoff[p] + nnz[p];
+    }
+    bsolve::Options opt;
+    std::string err;
+    bsolve::set_print_hook(capi_print);
+    if (!code && bsolve::parse_options(nopt, opts, opt, err)) {
+        bsolve::log_printf(1, "brisk: %s\n", err.c_str());
+        code = 1;
+    }
+    bgpu_batch *h = nullptr;
+    if (!code) {
+        auto view = [&](int p, bsolve::InputView &in) {
+            const int64_t e = eoff[p];
+            in.m = m[p];
+            in.nblk = nblk[p];
+            in.bs = bs + boff[p];
+            in.c = c ? c + coff[p] : nullptr;
+            in.nnz = nnz[p];
+            in.mat = mat ? mat + e : nullptr;
+            in.blk = blk ? blk + e : nullptr;
+            in.i = i ? i + e : nullptr;
+            in.j = j ? j + e : nullptr;
+            in.v = v ? v + e : nullptr;
+            return !(in.m < 0 || in.nblk <= 0 || (in.m > 0 && !in.c) ||
+                     (in.nnz > 0 && (!in.mat || !in.blk || !in.i || !in.j || !in.v)));
+        };
+        int rc2 = 0;
+        bsolve::BatchSession *s = bsolve::batch_session_create(count, nullptr, view, opt, rc2);
+        if (s) {
+            h = new bgpu_batch;
+            h->s = s;
+            h->count = count;
+            h->verbose = opt.verbose;
+        } else {
+            code = rc2 ? rc2 : BGPU_ERR_UNSUPPORTED;
+        }
+    }
+    if (rc) *rc = code;
+    fflush(stdout);
+    fflush(stderr);
+    return h;
+}
+
+BGPU_API int bgpu_batch_run(bgpu_batch *h, BriskResult *const *res, int *rc) {
+    if (!h || !res || !rc) return -1;
+    for (int p = 0; p < h->count; p++)
+        if (!res[p]) return -1;
+    auto put = [&](int p, bsolve::ResultData &r, int code) {
+        res[p]->r = std::move(r);
+        fill_result(res[p]);
+        rc[p] = code;
+    };
+    bsolve::set_print_hook(capi_print);
+    const int code = bsolve::batch_session_solve(h->s, put, h->verbose);
+    fflush(stdout);
+    fflush(stderr);
+    return code;
+}
+
+BGPU_API void bgpu_batch_destroy(bgpu_batch *h) {
+    if (!h) return;
+    bsolve::batch_session_destroy(h->s);
+    delete h;
+}
+
 struct bgpu_session {
     bsolve::Session *s = nullptr;
 };

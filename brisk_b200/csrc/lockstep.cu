@@ -18,7 +18,45 @@ __device__ __forceinline__ void unpk(int u, int &p, int &q) {
     p = u - c * (c + 1) / 2;
 }
 
-// one work item: ITEM constraints of one instance; shared: X, Z, A, W (n x n each)
+// C = A B for n x n matrices in shared memory (column-major), thread (tx, ty) of a 16 x 16 grid
+// owning the RT x RT outputs (tx + 16 r, ty + 16 c): consecutive tx read consecutive A rows.
+template <int RT>
+__device__ __forceinline__ void smem_gemm(int n, const double *__restrict__ A, const double *__restrict__ Bm,
+                                          double *__restrict__ C) {
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    double acc[RT][RT];
+#pragma unroll
+    for (int r = 0; r < RT; r++)
+#pragma unroll
+        for (int c = 0; c < RT; c++) acc[r][c] = 0.0;
+    for (int q = 0; q < n; q++) {
+        double a[RT], b[RT];
+#pragma unroll
+        for (int r = 0; r < RT; r++) { const int i = tx + 16 * r; a[r] = i < n ? A[i + q * n] : 0.0; }
+#pragma unroll
+        for (int c = 0; c < RT; c++) { const int j = ty + 16 * c; b[c] = j < n ? Bm[q + j * n] : 0.0; }
+#pragma unroll
+        for (int r = 0; r < RT; r++)
+#pragma unroll
+            for (int c = 0; c < RT; c++) acc[r][c] += a[r] * b[c];
+    }
+#pragma unroll
+    for (int r = 0; r < RT; r++)
+#pragma unroll
+        for (int c = 0; c < RT; c++) {
+            const int i = tx + 16 * r, j = ty + 16 * c;
+            if (i < n && j < n) C[i + j * n] = acc[r][c];
+        }
+}
+
+__device__ __forceinline__ void smem_gemm_n(int n, const double *A, const double *Bm, double *C) {
+    if (n <= 16) smem_gemm<1>(n, A, Bm, C);
+    else if (n <= 32) smem_gemm<2>(n, A, Bm, C);
+    else if (n <= 48) smem_gemm<3>(n, A, Bm, C);
+    else smem_gemm<4>(n, A, Bm, C);
+}
+
+// one work item: ITEM constraints of one instance; shared: X, Z, A, W (n x n each); 256 threads
 __global__ void __launch_bounds__(256) form_q_kernel(const int2 *__restrict__ items, const int *__restrict__ nv,
                                                      const int *__restrict__ mv, const long long *__restrict__ boff,
                                                      const long long *__restrict__ poff, const double *__restrict__ P,
@@ -36,29 +74,22 @@ __global__ void __launch_bounds__(256) form_q_kernel(const int2 *__restrict__ it
     const int a1 = min(m, a0 + ITEM);
     for (int a = a0; a < a1; a++) {
         const double *prow = Pk + (long long)a * t;
-        __syncthreads();   // the previous constraint's A and W are no longer read
-        for (int idx = threadIdx.x; idx < nn; idx += blockDim.x) {
-            const int i = idx % n, j = idx / n;
-            As[idx] = prow[i <= j ? upk(i, j) : upk(j, i)];
+        __syncthreads();   // the previous constraint's A (G) is no longer read
+        for (int u = threadIdx.x; u < t; u += blockDim.x) {   // A from its packed upper entries
+            int i, j;
+            unpk(u, i, j);
+            const double v = prow[u];
+            As[i + j * n] = v;
+            As[j + i * n] = v;
         }
         __syncthreads();
-        for (int idx = threadIdx.x; idx < nn; idx += blockDim.x) {   // W = A Zi
-            const int i = idx % n, j = idx / n;
-            double s = 0.0;
-            for (int q = 0; q < n; q++) s += As[i + q * n] * Zs[q + j * n];   // consecutive i: no bank conflicts
-            Ws[idx] = s;
-        }
+        smem_gemm_n(n, As, Zs, Ws);   // W = A Zi
         __syncthreads();
-        for (int idx = threadIdx.x; idx < nn; idx += blockDim.x) {   // G = X W, into A's buffer
-            const int i = idx % n, j = idx / n;
-            double s = 0.0;
-            for (int q = 0; q < n; q++) s += Xs[i + q * n] * Ws[q + j * n];
-            As[idx] = s;
-        }
+        smem_gemm_n(n, Xs, Ws, As);   // G = X W, into A's buffer
         __syncthreads();
         double *qrow = Qk + (long long)a * t;
         for (int u = threadIdx.x; u < t; u += blockDim.x) {   // Q = packed (G + G')
-            int j, i;
+            int i, j;
             unpk(u, i, j);
             qrow[u] = (i < j) ? As[i + j * n] + As[j + i * n] : As[i + i * n];
         }

@@ -2082,15 +2082,27 @@ int solve_problem_arena(const InputData &in, const Options &opt, ResultData &res
     return rc;
 }
 
-// The lockstep form of the batch when every problem has one SDP block of order <= 64: builds the
-// problems on the host threads and solves them together (Lockstep).  Returns false (nothing
-// solved, nothing reported) when a problem does not have that shape.
-static bool lockstep_batch(int count, const std::function<bool(int, InputData &)> &get,
-                           const std::function<bool(int, InputView &)> &view,
-                           const std::function<void(int, ResultData &, int)> &put, const Options &opt) {
+// The lockstep form of the batch when every problem has one SDP block of order <= 64: the problems
+// are built on the host threads (build_packed) and solved together (Lockstep).
+struct BatchSession {
+    std::vector<HProblem> good;
+    std::vector<int> idx;        // problem number of each good problem
+    std::vector<int> bad;        // problems rejected on input (exit code 2)
+    int count = 0;
+    Options opt;
+    Lockstep *L = nullptr;
+    double t_build = 0, t_setup = 0;
+    ~BatchSession() { delete L; }
+};
+
+// Builds the session; returns nullptr when a problem does not have that shape (rc = 0: nothing
+// reported), or on a GPU failure (rc < 0).
+BatchSession *batch_session_create(int count, const std::function<bool(int, InputData &)> &get,
+                                   const std::function<bool(int, InputView &)> &view, const Options &opt, int &rc) {
+    rc = 0;
     const double t0 = wtime();
     std::vector<HProblem> Ps(count);
-    std::vector<int> rc(count, 0);
+    std::vector<int> bad(count, 0);
     std::vector<char> shape_ok(count, 1);
     parallel_for(count, [&](long long pp) {
         const int p = (int)pp;
@@ -2099,9 +2111,9 @@ static bool lockstep_batch(int count, const std::function<bool(int, InputData &)
         InputData inD;
         InputView in;
         if (view) {
-            if (!view(p, in)) { rc[p] = 2; return; }
+            if (!view(p, in)) { bad[p] = 1; return; }
         } else {
-            if (!get(p, inD)) { rc[p] = 2; return; }
+            if (!get(p, inD)) { bad[p] = 1; return; }
             in.m = inD.m;
             in.nblk = inD.nblk;
             in.bs = inD.bs.data();
@@ -2117,48 +2129,84 @@ static bool lockstep_batch(int count, const std::function<bool(int, InputData &)
             shape_ok[p] = 0;
             return;
         }
-        if (build_packed(in, Ps[p], err)) rc[p] = 2;
+        if (build_packed(in, Ps[p], err)) bad[p] = 1;
     });
     for (int p = 0; p < count; p++)
-        if (!shape_ok[p]) return false;
-    if (opt.verbose > 2) log_printf(1, "lockstep batch: %d problems built on the host in %.3fs\n", count, wtime() - t0);
-    std::vector<int> idx;
-    std::vector<HProblem> good;
-    for (int p = 0; p < count; p++)
-        if (rc[p] == 0) { idx.push_back(p); good.push_back(std::move(Ps[p])); }
+        if (!shape_ok[p]) return nullptr;
+    BatchSession *S = new BatchSession;
+    S->count = count;
+    S->opt = opt;
+    S->opt.verbose = 0;
+    for (int p = 0; p < count; p++) {
+        if (bad[p]) S->bad.push_back(p);
+        else { S->idx.push_back(p); S->good.push_back(std::move(Ps[p])); }
+    }
     Ps.clear();
+    S->t_build = wtime() - t0;
+    if (!S->good.empty()) {
+        try {
+            S->L = new Lockstep(S->good, S->opt);
+            S->L->setup();
+        } catch (const GpuFail &f) {
+            log_printf(1, "brisk: GPU failure in the lockstep batch set-up (code %d at line %d)\n", f.rc, f.line);
+            delete S;
+            rc = -3;
+            return nullptr;
+        }
+    }
+    S->t_setup = wtime() - t0 - S->t_build;
+    return S;
+}
+
+// Solves the session's problems; put(p, res, rc) receives each.  Returns 0 or -3.
+int batch_session_solve(BatchSession *S, const std::function<void(int, ResultData &, int)> &put, int verbose) {
     std::vector<ResultData> res;
     int code = 0;
-    if (!good.empty()) {
-        Options o = opt;
-        o.verbose = 0;
+    if (S->L) {
         try {
-            const double t1 = wtime();
-            Lockstep L(good, o);
-            L.setup();
-            const double t2 = wtime();
-            L.run(res);
-            if (opt.verbose > 2)   // -vv: the phases of the batch (on the error channel: the batch runs quiet)
+            S->L->run(res);
+            if (verbose > 2)   // -vv: the phases of the batch (on the error channel: the batch runs quiet)
                 log_printf(1, "lockstep batch of %d: host build %.3fs, device setup %.3fs, start %.3fs, assembly %.3fs, "
-                           "factor %.3fs, PCG %.3fs, rest of the loop %.3fs, final %.3fs\n", (int)good.size(), t1 - t0,
-                           t2 - t1, L.t_start, L.t_asm, L.t_fac, L.t_pcg, L.t_loop, L.t_final);
+                           "factor %.3fs, PCG %.3fs, rest of the loop %.3fs, final %.3fs\n", (int)S->good.size(),
+                           S->t_build, S->t_setup, S->L->t_start, S->L->t_asm, S->L->t_fac, S->L->t_pcg,
+                           S->L->t_loop, S->L->t_final);
         } catch (const GpuFail &f) {
             log_printf(1, "brisk: GPU failure in the lockstep batch (code %d at line %d)\n", f.rc, f.line);
             code = -3;
         }
     }
-    for (size_t q = 0; q < idx.size(); q++) {
+    for (size_t q = 0; q < S->idx.size(); q++) {
         ResultData r = code ? ResultData() : std::move(res[q]);
-        if (code) r.status = 4;
-        r.exit_code = code ? code : r.exit_code;
-        put(idx[q], r, code ? code : r.exit_code);
+        if (code) { r.status = 4; r.exit_code = code; }
+        put(S->idx[q], r, code ? code : r.exit_code);
     }
-    for (int p = 0; p < count; p++)
-        if (rc[p]) {
+    for (int p : S->bad) {
+        ResultData r;
+        r.exit_code = 2;
+        put(p, r, 2);
+    }
+    return code;
+}
+
+void batch_session_destroy(BatchSession *S) { delete S; }
+
+static bool lockstep_batch(int count, const std::function<bool(int, InputData &)> &get,
+                           const std::function<bool(int, InputView &)> &view,
+                           const std::function<void(int, ResultData &, int)> &put, const Options &opt) {
+    int rc = 0;
+    BatchSession *S = batch_session_create(count, get, view, opt, rc);
+    if (!S) {
+        if (rc == 0) return false;   // not the lockstep shape: the concurrent form runs
+        for (int p = 0; p < count; p++) {
             ResultData r;
-            r.exit_code = rc[p];
-            put(p, r, rc[p]);
+            r.status = 4;
+            r.exit_code = rc;
+            put(p, r, rc);
         }
+        return true;
+    }
+    batch_session_solve(S, put, opt.verbose);
+    batch_session_destroy(S);
     return true;
 }
 

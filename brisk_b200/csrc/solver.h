@@ -117,6 +117,13 @@ int solve_batch(int count, const std::vector<double> &work, const std::function<
                 const std::function<void(int, ResultData &, int)> &put, const Options &opt, int workers,
                 std::string &err, const std::function<bool(int, InputView &)> &view = nullptr);
 
+// A batch of one-block problems (order <= 64) kept resident in HBM between lockstep solves.
+struct BatchSession;
+BatchSession *batch_session_create(int count, const std::function<bool(int, InputData &)> &get,
+                                   const std::function<bool(int, InputView &)> &view, const Options &opt, int &rc);
+int batch_session_solve(BatchSession *S, const std::function<void(int, ResultData &, int)> &put, int verbose);
+void batch_session_destroy(BatchSession *S);
+
 // A problem kept resident in HBM between solves (the benchmark's device-resident timing).
 struct Session;
 Session *session_create(const InputData &in, const Options &opt, std::string &err, int &rc);

@@ -65,6 +65,20 @@ BGPU_API int bgpu_batch_solve(int count, const int *m, const int *nblk, const in
                               const int64_t *nnz, const int *mat, const int *blk, const int *i, const int *j,
                               const double *v, int nopt, const char *const *opts, int workers,
                               struct BriskResult *const *res, int *rc);
+/* A batch kept resident in device memory between solves: bgpu_batch_create takes the arrays of
+ * bgpu_batch_solve for problems of one SDP block of order <= 64 each (the lockstep form), builds
+ * and uploads them, and returns a handle (NULL on failure; *rc: 1 bad options, -1 bad arguments,
+ * -6 a problem not of that shape, < 0 a GPU failure).  bgpu_batch_run solves every problem from
+ * the resident data into res[p] (brisk_result_new handles), rc[p] its exit code (2 for a problem
+ * rejected on input), and returns 0 or a negative GPU failure code.  Extension of this build: the
+ * reference re-reads every problem on every call. */
+typedef struct bgpu_batch bgpu_batch;
+BGPU_API bgpu_batch *bgpu_batch_create(int count, const int *m, const int *nblk, const int *bs, const double *c,
+                                       const int64_t *nnz, const int *mat, const int *blk, const int *i, const int *j,
+                                       const double *v, int nopt, const char *const *opts, int *rc);
+BGPU_API int bgpu_batch_run(bgpu_batch *h, struct BriskResult *const *res, int *rc);
+BGPU_API void bgpu_batch_destroy(bgpu_batch *h);
+
 /* Measures of the last solve of res: [0] device time (s, CUDA events on the library's
  * stream), [1] assembly device time (s), [2] assembly algorithmic flops, [3] host-to-device
  * bytes, [4] device-to-host bytes, [5] iterations, [6] float factorizations, [7] PCG steps. */

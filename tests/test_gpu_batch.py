@@ -93,3 +93,17 @@ def test_batch_rejects_bad_options():
     d = problems.batch_instance(5)
     with pytest.raises(RuntimeError):
         brisk_b200.solve_batch([d], options=["-tol", "abc"])
+
+
+def test_resident_batch_runs_twice_like_the_one_call_batch():
+    """bgpu_batch_create + bgpu_batch_run (resident) gives the bits of bgpu_batch_solve, run after run."""
+    arrs = brisk_b200.concat_problems([problems.batch_instance(q) for q in range(200, 240)])
+    ref = brisk_b200.solve_batch_arrays(**arrs, options=FP64)
+    sess = brisk_b200.BatchSession(**arrs, options=FP64)
+    for _ in range(2):
+        out = sess.run()
+        for a, b in zip(out, ref):
+            assert a.status == b.status and a.iterations == b.iterations
+            assert a.pobj == b.pobj and a.dobj == b.dobj
+            np.testing.assert_array_equal(a.y, b.y)
+    sess.close()
