@@ -2,13 +2,16 @@
 
     python -m brisk_b200 problem.dat-s -tol 1e-7 -v
     python -m brisk_b200 --workload rand1000 -asmprec tf32x3 -v
+    python -m brisk_b200 --batch 4096 -tol 1e-7 -mixed 0       (the first N instances of the
+                                                                uneven batch, one bgpu_batch_solve)
 
 The file form mirrors the reference's command line (`brisk <file> <options>`, main.c:3571); the
 workload form solves one of the seeded instances of brisk_b200.problems.
 """
 import sys
+import time
 
-from . import problems, solve_file, solve_sdpa
+from . import problems, solve_batch_arrays, solve_file, solve_sdpa
 
 WORKLOADS = {
     "theta50": lambda: problems.theta_problem(n=50, p=0.5, seed=1),
@@ -23,6 +26,18 @@ def main(argv):
     if not argv:
         print(__doc__)
         return 1
+    if argv[0] == "--batch":
+        if len(argv) < 2 or not argv[1].isdigit():
+            print("--batch N: the first N instances of the uneven 4096-instance batch")
+            return 1
+        arrs = problems.batch_arrays(int(argv[1]))
+        t0 = time.time()
+        out = solve_batch_arrays(**arrs, options=argv[2:])
+        st = {}
+        for r in out:
+            st[r.status_str] = st.get(r.status_str, 0) + 1
+        print(f"batch of {len(out)}: {st}, {time.time() - t0:.3f} s")
+        return max((r.exit_code for r in out), default=0)
     if argv[0] == "--workload":
         if len(argv) < 2 or argv[1] not in WORKLOADS:
             print("workloads: " + ", ".join(sorted(WORKLOADS)))
