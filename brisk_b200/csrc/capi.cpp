@@ -121,9 +121,9 @@ int parse_options(int argc, const char *const *argv, Options &opt, std::string &
             const char *s = need("a number");
             if (!s || !parse_double(s, opt.mu_switch)) { if (err.empty()) err = "bad -muswitch"; return 1; }
         } else if (a == "-mixedshift") {
-            const char *s = need("0, 1 or 2");
-            if (!s || !parse_int(s, opt.mixed_shift) || opt.mixed_shift < 0 || opt.mixed_shift > 2) {
-                if (err.empty()) err = "bad -mixedshift (0, 1 or 2)";
+            const char *s = need("0 or 1");
+            if (!s || !parse_int(s, opt.mixed_shift) || opt.mixed_shift < 0 || opt.mixed_shift > 1) {
+                if (err.empty()) err = "bad -mixedshift (0 or 1)";
                 return 1;
             }
         } else if (a == "-schurchunk") {

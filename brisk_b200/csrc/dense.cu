@@ -29,7 +29,7 @@ constexpr int LDS = NB + 1;     // padded smem stride
 // final once divided by L(k,k); the rows below subtract L(r,k) X(k,:).
 template <typename T>
 __global__ void __launch_bounds__(256) potrf_diag_kernel(int n, T *A, long long lda, int j0, T *dinv, int *info,
-                                                         double *pmin, double tiny, double repl, int *nrep) {
+                                                         double *pmin) {
     extern __shared__ __align__(16) unsigned char dsm_raw[];
     T *S = reinterpret_cast<T *>(dsm_raw);   // S[r + c*LDS]: factor, then L
     T *X = S + NB * LDS;                      // inverse of L
@@ -52,11 +52,7 @@ __global__ void __launch_bounds__(256) potrf_diag_kernel(int n, T *A, long long 
     int fail = 0;
     T prev_inv = (T)0, prev_piv = (T)0;
     for (int c = 0; c < nb; c++) {
-        T d = S[c + c * LDS];
-        if (tiny > 0 && isfinite((double)d) && !((double)d > tiny)) {   // pivot replacement: every thread
-            d = (T)repl;                                                 // decides alike on the same value
-            if (tid == 0) atomicAdd(nrep, 1);
-        }
+        const T d = S[c + c * LDS];
         if (!(d > (T)0) || !isfinite((double)d)) { fail = j0 + c + 1; break; }
         if ((double)d < pm) pm = (double)d;
         const T inv_d = (T)1 / d;
@@ -353,18 +349,12 @@ int diag_smem_attr() {
 }
 
 int potrf_f64(cudaStream_t st, int n, double *A, long long lda, double *dinv, int *d_info, double *d_pmin) {
-    return potrf_f64_repl(st, n, A, lda, dinv, d_info, d_pmin, 0.0, 0.0, nullptr);
-}
-
-int potrf_f64_repl(cudaStream_t st, int n, double *A, long long lda, double *dinv, int *d_info, double *d_pmin,
-                   double tiny, double repl, int *nrep) {
-    if (tiny > 0 && !nrep) return BGPU_ERR_ARG;
     if (int rc = diag_smem_attr<double>()) return rc;
     init_info_kernel<<<1, 1, 0, st>>>(d_info, d_pmin);
     BGPU_LAUNCH_CHECK();
     for (int j0 = 0; j0 < n; j0 += NB) {
         const int nb = (n - j0 < NB) ? n - j0 : NB;
-        potrf_diag_kernel<double><<<1, 256, 2 * NB * LDS * sizeof(double), st>>>(n, A, lda, j0, dinv + (size_t)(j0 / NB) * NB * NB, d_info, d_pmin, tiny, repl, nrep);
+        potrf_diag_kernel<double><<<1, 256, 2 * NB * LDS * sizeof(double), st>>>(n, A, lda, j0, dinv + (size_t)(j0 / NB) * NB * NB, d_info, d_pmin);
         BGPU_LAUNCH_CHECK();
         const int rest = n - j0 - nb;
         if (rest <= 0) break;
@@ -387,7 +377,7 @@ int potrf_f32(cudaStream_t st, int n, float *A, long long lda, float *dinv, int 
     BGPU_LAUNCH_CHECK();
     for (int j0 = 0; j0 < n; j0 += NB) {
         const int nb = (n - j0 < NB) ? n - j0 : NB;
-        potrf_diag_kernel<float><<<1, 256, 2 * NB * LDS * sizeof(float), st>>>(n, A, lda, j0, dinv + (size_t)(j0 / NB) * NB * NB, d_info, d_pmin, 0.0, 0.0, nullptr);
+        potrf_diag_kernel<float><<<1, 256, 2 * NB * LDS * sizeof(float), st>>>(n, A, lda, j0, dinv + (size_t)(j0 / NB) * NB * NB, d_info, d_pmin);
         BGPU_LAUNCH_CHECK();
         const int rest = n - j0 - nb;
         if (rest <= 0) break;

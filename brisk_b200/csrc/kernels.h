@@ -31,10 +31,6 @@ constexpr int TRI_NB = 64;   // diagonal block order of the blocked factor and s
 // 64*64, column-major), the first failing column (1-based, 0 when none) to *d_info and the
 // smallest squared pivot to *d_pmin (both device scalars, reset here).
 int potrf_f64(cudaStream_t st, int n, double *A, long long lda, double *dinv, int *d_info, double *d_pmin);
-// The same with pivot replacement: a pivot <= tiny is replaced by repl (and counted in *nrep),
-// so the factor of a matrix known only to FP32 accuracy stays a preconditioner.
-int potrf_f64_repl(cudaStream_t st, int n, double *A, long long lda, double *dinv, int *d_info, double *d_pmin,
-                   double tiny, double repl, int *nrep);
 int potrf_f32(cudaStream_t st, int n, float *A, long long lda, float *dinv, int *d_info, double *d_pmin);
 
 // Persistent flag-chained triangular solves with the factor of potrf_*: x <- L^{-1} x (trans=0)

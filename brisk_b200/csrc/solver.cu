@@ -585,8 +585,7 @@ class Solver {
     schol::Factor sp_f;
     void choose_sparse();
     float *Mf = nullptr, *dinvMf = nullptr;
-    int *mflags = nullptr, *d_info = nullptr, *d_err = nullptr, *d_nrep = nullptr;
-    int nrep = 0;   // pivots the last factor replaced (the mixed path's -mixedshift 2)
+    int *mflags = nullptr, *d_info = nullptr, *d_err = nullptr;
     double *d_pmin = nullptr;
     double *dv_in = nullptr, *dv_out = nullptr;   // m (or n) vectors
     float *fv = nullptr;
@@ -855,7 +854,6 @@ void Solver::setup() {
     mflags = g.alloc<int>(mb64);
     d_info = g.alloc<int>(1);
     d_err = g.alloc<int>(1);
-    d_nrep = g.alloc<int>(1);
     d_pmin = g.alloc<double>(1);
     const int vlen = std::max(m, nmax);
     dv_in = g.alloc<double>(vlen);
@@ -1199,24 +1197,6 @@ int Solver::factor() {
     }
     double r = reg_hint ? std::max(reg_floor, 0.01 * reg_ok) : 0.0;
     int info = 0;
-    nrep = 0;
-    if (!m_exact && opt.mixed_shift == 2) {
-        // the FP32-accurate M: a pivot below 1e-10 of its (unit) scaled diagonal is replaced by 1,
-        // no shift; PCG against the FP64 operator recovers those directions
-        CU(cudaMemsetAsync(d_nrep, 0, sizeof(int), g.st));
-        RC(schur_load_f64(g.st, m, M, m, 0.0, Dsc, Lm, m));
-        RC(potrf_f64_repl(g.st, m, Lm, m, dinvM, d_info, d_pmin, 1e-10, 1.0, d_nrep));
-        double pmin = 0;
-        CU(cudaMemcpyAsync(&info, d_info, sizeof(int), cudaMemcpyDeviceToHost, g.st));
-        CU(cudaMemcpyAsync(&pmin, d_pmin, sizeof(double), cudaMemcpyDeviceToHost, g.st));
-        CU(cudaMemcpyAsync(&nrep, d_nrep, sizeof(int), cudaMemcpyDeviceToHost, g.st));
-        CU(cudaStreamSynchronize(g.st));
-        if (info == 0) {
-            reg = 0;
-            min_pivot = pmin;
-            return 0;
-        }
-    }
     for (int attempt = 0; attempt < 10; attempt++) {
         RC(schur_load_f64(g.st, m, M, m, r, Dsc, Lm, m));
         RC(potrf_f64(g.st, m, Lm, m, dinvM, d_info, d_pmin));
@@ -1319,7 +1299,7 @@ double Solver::schur_solve(const std::vector<double> &rhs, std::vector<double> &
     p = z;
     double rz = dot(r, z);
     // the factor of a shifted 3xTF32 M preconditions the FP64 operator less well: more steps
-    const bool shifted = !m_exact && (reg > 0 || nrep > 0);
+    const bool shifted = !m_exact && reg > 0;
     const int maxit = shifted ? 150 : (reg > 0 || approx) ? 50 : 10;
     int stall = 0, used = 0;
     const double sgain = 0.9;
@@ -1995,9 +1975,8 @@ int Solver::run(ResultData &res) {
         for (int i = 0; i < m; i++) y[i] += adn * dy[i];
         theta *= (1.0 - adn);
         if (opt.verbose > 1)
-            log_printf(0, "     [schur %.3fs %s, factor %s reg %.0e pmin %.1e%s, pcg %d, step %.3fs]\n", tm.schur - ts_before,
-                       m_exact ? "fp64" : "tf32x3", is_float ? "fp32" : "fp64", reg, min_pivot,
-                       nrep ? (" repl " + std::to_string(nrep)).c_str() : "", pcg_iters, tm.step - tstep_before);
+            log_printf(0, "     [schur %.3fs %s, factor %s reg %.0e pmin %.1e, pcg %d, step %.3fs]\n", tm.schur - ts_before,
+                       m_exact ? "fp64" : "tf32x3", is_float ? "fp32" : "fp64", reg, min_pivot, pcg_iters, tm.step - tstep_before);
         alp = apn;
         ald = adn;
         stall = (apn < 1e-6 && adn < 1e-6) ? stall + 1 : 0;
