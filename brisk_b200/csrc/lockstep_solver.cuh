@@ -288,13 +288,21 @@ void Lockstep::segdots(int nq, const double *const *a, const double *const *b, s
 void Lockstep::assemble(const std::vector<int> &L, const double *X, const double *Zi) {
     if (L.empty()) return;
     const double t0 = wtime();
+    // the Q form's work items by block-order class (the shared memory of a launch is sized by its
+    // largest n: the small classes run several CTAs per SM)
+    const int cls_max[4] = {16, 32, 48, 64};
     std::vector<int2> items;
+    std::vector<int> cls_start(5, 0);
     std::vector<int4> tiles;
     const int TR = gemm_grouped_tile_rows();
-    int nm = 1;
+    for (int c = 0; c < 4; c++) {
+        cls_start[c] = (int)items.size();
+        for (int k : L)
+            if (n[k] <= cls_max[c] && (c == 0 || n[k] > cls_max[c - 1]))
+                for (int a0 = 0; a0 < m[k]; a0 += lockstep::ITEM) items.push_back(make_int2(k, a0));
+    }
+    cls_start[4] = (int)items.size();
     for (int k : L) {
-        nm = std::max(nm, n[k]);
-        for (int a0 = 0; a0 < m[k]; a0 += lockstep::ITEM) items.push_back(make_int2(k, a0));
         for (int ti = 0; ti < ceil_div(m[k], TR); ti++)
             for (int tj = 0; tj < ceil_div(m[k], 64); tj++)
                 if (ti * TR + TR - 1 >= tj * 64) tiles.push_back(make_int4(k, ti, tj, 0));
@@ -302,7 +310,9 @@ void Lockstep::assemble(const std::vector<int> &L, const double *X, const double
     }
     CU(cudaMemcpyAsync(d_items, items.data(), sizeof(int2) * items.size(), cudaMemcpyHostToDevice, g.st));
     CU(cudaMemcpyAsync(d_tiles, tiles.data(), sizeof(int4) * tiles.size(), cudaMemcpyHostToDevice, g.st));
-    RC(lockstep::form_q(g.st, Ld, d_items, (int)items.size(), nm, Pp, X, Zi, Qp));
+    for (int c = 0; c < 4; c++)
+        RC(lockstep::form_q(g.st, Ld, d_items + cls_start[c], cls_start[c + 1] - cls_start[c], cls_max[c], Pp, X, Zi,
+                            Qp));
     RC(gemm_f64_grouped(g.st, (int)tiles.size(), d_tiles, d_groups, 1.0, 0.0));
     upload_list(L);
     RC(lockstep::mirror(g.st, Ld, d_list, (int)L.size(), Mm));
