@@ -5,6 +5,7 @@
 #include "tf32x3.h"
 #include "small.h"
 #include "sparse.h"
+#include "nt.h"
 
 long long g_bgpu_launches = 0;
 static cudaStream_t S(void *s) { return (cudaStream_t)s; }
@@ -23,6 +24,55 @@ BGPU_API size_t bgpu_schur_ws_bytes(int n, int chunk, int precision) {
     return schur_ws_bytes(n, chunk, precision);
 }
 BGPU_API int bgpu_schur_chunk_default(int n, int precision) { return schur_chunk_default(n, precision); }
+
+BGPU_API size_t bgpu_nt_ws_bytes(int n) {
+    if (n <= 0) return 0;
+    if (n <= nt::SMALL_NMAX) return 256;
+    return 2 * (size_t)n * n * sizeof(double) + 256;
+}
+
+BGPU_API int bgpu_nt_scaling(int n, const double *d_LX, const double *d_LZ, double *d_G, double *d_lam,
+                             double *d_W, void *d_ws, size_t ws_bytes, int *sweeps, void *stream) {
+    if (sweeps) *sweeps = 0;
+    if (n <= 0 || !d_LX || !d_LZ || !d_G || !d_lam || !d_W || !d_ws || ws_bytes < bgpu_nt_ws_bytes(n))
+        return BGPU_ERR_ARG;
+    cudaStream_t st = S(stream);
+    int info = 0;
+    if (n <= nt::SMALL_NMAX) {
+        // the one-CTA form over a table of one block: 5 pointers, then n and info
+        struct Tab {
+            const double *LX, *LZ;
+            double *G, *lam, *W;
+            int n, info;
+        } h{d_LX, d_LZ, d_G, d_lam, d_W, n, 0};
+        Tab *t = (Tab *)d_ws;
+        BGPU_CHECK(cudaMemcpyAsync(t, &h, sizeof(Tab), cudaMemcpyHostToDevice, st));
+        int rc = nt::scaling_small(st, 1, &t->n, n, &t->LX, &t->LZ, &t->G, &t->lam, &t->W, &t->info);
+        if (rc) return rc;
+        BGPU_CHECK(cudaMemcpyAsync(&info, &t->info, sizeof(int), cudaMemcpyDeviceToHost, st));
+        BGPU_CHECK(cudaStreamSynchronize(st));
+        return info == 0 ? BGPU_OK : (info == 2 ? BGPU_ERR_TIMEOUT : BGPU_ERR_NOTPD);
+    }
+    double *Mb = (double *)d_ws, *Lz = Mb + (size_t)n * n;
+    int *flag = (int *)(Lz + (size_t)n * n), *dinfo = flag + 1;
+    int rc = nt::tril(st, n, d_LX, d_G);
+    if (!rc) rc = nt::tril(st, n, d_LZ, Lz);
+    if (!rc) rc = gemm_f64(st, 1, 1, n, n, n, 1.0, Lz, n, 0, d_G, n, 0, 0.0, Mb, n, 0, 1, 0);   // L_Z' L_X
+    if (rc) return rc;
+    int hflag = 0, sw = 0;
+    rc = nt::jacobi(st, n, Mb, d_G, flag, &hflag, &sw);
+    if (rc) return rc;
+    if (sweeps) *sweeps = sw;
+    if (sw < 0) return BGPU_ERR_TIMEOUT;
+    BGPU_CHECK(cudaMemsetAsync(dinfo, 0, sizeof(int), st));
+    rc = nt::finish(st, n, Mb, d_G, d_lam, dinfo);
+    if (!rc) rc = gemm_f64(st, 0, 0, n, n, n, 1.0, d_G, n, 0, d_G, n, 0, 0.0, d_W, n, 0, 1, 0);   // G G'
+    if (!rc) rc = symmetrize_f64(st, n, d_W, n);
+    if (rc) return rc;
+    BGPU_CHECK(cudaMemcpyAsync(&info, dinfo, sizeof(int), cudaMemcpyDeviceToHost, st));
+    BGPU_CHECK(cudaStreamSynchronize(st));
+    return info ? BGPU_ERR_NOTPD : BGPU_OK;
+}
 
 BGPU_API int bgpu_schur_colptr(int n, int ncon, const long long *d_cptr, const int *d_cpos, int *d_ccol, void *stream) {
     DevBlock B;

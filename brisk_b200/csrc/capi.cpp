@@ -151,7 +151,10 @@ int parse_options(int argc, const char *const *argv, Options &opt, std::string &
         } else if (a == "-dir") {
             const char *s = need("hkm, nt or auto");
             if (!s) return 1;
-            if (strcmp(s, "hkm") && strcmp(s, "auto")) { err = "this build solves with the HKM direction only (-dir hkm)"; return 1; }
+            if (!strcmp(s, "nt")) opt.direction = 1;
+            else if (!strcmp(s, "hkm")) opt.direction = 0;
+            else if (!strcmp(s, "auto")) opt.direction = -1;
+            else { err = "-dir must be auto, hkm or nt"; return 1; }
         } else if (a == "-init") {
             const char *s = need("0 or 1");
             if (!s || !parse_int(s, opt.init) || opt.init < 0) { if (err.empty()) err = "bad -init"; return 1; }

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <cstdio>
+#include <cmath>
 
 #if !defined(__CUDA_ARCH__) || (__CUDA_ARCH__ >= 1000)
 #else

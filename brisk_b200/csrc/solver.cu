@@ -1,15 +1,15 @@
-// The infeasible-start primal-dual interior-point loop (HKM direction, Mehrotra predictor-
+// The infeasible-start primal-dual interior-point loop (HKM or NT direction, Mehrotra predictor-
 // corrector) with every O(n^3), O(m^2 n) and O(m^3) step on the GPU.
 //
 // The loop follows the reference's infeasible-start method, brisk_solve_body
 // (solver.c:14394-15188), step by step:
-//   Z^-1 from the factor of Z                               (solver.c:14397-14421)
+//   Z^-1 from the factor of Z, or the NT scaling W          (solver.c:14397-14421, 7898-7912)
 //   residuals, objectives, stopping and infeasibility tests (solver.c:14423-14612)
 //   the dual residual kept as theta R0, with a re-base      (solver.c:14317-14326, 14587-14607)
 //   Schur complement M, its factor                          (solver.c:14652-14672)
 //   rhs pieces a0 = A(Z^-1), h = A(Z^-1 theta R0 X)         (solver.c:14715-14735)
-//   predictor, step lengths, sigma, gamma                   (solver.c:14787-14873)
-//   corrector and the refinement of A(dX) = rp              (solver.c:14998-15105)
+//   predictor, step lengths, sigma, gamma                   (solver.c:14740-14873)
+//   corrector and the refinement of A(dX) = rp              (solver.c:14876-15105)
 //   step lengths, catastrophe guard, try_step, y update     (solver.c:15108-15188)
 // and the reference's problem scaling (problem_prepare, problem.c:1866-1910), starting point
 // (start_sdpt3, solver.c:6622-6661), Schur factor rules (schur_factor_, solver.c:5296-5421),
@@ -24,6 +24,7 @@
 #include "solver.h"
 #include "sparse.h"
 #include "lockstep.h"
+#include "nt.h"
 #include "tf32x3.h"
 
 #include <algorithm>
@@ -477,6 +478,9 @@ namespace {
 
 struct DevArrays {   // per block
     double *X, *Z, *Zi, *LX, *LZ, *LiX, *LiZ, *dX, *dZ, *F, *Fd, *R0, *G, *Q, *W, *T, *Xb, *Zb, *Bm;
+    // the NT direction (allocated for it only): the scaling G (W = G G' is kept in Zi), the
+    // scaled predictor directions and the scaled rhs (solver.c:7803-7810)
+    double *NG, *dXt, *dZt, *Rt;
     double *dinvX, *dinvZ;
     int *flags;
 };
@@ -485,6 +489,7 @@ static double *DevArrays::*const kCatMembers[] = {
     &DevArrays::X,  &DevArrays::Z,  &DevArrays::Zi, &DevArrays::LX, &DevArrays::LZ, &DevArrays::LiX, &DevArrays::LiZ,
     &DevArrays::dX, &DevArrays::dZ, &DevArrays::F,  &DevArrays::Fd, &DevArrays::R0, &DevArrays::G,   &DevArrays::Q,
     &DevArrays::W,  &DevArrays::T,  &DevArrays::Xb, &DevArrays::Zb, &DevArrays::Bm};
+static double *DevArrays::*const kNtMembers[] = {&DevArrays::NG, &DevArrays::dXt, &DevArrays::dZt, &DevArrays::Rt};
 
 // Device memory of one solve.  Stand-alone solves allocate with cudaMalloc and own a stream; the
 // batch workers hand in an arena (one allocation and one stream per worker, reused by every
@@ -603,6 +608,21 @@ class Solver {
     // C = alpha A B (column-major n x n) on every block: per-block DMMA GEMMs for the large
     // blocks, one batched launch for the small ones
     void mul_all(double alpha, double *DevArrays::*A, double *DevArrays::*B, double *DevArrays::*C);
+    // the NT direction (solver.c:7803-8090; -dir auto picks it by the rule of solver.c:13585-13591)
+    bool nt_mode = false;
+    double *nlam = nullptr;                  // the blocks' lam, block k's from loff[k]
+    std::vector<long long> loff;
+    long long *d_loff = nullptr;
+    int *d_ntflag = nullptr, *h_ntflag = nullptr, *d_ntinfo = nullptr, *h_ntinfo = nullptr;
+    double **d_lamtab = nullptr;             // the small blocks' lam pointers
+    int small_nmax = 1;
+    bool nt_scaling();                       // G, lam and W (in Zi) for every block; false: a block failed
+    void nt_toZ(double *DevArrays::*D, double *DevArrays::*out);     // out = sym(G' D G)
+    void nt_fromS(double *DevArrays::*D, double *DevArrays::*out);   // out = sym(G D G')
+    void mul_sym_all(double *DevArrays::*A, double *DevArrays::*B, double *DevArrays::*C);   // C = sym(A B)
+    // the matrices the assembly and the HKM-style products take as X and Z^-1: X and Z^-1, or W and
+    // W under NT (the reference's nt_view, solver.c:7813-7819)
+    double *DevArrays::*xmem() const { return nt_mode ? &DevArrays::Zi : &DevArrays::X; }
     int chunk = 32, chunk64 = 32, asm_prec = 0;
     int chunk_fp64(int) const { return chunk64; }
     int epoch = 0;
@@ -769,6 +789,8 @@ void Solver::upload_block(int k) {
 
     DevArrays &a = da[k];
     for (double *DevArrays::*mem : kCatMembers) a.*mem = cat.*mem + boff[k];
+    if (nt_mode)
+        for (double *DevArrays::*mem : kNtMembers) a.*mem = cat.*mem + boff[k];
     const int nblk64 = ceil_div(n, TRI_NB);
     a.dinvX = g.alloc<double>((size_t)nblk64 * TRI_NB * TRI_NB);
     a.dinvZ = g.alloc<double>((size_t)nblk64 * TRI_NB * TRI_NB);
@@ -798,11 +820,37 @@ void Solver::setup() {
     int nmax = 1;
     const double t1 = wtime();
     boff.assign(nb + 1, 0);
-    for (int k = 0; k < nb; k++) boff[k + 1] = boff[k] + (long long)P.blk[k].n * P.blk[k].n;
+    loff.assign(nb + 1, 0);
+    for (int k = 0; k < nb; k++) {
+        boff[k + 1] = boff[k] + (long long)P.blk[k].n * P.blk[k].n;
+        loff[k + 1] = loff[k] + P.blk[k].n;
+    }
     Ntot2 = boff[nb];
+    {   // the direction: -dir auto takes NT when its dense work (15 sum n^3) is below a quarter of the
+        // Schur work (m^3/3 + 5 sum n^3) or negligible (<= 1e8 flops), solver.c:13585-13591
+        double n3 = 0;
+        for (auto &B : P.blk) n3 += (double)B.n * B.n * B.n;
+        const double mm = m;
+        nt_mode = opt.direction == 1 ||
+                  (opt.direction < 0 && (15.0 * n3 < 0.25 * (mm * mm * mm / 3.0 + 5.0 * n3) || 15.0 * n3 <= 1e8));
+    }
     for (double *DevArrays::*mem : kCatMembers) {
         cat.*mem = g.alloc<double>(Ntot2);
         if (!(cat.*mem)) throw GpuFail{BGPU_ERR_NOMEM, __LINE__};
+    }
+    if (nt_mode) {
+        for (double *DevArrays::*mem : kNtMembers) {
+            cat.*mem = g.alloc<double>(Ntot2);
+            if (!(cat.*mem)) throw GpuFail{BGPU_ERR_NOMEM, __LINE__};
+        }
+        nlam = g.alloc<double>(loff[nb]);
+        d_loff = g.alloc<long long>(nb + 1);
+        d_ntflag = g.alloc<int>(1);
+        d_ntinfo = g.alloc<int>(1);
+        h_ntflag = g.host_alloc<int>(1);
+        h_ntinfo = g.host_alloc<int>(1);
+        if (!nlam || !d_loff || !d_ntflag || !d_ntinfo || !h_ntflag || !h_ntinfo) throw GpuFail{BGPU_ERR_NOMEM, __LINE__};
+        CU(cudaMemcpyAsync(d_loff, loff.data(), sizeof(long long) * (nb + 1), cudaMemcpyHostToDevice, g.st));
     }
     Ccat = g.alloc<double>(Ntot2);
     Icat = g.alloc<double>(Ntot2);
@@ -840,6 +888,14 @@ void Solver::setup() {
         d_slam = g.alloc<double>(ns);
         if (!d_sns || !d_sinfo || !d_slam) throw GpuFail{BGPU_ERR_NOMEM, __LINE__};
         CU(cudaMemcpyAsync(d_sns, nsz.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, g.st));
+        for (int i = 0; i < ns; i++) small_nmax = std::max(small_nmax, nsz[i]);
+        if (nt_mode) {
+            std::vector<double *> lp(ns);
+            for (int i = 0; i < ns; i++) lp[i] = nlam + loff[small_ids[i]];
+            d_lamtab = g.alloc<double *>(ns);
+            if (!d_lamtab) throw GpuFail{BGPU_ERR_NOMEM, __LINE__};
+            CU(cudaMemcpyAsync(d_lamtab, lp.data(), sizeof(double *) * ns, cudaMemcpyHostToDevice, g.st));
+        }
         CU(cudaStreamSynchronize(g.st));
         h_sinfo = g.host_alloc<int>(ns);
         h_slam = g.host_alloc<double>(ns);
@@ -1108,22 +1164,108 @@ void Solver::zinv(int k) {
     RC(symmetrize_f64(g.st, n, a.Zi, n));
 }
 
+// nt_scaling (solver.c:7898-7912) for every block: from the Cholesky factors of X and Z to G, lam
+// and W = G G' (kept in Zi, which the assembly and the products read as both X and Z^-1).  A block
+// whose singular values are not all positive, or whose Jacobi iteration does not converge, fails the
+// iteration (status 4, as nt_fail).
+bool Solver::nt_scaling() {
+    for (int k : big_ids) {
+        const int n = db[k].n;
+        DevArrays &d = da[k];
+        RC(nt::tril(g.st, n, d.LX, d.NG));   // rotated into L_X V
+        RC(nt::tril(g.st, n, d.LZ, d.Q));
+        gemm(1, 1, n, 1.0, d.Q, n, d.NG, n, 0.0, d.T);   // Mb = L_Z' L_X
+        int sweeps = 0;
+        RC(nt::jacobi(g.st, n, d.T, d.NG, d_ntflag, h_ntflag, &sweeps));
+        if (sweeps < 0) {
+            if (opt.verbose > 1) log_printf(0, "   NT scaling: block %d did not converge\n", k + 1);
+            return false;
+        }
+        CU(cudaMemsetAsync(d_ntinfo, 0, sizeof(int), g.st));
+        RC(nt::finish(g.st, n, d.T, d.NG, nlam + loff[k], d_ntinfo));
+        CU(cudaMemcpyAsync(h_ntinfo, d_ntinfo, sizeof(int), cudaMemcpyDeviceToHost, g.st));
+        gemm(0, 0, n, 1.0, d.NG, n, d.NG, n, 0.0, d.Zi);   // W = G G'
+        RC(symmetrize_f64(g.st, n, d.Zi, n));
+        CU(cudaStreamSynchronize(g.st));
+        if (*h_ntinfo) return false;
+    }
+    if (!small_ids.empty()) {
+        const int ns = (int)small_ids.size();
+        RC(nt::scaling_small(g.st, ns, d_sns, small_nmax, (const double *const *)tab(&DevArrays::LX),
+                             (const double *const *)tab(&DevArrays::LZ), tab(&DevArrays::NG), d_lamtab,
+                             tab(&DevArrays::Zi), d_sinfo));
+        CU(cudaMemcpyAsync(h_sinfo, d_sinfo, sizeof(int) * ns, cudaMemcpyDeviceToHost, g.st));
+        CU(cudaStreamSynchronize(g.st));
+        for (int i = 0; i < ns; i++)
+            if (h_sinfo[i]) return false;
+    }
+    return true;
+}
+
+// nt_toZ (solver.c:7990-8008): out = G' D G, symmetrized (T is the scratch)
+void Solver::nt_toZ(double *DevArrays::*D, double *DevArrays::*out) {
+    for (int k : big_ids) {
+        const int n = db[k].n;
+        DevArrays &d = da[k];
+        gemm(0, 1, n, 1.0, d.*D, n, d.NG, n, 0.0, d.T);       // D G
+        gemm(1, 1, n, 1.0, d.NG, n, d.T, n, 0.0, d.*out);     // G' (D G)
+        RC(symmetrize_f64(g.st, n, d.*out, n));
+    }
+    if (!small_ids.empty()) {
+        const int ns = (int)small_ids.size();
+        RC(small_gemm(g.st, ns, d_sns, 0, 0, 1.0, (const double *const *)tab(D), (const double *const *)tab(&DevArrays::NG),
+                      0.0, tab(&DevArrays::T), 0));
+        RC(small_gemm(g.st, ns, d_sns, 1, 0, 1.0, (const double *const *)tab(&DevArrays::NG),
+                      (const double *const *)tab(&DevArrays::T), 0.0, tab(out), 1));
+    }
+}
+
+// nt_fromS (solver.c:8051-8068): out = G D G', symmetrized (T is the scratch)
+void Solver::nt_fromS(double *DevArrays::*D, double *DevArrays::*out) {
+    for (int k : big_ids) {
+        const int n = db[k].n;
+        DevArrays &d = da[k];
+        gemm(0, 1, n, 1.0, d.NG, n, d.*D, n, 0.0, d.T);       // G D
+        gemm(0, 0, n, 1.0, d.T, n, d.NG, n, 0.0, d.*out);     // (G D) G'
+        RC(symmetrize_f64(g.st, n, d.*out, n));
+    }
+    if (!small_ids.empty()) {
+        const int ns = (int)small_ids.size();
+        RC(small_gemm(g.st, ns, d_sns, 0, 0, 1.0, (const double *const *)tab(&DevArrays::NG), (const double *const *)tab(D),
+                      0.0, tab(&DevArrays::T), 0));
+        RC(small_gemm(g.st, ns, d_sns, 0, 1, 1.0, (const double *const *)tab(&DevArrays::T),
+                      (const double *const *)tab(&DevArrays::NG), 0.0, tab(out), 1));
+    }
+}
+
+void Solver::mul_sym_all(double *DevArrays::*A, double *DevArrays::*B, double *DevArrays::*C) {
+    for (int k : big_ids) {
+        const int n = db[k].n;
+        mul(n, 1.0, da[k].*A, da[k].*B, da[k].*C);
+        RC(symmetrize_f64(g.st, n, da[k].*C, n));
+    }
+    if (!small_ids.empty())
+        RC(small_gemm(g.st, (int)small_ids.size(), d_sns, 0, 0, 1.0, (const double *const *)tab(A),
+                      (const double *const *)tab(B), 0.0, tab(C), 1));
+}
+
 // ---- Schur complement ----------------------------------------------------------------------
 void Solver::assemble(std::vector<double> &) {
     CU(cudaMemsetAsync(M, 0, sizeof(double) * (size_t)m * m, g.st));
     CU(cudaEventRecord(ev0, g.st));
     const int prec = (asm_prec == 1 && !asm_fp64) ? 1 : 0;
     m_exact = prec == 0;
-    assemble_small(cat.X, cat.Zi);
+    assemble_small(cat.*xmem(), cat.Zi);
     for (int k = 0; k < nb; k++) {
         if (in_sb[k]) {
             schur_flops += 2.0 * db[k].n * db[k].n * db[k].n * db[k].ncon;
             continue;
         }
+        const double *Xa = da[k].*xmem();
         if (dense_route[k])
-            RC(schur_assemble_dense(g.st, db[k], da[k].X, da[k].Zi, M, m, prec, prec ? chunk : chunk64, ws, ws_bytes));
+            RC(schur_assemble_dense(g.st, db[k], Xa, da[k].Zi, M, m, prec, prec ? chunk : chunk64, ws, ws_bytes));
         else
-            RC(schur_assemble(g.st, db[k], da[k].X, da[k].Zi, M, m, prec, prec ? chunk : chunk64, ws, ws_bytes));
+            RC(schur_assemble(g.st, db[k], Xa, da[k].Zi, M, m, prec, prec ? chunk : chunk64, ws, ws_bytes));
         const double n = db[k].n;
         const double ncon = db[k].ncon;
         schur_flops += 2.0 * n * n * n * ncon;   // the row-product GEMMs: 2 n^2 r_a with r_a <= n
@@ -1267,7 +1409,7 @@ void Solver::schur_mv(const std::vector<double> &x, std::vector<double> &y) {
 void Solver::newton_mv(const std::vector<double> &x, std::vector<double> &y) {
     atop_cat(x, 1.0, 0.0, cat.W);   // A'(x)
     mul_all(1.0, &DevArrays::Zi, &DevArrays::W, &DevArrays::T);
-    mul_all(1.0, &DevArrays::T, &DevArrays::X, &DevArrays::F);   // Z^-1 A'(x) X
+    mul_all(1.0, &DevArrays::T, xmem(), &DevArrays::F);   // Z^-1 A'(x) X (W A'(x) W under NT)
     aop_cat(cat.F, y);
 }
 
@@ -1741,10 +1883,14 @@ int Solver::run(ResultData &res) {
         log_printf(0, " it   pobj            dobj            pinf     dinf     gap      mu       alp   ald   sigma  time\n");
     for (it = 0; it <= opt.maxit; it++) {
         double td = wtime();
-        for (int k : big_ids) zinv(k);
-        if (!small_ids.empty())   // Zi = LiZ' LiZ (symmetric part), LiZ from the last small Cholesky of Z
-            RC(small_gemm(g.st, (int)small_ids.size(), d_sns, 1, 0, 1.0, (const double *const *)tab(&DevArrays::LiZ),
-                          (const double *const *)tab(&DevArrays::LiZ), 0.0, tab(&DevArrays::Zi), 1));
+        if (nt_mode) {
+            if (!nt_scaling()) { status = 4; break; }
+        } else {
+            for (int k : big_ids) zinv(k);
+            if (!small_ids.empty())   // Zi = LiZ' LiZ (symmetric part), LiZ from the last small Cholesky of Z
+                RC(small_gemm(g.st, (int)small_ids.size(), d_sns, 1, 0, 1.0, (const double *const *)tab(&DevArrays::LiZ),
+                              (const double *const *)tab(&DevArrays::LiZ), 0.0, tab(&DevArrays::Zi), 1));
+        }
         // residuals and objectives
         std::vector<double> AX;
         aop_cat(cat.X, AX);
@@ -1850,10 +1996,10 @@ int Solver::run(ResultData &res) {
         td = wtime();
         const bool hasH = theta > 0;
         {
-            aop_cat(cat.Zi, a0);
+            if (!nt_mode) aop_cat(cat.Zi, a0);
             if (hasH) {
                 mul_all(theta, &DevArrays::Zi, &DevArrays::R0, &DevArrays::T);   // theta Zi R0
-                mul_all(1.0, &DevArrays::T, &DevArrays::X, &DevArrays::G);       // theta Zi R0 X
+                mul_all(1.0, &DevArrays::T, xmem(), &DevArrays::G);              // theta Zi R0 X (W theta R0 W)
                 aop_cat(cat.G, h);
             } else h.assign(m, 0.0);
         }
@@ -1866,9 +2012,16 @@ int Solver::run(ResultData &res) {
         td = wtime();
         atop_cat(dy, -1.0, 0.0, cat.dZ);
         lincomb_cat(1.0, cat.dZ, theta, cat.R0, 0.0, nullptr, cat.dZ);   // dZ = -A'dy + theta R0
-        mul_all(1.0, &DevArrays::Zi, &DevArrays::dZ, &DevArrays::T);
-        mul_all(1.0, &DevArrays::T, &DevArrays::X, &DevArrays::G);        // Zi dZ X
-        sym_cat(cat.G, -1.0, -1.0, cat.X, 0.0, nullptr, cat.dX);          // dX = -sym(G) - X
+        if (nt_mode) {   // the scaled predictor (solver.c:14740-14792): dXt = Rt - G' dZ G, Rt = -diag(lam)
+            RC(nt::rhs_scaled(g.st, nb, d_bn, d_boff, d_loff, Ntot2, nlam, 0.0, nullptr, cat.Rt));
+            nt_toZ(&DevArrays::dZ, &DevArrays::dZt);
+            lincomb_cat(1.0, cat.Rt, -1.0, cat.dZt, 0.0, nullptr, cat.dXt);
+            nt_fromS(&DevArrays::dXt, &DevArrays::dX);                    // dX = G dXt G'
+        } else {
+            mul_all(1.0, &DevArrays::Zi, &DevArrays::dZ, &DevArrays::T);
+            mul_all(1.0, &DevArrays::T, &DevArrays::X, &DevArrays::G);    // Zi dZ X
+            sym_cat(cat.G, -1.0, -1.0, cat.X, 0.0, nullptr, cat.dX);      // dX = -sym(G) - X
+        }
         tm.dense += wtime() - td;
         double tst = wtime();
         const double ap = std::min(1.0, maxstep(1, opt.lanczos_k));
@@ -1902,10 +2055,21 @@ int Solver::run(ResultData &res) {
         // ---- corrector ----
         const double smu = sigma * mu;
         td = wtime();
-        mul_all(1.0, &DevArrays::Zi, &DevArrays::dZ, &DevArrays::T);
-        mul_all(1.0, &DevArrays::T, &DevArrays::dX, &DevArrays::Q);   // Q = Zi dZp dXp
-        aop_cat(cat.Q, qv);
-        for (int i = 0; i < m; i++) rhs[i] = P.b[i] - smu * a0[i] + qv[i] + h[i];
+        if (nt_mode) {
+            // the scaled corrector (solver.c:14876-14906, 14976-14996): Rt = L_lam^-1(smu I - lam^2 -
+            // sym(dXt dZt)), rhs = b + h - A(G (Rt + lam) G'), then dX = G (Rt - G' dZ G) G'
+            mul_sym_all(&DevArrays::dXt, &DevArrays::dZt, &DevArrays::W);
+            RC(nt::rhs_scaled(g.st, nb, d_bn, d_boff, d_loff, Ntot2, nlam, smu, cat.W, cat.Rt));
+            RC(nt::add_lam(g.st, nb, d_bn, d_boff, d_loff, Ntot2, nlam, 1.0, cat.Rt, cat.Q));
+            nt_fromS(&DevArrays::Q, &DevArrays::G);
+            aop_cat(cat.G, qv);
+            for (int i = 0; i < m; i++) rhs[i] = P.b[i] + h[i] - qv[i];
+        } else {
+            mul_all(1.0, &DevArrays::Zi, &DevArrays::dZ, &DevArrays::T);
+            mul_all(1.0, &DevArrays::T, &DevArrays::dX, &DevArrays::Q);   // Q = Zi dZp dXp
+            aop_cat(cat.Q, qv);
+            for (int i = 0; i < m; i++) rhs[i] = P.b[i] - smu * a0[i] + qv[i] + h[i];
+        }
         tm.dense += wtime() - td;
         tc = wtime();
         schur_solve(rhs, dy, 0);
@@ -1913,10 +2077,16 @@ int Solver::run(ResultData &res) {
         td = wtime();
         atop_cat(dy, -1.0, 0.0, cat.dZ);
         lincomb_cat(1.0, cat.dZ, theta, cat.R0, 0.0, nullptr, cat.dZ);
-        mul_all(1.0, &DevArrays::Zi, &DevArrays::dZ, &DevArrays::T);
-        mul_all(1.0, &DevArrays::T, &DevArrays::X, &DevArrays::G);
-        lincomb_cat(1.0, cat.G, 1.0, cat.Q, 0.0, nullptr, cat.G);          // Zi dZ X + Q
-        sym_cat(cat.G, -1.0, smu, cat.Zi, -1.0, cat.X, cat.dX);            // -sym(.) + smu Zi - X
+        if (nt_mode) {
+            nt_toZ(&DevArrays::dZ, &DevArrays::Q);
+            lincomb_cat(1.0, cat.Rt, -1.0, cat.Q, 0.0, nullptr, cat.W);
+            nt_fromS(&DevArrays::W, &DevArrays::dX);
+        } else {
+            mul_all(1.0, &DevArrays::Zi, &DevArrays::dZ, &DevArrays::T);
+            mul_all(1.0, &DevArrays::T, &DevArrays::X, &DevArrays::G);
+            lincomb_cat(1.0, cat.G, 1.0, cat.Q, 0.0, nullptr, cat.G);          // Zi dZ X + Q
+            sym_cat(cat.G, -1.0, smu, cat.Zi, -1.0, cat.X, cat.dX);            // -sym(.) + smu Zi - X
+        }
         tm.dense += wtime() - td;
         // ---- refinement of A(dX) = rp ----
         for (int pass = 0; pass < 3; pass++) {
@@ -1933,7 +2103,7 @@ int Solver::run(ResultData &res) {
             td = wtime();
             atop_cat(wv, 1.0, 0.0, cat.W);                                       // A'w
             mul_all(1.0, &DevArrays::Zi, &DevArrays::W, &DevArrays::T);
-            mul_all(1.0, &DevArrays::T, &DevArrays::X, &DevArrays::F);           // Zi A'w X  (F is free here)
+            mul_all(1.0, &DevArrays::T, xmem(), &DevArrays::F);                  // Zi A'w X (W A'w W), F is free here
             sym_cat(cat.F, 1.0, 0.0, nullptr, 0.0, nullptr, cat.G);
             std::vector<double> AG;
             aop_cat(cat.G, AG);
@@ -1982,6 +2152,7 @@ int Solver::run(ResultData &res) {
         stall = (apn < 1e-6 && adn < 1e-6) ? stall + 1 : 0;
     }
     res.iters = it;
+    res.direction = nt_mode ? 1 : 0;
     // fall back to the best iterate seen
     if (status != 0 && status != 1 && status != 2 && best_score < res_score(R)) {
         R = best;
@@ -2052,6 +2223,8 @@ static int solve_impl(const InputData &in, const Options &opt, ResultData &res, 
         res.time = wtime() - t0;
         if (opt.verbose > 0) {
             log_printf(0, "status: %s   iterations: %d\n", status_string(res.status), res.iters);
+            log_printf(0, "  Solve:             interior-point method: infeasible start, %s direction, %d iterations\n",
+                       res.direction == 1 ? "NT" : "HKM", res.iters);
             log_printf(0, "  primal obj <C,X> = %.10e   dual obj b'y = %.10e\n", res.pobj, res.dobj);
             log_printf(0, "  DIMACS errors: %.1e %.1e %.1e %.1e %.1e %.1e\n", res.err[1], res.err[2], res.err[3],
                        res.err[4], res.err[5], res.err[6]);
@@ -2100,6 +2273,9 @@ struct BatchSession {
 BatchSession *batch_session_create(int count, const std::function<bool(int, InputData &)> &get,
                                    const std::function<bool(int, InputView &)> &view, const Options &opt, int &rc) {
     rc = 0;
+    // the lockstep loop takes the HKM direction; -dir auto picks NT for every block of order <= 64
+    // (15 n^3 <= 1e8), so those batches run the concurrent form
+    if (opt.direction != 0) return nullptr;
     const double t0 = wtime();
     std::vector<HProblem> Ps(count);
     std::vector<int> bad(count, 0);

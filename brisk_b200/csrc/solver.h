@@ -55,6 +55,7 @@ struct Options {
     int init = 1;               // 0: SDPT3 start (start_sdpt3); 1: least-squares start (solver.c:13939-14198)
     int batch_mode = -1;        // bgpu_batch_solve: -1/1 lockstep when every problem has one block of order
                                 // <= 64 (else concurrent), 0 concurrent per-problem solves
+    int direction = -1;         // -1 auto (solver.c:13585-13591), 0 HKM, 1 NT
     int route = -1;             // Schur route per block: -1 auto (dense when the constraints average >= 2 % of
                                 // n^2 entries, problem.c:1299), 0 row-product, 1 dense
 };
@@ -68,6 +69,7 @@ struct ResultData {
                                 // 4 numerical difficulties, 5 reduced accuracy, 6 time limit
     int exit_code = 0;
     int iters = 0;
+    int direction = 0;          // the search direction taken: 0 HKM, 1 NT
     int have_x = 0;
     int m = 0, nblk = 0;
     std::vector<int> bs;

@@ -63,6 +63,8 @@ def lib():
         "bgpu_small_chol_inv": ([I, P, P, P, P, P, P], I),
         "bgpu_small_lammin": ([I, P, P, P, P, P], I),
         "bgpu_small_gemm": ([I, P, I, I, D, P, P, D, P, I, P], I),
+        "bgpu_nt_ws_bytes": ([I], SZ),
+        "bgpu_nt_scaling": ([I, P, P, P, P, P, P, SZ, P, P], I),
     }
     for name, (args, res) in sigs.items():
         f = getattr(L, name)
@@ -86,6 +88,24 @@ def ws_bytes(n, chunk, precision):
 
 def chunk_default(n, precision):
     return int(lib().bgpu_schur_chunk_default(n, precision))
+
+
+def nt_scaling(LX, LZ):
+    """The NT scaling of one block from the Cholesky factors of X and Z (CUDA float64 tensors, n x n,
+    lower triangles read as column-major, i.e. the tensors hold the transposes row-major):
+    returns (G, lam, W, sweeps) with G, W column-major in row-major tensors (transpose to read)."""
+    import torch
+    n = LX.shape[0]
+    dev = LX.device
+    G = torch.empty((n, n), dtype=torch.float64, device=dev)
+    W = torch.empty((n, n), dtype=torch.float64, device=dev)
+    lam = torch.empty(n, dtype=torch.float64, device=dev)
+    nws = int(lib().bgpu_nt_ws_bytes(n))
+    ws = torch.empty(max(nws, 8), dtype=torch.uint8, device=dev)
+    sw = ctypes.c_int(0)
+    call("nt_scaling", n, LX.data_ptr(), LZ.data_ptr(), G.data_ptr(), lam.data_ptr(), W.data_ptr(), ws.data_ptr(),
+         nws, ctypes.byref(sw), None)
+    return G, lam, W, sw.value
 
 
 class SparseCholesky:

@@ -198,6 +198,18 @@ BGPU_API int bgpu_small_lammin(int nb, const int *d_n, const double *const *d_Li
 BGPU_API int bgpu_small_gemm(int nb, const int *d_n, int ta, int tb, double alpha, const double *const *d_A,
                              const double *const *d_B, double beta, double *const *d_C, int sym, void *stream);
 
+/* The NT scaling of one SDP block (nt_scaling, solver.c:7898-7912; nt_prep/nt_eig/nt_post,
+ * solver.c:7824-7896): from the Cholesky factors L_X, L_Z of X and Z (lower triangles, n x n
+ * column-major; the strict upper triangles are ignored) to G (n x n), lam (n) and W = G G'
+ * (n x n), with G' Z G = G^-1 X G^-T = diag(lam) and W Z W = X.  V (G = L_X V diag(lam)^-1/2)
+ * comes from one-sided Jacobi on L_Z' L_X: one CTA for n <= 64, block Jacobi above (d_ws of
+ * bgpu_nt_ws_bytes(n) bytes).  Returns BGPU_OK, BGPU_ERR_NOTPD when a singular value is not
+ * positive (nt_post's failure), BGPU_ERR_TIMEOUT when Jacobi did not converge in 40 sweeps;
+ * *sweeps (may be null): the sweeps of the block form, 0 for n <= 64.  Synchronizes the stream. */
+BGPU_API size_t bgpu_nt_ws_bytes(int n);
+BGPU_API int bgpu_nt_scaling(int n, const double *d_LX, const double *d_LZ, double *d_G, double *d_lam,
+                             double *d_W, void *d_ws, size_t ws_bytes, int *sweeps, void *stream);
+
 /* y = alpha M x + beta y for a full symmetric M (schur_mv_, solver.c:4815). */
 BGPU_API int bgpu_symv(int n, double alpha, const double *d_M, int ldm, const double *d_x, double beta,
                        double *d_y, void *stream);

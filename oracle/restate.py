@@ -15,6 +15,9 @@ It restates, on dense matrices (small sizes: tests), the reference BRISK 1.7 alg
   refinement of A(dX) = rp 15058-15105, try_step 6393-6447)
 * maxstep                the largest alpha with V + alpha dV >= 0     solver.c:6300-6390
   (exact eigenvalues here; the reference's Lanczos estimate theta - residual is <= it)
+* nt_scaling             the NT scaling G, lam, W = G G' from the     solver.c:7824-7912
+                         factors of X and Z (eigenvectors of Mb' Mb,
+                         Mb = L_Z' L_X; lam descending)
 * DIMACS errors on the data as given                                  postsolve.c:2880-2897
 * the final status rule                                               main.c:2349-2362
 
@@ -127,6 +130,23 @@ def maxstep(Ls, dVs):
         ak = 1e30 if lam >= 0 else -1.0 / lam
         a = min(a, ak)
     return a
+
+
+def nt_scaling(LX, LZ):
+    """nt_scaling (solver.c:7824-7912) on dense factors: Mb = L_Z' L_X, the eigenvectors V of
+    H = Mb' Mb with lam = sqrt of its eigenvalues in descending order (dsyevd's ascending order
+    reversed, solver.c:7853-7858), G = L_X V diag(lam)^-1/2 and W = G G' (solver.c:7886-7893).
+    Returns (G, lam, W), or None where an eigenvalue is not positive (the reference then tries
+    dgesdd; the oracle does not)."""
+    LX, LZ = np.tril(LX), np.tril(LZ)
+    Mb = LZ.T @ LX
+    w, Q = np.linalg.eigh(Mb.T @ Mb)
+    if not w[0] > 0:
+        return None
+    lam = np.sqrt(w[::-1])
+    V = Q[:, ::-1]
+    G = (LX @ V) / np.sqrt(lam)[None, :]
+    return G, lam, G @ G.T
 
 
 def try_step(Vs, dVs, alpha):

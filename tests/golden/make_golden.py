@@ -6,7 +6,11 @@ files written by brisk_b200.problems, with the reference's presolves off so that
 problem as given, and records per run: status, iterations, objectives, the six DIMACS errors,
 the iteration table of -v (pobj, dobj, pinf, dinf, gap, mu per iteration) and the time.
 
-usage: python tests/golden/make_golden.py [--big] [names]   (--big adds rand400 and mom700)
+Runs per instance: "init0" and "default" (HKM direction, SDPT3 and least-squares start) and "nt"
+(NT direction, least-squares start).
+
+usage: python tests/golden/make_golden.py [--big] [--runs r1,r2] [names]
+       (--big adds rand400 and mom700; --runs recomputes only those runs, keeping the others)
 """
 from __future__ import annotations
 
@@ -44,6 +48,10 @@ for _q in list(range(12)) + [3339]:
 BIG = {"rand400": (random_sdp, dict(n=400, m=2000, density=0.01, seed=0)),
        "mom700": (moment_relaxation, dict(nvars=700, clique=4, seed=0))}
 
+HKM = ["-nohsd", "-dir", "hkm", "-mixed", "0", "-tol", "1e-7"] + AS_GIVEN
+RUNS = {"init0": HKM + ["-init", "0"], "default": HKM,
+        "nt": ["-nohsd", "-dir", "nt", "-mixed", "0", "-tol", "1e-7"] + AS_GIVEN}
+
 ROW = re.compile(r"^\s*(\d+)\s+([+-]\S+)\s+([+-]\S+)\s+(\S+)\s+(\S+)\s+(\S+)\s+(\S+)\s+(\S+)\s+(\S+)\s+(\S+)\s+(\S+)\s*$")
 
 
@@ -79,7 +87,13 @@ def main():
     if os.path.exists(OUT):
         with open(OUT) as f:
             res = json.load(f)
-    only = [a for a in sys.argv[1:] if not a.startswith("--")]
+    args = sys.argv[1:]
+    wanted = []
+    if "--runs" in args:
+        i = args.index("--runs")
+        wanted = args[i + 1].split(",")
+        del args[i:i + 2]
+    only = [a for a in args if not a.startswith("--")]
     with tempfile.TemporaryDirectory() as td:
         for name, (fn, kw) in inst.items():
             if only and name not in only:
@@ -87,13 +101,15 @@ def main():
             d = fn(**kw)
             path = os.path.join(td, name + ".dat-s")
             write_sdpa(d, path)
-            entry = dict(generator=fn.__name__, kwargs=kw, m=d.m, n=int(d.bs[0]), nblk=d.nblk, runs={})
-            base = ["-nohsd", "-dir", "hkm", "-mixed", "0", "-tol", "1e-7"] + AS_GIVEN
-            entry["runs"]["init0"] = run(path, base + ["-init", "0"])
-            entry["runs"]["default"] = run(path, base)
+            old = res.get(name, {}).get("runs", {})
+            entry = dict(generator=fn.__name__, kwargs=kw, m=d.m, n=int(d.bs[0]), nblk=d.nblk, runs=dict(old))
+            for rname, opts in RUNS.items():
+                if rname in old and wanted and rname not in wanted:
+                    continue
+                entry["runs"][rname] = run(path, opts)
+                r = entry["runs"][rname]
+                print(name, rname, d.m, r["status"], r["iterations"], r["pobj"], r["dobj"], flush=True)
             res[name] = entry
-            r = entry["runs"]["init0"]
-            print(name, d.m, r["status"], r["iterations"], r["pobj"], r["dobj"], flush=True)
     with open(OUT, "w") as f:
         json.dump(res, f, indent=1)
 
