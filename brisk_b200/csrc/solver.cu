@@ -1884,6 +1884,8 @@ int Solver::run(ResultData &res) {
     for (it = 0; it <= opt.maxit; it++) {
         double td = wtime();
         if (nt_mode) {
+            // L_Z^-1 for the dual step length (zinv keeps it under HKM), then the scaling
+            for (int k : big_ids) inv_from_chol(db[k].n, da[k].LZ, da[k].dinvZ, da[k].LiZ);
             if (!nt_scaling()) { status = 4; break; }
         } else {
             for (int k : big_ids) zinv(k);
