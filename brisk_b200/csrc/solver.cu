@@ -616,6 +616,7 @@ class Solver {
     int *d_ntflag = nullptr, *h_ntflag = nullptr, *d_ntinfo = nullptr, *h_ntinfo = nullptr;
     double **d_lamtab = nullptr;             // the small blocks' lam pointers
     int small_nmax = 1;
+    int nt_sweeps = 0;                       // the most Jacobi sweeps of a large block this iteration
     bool nt_scaling();                       // G, lam and W (in Zi) for every block; false: a block failed
     void nt_toZ(double *DevArrays::*D, double *DevArrays::*out);     // out = sym(G' D G)
     void nt_fromS(double *DevArrays::*D, double *DevArrays::*out);   // out = sym(G D G')
@@ -1169,6 +1170,7 @@ void Solver::zinv(int k) {
 // whose singular values are not all positive, or whose Jacobi iteration does not converge, fails the
 // iteration (status 4, as nt_fail).
 bool Solver::nt_scaling() {
+    nt_sweeps = 0;
     for (int k : big_ids) {
         const int n = db[k].n;
         DevArrays &d = da[k];
@@ -1177,6 +1179,7 @@ bool Solver::nt_scaling() {
         gemm(1, 1, n, 1.0, d.Q, n, d.NG, n, 0.0, d.T);   // Mb = L_Z' L_X
         int sweeps = 0;
         RC(nt::jacobi(g.st, n, d.T, d.NG, d_ntflag, h_ntflag, &sweeps));
+        nt_sweeps = std::max(nt_sweeps, sweeps);
         if (sweeps < 0) {
             if (opt.verbose > 1) log_printf(0, "   NT scaling: block %d did not converge\n", k + 1);
             return false;
@@ -2147,8 +2150,9 @@ int Solver::run(ResultData &res) {
         for (int i = 0; i < m; i++) y[i] += adn * dy[i];
         theta *= (1.0 - adn);
         if (opt.verbose > 1)
-            log_printf(0, "     [schur %.3fs %s, factor %s reg %.0e pmin %.1e, pcg %d, step %.3fs]\n", tm.schur - ts_before,
-                       m_exact ? "fp64" : "tf32x3", is_float ? "fp32" : "fp64", reg, min_pivot, pcg_iters, tm.step - tstep_before);
+            log_printf(0, "     [schur %.3fs %s, factor %s reg %.0e pmin %.1e, pcg %d, step %.3fs%s]\n", tm.schur - ts_before,
+                       m_exact ? "fp64" : "tf32x3", is_float ? "fp32" : "fp64", reg, min_pivot, pcg_iters, tm.step - tstep_before,
+                       nt_mode && !big_ids.empty() ? (", NT sweeps " + std::to_string(nt_sweeps)).c_str() : "");
         alp = apn;
         ald = adn;
         stall = (apn < 1e-6 && adn < 1e-6) ? stall + 1 : 0;

@@ -90,7 +90,7 @@ def chunk_default(n, precision):
     return int(lib().bgpu_schur_chunk_default(n, precision))
 
 
-def nt_scaling(LX, LZ):
+def nt_scaling(LX, LZ, stream=None):
     """The NT scaling of one block from the Cholesky factors of X and Z (CUDA float64 tensors, n x n,
     lower triangles read as column-major, i.e. the tensors hold the transposes row-major):
     returns (G, lam, W, sweeps) with G, W column-major in row-major tensors (transpose to read)."""
@@ -104,7 +104,7 @@ def nt_scaling(LX, LZ):
     ws = torch.empty(max(nws, 8), dtype=torch.uint8, device=dev)
     sw = ctypes.c_int(0)
     call("nt_scaling", n, LX.data_ptr(), LZ.data_ptr(), G.data_ptr(), lam.data_ptr(), W.data_ptr(), ws.data_ptr(),
-         nws, ctypes.byref(sw), None)
+         nws, ctypes.byref(sw), stream)
     return G, lam, W, sw.value
 
 

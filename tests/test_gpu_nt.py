@@ -72,6 +72,23 @@ def test_nt_scaling_on_the_central_path(cuda, n):
     assert np.linalg.norm(W - X / np.sqrt(mu)) <= 1e-7 * np.linalg.norm(X / np.sqrt(mu))
 
 
+def test_nt_scaling_graph_replay_matches_direct_launches(cuda):
+    """On a created stream each sweep is a cached CUDA graph; on the default stream the rounds are
+    launched one by one: the same bits either way, and on a second (cached) replay."""
+    rng = np.random.default_rng(77)
+    n = 300
+    X, Z = spd(rng, n, 1e-4, 1.0), spd(rng, n, 1e-4, 1.0)
+    LX, LZ = colmajor(np.linalg.cholesky(X), cuda), colmajor(np.linalg.cholesky(Z), cuda)
+    G0, lam0, W0, s0 = step.nt_scaling(LX, LZ)
+    torch.cuda.synchronize()
+    st = torch.cuda.Stream()
+    for _ in range(2):
+        G1, lam1, W1, s1 = step.nt_scaling(LX, LZ, st.cuda_stream)
+        torch.cuda.synchronize()
+        assert s1 == s0
+        assert torch.equal(G0, G1) and torch.equal(lam0, lam1) and torch.equal(W0, W1)
+
+
 def test_nt_scaling_rejects_bad_arguments(cuda):
     z = torch.zeros((4, 4), dtype=torch.float64, device=cuda)
     rc = step.lib().bgpu_nt_scaling(0, z.data_ptr(), z.data_ptr(), z.data_ptr(), z.data_ptr(), z.data_ptr(),
