@@ -1996,6 +1996,13 @@ int Solver::run(ResultData &res) {
             frc = factor();
         }
         if (frc != 0) { status = 4; tm.chol += wtime() - tc; break; }
+        if (!m_exact && !opt.mixed_shift && min_pivot < 1e-4) {
+            // the FP32-accurate M is near the end of its use: its smallest scaled pivot falls by
+            // 10-20x an iteration, and the factor of the next one would need a shift (rand1000: pivot
+            // 7.9e-5, then a shift) — the next iterations assemble in FP64 directly
+            asm_fp64 = true;
+            if (opt.verbose > 1) log_printf(0, "   mixed path: smallest pivot %.1e: FP64 assembly from the next iteration\n", min_pivot);
+        }
         tm.chol += wtime() - tc;
         // ---- rhs pieces ----
         td = wtime();
