@@ -74,6 +74,29 @@ BGPU_API int bgpu_nt_scaling(int n, const double *d_LX, const double *d_LZ, doub
     return info ? BGPU_ERR_NOTPD : BGPU_OK;
 }
 
+BGPU_API size_t bgpu_ozaki_ws_bytes(int M, int N, int K) {
+    if (M <= 0 || N <= 0 || K <= 0) return 0;
+    return ozaki_operand_bytes(M, K) + ozaki_operand_bytes(N, K);
+}
+
+BGPU_API int bgpu_gemm_ozaki(int M, int N, int K, const double *d_A, int64_t lda, const double *d_B, int64_t ldb,
+                             double *d_C, int64_t ldc, void *d_ws, size_t ws_bytes, void *stream) {
+    if (M <= 0 || N <= 0 || K <= 0 || lda < K || ldb < K || ldc < M || !d_A || !d_B || !d_C || !d_ws ||
+        ws_bytes < bgpu_ozaki_ws_bytes(M, N, K))
+        return BGPU_ERR_ARG;
+    cudaStream_t st = S(stream);
+    OzakiOperand a, b;
+    uint8_t *wa = (uint8_t *)d_ws, *wb = wa + ozaki_operand_bytes(M, K);
+    int rc = ozaki_slice(st, M, K, d_A, lda, wa, &a);
+    if (!rc) rc = ozaki_slice(st, N, K, d_B, ldb, wb, &b);
+    if (!rc) rc = ozaki_gemm(st, a, b, d_C, ldc);
+    if (rc) return rc;
+    BGPU_CHECK(cudaStreamSynchronize(st));
+    int bad = 0;
+    if ((rc = ozaki_error_flag(&bad))) return rc;
+    return bad ? BGPU_ERR_TIMEOUT : BGPU_OK;
+}
+
 BGPU_API int bgpu_schur_colptr(int n, int ncon, const long long *d_cptr, const int *d_cpos, int *d_ccol, void *stream) {
     DevBlock B;
     B.n = n;
@@ -88,7 +111,7 @@ BGPU_API int bgpu_schur_assemble(int n, int m, int ncon, const int *d_con, const
                                  const int *d_ccol, const int *d_cpos, const double *d_cval, const double *d_X,
                                  const double *d_Zi, double *d_M, int precision, int chunk, void *d_ws,
                                  size_t ws_bytes, void *stream) {
-    if (n <= 0 || m <= 0 || ncon < 0 || (precision != 0 && precision != 1)) return BGPU_ERR_ARG;
+    if (n <= 0 || m <= 0 || ncon < 0 || precision < 0 || precision > 2) return BGPU_ERR_ARG;
     if (chunk <= 0) chunk = schur_chunk_default(n, precision);
     DevBlock B;
     B.n = n;
@@ -129,7 +152,7 @@ BGPU_API int bgpu_schur_assemble_sym(int n, int m, int ncon, const int *d_con, c
                                      const long long *d_uptr, const int *d_upos, const double *d_uval,
                                      const double *d_X, const double *d_Zi, double *d_M, int precision, int chunk,
                                      void *d_ws, size_t ws_bytes, void *stream) {
-    if (n <= 0 || m <= 0 || ncon < 0 || (precision != 0 && precision != 1)) return BGPU_ERR_ARG;
+    if (n <= 0 || m <= 0 || ncon < 0 || precision < 0 || precision > 2) return BGPU_ERR_ARG;
     if (ncon > 0 && (!d_uptr || !d_upos || !d_uval)) return BGPU_ERR_ARG;
     if (chunk <= 0) chunk = schur_chunk_default(n, precision);
     DevBlock B;

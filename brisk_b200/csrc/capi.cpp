@@ -112,11 +112,18 @@ int parse_options(int argc, const char *const *argv, Options &opt, std::string &
             const char *s = need("-1, 0 or 1");
             if (!s || !parse_int(s, opt.mixed)) { if (err.empty()) err = "bad -mixed"; return 1; }
         } else if (a == "-asmprec") {   // this build: the Schur assembly's precision
-            const char *s = need("fp64 or tf32x3");
+            const char *s = need("fp64, tf32x3 or ozaki");
             if (!s) return 1;
             if (!strcmp(s, "fp64")) opt.asm_prec = 0;
             else if (!strcmp(s, "tf32x3")) opt.asm_prec = 1;
-            else { err = "bad -asmprec (fp64 or tf32x3)"; return 1; }
+            else if (!strcmp(s, "ozaki")) opt.asm_prec = 2;
+            else { err = "bad -asmprec (fp64, tf32x3 or ozaki)"; return 1; }
+        } else if (a == "-asmlate") {   // this build: the 3xTF32 path's late assembly
+            const char *s = need("fp64 or ozaki");
+            if (!s) return 1;
+            if (!strcmp(s, "fp64")) opt.late_prec = 0;
+            else if (!strcmp(s, "ozaki")) opt.late_prec = 2;
+            else { err = "bad -asmlate (fp64 or ozaki)"; return 1; }
         } else if (a == "-muswitch") {
             const char *s = need("a number");
             if (!s || !parse_double(s, opt.mu_switch)) { if (err.empty()) err = "bad -muswitch"; return 1; }

@@ -23,6 +23,23 @@ int gemm_grouped_tile_rows();   // 128 (the tile is 128 x 64)
 int scale_matrix_f64(cudaStream_t st, int M, int N, double beta, double *C, long long ldc, long long sC, int batch,
                      int lower);
 
+// ---- FP64-accurate GEMM on the INT8 tensor cores (ozaki.cu) ---------------------------------
+// An operand cut into ozaki_slices() int8 slices (stacked, srows rows each, row stride ldk bytes)
+// with one power-of-two exponent per row.
+struct OzakiOperand {
+    long long rows = 0, srows = 0, ldk = 0;
+    int K = 0;
+    int8_t *q = nullptr;
+    int *e = nullptr;
+};
+int ozaki_slices();
+size_t ozaki_operand_bytes(long long rows, int K);
+// slices of the rows x K operand src (row r at src + r lds) into buf (ozaki_operand_bytes)
+int ozaki_slice(cudaStream_t st, long long rows, int K, const double *src, long long lds, void *buf, OzakiOperand *op);
+// C(i, j) = sum_k A(i, k) B(j, k), C column-major (ldc)
+int ozaki_gemm(cudaStream_t st, const OzakiOperand &A, const OzakiOperand &B, double *C, long long ldc);
+int ozaki_error_flag(int *host_value);
+
 // ---- dense factor / solves (dense.cu) -----------------------------------------------------
 constexpr int TRI_NB = 64;   // diagonal block order of the blocked factor and solves
 
@@ -137,6 +154,7 @@ int schur_upper(cudaStream_t st, const DevBlock &B);
 int schur_assemble_gram(cudaStream_t st, const DevBlock &B, double *M, int m, void *ws, size_t ws_bytes);
 int schur_chunk_default(int n, int precision);
 // M (m x m, column-major, full symmetric) += the block's contribution sum over its constraints
-// of M_ab = <A_b, X A_a Zi>.  precision 0: FP64 (DMMA), 1: 3xTF32 (tcgen05).
+// of M_ab = <A_b, X A_a Zi>.  precision 0: FP64 (DMMA), 1: 3xTF32 (tcgen05), 2: FP64-accurate
+// products on the INT8 tensor cores (ozaki.cu).
 int schur_assemble(cudaStream_t st, const DevBlock &B, const double *X, const double *Zi, double *M, int m,
                    int precision, int chunk, void *ws, size_t ws_bytes);

@@ -1,0 +1,280 @@
+// FP64-accurate GEMM on the INT8 tensor cores (tcgen05 kind::i8, sm_100a): the Ozaki scheme of
+// exact splitting into integer slices (Ozaki, Ogita, Oishi, Rump 2012; its integer form, Ootomo,
+// Ozaki, Yokota 2024), for the Schur assembly's G = T X where FP32 accuracy no longer suffices.
+//
+// C(i, j) = sum_k A(i, k) B(j, k), A and B row-major with K contiguous (A(i, k) = A[i lda + k],
+// B(j, k) = B[j ldb + k]), C column-major.
+//
+// Slicing (slice_kernel): each row r of A (of B) gets the exponent e_r with max_k |A(r, k)| < 2^e_r;
+// a = A(r, k) 2^-e_r lies in (-1, 1) and is cut exactly into S signed 7-bit digits:
+//   a = sum_{p=1..S} s_p 2^(-7p) + rest,  s_p = trunc(128 (rest of the previous digits)) in [-127, 127]
+// (multiplications by powers of two and subtractions of integers: no rounding).
+//
+// Products (ozaki_kernel): A B' = 2^(e_i + f_j) sum_{p,q} 2^(-7(p+q)) (S_p^A S_q^B') with the pairs
+// p + q <= S + 1 kept.  With S = 8 the dropped pairs (p + q >= 10: at most 127^2 2^-70 each) and the
+// slices' truncation (below 2^-56) leave an error below about 2^-53 K 2^(e_i + f_j): FP64-like
+// relative to the largest entries of row i of A and of row j of B.  Each product of int8 slices
+// accumulates exactly in int32 (|sum| <= S 127^2 K < 2^31 for K <= 16000), and
+// all pairs of one diagonal d = p + q share one TMEM accumulator: S accumulators of BN columns side
+// by side in the 512 TMEM columns for the whole K loop.  The epilogue drains them once, smallest
+// diagonal terms first, into FP64: C = 2^(e_i + f_j) sum_d 2^(-7d) ACC_d.
+//
+// One CTA per 128 x 64 tile, as tf32x3.cu: warp 0 / lane 0 the TMA producer (the S slices of A and
+// of B for a 64-byte k-block, 64-byte swizzle, a 2-deep ring), warp 1 / lane 0 the MMA issuer
+// (kind::i8, M = 128, N = 64, K = 32 per instruction), all 4 warps the epilogue.  Every mbarrier
+// wait is bounded; a wait that runs out sets *err and the CTA winds down.  No cluster, no multicast.
+#include "common.cuh"
+#include "kernels.h"
+#include "tcgen05.cuh"
+
+namespace {
+using namespace tc;
+constexpr int OZ_S = 8;                  // slices per operand (56 bits)
+constexpr int BM = 128, BN = 64, BK = 64, STAGES = 2, NTHREADS = 128;
+constexpr int A_TILE = BM * BK, B_TILE = BN * BK;            // bytes of one slice's tile
+constexpr int STAGE = OZ_S * (A_TILE + B_TILE);              // 96 KB
+constexpr int TMEM_COLS = 512;                               // OZ_S accumulators of BN columns
+constexpr size_t SMEM = (size_t)STAGES * STAGE + 1024 /*align*/ + 256 /*barriers*/;
+static_assert(OZ_S * BN <= TMEM_COLS, "accumulators must fit in TMEM");
+
+// tcgen05 shared-memory matrix descriptor: K-major, 64-byte swizzle, 8-row groups 512 B apart
+__device__ __forceinline__ uint64_t smem_desc64(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr & 0x3FFFFu) >> 4);        // start address
+    d |= (uint64_t)(16u >> 4) << 16;                  // leading byte offset (unused with this swizzle)
+    d |= (uint64_t)(512u >> 4) << 32;                 // stride byte offset: 8 rows x 64 B
+    d |= (uint64_t)1 << 46;                           // descriptor version
+    d |= (uint64_t)4 << 61;                           // swizzle: 64 B
+    return d;
+}
+// instruction descriptor: D s32, A and B signed 8-bit, both K-major, N and M
+__host__ __device__ constexpr uint32_t idesc_i8(int M, int N) {
+    return (2u << 4)                       // D format s32
+           | (1u << 7) | (1u << 10)        // A, B format s8
+           | ((uint32_t)(N >> 3) << 17)    // N / 8
+           | ((uint32_t)(M >> 4) << 24);   // M / 16
+}
+__device__ __forceinline__ void umma_i8(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n}\n"
+        ::"r"(tmem_d), "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+
+__global__ void __launch_bounds__(NTHREADS, 1)
+    ozaki_kernel(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorMap tB, long long a_slice_rows,
+                 long long b_slice_rows, const int *__restrict__ ea, const int *__restrict__ eb, double *C, long long ldc,
+                 int M, int N, int K, int *err) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint64_t *full = (uint64_t *)(smem + STAGES * STAGE);
+    uint64_t *empty = full + STAGES;
+    uint64_t *done = empty + STAGES;
+    uint32_t *tslot = (uint32_t *)(done + 1);
+    int *bad = (int *)(tslot + 1);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+    const int nkb = (K + BK - 1) / BK;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(done, 1);
+        *bad = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                     "r"(TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+
+    if (warp == 0 && lane == 0) {
+        // ---- TMA producer: the S slices of A (rows m0..) and of B (rows n0..) of a k-block ----
+        int issued = 0;
+        for (int kb = 0; kb < nkb; kb++) {
+            const int s = kb % STAGES, use = kb / STAGES;
+            if (use > 0 && !mbar_wait(&empty[s], (use - 1) & 1)) { atomicExch(bad, 1); break; }
+            uint8_t *st = smem + s * STAGE;
+            mbar_expect_tx(&full[s], STAGE);
+            const int x = kb * BK;
+            for (int p = 0; p < OZ_S; p++) {
+                tma_load_2d(st + p * A_TILE, &tA, &full[s], x, (int)(p * a_slice_rows + m0));
+                tma_load_2d(st + OZ_S * A_TILE + p * B_TILE, &tB, &full[s], x, (int)(p * b_slice_rows + n0));
+            }
+            issued++;
+        }
+        for (int kb = (issued > STAGES ? issued - STAGES : 0); kb < issued; kb++)
+            mbar_wait(&full[kb % STAGES], (kb / STAGES) & 1);
+    } else if (warp == 1 && lane == 0) {
+        // ---- MMA issuer: every slice pair p + q <= S + 1 into the accumulator of its diagonal ----
+        constexpr uint32_t idesc = idesc_i8(BM, BN);
+        for (int kb = 0; kb < nkb; kb++) {
+            const int s = kb % STAGES;
+            if (!mbar_wait(&full[s], (kb / STAGES) & 1)) { atomicExch(bad, 1); break; }
+            tc_fence_after();
+            const uint32_t base = smem_u32(smem + s * STAGE);
+#pragma unroll
+            for (int ks = 0; ks < BK / 32; ks++) {   // K-step of 32 int8 = 32 bytes inside the swizzle atom
+                const uint32_t off = ks * 32;
+#pragma unroll
+                for (int d = 0; d < OZ_S; d++) {       // diagonal p + q = d + 2 (0-based slices: p + q = d)
+#pragma unroll
+                    for (int p = 0; p <= d; p++) {
+                        const int q = d - p;
+                        const uint64_t a = smem_desc64(base + p * A_TILE + off);
+                        const uint64_t b = smem_desc64(base + OZ_S * A_TILE + q * B_TILE + off);
+                        umma_i8(tmem + (uint32_t)(d * BN), a, b, idesc, (kb | ks | p) != 0);
+                    }
+                }
+            }
+            umma_commit(&empty[s]);
+        }
+        umma_commit(done);
+    }
+    __syncwarp();
+    // ---- epilogue: the S accumulators -> FP64, smallest terms first, scaled by 2^(e_i + f_j) ----
+    const bool ok = mbar_wait(done, 0);
+    tc_fence_after();
+    const bool good = __all_sync(0xffffffffu, ok && !*(volatile int *)bad);
+    if (good) {
+        const int row = m0 + warp * 32 + lane;
+        double acc[BN];
+#pragma unroll
+        for (int c = 0; c < BN; c++) acc[c] = 0.0;
+#pragma unroll 1
+        for (int d = OZ_S - 1; d >= 0; d--) {
+            const double w = ldexp(1.0, -7 * (d + 2));
+#pragma unroll
+            for (int c0 = 0; c0 < BN; c0 += 16) {
+                uint32_t r[16];
+                tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(d * BN + c0), r);
+#pragma unroll
+                for (int j = 0; j < 16; j++) acc[c0 + j] += w * (double)(int)r[j];
+            }
+        }
+        if (row < M) {
+            const int e = ea[row];
+#pragma unroll
+            for (int c = 0; c < BN; c++) {
+                const int col = n0 + c;
+                if (col < N) C[(long long)row + (long long)col * ldc] = ldexp(acc[c], e + eb[col]);
+            }
+        }
+    } else if (threadIdx.x == 0) {
+        atomicExch(err, 1);
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+    }
+}
+
+// One warp per row: the row's exponent and its S digits (row stride ldk bytes, slice p at
+// dst + p * slice_bytes; the K..ldk padding is zero).
+__global__ void slice_kernel(int rows, int K, const double *__restrict__ src, long long lds, int8_t *dst, long long ldk,
+                             long long slice_bytes, int *exps) {
+    const int r = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    if (r >= rows) return;
+    const double *x = src + (long long)r * lds;
+    double mx = 0.0;
+    for (int k = lane; k < K; k += 32) mx = fmax(mx, fabs(x[k]));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    const int e = mx > 0.0 ? ilogb(mx) + 1 : 0;   // max |x| 2^-e < 1
+    if (lane == 0) exps[r] = e;
+    int8_t *out = dst + (long long)r * ldk;
+    for (long long k = lane; k < ldk; k += 32) {
+        double a = k < K ? ldexp(x[k], -e) : 0.0;
+#pragma unroll
+        for (int p = 0; p < OZ_S; p++) {
+            a *= 128.0;
+            const double t = trunc(a);
+            a -= t;
+            out[p * slice_bytes + k] = (int8_t)(int)t;
+        }
+    }
+}
+
+// the slices of rows x K bytes each, stacked (slice p at rows p * slice_rows), row stride ldk
+// bytes, box 64 (K) x box_rows, 64-byte swizzle
+int make_map_i8(CUtensorMap *map, const int8_t *ptr, long long total_rows, long long K, long long ldk, int box_rows) {
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) return BGPU_ERR_CUDA;
+    if (((uintptr_t)ptr & 15) || (ldk & 15)) return BGPU_ERR_ARG;   // TMA: 16-byte base and stride
+    cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)total_rows};
+    cuuint64_t strides[1] = {(cuuint64_t)ldk};
+    cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, (void *)ptr, dims, strides, box, estr,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? BGPU_OK : BGPU_ERR_ARG;
+}
+
+__device__ int g_ozaki_err = 0;   // sticky flag of the bounded waits (zero at module load)
+
+inline long long round_up(long long x, long long a) { return (x + a - 1) / a * a; }
+}  // namespace
+
+int ozaki_slices() { return OZ_S; }
+
+// bytes of the slices (and exponents) of a rows x K operand
+size_t ozaki_operand_bytes(long long rows, int K) {
+    const long long ldk = round_up(K, 64), srows = round_up(rows, 128);
+    return (size_t)OZ_S * srows * ldk + sizeof(int) * srows + 1024;
+}
+
+// The operand's slices into buf (ozaki_operand_bytes): returns the slice layout in *sl.
+int ozaki_slice(cudaStream_t st, long long rows, int K, const double *src, long long lds, void *buf, OzakiOperand *op) {
+    const long long ldk = round_up(K, 64), srows = round_up(rows, 128);
+    op->rows = rows;
+    op->srows = srows;
+    op->K = K;
+    op->ldk = ldk;
+    op->q = (int8_t *)(((uintptr_t)buf + 255) & ~(uintptr_t)255);
+    op->e = (int *)(op->q + (size_t)OZ_S * srows * ldk);
+    if (rows <= 0) return BGPU_OK;
+    if ((rows + 7) / 8 > (1LL << 31) - 1) return BGPU_ERR_TOOBIG;
+    slice_kernel<<<ceil_div(rows * 32, 256), 256, 0, st>>>((int)rows, K, src, lds, op->q, ldk, srows * ldk, op->e);
+    BGPU_LAUNCH_CHECK();
+    return BGPU_OK;
+}
+
+// C (column-major, ldc) = A B' from the sliced operands (A: M rows, B: N rows, both K)
+int ozaki_gemm(cudaStream_t st, const OzakiOperand &A, const OzakiOperand &B, double *C, long long ldc) {
+    const int M = (int)A.rows, N = (int)B.rows, K = A.K;
+    if (M <= 0 || N <= 0 || K <= 0) return BGPU_OK;
+    if (B.K != K || K > 16000 || OZ_S * A.srows > (1LL << 31) - 1 || OZ_S * B.srows > (1LL << 31) - 1)
+        return BGPU_ERR_ARG;
+    CUtensorMap mA, mB;
+    int rc;
+    if ((rc = make_map_i8(&mA, A.q, OZ_S * A.srows, K, A.ldk, BM)) || (rc = make_map_i8(&mB, B.q, OZ_S * B.srows, K, B.ldk, BN)))
+        return rc;
+    static bool attr = false;
+    if (!attr) {
+        BGPU_CHECK(cudaFuncSetAttribute(ozaki_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM));
+        attr = true;
+    }
+    void *d = nullptr;
+    BGPU_CHECK(cudaGetSymbolAddress(&d, g_ozaki_err));
+    if (ceil_div(M, BM) > 65535) return BGPU_ERR_TOOBIG;
+    dim3 grid(ceil_div(N, BN), ceil_div(M, BM));
+    ozaki_kernel<<<grid, NTHREADS, SMEM, st>>>(mA, mB, A.srows, B.srows, A.e, B.e, C, ldc, M, N, K, (int *)d);
+    BGPU_LAUNCH_CHECK();
+    return BGPU_OK;
+}
+
+int ozaki_error_flag(int *host_value) {
+    void *d = nullptr;
+    BGPU_CHECK(cudaGetSymbolAddress(&d, g_ozaki_err));
+    BGPU_CHECK(cudaMemcpy(host_value, d, sizeof(int), cudaMemcpyDeviceToHost));
+    return BGPU_OK;
+}

@@ -532,6 +532,8 @@ int schur_chunk_default(int n, int precision) {
 size_t schur_ws_bytes(int n, int chunk, int precision) {
     const size_t nn = (size_t)n * n * chunk;
     if (precision == 0) return 2 * nn * sizeof(double);            // T, G
+    if (precision == 2)                                            // T, G, the slices of T and of X
+        return 2 * nn * sizeof(double) + ozaki_operand_bytes((long long)n * chunk, n) + ozaki_operand_bytes(n, n);
     const size_t ld = tf32_ld(n);
     // T hi/lo (n K rows of ld), G (float, n K x n), X hi/lo (n rows of ld), plus 256 B alignment slack each
     return (2 * (size_t)n * chunk * ld + nn + 2 * (size_t)n * ld) * sizeof(float) + 5 * 256;
@@ -546,12 +548,23 @@ int schur_assemble(cudaStream_t st, const DevBlock &B, const double *X, const do
     if (ws_bytes < schur_ws_bytes(n, K, precision)) return BGPU_ERR_ARG;
     const size_t nnK = (size_t)n * n * K;
     dim3 tgrid(ceil_div(n, TP_Q), ceil_div(n, TP_K), K);
-    if (precision == 0) {
+    if (precision == 0 || precision == 2) {
         double *T = (double *)ws, *G = T + nnK;
+        // FP64-accurate products on the INT8 tensor cores: X's slices once, T's per chunk
+        uint8_t *sa = (uint8_t *)(G + nnK), *sb = sa + ozaki_operand_bytes((long long)n * K, n);
+        OzakiOperand opA, opB;
+        if (precision == 2)
+            if (int rc = ozaki_slice(st, n, n, X, n, sb, &opB)) return rc;
         for (int a0 = 0; a0 < B.ncon; a0 += K) {
             tprod_kernel<double><<<tgrid, 256, 0, st>>>(n, n, K, a0, B.ncon, B.cptr, B.ccol, B.cpos, B.cval, Zi, T, nullptr);
             BGPU_LAUNCH_CHECK();
-            int rc = gemm_f64(st, 1, 1, n * K, n, n, 1.0, T, n, 0, X, n, 0, 0.0, G, (long long)n * K, 0, 1, 0);
+            int rc;
+            if (precision == 2) {
+                if ((rc = ozaki_slice(st, (long long)n * K, n, T, n, sa, &opA))) return rc;
+                rc = ozaki_gemm(st, opA, opB, G, (long long)n * K);
+            } else {
+                rc = gemm_f64(st, 1, 1, n * K, n, n, 1.0, T, n, 0, X, n, 0, 0.0, G, (long long)n * K, 0, 1, 0);
+            }
             if (rc) return rc;
             if (B.upos) {   // T is free again: it takes the packed symmetric sum
                 if ((rc = sym_pack_launch<double>(st, K, n, G, T))) return rc;

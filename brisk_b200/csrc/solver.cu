@@ -624,7 +624,7 @@ class Solver {
     // the matrices the assembly and the HKM-style products take as X and Z^-1: X and Z^-1, or W and
     // W under NT (the reference's nt_view, solver.c:7813-7819)
     double *DevArrays::*xmem() const { return nt_mode ? &DevArrays::Zi : &DevArrays::X; }
-    int chunk = 32, chunk64 = 32, asm_prec = 0;
+    int chunk = 32, chunk64 = 32, chunk_oz = 32, asm_prec = 0;
     int chunk_fp64(int) const { return chunk64; }
     int epoch = 0;
     // factor state (Schur in solver.c:4511-4568)
@@ -938,7 +938,10 @@ void Solver::setup() {
     }
     chunk = opt.chunk > 0 ? opt.chunk : schur_chunk_default(nmax, asm_prec);
     chunk64 = opt.chunk > 0 ? opt.chunk : schur_chunk_default(nmax, 0);
+    chunk_oz = opt.chunk > 0 ? opt.chunk : schur_chunk_default(nmax, 2);
     ws_bytes = std::max(schur_ws_bytes(nmax, chunk, asm_prec), schur_ws_bytes(nmax, chunk64, 0));
+    if (asm_prec == 2 || (asm_prec == 1 && opt.late_prec == 2))
+        ws_bytes = std::max(ws_bytes, schur_ws_bytes(nmax, chunk_oz, 2));
     for (int k = 0; k < nb; k++)
         if (dense_route[k])
             ws_bytes = std::max(ws_bytes, std::max(schur_dense_ws_bytes(db[k].n, db[k].ncon, chunk, asm_prec),
@@ -1256,8 +1259,10 @@ void Solver::mul_sym_all(double *DevArrays::*A, double *DevArrays::*B, double *D
 void Solver::assemble(std::vector<double> &) {
     CU(cudaMemsetAsync(M, 0, sizeof(double) * (size_t)m * m, g.st));
     CU(cudaEventRecord(ev0, g.st));
-    const int prec = (asm_prec == 1 && !asm_fp64) ? 1 : 0;
-    m_exact = prec == 0;
+    // 3xTF32 until the mixed path turns to its late precision (FP64 or the Ozaki slices)
+    const int prec = asm_prec == 1 ? (asm_fp64 ? opt.late_prec : 1) : asm_prec;
+    m_exact = prec != 1;
+    const int kchunk = prec == 1 ? chunk : prec == 2 ? chunk_oz : chunk64;
     assemble_small(cat.*xmem(), cat.Zi);
     for (int k = 0; k < nb; k++) {
         if (in_sb[k]) {
@@ -1265,10 +1270,11 @@ void Solver::assemble(std::vector<double> &) {
             continue;
         }
         const double *Xa = da[k].*xmem();
-        if (dense_route[k])
-            RC(schur_assemble_dense(g.st, db[k], Xa, da[k].Zi, M, m, prec, prec ? chunk : chunk64, ws, ws_bytes));
+        if (dense_route[k])   // (the dense route has no Ozaki form: FP64 there)
+            RC(schur_assemble_dense(g.st, db[k], Xa, da[k].Zi, M, m, prec == 2 ? 0 : prec, prec == 1 ? chunk : chunk64,
+                                    ws, ws_bytes));
         else
-            RC(schur_assemble(g.st, db[k], Xa, da[k].Zi, M, m, prec, prec ? chunk : chunk64, ws, ws_bytes));
+            RC(schur_assemble(g.st, db[k], Xa, da[k].Zi, M, m, prec, kchunk, ws, ws_bytes));
         const double n = db[k].n;
         const double ncon = db[k].ncon;
         schur_flops += 2.0 * n * n * n * ncon;   // the row-product GEMMs: 2 n^2 r_a with r_a <= n
@@ -1278,9 +1284,9 @@ void Solver::assemble(std::vector<double> &) {
     float ms = 0;
     CU(cudaEventElapsedTime(&ms, ev0, ev1));
     schur_dev_time += ms * 1e-3;
-    if (prec == 1) {
+    if (prec == 1 || prec == 2) {
         int bad = 0;
-        RC(tf32x3_error_flag(&bad));
+        RC(prec == 1 ? tf32x3_error_flag(&bad) : ozaki_error_flag(&bad));
         if (bad) throw GpuFail{BGPU_ERR_TIMEOUT, __LINE__};
     }
 }

@@ -39,7 +39,10 @@ struct Options {
     double balance = 0.0;
     int sigma_rule = -1;
     int mixed = -1;             // FP32 Schur factor: -1 auto (m >= 1000), 0 never, 1 always
-    int asm_prec = -1;          // Schur assembly: -1 auto (FP64), 0 FP64, 1 3xTF32
+    int asm_prec = -1;          // Schur assembly: -1 auto (FP64), 0 FP64, 1 3xTF32, 2 FP64-accurate on the
+                                // INT8 tensor cores (Ozaki slices)
+    int late_prec = 2;          // 3xTF32 path: the assembly once the FP32-accurate M no longer serves (0 FP64,
+                                // 2 Ozaki slices)
     double mu_switch = 1e-4;    // 3xTF32 path: the factor goes to FP64 once scaled mu < mu_switch
     int mixed_shift = 0;        // 3xTF32 path: 1 keeps a shifted factor of M as the PCG preconditioner (slower
                                 // on rand1000: 170 PCG steps per solve); 0 re-assembles in FP64

@@ -64,6 +64,8 @@ def lib():
         "bgpu_small_lammin": ([I, P, P, P, P, P], I),
         "bgpu_small_gemm": ([I, P, I, I, D, P, P, D, P, I, P], I),
         "bgpu_nt_ws_bytes": ([I], SZ),
+        "bgpu_ozaki_ws_bytes": ([I, I, I], SZ),
+        "bgpu_gemm_ozaki": ([I, I, I, P, I64, P, I64, P, I64, P, SZ, P], I),
         "bgpu_nt_scaling": ([I, P, P, P, P, P, P, SZ, P, P], I),
     }
     for name, (args, res) in sigs.items():

@@ -199,6 +199,18 @@ BGPU_API int bgpu_small_lammin(int nb, const int *d_n, const double *const *d_Li
 BGPU_API int bgpu_small_gemm(int nb, const int *d_n, int ta, int tb, double alpha, const double *const *d_A,
                              const double *const *d_B, double beta, double *const *d_C, int sym, void *stream);
 
+/* C = A B' (C(i, j) = sum_k A[i lda + k] B[j ldb + k], C column-major) with FP64-accurate
+ * products on the INT8 tensor cores (tcgen05 kind::i8): each row of A and of B is cut exactly
+ * into 8 signed 7-bit slices under a power-of-two exponent, the slice products with p + q <= 9
+ * accumulate exactly in int32 and are summed in FP64 (the Ozaki scheme; K <= 16000).  The error
+ * is below about 2^-53 K max_k |A(i, k)| max_k |B(j, k)|.  d_ws: bgpu_ozaki_ws_bytes(M, N, K) bytes.
+ * Returns BGPU_ERR_TIMEOUT when a bounded wait of the kernel ran out; synchronizes the stream.
+ * Replaces the pdgemm of the Schur assembly's row products (solver.c:2571-2590) where FP32
+ * accuracy no longer suffices. */
+BGPU_API size_t bgpu_ozaki_ws_bytes(int M, int N, int K);
+BGPU_API int bgpu_gemm_ozaki(int M, int N, int K, const double *d_A, int64_t lda, const double *d_B, int64_t ldb,
+                             double *d_C, int64_t ldc, void *d_ws, size_t ws_bytes, void *stream);
+
 /* The NT scaling of one SDP block (nt_scaling, solver.c:7898-7912; nt_prep/nt_eig/nt_post,
  * solver.c:7824-7896): from the Cholesky factors L_X, L_Z of X and Z (lower triangles, n x n
  * column-major; the strict upper triangles are ignored) to G (n x n), lam (n) and W = G G'
