@@ -695,7 +695,8 @@ class Solver {
         else newton_mv(x, y);
     }
     bool m_exact = true;      // M was assembled in FP64 (the residual may use it)
-    bool asm_fp64 = false;    // the mixed path fell back to FP64 assembly
+    bool asm_fp64 = false;    // the mixed path turned to its late (FP64-accurate) assembly
+    const char *asm_label = "fp64";   // the last assembly's precision (the -vv log)
     double schur_solve(const std::vector<double> &rhs, std::vector<double> &x, double tol_rel);
     // step length
     double maxstep(int primal, int K);
@@ -1263,6 +1264,7 @@ void Solver::assemble(std::vector<double> &) {
     const int prec = asm_prec == 1 ? (asm_fp64 ? opt.late_prec : 1) : asm_prec;
     m_exact = prec != 1;
     const int kchunk = prec == 1 ? chunk : prec == 2 ? chunk_oz : chunk64;
+    asm_label = prec == 1 ? "tf32x3" : prec == 2 ? "ozaki" : "fp64";
     assemble_small(cat.*xmem(), cat.Zi);
     for (int k = 0; k < nb; k++) {
         if (in_sb[k]) {
@@ -1485,7 +1487,7 @@ double Solver::schur_solve(const std::vector<double> &rhs, std::vector<double> &
     // factor of the FP32-accurate M, the following iterations assemble M in FP64
     if (!m_exact && (best > tol || rel > std::max(1e-9, 10 * tol_rel)) && !asm_fp64) {
         asm_fp64 = true;
-        if (opt.verbose > 1) log_printf(0, "   mixed path: PCG missed %.1e (rel %.1e): FP64 assembly from here on\n", tol / nb_, rel);
+        if (opt.verbose > 1) log_printf(0, "   mixed path: PCG missed %.1e (rel %.1e): FP64-accurate assembly from here on\n", tol / nb_, rel);
     }
     return rel;
 }
@@ -1993,7 +1995,7 @@ int Solver::run(ResultData &res) {
             asm_fp64 = true;
             reg_hint = false;
             reg_ok = 0;
-            if (opt.verbose > 1) log_printf(0, "   mixed path: the FP32-accurate M needed a shift: FP64 assembly from here on\n");
+            if (opt.verbose > 1) log_printf(0, "   mixed path: the FP32-accurate M needed a shift: FP64-accurate assembly from here on\n");
             tm.chol += wtime() - tc;
             ts = wtime();
             assemble(tmpv);
@@ -2007,7 +2009,7 @@ int Solver::run(ResultData &res) {
             // 10-20x an iteration, and the factor of the next one would need a shift (rand1000: pivot
             // 7.9e-5, then a shift) — the next iterations assemble in FP64 directly
             asm_fp64 = true;
-            if (opt.verbose > 1) log_printf(0, "   mixed path: smallest pivot %.1e: FP64 assembly from the next iteration\n", min_pivot);
+            if (opt.verbose > 1) log_printf(0, "   mixed path: smallest pivot %.1e: FP64-accurate assembly from the next iteration\n", min_pivot);
         }
         tm.chol += wtime() - tc;
         // ---- rhs pieces ----
@@ -2164,7 +2166,7 @@ int Solver::run(ResultData &res) {
         theta *= (1.0 - adn);
         if (opt.verbose > 1)
             log_printf(0, "     [schur %.3fs %s, factor %s reg %.0e pmin %.1e, pcg %d, step %.3fs%s]\n", tm.schur - ts_before,
-                       m_exact ? "fp64" : "tf32x3", is_float ? "fp32" : "fp64", reg, min_pivot, pcg_iters, tm.step - tstep_before,
+                       asm_label, is_float ? "fp32" : "fp64", reg, min_pivot, pcg_iters, tm.step - tstep_before,
                        nt_mode && !big_ids.empty() ? (", NT sweeps " + std::to_string(nt_sweeps)).c_str() : "");
         alp = apn;
         ald = adn;
