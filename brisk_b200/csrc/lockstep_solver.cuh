@@ -57,6 +57,15 @@ class Lockstep {
     std::vector<int> pcg_iters, nfactor;
     double schur_flops = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // the NT direction (every instance's block has order <= 64, so -dir auto takes NT): the scaling
+    // G in NG, W = G G' in Zi, lam per instance from loff[k]
+    bool nt = false;
+    double *nlam = nullptr;
+    long long *d_loff = nullptr;
+    double **d_lamtab = nullptr;
+    int *d_ntinfo = nullptr, *h_ntinfo = nullptr;
+    void nt_toZ(double *DevArrays::*D, double *DevArrays::*out);     // out = sym(G' D G)
+    void nt_fromS(double *DevArrays::*D, double *DevArrays::*out);   // out = sym(G D G')
 
   public:
     // wall time of the phases (s): start, assembly, factor, PCG, the rest of the loop, final measures
@@ -125,6 +134,23 @@ void Lockstep::setup() {
     d_poff = g.alloc<long long>(B + 1);
     need(d_n); need(d_m); need(d_boff); need(d_coff); need(d_moff); need(d_poff);
     for (double *DevArrays::*mem : kCatMembers) { cat.*mem = g.alloc<double>(Ntot2); need(cat.*mem); }
+    nt = opt.direction != 0;   // auto: 15 n^3 <= 1e8 for every n <= 64 (solver.c:13585-13591)
+    if (nt) {
+        for (double *DevArrays::*mem : kNtMembers) { cat.*mem = g.alloc<double>(Ntot2); need(cat.*mem); }
+        std::vector<long long> loff(B + 1, 0);
+        for (int k = 0; k < B; k++) loff[k + 1] = loff[k] + n[k];
+        nlam = g.alloc<double>(loff[B]);
+        d_loff = g.alloc<long long>(B + 1);
+        d_lamtab = g.alloc<double *>(B);
+        d_ntinfo = g.alloc<int>(B);
+        h_ntinfo = g.host_alloc<int>(B);
+        need(nlam); need(d_loff); need(d_lamtab); need(d_ntinfo); need(h_ntinfo);
+        std::vector<double *> lp(B);
+        for (int k = 0; k < B; k++) lp[k] = nlam + loff[k];
+        CU(cudaMemcpyAsync(d_loff, loff.data(), sizeof(long long) * (B + 1), cudaMemcpyHostToDevice, g.st));
+        CU(cudaMemcpyAsync(d_lamtab, lp.data(), sizeof(double *) * B, cudaMemcpyHostToDevice, g.st));
+        CU(cudaStreamSynchronize(g.st));
+    }
     Ccat = g.alloc<double>(Ntot2);
     Icat = g.alloc<double>(Ntot2);
     Pp = g.alloc<double>(PT);
@@ -255,6 +281,20 @@ void Lockstep::upload_list(const std::vector<int> &L) {
 void Lockstep::set_coef(int i, const std::vector<double> &v) {
     CU(cudaMemcpyAsync(d_coef[i], v.data(), sizeof(double) * B, cudaMemcpyHostToDevice, g.st));
     CU(cudaStreamSynchronize(g.st));   // v is pageable host memory the caller may change next
+}
+
+// nt_toZ / nt_fromS (solver.c:7990-8008, 8051-8068) for every instance (T is the scratch)
+void Lockstep::nt_toZ(double *DevArrays::*D, double *DevArrays::*out) {
+    RC(small_gemm(g.st, B, d_n, 0, 0, 1.0, (const double *const *)tab(D), (const double *const *)tab(&DevArrays::NG),
+                  0.0, tab(&DevArrays::T), 0));
+    RC(small_gemm(g.st, B, d_n, 1, 0, 1.0, (const double *const *)tab(&DevArrays::NG),
+                  (const double *const *)tab(&DevArrays::T), 0.0, tab(out), 1));
+}
+void Lockstep::nt_fromS(double *DevArrays::*D, double *DevArrays::*out) {
+    RC(small_gemm(g.st, B, d_n, 0, 0, 1.0, (const double *const *)tab(&DevArrays::NG), (const double *const *)tab(D),
+                  0.0, tab(&DevArrays::T), 0));
+    RC(small_gemm(g.st, B, d_n, 0, 1, 1.0, (const double *const *)tab(&DevArrays::T),
+                  (const double *const *)tab(&DevArrays::NG), 0.0, tab(out), 1));
 }
 
 void Lockstep::mul(double *DevArrays::*A, double *DevArrays::*Bm, double *DevArrays::*C) {
@@ -738,9 +778,24 @@ void Lockstep::run(std::vector<ResultData> &res) {
         for (int k = 0; k < B; k++)
             if (status[k] < 0) act.push_back(k);
         if (act.empty()) break;
-        // Zi = LiZ' LiZ
-        RC(small_gemm(g.st, B, d_n, 1, 0, 1.0, (const double *const *)tab(&DevArrays::LiZ),
-                      (const double *const *)tab(&DevArrays::LiZ), 0.0, tab(&DevArrays::Zi), 1));
+        if (nt) {   // the NT scaling (solver.c:7898-7912): G, lam and W = G G' (in Zi); a failure ends the instance
+            RC(nt::scaling_small(g.st, B, d_n, nmax, (const double *const *)tab(&DevArrays::LX),
+                                 (const double *const *)tab(&DevArrays::LZ), tab(&DevArrays::NG), d_lamtab,
+                                 tab(&DevArrays::Zi), d_ntinfo));
+            CU(cudaMemcpyAsync(h_ntinfo, d_ntinfo, sizeof(int) * B, cudaMemcpyDeviceToHost, g.st));
+            CU(cudaStreamSynchronize(g.st));
+            std::vector<int> keep;
+            for (int k : act) {
+                if (h_ntinfo[k]) status[k] = 4;
+                else keep.push_back(k);
+            }
+            act.swap(keep);
+            if (act.empty()) break;
+        } else {   // Zi = LiZ' LiZ
+            RC(small_gemm(g.st, B, d_n, 1, 0, 1.0, (const double *const *)tab(&DevArrays::LiZ),
+                          (const double *const *)tab(&DevArrays::LiZ), 0.0, tab(&DevArrays::Zi), 1));
+        }
+        double *DevArrays::*Xw = nt ? &DevArrays::Zi : &DevArrays::X;   // X, or W under NT (nt_view)
         // residuals and objectives
         std::vector<double> AX;
         aop(cat.X, AX);
@@ -832,7 +887,7 @@ void Lockstep::run(std::vector<ResultData> &res) {
             if (status[k] < 0) act.push_back(k);
         if (act.empty()) break;
         // ---- Schur complement and its factor ----
-        assemble(act, cat.X, cat.Zi);
+        assemble(act, cat.*Xw, cat.Zi);
         std::vector<int> failed;
         factor(act, failed);
         for (int k : failed) status[k] = 4;
@@ -844,12 +899,12 @@ void Lockstep::run(std::vector<ResultData> &res) {
         }
         std::vector<double> dmask(B, 0.0);   // 1 on the active instances
         for (int k : act) dmask[k] = 1.0;
-        // ---- rhs pieces: a0 = A(Zi), h = A(theta Zi R0 X) ----
-        aop(cat.Zi, a0);
+        // ---- rhs pieces: a0 = A(Zi) (HKM), h = A(theta Zi R0 X) (W theta R0 W under NT) ----
+        if (!nt) aop(cat.Zi, a0);
         mul(&DevArrays::Zi, &DevArrays::R0, &DevArrays::T);
         set_coef(1, theta);
         RC(ew_lincomb_coef(g.st, B, d_boff, Ntot2, d_coef[1], cat.T, nullptr, nullptr, nullptr, nullptr, cat.T));
-        mul(&DevArrays::T, &DevArrays::X, &DevArrays::G);
+        mul(&DevArrays::T, Xw, &DevArrays::G);
         aop(cat.G, h);
         // ---- predictor ----
         for (int k : act)
@@ -859,9 +914,16 @@ void Lockstep::run(std::vector<ResultData> &res) {
         set_coef(0, ones);
         set_coef(1, theta);
         RC(ew_lincomb_coef(g.st, B, d_boff, Ntot2, d_coef[0], cat.dZ, d_coef[1], cat.R0, nullptr, nullptr, cat.dZ));
-        mul(&DevArrays::Zi, &DevArrays::dZ, &DevArrays::T);
-        mul(&DevArrays::T, &DevArrays::X, &DevArrays::G);
-        RC(ew_sym_lincomb_blocks(g.st, B, d_n, d_boff, Ntot2, cat.G, -1.0, -1.0, cat.X, 0.0, nullptr, cat.dX));
+        if (nt) {   // scaled: dXt = Rt - G' dZ G with Rt = -diag(lam), dX = G dXt G' (solver.c:14740-14792)
+            RC(nt::rhs_scaled(g.st, B, d_n, d_boff, d_loff, Ntot2, nlam, 0.0, nullptr, cat.Rt));
+            nt_toZ(&DevArrays::dZ, &DevArrays::dZt);
+            RC(ew_lincomb(g.st, Ntot2, 1.0, cat.Rt, -1.0, cat.dZt, 0.0, nullptr, cat.dXt));
+            nt_fromS(&DevArrays::dXt, &DevArrays::dX);
+        } else {
+            mul(&DevArrays::Zi, &DevArrays::dZ, &DevArrays::T);
+            mul(&DevArrays::T, &DevArrays::X, &DevArrays::G);
+            RC(ew_sym_lincomb_blocks(g.st, B, d_n, d_boff, Ntot2, cat.G, -1.0, -1.0, cat.X, 0.0, nullptr, cat.dX));
+        }
         std::vector<double> ap, ad;
         maxstep(1, ap);
         maxstep(0, ad);
@@ -896,23 +958,42 @@ void Lockstep::run(std::vector<ResultData> &res) {
             smu[k] = sg * mu[k];
         }
         // ---- corrector ----
-        mul(&DevArrays::Zi, &DevArrays::dZ, &DevArrays::T);
-        mul(&DevArrays::T, &DevArrays::dX, &DevArrays::Q);   // Q = Zi dZp dXp
-        aop(cat.Q, qv);
-        for (int k : act)
-            for (int i = 0; i < m[k]; i++) {
-                const long long c = coff[k] + i;
-                rhs[c] = Pb[k].b[i] - smu[k] * a0[c] + qv[c] + h[c];
-            }
+        if (nt) {   // Rt = L_lam^-1(smu I - lam^2 - sym(dXt dZt)), rhs = b + h - A(G (Rt + lam) G') (solver.c:14876-14906)
+            RC(small_gemm(g.st, B, d_n, 0, 0, 1.0, (const double *const *)tab(&DevArrays::dXt),
+                          (const double *const *)tab(&DevArrays::dZt), 0.0, tab(&DevArrays::W), 1));
+            set_coef(3, smu);
+            RC(nt::rhs_scaled(g.st, B, d_n, d_boff, d_loff, Ntot2, nlam, 0.0, cat.W, cat.Rt, d_coef[3]));
+            RC(nt::add_lam(g.st, B, d_n, d_boff, d_loff, Ntot2, nlam, 1.0, cat.Rt, cat.Q));
+            nt_fromS(&DevArrays::Q, &DevArrays::G);
+            aop(cat.G, qv);
+            for (int k : act)
+                for (int i = 0; i < m[k]; i++) {
+                    const long long c = coff[k] + i;
+                    rhs[c] = Pb[k].b[i] + h[c] - qv[c];
+                }
+        } else {
+            mul(&DevArrays::Zi, &DevArrays::dZ, &DevArrays::T);
+            mul(&DevArrays::T, &DevArrays::dX, &DevArrays::Q);   // Q = Zi dZp dXp
+            aop(cat.Q, qv);
+            for (int k : act)
+                for (int i = 0; i < m[k]; i++) {
+                    const long long c = coff[k] + i;
+                    rhs[c] = Pb[k].b[i] - smu[k] * a0[c] + qv[c] + h[c];
+                }
+        }
         pcg(act, rhs, dy, 0);
         atop(dy, -1.0, 0.0, cat.dZ);
         set_coef(0, ones);
         set_coef(1, theta);
         RC(ew_lincomb_coef(g.st, B, d_boff, Ntot2, d_coef[0], cat.dZ, d_coef[1], cat.R0, nullptr, nullptr, cat.dZ));
-        mul(&DevArrays::Zi, &DevArrays::dZ, &DevArrays::T);
-        mul(&DevArrays::T, &DevArrays::X, &DevArrays::G);
-        RC(ew_lincomb(g.st, Ntot2, 1.0, cat.G, 1.0, cat.Q, 0.0, nullptr, cat.G));   // Zi dZ X + Q
-        {
+        if (nt) {   // dX = G (Rt - G' dZ G) G' (solver.c:14976-14996)
+            nt_toZ(&DevArrays::dZ, &DevArrays::Q);
+            RC(ew_lincomb(g.st, Ntot2, 1.0, cat.Rt, -1.0, cat.Q, 0.0, nullptr, cat.W));
+            nt_fromS(&DevArrays::W, &DevArrays::dX);
+        } else {
+            mul(&DevArrays::Zi, &DevArrays::dZ, &DevArrays::T);
+            mul(&DevArrays::T, &DevArrays::X, &DevArrays::G);
+            RC(ew_lincomb(g.st, Ntot2, 1.0, cat.G, 1.0, cat.Q, 0.0, nullptr, cat.G));   // Zi dZ X + Q
             std::vector<double> mones(B, -1.0);
             set_coef(0, mones);
             set_coef(1, smu);
@@ -943,7 +1024,7 @@ void Lockstep::run(std::vector<ResultData> &res) {
                 pcg(go, ev, wv, 0);
                 atop(wv, 1.0, 0.0, cat.W);   // A'w (zero on the instances outside go)
                 mul(&DevArrays::Zi, &DevArrays::W, &DevArrays::T);
-                mul(&DevArrays::T, &DevArrays::X, &DevArrays::F);
+                mul(&DevArrays::T, Xw, &DevArrays::F);   // Zi A'w X (W A'w W under NT)
                 RC(ew_sym_lincomb_blocks(g.st, B, d_n, d_boff, Ntot2, cat.F, 1.0, 0.0, nullptr, 0.0, nullptr, cat.G));
                 std::vector<double> AG;
                 aop(cat.G, AG);

@@ -452,7 +452,8 @@ __device__ __forceinline__ int block_of(long long g, int nb, const long long *__
 
 __global__ void rhs_scaled_kernel(int nb, const int *__restrict__ ns, const long long *__restrict__ off,
                                   const long long *__restrict__ loff, long long total, const double *__restrict__ lam,
-                                  double smu, const double *__restrict__ H, double *__restrict__ Rt) {
+                                  double smu, const double *__restrict__ H, double *__restrict__ Rt,
+                                  const double *__restrict__ smu_blk) {
     const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= total) return;
     const int k = block_of(g, nb, off), n = ns[k];
@@ -460,7 +461,7 @@ __global__ void rhs_scaled_kernel(int nb, const int *__restrict__ ns, const long
     const int j = (int)(l / n), i = (int)(l - (long long)j * n);
     const double li = lam[loff[k] + i], lj = lam[loff[k] + j];
     double v = -2.0 * (H ? H[g] : 0.0) / (li + lj);
-    if (i == j) v += smu / li - li;
+    if (i == j) v += (smu_blk ? smu_blk[k] : smu) / li - li;
     Rt[g] = v;
 }
 
@@ -612,9 +613,9 @@ int finish(cudaStream_t st, int n, const double *Mb, double *U, double *lam, int
 }
 
 int rhs_scaled(cudaStream_t st, int nb, const int *d_n, const long long *d_off, const long long *d_loff,
-               long long total, const double *lam, double smu, const double *H, double *Rt) {
+               long long total, const double *lam, double smu, const double *H, double *Rt, const double *d_smu) {
     if (total <= 0) return BGPU_OK;
-    rhs_scaled_kernel<<<ceil_div(total, 256), 256, 0, st>>>(nb, d_n, d_off, d_loff, total, lam, smu, H, Rt);
+    rhs_scaled_kernel<<<ceil_div(total, 256), 256, 0, st>>>(nb, d_n, d_off, d_loff, total, lam, smu, H, Rt, d_smu);
     BGPU_LAUNCH_CHECK();
     return BGPU_OK;
 }

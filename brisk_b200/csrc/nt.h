@@ -30,9 +30,11 @@ int finish(cudaStream_t st, int n, const double *Mb, double *U, double *lam, int
 
 // Over blocks stored one after another (block k: order d_n[k], n x n entries from d_off[k], its
 // lam from d_loff[k]; total = d_off[nb]):
-// Rt = L_lam^-1 (smu I - diag(lam)^2 - H), L_lam^-1(M)_ij = 2 M_ij / (lam_i + lam_j) (H may be null)
+// Rt = L_lam^-1 (smu I - diag(lam)^2 - H), L_lam^-1(M)_ij = 2 M_ij / (lam_i + lam_j) (H may be null;
+// d_smu, when not null, holds one smu per block instead)
 int rhs_scaled(cudaStream_t st, int nb, const int *d_n, const long long *d_off, const long long *d_loff,
-               long long total, const double *lam, double smu, const double *H, double *Rt);
+               long long total, const double *lam, double smu, const double *H, double *Rt,
+               const double *d_smu = nullptr);
 // out = src + alpha diag(lam) (out may alias src)
 int add_lam(cudaStream_t st, int nb, const int *d_n, const long long *d_off, const long long *d_loff,
             long long total, const double *lam, double alpha, const double *src, double *out);

@@ -2294,9 +2294,6 @@ struct BatchSession {
 BatchSession *batch_session_create(int count, const std::function<bool(int, InputData &)> &get,
                                    const std::function<bool(int, InputView &)> &view, const Options &opt, int &rc) {
     rc = 0;
-    // the lockstep loop takes the HKM direction; -dir auto picks NT for every block of order <= 64
-    // (15 n^3 <= 1e8), so those batches run the concurrent form
-    if (opt.direction != 0) return nullptr;
     const double t0 = wtime();
     std::vector<HProblem> Ps(count);
     std::vector<int> bad(count, 0);

@@ -66,10 +66,9 @@ BGPU_API int bgpu_batch_solve(int count, const int *m, const int *nblk, const in
                               const double *v, int nopt, const char *const *opts, int workers,
                               struct BriskResult *const *res, int *rc);
 /* A batch kept resident in device memory between solves: bgpu_batch_create takes the arrays of
- * bgpu_batch_solve for problems of one SDP block of order <= 64 each (the lockstep form, which
- * takes the HKM direction: the options must hold -dir hkm), builds and uploads them, and returns
- * a handle (NULL on failure; *rc: 1 bad options, -1 bad arguments, -6 a problem not of that shape
- * or another direction, < 0 a GPU failure).  bgpu_batch_run solves every problem from
+ * bgpu_batch_solve for problems of one SDP block of order <= 64 each (the lockstep form), builds
+ * and uploads them, and returns a handle (NULL on failure; *rc: 1 bad options, -1 bad arguments,
+ * -6 a problem not of that shape, < 0 a GPU failure).  bgpu_batch_run solves every problem from
  * the resident data into res[p] (brisk_result_new handles), rc[p] its exit code (2 for a problem
  * rejected on input), and returns 0 or a negative GPU failure code.  Extension of this build: the
  * reference re-reads every problem on every call. */

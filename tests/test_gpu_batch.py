@@ -107,3 +107,31 @@ def test_resident_batch_runs_twice_like_the_one_call_batch():
             assert a.pobj == b.pobj and a.dobj == b.dobj
             np.testing.assert_array_equal(a.y, b.y)
     sess.close()
+
+
+NT = ["-nohsd", "-dir", "nt", "-mixed", "0", "-tol", "1e-7"]
+
+
+@pytest.mark.parametrize("mode", ["lockstep", "concurrent"])
+def test_nt_batch_matches_reference(golden, mode):
+    """The NT direction in both batch forms against the reference's -dir nt solves."""
+    insts = [problems.batch_instance(q) for q in GOLDEN_Q]
+    out = brisk_b200.solve_batch(insts, options=NT + ["-batchmode", mode], workers=6)
+    for q, res in zip(GOLDEN_Q, out):
+        ref = golden[f"batch_q{q}"]["runs"]["nt"]
+        assert res.exit_code == 0, (q, res.exit_code)
+        check(res, ref)
+        assert abs(res.iterations - ref["iterations"]) <= 2, (q, res.iterations, ref["iterations"])
+
+
+def test_default_direction_batch_is_nt_in_lockstep():
+    """Without -dir the batch's blocks (order <= 64) take NT, as the reference's rule does, and the
+    resident lockstep batch gives the bits of the one-call batch with -dir nt."""
+    arrs = brisk_b200.concat_problems([problems.batch_instance(q) for q in range(200, 232)])
+    ref = brisk_b200.solve_batch_arrays(**arrs, options=NT)
+    sess = brisk_b200.BatchSession(**arrs, options=["-nohsd", "-mixed", "0", "-tol", "1e-7"])
+    out = sess.run()
+    sess.close()
+    for a, b in zip(out, ref):
+        assert a.status == b.status and a.iterations == b.iterations
+        assert a.pobj == b.pobj and a.dobj == b.dobj
