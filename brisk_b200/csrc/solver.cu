@@ -36,6 +36,7 @@
 #include <map>
 #include <numeric>
 #include <thread>
+#include <functional>
 
 namespace bsolve {
 
@@ -71,12 +72,33 @@ int exit_code_of(int s) {
 // ---------------------------------------------------------------------------------------------
 // host problem (scaled)
 // ---------------------------------------------------------------------------------------------
+// An allocator whose resize() leaves new elements uninitialised: the big entry arrays are written
+// in full right after they are sized (in parallel), so a serial zero fill first would be wasted.
+template <typename T>
+struct NoInitAlloc : std::allocator<T> {
+    template <typename U>
+    struct rebind {
+        using other = NoInitAlloc<U>;
+    };
+    NoInitAlloc() = default;
+    template <typename U>
+    NoInitAlloc(const NoInitAlloc<U> &) noexcept {}
+    template <typename U>
+    void construct(U *p) noexcept {
+        ::new (static_cast<void *>(p)) U;
+    }
+    template <typename U, typename... Args>
+    void construct(U *p, Args &&...args) {
+        ::new (static_cast<void *>(p)) U(std::forward<Args>(args)...);
+    }
+};
+
 struct HBlock {
     int n = 0;
     std::vector<int> con;                 // global constraint ids (ascending)
     std::vector<long long> cptr;          // per local constraint, into cpos/cval (full expansion)
-    std::vector<int> cpos;
-    std::vector<double> cval;
+    std::vector<int, NoInitAlloc<int>> cpos;
+    std::vector<double, NoInitAlloc<double>> cval;
     std::vector<int> Cpos;                // C, full expansion
     std::vector<double> Cval;
 };
@@ -226,20 +248,27 @@ static int build_problem(const InputData &in, HProblem &P, std::string &err) {
     const size_t nnz = in.v.size();
     const long long nkey = (long long)nb * (m + 1);
     std::vector<long long> start(nkey + 1, 0);
+    bool sorted = true;   // SDPA data usually lists the entries by block and matrix already
+    long long prev = -1;
     for (size_t e = 0; e < nnz; e++) {
         const int k = in.blk[e] - 1, mt = in.mat[e];
         if (k < 0 || k >= nb || mt < 0 || mt > m) { err = "entry out of range"; return 2; }
         const int n = P.blk[k].n;
         const int i = in.i[e], j = in.j[e];
         if (i < 1 || j < 1 || i > n || j > n) { err = "entry index out of the block"; return 2; }
-        start[(long long)k * (m + 1) + mt + 1]++;
+        const long long key = (long long)k * (m + 1) + mt;
+        sorted = sorted && key >= prev;
+        prev = key;
+        start[key + 1]++;
     }
     for (long long q = 0; q < nkey; q++) start[q + 1] += start[q];
-    std::vector<long long> order(nnz);
-    {
+    std::vector<long long> order;   // the entries in bucket order (empty: the input order is it)
+    if (!sorted) {
+        order.resize(nnz);
         std::vector<long long> fill(start.begin(), start.end() - 1);
         for (size_t e = 0; e < nnz; e++) order[fill[(long long)(in.blk[e] - 1) * (m + 1) + in.mat[e]]++] = (long long)e;
     }
+    auto entry = [&](long long u) { return sorted ? u : order[u]; };
     // per (block, matrix): merge duplicates, expand to both triangles, sort by position p + q n
     struct Bucket { std::vector<int> pos; std::vector<double> val; double ss = 0, sa = 0; };
     std::vector<Bucket> bk(nkey);
@@ -256,7 +285,7 @@ static int build_problem(const InputData &in, HProblem &P, std::string &err) {
             thread_local std::vector<char> mark;
             if ((long long)acc.size() < nn) { acc.assign(nn, 0.0); mark.assign(nn, 0); }
             for (long long u = s0; u < s1; u++) {
-                const long long e = order[u];
+                const long long e = entry(u);
                 int i = in.i[e] - 1, j = in.j[e] - 1;
                 if (i > j) std::swap(i, j);
                 const long long q = (long long)j * n + i;
@@ -277,7 +306,7 @@ static int build_problem(const InputData &in, HProblem &P, std::string &err) {
                     b.sa += std::fabs(v);
                 }
             for (long long u = s0; u < s1; u++) {   // clear the scratch for the next bucket
-                const long long e = order[u];
+                const long long e = entry(u);
                 int i = in.i[e] - 1, j = in.j[e] - 1;
                 if (i > j) std::swap(i, j);
                 const long long q = (long long)j * n + i;
@@ -286,40 +315,93 @@ static int build_problem(const InputData &in, HProblem &P, std::string &err) {
             }
             return;
         }
-        std::vector<std::pair<long long, double>> up;   // (upper position q*n + p with p <= q, value)
-        up.reserve(s1 - s0);
-        for (long long u = s0; u < s1; u++) {
-            const long long e = order[u];
+        // sparse: counting sorts by column instead of comparison sorts.  The upper entries (p, q),
+        // p <= q, go to column q in input order and then by row (insertion sort: a column holds few
+        // entries), duplicates summed in input order; the full expansion is then written column by
+        // column, the upper part (rows <= c, from column c's list) before the mirrored part (rows > c,
+        // from the entries (c, q) in order of q): position order with no sort.
+        thread_local std::vector<int> cnt;
+        if ((int)cnt.size() < n + 1) cnt.assign(n + 1, 0);
+        const long long ne = s1 - s0;
+        thread_local std::vector<int> row, col, ur, uc, lo_cnt, up_start;
+        thread_local std::vector<double> val, uv;
+        thread_local std::vector<long long> cstart, wpos;
+        if ((long long)row.size() < ne) {
+            row.resize(ne); col.resize(ne); ur.resize(ne); uc.resize(ne); val.resize(ne); uv.resize(ne);
+        }
+        for (long long u = 0; u < ne; u++) {
+            const long long e = entry(s0 + u);
             int i = in.i[e] - 1, j = in.j[e] - 1;
             if (i > j) std::swap(i, j);
-            up.push_back({(long long)j * n + i, in.v[e]});
+            cnt[j + 1]++;
+            row[u] = i;
+            col[u] = j;
+            val[u] = in.v[e];
         }
-        std::stable_sort(up.begin(), up.end(),
-                         [](const std::pair<long long, double> &a, const std::pair<long long, double> &b) {
-                             return a.first < b.first;
-                         });
-        std::vector<std::pair<int, double>> full;
-        full.reserve(2 * up.size());
-        for (size_t u = 0; u < up.size();) {
-            size_t w = u;
-            double v = 0;
-            while (w < up.size() && up[w].first == up[u].first) v += up[w++].second;   // duplicates summed
-            if (v != 0.0) {
-                const int q = (int)(up[u].first / n), pp = (int)(up[u].first % n);
-                full.push_back({pp + q * n, v});
-                if (pp != q) full.push_back({q + pp * n, v});
+        for (int c = 0; c < n; c++) cnt[c + 1] += cnt[c];
+        for (long long u = 0; u < ne; u++) {   // stable scatter by column
+            const int d = cnt[col[u]]++;
+            ur[d] = row[u];
+            uc[d] = col[u];
+            uv[d] = val[u];
+        }
+        for (int c = n; c > 0; c--) cnt[c] = cnt[c - 1];   // cnt[c]: the start of column c again
+        cnt[0] = 0;
+        long long nu = 0;   // merged upper entries, in (column, row) order, written over ur/uc/uv
+        for (int c = 0; c < n; c++) {
+            const int b0 = cnt[c], b1 = cnt[c + 1];
+            for (int a = b0 + 1; a < b1; a++) {   // stable insertion sort by row
+                const int r = ur[a];
+                const double v = uv[a];
+                int z = a;
+                while (z > b0 && ur[z - 1] > r) {
+                    ur[z] = ur[z - 1];
+                    uv[z] = uv[z - 1];
+                    z--;
+                }
+                ur[z] = r;
+                uv[z] = v;
             }
-            u = w;
+            for (int a = b0; a < b1;) {
+                int w = a;
+                double v = 0;
+                while (w < b1 && ur[w] == ur[a]) v += uv[w++];   // duplicates summed in input order
+                if (v != 0.0) {
+                    ur[nu] = ur[a];
+                    uc[nu] = c;
+                    uv[nu] = v;
+                    nu++;
+                }
+                a = w;
+            }
         }
-        std::sort(full.begin(), full.end());
+        for (int c = 0; c <= n; c++) cnt[c] = 0;
+        // per column c: its upper entries (rows <= c), then the mirrors of the row-c entries
+        lo_cnt.assign(n + 1, 0);
+        up_start.assign(n + 1, 0);
+        cstart.assign(n + 1, 0);
+        for (long long u = 0; u < nu; u++)
+            if (ur[u] != uc[u]) lo_cnt[ur[u] + 1]++;
+        for (long long u = 0; u < nu; u++) up_start[uc[u] + 1]++;
+        for (int c = 0; c < n; c++) cstart[c + 1] = cstart[c] + up_start[c + 1] + lo_cnt[c + 1];
         Bucket &b = bk[key];
-        b.pos.resize(full.size());
-        b.val.resize(full.size());
-        for (size_t u = 0; u < full.size(); u++) {
-            b.pos[u] = full[u].first;
-            b.val[u] = full[u].second;
-            b.ss += full[u].second * full[u].second;
-            b.sa += std::fabs(full[u].second);
+        b.pos.resize(cstart[n]);
+        b.val.resize(cstart[n]);
+        wpos.assign(cstart.begin(), cstart.end() - 1);
+        for (long long u = 0; u < nu; u++) {   // upper parts first (their columns in order)
+            const long long d = wpos[uc[u]]++;
+            b.pos[d] = ur[u] + uc[u] * n;
+            b.val[d] = uv[u];
+        }
+        for (long long u = 0; u < nu; u++) {   // then the mirrors: entry (p, q), p < q, at row q of column p
+            if (ur[u] == uc[u]) continue;
+            const long long d = wpos[ur[u]]++;
+            b.pos[d] = uc[u] + ur[u] * n;
+            b.val[d] = uv[u];
+        }
+        for (size_t u = 0; u < b.val.size(); u++) {
+            b.ss += b.val[u] * b.val[u];
+            b.sa += std::fabs(b.val[u]);
         }
     });
     std::vector<double> nrm2(P.m, 0.0);
@@ -767,19 +849,60 @@ void Solver::upload_block(int k) {
             RC(schur_densify(g.st, d));
         }
     }
-    // position-major copy (A'(y) without atomics): entries of each position in constraint order
-    std::vector<long long> pptr(nn + 1, 0);
-    for (long long e = 0; e < d.ne; e++) pptr[B.cpos[e] + 1]++;
-    for (long long p = 0; p < nn; p++) pptr[p + 1] += pptr[p];
-    std::vector<int> pcon(d.ne);
-    std::vector<double> pval(d.ne);
-    std::vector<long long> fill(pptr.begin(), pptr.end() - 1);
-    for (int t = 0; t < d.ncon; t++)
-        for (long long e = B.cptr[t]; e < B.cptr[t + 1]; e++) {
-            const long long q = fill[B.cpos[e]]++;
-            pcon[q] = B.con[t];
-            pval[q] = B.cval[e];
+    // position-major copy (A'(y) without atomics): entries of each position in constraint order, by
+    // a stable counting sort on the host's threads.  Thread r counts the positions of a contiguous run
+    // of constraints; the counts become each thread's offset inside each position, so a position's
+    // entries keep the constraints' order.
+    std::vector<long long, NoInitAlloc<long long>> pptr(nn + 1);
+    std::vector<int, NoInitAlloc<int>> pcon(d.ne);
+    std::vector<double, NoInitAlloc<double>> pval(d.ne);
+    {
+        int T = tl_serial || d.ne < 100000 ? 1 : (int)std::max(1u, std::min(std::thread::hardware_concurrency(), 32u));
+        while (T > 1 && (double)T * nn * sizeof(int) > 256e6) T--;   // the counts: at most 256 MB
+        std::vector<int> t0(T + 1, d.ncon);
+        t0[0] = 0;
+        for (int r = 1, t = 0; r < T; r++) {
+            const long long target = d.ne * r / T;
+            while (t < d.ncon && B.cptr[t] < target) t++;
+            t0[r] = t;
         }
+        std::vector<std::vector<int>> cnt(T);
+        auto on_threads = [&](int count, const std::function<void(int)> &f) {
+            if (count == 1) { f(0); return; }
+            std::vector<std::thread> th;
+            for (int r = 0; r < count; r++) th.emplace_back(f, r);
+            for (auto &x : th) x.join();
+        };
+        on_threads(T, [&](int r) {
+            cnt[r].assign(nn, 0);
+            for (long long e = B.cptr[t0[r]]; e < B.cptr[t0[r + 1]]; e++) cnt[r][B.cpos[e]]++;
+        });
+        const long long pchunk = (nn + T - 1) / T;
+        on_threads(T, [&](int r) {   // per position: the total, and each thread's offset in place of its count
+            const long long p1 = std::min((long long)nn, (r + 1) * pchunk);
+            for (long long p = r * pchunk; p < p1; p++) {
+                int rel = 0;
+                for (int q = 0; q < T; q++) {
+                    const int c = cnt[q][p];
+                    cnt[q][p] = rel;
+                    rel += c;
+                }
+                pptr[p + 1] = rel;
+            }
+        });
+        pptr[0] = 0;
+        for (long long p = 0; p < nn; p++) pptr[p + 1] += pptr[p];
+        on_threads(T, [&](int r) {
+            std::vector<int> &off = cnt[r];
+            for (int t = t0[r]; t < t0[r + 1]; t++)
+                for (long long e = B.cptr[t]; e < B.cptr[t + 1]; e++) {
+                    const int pos = B.cpos[e];
+                    const long long q = pptr[pos] + off[pos]++;
+                    pcon[q] = B.con[t];
+                    pval[q] = B.cval[e];
+                }
+        });
+    }
     CU(cudaMemcpyAsync(d.pptr, pptr.data(), sizeof(long long) * (nn + 1), cudaMemcpyHostToDevice, g.st));
     CU(cudaMemcpyAsync(d.pcon, pcon.data(), sizeof(int) * d.ne, cudaMemcpyHostToDevice, g.st));
     CU(cudaMemcpyAsync(d.pval, pval.data(), sizeof(double) * d.ne, cudaMemcpyHostToDevice, g.st));
