@@ -68,8 +68,9 @@ class Lockstep {
     void nt_fromS(double *DevArrays::*D, double *DevArrays::*out);   // out = sym(G D G')
 
   public:
-    // wall time of the phases (s): start, assembly, factor, PCG, the rest of the loop, final measures
-    double t_start = 0, t_asm = 0, t_fac = 0, t_pcg = 0, t_loop = 0, t_final = 0;
+    // wall time of the phases (s): start, assembly, factor, PCG, the rest of the loop, final measures;
+    // of the set-up: allocations and tables, the upload of P
+    double t_start = 0, t_asm = 0, t_fac = 0, t_pcg = 0, t_loop = 0, t_final = 0, t_alloc = 0, t_upload = 0;
 
   private:
 
@@ -97,6 +98,7 @@ class Lockstep {
 };
 
 void Lockstep::setup() {
+    const double t_setup0 = wtime();
     CU(cudaSetDevice(opt.device));
     CU(cudaStreamCreateWithFlags(&g.st, cudaStreamNonBlocking));
     CU(cudaEventCreate(&ev0));
@@ -235,17 +237,58 @@ void Lockstep::setup() {
         CU(cudaMemcpyAsync(d_groups, gr.data(), sizeof(GemmGroup) * B, cudaMemcpyHostToDevice, g.st));
         CU(cudaStreamSynchronize(g.st));
     }
-    // P (the packed constraints, built with the problems) and C, uploaded
+    t_alloc = wtime() - t_setup0;
+    // P (the packed constraints, built with the problems) and C, uploaded.  P (gigabytes for
+    // thousands of instances) goes through two pinned 64 MB buffers in turn: the host threads fill
+    // one with the next instances' rows while the copy engine drains the other.
     std::vector<double> Ch(Ntot2, 0.0);
     {
         for (int k = 0; k < B; k++) {
             if ((long long)Pb[k].Cdense.size() != (long long)n[k] * n[k]) throw GpuFail{BGPU_ERR_ARG, __LINE__};
             std::copy(Pb[k].Cdense.begin(), Pb[k].Cdense.end(), Ch.begin() + boff[k]);
             if ((long long)Pb[k].packed.size() != (long long)m[k] * t[k]) throw GpuFail{BGPU_ERR_ARG, __LINE__};
-            if (!Pb[k].packed.empty())
-                CU(cudaMemcpyAsync(Pp + poff[k], Pb[k].packed.data(), sizeof(double) * Pb[k].packed.size(),
-                                   cudaMemcpyHostToDevice, g.st));
         }
+        constexpr long long RING = (64LL << 20) / (long long)sizeof(double);   // doubles per buffer
+        double *ring[2] = {g.host_alloc<double>(RING), g.host_alloc<double>(RING)};
+        need(ring[0]); need(ring[1]);
+        cudaEvent_t done[2];
+        CU(cudaEventCreateWithFlags(&done[0], cudaEventDisableTiming));
+        CU(cudaEventCreateWithFlags(&done[1], cudaEventDisableTiming));
+        bool used[2] = {false, false};
+        int k = 0, buf = 0;
+        long long kpos = 0;   // doubles of instance k already staged
+        while (k < B) {
+            if (used[buf]) CU(cudaEventSynchronize(done[buf]));
+            // the pieces of this buffer: (instance, first double, count), in P's order
+            struct Piece { int k; long long from, cnt, at; };
+            std::vector<Piece> pieces;
+            long long fill = 0;
+            const long long first = poff[k] + kpos;
+            while (k < B && fill < RING) {
+                const long long left = (long long)Pb[k].packed.size() - kpos;
+                const long long take = std::min(left, RING - fill);
+                for (long long c = 0; c < take; c += (1LL << 17))   // 1 MB pieces for the threads
+                    pieces.push_back({k, kpos + c, std::min(take - c, 1LL << 17), fill + c});
+                fill += take;
+                kpos += take;
+                if (kpos == (long long)Pb[k].packed.size()) { k++; kpos = 0; }
+            }
+            double *dst = ring[buf];
+            parallel_for((long long)pieces.size(), [&](long long q) {
+                const Piece &pc = pieces[q];
+                std::memcpy(dst + pc.at, Pb[pc.k].packed.data() + pc.from, sizeof(double) * pc.cnt);
+            });
+            if (fill > 0) {
+                CU(cudaMemcpyAsync(Pp + first, dst, sizeof(double) * fill, cudaMemcpyHostToDevice, g.st));
+                CU(cudaEventRecord(done[buf], g.st));
+                used[buf] = true;
+            }
+            buf ^= 1;
+        }
+        CU(cudaStreamSynchronize(g.st));
+        cudaEventDestroy(done[0]);
+        cudaEventDestroy(done[1]);
+        t_upload = wtime() - t_setup0 - t_alloc;
         CU(cudaMemcpyAsync(Ccat, Ch.data(), sizeof(double) * Ntot2, cudaMemcpyHostToDevice, g.st));
         std::vector<double> ones(B, 1.0);
         CU(cudaMemcpyAsync(d_coef[0], ones.data(), sizeof(double) * B, cudaMemcpyHostToDevice, g.st));
