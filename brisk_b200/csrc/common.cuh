@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <atomic>
 #include <cstdio>
 #include <cmath>
 

@@ -181,7 +181,7 @@ template <bool A_KM, bool B_KM, int BN>
 int launch(cudaStream_t st, int M, int N, int K, double alpha, const double *A, long long lda, long long sA,
            const double *B, long long ldb, long long sB, double beta, double *C, long long ldc, long long sC,
            int batch, int lower) {
-    static bool attr_set = false;
+    static std::atomic<bool> attr_set{false};   // (set once; a second setter is harmless)
     if (!attr_set) {
         BGPU_CHECK(cudaFuncSetAttribute(dgemm_kernel<A_KM, B_KM, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)TileN<BN>::SMEM));
@@ -243,7 +243,7 @@ __global__ void scale_kernel(int M, int N, double beta, double *C, long long ldc
 int gemm_f64_grouped(cudaStream_t st, int ntiles, const int4 *d_tiles, const GemmGroup *d_groups, double alpha,
                      double beta) {
     if (ntiles <= 0) return BGPU_OK;
-    static bool attr_set = false;
+    static std::atomic<bool> attr_set{false};   // (set once; a second setter is harmless)
     if (!attr_set) {
         BGPU_CHECK(cudaFuncSetAttribute(dgemm_grouped_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)TileN<64>::SMEM));

@@ -366,7 +366,7 @@ int form_q(cudaStream_t st, const Layout &L, const int2 *items, int nitems, int 
            const double *Xc, const double *Zc, double *Q) {
     if (nitems <= 0) return BGPU_OK;
     if (nmax <= 0 || nmax > NMAX) return BGPU_ERR_ARG;
-    static bool attr = false;
+    static std::atomic<bool> attr{false};   // (set once; a second setter is harmless)
     if (!attr) {
         BGPU_CHECK(cudaFuncSetAttribute(form_q_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)form_q_smem(NMAX)));
@@ -397,7 +397,7 @@ int prec(cudaStream_t st, const Layout &L, const int *list, int cnt, int mmax, c
     if (cnt <= 0) return BGPU_OK;
     const size_t smem = (size_t)std::max(mmax, 1) * sizeof(double);
     if (smem > 200 * 1024) return BGPU_ERR_TOOBIG;
-    static bool attr = false;
+    static std::atomic<bool> attr{false};   // (set once; a second setter is harmless)
     if (!attr) {
         BGPU_CHECK(cudaFuncSetAttribute(prec_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
         attr = true;

@@ -258,7 +258,7 @@ int ozaki_gemm(cudaStream_t st, const OzakiOperand &A, const OzakiOperand &B, do
     int rc;
     if ((rc = make_map_i8(&mA, A.q, OZ_S * A.srows, K, A.ldk, BM)) || (rc = make_map_i8(&mB, B.q, OZ_S * B.srows, K, B.ldk, BN)))
         return rc;
-    static bool attr = false;
+    static std::atomic<bool> attr{false};   // (set once; a second setter is harmless)
     if (!attr) {
         BGPU_CHECK(cudaFuncSetAttribute(ozaki_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM));
         attr = true;

@@ -715,7 +715,7 @@ int schur_assemble_small(cudaStream_t st, int count, const int *d_blocks, int nm
                          const double *Xcat, const double *Zicat, double *M, int m) {
     if (count <= 0) return BGPU_OK;
     if (nmax <= 0 || nmax > SB_NMAX) return BGPU_ERR_ARG;
-    static bool attr = false;
+    static std::atomic<bool> attr{false};   // (set once; a second setter is harmless)
     if (!attr) {
         BGPU_CHECK(cudaFuncSetAttribute(small_schur_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)schur_small_smem(SB_NMAX)));

@@ -686,7 +686,7 @@ int factor(cudaStream_t st, Factor &F, const double *M, long long ldm, const dou
     const Analysis &A = *F.A;
     sp_init_kernel<<<1, 1, 0, st>>>(F.info, F.pmin);
     BGPU_LAUNCH_CHECK();
-    static bool attr = false;
+    static std::atomic<bool> attr{false};   // (set once; a second setter is harmless)
     if (!attr) {
         BGPU_CHECK(cudaFuncSetAttribute(front_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)((FS_MAX | 1) * FS_MAX * sizeof(double))));

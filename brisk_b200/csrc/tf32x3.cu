@@ -209,7 +209,7 @@ int launch(cudaStream_t st, int M, int N, int K, const float *Ah, const float *A
     if ((rc = make_map(&mAh, Ah, M, K, lda, BM)) || (rc = make_map(&mAl, Al, M, K, lda, BM)) ||
         (rc = make_map(&mBh, Bh, N, K, ldb, BN)) || (rc = make_map(&mBl, Bl, N, K, ldb, BN)))
         return rc;
-    static bool attr = false;
+    static std::atomic<bool> attr{false};   // (set once; a second setter is harmless)
     if (!attr) {
         BGPU_CHECK(cudaFuncSetAttribute(tf32x3_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)Cfg<BN>::SMEM));
