@@ -649,7 +649,7 @@ struct Gpu {
     // Stand-alone solves and lockstep batches allocate from the device's stream-ordered pool on
     // their own stream; the pool keeps up to 32 GB after a solve (release threshold), so the next
     // solve of a similar problem reuses that memory instead of mapping new memory (about 0.1 s per
-    // rand400 solve, 1 s for the 15 GB of a 4096-instance batch).
+    // rand400 solve, 1 s for the 23 GB of a 4096-instance batch).
     bool pool_alloc(void **p, size_t bytes) {
         static std::once_flag once[64];
         int dev = 0;
