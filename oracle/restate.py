@@ -9,7 +9,7 @@ It restates, on dense matrices (small sizes: tests), the reference BRISK 1.7 alg
 * problem_prepare        row equilibration and b/C scaling         problem.c:1866-1910
 * start_sdpt3            X0 = xi I, Z0 = eta I, y = 0               solver.c:6622-6661
 * schur (HKM)            M_ij = <A_i, X A_j Z^-1>                    solver.c:1969, 2339-3021
-* the infeasible-start HKM predictor-corrector loop                   solver.c:14394-15188
+* the infeasible-start predictor-corrector loop, HKM or NT          solver.c:14394-15188
   (residuals 14423-14484, theta R0 recurrence 14317-14326 / 14587-14607, rhs pieces
   14715-14735, predictor 14787-14818, sigma rule 14829-14873, corrector 14998-15050,
   refinement of A(dX) = rp 15058-15105, try_step 6393-6447)
@@ -184,8 +184,13 @@ STATUS = {0: "OPTIMAL", 1: "PRIMAL INFEASIBLE", 2: "DUAL INFEASIBLE", 3: "ITERAT
           4: "NUMERICAL DIFFICULTIES", 5: "REDUCED ACCURACY", 6: "TIME LIMIT"}
 
 
-def solve(data, tol=1e-8, maxit=100, gamma_max=0.99, red_acc=None, log=None):
-    """The infeasible-start HKM predictor-corrector loop (solver.c:14394-15188), FP64, dense.
+def solve(data, tol=1e-8, maxit=100, gamma_max=0.99, red_acc=None, log=None, direction="hkm"):
+    """The infeasible-start predictor-corrector loop (solver.c:14394-15188), FP64, dense, with the
+    HKM direction or (direction="nt") the NT direction in the scaled space: the scaling W = G G'
+    from nt_scaling each iteration (solver.c:14403-14410), the Schur complement at X = Zi = W
+    (nt_view), h = A(W theta R0 W), the predictor dXt = -lam - G' dZ G (solver.c:14740-14792), the
+    corrector Rt = L_lam^-1(smu I - lam^2 - sym(dXt dZt)), rhs = b + h - A(G (Rt + lam) G'),
+    dX = G (Rt - G' dZ G) G' (solver.c:14876-14996) and the refinement with W A'w W.
 
     Returns a dict with status, iterations, pobj, dobj, dimacs (errors 1..6), the iteration-0
     measures (it0: pobj, dobj, pinf, dinf, gap, mu in the reference's -v table convention) and
@@ -206,9 +211,21 @@ def solve(data, tol=1e-8, maxit=100, gamma_max=0.99, red_acc=None, log=None):
     status, stall, alp, ald, sigma = -1, 0, 0.0, 0.0, 0.0
     out = {"M0": None, "it0": None, "table": []}
     it = 0
+    nt = direction == "nt"
+    sym = lambda A: 0.5 * (A + A.T)   # noqa: E731
     for it in range(maxit + 1):
-        Zi = [np.linalg.inv(L).T @ np.linalg.inv(L) for L in LZ]
-        Zi = [0.5 * (Q + Q.T) for Q in Zi]
+        if nt:
+            scal = [nt_scaling(Lx, Lz) for Lx, Lz in zip(LX, LZ)]
+            if any(sc_ is None for sc_ in scal):
+                status = 4
+                break
+            Gn = [sc_[0] for sc_ in scal]
+            lamn = [sc_[1] for sc_ in scal]
+            Zi = [sym(sc_[2]) for sc_ in scal]
+        else:
+            Zi = [np.linalg.inv(L).T @ np.linalg.inv(L) for L in LZ]
+            Zi = [0.5 * (Q + Q.T) for Q in Zi]
+        Xv = Zi if nt else None   # the X the products read: W under NT
         rp = S.b - aop(S.A, Xs)
         ATy = atop(S.A, y)
         Fs = [a + Zk for a, Zk in zip(ATy, Zs)]
@@ -268,18 +285,28 @@ def solve(data, tol=1e-8, maxit=100, gamma_max=0.99, red_acc=None, log=None):
             R0 = [-F for F in Fd]
         if theta * r0norm <= 1e-13:
             theta = 0.0
-        M = schur(S.A, Xs, Zi)
+        Xp = Xv if nt else Xs
+        M = schur(S.A, Xp, Zi)
         if out["M0"] is None:
             out["M0"] = M.copy()
         Minv = np.linalg.inv(M)
         a0 = aop(S.A, Zi)
-        h = aop(S.A, [theta * Zk @ R @ Xk for Zk, R, Xk in zip(Zi, R0, Xs)]) if theta > 0 else np.zeros(m)
+        h = aop(S.A, [theta * Zk @ R @ Xk for Zk, R, Xk in zip(Zi, R0, Xp)]) if theta > 0 else np.zeros(m)
         dy = Minv @ (S.b + h)
         dZ = [-a + theta * R for a, R in zip(atop(S.A, dy), R0)]
         dX = []
-        for Zk, dZk, Xk in zip(Zi, dZ, Xs):
-            G = Zk @ dZk @ Xk
-            dX.append(-0.5 * (G + G.T) - Xk)
+        if nt:
+            dXt, dZt = [], []
+            for Gk, lk, dZk in zip(Gn, lamn, dZ):
+                zt = sym(Gk.T @ dZk @ Gk)
+                xt = -np.diag(lk) - zt
+                dZt.append(zt)
+                dXt.append(xt)
+                dX.append(sym(Gk @ xt @ Gk.T))
+        else:
+            for Zk, dZk, Xk in zip(Zi, dZ, Xs):
+                G = Zk @ dZk @ Xk
+                dX.append(-0.5 * (G + G.T) - Xk)
         ap = min(1.0, maxstep(LX, dX))
         ad = min(1.0, maxstep(LZ, dZ))
         xdz = sum(float(np.sum(a * b)) for a, b in zip(Xs, dZ))
@@ -292,14 +319,29 @@ def solve(data, tol=1e-8, maxit=100, gamma_max=0.99, red_acc=None, log=None):
         sigma = min(1.0, frac ** expon)
         gamma = 0.9 + (gamma_max - 0.9) * mina
         smu = sigma * mu
-        Q = [Zk @ dZk @ dXk for Zk, dZk, dXk in zip(Zi, dZ, dX)]
-        rhs = S.b - smu * a0 + aop(S.A, Q) + h
+        if nt:
+            Rt = []
+            for lk, xt, zt in zip(lamn, dXt, dZt):
+                H = sym(xt @ zt)
+                L2 = lk[:, None] + lk[None, :]
+                R_ = -2.0 * H / L2
+                R_[np.diag_indices_from(R_)] += smu / lk - lk
+                Rt.append(R_)
+            Gt = [sym(Gk @ (R_ + np.diag(lk)) @ Gk.T) for Gk, R_, lk in zip(Gn, Rt, lamn)]
+            rhs = S.b + h - aop(S.A, Gt)
+        else:
+            Q = [Zk @ dZk @ dXk for Zk, dZk, dXk in zip(Zi, dZ, dX)]
+            rhs = S.b - smu * a0 + aop(S.A, Q) + h
         dy = Minv @ rhs
         dZ = [-a + theta * R for a, R in zip(atop(S.A, dy), R0)]
         dX = []
-        for Zk, dZk, Xk, Qk in zip(Zi, dZ, Xs, Q):
-            G = Zk @ dZk @ Xk + Qk
-            dX.append(-0.5 * (G + G.T) + smu * Zk - Xk)
+        if nt:
+            for Gk, R_, dZk in zip(Gn, Rt, dZ):
+                dX.append(sym(Gk @ (R_ - sym(Gk.T @ dZk @ Gk)) @ Gk.T))
+        else:
+            for Zk, dZk, Xk, Qk in zip(Zi, dZ, Xs, Q):
+                G = Zk @ dZk @ Xk + Qk
+                dX.append(-0.5 * (G + G.T) + smu * Zk - Xk)
         for _ in range(3):
             ev = rp - aop(S.A, dX)
             ne, nrp = np.linalg.norm(ev), np.linalg.norm(rp)
@@ -308,7 +350,7 @@ def solve(data, tol=1e-8, maxit=100, gamma_max=0.99, red_acc=None, log=None):
             wv = Minv @ ev
             Qd = atop(S.A, wv)
             Gs = []
-            for Zk, Qk, Xk in zip(Zi, Qd, Xs):
+            for Zk, Qk, Xk in zip(Zi, Qd, Xp):
                 G = Zk @ Qk @ Xk
                 Gs.append(0.5 * (G + G.T))
             ne2 = np.linalg.norm(ev - aop(S.A, Gs))

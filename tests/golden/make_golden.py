@@ -6,8 +6,8 @@ files written by brisk_b200.problems, with the reference's presolves off so that
 problem as given, and records per run: status, iterations, objectives, the six DIMACS errors,
 the iteration table of -v (pobj, dobj, pinf, dinf, gap, mu per iteration) and the time.
 
-Runs per instance: "init0" and "default" (HKM direction, SDPT3 and least-squares start) and "nt"
-(NT direction, least-squares start).
+Runs per instance: "init0" and "default" (HKM direction, SDPT3 and least-squares start), "nt"
+and "nt_init0" (NT direction, least-squares and SDPT3 start).
 
 usage: python tests/golden/make_golden.py [--big] [--runs r1,r2] [names]
        (--big adds rand400 and mom700; --runs recomputes only those runs, keeping the others)
@@ -49,8 +49,8 @@ BIG = {"rand400": (random_sdp, dict(n=400, m=2000, density=0.01, seed=0)),
        "mom700": (moment_relaxation, dict(nvars=700, clique=4, seed=0))}
 
 HKM = ["-nohsd", "-dir", "hkm", "-mixed", "0", "-tol", "1e-7"] + AS_GIVEN
-RUNS = {"init0": HKM + ["-init", "0"], "default": HKM,
-        "nt": ["-nohsd", "-dir", "nt", "-mixed", "0", "-tol", "1e-7"] + AS_GIVEN}
+NTD = ["-nohsd", "-dir", "nt", "-mixed", "0", "-tol", "1e-7"] + AS_GIVEN
+RUNS = {"init0": HKM + ["-init", "0"], "default": HKM, "nt": NTD, "nt_init0": NTD + ["-init", "0"]}
 
 ROW = re.compile(r"^\s*(\d+)\s+([+-]\S+)\s+([+-]\S+)\s+(\S+)\s+(\S+)\s+(\S+)\s+(\S+)\s+(\S+)\s+(\S+)\s+(\S+)\s+(\S+)\s*$")
 

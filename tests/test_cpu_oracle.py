@@ -65,6 +65,29 @@ def test_oracle_solve_matches_reference(golden, name):
     assert max(abs(x) for x in ref["dimacs"]) <= 1e-7
 
 
+@pytest.mark.parametrize("name", ["theta30", "rand30", "rand60", "mom8"])
+def test_oracle_nt_solve_matches_reference(golden, name):
+    """The restated NT loop against the reference's -dir nt -init 0 run: same status, objectives
+    within 1e-7 relative, DIMACS errors <= 1e-7, iterations within 2, and the first rows of the
+    iteration table: three rows where every block has order <= 32 (the reference then takes exact
+    step lengths, as the oracle does), else the start's row (above 32 the reference's step
+    lengths are Lanczos estimates)."""
+    e = golden[name]
+    ref = e["runs"]["nt_init0"]
+    out = restate.solve(make(e), tol=1e-7, direction="nt")
+    assert out["status_str"] == ref["status"] == "OPTIMAL"
+    den = 1 + abs(ref["pobj"]) + abs(ref["dobj"])
+    assert abs(out["pobj"] - ref["pobj"]) <= 1e-7 * den
+    assert abs(out["dobj"] - ref["dobj"]) <= 1e-7 * den
+    assert np.max(np.abs(out["dimacs"])) <= 1e-7
+    assert abs(out["iterations"] - ref["iterations"]) <= 2
+    d = make(e)
+    nrows = 3 if max(int(b) for b in d.bs) <= 32 else 1
+    for mine, theirs in zip(out["table"][:nrows], ref["rows"][:nrows]):
+        assert mine["pobj"] == pytest.approx(theirs["pobj"], rel=1e-6, abs=1e-8)
+        assert mine["dobj"] == pytest.approx(theirs["dobj"], rel=1e-6, abs=1e-8)
+
+
 @pytest.mark.skipif(not os.path.exists("/root/reference/examples/theta1.dat-s"), reason="reference tree absent")
 def test_oracle_theta1_published_value():
     """theta1 -> 2.2999999997e+01 (the reference's INSTALL.md:44-45)."""
