@@ -65,6 +65,17 @@ def make_instance(w):
 BASE_OPTS = ["-nohsd", "-dir", "hkm", "-tol", "1e-7", "-q"]
 
 
+def max_over_ranks(value, world, device="cuda"):
+    """The slowest rank's value (an all-reduce MAX over the process group); the value itself on one
+    rank.  device: where the reduced tensor lives ("cuda" under NCCL, "cpu" under gloo)."""
+    if world <= 1:
+        return value
+    import torch
+    t = torch.tensor([value], device=device, dtype=torch.float64)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
 def dist_info():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -300,11 +311,7 @@ def run_ours_batch(args, w, torch):
         st[r.status_str] = st.get(r.status_str, 0) + 1
     worst = max(float(np.max(np.abs(r.dimacs))) for r in out)
     its = sum(r.iterations for r in out)
-    v = statistics.mean(times)
-    if world > 1:
-        tt = torch.tensor([v], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        v = float(tt.item())
+    v = max_over_ranks(statistics.mean(times), world)
     # end to end: the whole batch call on the host arrays
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -442,11 +449,7 @@ def run_ours(args):
                 L.brisk_result_dimacs(res, dimacs)
         torch.cuda.synchronize()
         launches = S.bgpu_launch_count() - launches0
-        t_step = statistics.mean(dev_times)
-        if world > 1:
-            tt = torch.tensor([t_step], device="cuda", dtype=torch.float64)
-            torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-            t_step = float(tt.item())
+        t_step = max_over_ranks(statistics.mean(dev_times), world)
         results[pname] = dict(value=t_step, status=statuses[-1], iterations=iters[-1],
                               schur_tflops=sum(schur_f) / max(sum(schur_t), 1e-30) / 1e12,
                               schur_s_per_solve=statistics.mean(schur_t), launches_per_step=launches / nsteps,
