@@ -113,7 +113,7 @@ struct HProblem {
     long long Ntot = 0;
     // the lockstep batch keeps, instead of its one block's entry lists: the constraints as packed
     // upper rows (m x n(n+1)/2) and the start's scalings xi, eta
-    std::vector<double> packed;
+    std::vector<double, NoInitAlloc<double>> packed;
     std::vector<double> Cdense;   // C (scaled), n x n
     double xi0 = 0, eta0 = 0;
 };
@@ -132,7 +132,8 @@ static int build_packed(const InputView &in, HProblem &P, std::string &err) {
     P.blk.resize(1);
     P.blk[0].n = n;
     P.Ntot = n;
-    P.packed.assign((size_t)m * t, 0.0);
+    P.packed.resize((size_t)m * t);   // each row zeroed as its matrix first appears (in cache)
+    std::vector<char> zeroed(m, 0);
     std::vector<double> Cu(t, 0.0);
     for (long long e = 0; e < in.nnz; e++) {
         const double v = in.v[e];
@@ -143,9 +144,19 @@ static int build_packed(const InputView &in, HProblem &P, std::string &err) {
         if (i < 1 || j < 1 || i > n || j > n) { err = "entry index out of the block"; return 2; }
         if (i > j) std::swap(i, j);
         const size_t u = (size_t)(j - 1) * j / 2 + (i - 1);
-        if (mt == 0) Cu[u] += v;
-        else P.packed[(size_t)(mt - 1) * t + u] += v;
+        if (mt == 0) {
+            Cu[u] += v;
+            continue;
+        }
+        double *row = P.packed.data() + (size_t)(mt - 1) * t;
+        if (!zeroed[mt - 1]) {
+            std::fill(row, row + t, 0.0);
+            zeroed[mt - 1] = 1;
+        }
+        row[u] += v;
     }
+    for (int a = 0; a < m; a++)
+        if (!zeroed[a]) std::fill(P.packed.data() + (size_t)a * t, P.packed.data() + (size_t)(a + 1) * t, 0.0);
     auto w = [](int u) {   // 2 off the diagonal: both triangles count
         int c = (int)((std::sqrt(8.0 * u + 1.0) - 1.0) * 0.5);
         while (c * (c + 1) / 2 > u) c--;
@@ -154,12 +165,22 @@ static int build_packed(const InputView &in, HProblem &P, std::string &err) {
     };
     std::vector<double> wt(t);
     for (int u = 0; u < t; u++) wt[u] = w(u);
-    std::vector<double> nrm2(m, 0.0);
+    // per row, while it is in cache: its squared norm, the row equilibration d = 1/norm, the row
+    // scaled by d, and the scaled row's norm (for the start's scalings below)
+    std::vector<double> nrm2(m, 0.0), snorm(m, 0.0);
+    P.d.resize(m);
     for (int a = 0; a < m; a++) {
-        const double *row = P.packed.data() + (size_t)a * t;
+        double *row = P.packed.data() + (size_t)a * t;
         double s = 0;
         for (int u = 0; u < t; u++) s += wt[u] * row[u] * row[u];
         nrm2[a] = s;
+        const double d = s > 0 ? 1.0 / std::sqrt(s) : 1.0;
+        P.d[a] = d;
+        for (int u = 0; u < t; u++) row[u] *= d;
+        if (s == 0) continue;
+        double s2 = 0;
+        for (int u = 0; u < t; u++) s2 += wt[u] * row[u] * row[u];
+        snorm[a] = std::sqrt(s2);
     }
     double c2 = 0, c1 = 0;
     for (int u = 0; u < t; u++) { c2 += wt[u] * Cu[u] * Cu[u]; c1 += wt[u] * std::fabs(Cu[u]); }
@@ -167,19 +188,12 @@ static int build_packed(const InputView &in, HProblem &P, std::string &err) {
     P.normC1 = c1;
     for (int i = 0; i < m; i++) { P.normb1 += std::fabs(P.b0[i]); P.normb2 += P.b0[i] * P.b0[i]; }
     P.normb2 = std::sqrt(P.normb2);
-    P.d.resize(m);
-    for (int i = 0; i < m; i++) {
-        P.d[i] = nrm2[i] > 0 ? 1.0 / std::sqrt(nrm2[i]) : 1.0;
+    for (int i = 0; i < m; i++)
         if (nrm2[i] == 0 && P.b[i] != 0) log_printf(1, "brisk: warning: constraint %d is empty but b != 0 (infeasible)\n", i + 1);
-    }
     double nbv = 0;
     for (int i = 0; i < m; i++) nbv += P.d[i] * P.b[i] * P.d[i] * P.b[i];
     nbv = std::sqrt(nbv);
     P.bs = nbv > 1 ? nbv : 1.0;
-    for (int a = 0; a < m; a++) {
-        double *row = P.packed.data() + (size_t)a * t;
-        for (int u = 0; u < t; u++) row[u] *= P.d[a];
-    }
     for (int i = 0; i < m; i++) P.b[i] *= P.d[i];
     P.du.resize(m);
     for (int i = 0; i < m; i++) P.du[i] = P.bs / P.d[i];
@@ -199,10 +213,7 @@ static int build_packed(const InputView &in, HProblem &P, std::string &err) {
     double maxA = 0, ratio = 0;
     for (int a = 0; a < m; a++) {
         if (nrm2[a] == 0) continue;   // not a constraint of the block
-        const double *row = P.packed.data() + (size_t)a * t;
-        double s = 0;
-        for (int u = 0; u < t; u++) s += wt[u] * row[u] * row[u];
-        s = std::sqrt(s);
+        const double s = snorm[a];
         maxA = std::max(maxA, s);
         ratio = std::max(ratio, (1 + std::fabs(P.b[a])) / (1 + s));
     }
