@@ -73,6 +73,8 @@ def load_library(path=None):
     L.bgpu_batch_solve.argtypes = [I, pi, pi, pi, pd, ctypes.POINTER(ctypes.c_int64), pi, pi, pi, pi, pd, I, ppc, I,
                                    ctypes.POINTER(P), pi]
     L.bgpu_batch_solve.restype = I
+    L.bgpu_sdpa_read.argtypes, L.bgpu_sdpa_read.restype = [ctypes.c_char_p, ctypes.POINTER(_SdpaArrays)], I
+    L.bgpu_sdpa_free.argtypes, L.bgpu_sdpa_free.restype = [ctypes.POINTER(_SdpaArrays)], None
     L.brisk_interrupt.argtypes, L.brisk_interrupt.restype = [], None
     L.brisk_interrupted.argtypes, L.brisk_interrupted.restype = [], I
     _lib, _lib_path = L, path
@@ -217,6 +219,53 @@ def solve_sdpa(blocksizes, c, mat, blk, i, j, v, options=None, verbose=True):
     return _run(lambda L, n, a, r: L.brisk_solve_data(
         int(c.size), int(bs.size), P(bs, pi), P(c, pd), nnz, P(arrs[0], pi), P(arrs[1], pi),
         P(arrs[2], pi), P(arrs[3], pi), P(v, pd), n, a, r), options, verbose)
+
+
+class _SdpaArrays(ctypes.Structure):
+    """struct bgpu_sdpa (include/bgpu.h)."""
+    _fields_ = [("m", ctypes.c_int), ("nblk", ctypes.c_int), ("nnz", ctypes.c_int64),
+                ("bs", ctypes.POINTER(ctypes.c_int)), ("c", ctypes.POINTER(ctypes.c_double)),
+                ("mat", ctypes.POINTER(ctypes.c_int)), ("blk", ctypes.POINTER(ctypes.c_int)),
+                ("i", ctypes.POINTER(ctypes.c_int)), ("j", ctypes.POINTER(ctypes.c_int)),
+                ("v", ctypes.POINTER(ctypes.c_double)), ("owner", ctypes.c_void_p)]
+
+
+def read_sdpa_file(path, verbose=False):
+    """Read an SDPA sparse file with the library's reader (bgpu_sdpa_read, the reader of
+    brisk_solve_file).  Returns (SdpaData, log); raises ValueError with the reader's message when
+    the file cannot be read or is malformed."""
+    from .problems import SdpaData
+    L = load_library()
+    chunks = []
+
+    def cb(s, is_err):
+        txt = s.decode(errors="replace")
+        chunks.append(txt)
+        if verbose:
+            sys.stderr.write(txt)
+        return 0
+
+    cbf = _PRINT(cb)
+    out = _SdpaArrays()
+    with _lock:
+        L.brisk_set_output(2, cbf)
+        try:
+            rc = L.bgpu_sdpa_read(os.fsencode(path), ctypes.byref(out))
+            if rc != 0:
+                raise ValueError("".join(chunks).strip() or f"bgpu_sdpa_read returned {rc}")
+            try:
+                def arr(ptr, n, dt):
+                    return np.ctypeslib.as_array(ptr, shape=(n,)).astype(dt, copy=True) if n else np.zeros(0, dt)
+                nnz = int(out.nnz)
+                d = SdpaData(bs=arr(out.bs, out.nblk, np.int32), c=arr(out.c, out.m, np.float64),
+                             mat=arr(out.mat, nnz, np.int32), blk=arr(out.blk, nnz, np.int32),
+                             i=arr(out.i, nnz, np.int32), j=arr(out.j, nnz, np.int32),
+                             v=arr(out.v, nnz, np.float64), name=os.path.basename(os.fsdecode(path)))
+            finally:
+                L.bgpu_sdpa_free(ctypes.byref(out))
+        finally:
+            L.brisk_set_output(0, _PRINT(0))
+    return d, "".join(chunks)
 
 
 def solve_file(path, options=None, verbose=True):

@@ -24,7 +24,7 @@ FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", 
          "--expt-relaxed-constexpr", "-I" + CSRC, "-I" + os.path.join(ROOT, "include")]
 
 SOURCES = ["gemm_f64.cu", "dense.cu", "schur.cu", "elementwise.cu", "tf32x3.cu", "small.cu", "sparse.cu", "lockstep.cu", "nt.cu", "ozaki.cu", "solver.cu",
-           "bgpu.cu", "capi.cpp"]
+           "bgpu.cu", "capi.cpp", "sdpa.cpp"]
 
 
 def _digest(path: str, extra: str) -> str:

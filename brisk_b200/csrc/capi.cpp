@@ -204,80 +204,6 @@ int parse_options(int argc, const char *const *argv, Options &opt, std::string &
     return 0;
 }
 
-// SDPA sparse reader: "m", "nblk", block sizes, c, then "mat blk i j v" lines; '"' and '*'
-// start comment lines, and ",(){}" are separators (as the reference's read_sdpa, problem.c:426).
-int read_sdpa_file(const char *path, InputData &in, std::string &err) {
-    FILE *f = fopen(path, "rb");
-    if (!f) { err = std::string("cannot open ") + path; return 2; }
-    std::string text;
-    {
-        std::vector<char> buf(1 << 20);
-        size_t n;
-        while ((n = fread(buf.data(), 1, buf.size(), f)) > 0) text.append(buf.data(), n);
-        fclose(f);
-    }
-    // drop comment lines, map separators to blanks
-    std::string clean;
-    clean.reserve(text.size());
-    size_t pos = 0;
-    while (pos < text.size()) {
-        size_t e = text.find('\n', pos);
-        if (e == std::string::npos) e = text.size();
-        size_t s = pos;
-        while (s < e && (text[s] == ' ' || text[s] == '\t' || text[s] == '\r')) s++;
-        if (s < e && text[s] != '"' && text[s] != '*') {
-            for (size_t q = pos; q < e; q++) {
-                char c = text[q];
-                if (c == ',' || c == '(' || c == ')' || c == '{' || c == '}' || c == '\r') c = ' ';
-                clean.push_back(c);
-            }
-            clean.push_back('\n');
-        }
-        pos = e + 1;
-    }
-    const char *p = clean.c_str();
-    char *endp = nullptr;
-    auto next = [&](double &v) -> bool {
-        while (*p && isspace((unsigned char)*p)) p++;
-        if (!*p) return false;
-        v = strtod(p, &endp);
-        if (endp == p) return false;
-        p = endp;
-        return true;
-    };
-    double v;
-    if (!next(v)) { err = "bad SDPA header (m)"; return 2; }
-    in.m = (int)v;
-    if (!next(v)) { err = "bad SDPA header (nblk)"; return 2; }
-    in.nblk = (int)v;
-    if (in.m < 0 || in.nblk <= 0) { err = "bad SDPA header"; return 2; }
-    in.bs.resize(in.nblk);
-    for (int k = 0; k < in.nblk; k++) {
-        if (!next(v)) { err = "bad block sizes"; return 2; }
-        in.bs[k] = (int)v;
-    }
-    in.c.resize(in.m);
-    for (int i = 0; i < in.m; i++) {
-        if (!next(v)) { err = "bad c vector"; return 2; }
-        in.c[i] = v;
-    }
-    double q[5];
-    while (true) {
-        int got = 0;
-        for (; got < 5; got++)
-            if (!next(q[got])) break;
-        if (got == 0) break;
-        if (got < 5) { err = "truncated entry line"; return 2; }
-        if (q[4] == 0) continue;
-        in.mat.push_back((int)q[0]);
-        in.blk.push_back((int)q[1]);
-        in.i.push_back((int)q[2]);
-        in.j.push_back((int)q[3]);
-        in.v.push_back(q[4]);
-    }
-    return 0;
-}
-
 }  // namespace bsolve
 
 // ---------------------------------------------------------------------------------------------
@@ -583,6 +509,39 @@ BRISK_API int brisk_solve_file(const char *fname, int nopt, const char *const *o
         return 2;
     }
     return run(in, nopt, opts, res);
+}
+
+BGPU_API int bgpu_sdpa_read(const char *path, bgpu_sdpa *out) {
+    if (!path || !out) return BGPU_ERR_ARG;
+    *out = bgpu_sdpa();
+    auto *in = new (std::nothrow) bsolve::InputData;
+    if (!in) return BGPU_ERR_NOMEM;
+    std::string err;
+    bsolve::set_print_hook(capi_print);
+    const int rc = bsolve::read_sdpa_file(path, *in, err);
+    if (rc) {
+        bsolve::log_printf(1, "brisk: %s\n", err.c_str());
+        delete in;
+        return rc;
+    }
+    out->m = in->m;
+    out->nblk = in->nblk;
+    out->nnz = (int64_t)in->v.size();
+    out->bs = in->bs.data();
+    out->c = in->c.data();
+    out->mat = in->mat.data();
+    out->blk = in->blk.data();
+    out->i = in->i.data();
+    out->j = in->j.data();
+    out->v = in->v.data();
+    out->owner = in;
+    return 0;
+}
+
+BGPU_API void bgpu_sdpa_free(bgpu_sdpa *s) {
+    if (!s) return;
+    delete static_cast<bsolve::InputData *>(s->owner);
+    *s = bgpu_sdpa();
 }
 
 }  // extern "C"

@@ -73,27 +73,6 @@ int exit_code_of(int s) {
 // ---------------------------------------------------------------------------------------------
 // host problem (scaled)
 // ---------------------------------------------------------------------------------------------
-// An allocator whose resize() leaves new elements uninitialised: the big entry arrays are written
-// in full right after they are sized (in parallel), so a serial zero fill first would be wasted.
-template <typename T>
-struct NoInitAlloc : std::allocator<T> {
-    template <typename U>
-    struct rebind {
-        using other = NoInitAlloc<U>;
-    };
-    NoInitAlloc() = default;
-    template <typename U>
-    NoInitAlloc(const NoInitAlloc<U> &) noexcept {}
-    template <typename U>
-    void construct(U *p) noexcept {
-        ::new (static_cast<void *>(p)) U;
-    }
-    template <typename U, typename... Args>
-    void construct(U *p, Args &&...args) {
-        ::new (static_cast<void *>(p)) U(std::forward<Args>(args)...);
-    }
-};
-
 struct HBlock {
     int n = 0;
     std::vector<int> con;                 // global constraint ids (ascending)

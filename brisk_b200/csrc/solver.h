@@ -2,10 +2,33 @@
 #pragma once
 #include <cstdint>
 #include <functional>
+#include <memory>
 #include <string>
+#include <utility>
 #include <vector>
 
 namespace bsolve {
+
+// An allocator whose resize() leaves new elements uninitialised: the big arrays are written in
+// full right after they are sized (in parallel), so a serial zero fill first would be wasted.
+template <typename T>
+struct NoInitAlloc : std::allocator<T> {
+    template <typename U>
+    struct rebind {
+        using other = NoInitAlloc<U>;
+    };
+    NoInitAlloc() = default;
+    template <typename U>
+    NoInitAlloc(const NoInitAlloc<U> &) noexcept {}
+    template <typename U>
+    void construct(U *p) noexcept {
+        ::new (static_cast<void *>(p)) U;
+    }
+    template <typename U, typename... Args>
+    void construct(U *p, Args &&...args) {
+        ::new (static_cast<void *>(p)) U(std::forward<Args>(args)...);
+    }
+};
 
 // The numbers of an SDPA sparse problem (brisk.h:128-140), already checked and with zero
 // values dropped.  mat 0 = F0 = -C; 1..m = A_i; i, j are 1-based within the block.
@@ -13,8 +36,8 @@ struct InputData {
     int m = 0, nblk = 0;
     std::vector<int> bs;
     std::vector<double> c;
-    std::vector<int> mat, blk, i, j;
-    std::vector<double> v;
+    std::vector<int, NoInitAlloc<int>> mat, blk, i, j;
+    std::vector<double, NoInitAlloc<double>> v;
 };
 
 // The same numbers seen in place (the caller's arrays; nothing copied; zero values are skipped
@@ -135,7 +158,8 @@ Session *session_create(const InputData &in, const Options &opt, std::string &er
 int session_solve(Session *s, const Options &opt, ResultData &res);
 void session_destroy(Session *s);
 
-// Reads an SDPA sparse file.  Returns 0 or an error message in err.
+// Reads an SDPA sparse file (sdpa.cpp; the reference's read_sdpa, problem.c:426).  Returns 0, or
+// 2 with a message in err.
 int read_sdpa_file(const char *path, InputData &in, std::string &err);
 
 // Output (the C API's brisk_set_output routes it).

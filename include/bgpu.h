@@ -38,6 +38,26 @@ BGPU_API const char *bgpu_version(void);
 /* Number of kernels this library has launched since it was loaded (all entry points). */
 BGPU_API long long bgpu_launch_count(void);
 
+/* An SDPA sparse file read into host arrays that the library owns: the reader of brisk_solve_file
+ * (the reference's read_sdpa, problem.c:426, and its tokenizers, problem.c:58-91: comment lines,
+ * the separators ",{}()=", Fortran exponents, text after the last entry, the same checks and
+ * messages), on all host threads.  The arrays hold the numbers brisk_solve_data (capi.c:175)
+ * takes: 1-based indices as written (a lower-triangle entry is not swapped), F0 as mat 0, entries
+ * with value 0 left out.  Returns 0 and fills *out, whose arrays stay valid until
+ * bgpu_sdpa_free(out); 2 when the file cannot be read or is malformed (the message goes to the
+ * output set by brisk_set_output); BGPU_ERR_ARG for a NULL argument. */
+typedef struct bgpu_sdpa {
+    int m, nblk;
+    int64_t nnz;
+    const int *bs;
+    const double *c;
+    const int *mat, *blk, *i, *j;
+    const double *v;
+    void *owner;
+} bgpu_sdpa;
+BGPU_API int bgpu_sdpa_read(const char *path, bgpu_sdpa *out);
+BGPU_API void bgpu_sdpa_free(bgpu_sdpa *s);
+
 /* A problem kept resident in device memory between solves: bgpu_session_create takes the
  * numbers of brisk_solve_data (capi.c:175) and the options, uploads the scaled problem and
  * returns a handle (NULL on failure, *rc the exit code: 1 bad options, 2 bad problem, < 0 GPU
