@@ -48,7 +48,7 @@ void fill_result(BriskResult *res) {
     }
 }
 
-int run(const bsolve::InputData &in, int nopt, const char *const *opts, BriskResult *res) {
+int run(const bsolve::InputView &in, int nopt, const char *const *opts, BriskResult *res) {
     bsolve::Options opt;
     std::string err;
     bsolve::set_print_hook(capi_print);
@@ -209,9 +209,28 @@ int parse_options(int argc, const char *const *argv, Options &opt, std::string &
 // ---------------------------------------------------------------------------------------------
 // exported interface
 // ---------------------------------------------------------------------------------------------
+// The caller's arrays as they are (nothing copied; build_problem skips the entries of value 0).
+static bool make_view(int m, int nblk, const int *bs, const double *c, int64_t nnz, const int *mat, const int *blk,
+                      const int *i, const int *j, const double *v, bsolve::InputView &in) {
+    if (nnz < 0 || m < 0 || nblk <= 0 || !bs || (m > 0 && !c) || (nnz > 0 && (!mat || !blk || !i || !j || !v))) return false;
+    in.m = m;
+    in.nblk = nblk;
+    in.bs = bs;
+    in.c = c;
+    in.nnz = nnz;
+    in.mat = mat;
+    in.blk = blk;
+    in.i = i;
+    in.j = j;
+    in.v = v;
+    return true;
+}
+
+// The same numbers copied, zero values dropped (for callers that keep them past the call).
 static bool make_input(int m, int nblk, const int *bs, const double *c, int64_t nnz, const int *mat, const int *blk,
                        const int *i, const int *j, const double *v, bsolve::InputData &in) {
-    if (nnz < 0 || m < 0 || nblk <= 0 || !bs || (m > 0 && !c) || (nnz > 0 && (!mat || !blk || !i || !j || !v))) return false;
+    bsolve::InputView w;
+    if (!make_view(m, nblk, bs, c, nnz, mat, blk, i, j, v, w)) return false;
     in.m = m;
     in.nblk = nblk;
     in.bs.assign(bs, bs + nblk);
@@ -293,8 +312,8 @@ BRISK_API int brisk_solve_data(int m, int nblk, const int *bs, const double *c, 
     if (!res) return -1;
     res->r = bsolve::ResultData();
     if (!g_stop_owner) g_stop = 0;
-    bsolve::InputData in;
-    if (!make_input(m, nblk, bs, c, nnz, mat, blk, i, j, v, in)) return 2;
+    bsolve::InputView in;
+    if (!make_view(m, nblk, bs, c, nnz, mat, blk, i, j, v, in)) return 2;
     return run(in, nopt, opts, res);
 }
 
@@ -444,11 +463,11 @@ BGPU_API bgpu_session *bgpu_session_create(int m, int nblk, const int *bs, const
                                            const int *mat, const int *blk, const int *i, const int *j,
                                            const double *v, int nopt, const char *const *opts, int *rc) {
     int code = 0;
-    bsolve::InputData in;
+    bsolve::InputView in;
     bsolve::Options opt;
     std::string err;
     bsolve::set_print_hook(capi_print);
-    if (!make_input(m, nblk, bs, c, nnz, mat, blk, i, j, v, in)) code = 2;
+    if (!make_view(m, nblk, bs, c, nnz, mat, blk, i, j, v, in)) code = 2;
     else if (bsolve::parse_options(nopt, opts, opt, err)) code = 1;
     bgpu_session *h = nullptr;
     if (!code) {
@@ -508,7 +527,7 @@ BRISK_API int brisk_solve_file(const char *fname, int nopt, const char *const *o
         bsolve::log_printf(1, "brisk: %s\n", err.c_str());
         return 2;
     }
-    return run(in, nopt, opts, res);
+    return run(bsolve::view_of(in), nopt, opts, res);
 }
 
 BGPU_API int bgpu_sdpa_read(const char *path, bgpu_sdpa *out) {

@@ -224,69 +224,165 @@ static void parallel_for(long long count, F f) {
     for (auto &t : th) t.join();
 }
 
-static int build_problem(const InputData &in, HProblem &P, std::string &err) {
-    P.m = in.m;
-    P.b0 = in.c;
-    P.b = in.c;
+// Runs f(t) for t in [0, count), each on its own host thread (on the calling thread for count 1).
+template <typename F>
+static void run_chunks(int count, F f) {
+    if (count <= 1) {
+        if (count == 1) f(0);
+        return;
+    }
+    std::vector<std::thread> th;
+    for (int t = 0; t < count; t++) th.emplace_back(f, t);
+    for (auto &x : th) x.join();
+}
+
+// Host threads for a pass over `work` items: one per 64k items, up to the cores (at most 32);
+// one in batch workers.
+static int host_threads(long long work) {
+    if (tl_serial) return 1;
+    const long long hw = std::max(1u, std::min(std::thread::hardware_concurrency(), 32u));
+    return (int)std::max(1LL, std::min(hw, work / 65536));
+}
+
+static int build_problem(const InputView &in, HProblem &P, std::string &err) {
     const int nb = in.nblk, m = in.m;
+    P.m = m;
+    P.b0.assign(in.c, in.c + m);
+    P.b = P.b0;
     P.blk.resize(nb);
     for (int k = 0; k < nb; k++) {
         if (in.bs[k] <= 0) { err = "LP (negative size) blocks are not supported by this build"; return 2; }
         P.blk[k].n = in.bs[k];
         P.Ntot += in.bs[k];
     }
-    // entries bucketed by block (a stable counting sort), then by matrix inside each block (already
-    // so in most SDPA data; else a stable sort): input order within a (block, matrix) bucket, and
-    // only the buckets that occur are kept (a dense (block, matrix) table would have nb (m + 1)
-    // entries: 17 million for 697 blocks and 24k constraints)
-    const size_t nnz = in.v.size();
-    std::vector<long long> bstart(nb + 1, 0);
+    // The caller's entries are read in place; an entry of value 0 is no entry (neither checked nor
+    // kept).  They are bucketed by block (a stable counting sort), then by matrix inside each block
+    // (already so in most SDPA data; else a stable sort): input order within a (block, matrix)
+    // bucket, and only the buckets that occur are kept (a dense (block, matrix) table would have
+    // nb (m + 1) entries: 17 million for 697 blocks and 24k constraints).
+    //
+    // Pass 1, a chunk of the entries per host thread: the checks (the first failing entry in input
+    // order gives the message), the entries per block, and whether they come block by block.
+    const long long nnz = in.nnz;
+    int T = host_threads(nnz);
+    while (T > 1 && (double)T * nb * sizeof(long long) > 256e6) T--;   // the counts: at most 256 MB
+    struct Chunk { std::vector<long long> cnt; long long nz = 0; int why = 0, k0 = -1, k1 = -1; bool sorted = true; };
+    std::vector<Chunk> ch(T);
+    run_chunks(T, [&](int t) {
+        Chunk &c = ch[t];
+        c.cnt.assign(nb, 0);
+        int prev = -1;
+        for (long long e = nnz * t / T, hi = nnz * (t + 1) / T; e < hi; e++) {
+            if (in.v[e] == 0) continue;
+            const int k = in.blk[e] - 1, mt = in.mat[e];
+            if (k < 0 || k >= nb || mt < 0 || mt > m) { c.why = 1; return; }
+            const int n = P.blk[k].n;
+            const int i = in.i[e], j = in.j[e];
+            if (i < 1 || j < 1 || i > n || j > n) { c.why = 2; return; }
+            if (prev < 0) c.k0 = k;
+            c.sorted = c.sorted && k >= prev;
+            prev = k;
+            c.cnt[k]++;
+            c.nz++;
+        }
+        c.k1 = prev;
+    });
+    for (int t = 0; t < T; t++)
+        if (ch[t].why) { err = ch[t].why == 1 ? "entry out of range" : "entry index out of the block"; return 2; }
     bool by_block = true;
-    int prevk = -1;
-    for (size_t e = 0; e < nnz; e++) {
-        const int k = in.blk[e] - 1, mt = in.mat[e];
-        if (k < 0 || k >= nb || mt < 0 || mt > m) { err = "entry out of range"; return 2; }
-        const int n = P.blk[k].n;
-        const int i = in.i[e], j = in.j[e];
-        if (i < 1 || j < 1 || i > n || j > n) { err = "entry index out of the block"; return 2; }
-        by_block = by_block && k >= prevk;
-        prevk = k;
-        bstart[k + 1]++;
+    long long nz = 0;
+    for (int t = 0, last = -1; t < T; t++) {
+        nz += ch[t].nz;
+        if (ch[t].k0 < 0) continue;   // no entry in the chunk
+        by_block = by_block && ch[t].sorted && ch[t].k0 >= last;
+        last = ch[t].k1;
     }
-    for (int k = 0; k < nb; k++) bstart[k + 1] += bstart[k];
-    std::vector<long long, NoInitAlloc<long long>> ord(nnz);   // the entries by block, then matrix
-    if (by_block) {
-        parallel_for((long long)nnz, [&](long long e) { ord[e] = e; });
-    } else {
-        std::vector<long long> fill(bstart.begin(), bstart.end() - 1);
-        for (size_t e = 0; e < nnz; e++) ord[fill[in.blk[e] - 1]++] = (long long)e;
+    std::vector<long long> bstart(nb + 1, 0);
+    for (int k = 0; k < nb; k++) {   // block starts; each chunk's count becomes its offset in the block
+        long long o = bstart[k];
+        for (int t = 0; t < T; t++) {
+            const long long c = ch[t].cnt[k];
+            ch[t].cnt[k] = o;
+            o += c;
+        }
+        bstart[k + 1] = o;
     }
-    struct Run { int k, mt; long long s0, s1; };   // one (block, matrix) bucket: ord[s0 .. s1)
-    std::vector<std::vector<Run>> kruns(nb);
-    parallel_for(nb, [&](long long kk) {
-        const int k = (int)kk;
-        const long long b0 = bstart[k], b1 = bstart[k + 1];
-        bool srt = true;
-        for (long long u = b0 + 1; u < b1 && srt; u++) srt = in.mat[ord[u]] >= in.mat[ord[u - 1]];
-        if (!srt)
-            std::stable_sort(ord.begin() + b0, ord.begin() + b1,
+    // ord[u]: the u-th entry by block.  Not formed when the entries already come block by block
+    // with no zero among them (then entry u is the u-th).
+    bool ident = by_block && nz == nnz;
+    std::vector<long long, NoInitAlloc<long long>> ord;
+    if (!ident) {
+        ord.resize(nz);
+        run_chunks(T, [&](int t) {
+            std::vector<long long> &fill = ch[t].cnt;
+            for (long long e = nnz * t / T, hi = nnz * (t + 1) / T; e < hi; e++)
+                if (in.v[e] != 0) ord[fill[in.blk[e] - 1]++] = e;
+        });
+    }
+    ch.clear();
+    auto entry = [&](long long u) { return ident ? u : ord[u]; };
+    const int U = host_threads(nz);
+    auto block_of = [&](long long u) {   // the block whose entries hold position u
+        return (int)(std::upper_bound(bstart.begin(), bstart.end(), u) - bstart.begin()) - 1;
+    };
+    // the blocks whose entries are not in matrix order, which are then sorted (stably)
+    std::vector<std::vector<int>> uns(U);
+    run_chunks(U, [&](int t) {
+        const long long lo = nz * t / U, hi = nz * (t + 1) / U;
+        if (lo >= hi) return;
+        int k = block_of(lo);
+        for (long long u = lo; u < hi; u++) {
+            while (u >= bstart[k + 1]) k++;
+            if (u > bstart[k] && in.mat[entry(u)] < in.mat[entry(u - 1)] && (uns[t].empty() || uns[t].back() != k))
+                uns[t].push_back(k);
+        }
+    });
+    std::vector<int> unsorted;
+    for (auto &x : uns)
+        for (int k : x)
+            if (unsorted.empty() || unsorted.back() != k) unsorted.push_back(k);
+    if (!unsorted.empty()) {
+        if (ident) {
+            ord.resize(nz);
+            parallel_for(nz, [&](long long u) { ord[u] = u; });
+            ident = false;
+        }
+        parallel_for((long long)unsorted.size(), [&](long long q) {
+            const int k = unsorted[q];
+            std::stable_sort(ord.begin() + bstart[k], ord.begin() + bstart[k + 1],
                              [&](long long x, long long y) { return in.mat[x] < in.mat[y]; });
-        for (long long u = b0; u < b1;) {
-            const int mt = in.mat[ord[u]];
-            long long w = u;
-            while (w < b1 && in.mat[ord[w]] == mt) w++;
-            kruns[k].push_back({k, mt, u, w});
-            u = w;
+        });
+    }
+    // the (block, matrix) buckets: a run starts at each block's first entry and where the matrix
+    // changes; runs in block order, then matrix order
+    struct Run { int k, mt; long long s0, s1; };   // one (block, matrix) bucket: entries s0 .. s1 - 1
+    std::vector<std::vector<long long>> starts(U);
+    run_chunks(U, [&](int t) {
+        const long long lo = nz * t / U, hi = nz * (t + 1) / U;
+        if (lo >= hi) return;
+        int k = block_of(lo);
+        for (long long u = lo; u < hi; u++) {
+            while (u >= bstart[k + 1]) k++;
+            if (u == bstart[k] || in.mat[entry(u)] != in.mat[entry(u - 1)]) starts[t].push_back(u);
         }
     });
     std::vector<Run> runs;
     std::vector<size_t> rstart(nb + 1, 0);
-    for (int k = 0; k < nb; k++) {
-        runs.insert(runs.end(), kruns[k].begin(), kruns[k].end());
-        rstart[k + 1] = runs.size();
+    {
+        size_t R = 0;
+        for (auto &x : starts) R += x.size();
+        runs.reserve(R);
+        int k = 0;
+        for (auto &x : starts)
+            for (long long u : x) {
+                while (u >= bstart[k + 1]) k++;
+                if (!runs.empty()) runs.back().s1 = u;
+                runs.push_back({k, in.mat[entry(u)], u, nz});
+            }
+        for (const Run &r : runs) rstart[r.k + 1]++;
+        for (int q = 0; q < nb; q++) rstart[q + 1] += rstart[q];
     }
-    kruns.clear();
-    auto entry = [&](long long u) { return ord[u]; };
+    starts.clear();
     // per (block, matrix): merge duplicates, expand to both triangles, sort by position p + q n
     struct Bucket { std::vector<int> pos; std::vector<double> val; double ss = 0, sa = 0; };
     std::vector<Bucket> bk(runs.size());
@@ -450,13 +546,6 @@ static int build_problem(const InputData &in, HProblem &P, std::string &err) {
         B.cpos.resize(total);
         B.cval.resize(total);
     }
-    parallel_for((long long)pieces.size(), [&](long long q) {   // one pass over every block's buckets
-        const Piece &pc = pieces[q];
-        HBlock &B = P.blk[pc.k];
-        const Bucket &b = bk[pc.r];
-        std::copy(b.pos.begin(), b.pos.end(), B.cpos.begin() + B.cptr[pc.t]);
-        std::copy(b.val.begin(), b.val.end(), B.cval.begin() + B.cptr[pc.t]);
-    });
     // problem_prepare (problem.c:1866-1910): row equilibration, b and C scaling
     P.normC2 = std::sqrt(c2);
     P.normC1 = c1;
@@ -472,9 +561,15 @@ static int build_problem(const InputData &in, HProblem &P, std::string &err) {
     for (int i = 0; i < P.m; i++) nbv += P.d[i] * P.b[i] * P.d[i] * P.b[i];
     nbv = std::sqrt(nbv);
     P.bs = nbv > 1 ? nbv : 1.0;
-    for (auto &B : P.blk)
-        for (size_t t = 0; t < B.con.size(); t++)
-            for (long long e = B.cptr[t]; e < B.cptr[t + 1]; e++) B.cval[e] *= P.d[B.con[t]];
+    parallel_for((long long)pieces.size(), [&](long long q) {   // every block's buckets, each row scaled by d
+        const Piece &pc = pieces[q];
+        HBlock &B = P.blk[pc.k];
+        const Bucket &b = bk[pc.r];
+        const double dq = P.d[B.con[pc.t]];
+        std::copy(b.pos.begin(), b.pos.end(), B.cpos.begin() + B.cptr[pc.t]);
+        double *out = B.cval.data() + B.cptr[pc.t];
+        for (size_t u = 0; u < b.val.size(); u++) out[u] = b.val[u] * dq;
+    });
     for (int i = 0; i < P.m; i++) P.b[i] *= P.d[i];
     P.du.resize(P.m);
     for (int i = 0; i < P.m; i++) P.du[i] = P.bs / P.d[i];
@@ -2399,14 +2494,14 @@ int Solver::run(ResultData &res) {
 
 }  // namespace
 
-static int solve_impl(const InputData &in, const Options &opt, ResultData &res, Arena *arena) {
+static int solve_impl(const InputView &in, const Options &opt, ResultData &res, Arena *arena) {
     HProblem P;
     std::string err;
     const double t0 = wtime();
     res = ResultData();
     res.m = in.m;
     res.nblk = in.nblk;
-    res.bs = in.bs;
+    res.bs.assign(in.bs, in.bs + in.nblk);
     if (int rc = build_problem(in, P, err)) {
         log_printf(1, "brisk: %s\n", err.c_str());
         return rc;
@@ -2453,9 +2548,9 @@ static int solve_impl(const InputData &in, const Options &opt, ResultData &res, 
     }
 }
 
-int solve_problem(const InputData &in, const Options &opt, ResultData &res) { return solve_impl(in, opt, res, nullptr); }
+int solve_problem(const InputView &in, const Options &opt, ResultData &res) { return solve_impl(in, opt, res, nullptr); }
 
-int solve_problem_arena(const InputData &in, const Options &opt, ResultData &res, Arena *arena) {
+int solve_problem_arena(const InputView &in, const Options &opt, ResultData &res, Arena *arena) {
     tl_serial = true;
     const int rc = solve_impl(in, opt, res, arena);
     tl_serial = false;
@@ -2617,15 +2712,17 @@ int solve_batch(int count, const std::vector<double> &work, const std::function<
             const int q = next.fetch_add(1);
             if (q >= count) break;
             const int p = order[q];
-            InputData in;
+            InputData held;   // (only when the caller gives no views)
+            InputView in;
             ResultData r;
             int rc = -3;
             try {
                 if (!ok) {
                     r.status = 4;
-                } else if (!get(p, in)) {
+                } else if (view ? !view(p, in) : !get(p, held)) {
                     rc = 2;
                 } else {
+                    if (!view) in = view_of(held);
                     for (int grow = 0; grow < 8; grow++) {
                         rc = solve_problem_arena(in, o, r, &a);
                         if (rc != BGPU_ERR_NOMEM) break;
@@ -2677,11 +2774,11 @@ struct Session {
     ~Session() { delete S; }
 };
 
-Session *session_create(const InputData &in, const Options &opt, std::string &err, int &rc) {
+Session *session_create(const InputView &in, const Options &opt, std::string &err, int &rc) {
     Session *s = new Session;
     s->m = in.m;
     s->nblk = in.nblk;
-    s->bs = in.bs;
+    s->bs.assign(in.bs, in.bs + in.nblk);
     rc = build_problem(in, s->P, err);
     if (rc) { delete s; return nullptr; }
     try {

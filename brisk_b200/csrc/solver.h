@@ -51,6 +51,21 @@ struct InputView {
     const double *v = nullptr;
 };
 
+inline InputView view_of(const InputData &d) {
+    InputView w;
+    w.m = d.m;
+    w.nblk = d.nblk;
+    w.bs = d.bs.data();
+    w.c = d.c.data();
+    w.nnz = (long long)d.v.size();
+    w.mat = d.mat.data();
+    w.blk = d.blk.data();
+    w.i = d.i.data();
+    w.j = d.j.data();
+    w.v = d.v.data();
+    return w;
+}
+
 struct Options {
     double tol = 1e-8;
     int maxit = 100;
@@ -119,7 +134,7 @@ int exit_code_of(int status);
 int parse_options(int argc, const char *const *argv, Options &opt, std::string &err);
 
 // Solves on the GPU; fills res.  Returns the exit code (0, 10-15) or a negative abort code.
-int solve_problem(const InputData &in, const Options &opt, ResultData &res);
+int solve_problem(const InputView &in, const Options &opt, ResultData &res);
 
 // A device arena for a batch worker: one allocation and one stream reused by every instance.
 struct Arena {
@@ -133,7 +148,7 @@ struct Arena {
 // Solves with the device memory and stream of the arena (no cudaMalloc / cudaFree, no device-wide
 // synchronisation) and builds the host problem on the calling thread.  Returns BGPU_ERR_NOMEM
 // (arena->need set) when the arena is too small; the caller grows it and calls again.
-int solve_problem_arena(const InputData &in, const Options &opt, ResultData &res, Arena *arena);
+int solve_problem_arena(const InputView &in, const Options &opt, ResultData &res, Arena *arena);
 
 // Solves `count` independent problems on `workers` host threads (0: one per host core), each
 // with its own stream and arena, largest estimated work first.  get(p, in) fills problem p
@@ -154,7 +169,7 @@ void batch_session_destroy(BatchSession *S);
 
 // A problem kept resident in HBM between solves (the benchmark's device-resident timing).
 struct Session;
-Session *session_create(const InputData &in, const Options &opt, std::string &err, int &rc);
+Session *session_create(const InputView &in, const Options &opt, std::string &err, int &rc);
 int session_solve(Session *s, const Options &opt, ResultData &res);
 void session_destroy(Session *s);
 
