@@ -166,8 +166,12 @@ def _collect(L, r, rc, log):
     if L.brisk_result_have_x(r):
         X, Z = [], []
         for k, n in enumerate(bsz):
-            shape = (abs(n), abs(n))
             xp, zp = L.brisk_result_X(r, k), L.brisk_result_Z(r, k)
+            if n < 0:   # an LP block: its vector of -n values
+                X.append(np.ctypeslib.as_array(xp, shape=(-n,)).copy() if xp else None)
+                Z.append(np.ctypeslib.as_array(zp, shape=(-n,)).copy() if zp else None)
+                continue
+            shape = (n, n)
             X.append(np.ctypeslib.as_array(xp, shape=shape).T.copy() if xp else None)
             Z.append(np.ctypeslib.as_array(zp, shape=shape).T.copy() if zp else None)
     return Result(status=L.brisk_result_status(r), status_str=L.brisk_result_status_str(r).decode(),

@@ -90,6 +90,8 @@ struct HProblem {
     std::vector<double> d, du;
     double bs = 1, cs = 1, normb1 = 0, normb2 = 0, normC1 = 0, normC2 = 0;
     long long Ntot = 0;
+    // the blocks as given: their sizes (negative: LP) and the first of their blocks here
+    std::vector<int> in_n, in_first;
     // the lockstep batch keeps, instead of its one block's entry lists: the constraints as packed
     // upper rows (m x n(n+1)/2) and the start's scalings xi, eta
     std::vector<double, NoInitAlloc<double>> packed;
@@ -245,16 +247,42 @@ static int host_threads(long long work) {
 }
 
 static int build_problem(const InputView &in, HProblem &P, std::string &err) {
-    const int nb = in.nblk, m = in.m;
+    const int nbin = in.nblk, m = in.m;
     P.m = m;
     P.b0.assign(in.c, in.c + m);
     P.b = P.b0;
-    P.blk.resize(nb);
-    for (int k = 0; k < nb; k++) {
-        if (in.bs[k] <= 0) { err = "LP (negative size) blocks are not supported by this build"; return 2; }
-        P.blk[k].n = in.bs[k];
-        P.Ntot += in.bs[k];
+    // An LP block of size N (a negative size, brisk.h:128-140) is N semidefinite blocks of order 1:
+    // x >= 0 is X = diag(x) >= 0, and an LP block's X stays diagonal on the way (its data are).
+    // P.in_first[k]: the first block here of block k as given.
+    P.in_n.assign(in.bs, in.bs + nbin);
+    P.in_first.resize(nbin + 1);
+    int nb = 0;
+    for (int k = 0; k < nbin; k++) {
+        if (in.bs[k] == 0) { err = "a block of size 0"; return 2; }
+        P.in_first[k] = nb;
+        nb += in.bs[k] > 0 ? 1 : -in.bs[k];
     }
+    P.in_first[nbin] = nb;
+    P.blk.resize(nb);
+    for (int k = 0; k < nbin; k++)
+        for (int q = P.in_first[k]; q < P.in_first[k + 1]; q++) {
+            P.blk[q].n = in.bs[k] > 0 ? in.bs[k] : 1;
+            P.Ntot += P.blk[q].n;
+        }
+    const int *first = P.in_first.data();
+    const int *bsz = in.bs;
+    auto block_here = [&](long long e) {   // entry e's block here (an LP entry: its variable's)
+        const int k = in.blk[e] - 1;
+        return bsz[k] > 0 ? first[k] : first[k] + in.i[e] - 1;
+    };
+    auto rc_here = [&](long long e, int &i, int &j) {   // its 0-based row and column there
+        if (bsz[in.blk[e] - 1] > 0) {
+            i = in.i[e] - 1;
+            j = in.j[e] - 1;
+        } else {
+            i = j = 0;
+        }
+    };
     // The caller's entries are read in place; an entry of value 0 is no entry (neither checked nor
     // kept).  They are bucketed by block (a stable counting sort), then by matrix inside each block
     // (already so in most SDPA data; else a stable sort): input order within a (block, matrix)
@@ -274,11 +302,13 @@ static int build_problem(const InputView &in, HProblem &P, std::string &err) {
         int prev = -1;
         for (long long e = nnz * t / T, hi = nnz * (t + 1) / T; e < hi; e++) {
             if (in.v[e] == 0) continue;
-            const int k = in.blk[e] - 1, mt = in.mat[e];
-            if (k < 0 || k >= nb || mt < 0 || mt > m) { c.why = 1; return; }
-            const int n = P.blk[k].n;
+            const int kin = in.blk[e] - 1, mt = in.mat[e];
+            if (kin < 0 || kin >= nbin || mt < 0 || mt > m) { c.why = 1; return; }
+            const int n = std::abs(bsz[kin]);
             const int i = in.i[e], j = in.j[e];
             if (i < 1 || j < 1 || i > n || j > n) { c.why = 2; return; }
+            if (bsz[kin] < 0 && i != j) { c.why = 3; return; }
+            const int k = block_here(e);
             if (prev < 0) c.k0 = k;
             c.sorted = c.sorted && k >= prev;
             prev = k;
@@ -288,7 +318,11 @@ static int build_problem(const InputView &in, HProblem &P, std::string &err) {
         c.k1 = prev;
     });
     for (int t = 0; t < T; t++)
-        if (ch[t].why) { err = ch[t].why == 1 ? "entry out of range" : "entry index out of the block"; return 2; }
+        if (ch[t].why) {
+            err = ch[t].why == 1 ? "entry out of range"
+                  : ch[t].why == 2 ? "entry index out of the block" : "off-diagonal entry in LP block";
+            return 2;
+        }
     bool by_block = true;
     long long nz = 0;
     for (int t = 0, last = -1; t < T; t++) {
@@ -316,7 +350,7 @@ static int build_problem(const InputView &in, HProblem &P, std::string &err) {
         run_chunks(T, [&](int t) {
             std::vector<long long> &fill = ch[t].cnt;
             for (long long e = nnz * t / T, hi = nnz * (t + 1) / T; e < hi; e++)
-                if (in.v[e] != 0) ord[fill[in.blk[e] - 1]++] = e;
+                if (in.v[e] != 0) ord[fill[block_here(e)]++] = e;
         });
     }
     ch.clear();
@@ -400,7 +434,8 @@ static int build_problem(const InputView &in, HProblem &P, std::string &err) {
             if ((long long)acc.size() < nn) { acc.assign(nn, 0.0); mark.assign(nn, 0); }
             for (long long u = s0; u < s1; u++) {
                 const long long e = entry(u);
-                int i = in.i[e] - 1, j = in.j[e] - 1;
+                int i, j;
+                rc_here(e, i, j);
                 if (i > j) std::swap(i, j);
                 const long long q = (long long)j * n + i;
                 acc[q] += in.v[e];
@@ -421,7 +456,8 @@ static int build_problem(const InputView &in, HProblem &P, std::string &err) {
                 }
             for (long long u = s0; u < s1; u++) {   // clear the scratch for the next bucket
                 const long long e = entry(u);
-                int i = in.i[e] - 1, j = in.j[e] - 1;
+                int i, j;
+                rc_here(e, i, j);
                 if (i > j) std::swap(i, j);
                 const long long q = (long long)j * n + i;
                 acc[q] = 0.0;
@@ -445,7 +481,8 @@ static int build_problem(const InputView &in, HProblem &P, std::string &err) {
         }
         for (long long u = 0; u < ne; u++) {
             const long long e = entry(s0 + u);
-            int i = in.i[e] - 1, j = in.j[e] - 1;
+            int i, j;
+            rc_here(e, i, j);
             if (i > j) std::swap(i, j);
             cnt[j + 1]++;
             row[u] = i;
@@ -2494,6 +2531,27 @@ int Solver::run(ResultData &res) {
 
 }  // namespace
 
+// X and Z per block as given: an LP block's N blocks of order 1 become its vector of N values
+// (brisk_result_X, capi.c:131-136: "n*n column-major or n for LP").
+static void blocks_as_given(const HProblem &P, ResultData &res) {
+    const int nbin = (int)P.in_n.size();
+    if (nbin == (int)P.blk.size()) return;   // no LP block
+    for (auto *V : {&res.X, &res.Z}) {
+        if (V->empty()) continue;
+        std::vector<std::vector<double>> out(nbin);
+        for (int k = 0; k < nbin; k++) {
+            const int q0 = P.in_first[k], q1 = P.in_first[k + 1];
+            if (P.in_n[k] > 0) {
+                out[k] = std::move((*V)[q0]);
+                continue;
+            }
+            out[k].resize(q1 - q0);
+            for (int q = q0; q < q1; q++) out[k][q - q0] = (*V)[q].empty() ? 0.0 : (*V)[q][0];
+        }
+        *V = std::move(out);
+    }
+}
+
 static int solve_impl(const InputView &in, const Options &opt, ResultData &res, Arena *arena) {
     HProblem P;
     std::string err;
@@ -2520,6 +2578,7 @@ static int solve_impl(const InputView &in, const Options &opt, ResultData &res, 
         const double t1 = wtime();
         if (opt.verbose > 1) log_printf(0, "   [device setup and upload %.3fs]\n", t1 - tsu);
         int rc = S.run(res);
+        blocks_as_given(P, res);
         res.t.setup = t1 - t0;
         res.h2d_bytes = S.upload_bytes;
         res.time = wtime() - t0;
@@ -2800,7 +2859,9 @@ int session_solve(Session *s, const Options &opt, ResultData &res) {
     res.bs = s->bs;
     s->S->set_options(opt);
     try {
-        return s->S->run(res);
+        const int rc = s->S->run(res);
+        blocks_as_given(s->P, res);
+        return rc;
     } catch (const GpuFail &f) {
         log_printf(1, "brisk: GPU failure (code %d at solver.cu:%d)\n", f.rc, f.line);
         res.status = 4;

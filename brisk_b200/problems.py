@@ -158,6 +158,52 @@ def random_sdp(n: int = 400, m: int = 2000, density: float = 0.01, seed: int = 0
                     meta=dict(kind="random", n=n, m=m, density=density, seed=seed, upper_per_con=k))
 
 
+def sdp_lp_problem(blocks=(30, -40, 6), m: int = 50, density: float = 0.1, lp_per_con: int = 4,
+                   seed: int = 0) -> SdpaData:
+    """A random problem with LP blocks (negative sizes) among SDP blocks.
+
+    SDP block of order n: C = G G'/n + I, each A_i with round(density n(n+1)/2) N(0,1) upper
+    entries at distinct positions.  LP block of size N: c ~ U(0.5, 1.5), each A_i with
+    min(lp_per_con, N) N(0,1) entries on distinct variables.  b = A(I, 1, ...), so X = I, x = 1
+    is feasible, and y = 0 gives Z = C > 0, z = c > 0: both sides strictly feasible.
+    """
+    rng = np.random.default_rng(seed)
+    mats, blks, ii, jj, vv = [], [], [], [], []
+    b = np.zeros(m)
+    for kb, sz in enumerate(blocks, start=1):
+        if sz > 0:
+            n = sz
+            G = rng.standard_normal((n, n))
+            C = G @ G.T / n + np.eye(n)
+            iu, ju = np.triu_indices(n)
+            mats.append(np.zeros(iu.size, np.int32)); blks.append(np.full(iu.size, kb, np.int32))
+            ii.append(iu + 1); jj.append(ju + 1); vv.append(-C[iu, ju])
+            k = max(1, int(round(density * n * (n + 1) / 2)))
+            for t in range(m):
+                r, cc = _random_upper_positions(rng, n, k)
+                val = rng.standard_normal(k)
+                mats.append(np.full(k, t + 1, np.int32)); blks.append(np.full(k, kb, np.int32))
+                ii.append(r + 1); jj.append(cc + 1); vv.append(val)
+                b[t] += val[r == cc].sum()
+        else:
+            N = -sz
+            c = rng.uniform(0.5, 1.5, N)
+            idx = np.arange(1, N + 1)
+            mats.append(np.zeros(N, np.int32)); blks.append(np.full(N, kb, np.int32))
+            ii.append(idx); jj.append(idx); vv.append(-c)
+            q = min(lp_per_con, N)
+            for t in range(m):
+                var = rng.choice(N, size=q, replace=False) + 1
+                val = rng.standard_normal(q)
+                mats.append(np.full(q, t + 1, np.int32)); blks.append(np.full(q, kb, np.int32))
+                ii.append(var); jj.append(var); vv.append(val)
+                b[t] += val.sum()
+    d = _normalise(np.concatenate(mats), np.concatenate(blks), np.concatenate(ii), np.concatenate(jj),
+                   np.concatenate(vv))
+    return SdpaData(np.array(blocks, np.int32), b, *d, name=f"sdp_lp_{'_'.join(map(str, blocks))}_m{m}_seed{seed}",
+                    meta=dict(kind="sdp_lp", blocks=list(blocks), m=m, seed=seed))
+
+
 def random_dense_instance(rng, n: int, m: int, name: str = "") -> SdpaData:
     """One small dense instance: A_i dense N(0,1) symmetric, b = A(I), C = G G'/n + I."""
     iu, ju = np.triu_indices(n)

@@ -23,8 +23,8 @@ import tempfile
 
 ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 sys.path.insert(0, ROOT)
-from brisk_b200.problems import (batch_instance, dense_instance, moment_relaxation, random_sdp, theta_problem,  # noqa: E402
-                                 write_sdpa)
+from brisk_b200.problems import (batch_instance, dense_instance, moment_relaxation, random_sdp, sdp_lp_problem,  # noqa: E402
+                                 theta_problem, write_sdpa)
 
 REF = os.path.join(ROOT, "oracle", "_ref", "brisk_ref")
 OUT = os.path.join(ROOT, "tests", "golden", "ref_runs.json")
@@ -40,6 +40,9 @@ INSTANCES = {
     "mom60": (moment_relaxation, dict(nvars=60, clique=4, seed=0)),
     "dense24": (dense_instance, dict(n=24, m=100, seed=11)),
     "dense48": (dense_instance, dict(n=48, m=500, seed=12)),
+    # LP blocks (negative sizes) among SDP blocks, and an LP alone
+    "lp_mixed": (sdp_lp_problem, dict(blocks=(30, -40, 6), m=50, density=0.1, lp_per_con=4, seed=3)),
+    "lp_only": (sdp_lp_problem, dict(blocks=(-60,), m=30, lp_per_con=6, seed=4)),
 }
 # instances of the 4096-instance uneven batch (n ~ U{8..64}, m ~ U{n..n(n+1)/4}, seed 0): the
 # first twelve and the largest (q = 3339: n = 64, m = 1038)

@@ -93,3 +93,31 @@ def test_dense_constraints_match_reference(golden, name, route):
     e = golden[name]
     res = brisk_b200.solve_sdpa(*make(e).args(), options=FP64 + ["-schurroute", route], verbose=False)
     check(res, e["runs"]["default"])
+
+
+NT = ["-nohsd", "-dir", "nt", "-mixed", "0", "-tol", "1e-7"]
+
+
+@pytest.mark.parametrize("name", ["lp_mixed", "lp_only"])
+@pytest.mark.parametrize("run,opts", [("default", FP64), ("init0", FP64 + ["-init", "0"]), ("nt", NT)])
+def test_lp_blocks_match_reference(golden, name, run, opts):
+    """LP blocks (negative sizes; here each variable a block of order 1) against the reference's
+    solves of the same problems: status, objectives, DIMACS.  An LP block's X and Z come back as
+    vectors (brisk_result_X: "n for LP", capi.c:131), of positive values at an interior point,
+    and <C, X> summed from the blocks returned is pobj."""
+    e = golden[name]
+    d = make(e)
+    res = brisk_b200.solve_sdpa(*d.args(), options=opts, verbose=False)
+    check(res, e["runs"][run])
+    C, _ = d.dense_blocks()
+    pobj = 0.0
+    for k, n in enumerate(d.bs.tolist()):
+        if n < 0:
+            x, z = res.X[k], res.Z[k]
+            assert x.shape == (-n,) and z.shape == (-n,)
+            assert x.min() > 0 and z.min() > 0
+            pobj += float(np.diag(C[k]) @ x)
+        else:
+            assert res.X[k].shape == (n, n)
+            pobj += float(np.sum(C[k] * res.X[k]))
+    assert pobj == pytest.approx(res.pobj, rel=1e-9, abs=1e-9)
