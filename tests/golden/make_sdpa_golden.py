@@ -5,7 +5,7 @@ entry, an incomplete last entry, zero values, LP blocks) and its errors (non-int
 out-of-range indices, non-finite values, non-numeric tokens, bad block sizes, short headers).
 
 Runs oracle/_ref/brisk_ref (the reference compiled from its sources by oracle/Makefile) on each
-file with the presolves off and BRISK_WRITEFR set: the reference then writes the problem as read
+file with the presolves off (the elimination of split free variables too) and BRISK_WRITEFR set: the reference then writes the problem as read
 (entries sorted, i <= j, duplicates summed, values at %.17g so every double survives) and exits
 before solving.  Records per case: the file's text, the exit code, the reader's messages (lines
 starting "brisk:"; the file's path replaced by <path>) and, for a file read, m, the block sizes, c
@@ -24,7 +24,7 @@ import tempfile
 ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 REF = os.path.join(ROOT, "oracle", "_ref", "brisk_ref")
 OUT = os.path.join(ROOT, "tests", "golden", "sdpa_reader.json")
-AS_GIVEN = ["-sym", "none", "-symalg", "0", "-chordal", "0", "-nofr", "-deprows", "0"]
+AS_GIVEN = ["-sym", "none", "-symalg", "0", "-chordal", "0", "-nofr", "-deprows", "0", "-freeelim", "0"]
 
 # the base problem: m = 3, blocks of order 3 and 2; every entry below is one of its entries
 BASE_ENTRIES = """0 1 1 1 1.0

@@ -139,3 +139,40 @@ def test_solve_file_reads_with_the_library_reader(tmp_path):
     res = brisk_b200.solve_file(p, verbose=False)
     assert res.exit_code == 2
     assert "non-integer index in entry 2 1 2.5 3 1.5" in res.log
+
+
+REF_EXAMPLES = "/root/reference/examples"
+REF_BIN = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref", "brisk_ref")
+
+
+def _ref_examples():
+    if not os.path.isdir(REF_EXAMPLES):
+        return []
+    return sorted(f for f in os.listdir(REF_EXAMPLES) if f.endswith(".dat-s"))
+
+
+@pytest.mark.skipif(not os.path.exists(REF_BIN) or not _ref_examples(), reason="reference tree or oracle/_ref absent")
+@pytest.mark.parametrize("fname", _ref_examples() or ["-"])
+def test_reader_matches_reference_on_its_example_files(tmp_path, fname):
+    """The reference's own example files (SDPLIB-style headers, braces and commas, LP blocks,
+    comment lines): the reader's numbers equal what oracle/_ref/brisk_ref writes back with
+    BRISK_WRITEFR (presolves off, the elimination of split free variables too), bit for bit after
+    its canonical form."""
+    import subprocess
+    path = os.path.join(REF_EXAMPLES, fname)
+    out = str(tmp_path / "read.dat-s")
+    env = dict(os.environ, BRISK_NOBUSY="1", BRISK_WRITEFR=out)
+    subprocess.run([REF_BIN, path, "-threads", "1", "-nohsd", "-sym", "none", "-symalg", "0", "-chordal", "0",
+                    "-nofr", "-deprows", "0", "-freeelim", "0"], capture_output=True, env=env, timeout=300)
+    assert os.path.exists(out)
+    tok = open(out).read().split()
+    m, nblk = int(tok[0]), int(tok[1])
+    bs = [int(x) for x in tok[2:2 + nblk]]
+    c = [float(x) for x in tok[2 + nblk:2 + nblk + m]]
+    rest = tok[2 + nblk + m:]
+    ents = [[int(rest[q]), int(rest[q + 1]), int(rest[q + 2]), int(rest[q + 3]), float(rest[q + 4])]
+            for q in range(0, len(rest), 5)]
+    d, _ = brisk_b200.read_sdpa_file(path)
+    assert d.m == m and d.bs.tolist() == bs
+    assert [float(x).hex() for x in d.c] == [float(x).hex() for x in c]
+    assert canonical(d) == ref_canonical(ents)
