@@ -92,6 +92,7 @@ struct HProblem {
     long long Ntot = 0;
     // the blocks as given: their sizes (negative: LP) and the first of their blocks here
     std::vector<int> in_n, in_first;
+    bool lp_only = false;   // no SDP block as given
     // the lockstep batch keeps, instead of its one block's entry lists: the constraints as packed
     // upper rows (m x n(n+1)/2) and the start's scalings xi, eta
     std::vector<double, NoInitAlloc<double>> packed;
@@ -263,6 +264,7 @@ static int build_problem(const InputView &in, HProblem &P, std::string &err) {
         nb += in.bs[k] > 0 ? 1 : -in.bs[k];
     }
     P.in_first[nbin] = nb;
+    P.lp_only = std::all_of(in.bs, in.bs + nbin, [](int b) { return b < 0; });
     P.blk.resize(nb);
     for (int k = 0; k < nbin; k++)
         for (int q = P.in_first[k]; q < P.in_first[k + 1]; q++) {
@@ -2144,8 +2146,40 @@ int Solver::run(ResultData &res) {
     CU(cudaEventRecord(evs0, g.st));
     std::vector<double> y(m, 0.0), ybest(m, 0.0), dy, rp(m), a0, h(m, 0.0), rhs(m), qv, ev(m), wv;
     std::vector<double> tmpv;
-    // start_sdpt3 (solver.c:6622-6661)
+    // start_sdpt3 (solver.c:6622-6661).  An LP block as given takes one xi and one eta, from its
+    // order N and the norms over all its variables, for each of its blocks of order 1.
     std::vector<std::vector<double>> sval(6, std::vector<double>(nb, 0.0));
+    std::vector<double> lp_xi(nb, 0.0), lp_eta(nb, 0.0);
+    for (size_t kin = 0; kin < P.in_n.size(); kin++) {
+        if (P.in_n[kin] > 0) continue;
+        const int q0 = P.in_first[kin], q1 = P.in_first[kin + 1];
+        double nC = 0, maxA = 0, ratio = 0;
+        std::vector<double> a2(m, 0.0);
+        std::vector<int> touched;
+        for (int q = q0; q < q1; q++) {
+            const HBlock &B = P.blk[q];
+            for (double v : B.Cval) nC += v * v;
+            for (size_t t = 0; t < B.con.size(); t++) {
+                const int c = B.con[t];
+                if (a2[c] == 0.0) touched.push_back(c);
+                for (long long e = B.cptr[t]; e < B.cptr[t + 1]; e++) a2[c] += B.cval[e] * B.cval[e];
+            }
+        }
+        nC = std::sqrt(nC);
+        std::sort(touched.begin(), touched.end());
+        for (int c : touched) {
+            const double a = std::sqrt(a2[c]);
+            maxA = std::max(maxA, a);
+            ratio = std::max(ratio, (1 + std::fabs(P.b[c])) / (1 + a));
+        }
+        const int n = q1 - q0;
+        const double xi = std::max(10.0, std::max(std::sqrt((double)n), n * ratio));
+        const double eta = std::max(10.0, std::max(std::sqrt((double)n), std::max(maxA, nC)));
+        for (int q = q0; q < q1; q++) {
+            lp_xi[q] = xi;
+            lp_eta[q] = eta;
+        }
+    }
     for (int k = 0; k < nb; k++) {
         const HBlock &B = P.blk[k];
         const int n = B.n;
@@ -2159,8 +2193,9 @@ int Solver::run(ResultData &res) {
             maxA = std::max(maxA, a);
             ratio = std::max(ratio, (1 + std::fabs(P.b[B.con[t]])) / (1 + a));
         }
-        const double xi = std::max(10.0, std::max(std::sqrt((double)n), n * ratio));
-        const double eta = std::max(10.0, std::max(std::sqrt((double)n), std::max(maxA, nC)));
+        const bool lp = lp_xi[k] > 0;
+        const double xi = lp ? lp_xi[k] : std::max(10.0, std::max(std::sqrt((double)n), n * ratio));
+        const double eta = lp ? lp_eta[k] : std::max(10.0, std::max(std::sqrt((double)n), std::max(maxA, nC)));
         DevArrays &d = da[k];
         if (n <= SMALL_N_MAX) {   // set below for all small blocks at once (closed form)
             sval[0][k] = xi;
@@ -2375,7 +2410,9 @@ int Solver::run(ResultData &res) {
         const double mu_a = (xz + ap * dxz + ad * xdz + ap * ad * dxdz) / Ntot;
         const double frac = std::max(0.0, mu_a / mu);
         const double mina = std::min(ap, ad);
-        int rule = opt.sigma_rule < 0 ? 0 : opt.sigma_rule;   // SDP blocks present: the adaptive rule
+        // the default (solver.c:14848-14851): the adaptive rule, the cubic one when the problem
+        // as given has no SDP block (LP blocks only)
+        int rule = opt.sigma_rule < 0 ? (P.lp_only ? 1 : 0) : opt.sigma_rule;
         double expon;
         if (rule == 1) expon = 3.0;
         else if (rule == 2) expon = (mina < 0.1) ? 1.0 : 3.0;

@@ -197,6 +197,7 @@ def solve(data, tol=1e-8, maxit=100, gamma_max=0.99, red_acc=None, log=None, dir
     the first Schur complement M0 (scaled problem)."""
     if red_acc is None:
         red_acc = max(1e-6, 100 * tol)
+    lp_only = all(int(b) < 0 for b in data.bs)   # LP blocks (negative sizes) only
     S = scale_problem(data)
     Xs, Zs, y, xis, etas = start_point(S)
     LX = [np.linalg.cholesky(X) for X in Xs]
@@ -315,7 +316,12 @@ def solve(data, tol=1e-8, maxit=100, gamma_max=0.99, red_acc=None, log=None, dir
         mu_a = (xz + ap * dxz + ad * xdz + ap * ad * dxdz) / Ntot
         frac = max(0.0, mu_a / mu)
         mina = min(ap, ad)
-        expon = max(1.0, 3 * mina * mina) if relgap > 1e-6 else 3.0
+        # the default sigma rule (solver.c:14848-14855): cubic when the problem has no SDP block
+        # (only LP blocks), else adaptive
+        if lp_only:
+            expon = 3.0
+        else:
+            expon = max(1.0, 3 * mina * mina) if relgap > 1e-6 else 3.0
         sigma = min(1.0, frac ** expon)
         gamma = 0.9 + (gamma_max - 0.9) * mina
         smu = sigma * mu

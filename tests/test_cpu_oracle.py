@@ -123,3 +123,23 @@ def test_generators_match_workload_shapes():
     sizes = problems.random_dense_batch(count=64, seed=0, sizes_only=True)
     for n, m in sizes:
         assert 8 <= n <= 64 and n <= m <= n * (n + 1) // 4
+
+
+@pytest.mark.parametrize("name", ["lp_mixed", "lp_only"])
+@pytest.mark.parametrize("run,direction", [("init0", "hkm"), ("nt_init0", "nt")])
+def test_oracle_lp_blocks_match_reference(golden, name, run, direction):
+    """LP blocks (negative sizes) in the restatement: a dense block with diagonal data, whose
+    iterates stay diagonal (the LP's own iteration), and the reference's sigma rule for problems
+    with LP blocks only (cubic, solver.c:14848-14851).  The reference's -init 0 runs are followed
+    to every printed digit: same status and iterations, the first four table rows."""
+    e = golden[name]
+    ref = e["runs"][run]
+    out = restate.solve(make(e), tol=1e-7, direction=direction)
+    assert out["status_str"] == ref["status"] == "OPTIMAL"
+    assert out["iterations"] == ref["iterations"]
+    den = 1 + abs(ref["pobj"]) + abs(ref["dobj"])
+    assert abs(out["pobj"] - ref["pobj"]) <= 1e-9 * den
+    assert abs(out["dobj"] - ref["dobj"]) <= 1e-9 * den
+    for mine, theirs in zip(out["table"][:4], ref["rows"][:4]):
+        assert mine["pobj"] == pytest.approx(theirs["pobj"], rel=1e-8, abs=1e-8)
+        assert mine["dobj"] == pytest.approx(theirs["dobj"], rel=1e-8, abs=1e-8)

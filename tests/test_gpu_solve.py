@@ -99,16 +99,19 @@ NT = ["-nohsd", "-dir", "nt", "-mixed", "0", "-tol", "1e-7"]
 
 
 @pytest.mark.parametrize("name", ["lp_mixed", "lp_only"])
-@pytest.mark.parametrize("run,opts", [("default", FP64), ("init0", FP64 + ["-init", "0"]), ("nt", NT)])
+@pytest.mark.parametrize("run,opts", [("default", FP64), ("init0", FP64 + ["-init", "0"]), ("nt", NT),
+                                      ("nt_init0", NT + ["-init", "0"])])
 def test_lp_blocks_match_reference(golden, name, run, opts):
-    """LP blocks (negative sizes; here each variable a block of order 1) against the reference's
-    solves of the same problems: status, objectives, DIMACS.  An LP block's X and Z come back as
-    vectors (brisk_result_X: "n for LP", capi.c:131), of positive values at an interior point,
-    and <C, X> summed from the blocks returned is pobj."""
+    """LP blocks (negative sizes; here each variable a block of order 1, with its LP block's start
+    scalings and, for LP blocks only, the cubic sigma rule) against the reference's solves of the
+    same problems: status, objectives, DIMACS and the same iteration count.  An LP block's X and Z
+    come back as vectors (brisk_result_X: "n for LP", capi.c:131), of positive values at an
+    interior point, and <C, X> summed from the blocks returned is pobj."""
     e = golden[name]
     d = make(e)
     res = brisk_b200.solve_sdpa(*d.args(), options=opts, verbose=False)
     check(res, e["runs"][run])
+    assert res.iterations == e["runs"][run]["iterations"]
     C, _ = d.dense_blocks()
     pobj = 0.0
     for k, n in enumerate(d.bs.tolist()):
