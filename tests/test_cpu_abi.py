@@ -52,8 +52,10 @@ def test_bad_input_is_rejected_before_any_gpu_work(libpath):
     # a bad option returns exit code 1 without touching the device
     res = _core.solve_sdpa([2], [1.0], [1], [1], [1], [1], [1.0], options=["-tol", "x"], verbose=False)
     assert res.exit_code == 1
-    # LP blocks are outside this build: input error 2
-    res = _core.solve_sdpa([-2], [1.0], [1], [1], [1], [1], [1.0], verbose=False)
+    # an LP block takes diagonal entries only, and no block has size 0: input error 2
+    res = _core.solve_sdpa([-2], [1.0], [1], [1], [1], [2], [1.0], verbose=False)
+    assert res.exit_code == 2 and "off-diagonal entry in LP block" in res.log
+    res = _core.solve_sdpa([2, 0], [1.0], [1], [1], [1], [1], [1.0], verbose=False)
     assert res.exit_code == 2
 
 
