@@ -100,12 +100,35 @@ struct HProblem {
     double xi0 = 0, eta0 = 0;
 };
 
+// The messages of brisk_solve_data's checks of an entry (problem.c, problem_from_sdpa_data), with
+// the entry as given: why 1 a value not finite, 2 an index out of range, 3 an LP entry off the
+// diagonal.
+static std::string entry_fault(const InputView &in, long long e, int why) {
+    char s[128];
+    if (why == 1)
+        std::snprintf(s, sizeof s, "non-finite value in entry %d %d %d %d", in.mat[e], in.blk[e], in.i[e], in.j[e]);
+    else if (why == 2)
+        std::snprintf(s, sizeof s, "bad entry %d %d %d %d", in.mat[e], in.blk[e], in.i[e], in.j[e]);
+    else
+        std::snprintf(s, sizeof s, "off-diagonal entry in LP block");
+    return s;
+}
+
+// c[i] not finite (problem.c, problem_from_sdpa_data): its message, or "" when every c[i] is finite.
+static std::string c_fault(const InputView &in) {
+    for (int i = 0; i < in.m; i++)
+        if (!std::isfinite(in.c[i])) return "non-finite value c[" + std::to_string(i + 1) + "]";
+    return "";
+}
+
 // build_problem for a problem of one SDP block, straight from the caller's arrays into the packed
 // rows of the lockstep batch (the same checks, duplicate sums in input order, problem_prepare
 // scaling and start_sdpt3 scalings; the row norms are summed over the packed upper entries).
 static int build_packed(const InputView &in, HProblem &P, std::string &err) {
     const int m = in.m, n = in.bs[0];
     if (in.nblk != 1 || n <= 0) { err = "not a one-block problem"; return 2; }
+    err = c_fault(in);
+    if (!err.empty()) return 2;
     const int t = n * (n + 1) / 2;
     P = HProblem();
     P.m = m;
@@ -119,11 +142,11 @@ static int build_packed(const InputView &in, HProblem &P, std::string &err) {
     std::vector<double> Cu(t, 0.0);
     for (long long e = 0; e < in.nnz; e++) {
         const double v = in.v[e];
+        if (!std::isfinite(v)) { err = entry_fault(in, e, 1); return 2; }
         if (v == 0) continue;
         const int k = in.blk[e] - 1, mt = in.mat[e];
-        if (k != 0 || mt < 0 || mt > m) { err = "entry out of range"; return 2; }
         int i = in.i[e], j = in.j[e];
-        if (i < 1 || j < 1 || i > n || j > n) { err = "entry index out of the block"; return 2; }
+        if (k != 0 || mt < 0 || mt > m || i < 1 || j < 1 || i > n || j > n) { err = entry_fault(in, e, 2); return 2; }
         if (i > j) std::swap(i, j);
         const size_t u = (size_t)(j - 1) * j / 2 + (i - 1);
         if (mt == 0) {
@@ -250,6 +273,8 @@ static int host_threads(long long work) {
 static int build_problem(const InputView &in, HProblem &P, std::string &err) {
     const int nbin = in.nblk, m = in.m;
     P.m = m;
+    err = c_fault(in);
+    if (!err.empty()) return 2;
     P.b0.assign(in.c, in.c + m);
     P.b = P.b0;
     // An LP block of size N (a negative size, brisk.h:128-140) is N semidefinite blocks of order 1:
@@ -296,20 +321,23 @@ static int build_problem(const InputView &in, HProblem &P, std::string &err) {
     const long long nnz = in.nnz;
     int T = host_threads(nnz);
     while (T > 1 && (double)T * nb * sizeof(long long) > 256e6) T--;   // the counts: at most 256 MB
-    struct Chunk { std::vector<long long> cnt; long long nz = 0; int why = 0, k0 = -1, k1 = -1; bool sorted = true; };
+    struct Chunk { std::vector<long long> cnt; long long nz = 0, bad = -1; int why = 0, k0 = -1, k1 = -1; bool sorted = true; };
     std::vector<Chunk> ch(T);
     run_chunks(T, [&](int t) {
         Chunk &c = ch[t];
         c.cnt.assign(nb, 0);
         int prev = -1;
         for (long long e = nnz * t / T, hi = nnz * (t + 1) / T; e < hi; e++) {
+            // the checks in the reference's order: a finite value, then (for a nonzero one) the
+            // indices, then an LP entry's place on the diagonal
+            if (!std::isfinite(in.v[e])) { c.why = 1; c.bad = e; return; }
             if (in.v[e] == 0) continue;
             const int kin = in.blk[e] - 1, mt = in.mat[e];
-            if (kin < 0 || kin >= nbin || mt < 0 || mt > m) { c.why = 1; return; }
-            const int n = std::abs(bsz[kin]);
             const int i = in.i[e], j = in.j[e];
-            if (i < 1 || j < 1 || i > n || j > n) { c.why = 2; return; }
-            if (bsz[kin] < 0 && i != j) { c.why = 3; return; }
+            if (kin < 0 || kin >= nbin || mt < 0 || mt > m) { c.why = 2; c.bad = e; return; }
+            const int n = std::abs(bsz[kin]);
+            if (i < 1 || j < 1 || i > n || j > n) { c.why = 2; c.bad = e; return; }
+            if (bsz[kin] < 0 && i != j) { c.why = 3; c.bad = e; return; }
             const int k = block_here(e);
             if (prev < 0) c.k0 = k;
             c.sorted = c.sorted && k >= prev;
@@ -321,8 +349,7 @@ static int build_problem(const InputView &in, HProblem &P, std::string &err) {
     });
     for (int t = 0; t < T; t++)
         if (ch[t].why) {
-            err = ch[t].why == 1 ? "entry out of range"
-                  : ch[t].why == 2 ? "entry index out of the block" : "off-diagonal entry in LP block";
+            err = entry_fault(in, ch[t].bad, ch[t].why);
             return 2;
         }
     bool by_block = true;

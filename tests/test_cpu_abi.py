@@ -112,3 +112,37 @@ def test_batch_entry_checks_before_any_gpu_work(libpath):
     with pytest.raises(RuntimeError):
         brisk_b200.solve_batch_arrays(**arrs, options=["-tol", "abc"])
     assert int(arrs["nnz"].sum()) == arrs["v"].size and list(arrs["m"]) == [11, 15]
+
+
+def _solve_data_raw(bs, c, mat, blk, i, j, v):
+    """brisk_solve_data called straight through ctypes (no Python-side checks); returns the Result."""
+    from brisk_b200 import _core
+    bs = np.ascontiguousarray(bs, dtype=np.intc)
+    c = np.ascontiguousarray(c, dtype=np.float64)
+    arrs = [np.ascontiguousarray(a, dtype=np.intc) for a in (mat, blk, i, j)]
+    v = np.ascontiguousarray(v, dtype=np.float64)
+    pi, pd = ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)
+    return _core._run(lambda L, n, a, r: L.brisk_solve_data(
+        int(c.size), int(bs.size), bs.ctypes.data_as(pi), c.ctypes.data_as(pd), int(v.size),
+        arrs[0].ctypes.data_as(pi), arrs[1].ctypes.data_as(pi), arrs[2].ctypes.data_as(pi),
+        arrs[3].ctypes.data_as(pi), v.ctypes.data_as(pd), n, a, r), None, False)
+
+
+def test_solve_data_checks_entries_as_the_reference(libpath):
+    """The checks of problem_from_sdpa_data (problem.c) in its order and with its messages, on the
+    host before any GPU work: a value not finite (even where the indices are bad), c not finite,
+    an index out of range ("bad entry" with the entry as given), an LP entry off the diagonal;
+    exit code 2."""
+    r = _solve_data_raw([3], [1.0], [1, 1], [1, 1], [1, 9], [1, 9], [1.0, np.nan])
+    assert r.exit_code == 2 and "non-finite value in entry 1 1 9 9" in r.log
+    r = _solve_data_raw([3], [np.inf], [1], [1], [1], [1], [1.0])
+    assert r.exit_code == 2 and "non-finite value c[1]" in r.log
+    r = _solve_data_raw([3], [1.0], [0, 1], [1, 1], [1, 4], [1, 1], [2.0, 1.0])
+    assert r.exit_code == 2 and "bad entry 1 1 4 1" in r.log
+    r = _solve_data_raw([3], [1.0], [2], [1], [1], [1], [1.0])
+    assert r.exit_code == 2 and "bad entry 2 1 1 1" in r.log
+    # zero values are no entries: not checked (the reference skips them before its range test)
+    r = _solve_data_raw([3], [1.0], [7, 1], [5, 1], [0, 1], [0, 1], [0.0, np.nan])
+    assert r.exit_code == 2 and "non-finite value in entry 1 1 1 1" in r.log
+    r = _solve_data_raw([-2], [1.0], [1], [1], [1], [2], [1.0])
+    assert r.exit_code == 2 and "off-diagonal entry in LP block" in r.log
