@@ -197,7 +197,15 @@ int parse_options(int argc, const char *const *argv, Options &opt, std::string &
             // options of the reference that take a value and do not change this path's arithmetic
             if (!need("a value")) return 1;
         } else {
-            log_printf(1, "brisk: note: option %s is not used by the GPU Newton step (ignored)\n", a.c_str());
+            // another of the reference's options (OPTIONS.md's table): its value, if it has one,
+            // is the next argument when that is no option (a word, or a number such as -1)
+            std::string shown = a;
+            if (i + 1 < argc && argv[i + 1]) {
+                const char *nx = argv[i + 1];
+                const bool is_option = nx[0] == '-' && nx[1] != '\0' && !std::isdigit((unsigned char)nx[1]) && nx[1] != '.';
+                if (!is_option) shown += std::string(" ") + argv[++i];
+            }
+            log_printf(1, "brisk: note: option %s is not used by the GPU Newton step (ignored)\n", shown.c_str());
         }
     }
     if (tol_given && 100.0 * opt.tol > opt.red_acc) opt.red_acc = 100.0 * opt.tol;

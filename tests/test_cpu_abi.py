@@ -146,3 +146,20 @@ def test_solve_data_checks_entries_as_the_reference(libpath):
     assert r.exit_code == 2 and "non-finite value in entry 1 1 1 1" in r.log
     r = _solve_data_raw([-2], [1.0], [1], [1], [1], [2], [1.0])
     assert r.exit_code == 2 and "off-diagonal entry in LP block" in r.log
+
+
+def test_other_reference_options_take_their_values(libpath):
+    """An option of the reference that this path does not use is passed over with its value (the
+    next argument when it is no option: a word or a number such as -1), in one note; the options
+    after it are still read (a bad -tol then stops the call with exit code 1 before any GPU work)."""
+    from brisk_b200 import _core
+    res = _core.solve_sdpa([2], [1.0], [1], [1], [1], [1], [1.0],
+                           options=["-freeelim", "0", "-lpmethod", "-1", "-lralm", "yes", "-nosuchflag", "-tol", "x"],
+                           verbose=False)
+    assert res.exit_code == 1
+    assert "option -freeelim 0 is not used" in res.log
+    assert "option -lpmethod -1 is not used" in res.log
+    assert "option -lralm yes is not used" in res.log
+    assert "option -nosuchflag is not used" in res.log
+    assert "option 0 " not in res.log and "option yes" not in res.log
+    assert "bad -tol" in res.log
