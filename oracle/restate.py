@@ -97,6 +97,45 @@ def start_point(S: Scaled):
     return X, Z, np.zeros(S.m), xis, etas
 
 
+def start_least_squares(S: Scaled):
+    """The least-squares start (init 1, the default, solver.c:13939-14198), with exact solves and
+    exact eigenvalues: dy = (A A')^-1 b and y = (A A')^-1 A(C) (A A' the Schur complement at
+    X = Zi = I); with ax, az the largest -lambda_min over the blocks of X0 = A'dy and Z0 = C - A'y,
+    X0 is shifted by 1 + ax when ax >= -1e-8 (else kept) and Z0 by max(0, 1 + az)
+    (solver.c:14099-14104); then each block's X0, Z0 is raised by 1e-8, 1e-7, ... on the diagonal
+    until a Cholesky factor exists (solver.c:14190-14199).  None when A A' has no Cholesky factor (the
+    reference then takes the SDPT3 start).  The reference solves by CG to 1e-10 first (its direct
+    solve when that misses 1e-3) and takes lmin by Lanczos for blocks above order 32: the same
+    start to that accuracy, exactly the same shifts where every block has order <= 32."""
+    eye = [np.eye(Ck.shape[0]) for Ck in S.C]
+    G = schur(S.A, eye, eye)
+    try:
+        np.linalg.cholesky(G)
+    except np.linalg.LinAlgError:
+        return None
+    dy = np.linalg.solve(G, S.b)
+    y = np.linalg.solve(G, aop(S.A, S.C))
+    X = atop(S.A, dy)
+    Z = [Ck - a for Ck, a in zip(S.C, atop(S.A, y))]
+    ax = max(-float(np.linalg.eigvalsh(0.5 * (Xk + Xk.T))[0]) for Xk in X)
+    az = max(-float(np.linalg.eigvalsh(0.5 * (Zk + Zk.T))[0]) for Zk in Z)
+    shx = 1.0 + ax if ax >= -1e-8 else 0.0
+    shz = max(0.0, 1.0 + az)
+    X = [Xk + shx * I for Xk, I in zip(X, eye)]
+    Z = [Zk + shz * I for Zk, I in zip(Z, eye)]
+    for V in (X, Z):
+        for k, I in enumerate(eye):
+            extra = 1e-8
+            while True:
+                try:
+                    np.linalg.cholesky(V[k])
+                    break
+                except np.linalg.LinAlgError:
+                    V[k] = V[k] + extra * I
+                    extra *= 10
+    return X, Z, y
+
+
 def schur(A_blocks, X_blocks, Zi_blocks):
     """M_ij = sum_blocks <A_i, X A_j Zi> (the HKM Schur complement, dense formula)."""
     m = A_blocks[0].shape[0]
@@ -184,7 +223,7 @@ STATUS = {0: "OPTIMAL", 1: "PRIMAL INFEASIBLE", 2: "DUAL INFEASIBLE", 3: "ITERAT
           4: "NUMERICAL DIFFICULTIES", 5: "REDUCED ACCURACY", 6: "TIME LIMIT"}
 
 
-def solve(data, tol=1e-8, maxit=100, gamma_max=0.99, red_acc=None, log=None, direction="hkm"):
+def solve(data, tol=1e-8, maxit=100, gamma_max=0.99, red_acc=None, log=None, direction="hkm", init=0):
     """The infeasible-start predictor-corrector loop (solver.c:14394-15188), FP64, dense, with the
     HKM direction or (direction="nt") the NT direction in the scaled space: the scaling W = G G'
     from nt_scaling each iteration (solver.c:14403-14410), the Schur complement at X = Zi = W
@@ -200,6 +239,10 @@ def solve(data, tol=1e-8, maxit=100, gamma_max=0.99, red_acc=None, log=None, dir
     lp_only = all(int(b) < 0 for b in data.bs)   # LP blocks (negative sizes) only
     S = scale_problem(data)
     Xs, Zs, y, xis, etas = start_point(S)
+    if init >= 1 and S.m > 0:   # the least-squares start (the reference's default)
+        ls = start_least_squares(S)
+        if ls is not None:
+            Xs, Zs, y = ls
     LX = [np.linalg.cholesky(X) for X in Xs]
     LZ = [np.linalg.cholesky(Z) for Z in Zs]
     m = S.m

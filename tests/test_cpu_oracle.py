@@ -143,3 +143,23 @@ def test_oracle_lp_blocks_match_reference(golden, name, run, direction):
     for mine, theirs in zip(out["table"][:4], ref["rows"][:4]):
         assert mine["pobj"] == pytest.approx(theirs["pobj"], rel=1e-8, abs=1e-8)
         assert mine["dobj"] == pytest.approx(theirs["dobj"], rel=1e-8, abs=1e-8)
+
+
+@pytest.mark.parametrize("name", ["theta30", "rand30", "mom8", "lp_mixed", "lp_only", "batch_q5"])
+@pytest.mark.parametrize("run,direction", [("default", "hkm"), ("nt", "nt")])
+def test_oracle_default_start_matches_reference(golden, name, run, direction):
+    """The least-squares start (the reference's default, solver.c:13939-14198) in the restatement:
+    where every block has order <= 32 (the reference's eigenvalues and step lengths then exact, as
+    the oracle's), its default runs are followed row by row over the whole iteration table, HKM and
+    NT: the same status and iterations, pobj and dobj of every row to the printed digits."""
+    e = golden[name]
+    ref = e["runs"][run]
+    d = make(e)
+    assert max(abs(int(b)) if b > 0 else 1 for b in d.bs) <= 32
+    out = restate.solve(d, tol=1e-7, direction=direction, init=1)
+    assert out["status_str"] == ref["status"] == "OPTIMAL"
+    assert out["iterations"] == ref["iterations"]
+    assert len(out["table"]) == len(ref["rows"])
+    for mine, theirs in zip(out["table"], ref["rows"]):
+        assert mine["pobj"] == pytest.approx(theirs["pobj"], rel=1e-7, abs=1e-8)
+        assert mine["dobj"] == pytest.approx(theirs["dobj"], rel=1e-7, abs=1e-8)
