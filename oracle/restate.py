@@ -97,7 +97,7 @@ def start_point(S: Scaled):
     return X, Z, np.zeros(S.m), xis, etas
 
 
-def start_least_squares(S: Scaled):
+def start_least_squares(S: Scaled, lp=None):
     """The least-squares start (init 1, the default, solver.c:13939-14198), with exact solves and
     exact eigenvalues: dy = (A A')^-1 b and y = (A A')^-1 A(C) (A A' the Schur complement at
     X = Zi = I); with ax, az the largest -lambda_min over the blocks of X0 = A'dy and Z0 = C - A'y,
@@ -117,8 +117,9 @@ def start_least_squares(S: Scaled):
     y = np.linalg.solve(G, aop(S.A, S.C))
     X = atop(S.A, dy)
     Z = [Ck - a for Ck, a in zip(S.C, atop(S.A, y))]
-    ax = max(-float(np.linalg.eigvalsh(0.5 * (Xk + Xk.T))[0]) for Xk in X)
-    az = max(-float(np.linalg.eigvalsh(0.5 * (Zk + Zk.T))[0]) for Zk in Z)
+    lp = lp if lp is not None else [False] * len(X)
+    ax = max(-block_lam_min(None, Xk, f) for Xk, f in zip(X, lp))
+    az = max(-block_lam_min(None, Zk, f) for Zk, f in zip(Z, lp))
     shx = 1.0 + ax if ax >= -1e-8 else 0.0
     shz = max(0.0, 1.0 + az)
     X = [Xk + shx * I for Xk, I in zip(X, eye)]
@@ -154,6 +155,11 @@ def atop(A_blocks, y):
     return [np.einsum("t,tij->ij", y, Ak) for Ak in A_blocks]
 
 
+SMALL_BLOCK = 32     # solver.c:5944: exact eigenvalues up to this order
+LANCZOS_K = 30       # solver.c:81, and the default -lanczos (solver.c:122)
+LZ_TOL = 0.02        # solver.c:6041: the relative Ritz accuracy that ends the Lanczos steps
+
+
 def lam_min(L, D):
     """lambda_min(L^-1 D L^-T) (exact)."""
     Li = np.linalg.inv(L)
@@ -161,11 +167,74 @@ def lam_min(L, D):
     return float(np.linalg.eigvalsh(0.5 * (B + B.T))[0])
 
 
-def maxstep(Ls, dVs):
-    """maxstep (solver.c:6300-6390) with exact eigenvalues: 1e30 when unbounded."""
+def _ritz_bound(alpha, beta, kk):
+    """ritz_bound (solver.c:6030-6039): theta, the smallest eigenvalue of the tridiagonal
+    T_kk, and |beta_kk z_kk| for its unit eigenvector z."""
+    T = np.diag(alpha[:kk]) + np.diag(beta[:kk - 1], 1) + np.diag(beta[:kk - 1], -1)
+    w, V = np.linalg.eigh(T)
+    return abs(beta[kk - 1] * V[kk - 1, 0]), float(w[0])
+
+
+def lam_min_lanczos(L, D, kmax=LANCZOS_K):
+    """sdp_maxstep_lam for blocks above SMALL_BLOCK (solver.c:6083-6225), cold start: Lanczos on
+    L^-1 D L^-T (on D when L is None; D read by its lower triangle, as dsymv) from the fixed
+    vector q_i = 1 + 0.5 sin(1.7 i + 0.3), normalised; each new vector orthogonalised twice against
+    all earlier ones; stopped when beta <= 1e-12 max|alpha|, or from the sixth step every third
+    step when the Ritz bound res <= 0.02 |theta| + 1e-14 max|alpha|.  Returns theta - res, the
+    reference's conservative estimate of lambda_min."""
+    from scipy.linalg import solve_triangular
+    n = D.shape[0]
+    K = min(n, kmax, LANCZOS_K)
+    Dl = np.tril(D) + np.tril(D, -1).T
+    i = np.arange(n)
+    q = 1.0 + 0.5 * np.sin(1.7 * i + 0.3)
+    Q = [q / np.linalg.norm(q)]
+    alpha, beta = [], []
+    scale, kk = 0.0, 0
+    for j in range(K):
+        v = Q[j] if L is None else solve_triangular(L, Q[j], trans="T", lower=True)
+        w = Dl @ v
+        if L is not None:
+            w = solve_triangular(L, w, lower=True)
+        a = float(Q[j] @ w)
+        alpha.append(a)
+        for _ in range(2):
+            for qi in Q[:j + 1]:
+                w = w - float(qi @ w) * qi
+        b = float(np.linalg.norm(w))
+        beta.append(b)
+        kk = j + 1
+        scale = max(scale, abs(a))
+        if b <= 1e-12 * (scale + 1e-300):
+            beta[j] = 0.0
+            break
+        if kk >= 6 and kk % 3 == 0:
+            res, theta = _ritz_bound(alpha, beta, kk)
+            if res <= LZ_TOL * abs(theta) + 1e-14 * scale:
+                break
+        if j + 1 < K:
+            Q.append(w / b)
+    res, theta = _ritz_bound(alpha, beta, kk)
+    return theta - res
+
+
+def block_lam_min(L, D, lp=False):
+    """The reference's lambda_min of L^-1 D L^-T for one block: exact up to order SMALL_BLOCK
+    (small_lammin) and for an LP block (the ratio test of lp_maxstep, solver.c:6227-6235, on its
+    diagonal), the Lanczos estimate above (sdp_maxstep_lam).  L None: of D itself."""
+    n = D.shape[0]
+    if n <= SMALL_BLOCK or lp:
+        if L is None:
+            return float(np.linalg.eigvalsh(0.5 * (D + D.T))[0])
+        return lam_min(L, D)
+    return lam_min_lanczos(L, D)
+
+
+def maxstep(Ls, dVs, lp=None):
+    """maxstep (solver.c:6300-6390): 1e30 when unbounded.  lp[k]: block k is an LP block."""
     a = 1e30
-    for L, dV in zip(Ls, dVs):
-        lam = lam_min(L, dV)
+    for k, (L, dV) in enumerate(zip(Ls, dVs)):
+        lam = block_lam_min(L, dV, bool(lp[k]) if lp is not None else False)
         ak = 1e30 if lam >= 0 else -1.0 / lam
         a = min(a, ak)
     return a
@@ -236,11 +305,12 @@ def solve(data, tol=1e-8, maxit=100, gamma_max=0.99, red_acc=None, log=None, dir
     the first Schur complement M0 (scaled problem)."""
     if red_acc is None:
         red_acc = max(1e-6, 100 * tol)
-    lp_only = all(int(b) < 0 for b in data.bs)   # LP blocks (negative sizes) only
+    lp = [int(b) < 0 for b in data.bs]          # LP blocks (negative sizes)
+    lp_only = all(lp)
     S = scale_problem(data)
     Xs, Zs, y, xis, etas = start_point(S)
     if init >= 1 and S.m > 0:   # the least-squares start (the reference's default)
-        ls = start_least_squares(S)
+        ls = start_least_squares(S, lp)
         if ls is not None:
             Xs, Zs, y = ls
     LX = [np.linalg.cholesky(X) for X in Xs]
@@ -351,8 +421,8 @@ def solve(data, tol=1e-8, maxit=100, gamma_max=0.99, red_acc=None, log=None, dir
             for Zk, dZk, Xk in zip(Zi, dZ, Xs):
                 G = Zk @ dZk @ Xk
                 dX.append(-0.5 * (G + G.T) - Xk)
-        ap = min(1.0, maxstep(LX, dX))
-        ad = min(1.0, maxstep(LZ, dZ))
+        ap = min(1.0, maxstep(LX, dX, lp))
+        ad = min(1.0, maxstep(LZ, dZ, lp))
         xdz = sum(float(np.sum(a * b)) for a, b in zip(Xs, dZ))
         dxz = sum(float(np.sum(a * b)) for a, b in zip(dX, Zs))
         dxdz = sum(float(np.sum(a * b)) for a, b in zip(dX, dZ))
@@ -408,8 +478,8 @@ def solve(data, tol=1e-8, maxit=100, gamma_max=0.99, red_acc=None, log=None, dir
             dy = dy + wv
             dZ = [a - b for a, b in zip(dZ, Qd)]
             dX = [a + b for a, b in zip(dX, Gs)]
-        apr = min(1.0, maxstep(LX, dX))
-        adr = min(1.0, maxstep(LZ, dZ))
+        apr = min(1.0, maxstep(LX, dX, lp))
+        adr = min(1.0, maxstep(LZ, dZ, lp))
         apn, adn = min(1.0, gamma * apr), min(1.0, gamma * adr)
         if pinf < 1e-6:
             ev = rp - aop(S.A, dX)

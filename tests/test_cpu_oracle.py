@@ -145,21 +145,22 @@ def test_oracle_lp_blocks_match_reference(golden, name, run, direction):
         assert mine["dobj"] == pytest.approx(theirs["dobj"], rel=1e-8, abs=1e-8)
 
 
-@pytest.mark.parametrize("name", ["theta30", "rand30", "mom8", "dense24", "lp_mixed", "lp_only", "batch_q3", "batch_q5"])
+@pytest.mark.parametrize("name", ["theta30", "rand30", "mom8", "dense24", "lp_mixed", "lp_only", "batch_q3", "batch_q5",
+                                  "batch_q2", "batch_q1"])
 @pytest.mark.parametrize("run,direction,init", [("default", "hkm", 1), ("nt", "nt", 1), ("init0", "hkm", 0),
                                                 ("nt_init0", "nt", 0)])
 def test_oracle_follows_reference_row_by_row(golden, name, run, direction, init):
-    """Where every block has order <= 32 (the reference's eigenvalues and step lengths are then
-    exact, as the oracle's), the restatement follows the reference's runs row by row over the
-    whole iteration table, from both starts (the least-squares start, the reference's default,
-    solver.c:13939-14198; the SDPT3 start, -init 0) and in both directions: the same status and
-    iterations, pobj and dobj of every row to the printed digits."""
+    """The restatement follows the reference's runs row by row over the whole iteration table,
+    from both starts (the least-squares start, the reference's default, solver.c:13939-14198; the
+    SDPT3 start, -init 0) and in both directions: the same status and iterations, pobj and dobj of
+    every row to the printed digits.  Blocks of order <= 32 take exact eigenvalues, larger ones the
+    reference's Lanczos estimate (batch_q2: n = 37, batch_q1: n = 44), in the step lengths and in
+    the least-squares start's shifts."""
     e = golden[name]
     if run not in e["runs"]:
         pytest.skip("run not in the fixtures")
     ref = e["runs"][run]
     d = make(e)
-    assert max(abs(int(b)) if b > 0 else 1 for b in d.bs) <= 32
     out = restate.solve(d, tol=1e-7, direction=direction, init=init)
     assert out["status_str"] == ref["status"] == "OPTIMAL"
     assert out["iterations"] == ref["iterations"]
