@@ -36,6 +36,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 WORKLOADS = {
+    "theta50": dict(kind="theta", gen=dict(n=50, p=0.5, seed=1),
+                    desc="Lovasz theta SDP of a seeded G(50, 0.5): one 50x50 block, m=588 (tr X = 1 and one "
+                         "constraint X_ij = 0 per edge), C = -J",
+                    paths={"fp64": ["-mixed", "0"]}, primary="fp64"),
     "rand400": dict(kind="random", gen=dict(n=400, m=2000, density=0.01, seed=0),
                     desc="random SDP: one 400x400 block, m=2000, A_i 1% dense N(0,1), b=A(I), C=GG'/n+I, seed 0",
                     paths={"fp64": ["-mixed", "0"]}, primary="fp64"),
@@ -61,6 +65,8 @@ def make_instance(w):
     from brisk_b200 import problems
     if w["kind"] == "moment":
         return problems.moment_relaxation(**w["gen"])
+    if w["kind"] == "theta":
+        return problems.theta_problem(**w["gen"])
     return problems.random_sdp(**w["gen"])
 BASE_OPTS = ["-nohsd", "-dir", "hkm", "-tol", "1e-7", "-q"]
 
