@@ -7,14 +7,18 @@ calls it and has no CPU path.
 It restates, on dense matrices (small sizes: tests), the reference BRISK 1.7 algorithm:
 
 * problem_prepare        row equilibration and b/C scaling         problem.c:1866-1910
-* start_sdpt3            X0 = xi I, Z0 = eta I, y = 0               solver.c:6622-6661
+* start_sdpt3            X0 = xi I, Z0 = eta I, y = 0 (-init 0)     solver.c:6622-6661
+* the least-squares start (the default) from A A' and shifts         solver.c:13939-14198
 * schur (HKM)            M_ij = <A_i, X A_j Z^-1>                    solver.c:1969, 2339-3021
 * the infeasible-start predictor-corrector loop, HKM or NT          solver.c:14394-15188
   (residuals 14423-14484, theta R0 recurrence 14317-14326 / 14587-14607, rhs pieces
   14715-14735, predictor 14787-14818, sigma rule 14829-14873, corrector 14998-15050,
   refinement of A(dX) = rp 15058-15105, try_step 6393-6447)
 * maxstep                the largest alpha with V + alpha dV >= 0     solver.c:6300-6390
-  (exact eigenvalues here; the reference's Lanczos estimate theta - residual is <= it)
+  (exact eigenvalues up to order 32 and for LP blocks; above, the Lanczos   solver.c:6083-6225
+  estimate theta - residual, as the reference takes it)
+* LP blocks (negative sizes) as dense blocks of diagonal data, their iterates diagonal, and the
+  cubic sigma rule for problems of LP blocks only                      solver.c:14848-14851
 * nt_scaling             the NT scaling G, lam, W = G G' from the     solver.c:7824-7912
                          factors of X and Z (eigenvectors of Mb' Mb,
                          Mb = L_Z' L_X; lam descending)
@@ -23,8 +27,9 @@ It restates, on dense matrices (small sizes: tests), the reference BRISK 1.7 alg
 
 Pinned against the reference's own runs on the same seeded inputs (tests/golden/, made by
 tests/golden/make_golden.py from oracle/_ref/brisk_ref, the reference compiled by
-oracle/Makefile), and against the reference's published golden value for theta1
-(INSTALL.md:44-45).
+oracle/Makefile): their iteration tables are followed row by row, from both starts and in both
+directions (tests/test_cpu_oracle.py); and against the reference's published golden value for
+theta1 (INSTALL.md:44-45).
 """
 from __future__ import annotations
 
