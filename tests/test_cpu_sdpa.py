@@ -176,3 +176,34 @@ def test_reader_matches_reference_on_its_example_files(tmp_path, fname):
     assert d.m == m and d.bs.tolist() == bs
     assert [float(x).hex() for x in d.c] == [float(x).hex() for x in c]
     assert canonical(d) == ref_canonical(ents)
+
+
+def test_reader_takes_a_pipe(tmp_path):
+    """A file that is not a regular one (a named pipe: no size to split by) is read to its end on
+    one thread, with the same result as the regular file."""
+    import threading
+    text = GOLD["sdplib_style"]["text"]
+    reg = _w(tmp_path, "reg.dat-s", text)
+    fifo = str(tmp_path / "pipe.dat-s")
+    os.mkfifo(fifo)
+
+    def feed():
+        with open(fifo, "w", newline="") as f:
+            f.write(text)
+
+    th = threading.Thread(target=feed)
+    th.start()
+    d_pipe, _ = brisk_b200.read_sdpa_file(fifo)
+    th.join(timeout=30)
+    d_reg, _ = brisk_b200.read_sdpa_file(reg)
+    for a, b in zip(arrays(d_pipe), arrays(d_reg)):
+        np.testing.assert_array_equal(a, b)
+    np.testing.assert_array_equal(d_pipe.c, d_reg.c)
+    assert d_pipe.bs.tolist() == d_reg.bs.tolist()
+
+
+def test_reader_refuses_a_directory_and_a_missing_file(tmp_path):
+    with pytest.raises(ValueError, match="is a directory"):
+        brisk_b200.read_sdpa_file(str(tmp_path))
+    with pytest.raises(ValueError, match="cannot open"):
+        brisk_b200.read_sdpa_file(str(tmp_path / "absent.dat-s"))
