@@ -220,7 +220,12 @@ int parse_options(int argc, const char *const *argv, Options &opt, std::string &
 // The caller's arrays as they are (nothing copied; build_problem skips the entries of value 0).
 static bool make_view(int m, int nblk, const int *bs, const double *c, int64_t nnz, const int *mat, const int *blk,
                       const int *i, const int *j, const double *v, bsolve::InputView &in) {
-    if (nnz < 0 || m < 0 || nblk <= 0 || !bs || (m > 0 && !c) || (nnz > 0 && (!mat || !blk || !i || !j || !v))) return false;
+    if (nnz < 0 || m < 0 || m > 100000000 || nblk <= 0 || !bs || (m > 0 && !c) ||
+        (nnz > 0 && (!mat || !blk || !i || !j || !v))) {
+        // the reference's message (problem.c, problem_from_sdpa_data)
+        bsolve::log_printf(1, "brisk: invalid problem data (m = %d, %d blocks)\n", m, nblk);
+        return false;
+    }
     in.m = m;
     in.nblk = nblk;
     in.bs = bs;
@@ -321,6 +326,7 @@ BRISK_API int brisk_solve_data(int m, int nblk, const int *bs, const double *c, 
     res->r = bsolve::ResultData();
     if (!g_stop_owner) g_stop = 0;
     bsolve::InputView in;
+    bsolve::set_print_hook(capi_print);
     if (!make_view(m, nblk, bs, c, nnz, mat, blk, i, j, v, in)) return 2;
     return run(in, nopt, opts, res);
 }

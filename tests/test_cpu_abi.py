@@ -146,6 +146,8 @@ def test_solve_data_checks_entries_as_the_reference(libpath):
     assert r.exit_code == 2 and "non-finite value in entry 1 1 1 1" in r.log
     r = _solve_data_raw([-2], [1.0], [1], [1], [1], [2], [1.0])
     assert r.exit_code == 2 and "off-diagonal entry in LP block" in r.log
+    r = _solve_data_raw([], [1.0], [1], [1], [1], [1], [1.0])   # no block
+    assert r.exit_code == 2 and "invalid problem data (m = 1, 0 blocks)" in r.log
 
 
 def test_other_reference_options_take_their_values(libpath):
