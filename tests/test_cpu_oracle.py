@@ -154,9 +154,9 @@ def test_oracle_follows_reference_row_by_row(golden, name, run, direction, init)
     from both starts (the least-squares start, the reference's default, solver.c:13939-14198; the
     SDPT3 start, -init 0) and in both directions: the same status and iterations, pobj and dobj of
     every row to the printed digits, and its gap, mu, pinf and dinf to theirs (three significant
-    digits, to 1 %; dinf to 2e-11 absolute and pinf to 2e-10 in the last rows, where the oracle's primal
-    residual stays near 1e-10 and the reference's refinement of A(dX) = rp takes it to about
-    1e-13, below the 1e-7 that ends the solve).
+    digits, to 1 %; dinf to 2e-11 absolute and pinf to 2e-10 in the last rows, where the oracle's
+    primal residual stays near 1e-10 and the reference's reaches about 1e-13, below the 1e-7 that
+    ends the solve).
     Blocks of order <= 32 take exact eigenvalues, larger ones the reference's Lanczos estimate
     (batch_q2: n = 37, batch_q1: n = 44), in the step lengths and in the least-squares start's
     shifts."""
