@@ -1,9 +1,12 @@
-"""Benchmark: time to a 1e-7 DIMACS solution of the seeded random SDP on B200s.
+"""Benchmark: time to a 1e-7 DIMACS solution of a seeded random SDP on B200s.
 
 A step is one interior-point solve of the workload to DIMACS error 1e-7 (the whole Newton-step
-path: Schur assembly, factor and PCG solves, step lengths).  Default workload: one 400 x 400
-block, m = 2000 constraints of 1 % density, FP64 on the GPU (`rand400`); `--workload rand1000`
-is the n = 1000, m = 8000, 0.5 % instance, solved both with the 3xTF32 mixed path and in FP64.
+path: Schur assembly, factor and PCG solves, step lengths).  The default workload is `rand1000`:
+one 1000 x 1000 block, m = 8000 constraints of 0.5 % density, solved by the mixed-precision path
+(3xTF32 Schur assembly on the tensor cores, FP32 factor early, FP64-accurate assembly and factor
+late, FP64-residual refinement throughout; `value`) and by the all-FP64 GPU path on the same
+instance (`paths.fp64`, with `mixed_speedup_over_fp64`).  `--workload rand400` is the n = 400,
+m = 2000, 1 % FP64 instance; the others are listed in WORKLOADS.
 
   value  seconds per solve with the problem resident in HBM (bgpu_session: uploaded once before
          the timed region), CUDA events on the library's stream, max over ranks
@@ -13,8 +16,12 @@ is the n = 1000, m = 8000, 0.5 % instance, solved both with the 3xTF32 mixed pat
 Multi-GPU: the solve does not shard (one Schur complement per solve); N GPUs run N independent
 replicas (`scaling: weak`, one solve per rank per step), launched by torchrun.
 
-`--impl reference` runs the reference's own CPU solver (oracle/_ref/brisk_ref, compiled from
-its sources by oracle/Makefile) on the same instance with every host thread (rank 0 only).
+`--impl reference` times the reference's own CPU solver (compiled from its sources by
+oracle/Makefile into oracle/_ref/) on the same instance with every host thread (rank 0 only).
+Where its full solve takes many minutes (rand1000: about 7 minutes on 16 cores), a step is one of
+its interior-point iterations, timed from the time column of its own iteration table, and the
+time to 1e-7 is its start plus the mean iteration times its own iteration count for the whole
+solve (recorded in tests/golden/ref_runs.json).
 """
 from __future__ import annotations
 
@@ -46,7 +53,7 @@ WORKLOADS = {
     "rand1000": dict(kind="random", gen=dict(n=1000, m=8000, density=0.005, seed=0),
                      desc="random SDP: one 1000x1000 block, m=8000, A_i 0.5% dense N(0,1), b=A(I), C=GG'/n+I, seed 0",
                      paths={"mixed": ["-asmprec", "tf32x3"], "fp64": ["-mixed", "0"]}, primary="mixed",
-                     ref_maxit=1),
+                     ref_sample_its=3),
     "mom60": dict(kind="moment", gen=dict(nvars=60, clique=4, seed=0),
                   desc="degree-2 moment relaxation of a seeded quartic in 60 variables, cliques of 4 consecutive "
                        "variables: 57 blocks of 15, m=2029, sparse Schur factor",
@@ -68,7 +75,16 @@ def make_instance(w):
     if w["kind"] == "theta":
         return problems.theta_problem(**w["gen"])
     return problems.random_sdp(**w["gen"])
+
+
 BASE_OPTS = ["-nohsd", "-dir", "hkm", "-tol", "1e-7", "-q"]
+L2_NOTE = ("GPU arm: a 256 MB device buffer written between timed solves (L2 flushed); reference arm: "
+           "host-resident inputs on the CPU")
+
+
+def config_of(name, w):
+    """The workload's description, the same dict in both arms (what is solved, not how)."""
+    return {"workload": name, "desc": w["desc"], "generator": dict(w["gen"]), "tol": 1e-7, "l2": L2_NOTE}
 
 
 def max_over_ranks(value, world, device="cuda"):
@@ -194,29 +210,117 @@ def gemm_roofline(torch, step, n, chunk, peak_tflops, launches=10):
             "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 entry)"}
 
 
-def cpu_reference_sample(d, workload, threads, opts_extra):
-    """The reference's CPU solve (oracle/_ref/brisk_ref) of the same instance: the bounded
-    sample is one full solve; value = its reported solve time without reading the file."""
-    from brisk_b200.problems import write_sdpa
-    ref = os.path.join(ROOT, "oracle", "_ref", "brisk_ref")
-    if not os.path.exists(ref):
+REF_LIB = os.path.join(ROOT, "oracle", "_ref", "libbrisk_ref.so")
+REF_ROW = re.compile(r"^\s*(\d+)\s+[+-]\S+\s+[+-]\S+(?:\s+\S+){7}\s+(\S+)\s*$")
+METRIC = "time_to_1e-7_dimacs_s"
+
+
+def reference_solve(d, threads, opts):
+    """One solve by the reference's own C API: brisk_solve_data of oracle/_ref/libbrisk_ref.so
+    (the reference compiled from its sources by oracle/Makefile) on the instance's arrays, in this
+    process, with -v and every given host thread (BRISK_NOBUSY=1 keeps the count exact).  Returns
+    its status, iterations, its reported total time and the time column of its iteration table
+    (seconds since its iterations began, one entry per row), or None when the library is absent."""
+    if not os.path.exists(REF_LIB):
         return None
-    with tempfile.TemporaryDirectory() as td:
-        path = os.path.join(td, workload + ".dat-s")
-        write_sdpa(d, path)
-        cmd = [ref, path, "-nohsd", "-dir", "hkm", "-tol", "1e-7", "-v", "-threads", str(threads)] + opts_extra
-        env = dict(os.environ, BRISK_NOBUSY="1")
-        t0 = time.time()
-        p = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=3600)
-        wall = time.time() - t0
-    out = p.stdout + p.stderr + f" [exit {p.returncode}]"
+    os.environ["BRISK_NOBUSY"] = "1"
+    L = ctypes.CDLL(REF_LIB, mode=os.RTLD_LOCAL)
+    PRINT = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_char_p, ctypes.c_int)
+    chunks = []
+
+    def cb(s, is_err):
+        chunks.append(s.decode(errors="replace"))
+        return 0
+
+    cbf = PRINT(cb)
+    L.brisk_set_output.argtypes = [ctypes.c_int, PRINT]
+    L.brisk_result_new.restype = ctypes.c_void_p
+    L.brisk_result_delete.argtypes = [ctypes.c_void_p]
+    L.brisk_result_status_str.argtypes, L.brisk_result_status_str.restype = [ctypes.c_void_p], ctypes.c_char_p
+    L.brisk_result_iterations.argtypes, L.brisk_result_iterations.restype = [ctypes.c_void_p], ctypes.c_int
+    pi, pd = ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)
+    L.brisk_solve_data.argtypes = [ctypes.c_int, ctypes.c_int, pi, pd, ctypes.c_int64, pi, pi, pi, pi, pd, ctypes.c_int,
+                                   ctypes.POINTER(ctypes.c_char_p), ctypes.c_void_p]
+    bs, c, mat, blk, ii, jj, v = [np.ascontiguousarray(a) for a in d.args()]
+    bs, mat, blk, ii, jj = [a.astype(np.intc) for a in (bs, mat, blk, ii, jj)]
+    av = list(opts) + ["-v", "-threads", str(threads)]
+    arr = (ctypes.c_char_p * len(av))(*[a.encode() for a in av])
+    L.brisk_set_output(2, cbf)
+    res = L.brisk_result_new()
+    t0 = time.perf_counter()
+    rc = L.brisk_solve_data(d.m, d.nblk, bs.ctypes.data_as(pi), c.ctypes.data_as(pd), d.nnz, mat.ctypes.data_as(pi),
+                            blk.ctypes.data_as(pi), ii.ctypes.data_as(pi), jj.ctypes.data_as(pi),
+                            v.ctypes.data_as(pd), len(av), arr, res)
+    wall = time.perf_counter() - t0
+    status = L.brisk_result_status_str(res).decode()
+    iters = L.brisk_result_iterations(res)
+    L.brisk_result_delete(res)
+    L.brisk_set_output(0, PRINT(0))
+    out = "".join(chunks)
     tt = re.search(r"time: total (\S+)s \(read (\S+),", out)
-    st = re.search(r"^status: (.+?)\s+iterations: (\d+)", out, re.M)
+    rows = [float(mm.group(2)) for mm in map(REF_ROW.match, out.splitlines()) if mm]
     if not tt:
-        return {"error": out[-500:]}
-    return {"time": float(tt.group(1)) - float(tt.group(2)), "wall": wall,
-            "status": st.group(1).strip() if st else None, "iterations": int(st.group(2)) if st else None,
-            "cmd": " ".join(["brisk_ref", workload + ".dat-s"] + cmd[2:])}
+        return {"error": f"exit {rc}: " + out[-300:]}
+    return {"time": float(tt.group(1)) - float(tt.group(2)), "wall": wall, "status": status, "iterations": iters,
+            "row_times": rows, "exit_code": rc}
+
+
+def golden_iterations(workload, run):
+    """The reference's own iteration count to 1e-7 on this instance (tests/golden/ref_runs.json)."""
+    try:
+        with open(os.path.join(ROOT, "tests", "golden", "ref_runs.json")) as f:
+            return int(json.load(f)[workload]["runs"][run]["iterations"])
+    except (OSError, KeyError, ValueError, TypeError):
+        return None
+
+
+def reference_options(w):
+    """The reference's options on a workload: its own default precision where this build's primary
+    path is the mixed one (its float Schur factor + PCG for m >= 1000), -mixed 0 where it is FP64."""
+    return ["-nohsd", "-dir", "hkm", "-tol", "1e-7"] + (w["paths"]["fp64"] if w["primary"] == "fp64" else [])
+
+
+def reference_measure(workload, w, d, steps, warmup, threads):
+    """The reference arm's measurement.  Full solves (`steps` of them after `warmup` solves stopped
+    after one iteration) where a solve is short; where `ref_sample_its` is set, one solve stopped
+    after that many iterations: its iteration times are the steps, and the time to 1e-7 is its
+    total time plus (the reference's own iteration count - the sampled ones) x the mean iteration."""
+    opts = reference_options(w)
+    S = w.get("ref_sample_its")
+    if S:
+        run = "mixed" if w["primary"] == "mixed" else "default"
+        n_ref = golden_iterations(workload, run)
+        if n_ref is None:
+            return {"error": f"no recorded reference iteration count for {workload} ({run} run)"}
+        if warmup > 0:
+            reference_solve(d, threads, opts + ["-maxit", "0"])
+        r = reference_solve(d, threads, opts + ["-maxit", str(S)])
+        if r is None or "error" in r:
+            return r or {"error": "oracle/_ref/libbrisk_ref.so absent"}
+        rt = r["row_times"]
+        its = [rt[k] - rt[k - 1] for k in range(1, len(rt))]
+        if not its:
+            return {"error": "no iteration rows in the reference's output"}
+        per_it = statistics.mean(its)
+        value = r["time"] + max(0, n_ref - len(its)) * per_it
+        return {"value": value, "steps": len(its), "warmup": 1 if warmup > 0 else 0, "status": r["status"],
+                "iterations": n_ref,
+                "sample": f"one reference solve through its C API stopped after {len(its)} iterations ({r['time']:.1f} s "
+                          f"with set-up and start; iterations {', '.join('%.2f' % t for t in its)} s); time to 1e-7 = "
+                          f"that + {n_ref - len(its)} x the mean iteration ({per_it:.2f} s), {n_ref} being the "
+                          f"reference's own iteration count on this instance (its recorded {run} run)"}
+    for _ in range(warmup):
+        reference_solve(d, threads, opts + ["-maxit", "1"])
+    times, r = [], None
+    for _ in range(steps):
+        r = reference_solve(d, threads, opts)
+        if r is None or "error" in r:
+            return r or {"error": "oracle/_ref/libbrisk_ref.so absent"}
+        times.append(r["time"])
+    return {"value": statistics.mean(times), "steps": steps, "warmup": warmup, "status": r["status"],
+            "iterations": r["iterations"],
+            "sample": f"full reference solves to 1e-7 through its C API, mean of {steps} (reported time); "
+                      f"{warmup} warm-up solve(s) stopped after one iteration"}
 
 
 def _ref_batch_one(q):
@@ -268,11 +372,11 @@ def run_reference_batch(args, w):
         print(json.dumps({"impl": "reference", "unavailable": (r or {}).get("error", "oracle/_ref/brisk_ref absent")}))
         return
     v = r["value"]
-    print(json.dumps({"impl": "reference", "metric": "time_to_1e-7_dimacs_s", "value": v, "unit": "s",
+    print(json.dumps({"impl": "reference", "metric": METRIC, "value": v, "unit": "s",
                       "n_gpus": args.gpus, "steps": 1, "warmup": 0, "ms_per_step": v * 1e3, "higher_is_better": False,
                       "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
-                      "config": {"workload": "batch", "count": args.batch_count, "desc": w["desc"],
-                                 "parallelism": "one process per host core"},
+                      "config": dict(config_of("batch", w), count=args.batch_count),
+                      "parallelism": "one process per host core",
                       "cpu_baseline": {"value": v, "unit": "s", "cores": r["cores"], "kind": "reference",
                                        "sample": r["sample"]},
                       "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
@@ -336,14 +440,13 @@ def run_ours_batch(args, w, torch):
             cpu = {"value": None, "error": (r or {}).get("error", "oracle/_ref/brisk_ref absent")}
     if rank == 0:
         print(json.dumps({
-            "metric": "time_to_1e-7_dimacs_s", "value": v, "unit": "s", "n_gpus": world, "steps": args.steps,
+            "metric": METRIC, "value": v, "unit": "s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
-            "config": {"workload": "batch", "count": count, "desc": w["desc"], "form": "lockstep (bgpu_batch_run)",
-                       "l2": "inputs larger than L2 (packed constraints %.1f GB)" % (8e-9 * sum(
-                           m_ * n_ * (n_ + 1) / 2 for n_, m_ in sizes)),
-                       "parallelism": f"replicas x{world}", "generation_s": round(gen_s, 1),
-                       "resident_setup_s": round(setup_s, 2)},
+            "config": dict(config_of("batch", w), count=count), "form": "lockstep (bgpu_batch_run)",
+            "inputs_gb": round(8e-9 * sum(m_ * n_ * (n_ + 1) / 2 for n_, m_ in sizes), 2),
+            "parallelism": f"replicas x{world}", "generation_s": round(gen_s, 1),
+            "resident_setup_s": round(setup_s, 2),
             "status": st, "dimacs_max": worst, "iterations_total": int(its),
             "instances_per_s": count / v, "assembly_flops_per_iteration": asm_flops,
             "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
@@ -364,27 +467,96 @@ def run_reference(args):
         return run_reference_batch(args, w)
     d = make_instance(w)
     threads = os.cpu_count() or 1
-    opts = w["paths"]["fp64"] if w["primary"] == "fp64" else []
-    times = []
-    for i in range(args.warmup + args.steps):
-        r = cpu_reference_sample(d, args.workload, threads, opts + (["-maxit", "1"] if i < args.warmup else []))
-        if r is None or "error" in r:
-            print(json.dumps({"impl": "reference", "unavailable": "reference binary missing or failed: "
-                              + (r or {}).get("error", "oracle/_ref/brisk_ref absent")[-200:]}))
-            return
-        if i >= args.warmup:
-            times.append(r["time"])
-    v = statistics.mean(times)
-    line = {"impl": "reference", "metric": "time_to_1e-7_dimacs_s", "value": v, "unit": "s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False,
+    r = reference_measure(args.workload, w, d, args.steps, args.warmup, threads)
+    if r is None or "error" in r:
+        print(json.dumps({"impl": "reference", "unavailable": "reference solve failed or absent: "
+                          + (r or {}).get("error", "oracle/_ref/libbrisk_ref.so absent")[-200:]}))
+        return
+    v = r["value"]
+    prec = "fp64 (reference -mixed 0)" if w["primary"] == "fp64" else "the reference's default (float Schur factor + PCG)"
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "s", "n_gpus": args.gpus,
+            "steps": r["steps"], "warmup": r["warmup"], "ms_per_step": v * 1e3, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
-            "config": {"workload": args.workload, "desc": w["desc"], "precision": "fp64 (reference -mixed 0)" if opts else
-                       "reference default mixed", "parallelism": "cpu threads"},
-            "cpu_baseline": {"value": v, "unit": "s", "cores": threads, "kind": "reference",
-                             "sample": f"full solve to 1e-7 of {args.workload}, mean of {args.steps}; warm-up runs -maxit 1"},
+            "config": config_of(args.workload, w), "precision": prec, "parallelism": f"cpu threads x{threads}",
+            "cpu_baseline": {"value": v, "unit": "s", "cores": threads, "kind": "reference", "sample": r["sample"]},
             "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "reference_status": r["status"], "reference_iterations": r["iterations"]}
     print(json.dumps(line), flush=True)
+
+
+ROW = re.compile(r"^\s*(\d+)\s+([+-]\S+)\s+([+-]\S+)\s+(\S+)\s+(\S+)\s+(\S+)\s+(\S+)\s+\S+\s+\S+\s+\S+\s+\S+\s*$")
+
+
+def table_rows(log):
+    """The iteration table of a -v log: it -> (pobj, dobj, pinf, dinf, gap, mu) as printed."""
+    rows = {}
+    for line in log.splitlines():
+        mm = ROW.match(line)
+        if mm:
+            rows[int(mm.group(1))] = tuple(float(x) for x in mm.groups()[1:])
+    return rows
+
+
+def per_iteration_errors(mixed_log, fp64_log):
+    """Each iteration of the mixed solve against the FP64 solve of the same instance from the same
+    start: the mixed iterate's own infeasibilities and gap, and its objectives' relative distance
+    from the FP64 solve's at the same iteration (to the 9 digits the table prints)."""
+    a, b = table_rows(mixed_log), table_rows(fp64_log)
+    out = []
+    for it in sorted(a):
+        pm, dm, pinf, dinf, gap, mu = a[it]
+        row = {"it": it, "pinf": pinf, "dinf": dinf, "gap": gap, "mu": mu}
+        if it in b:
+            pf, df = b[it][0], b[it][1]
+            row["pobj_rel_vs_fp64"] = float("%.2e" % (abs(pm - pf) / (1 + abs(pf))))
+            row["dobj_rel_vs_fp64"] = float("%.2e" % (abs(dm - df) / (1 + abs(df))))
+        out.append(row)
+    return out
+
+
+def load_peaks():
+    """MEASURED_PEAKS.json (driver-written: measured copy bandwidth and cuBLAS bf16 GEMM on this
+    pool's B200s), else the earlier measurement on this pool."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            pk = json.load(f)
+        return float(pk["bf16_tflops"]), float(pk["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 1590.0, 6650.0, "fallback"
+
+
+def tf32x3_roofline(torch, step, n, chunk, launches=10):
+    """The dominant kernel of the mixed path (the 3xTF32 row-product GEMM of the Schur assembly,
+    (n K) x n x n per launch, three tf32 MMAs per product on tcgen05) timed alone with CUDA events
+    on the stream it is launched on.  Useful flops 2 (n K) n^2 against the 3xTF32-useful peak:
+    the measured dense bf16 rate / 2 (TF32 runs at half the bf16 rate) / 3 (MMAs per product)."""
+    bf16, _, src = load_peaks()
+    peak = bf16 / 2.0 / 3.0
+    M, ld = n * chunk, (n + 3) // 4 * 4
+    f32 = torch.float32
+    Ah, Al = torch.randn(M * ld, dtype=f32, device="cuda"), torch.randn(M * ld, dtype=f32, device="cuda") * 1e-4
+    Bh, Bl = torch.randn(n * ld, dtype=f32, device="cuda"), torch.randn(n * ld, dtype=f32, device="cuda") * 1e-4
+    G = torch.empty(M * n, dtype=f32, device="cuda")
+    s = torch.cuda.current_stream()
+    sp = ctypes.c_void_p(s.cuda_stream)
+    args = (M, n, n, Ah.data_ptr(), Al.data_ptr(), ld, Bh.data_ptr(), Bl.data_ptr(), ld, G.data_ptr(), M, sp)
+    for _ in range(3):
+        step.call("gemm_tf32x3", *args)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    for _ in range(launches):
+        step.call("gemm_tf32x3", *args)
+    e1.record(s)
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) * 1e-3 / launches
+    flops = 2.0 * M * n * n
+    ach = flops / t / 1e12
+    return {"bound": "tensor", "kernel": "tf32x3_kernel (3xTF32, tcgen05.mma kind::tf32, TMEM accumulator)",
+            "achieved": round(ach, 2), "peak": round(peak, 2), "unit": "TFLOP/s", "frac": round(ach / peak, 4),
+            "traffic": None, "flops_per_launch": flops, "launch_ms": round(t * 1e3, 4),
+            "peak_source": f"{src} bf16 {bf16:.1f} TF/s (burst) / 2 for TF32 / 3 MMAs per useful product "
+                           f"({'of measured' if src == 'measured' else 'of fallback'})"}
 
 
 def run_ours(args):
@@ -418,9 +590,23 @@ def run_ours(args):
         arr = (ctypes.c_char_p * max(len(lst), 1))(*[a.encode() for a in lst])
         return len(lst), arr
 
+    chunks = []
+    cbf = _core._PRINT(lambda s_, e_: (chunks.append(s_.decode(errors="replace")), 0)[1])
+
+    def logged_solve(sess, opts, res):
+        """An untimed solve with -v, its output captured (the iteration table)."""
+        n_v, a_v = argv([o for o in opts if o != "-q"] + ["-v"])
+        chunks.clear()
+        L.brisk_set_output(2, cbf)
+        try:
+            S.bgpu_session_solve(sess, n_v, a_v, res)
+        finally:
+            L.brisk_set_output(0, _core._PRINT(0))
+        return "".join(chunks)
+
     flush_buf = torch.zeros(32 * 1024 * 1024, dtype=torch.float64, device="cuda")
     dev_opt = ["-device", str(local)]
-    results = {}
+    results, logs = {}, {}
     for pname, popts in w["paths"].items():
         opts = BASE_OPTS + popts + dev_opt
         n_o, a_o = argv(opts)
@@ -432,96 +618,110 @@ def run_ours(args):
             raise RuntimeError(f"session create failed: exit code {rc.value}")
         res = L.brisk_result_new()
         meas = (ctypes.c_double * 8)()
-        nsteps = args.steps if pname == w["primary"] else max(1, min(args.steps, 2))
-        for _ in range(args.warmup if pname == w["primary"] else 1):
-            S.bgpu_session_solve(sess, n_o, a_o, res)
+        primary = pname == w["primary"]
+        nsteps = args.steps if primary else max(1, min(args.steps, 2))
+        nwarm = args.warmup if primary else 1
+        for k in range(nwarm):
+            if k == 0:
+                logs[pname] = logged_solve(sess, opts, res)
+            else:
+                S.bgpu_session_solve(sess, n_o, a_o, res)
         if world > 1:
             torch.distributed.barrier()
         torch.cuda.synchronize()
         dev_times, statuses, iters, schur_t, schur_f = [], [], [], [], []
         launches0 = S.bgpu_launch_count()
+        dimacs = (ctypes.c_double * 6)()
         with Clocks(local) as clk:
             for _ in range(nsteps):
                 flush_l2(torch, flush_buf)
                 torch.cuda.synchronize()
-                code = S.bgpu_session_solve(sess, n_o, a_o, res)
+                S.bgpu_session_solve(sess, n_o, a_o, res)
                 S.bgpu_result_measures(res, meas)
                 dev_times.append(meas[0])
                 schur_t.append(meas[1])
                 schur_f.append(meas[2])
                 iters.append(int(meas[5]))
                 statuses.append(L.brisk_result_status_str(res).decode())
-                dimacs = (ctypes.c_double * 6)()
                 L.brisk_result_dimacs(res, dimacs)
         torch.cuda.synchronize()
         launches = S.bgpu_launch_count() - launches0
+        if pname not in logs:
+            logs[pname] = logged_solve(sess, opts, res)
         t_step = max_over_ranks(statistics.mean(dev_times), world)
         results[pname] = dict(value=t_step, status=statuses[-1], iterations=iters[-1],
                               schur_tflops=sum(schur_f) / max(sum(schur_t), 1e-30) / 1e12,
                               schur_s_per_solve=statistics.mean(schur_t), launches_per_step=launches / nsteps,
-                              clocks=clk.summary(), dimacs=max(abs(x) for x in dimacs), steps=nsteps)
+                              clocks=clk.summary(), dimacs=[float(x) for x in dimacs], steps=nsteps,
+                              pobj=float(L.brisk_result_pobj(res)), dobj=float(L.brisk_result_dobj(res)),
+                              pcg_steps=int(meas[7]))
         S.bgpu_session_destroy(sess)
         # end to end through the reference's public call (host arrays, upload + download timed)
-        if pname == w["primary"]:
+        if primary:
             e2e_times = []
             for k in range(1 + max(1, min(args.steps, 3))):   # the first call untimed (warm-up)
                 torch.cuda.synchronize()
                 t0 = time.perf_counter()
-                rc2 = L.brisk_solve_data(d.m, d.nblk, bs.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
-                                         c.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), d.nnz,
-                                         mat.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
-                                         blk.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
-                                         ii.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
-                                         jj.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
-                                         v.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), n_o,
-                                         ctypes.cast(a_o, ctypes.POINTER(ctypes.c_char_p)), res)
+                L.brisk_solve_data(d.m, d.nblk, bs.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                   c.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), d.nnz,
+                                   mat.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                   blk.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                   ii.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                   jj.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                   v.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), n_o,
+                                   ctypes.cast(a_o, ctypes.POINTER(ctypes.c_char_p)), res)
                 if k > 0:
                     e2e_times.append(time.perf_counter() - t0)
             S.bgpu_result_measures(res, meas)
             results[pname]["e2e"] = dict(value=statistics.mean(e2e_times), h2d=meas[3], d2h=meas[4])
         L.brisk_result_delete(res)
     prim = results[w["primary"]]
-    roof = None
-    cpu = None
+    roof, roof64, cpu = None, None, None
     if rank == 0:
         if w["kind"] == "random":
+            n = w["gen"]["n"]
             peak64 = measure_fp64_peak(torch)
-            roof = gemm_roofline(torch, step, w["gen"]["n"], step.chunk_default(w["gen"]["n"], 0), peak64)
+            roof64 = gemm_roofline(torch, step, n, step.chunk_default(n, 0), peak64)
+            roof = tf32x3_roofline(torch, step, n, step.chunk_default(n, 1)) if w["primary"] == "mixed" else roof64
         if not args.no_cpu_baseline and world == 1:
-            threads = os.cpu_count() or 1
-            opts_ref = w["paths"]["fp64"] if w["primary"] == "fp64" else []
-            maxit = w.get("ref_maxit")
-            r = cpu_reference_sample(d, args.workload, threads, opts_ref + (["-maxit", str(maxit)] if maxit else []))
-            if r and "error" not in r and not maxit:
-                cpu = {"value": r["time"], "unit": "s", "cores": threads, "kind": "reference",
-                       "sample": f"one full reference solve to 1e-7 ({r['status']}, {r['iterations']} iterations)"}
-            elif r and "error" not in r:
-                # the full reference solve takes tens of minutes: a bounded sample of `maxit` iterations
-                # (start included), scaled to the iterations this build's solve took
-                per_it = r["time"] / max(1, maxit)
-                cpu = {"value": per_it * prim["iterations"], "unit": "s", "cores": threads, "kind": "reference",
-                       "sample": f"reference solve stopped after {maxit} iteration(s) ({r['time']:.1f} s, start "
-                                 f"included), scaled to {prim['iterations']} iterations"}
+            # the reference arm's own measurement, in a separate process (no CUDA or torch there)
+            cmd = [sys.executable, os.path.abspath(__file__), "--impl", "reference", "--workload", args.workload,
+                   "--steps", "1", "--warmup", "0"]
+            p = subprocess.run(cmd, capture_output=True, text=True, timeout=3000, env=dict(os.environ, RANK="0"))
+            line = next((ln for ln in p.stdout.splitlines()[::-1] if ln.startswith("{")), None)
+            rj = json.loads(line) if line else {}
+            if "cpu_baseline" in rj:
+                cpu = dict(rj["cpu_baseline"], kind="reference")
             else:
-                cpu = {"value": None, "error": (r or {}).get("error", "oracle/_ref/brisk_ref absent")[-300:]}
+                cpu = {"value": None, "error": (rj.get("unavailable") or p.stderr[-300:] or "no output")}
     if world > 1:
         torch.distributed.barrier()
     if rank == 0:
-        line = {"metric": "time_to_1e-7_dimacs_s", "value": prim["value"], "unit": "s", "n_gpus": world,
+        line = {"metric": METRIC, "value": prim["value"], "unit": "s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": prim["value"] * 1e3,
                 "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f64" if w["primary"] == "fp64" else "tf32x3+f64", "data": "synthetic (seeded generator)",
-                "config": {"workload": args.workload, "desc": w["desc"], "precision": w["primary"],
-                           "l2": "256 MB buffer written between steps", "parallelism": f"replicas x{world}"},
-                "status": prim["status"], "iterations": prim["iterations"], "dimacs_max": prim["dimacs"],
+                "config": config_of(args.workload, w), "precision": w["primary"], "parallelism": f"replicas x{world}",
+                "status": prim["status"], "iterations": prim["iterations"], "dimacs": prim["dimacs"],
+                "dimacs_max": max(abs(x) for x in prim["dimacs"]),
                 "schur_tflops": round(prim["schur_tflops"], 3), "schur_s_per_solve": prim["schur_s_per_solve"],
                 "e2e": {"value": prim["e2e"]["value"], "unit": "s", "h2d_bytes_per_step": int(prim["e2e"]["h2d"]),
                         "d2h_bytes_per_step": int(prim["e2e"]["d2h"])},
                 "gpu_launches": int(prim["launches_per_step"] * prim["steps"]),
                 "clocks": prim["clocks"], "roofline": roof, "cpu_baseline": cpu,
                 "roofline_note": None if roof else "no dominant GEMM on this workload (small blocks, sparse factor)",
-                "paths": {k: {kk: vv for kk, vv in r.items() if kk in ("value", "status", "iterations", "schur_tflops")}
+                "paths": {k: {kk: vv for kk, vv in r.items()
+                              if kk in ("value", "status", "iterations", "schur_tflops", "schur_s_per_solve", "pobj",
+                                        "dobj", "dimacs", "steps", "pcg_steps")}
                           for k, r in results.items()}}
+        if "fp64" in results and w["primary"] != "fp64":
+            f = results["fp64"]
+            line["mixed_speedup_over_fp64"] = round(f["value"] / prim["value"], 3)
+            line["mixed_vs_fp64"] = {
+                "pobj_rel": abs(prim["pobj"] - f["pobj"]) / (1 + abs(f["pobj"])),
+                "dobj_rel": abs(prim["dobj"] - f["dobj"]) / (1 + abs(f["dobj"])),
+                "per_iteration": per_iteration_errors(logs.get(w["primary"], ""), logs.get("fp64", ""))}
+            line["roofline_fp64"] = roof64
         print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()
@@ -533,7 +733,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="rand400", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="rand1000", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-count", type=int, default=4096, help="instances of the batch workload")
     ap.add_argument("--batch-sample", type=int, default=64, help="instances the reference solves for its sample")

@@ -9,6 +9,17 @@
 
 long long g_bgpu_launches = 0;
 static cudaStream_t S(void *s) { return (cudaStream_t)s; }
+// the assembly's precision codes: 0 FP64, 1 3xTF32, 2 Ozaki (8 slices), (S << 8) | 2 Ozaki with S
+static bool valid_precision(int p) {
+    if (p == 0 || p == 1 || p == 2) return true;
+    const int sl = (p >> 8) & 0xf;
+    return (p & 0xff) == 2 && (p >> 12) == 0 && sl >= 4 && sl <= 8;
+}
+
+static std::atomic<unsigned> g_wait_limit{BGPU_SPIN_LIMIT};
+static std::atomic<int> g_trsv_hold{-1};
+unsigned wait_limit() { return g_wait_limit.load(std::memory_order_relaxed); }
+int trsv_hold_row() { return g_trsv_hold.load(std::memory_order_relaxed); }
 
 extern "C" {
 
@@ -18,6 +29,8 @@ BGPU_API int bgpu_sync(void *stream) {
 }
 BGPU_API const char *bgpu_version(void) { return "brisk_b200 1.7-b200 sm_100a"; }
 BGPU_API long long bgpu_launch_count(void) { return __atomic_load_n(&g_bgpu_launches, __ATOMIC_RELAXED); }
+BGPU_API void bgpu_set_wait_limit(unsigned polls) { g_wait_limit.store(polls ? polls : BGPU_SPIN_LIMIT); }
+BGPU_API void bgpu_test_hold_trsv_row(int r) { g_trsv_hold.store(r < 0 ? -1 : r); }
 
 BGPU_API size_t bgpu_schur_ws_bytes(int n, int chunk, int precision) {
     if (chunk <= 0) chunk = schur_chunk_default(n, precision);
@@ -76,19 +89,25 @@ BGPU_API int bgpu_nt_scaling(int n, const double *d_LX, const double *d_LZ, doub
 
 BGPU_API size_t bgpu_ozaki_ws_bytes(int M, int N, int K) {
     if (M <= 0 || N <= 0 || K <= 0) return 0;
-    return ozaki_operand_bytes(M, K) + ozaki_operand_bytes(N, K);
+    return ozaki_operand_bytes(M, K, 8) + ozaki_operand_bytes(N, K, 8);
 }
 
 BGPU_API int bgpu_gemm_ozaki(int M, int N, int K, const double *d_A, int64_t lda, const double *d_B, int64_t ldb,
                              double *d_C, int64_t ldc, void *d_ws, size_t ws_bytes, void *stream) {
+    return bgpu_gemm_ozaki_slices(8, M, N, K, d_A, lda, d_B, ldb, d_C, ldc, d_ws, ws_bytes, stream);
+}
+
+BGPU_API int bgpu_gemm_ozaki_slices(int slices, int M, int N, int K, const double *d_A, int64_t lda, const double *d_B,
+                                    int64_t ldb, double *d_C, int64_t ldc, void *d_ws, size_t ws_bytes, void *stream) {
+    if (slices < 4 || slices > 8) return BGPU_ERR_ARG;
     if (M <= 0 || N <= 0 || K <= 0 || lda < K || ldb < K || ldc < M || !d_A || !d_B || !d_C || !d_ws ||
         ws_bytes < bgpu_ozaki_ws_bytes(M, N, K))
         return BGPU_ERR_ARG;
     cudaStream_t st = S(stream);
     OzakiOperand a, b;
-    uint8_t *wa = (uint8_t *)d_ws, *wb = wa + ozaki_operand_bytes(M, K);
-    int rc = ozaki_slice(st, M, K, d_A, lda, wa, &a);
-    if (!rc) rc = ozaki_slice(st, N, K, d_B, ldb, wb, &b);
+    uint8_t *wa = (uint8_t *)d_ws, *wb = wa + ozaki_operand_bytes(M, K, slices);
+    int rc = ozaki_slice(st, M, K, d_A, lda, wa, &a, slices);
+    if (!rc) rc = ozaki_slice(st, N, K, d_B, ldb, wb, &b, slices);
     if (!rc) rc = ozaki_gemm(st, a, b, d_C, ldc);
     if (rc) return rc;
     BGPU_CHECK(cudaStreamSynchronize(st));
@@ -111,7 +130,7 @@ BGPU_API int bgpu_schur_assemble(int n, int m, int ncon, const int *d_con, const
                                  const int *d_ccol, const int *d_cpos, const double *d_cval, const double *d_X,
                                  const double *d_Zi, double *d_M, int precision, int chunk, void *d_ws,
                                  size_t ws_bytes, void *stream) {
-    if (n <= 0 || m <= 0 || ncon < 0 || precision < 0 || precision > 2) return BGPU_ERR_ARG;
+    if (n <= 0 || m <= 0 || ncon < 0 || !valid_precision(precision)) return BGPU_ERR_ARG;
     if (chunk <= 0) chunk = schur_chunk_default(n, precision);
     DevBlock B;
     B.n = n;
@@ -152,7 +171,7 @@ BGPU_API int bgpu_schur_assemble_sym(int n, int m, int ncon, const int *d_con, c
                                      const long long *d_uptr, const int *d_upos, const double *d_uval,
                                      const double *d_X, const double *d_Zi, double *d_M, int precision, int chunk,
                                      void *d_ws, size_t ws_bytes, void *stream) {
-    if (n <= 0 || m <= 0 || ncon < 0 || precision < 0 || precision > 2) return BGPU_ERR_ARG;
+    if (n <= 0 || m <= 0 || ncon < 0 || !valid_precision(precision)) return BGPU_ERR_ARG;
     if (ncon > 0 && (!d_uptr || !d_upos || !d_uval)) return BGPU_ERR_ARG;
     if (chunk <= 0) chunk = schur_chunk_default(n, precision);
     DevBlock B;

@@ -119,11 +119,12 @@ int parse_options(int argc, const char *const *argv, Options &opt, std::string &
             else if (!strcmp(s, "ozaki")) opt.asm_prec = 2;
             else { err = "bad -asmprec (fp64, tf32x3 or ozaki)"; return 1; }
         } else if (a == "-asmlate") {   // this build: the 3xTF32 path's late assembly
-            const char *s = need("fp64 or ozaki");
+            const char *s = need("fp64, ozaki or ozaki4..ozaki7");
             if (!s) return 1;
             if (!strcmp(s, "fp64")) opt.late_prec = 0;
-            else if (!strcmp(s, "ozaki")) opt.late_prec = 2;
-            else { err = "bad -asmlate (fp64 or ozaki)"; return 1; }
+            else if (!strcmp(s, "ozaki") || !strcmp(s, "ozaki8")) opt.late_prec = 2;
+            else if (!strncmp(s, "ozaki", 5) && s[5] >= '4' && s[5] <= '7' && s[6] == 0) opt.late_prec = ((s[5] - '0') << 8) | 2;
+            else { err = "bad -asmlate (fp64, ozaki or ozaki4..ozaki7)"; return 1; }
         } else if (a == "-muswitch") {
             const char *s = need("a number");
             if (!s || !parse_double(s, opt.mu_switch)) { if (err.empty()) err = "bad -muswitch"; return 1; }
@@ -180,6 +181,27 @@ int parse_options(int argc, const char *const *argv, Options &opt, std::string &
             opt.verbose = 3;
         } else if (a == "-nohsd" || a == "-nofr" || a == "-feasible") {
             if (a == "-feasible") opt.known_feasible = 1;
+        } else if (a == "-hsd") {
+            // a flag in the reference (OPTIONS.md: "-hsd | -nohsd"): the self-dual embedding
+            // (hsd_run, solver.c:9803) is not part of this build
+            log_printf(1, "brisk: note: -hsd asks for the self-dual embedding, which this build does not have: "
+                          "the infeasible-start method runs\n");
+        } else if (a == "-corr" || a == "-chordal" || a == "-sym" || a == "-symalg" || a == "-deprows" ||
+                   a == "-mixedfrac") {
+            // options of the reference that change its method; this build solves the problem as
+            // given with the infeasible-start predictor-corrector, so a value other than the one
+            // that method already has is passed over with a note
+            const char *s = need("a value");
+            if (!s) return 1;
+            const std::string v = s;
+            const char *what = nullptr;
+            if (a == "-corr" && v != "0") what = "centrality correctors are not run";
+            else if (a == "-chordal" && v == "1") what = "no chordal decomposition is applied: the blocks are solved as given";
+            else if (a == "-sym" && v != "none") what = "no symmetry reduction is applied";
+            else if (a == "-symalg" && v != "0") what = "no block-algebra reduction is applied";
+            else if (a == "-deprows" && v != "0") what = "dependent constraints are not removed";
+            else if (a == "-mixedfrac") what = "the float-factor rule of this build does not use it";
+            if (what) log_printf(1, "brisk: note: option %s %s: %s\n", a.c_str(), s, what);
         } else if (a == "-batchmode") {
             const char *s = need("lockstep or concurrent");
             if (!s) return 1;
@@ -192,9 +214,9 @@ int parse_options(int argc, const char *const *argv, Options &opt, std::string &
                 if (err.empty()) err = "bad -sparse (-1 auto, 0 dense, 1 sparse)";
                 return 1;
             }
-        } else if (a == "-hsd" || a == "-threads" || a == "-chordal" || a == "-sym" ||
-                   a == "-symalg" || a == "-deprows" || a == "-caller" || a == "-corr" || a == "-mixedfrac") {
-            // options of the reference that take a value and do not change this path's arithmetic
+        } else if (a == "-threads" || a == "-caller") {
+            // options of the reference that take a value and do not change the method (host
+            // threads of its CPU solve; the calling language)
             if (!need("a value")) return 1;
         } else {
             // another of the reference's options (OPTIONS.md's table): its value, if it has one,

@@ -35,6 +35,31 @@ extern long long g_bgpu_launches;
 
 static inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
 
+// Kernel attributes (cudaFuncSetAttribute) and occupancy figures belong to one device: a launcher
+// sets them once per device.  `done` keeps one bit per device 0-63 (the setter runs on every call
+// on a device above 63); two threads that set the same attribute at once do no harm.
+template <class F>
+inline int once_per_device(std::atomic<unsigned long long> &done, F &&set) {
+    int dev = 0;
+    BGPU_CHECK(cudaGetDevice(&dev));
+    const unsigned long long bit = (dev >= 0 && dev < 64) ? 1ull << dev : 0ull;
+    if (bit && (done.load(std::memory_order_acquire) & bit)) return BGPU_OK;
+    const int rc = set();
+    if (rc == BGPU_OK && bit) done.fetch_or(bit, std::memory_order_acq_rel);
+    return rc;
+}
+#define BGPU_ATTR_ONCE(...)                                                                           \
+    do {                                                                                              \
+        static std::atomic<unsigned long long> attr_done_{0};                                          \
+        if (int rc_ = once_per_device(attr_done_, [&]() -> int { __VA_ARGS__; return BGPU_OK; })) return rc_; \
+    } while (0)
+
+// The bound of the triangular solves' device-side waits, in polls of the awaited flag (each
+// followed by a 64 ns sleep), and the failure-path test's held block row (bgpu_set_wait_limit,
+// bgpu_test_hold_trsv_row).
+unsigned wait_limit();
+int trsv_hold_row();
+
 // ---- device helpers -------------------------------------------------------------------
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll

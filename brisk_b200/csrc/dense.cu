@@ -165,9 +165,13 @@ __global__ void __launch_bounds__(256) syrk_f32(int n2, int K, const float *A, l
 
 // ---- persistent triangular solve -----------------------------------------------------------
 // trans = 0: solve L x = b (block rows top-down); trans = 1: solve L' x = b (bottom-up).
+// One CTA per block row (all co-resident: a cooperative launch); the CTA of block row r waits
+// for the flags of the rows it depends on, at most `limit` polls each, then publishes its own.
+// hold >= 0 (failure-path tests only): the CTA of that block row computes its rows but does
+// not publish its flag, so the rows after it give up waiting and report through *err.
 template <typename T>
 __global__ void __launch_bounds__(256) trsv_kernel(int n, const T *L, long long lda, const T *dinv, T *x, int trans,
-                                                   int *flags, int epoch, int *err) {
+                                                   int *flags, int epoch, int *err, unsigned limit, int hold) {
     __shared__ T acc[NB];
     __shared__ T part[4][NB];
     __shared__ T xc[NB];
@@ -186,7 +190,7 @@ __global__ void __launch_bounds__(256) trsv_kernel(int n, const T *L, long long 
         if (tid == 0) {
             unsigned spins = 0;
             while (ld_acquire(&flags[c]) != epoch) {
-                if (++spins > BGPU_SPIN_LIMIT) { bad = 1; break; }
+                if (++spins > limit) { bad = 1; break; }
                 __nanosleep(64);
             }
         }
@@ -224,7 +228,27 @@ __global__ void __launch_bounds__(256) trsv_kernel(int n, const T *L, long long 
     if (tid < nr) x[r0 + tid] = (part[0][tid] + part[1][tid]) + (part[2][tid] + part[3][tid]);
     __threadfence();
     __syncthreads();
-    if (tid == 0) st_release(&flags[r], epoch);
+    if (tid == 0 && r != hold) st_release(&flags[r], epoch);
+}
+
+// The largest number of block rows one solve can take on the current device: every CTA of the
+// cooperative launch must be resident at once (SMs x resident CTAs per SM).
+std::atomic<int> g_trsv_cap[2][64];
+template <typename T>
+int trsv_max_blocks(int *cap) {
+    int dev = 0;
+    BGPU_CHECK(cudaGetDevice(&dev));
+    std::atomic<int> *slot = (dev >= 0 && dev < 64) ? &g_trsv_cap[sizeof(T) == 8][dev] : nullptr;
+    if (slot && slot->load(std::memory_order_relaxed) > 0) {
+        *cap = slot->load(std::memory_order_relaxed);
+        return BGPU_OK;
+    }
+    int nsm = 0, per = 0;
+    BGPU_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    BGPU_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, trsv_kernel<T>, 256, 0));
+    *cap = nsm * per;
+    if (slot) slot->store(*cap, std::memory_order_relaxed);
+    return BGPU_OK;
 }
 
 template <typename T>
@@ -232,17 +256,13 @@ int trsv_launch(cudaStream_t st, int n, const T *L, long long lda, const T *dinv
                 int epoch, int *d_err) {
     if (n <= 0) return BGPU_OK;
     const int nblk = (n + NB - 1) / NB;
-    static int max_coresident = -1;
-    if (max_coresident < 0) {
-        int dev = 0, nsm = 0, per = 0;
-        BGPU_CHECK(cudaGetDevice(&dev));
-        BGPU_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-        BGPU_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, trsv_kernel<T>, 256, 0));
-        max_coresident = nsm * per;
-    }
-    if (nblk > max_coresident) return BGPU_ERR_TOOBIG;
+    int cap = 0;
+    if (int rc = trsv_max_blocks<T>(&cap)) return rc;
+    if (nblk > cap) return BGPU_ERR_TOOBIG;
+    unsigned limit = wait_limit();
+    int hold = trsv_hold_row();
     void *args[] = {(void *)&n, (void *)&L, (void *)&lda, (void *)&dinv, (void *)&x, (void *)&trans,
-                    (void *)&flags, (void *)&epoch, (void *)&d_err};
+                    (void *)&flags, (void *)&epoch, (void *)&d_err, (void *)&limit, (void *)&hold};
     BGPU_CHECK(cudaLaunchCooperativeKernel((void *)trsv_kernel<T>, dim3(nblk), dim3(256), args, 0, st));
     BGPU_LAUNCH_CHECK();
     return BGPU_OK;
@@ -339,12 +359,8 @@ __global__ void dots_final_kernel(const double *scratch, double *out) {
 // ---- host launchers -------------------------------------------------------------------------
 template <typename T>
 int diag_smem_attr() {
-    static bool done = false;
-    if (!done) {
-        BGPU_CHECK(cudaFuncSetAttribute(potrf_diag_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)(2 * NB * LDS * sizeof(T))));
-        done = true;
-    }
+    BGPU_ATTR_ONCE(BGPU_CHECK(cudaFuncSetAttribute(potrf_diag_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)(2 * NB * LDS * sizeof(T)))));
     return BGPU_OK;
 }
 
@@ -482,9 +498,14 @@ int dots_f64(cudaStream_t st, int nq, const double *const *a, const double *cons
 // owned by another allocator (a framework's caching pool, a fixed budget).  For them,
 // bgpu_trsv_noalloc keeps the block-row flags and the wait-error flag of the solve in this
 // file-scope array instead of buffers the caller passes.  Every GPU that loads the library holds
-// the array (16 KB) until the process exits.
+// the array (8 KB) until the process exits.
+//
+// Its size limit is the solve's own: one CTA per block row of 64, all resident at once (a
+// cooperative launch), so n <= 64 x (SMs x resident CTAs of trsv_kernel per SM); on a B200,
+// 148 x 8 = 1184 block rows, n <= 75776.  The array holds 2048 block rows, more than any device
+// of up to 256 SMs can keep resident.
 #include <mutex>
-#define BGPU_NOALLOC_TRSV_MAXBLK 4096   // block rows of 64: n <= 262144
+#define BGPU_NOALLOC_TRSV_MAXBLK 2048
 static __device__ __align__(256) int g_trsv_noalloc_scratch[BGPU_NOALLOC_TRSV_MAXBLK + 1];
 
 namespace {
@@ -501,9 +522,13 @@ extern "C" BGPU_API int bgpu_trsv_noalloc(int n, const double *d_L, int lda, con
                                           int trans, void *stream) {
     if (n <= 0 || lda < n || !d_L || !d_dinv || !d_x) return BGPU_ERR_ARG;
     const int nblk = (n + NB - 1) / NB;
-    if (nblk > BGPU_NOALLOC_TRSV_MAXBLK) {
-        fprintf(stderr, "bgpu_trsv_noalloc: n = %d is above this entry point's maximum of %d\n", n,
-                BGPU_NOALLOC_TRSV_MAXBLK * NB);
+    int cap = 0;
+    if (int rc = trsv_max_blocks<double>(&cap)) return rc;
+    cap = std::min(cap, BGPU_NOALLOC_TRSV_MAXBLK);
+    if (nblk > cap) {
+        fprintf(stderr,
+                "bgpu_trsv_noalloc: n = %d needs %d block rows of %d; this device keeps at most %d resident at once "
+                "(n <= %d)\n", n, nblk, NB, cap, cap * NB);
         return BGPU_ERR_TOOBIG;
     }
     int dev = 0;
@@ -516,10 +541,10 @@ extern "C" BGPU_API int bgpu_trsv_noalloc(int n, const double *d_L, int lda, con
         NoallocDev &d = g_noalloc[dev];
         if (!d.ptr) {
             // set-up on the first call on this device: the array's device address (the host-side
-            // symbol is only a stand-in) and its flags cleared to 0 (every epoch below is > 0)
+            // symbol is only a stand-in).  The array is zero when the module loads (static
+            // device storage), and every epoch below is > 0, so no flag needs clearing here.
             void *p = nullptr;
             BGPU_CHECK(cudaGetSymbolAddress(&p, g_trsv_noalloc_scratch));
-            BGPU_CHECK(cudaMemset(p, 0, sizeof(int) * (BGPU_NOALLOC_TRSV_MAXBLK + 1)));
             d.ptr = (int *)p;
         }
         if (d.epoch == 0x7fffffff) {   // epochs exhausted: start over from cleared flags

@@ -181,12 +181,8 @@ template <bool A_KM, bool B_KM, int BN>
 int launch(cudaStream_t st, int M, int N, int K, double alpha, const double *A, long long lda, long long sA,
            const double *B, long long ldb, long long sB, double beta, double *C, long long ldc, long long sC,
            int batch, int lower) {
-    static std::atomic<bool> attr_set{false};   // (set once; a second setter is harmless)
-    if (!attr_set) {
-        BGPU_CHECK(cudaFuncSetAttribute(dgemm_kernel<A_KM, B_KM, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)TileN<BN>::SMEM));
-        attr_set = true;
-    }
+    BGPU_ATTR_ONCE(BGPU_CHECK(cudaFuncSetAttribute(dgemm_kernel<A_KM, B_KM, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)TileN<BN>::SMEM)));
     if (ceil_div(M, BM) > 65535) return BGPU_ERR_TOOBIG;
     dim3 grid(ceil_div(N, BN), ceil_div(M, BM), batch);
     dgemm_kernel<A_KM, B_KM, BN><<<grid, NT, TileN<BN>::SMEM, st>>>(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C,
@@ -243,12 +239,8 @@ __global__ void scale_kernel(int M, int N, double beta, double *C, long long ldc
 int gemm_f64_grouped(cudaStream_t st, int ntiles, const int4 *d_tiles, const GemmGroup *d_groups, double alpha,
                      double beta) {
     if (ntiles <= 0) return BGPU_OK;
-    static std::atomic<bool> attr_set{false};   // (set once; a second setter is harmless)
-    if (!attr_set) {
-        BGPU_CHECK(cudaFuncSetAttribute(dgemm_grouped_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)TileN<64>::SMEM));
-        attr_set = true;
-    }
+    BGPU_ATTR_ONCE(BGPU_CHECK(cudaFuncSetAttribute(dgemm_grouped_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)TileN<64>::SMEM)));
     dgemm_grouped_kernel<<<ntiles, NT, TileN<64>::SMEM, st>>>(d_tiles, d_groups, alpha, beta);
     BGPU_LAUNCH_CHECK();
     return BGPU_OK;

@@ -24,19 +24,20 @@ int scale_matrix_f64(cudaStream_t st, int M, int N, double beta, double *C, long
                      int lower);
 
 // ---- FP64-accurate GEMM on the INT8 tensor cores (ozaki.cu) ---------------------------------
-// An operand cut into ozaki_slices() int8 slices (stacked, srows rows each, row stride ldk bytes)
-// with one power-of-two exponent per row.
+// An operand cut into `slices` int8 slices (stacked, srows rows each, row stride ldk bytes) with
+// one power-of-two exponent per row.
 struct OzakiOperand {
     long long rows = 0, srows = 0, ldk = 0;
-    int K = 0;
+    int K = 0, slices = 8;
     int8_t *q = nullptr;
     int *e = nullptr;
 };
-int ozaki_slices();
-size_t ozaki_operand_bytes(long long rows, int K);
-// slices of the rows x K operand src (row r at src + r lds) into buf (ozaki_operand_bytes)
-int ozaki_slice(cudaStream_t st, long long rows, int K, const double *src, long long lds, void *buf, OzakiOperand *op);
-// C(i, j) = sum_k A(i, k) B(j, k), C column-major (ldc)
+int ozaki_max_slices();   // 8: FP64-like products
+size_t ozaki_operand_bytes(long long rows, int K, int S);
+// S (4..8) slices of the rows x K operand src (row r at src + r lds) into buf (ozaki_operand_bytes)
+int ozaki_slice(cudaStream_t st, long long rows, int K, const double *src, long long lds, void *buf, OzakiOperand *op,
+                int S);
+// C(i, j) = sum_k A(i, k) B(j, k), C column-major (ldc); A and B cut into the same number of slices
 int ozaki_gemm(cudaStream_t st, const OzakiOperand &A, const OzakiOperand &B, double *C, long long ldc);
 int ozaki_error_flag(int *host_value);
 
@@ -153,8 +154,9 @@ int schur_upper(cudaStream_t st, const DevBlock &B);
 // products): needs the upper lists.
 int schur_assemble_gram(cudaStream_t st, const DevBlock &B, double *M, int m, void *ws, size_t ws_bytes);
 int schur_chunk_default(int n, int precision);
+int schur_ozaki_slices(int precision);   // the slices of an Ozaki precision code (8 when unset)
 // M (m x m, column-major, full symmetric) += the block's contribution sum over its constraints
-// of M_ab = <A_b, X A_a Zi>.  precision 0: FP64 (DMMA), 1: 3xTF32 (tcgen05), 2: FP64-accurate
-// products on the INT8 tensor cores (ozaki.cu).
+// of M_ab = <A_b, X A_a Zi>.  precision 0: FP64 (DMMA), 1: 3xTF32 (tcgen05), 2: products on the
+// INT8 tensor cores (ozaki.cu) with 8 slices (FP64-accurate), (S << 8) | 2 with S = 4..8 slices.
 int schur_assemble(cudaStream_t st, const DevBlock &B, const double *X, const double *Zi, double *M, int m,
                    int precision, int chunk, void *ws, size_t ws_bytes);

@@ -366,12 +366,8 @@ int form_q(cudaStream_t st, const Layout &L, const int2 *items, int nitems, int 
            const double *Xc, const double *Zc, double *Q) {
     if (nitems <= 0) return BGPU_OK;
     if (nmax <= 0 || nmax > NMAX) return BGPU_ERR_ARG;
-    static std::atomic<bool> attr{false};   // (set once; a second setter is harmless)
-    if (!attr) {
-        BGPU_CHECK(cudaFuncSetAttribute(form_q_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)form_q_smem(NMAX)));
-        attr = true;
-    }
+    BGPU_ATTR_ONCE(BGPU_CHECK(cudaFuncSetAttribute(form_q_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)form_q_smem(NMAX))));
     form_q_kernel<<<nitems, 256, form_q_smem(nmax), st>>>(items, L.n, L.m, L.boff, L.poff, P, Xc, Zc, Q);
     BGPU_LAUNCH_CHECK();
     return BGPU_OK;
@@ -397,11 +393,8 @@ int prec(cudaStream_t st, const Layout &L, const int *list, int cnt, int mmax, c
     if (cnt <= 0) return BGPU_OK;
     const size_t smem = (size_t)std::max(mmax, 1) * sizeof(double);
     if (smem > 200 * 1024) return BGPU_ERR_TOOBIG;
-    static std::atomic<bool> attr{false};   // (set once; a second setter is harmless)
-    if (!attr) {
-        BGPU_CHECK(cudaFuncSetAttribute(prec_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-        attr = true;
-    }
+    BGPU_ATTR_ONCE(BGPU_CHECK(cudaFuncSetAttribute(prec_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   200 * 1024)));
     prec_kernel<<<cnt, 256, smem, st>>>(list, L.m, L.moff, L.coff, Lf, D, x);
     BGPU_LAUNCH_CHECK();
     return BGPU_OK;

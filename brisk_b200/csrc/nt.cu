@@ -485,12 +485,8 @@ int scaling_small(cudaStream_t st, int nb, const int *d_n, int nmax, const doubl
     if (nb <= 0) return BGPU_OK;
     if (nmax < 1 || nmax > SMALL_NMAX) return BGPU_ERR_ARG;
     const size_t smem = sizeof(double) * 3 * (size_t)small_ld(nmax) * nmax;
-    static std::atomic<bool> attr{false};   // (set once; a second setter is harmless)
-    if (!attr) {
-        BGPU_CHECK(cudaFuncSetAttribute(scaling_small_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)(sizeof(double) * 3 * small_ld(SMALL_NMAX) * SMALL_NMAX)));
-        attr = true;
-    }
+    BGPU_ATTR_ONCE(BGPU_CHECK(cudaFuncSetAttribute(scaling_small_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)(sizeof(double) * 3 * small_ld(SMALL_NMAX) * SMALL_NMAX))));
     scaling_small_kernel<<<nb, SM_THREADS, smem, st>>>(d_n, LX, LZ, G, lam, W, info);
     BGPU_LAUNCH_CHECK();
     return BGPU_OK;

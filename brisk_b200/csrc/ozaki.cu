@@ -11,31 +11,52 @@
 // (multiplications by powers of two and subtractions of integers: no rounding).
 //
 // Products (ozaki_kernel): A B' = 2^(e_i + f_j) sum_{p,q} 2^(-7(p+q)) (S_p^A S_q^B') with the pairs
-// p + q <= S + 1 kept.  With S = 8 the dropped pairs (p + q >= 10: at most 127^2 2^-70 each) and the
-// slices' truncation (below 2^-56) leave an error below about 2^-53 K 2^(e_i + f_j): FP64-like
-// relative to the largest entries of row i of A and of row j of B.  Each product of int8 slices
-// accumulates exactly in int32 (|sum| <= S 127^2 K < 2^31 for K <= 16000), and
-// all pairs of one diagonal d = p + q share one TMEM accumulator: S accumulators of BN columns side
-// by side in the 512 TMEM columns for the whole K loop.  The epilogue drains them once, smallest
-// diagonal terms first, into FP64: C = 2^(e_i + f_j) sum_d 2^(-7d) ACC_d.
+// p + q <= S + 1 kept.  The dropped pairs (p + q >= S + 2: at most 127^2 2^(-7(p+q)) each) and the
+// slices' truncation (below 2^(-7S) per entry) leave an error below about (S + 3) 2^(-7S) K
+// 2^(e_i + f_j): with S = 8, about 2^-53 K relative to the largest entries of row i of A and of
+// row j of B (FP64-like); with S = 6, 2^-39 K; with S = 5, 2^-32 K.  Each product of int8 slices
+// accumulates exactly in int32 (|sum| <= S 127^2 K < 2^31 for K <= 16000), and all pairs of one
+// diagonal d = p + q share one TMEM accumulator: S accumulators of BN columns side by side in the
+// 512 TMEM columns for the whole K loop.  The epilogue drains them once, smallest diagonal terms
+// first, into FP64: C = 2^(e_i + f_j) sum_d 2^(-7d) ACC_d.
 //
-// One CTA per 128 x 64 tile, as tf32x3.cu: warp 0 / lane 0 the TMA producer (the S slices of A and
-// of B for a 64-byte k-block, 64-byte swizzle, a 2-deep ring), warp 1 / lane 0 the MMA issuer
-// (kind::i8, M = 128, N = 64, K = 32 per instruction), all 4 warps the epilogue.  Every mbarrier
-// wait is bounded; a wait that runs out sets *err and the CTA winds down.  No cluster, no multicast.
+// Tiles (S accumulators of BN columns must fit the 512 TMEM columns): S = 8 and 7 take BN = 64,
+// S = 6 BN = 80, S = 5 BN = 96, S = 4 BN = 128.  With fewer slices the tile is wider, so each
+// MMA reads less shared memory per multiply-add (a 128 x 64 x 32 int8 MMA reads 6 KB for 262 k
+// multiply-adds; 128 x 96 x 32 reads 7 KB for 393 k) as well as issuing fewer MMAs: S = 5 issues
+// 15 per 32-deep k-step and 96 columns, S = 8 36 per 64 columns.
+//
+// One CTA per 128 x BN tile, as tf32x3.cu: warp 0 / lane 0 the TMA producer (the S slices of A and
+// of B for a 64-byte k-block, 64-byte swizzle, a 2- or 3-deep ring), warp 1 / lane 0 the MMA
+// issuer (kind::i8, M = 128, N = BN, K = 32 per instruction), all 4 warps the epilogue (16
+// columns at a time over all S accumulators).  Every mbarrier wait is bounded; a wait that runs
+// out sets *err and the CTA winds down.  No cluster, no multicast.
 #include "common.cuh"
 #include "kernels.h"
 #include "tcgen05.cuh"
 
 namespace {
 using namespace tc;
-constexpr int OZ_S = 8;                  // slices per operand (56 bits)
-constexpr int BM = 128, BN = 64, BK = 64, STAGES = 2, NTHREADS = 128;
-constexpr int A_TILE = BM * BK, B_TILE = BN * BK;            // bytes of one slice's tile
-constexpr int STAGE = OZ_S * (A_TILE + B_TILE);              // 96 KB
-constexpr int TMEM_COLS = 512;                               // OZ_S accumulators of BN columns
-constexpr size_t SMEM = (size_t)STAGES * STAGE + 1024 /*align*/ + 256 /*barriers*/;
-static_assert(OZ_S * BN <= TMEM_COLS, "accumulators must fit in TMEM");
+constexpr int OZ_SMAX = 8;               // most slices per operand (56 bits)
+constexpr int BM = 128, BK = 64, NTHREADS = 128;
+constexpr int A_TILE = BM * BK;          // bytes of one slice's A tile
+constexpr int TMEM_COLS = 512;           // S accumulators of BN columns
+
+template <int S> struct OzCfg;           // tile width and ring depth per slice count
+template <> struct OzCfg<8> { static constexpr int BN = 64, STAGES = 2; };
+template <> struct OzCfg<7> { static constexpr int BN = 64, STAGES = 2; };
+template <> struct OzCfg<6> { static constexpr int BN = 80, STAGES = 2; };
+template <> struct OzCfg<5> { static constexpr int BN = 96, STAGES = 3; };
+template <> struct OzCfg<4> { static constexpr int BN = 128, STAGES = 3; };
+template <int S> struct OzShape {
+    static constexpr int BN = OzCfg<S>::BN, STAGES = OzCfg<S>::STAGES;
+    static constexpr int B_TILE = BN * BK;
+    static constexpr int STAGE = S * (A_TILE + B_TILE);
+    static constexpr size_t SMEM = (size_t)STAGES * STAGE + 1024 /*align*/ + 256 /*barriers*/;
+    static_assert(S * BN <= TMEM_COLS, "accumulators must fit in TMEM");
+    static_assert(STAGE % 1024 == 0, "stages keep the 1024-byte alignment of the swizzled tiles");
+    static_assert(SMEM <= 232448, "shared memory of one CTA");
+};
 
 // tcgen05 shared-memory matrix descriptor: K-major, 64-byte swizzle, 8-row groups 512 B apart
 __device__ __forceinline__ uint64_t smem_desc64(uint32_t saddr) {
@@ -60,10 +81,13 @@ __device__ __forceinline__ void umma_i8(uint32_t tmem_d, uint64_t a, uint64_t b,
         ::"r"(tmem_d), "l"(a), "l"(b), "r"(idesc), "r"(acc));
 }
 
+template <int S>
 __global__ void __launch_bounds__(NTHREADS, 1)
     ozaki_kernel(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorMap tB, long long a_slice_rows,
                  long long b_slice_rows, const int *__restrict__ ea, const int *__restrict__ eb, double *C, long long ldc,
                  int M, int N, int K, int *err) {
+    using Sh = OzShape<S>;
+    constexpr int BN = Sh::BN, STAGES = Sh::STAGES, B_TILE = Sh::B_TILE, STAGE = Sh::STAGE;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     uint64_t *full = (uint64_t *)(smem + STAGES * STAGE);
@@ -104,9 +128,9 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             uint8_t *st = smem + s * STAGE;
             mbar_expect_tx(&full[s], STAGE);
             const int x = kb * BK;
-            for (int p = 0; p < OZ_S; p++) {
+            for (int p = 0; p < S; p++) {
                 tma_load_2d(st + p * A_TILE, &tA, &full[s], x, (int)(p * a_slice_rows + m0));
-                tma_load_2d(st + OZ_S * A_TILE + p * B_TILE, &tB, &full[s], x, (int)(p * b_slice_rows + n0));
+                tma_load_2d(st + S * A_TILE + p * B_TILE, &tB, &full[s], x, (int)(p * b_slice_rows + n0));
             }
             issued++;
         }
@@ -124,12 +148,12 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             for (int ks = 0; ks < BK / 32; ks++) {   // K-step of 32 int8 = 32 bytes inside the swizzle atom
                 const uint32_t off = ks * 32;
 #pragma unroll
-                for (int d = 0; d < OZ_S; d++) {       // diagonal p + q = d + 2 (0-based slices: p + q = d)
+                for (int d = 0; d < S; d++) {          // diagonal p + q = d + 2 (0-based slices: p + q = d)
 #pragma unroll
                     for (int p = 0; p <= d; p++) {
                         const int q = d - p;
                         const uint64_t a = smem_desc64(base + p * A_TILE + off);
-                        const uint64_t b = smem_desc64(base + OZ_S * A_TILE + q * B_TILE + off);
+                        const uint64_t b = smem_desc64(base + S * A_TILE + q * B_TILE + off);
                         umma_i8(tmem + (uint32_t)(d * BN), a, b, idesc, (kb | ks | p) != 0);
                     }
                 }
@@ -144,27 +168,28 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     tc_fence_after();
     const bool good = __all_sync(0xffffffffu, ok && !*(volatile int *)bad);
     if (good) {
+        // 16 columns at a time: their S accumulators, smallest diagonal terms first
         const int row = m0 + warp * 32 + lane;
-        double acc[BN];
-#pragma unroll
-        for (int c = 0; c < BN; c++) acc[c] = 0.0;
+        const int e = row < M ? ea[row] : 0;
 #pragma unroll 1
-        for (int d = OZ_S - 1; d >= 0; d--) {
-            const double w = ldexp(1.0, -7 * (d + 2));
+        for (int c0 = 0; c0 < BN; c0 += 16) {
+            double acc[16];
 #pragma unroll
-            for (int c0 = 0; c0 < BN; c0 += 16) {
+            for (int j = 0; j < 16; j++) acc[j] = 0.0;
+#pragma unroll
+            for (int d = S - 1; d >= 0; d--) {
+                const double w = ldexp(1.0, -7 * (d + 2));
                 uint32_t r[16];
                 tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(d * BN + c0), r);
 #pragma unroll
-                for (int j = 0; j < 16; j++) acc[c0 + j] += w * (double)(int)r[j];
+                for (int j = 0; j < 16; j++) acc[j] += w * (double)(int)r[j];
             }
-        }
-        if (row < M) {
-            const int e = ea[row];
+            if (row < M) {
 #pragma unroll
-            for (int c = 0; c < BN; c++) {
-                const int col = n0 + c;
-                if (col < N) C[(long long)row + (long long)col * ldc] = ldexp(acc[c], e + eb[col]);
+                for (int j = 0; j < 16; j++) {
+                    const int col = n0 + c0 + j;
+                    if (col < N) C[(long long)row + (long long)col * ldc] = ldexp(acc[j], e + eb[col]);
+                }
             }
         }
     } else if (threadIdx.x == 0) {
@@ -179,8 +204,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
 
 // One warp per row: the row's exponent and its S digits (row stride ldk bytes, slice p at
 // dst + p * slice_bytes; the K..ldk padding is zero).
-__global__ void slice_kernel(int rows, int K, const double *__restrict__ src, long long lds, int8_t *dst, long long ldk,
-                             long long slice_bytes, int *exps) {
+__global__ void slice_kernel(int rows, int K, int S, const double *__restrict__ src, long long lds, int8_t *dst,
+                             long long ldk, long long slice_bytes, int *exps) {
     const int r = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
     if (r >= rows) return;
     const double *x = src + (long long)r * lds;
@@ -194,7 +219,8 @@ __global__ void slice_kernel(int rows, int K, const double *__restrict__ src, lo
     for (long long k = lane; k < ldk; k += 32) {
         double a = k < K ? ldexp(x[k], -e) : 0.0;
 #pragma unroll
-        for (int p = 0; p < OZ_S; p++) {
+        for (int p = 0; p < OZ_SMAX; p++) {
+            if (p >= S) break;
             a *= 128.0;
             const double t = trunc(a);
             a -= t;
@@ -224,52 +250,71 @@ __device__ int g_ozaki_err = 0;   // sticky flag of the bounded waits (zero at m
 inline long long round_up(long long x, long long a) { return (x + a - 1) / a * a; }
 }  // namespace
 
-int ozaki_slices() { return OZ_S; }
+int ozaki_max_slices() { return OZ_SMAX; }
 
-// bytes of the slices (and exponents) of a rows x K operand
-size_t ozaki_operand_bytes(long long rows, int K) {
+// bytes of the S slices (and exponents) of a rows x K operand
+size_t ozaki_operand_bytes(long long rows, int K, int S) {
     const long long ldk = round_up(K, 64), srows = round_up(rows, 128);
-    return (size_t)OZ_S * srows * ldk + sizeof(int) * srows + 1024;
+    return (size_t)S * srows * ldk + sizeof(int) * srows + 1024;
 }
 
-// The operand's slices into buf (ozaki_operand_bytes): returns the slice layout in *sl.
-int ozaki_slice(cudaStream_t st, long long rows, int K, const double *src, long long lds, void *buf, OzakiOperand *op) {
+// The operand's S slices into buf (ozaki_operand_bytes): returns the slice layout in *op.
+int ozaki_slice(cudaStream_t st, long long rows, int K, const double *src, long long lds, void *buf, OzakiOperand *op,
+                int S) {
+    if (S < 4 || S > OZ_SMAX) return BGPU_ERR_ARG;
     const long long ldk = round_up(K, 64), srows = round_up(rows, 128);
     op->rows = rows;
     op->srows = srows;
     op->K = K;
     op->ldk = ldk;
+    op->slices = S;
     op->q = (int8_t *)(((uintptr_t)buf + 255) & ~(uintptr_t)255);
-    op->e = (int *)(op->q + (size_t)OZ_S * srows * ldk);
+    op->e = (int *)(op->q + (size_t)S * srows * ldk);
     if (rows <= 0) return BGPU_OK;
     if ((rows + 7) / 8 > (1LL << 31) - 1) return BGPU_ERR_TOOBIG;
-    slice_kernel<<<ceil_div(rows * 32, 256), 256, 0, st>>>((int)rows, K, src, lds, op->q, ldk, srows * ldk, op->e);
+    slice_kernel<<<ceil_div(rows * 32, 256), 256, 0, st>>>((int)rows, K, S, src, lds, op->q, ldk, srows * ldk, op->e);
     BGPU_LAUNCH_CHECK();
     return BGPU_OK;
 }
 
-// C (column-major, ldc) = A B' from the sliced operands (A: M rows, B: N rows, both K)
-int ozaki_gemm(cudaStream_t st, const OzakiOperand &A, const OzakiOperand &B, double *C, long long ldc) {
+namespace {
+template <int S>
+int ozaki_launch(cudaStream_t st, const OzakiOperand &A, const OzakiOperand &B, double *C, long long ldc) {
+    using Sh = OzShape<S>;
     const int M = (int)A.rows, N = (int)B.rows, K = A.K;
-    if (M <= 0 || N <= 0 || K <= 0) return BGPU_OK;
-    if (B.K != K || K > 16000 || OZ_S * A.srows > (1LL << 31) - 1 || OZ_S * B.srows > (1LL << 31) - 1)
-        return BGPU_ERR_ARG;
     CUtensorMap mA, mB;
     int rc;
-    if ((rc = make_map_i8(&mA, A.q, OZ_S * A.srows, K, A.ldk, BM)) || (rc = make_map_i8(&mB, B.q, OZ_S * B.srows, K, B.ldk, BN)))
+    if ((rc = make_map_i8(&mA, A.q, S * A.srows, K, A.ldk, BM)) || (rc = make_map_i8(&mB, B.q, S * B.srows, K, B.ldk, Sh::BN)))
         return rc;
-    static std::atomic<bool> attr{false};   // (set once; a second setter is harmless)
-    if (!attr) {
-        BGPU_CHECK(cudaFuncSetAttribute(ozaki_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM));
-        attr = true;
-    }
+    BGPU_ATTR_ONCE(BGPU_CHECK(cudaFuncSetAttribute(ozaki_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)Sh::SMEM)));
     void *d = nullptr;
     BGPU_CHECK(cudaGetSymbolAddress(&d, g_ozaki_err));
     if (ceil_div(M, BM) > 65535) return BGPU_ERR_TOOBIG;
-    dim3 grid(ceil_div(N, BN), ceil_div(M, BM));
-    ozaki_kernel<<<grid, NTHREADS, SMEM, st>>>(mA, mB, A.srows, B.srows, A.e, B.e, C, ldc, M, N, K, (int *)d);
+    dim3 grid(ceil_div(N, Sh::BN), ceil_div(M, BM));
+    ozaki_kernel<S><<<grid, NTHREADS, Sh::SMEM, st>>>(mA, mB, A.srows, B.srows, A.e, B.e, C, ldc, M, N, K, (int *)d);
     BGPU_LAUNCH_CHECK();
     return BGPU_OK;
+}
+}  // namespace
+
+// C (column-major, ldc) = A B' from the sliced operands (A: M rows, B: N rows, both K, the same
+// number of slices)
+int ozaki_gemm(cudaStream_t st, const OzakiOperand &A, const OzakiOperand &B, double *C, long long ldc) {
+    const int M = (int)A.rows, N = (int)B.rows, K = A.K;
+    if (M <= 0 || N <= 0 || K <= 0) return BGPU_OK;
+    const int S = A.slices;
+    if (B.K != K || B.slices != S || K > 16000 || (long long)S * A.srows > (1LL << 31) - 1 ||
+        (long long)S * B.srows > (1LL << 31) - 1)
+        return BGPU_ERR_ARG;
+    switch (S) {
+        case 8: return ozaki_launch<8>(st, A, B, C, ldc);
+        case 7: return ozaki_launch<7>(st, A, B, C, ldc);
+        case 6: return ozaki_launch<6>(st, A, B, C, ldc);
+        case 5: return ozaki_launch<5>(st, A, B, C, ldc);
+        case 4: return ozaki_launch<4>(st, A, B, C, ldc);
+        default: return BGPU_ERR_ARG;
+    }
 }
 
 int ozaki_error_flag(int *host_value) {

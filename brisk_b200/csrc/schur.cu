@@ -519,6 +519,11 @@ int atop_f64(cudaStream_t st, const DevBlock &B, const double *y, double alpha, 
 // tf32 operand rows padded to a multiple of 4 floats: the tensor maps need 16-byte strides
 static inline int tf32_ld(int n) { return (n + 3) / 4 * 4; }
 
+int schur_ozaki_slices(int precision) {
+    const int S = (precision >> 8) & 0xf;
+    return S == 0 ? 8 : S;
+}
+
 int schur_chunk_default(int n, int precision) {
     // the widest chunk whose workspace stays within 4 GB: a wider chunk reads each constraint's
     // entry list fewer times in the gather.  Measured on B200 (rand400 FP64, rand1000 FP64 and
@@ -532,8 +537,10 @@ int schur_chunk_default(int n, int precision) {
 size_t schur_ws_bytes(int n, int chunk, int precision) {
     const size_t nn = (size_t)n * n * chunk;
     if (precision == 0) return 2 * nn * sizeof(double);            // T, G
-    if (precision == 2)                                            // T, G, the slices of T and of X
-        return 2 * nn * sizeof(double) + ozaki_operand_bytes((long long)n * chunk, n) + ozaki_operand_bytes(n, n);
+    if ((precision & 0xff) == 2) {                                 // T, G, the slices of T and of X
+        const int S = schur_ozaki_slices(precision);
+        return 2 * nn * sizeof(double) + ozaki_operand_bytes((long long)n * chunk, n, S) + ozaki_operand_bytes(n, n, S);
+    }
     const size_t ld = tf32_ld(n);
     // T hi/lo (n K rows of ld), G (float, n K x n), X hi/lo (n rows of ld), plus 256 B alignment slack each
     return (2 * (size_t)n * chunk * ld + nn + 2 * (size_t)n * ld) * sizeof(float) + 5 * 256;
@@ -548,19 +555,21 @@ int schur_assemble(cudaStream_t st, const DevBlock &B, const double *X, const do
     if (ws_bytes < schur_ws_bytes(n, K, precision)) return BGPU_ERR_ARG;
     const size_t nnK = (size_t)n * n * K;
     dim3 tgrid(ceil_div(n, TP_Q), ceil_div(n, TP_K), K);
-    if (precision == 0 || precision == 2) {
+    const bool oz = (precision & 0xff) == 2;
+    if (precision == 0 || oz) {
         double *T = (double *)ws, *G = T + nnK;
-        // FP64-accurate products on the INT8 tensor cores: X's slices once, T's per chunk
-        uint8_t *sa = (uint8_t *)(G + nnK), *sb = sa + ozaki_operand_bytes((long long)n * K, n);
+        // products on the INT8 tensor cores: X's slices once, T's per chunk
+        const int S = oz ? schur_ozaki_slices(precision) : 0;
+        uint8_t *sa = (uint8_t *)(G + nnK), *sb = oz ? sa + ozaki_operand_bytes((long long)n * K, n, S) : nullptr;
         OzakiOperand opA, opB;
-        if (precision == 2)
-            if (int rc = ozaki_slice(st, n, n, X, n, sb, &opB)) return rc;
+        if (oz)
+            if (int rc = ozaki_slice(st, n, n, X, n, sb, &opB, S)) return rc;
         for (int a0 = 0; a0 < B.ncon; a0 += K) {
             tprod_kernel<double><<<tgrid, 256, 0, st>>>(n, n, K, a0, B.ncon, B.cptr, B.ccol, B.cpos, B.cval, Zi, T, nullptr);
             BGPU_LAUNCH_CHECK();
             int rc;
-            if (precision == 2) {
-                if ((rc = ozaki_slice(st, (long long)n * K, n, T, n, sa, &opA))) return rc;
+            if (oz) {
+                if ((rc = ozaki_slice(st, (long long)n * K, n, T, n, sa, &opA, S))) return rc;
                 rc = ozaki_gemm(st, opA, opB, G, (long long)n * K);
             } else {
                 rc = gemm_f64(st, 1, 1, n * K, n, n, 1.0, T, n, 0, X, n, 0, 0.0, G, (long long)n * K, 0, 1, 0);
@@ -715,12 +724,8 @@ int schur_assemble_small(cudaStream_t st, int count, const int *d_blocks, int nm
                          const double *Xcat, const double *Zicat, double *M, int m) {
     if (count <= 0) return BGPU_OK;
     if (nmax <= 0 || nmax > SB_NMAX) return BGPU_ERR_ARG;
-    static std::atomic<bool> attr{false};   // (set once; a second setter is harmless)
-    if (!attr) {
-        BGPU_CHECK(cudaFuncSetAttribute(small_schur_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)schur_small_smem(SB_NMAX)));
-        attr = true;
-    }
+    BGPU_ATTR_ONCE(BGPU_CHECK(cudaFuncSetAttribute(small_schur_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)schur_small_smem(SB_NMAX))));
     small_schur_kernel<<<count, SB_W * 32, schur_small_smem(nmax), st>>>(d_blocks, d_n, d_ncon, con_tab, cptr_tab,
                                                                          cpos_tab, cval_tab, d_boff, Xcat, Zicat, M, m);
     BGPU_LAUNCH_CHECK();

@@ -252,15 +252,14 @@ int set_smem(F f, size_t bytes) {
     BGPU_CHECK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
     return BGPU_OK;
 }
-bool g_attr_done = false;
+std::atomic<unsigned long long> g_attr_done{0};   // one bit per device
 int attrs() {
-    if (g_attr_done) return BGPU_OK;
-    int rc;
-    if ((rc = set_smem(chol_inv_kernel, smem2()))) return rc;
-    if ((rc = set_smem(gemm_small_kernel, smem2()))) return rc;
-    if ((rc = set_smem(lammin_kernel, smem3()))) return rc;
-    g_attr_done = true;
-    return BGPU_OK;
+    return once_per_device(g_attr_done, [] {
+        int rc;
+        if ((rc = set_smem(chol_inv_kernel, smem2()))) return rc;
+        if ((rc = set_smem(gemm_small_kernel, smem2()))) return rc;
+        return set_smem(lammin_kernel, smem3());
+    });
 }
 }  // namespace
 

@@ -998,8 +998,28 @@ class Solver {
         else newton_mv(x, y);
     }
     bool m_exact = true;      // M was assembled in FP64 (the residual may use it)
-    bool asm_fp64 = false;    // the mixed path turned to its late (FP64-accurate) assembly
-    const char *asm_label = "fp64";   // the last assembly's precision (the -vv log)
+    bool asm_fp64 = false;    // the mixed path turned to its late assembly
+    bool late_exact = false;  // ... and from its preconditioner-grade late form to the FP64-accurate one
+    int cur_prec = 0;         // the last assembly's precision code (schur_assemble's)
+    char asm_label[16] = "fp64";   // the last assembly's precision (the -vv log)
+    // the precision of the next assembly: the 3xTF32 path's late form once asm_fp64 is set (with
+    // fewer than 8 Ozaki slices a preconditioner-grade M, until late_exact turns it to 8 slices)
+    int next_prec() const {
+        if (asm_prec != 1) return asm_prec;
+        if (!asm_fp64) return 1;
+        const int late = opt.late_prec;
+        return (late_exact && late != 0) ? 2 : late;
+    }
+    static bool prec_exact(int p) { return p == 0 || p == 2; }
+    // the mixed path's response to a late M that no longer preconditions the FP64 operator: from
+    // 3xTF32 to the late form; from a preconditioner-grade late form to the FP64-accurate one.
+    // Returns false when nothing more accurate is left.
+    bool raise_precision() {
+        if (asm_prec != 1) return false;
+        if (!asm_fp64) { asm_fp64 = true; return true; }
+        if (!late_exact && !prec_exact(opt.late_prec)) { late_exact = true; return true; }
+        return false;
+    }
     double schur_solve(const std::vector<double> &rhs, std::vector<double> &x, double tol_rel);
     // step length
     double maxstep(int primal, int K);
@@ -1288,7 +1308,7 @@ void Solver::setup() {
     chunk64 = opt.chunk > 0 ? opt.chunk : schur_chunk_default(nmax, 0);
     chunk_oz = opt.chunk > 0 ? opt.chunk : schur_chunk_default(nmax, 2);
     ws_bytes = std::max(schur_ws_bytes(nmax, chunk, asm_prec), schur_ws_bytes(nmax, chunk64, 0));
-    if (asm_prec == 2 || (asm_prec == 1 && opt.late_prec == 2))
+    if (asm_prec == 2 || (asm_prec == 1 && (opt.late_prec & 0xff) == 2))   // (8 slices: the most workspace)
         ws_bytes = std::max(ws_bytes, schur_ws_bytes(nmax, chunk_oz, 2));
     for (int k = 0; k < nb; k++)
         if (dense_route[k])
@@ -1608,10 +1628,13 @@ void Solver::assemble(std::vector<double> &) {
     CU(cudaMemsetAsync(M, 0, sizeof(double) * (size_t)m * m, g.st));
     CU(cudaEventRecord(ev0, g.st));
     // 3xTF32 until the mixed path turns to its late precision (FP64 or the Ozaki slices)
-    const int prec = asm_prec == 1 ? (asm_fp64 ? opt.late_prec : 1) : asm_prec;
-    m_exact = prec != 1;
-    const int kchunk = prec == 1 ? chunk : prec == 2 ? chunk_oz : chunk64;
-    asm_label = prec == 1 ? "tf32x3" : prec == 2 ? "ozaki" : "fp64";
+    const int prec = next_prec();
+    const bool oz = (prec & 0xff) == 2;
+    cur_prec = prec;
+    m_exact = prec_exact(prec);
+    const int kchunk = prec == 1 ? chunk : oz ? chunk_oz : chunk64;
+    if (oz) snprintf(asm_label, sizeof asm_label, "ozaki%d", schur_ozaki_slices(prec));
+    else snprintf(asm_label, sizeof asm_label, "%s", prec == 1 ? "tf32x3" : "fp64");
     assemble_small(cat.*xmem(), cat.Zi);
     for (int k = 0; k < nb; k++) {
         if (in_sb[k]) {
@@ -1620,7 +1643,7 @@ void Solver::assemble(std::vector<double> &) {
         }
         const double *Xa = da[k].*xmem();
         if (dense_route[k])   // (the dense route has no Ozaki form: FP64 there)
-            RC(schur_assemble_dense(g.st, db[k], Xa, da[k].Zi, M, m, prec == 2 ? 0 : prec, prec == 1 ? chunk : chunk64,
+            RC(schur_assemble_dense(g.st, db[k], Xa, da[k].Zi, M, m, oz ? 0 : prec, prec == 1 ? chunk : chunk64,
                                     ws, ws_bytes));
         else
             RC(schur_assemble(g.st, db[k], Xa, da[k].Zi, M, m, prec, kchunk, ws, ws_bytes));
@@ -1633,7 +1656,7 @@ void Solver::assemble(std::vector<double> &) {
     float ms = 0;
     CU(cudaEventElapsedTime(&ms, ev0, ev1));
     schur_dev_time += ms * 1e-3;
-    if (prec == 1 || prec == 2) {
+    if (prec == 1 || oz) {
         int bad = 0;
         RC(prec == 1 ? tf32x3_error_flag(&bad) : ozaki_error_flag(&bad));
         if (bad) throw GpuFail{BGPU_ERR_TIMEOUT, __LINE__};
@@ -1831,10 +1854,10 @@ double Solver::schur_solve(const std::vector<double> &rhs, std::vector<double> &
     const double rel = nrm(r) / nb_;
     if (is_float && (used > 4 || best > tol || rel > std::max(1e-9, 10 * tol_rel))) want_double = true;
     // the mixed path: when PCG cannot reach the tolerance against the FP64 operator with the
-    // factor of the FP32-accurate M, the following iterations assemble M in FP64
-    if (!m_exact && (best > tol || rel > std::max(1e-9, 10 * tol_rel)) && !asm_fp64) {
-        asm_fp64 = true;
-        if (opt.verbose > 1) log_printf(0, "   mixed path: PCG missed %.1e (rel %.1e): FP64-accurate assembly from here on\n", tol / nb_, rel);
+    // factor of the approximate M, the following iterations assemble M more accurately
+    if (!m_exact && (best > tol || rel > std::max(1e-9, 10 * tol_rel)) && raise_precision()) {
+        if (opt.verbose > 1)
+            log_printf(0, "   mixed path: PCG missed %.1e (rel %.1e): more accurate assembly from here on\n", tol / nb_, rel);
     }
     return rel;
 }
@@ -2168,7 +2191,7 @@ int Solver::run(ResultData &res) {
     nfloat = nfactor = pcg_iters = 0;
     mu_now = 1e300;
     m_exact = true;
-    asm_fp64 = false;
+    asm_fp64 = late_exact = false;
     schur_flops = schur_dev_time = 0;
     CU(cudaEventRecord(evs0, g.st));
     std::vector<double> y(m, 0.0), ybest(m, 0.0), dy, rp(m), a0, h(m, 0.0), rhs(m), qv, ev(m), wv;
@@ -2369,22 +2392,34 @@ int Solver::run(ResultData &res) {
             // the 3xTF32 M is FP32-accurate and its factor needed a shift: PCG against the FP64
             // operator with the shifted factor (schur_solve turns to FP64 assembly if it misses)
             if (opt.verbose > 1) log_printf(0, "   mixed path: the 3xTF32 M factored with shift %.1e\n", reg);
-        } else if (!m_exact && (frc != 0 || reg > 0)) {
-            // the 3xTF32 M is FP32-accurate: once its factor needs a regularization it no longer
-            // preconditions the FP64 system; this and the later iterations assemble in FP64
-            asm_fp64 = true;
+        } else if (!m_exact && (frc != 0 || reg > 0) && raise_precision()) {
+            // an approximate M (3xTF32, or the preconditioner-grade late form): once its factor
+            // needs a regularization it no longer preconditions the FP64 system; this and the later
+            // iterations assemble more accurately
             reg_hint = false;
             reg_ok = 0;
-            if (opt.verbose > 1) log_printf(0, "   mixed path: the FP32-accurate M needed a shift: FP64-accurate assembly from here on\n");
+            if (opt.verbose > 1)
+                log_printf(0, "   mixed path: the %s M needed a shift: more accurate assembly from here on\n", asm_label);
             tm.chol += wtime() - tc;
             ts = wtime();
             assemble(tmpv);
             tc = wtime();
             tm.schur += tc - ts;
             frc = factor();
+            if (!m_exact && (frc != 0 || reg > 0) && raise_precision()) {   // the late form needed one too
+                if (opt.verbose > 1)
+                    log_printf(0, "   mixed path: the %s M needed a shift: FP64-accurate assembly from here on\n", asm_label);
+                reg_hint = false;
+                reg_ok = 0;
+                ts = wtime();
+                assemble(tmpv);
+                tc = wtime();
+                tm.schur += tc - ts;
+                frc = factor();
+            }
         }
         if (frc != 0) { status = 4; tm.chol += wtime() - tc; break; }
-        if (!m_exact && !opt.mixed_shift && min_pivot < 1e-4) {
+        if (cur_prec == 1 && !asm_fp64 && !opt.mixed_shift && min_pivot < 1e-4) {
             // the FP32-accurate M is near the end of its use: its smallest scaled pivot falls by
             // 10-20x an iteration, and the factor of the next one would need a shift (rand1000: pivot
             // 7.9e-5, then a shift) — the next iterations assemble in FP64 directly

@@ -80,7 +80,9 @@ struct Options {
     int asm_prec = -1;          // Schur assembly: -1 auto (FP64), 0 FP64, 1 3xTF32, 2 FP64-accurate on the
                                 // INT8 tensor cores (Ozaki slices)
     int late_prec = 2;          // 3xTF32 path: the assembly once the FP32-accurate M no longer serves (0 FP64,
-                                // 2 Ozaki slices)
+                                // 2 Ozaki with 8 slices, FP64-accurate; (S << 8) | 2 with S = 4..7 slices, a
+                                // preconditioner-grade M whose PCG residuals are taken with the FP64 operator,
+                                // turned to 8 slices if its factor needs a shift or PCG misses)
     double mu_switch = 1e-4;    // 3xTF32 path: the factor goes to FP64 once scaled mu < mu_switch
     int mixed_shift = 0;        // 3xTF32 path: 1 keeps a shifted factor of M as the PCG preconditioner (slower
                                 // on rand1000: 170 PCG steps per solve); 0 re-assembles in FP64

@@ -686,12 +686,8 @@ int factor(cudaStream_t st, Factor &F, const double *M, long long ldm, const dou
     const Analysis &A = *F.A;
     sp_init_kernel<<<1, 1, 0, st>>>(F.info, F.pmin);
     BGPU_LAUNCH_CHECK();
-    static std::atomic<bool> attr{false};   // (set once; a second setter is harmless)
-    if (!attr) {
-        BGPU_CHECK(cudaFuncSetAttribute(front_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)((FS_MAX | 1) * FS_MAX * sizeof(double))));
-        attr = true;
-    }
+    BGPU_ATTR_ONCE(BGPU_CHECK(cudaFuncSetAttribute(front_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)((FS_MAX | 1) * FS_MAX * sizeof(double)))));
     for (size_t l = 0; l + 1 < A.lvptr.size(); l++) {
         const int lo = A.lvptr[l], cnt = A.lvptr[l + 1] - lo, ns_ = F.lvsplit[l];
         if (ns_ > 0) {

@@ -209,12 +209,8 @@ int launch(cudaStream_t st, int M, int N, int K, const float *Ah, const float *A
     if ((rc = make_map(&mAh, Ah, M, K, lda, BM)) || (rc = make_map(&mAl, Al, M, K, lda, BM)) ||
         (rc = make_map(&mBh, Bh, N, K, ldb, BN)) || (rc = make_map(&mBl, Bl, N, K, ldb, BN)))
         return rc;
-    static std::atomic<bool> attr{false};   // (set once; a second setter is harmless)
-    if (!attr) {
-        BGPU_CHECK(cudaFuncSetAttribute(tf32x3_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)Cfg<BN>::SMEM));
-        attr = true;
-    }
+    BGPU_ATTR_ONCE(BGPU_CHECK(cudaFuncSetAttribute(tf32x3_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)Cfg<BN>::SMEM)));
     int *err = err_flag();
     if (!err) return BGPU_ERR_NOMEM;
     dim3 grid(ceil_div(N, BN), ceil_div(M, BM));

@@ -66,6 +66,7 @@ def lib():
         "bgpu_nt_ws_bytes": ([I], SZ),
         "bgpu_ozaki_ws_bytes": ([I, I, I], SZ),
         "bgpu_gemm_ozaki": ([I, I, I, P, I64, P, I64, P, I64, P, SZ, P], I),
+        "bgpu_gemm_ozaki_slices": ([I, I, I, I, P, I64, P, I64, P, I64, P, SZ, P], I),
         "bgpu_nt_scaling": ([I, P, P, P, P, P, P, SZ, P, P], I),
     }
     for name, (args, res) in sigs.items():

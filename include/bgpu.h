@@ -37,6 +37,19 @@ BGPU_API int bgpu_sync(void *stream);
 BGPU_API const char *bgpu_version(void);
 /* Number of kernels this library has launched since it was loaded (all entry points). */
 BGPU_API long long bgpu_launch_count(void);
+/* The bound of the triangular solves' device-side waits (bgpu_trsv, bgpu_trsv_f32,
+ * bgpu_trsv_noalloc and the solves inside brisk_solve_*): the number of polls of an awaited flag,
+ * each followed by a 64 ns sleep, after which the waiting block row gives up, the solve sets its
+ * error flag and every CTA returns.  0 restores the default, 2^22 polls (about a second).  The
+ * tensor-core GEMMs' barrier waits keep their fixed bound of 2^22 polls.  No counterpart in the
+ * reference (its CPU solves do not wait on other threads' flags). */
+BGPU_API void bgpu_set_wait_limit(unsigned polls);
+/* Failure-path testing of the bounded waits: from now on, the CTA of block row r (64 rows each)
+ * of every triangular solve computes its rows but does not publish its flag, so the block rows
+ * that depend on it wait until the bound of bgpu_set_wait_limit runs out and the solve reports
+ * BGPU_ERR_TIMEOUT; r < 0 restores normal solves (the default).  A test hook with no
+ * counterpart in the reference: no GPU fault, hang or trap is involved. */
+BGPU_API void bgpu_test_hold_trsv_row(int r);
 
 /* An SDPA sparse file read into host arrays that the library owns: the reader of brisk_solve_file
  * (the reference's read_sdpa, problem.c:426, and its tokenizers, problem.c:58-91: comment lines,
@@ -105,7 +118,8 @@ BGPU_API void bgpu_batch_destroy(bgpu_batch *h);
 BGPU_API int bgpu_result_measures(const struct BriskResult *res, double *out8);
 
 /* Workspace bytes of bgpu_schur_assemble for a block of order n, chunk constraints per GEMM
- * (8, 16, 32 or 64; 0 picks the default) and precision (0 FP64, 1 3xTF32). */
+ * (8, 16, 32 or 64; 0 picks the default) and precision (0 FP64, 1 3xTF32, 2 the Ozaki products
+ * with 8 slices, (S << 8) | 2 with S = 4..8 slices, as bgpu_gemm_ozaki_slices). */
 BGPU_API size_t bgpu_schur_ws_bytes(int n, int chunk, int precision);
 BGPU_API int bgpu_schur_chunk_default(int n, int precision);
 
@@ -179,12 +193,14 @@ BGPU_API int bgpu_trsv_f32(int n, const float *d_L, int lda, const float *d_dinv
 /* bgpu_trsv without caller-provided scratch, for callers that cannot allocate device memory
  * where they solve (between loop steps where cudaMalloc/cudaFree would synchronize the device,
  * or under another allocator that owns the device memory).  It has no counterpart in the
- * reference.  The block-row flags and the wait-error flag live in a static 16 KB device array of
- * the library, so n <= 262144 (64 x 4096 block rows); a larger n returns BGPU_ERR_TOOBIG with a
- * message.  The first call on each device sets the array up (its device address and cleared
- * flags); make that first call before any stream capture.  The call waits for the stream and
- * returns BGPU_ERR_TIMEOUT when a bounded device wait gave up.  Every call on a device shares the
- * array: calls that overlap on the GPU (other streams, other threads) race. */
+ * reference.  The block-row flags and the wait-error flag live in a static 8 KB device array of
+ * the library.  The limit on n is the solve's own: one CTA per block row of 64 rows, all resident
+ * at once, so n <= 64 x (SMs x resident CTAs per SM) -- on a B200 148 x 8 block rows, n <= 75776;
+ * a larger n returns BGPU_ERR_TOOBIG with a message that gives the limit.  The first call on each
+ * device looks up the array's device address.  Every call waits for the stream (it reads the
+ * error flag back), so a call cannot be made while the stream is being captured into a CUDA
+ * graph; it returns BGPU_ERR_TIMEOUT when a bounded device wait gave up.  Every call on a device
+ * shares the array: calls that overlap on the GPU (other streams, other threads) race. */
 BGPU_API int bgpu_trsv_noalloc(int n, const double *d_L, int lda, const double *d_dinv, double *d_x, int trans,
                                void *stream);
 
@@ -229,6 +245,14 @@ BGPU_API int bgpu_small_gemm(int nb, const int *d_n, int ta, int tb, double alph
 BGPU_API size_t bgpu_ozaki_ws_bytes(int M, int N, int K);
 BGPU_API int bgpu_gemm_ozaki(int M, int N, int K, const double *d_A, int64_t lda, const double *d_B, int64_t ldb,
                              double *d_C, int64_t ldc, void *d_ws, size_t ws_bytes, void *stream);
+/* bgpu_gemm_ozaki with `slices` = 4..8 slices per operand: the pairs p + q <= slices + 1 are kept,
+ * so the error is below about (slices + 3) 2^(-7 slices) K max_k |A(i, k)| max_k |B(j, k)|
+ * (slices 6: 2^-39 K, slices 5: 2^-32 K), for 21 (6) or 15 (5) int8 products instead of 36, on
+ * tiles of 80 (6) or 96 (5) columns instead of 64.  The workspace of bgpu_ozaki_ws_bytes serves
+ * every slice count.  The mixed path's late Schur complements, a preconditioner whose residuals
+ * are taken in FP64, need no more. */
+BGPU_API int bgpu_gemm_ozaki_slices(int slices, int M, int N, int K, const double *d_A, int64_t lda, const double *d_B,
+                                    int64_t ldb, double *d_C, int64_t ldc, void *d_ws, size_t ws_bytes, void *stream);
 
 /* The NT scaling of one SDP block (nt_scaling, solver.c:7898-7912; nt_prep/nt_eig/nt_post,
  * solver.c:7824-7896): from the Cholesky factors L_X, L_Z of X and Z (lower triangles, n x n

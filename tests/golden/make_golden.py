@@ -9,8 +9,10 @@ the iteration table of -v (pobj, dobj, pinf, dinf, gap, mu per iteration) and th
 Runs per instance: "init0" and "default" (HKM direction, SDPT3 and least-squares start), "nt"
 and "nt_init0" (NT direction, least-squares and SDPT3 start).
 
-usage: python tests/golden/make_golden.py [--big] [--runs r1,r2] [names]
-       (--big adds rand400 and mom700; --runs recomputes only those runs, keeping the others)
+usage: python tests/golden/make_golden.py [--big] [--huge] [--runs r1,r2] [names]
+       (--big adds rand400 and mom700; --huge adds rand1000, the n = 1000, m = 8000 instance, with
+       two runs only: "default" (-mixed 0, FP64) and "mixed" (the reference's own default, an FP32
+       Schur factor with PCG); --runs recomputes only those runs, keeping the others)
 """
 from __future__ import annotations
 
@@ -50,10 +52,13 @@ for _q in list(range(12)) + [3339]:
     INSTANCES[f"batch_q{_q}"] = (batch_instance, dict(q=_q))
 BIG = {"rand400": (random_sdp, dict(n=400, m=2000, density=0.01, seed=0)),
        "mom700": (moment_relaxation, dict(nvars=700, clique=4, seed=0))}
+# about 30 CPU-minutes per run on 8 host threads: the FP64 run and the reference's default mixed run
+HUGE = {"rand1000": (random_sdp, dict(n=1000, m=8000, density=0.005, seed=0))}
 
 HKM = ["-nohsd", "-dir", "hkm", "-mixed", "0", "-tol", "1e-7"] + AS_GIVEN
 NTD = ["-nohsd", "-dir", "nt", "-mixed", "0", "-tol", "1e-7"] + AS_GIVEN
 RUNS = {"init0": HKM + ["-init", "0"], "default": HKM, "nt": NTD, "nt_init0": NTD + ["-init", "0"]}
+HUGE_RUNS = {"default": HKM, "mixed": ["-nohsd", "-dir", "hkm", "-tol", "1e-7"] + AS_GIVEN}
 
 ROW = re.compile(r"^\s*(\d+)\s+([+-]\S+)\s+([+-]\S+)\s+(\S+)\s+(\S+)\s+(\S+)\s+(\S+)\s+(\S+)\s+(\S+)\s+(\S+)\s+(\S+)\s*$")
 
@@ -86,6 +91,8 @@ def main():
     inst = dict(INSTANCES)
     if "--big" in sys.argv:
         inst.update(BIG)
+    if "--huge" in sys.argv:
+        inst.update(HUGE)
     res = {}
     if os.path.exists(OUT):
         with open(OUT) as f:
@@ -106,7 +113,7 @@ def main():
             write_sdpa(d, path)
             old = res.get(name, {}).get("runs", {})
             entry = dict(generator=fn.__name__, kwargs=kw, m=d.m, n=int(d.bs[0]), nblk=d.nblk, runs=dict(old))
-            for rname, opts in RUNS.items():
+            for rname, opts in (HUGE_RUNS if name in HUGE else RUNS).items():
                 if rname in old and wanted and rname not in wanted:
                     continue
                 entry["runs"][rname] = run(path, opts)

@@ -5,6 +5,7 @@ import re
 
 import numpy as np
 import pytest
+from refdir import REF_DIR
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
@@ -83,13 +84,13 @@ def test_exports_what_the_reference_loader_binds(libpath):
     assert [s for s in REFERENCE_LOADER_SYMBOLS if not hasattr(L, s)] == []
 
 
-@pytest.mark.skipif(not os.path.isdir("/root/reference/python/brisk"), reason="reference tree absent")
+@pytest.mark.skipif(not os.path.isdir(os.path.join(REF_DIR, "python", "brisk")), reason="reference tree absent")
 def test_reference_python_package_loads_this_library(libpath, monkeypatch):
     """The reference's own binding loads libbrisk (B200 build) through BRISK_LIBRARY."""
     import importlib
     import sys
     monkeypatch.setenv("BRISK_LIBRARY", libpath)
-    monkeypatch.syspath_prepend("/root/reference/python")
+    monkeypatch.syspath_prepend(os.path.join(REF_DIR, "python"))
     sys.modules.pop("brisk", None)
     sys.modules.pop("brisk._core", None)
     brisk = importlib.import_module("brisk")
@@ -165,3 +166,28 @@ def test_other_reference_options_take_their_values(libpath):
     assert "option -nosuchflag is not used" in res.log
     assert "option 0 " not in res.log and "option yes" not in res.log
     assert "bad -tol" in res.log
+
+
+def test_options_that_change_the_method_are_noted(libpath):
+    """The reference's options that ask for another method or a presolve this build does not run
+    print a note naming what is not applied (-hsd is a flag, as in the reference: the option after
+    it is still read); the values that turn those presolves off are silent."""
+    from brisk_b200 import _core
+    res = _core.solve_sdpa([2], [1.0], [1], [1], [1], [1], [1.0],
+                           options=["-hsd", "-corr", "2", "-chordal", "1", "-sym", "auto", "-symalg", "-1",
+                                    "-deprows", "1", "-mixedfrac", "0.3", "-threads", "4", "-tol", "x"],
+                           verbose=False)
+    assert res.exit_code == 1 and "bad -tol" in res.log
+    assert "-hsd asks for the self-dual embedding" in res.log and "infeasible-start method runs" in res.log
+    for frag in ("option -corr 2: centrality correctors are not run",
+                 "option -chordal 1: no chordal decomposition",
+                 "option -sym auto: no symmetry reduction",
+                 "option -symalg -1: no block-algebra reduction",
+                 "option -deprows 1: dependent constraints are not removed",
+                 "option -mixedfrac 0.3"):
+        assert frag in res.log, frag
+    assert "-threads" not in res.log
+    quiet = _core.solve_sdpa([2], [1.0], [1], [1], [1], [1], [1.0],
+                             options=["-nohsd", "-sym", "none", "-symalg", "0", "-chordal", "0", "-deprows", "0",
+                                      "-corr", "0", "-nofr", "-tol", "x"], verbose=False)
+    assert quiet.exit_code == 1 and "note" not in quiet.log

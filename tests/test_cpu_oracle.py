@@ -7,6 +7,7 @@ import pytest
 
 from brisk_b200 import problems
 from oracle import restate
+from refdir import REF_DIR
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 SMALL = ["theta30", "rand30", "rand60"]
@@ -88,10 +89,10 @@ def test_oracle_nt_solve_matches_reference(golden, name):
         assert mine["dobj"] == pytest.approx(theirs["dobj"], rel=1e-6, abs=1e-8)
 
 
-@pytest.mark.skipif(not os.path.exists("/root/reference/examples/theta1.dat-s"), reason="reference tree absent")
+@pytest.mark.skipif(not os.path.exists(os.path.join(REF_DIR, "examples", "theta1.dat-s")), reason="reference tree absent")
 def test_oracle_theta1_published_value():
     """theta1 -> 2.2999999997e+01 (the reference's INSTALL.md:44-45)."""
-    d = problems.read_sdpa("/root/reference/examples/theta1.dat-s")
+    d = problems.read_sdpa(os.path.join(REF_DIR, "examples", "theta1.dat-s"))
     out = restate.solve(d, tol=1e-8)
     assert out["status_str"] == "OPTIMAL"
     assert -out["pobj"] == pytest.approx(23.0, rel=1e-7)

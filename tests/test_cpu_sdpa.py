@@ -12,6 +12,7 @@ import numpy as np
 import pytest
 
 import brisk_b200
+from refdir import REF_DIR
 
 GOLD = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "sdpa_reader.json")))
 # the messages of read_sdpa itself (others in the reference's output come from later stages)
@@ -141,7 +142,7 @@ def test_solve_file_reads_with_the_library_reader(tmp_path):
     assert "non-integer index in entry 2 1 2.5 3 1.5" in res.log
 
 
-REF_EXAMPLES = "/root/reference/examples"
+REF_EXAMPLES = os.path.join(REF_DIR, "examples")
 REF_BIN = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref", "brisk_ref")
 
 

@@ -11,17 +11,16 @@ pytestmark = pytest.mark.gpu
 
 import brisk_b200  # noqa: E402
 from brisk_b200 import problems  # noqa: E402
+from parity import objectives_close  # noqa: E402
 
 FP64 = ["-nohsd", "-dir", "hkm", "-mixed", "0", "-tol", "1e-7"]
 GOLDEN_Q = list(range(12)) + [3339]
 
 
 def check(res, ref):
-    """Same status; objectives within 1e-7 relative to 1 + |<C,X>| + |b'y|; DIMACS <= 1e-7."""
+    """Same status; objectives within 1e-7 relative (parity.objectives_close); DIMACS <= 1e-7."""
     assert res.status_str == ref["status"]
-    den = 1 + abs(ref["pobj"]) + abs(ref["dobj"])
-    assert abs(res.pobj - ref["pobj"]) <= 1e-7 * den, (res.pobj, ref["pobj"])
-    assert abs(res.dobj - ref["dobj"]) <= 1e-7 * den, (res.dobj, ref["dobj"])
+    objectives_close(res.pobj, res.dobj, ref["pobj"], ref["dobj"])
     assert np.max(np.abs(res.dimacs)) <= 1e-7, res.dimacs
 
 
@@ -44,8 +43,7 @@ def test_lockstep_batch_matches_standalone_solves():
     for d, res in zip(insts, out):
         ref = brisk_b200.solve_sdpa(*d.args(), options=FP64, verbose=False)
         assert res.status == ref.status and res.exit_code == 0
-        den = 1 + abs(ref.pobj) + abs(ref.dobj)
-        assert abs(res.pobj - ref.pobj) <= 1e-7 * den and abs(res.dobj - ref.dobj) <= 1e-7 * den
+        objectives_close(res.pobj, res.dobj, ref.pobj, ref.dobj)
         assert np.max(np.abs(res.dimacs)) <= 1e-7
         assert abs(res.iterations - ref.iterations) <= 2
 

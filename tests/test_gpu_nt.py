@@ -12,6 +12,7 @@ torch = pytest.importorskip("torch")
 import brisk_b200  # noqa: E402
 from brisk_b200 import problems, step  # noqa: E402
 from oracle import restate  # noqa: E402
+from parity import objectives_close  # noqa: E402
 
 NT = ["-nohsd", "-dir", "nt", "-mixed", "0", "-tol", "1e-7"]
 
@@ -104,11 +105,9 @@ def make(entry):
 
 
 def check(res, ref):
-    """Same status; objectives within 1e-7 of the DIMACS denominator; DIMACS <= 1e-7."""
+    """Same status; objectives within 1e-7 relative (parity.objectives_close); DIMACS <= 1e-7."""
     assert res.status_str == ref["status"], res.log
-    den = 1 + abs(ref["pobj"]) + abs(ref["dobj"])
-    assert abs(res.pobj - ref["pobj"]) <= 1e-7 * den, (res.pobj, ref["pobj"])
-    assert abs(res.dobj - ref["dobj"]) <= 1e-7 * den, (res.dobj, ref["dobj"])
+    objectives_close(res.pobj, res.dobj, ref["pobj"], ref["dobj"])
     assert np.max(np.abs(res.dimacs)) <= 1e-7, res.dimacs
 
 

@@ -52,7 +52,16 @@ def test_trsv_noalloc_matches_trsv_twice(n):
         np.testing.assert_allclose(got, np.linalg.solve(A, b), rtol=1e-8, atol=1e-10)
 
 
-def test_trsv_noalloc_rejects_sizes_above_its_maximum():
-    with pytest.raises(step.BgpuError) as e:
-        step.call("trsv_noalloc", 64 * 4096 + 1, 1, 64 * 4096 + 1, 1, 1, 0, None)
-    assert e.value.rc == -7
+def test_trsv_noalloc_rejects_sizes_above_its_maximum(capfd):
+    """The limit is the solve's own co-residency: one CTA of 256 threads (32 registers each) per
+    block row of 64, all resident at once, 8 per SM.  One block row more is refused with
+    BGPU_ERR_TOOBIG and a message that gives the limit, before anything is launched (the
+    pointers below are never read)."""
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    cap = sms * 8
+    for n in (64 * cap + 1, 64 * 4096 + 1):
+        with pytest.raises(step.BgpuError) as e:
+            step.call("trsv_noalloc", n, 1, n, 1, 1, 0, None)
+        assert e.value.rc == -7
+        err = capfd.readouterr().err
+        assert f"n <= {64 * cap}" in err, err
