@@ -112,12 +112,13 @@ int parse_options(int argc, const char *const *argv, Options &opt, std::string &
             const char *s = need("-1, 0 or 1");
             if (!s || !parse_int(s, opt.mixed)) { if (err.empty()) err = "bad -mixed"; return 1; }
         } else if (a == "-asmprec") {   // this build: the Schur assembly's precision
-            const char *s = need("fp64, tf32x3 or ozaki");
+            const char *s = need("fp64, tf32x3, ozaki or ozaki4..ozaki7");
             if (!s) return 1;
             if (!strcmp(s, "fp64")) opt.asm_prec = 0;
             else if (!strcmp(s, "tf32x3")) opt.asm_prec = 1;
-            else if (!strcmp(s, "ozaki")) opt.asm_prec = 2;
-            else { err = "bad -asmprec (fp64, tf32x3 or ozaki)"; return 1; }
+            else if (!strcmp(s, "ozaki") || !strcmp(s, "ozaki8")) opt.asm_prec = 2;
+            else if (!strncmp(s, "ozaki", 5) && s[5] >= '4' && s[5] <= '7' && s[6] == 0) opt.asm_prec = ((s[5] - '0') << 8) | 2;
+            else { err = "bad -asmprec (fp64, tf32x3, ozaki or ozaki4..ozaki7)"; return 1; }
         } else if (a == "-asmlate") {   // this build: the 3xTF32 path's late assembly
             const char *s = need("fp64, ozaki or ozaki4..ozaki7");
             if (!s) return 1;

@@ -34,6 +34,8 @@ struct OzakiOperand {
 };
 int ozaki_max_slices();   // 8: FP64-like products
 size_t ozaki_operand_bytes(long long rows, int K, int S);
+// the slice layout of a rows x K operand in buf (ozaki_operand_bytes)
+int ozaki_layout(long long rows, int K, void *buf, OzakiOperand *op, int S);
 // S (4..8) slices of the rows x K operand src (row r at src + r lds) into buf (ozaki_operand_bytes)
 int ozaki_slice(cudaStream_t st, long long rows, int K, const double *src, long long lds, void *buf, OzakiOperand *op,
                 int S);

@@ -258,9 +258,9 @@ size_t ozaki_operand_bytes(long long rows, int K, int S) {
     return (size_t)S * srows * ldk + sizeof(int) * srows + 1024;
 }
 
-// The operand's S slices into buf (ozaki_operand_bytes): returns the slice layout in *op.
-int ozaki_slice(cudaStream_t st, long long rows, int K, const double *src, long long lds, void *buf, OzakiOperand *op,
-                int S) {
+// The layout of a rows x K operand's S slices in buf (ozaki_operand_bytes): row stride ldk = K
+// rounded up to 64 bytes, srows = rows rounded up to 128, slice p at q + p srows ldk.
+int ozaki_layout(long long rows, int K, void *buf, OzakiOperand *op, int S) {
     if (S < 4 || S > OZ_SMAX) return BGPU_ERR_ARG;
     const long long ldk = round_up(K, 64), srows = round_up(rows, 128);
     op->rows = rows;
@@ -270,6 +270,14 @@ int ozaki_slice(cudaStream_t st, long long rows, int K, const double *src, long 
     op->slices = S;
     op->q = (int8_t *)(((uintptr_t)buf + 255) & ~(uintptr_t)255);
     op->e = (int *)(op->q + (size_t)S * srows * ldk);
+    return BGPU_OK;
+}
+
+// The operand's S slices into buf (ozaki_operand_bytes): returns the slice layout in *op.
+int ozaki_slice(cudaStream_t st, long long rows, int K, const double *src, long long lds, void *buf, OzakiOperand *op,
+                int S) {
+    if (int rc = ozaki_layout(rows, K, buf, op, S)) return rc;
+    const long long ldk = op->ldk, srows = op->srows;
     if (rows <= 0) return BGPU_OK;
     if ((rows + 7) / 8 > (1LL << 31) - 1) return BGPU_ERR_TOOBIG;
     slice_kernel<<<ceil_div(rows * 32, 256), 256, 0, st>>>((int)rows, K, S, src, lds, op->q, ldk, srows * ldk, op->e);

@@ -79,7 +79,7 @@ struct Options {
     int mixed = -1;             // FP32 Schur factor: -1 auto (m >= 1000), 0 never, 1 always
     int asm_prec = -1;          // Schur assembly: -1 auto (FP64), 0 FP64, 1 3xTF32, 2 FP64-accurate on the
                                 // INT8 tensor cores (Ozaki slices)
-    int late_prec = 2;          // 3xTF32 path: the assembly once the FP32-accurate M no longer serves (0 FP64,
+    int late_prec = (5 << 8) | 2;   // 3xTF32 path: the assembly once the FP32-accurate M no longer serves (0 FP64,
                                 // 2 Ozaki with 8 slices, FP64-accurate; (S << 8) | 2 with S = 4..7 slices, a
                                 // preconditioner-grade M whose PCG residuals are taken with the FP64 operator,
                                 // turned to 8 slices if its factor needs a shift or PCG misses)

@@ -146,7 +146,7 @@ def test_schur_ozaki_fewer_slices(cuda, S, tol):
 
 def check(res, ref):
     assert res.status_str == ref["status"], res.log
-    objectives_close(res.pobj, res.dobj, ref["pobj"], ref["dobj"])
+    objectives_close(res.pobj, res.dobj, ref["pobj"], ref["dobj"], each=res.iterations == ref["iterations"])
     assert np.max(np.abs(res.dimacs)) <= 1e-7, res.dimacs
 
 

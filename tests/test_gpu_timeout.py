@@ -85,14 +85,14 @@ def test_trsv_wait_runs_out_and_the_context_stays_usable(held_row, trans):
 
 def test_solve_reports_the_timeout_and_the_next_solve_succeeds(held_row):
     """Inside a whole solve (the PCG preconditioner's triangular solves of the dense factor of
-    M, m = 200: 4 block rows): the solve ends with the abort exit code and a GPU-failure message
-    naming the timeout code, and the next solve on the same context is OPTIMAL."""
+    M, m = 200: 4 block rows): brisk_solve_data returns the abort exit code -3 with a GPU-failure
+    message naming the timeout code (-4), and the next solve on the same context is OPTIMAL."""
     d = problems.random_sdp(n=30, m=200, density=0.1, seed=1)
     opts = ["-nohsd", "-dir", "hkm", "-tol", "1e-7", "-mixed", "0", "-init", "0"]
     held_row(1)
-    r = _core.solve_sdpa(*d.args(), options=opts, verbose=False)
-    assert r.exit_code < 0, r.log
-    assert "GPU failure (code -4" in r.log, r.log
+    with pytest.raises(RuntimeError) as e:   # the binding raises on an aborted solve (exit code < 0)
+        _core.solve_sdpa(*d.args(), options=opts, verbose=False)
+    assert "aborted (code -3)" in str(e.value) and "GPU failure (code -4" in str(e.value), str(e.value)
     held_row(-1, 0)
     r = _core.solve_sdpa(*d.args(), options=opts, verbose=False)
     assert r.status_str == "OPTIMAL", r.log
