@@ -16,92 +16,166 @@
 #include "common.cuh"
 #include "kernels.h"
 #include <cooperative_groups.h>
+#include <algorithm>
 
 namespace {
 constexpr int NB = TRI_NB;      // 64
 constexpr int LDS = NB + 1;     // padded smem stride
 
 // ---- diagonal-block factor + inverse ----------------------------------------------------
-// One CTA of 256 threads (a 16 x 16 grid tx, ty) on the 64 x 64 block in shared memory.  Column
-// c: every thread reads the pivot (a broadcast), the column below is scaled, then the trailing
-// lower triangle is updated with the 2-D thread grid (two barriers a column, no integer
-// division in the loops).  The inverse of the factor follows the same pattern: row k of X is
-// final once divided by L(k,k); the rows below subtract L(r,k) X(k,:).
+// One CTA of 256 threads on the 64 x 64 diagonal block in shared memory, in four steps of 16
+// columns.  Step k: one warp factors the 16 x 16 diagonal sub-block L_kk and inverts it in its
+// registers (lane r holds row r; the pivots and rows travel by shuffles, no barrier), the rows
+// below are solved against it (L_ik = A_ik L_kk^-T: one thread a row), and the trailing lower
+// triangle takes the rank-16 update.  The inverse X = L^-1 of the whole block then follows by
+// its block diagonals: X_kk from the steps, X_ij = -X_ii sum_{k=j}^{i-1} L_ik X_kj for i - j =
+// 1, 2, 3.  About twenty barriers instead of two a column.  Rows and columns past the block's
+// order are the identity, so a partial last block factors and inverts as a whole one.
+constexpr int DB = 16;   // sub-block order (16 lanes of a warp)
+
+// Cholesky of the 16 x 16 block held by lanes 0-15 (a[j], j <= lane; lanes 16-31 hold zeros)
+// and its inverse (x[j], j <= lane).  `real` columns count for the smallest pivot; returns the
+// first failing column (0-based) or -1.
+template <typename T>
+__device__ __forceinline__ int chol_inv16(T (&a)[DB], T (&x)[DB], int lane, int real, double &pm) {
+    int fail = -1;   // (the loops run on past a failure, on values the caller then discards: no early
+                     // exit, so they unroll whole and the rows stay in registers)
+#pragma unroll
+    for (int c = 0; c < DB; c++) {
+        const T d = __shfl_sync(0xffffffffu, a[c], c);
+        if (fail < 0 && (!(d > (T)0) || !isfinite((double)d))) fail = c;   // uniform over the warp
+        if (c < real && (double)d < pm) pm = (double)d;
+        const T sd = sqrt(d), isd = (T)1 / sd;
+        if (lane == c) a[c] = sd;
+        else if (lane > c) a[c] *= isd;
+#pragma unroll
+        for (int j = 0; j < DB; j++) {   // (fixed bounds: both loops unroll and a[] stays in registers)
+            const T ljc = __shfl_sync(0xffffffffu, a[c], j);
+            if (j > c && lane >= j) a[j] -= a[c] * ljc;
+        }
+    }
+    T diag = (T)1;
+#pragma unroll
+    for (int j = 0; j < DB; j++)
+        if (lane == j) diag = a[j];
+    const T rd = (T)1 / diag;
+#pragma unroll
+    for (int j = 0; j < DB; j++) x[j] = (T)0;
+#pragma unroll
+    for (int j = 0; j < DB; j++) {   // column j of X: X[k][j] = -(sum_{i=j}^{k-1} L[k][i] X[i][j]) / L[k][k]
+        T acc = (T)0;
+#pragma unroll
+        for (int k = 0; k < DB; k++) {
+            if (k < j) continue;
+            if (lane == k) x[j] = (k == j) ? rd : -acc * rd;
+            const T xk = __shfl_sync(0xffffffffu, x[j], k);
+            if (lane > k) acc += a[k] * xk;
+        }
+    }
+    return fail;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256) potrf_diag_kernel(int n, T *A, long long lda, int j0, T *dinv, int *info,
                                                          double *pmin) {
     extern __shared__ __align__(16) unsigned char dsm_raw[];
-    T *S = reinterpret_cast<T *>(dsm_raw);   // S[r + c*LDS]: factor, then L
-    T *X = S + NB * LDS;                      // inverse of L
-    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    T *S = reinterpret_cast<T *>(dsm_raw);   // S[r + c*LDS]: the block, then L
+    T *X = S + NB * LDS;                      // the inverse of L
+    __shared__ T P[3][DB][DB + 1];            // the sums of the off-diagonal inverse blocks
+    __shared__ int s_fail;
+    __shared__ double s_pm;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nb = min(NB, n - j0);
     if (*(volatile int *)info != 0) return;   // an earlier panel failed: nothing to do
     T *Ad = A + (long long)j0 + (long long)j0 * lda;
-    for (int c = ty; c < NB; c += 16)
-        for (int r = tx; r < NB; r += 16) {   // column c: rows r coalesced over tx
-            T v = (T)0;
-            if (r < nb && c < nb && r >= c) v = Ad[r + (long long)c * lda];
-            S[r + c * LDS] = v;
-            X[r + c * LDS] = (r == c) ? (T)1 : (T)0;
-        }
+    for (int idx = tid; idx < NB * NB; idx += 256) {
+        const int r = idx & (NB - 1), c = idx >> 6;   // column c: rows coalesced
+        T v = (r == c) ? (T)1 : (T)0;                 // the identity past the block's order
+        if (r < nb && c < nb && r >= c) v = Ad[r + (long long)c * lda];
+        S[r + c * LDS] = v;
+        X[r + c * LDS] = (T)0;
+    }
+    if (tid == 0) { s_fail = -1; s_pm = 1e300; }
     __syncthreads();
-    // Column c (one barrier a column): every thread reads d = S(c,c); the trailing update uses the
-    // unscaled column, S(r,q) -= S(r,c) S(q,c) / d, and column c is scaled by 1/sqrt(d) one phase
-    // later, when nothing reads it any more.
-    double pm = 1e300;
-    int fail = 0;
-    T prev_inv = (T)0, prev_piv = (T)0;
-    for (int c = 0; c < nb; c++) {
-        const T d = S[c + c * LDS];
-        if (!(d > (T)0) || !isfinite((double)d)) { fail = j0 + c + 1; break; }
-        if ((double)d < pm) pm = (double)d;
-        const T inv_d = (T)1 / d;
-        if (c > 0) {   // scale column c-1 (its pivot was d_{c-1})
-            for (int r = c - 1 + tid; r < nb; r += 256)
-                S[r + (c - 1) * LDS] = (r == c - 1) ? prev_piv : S[r + (c - 1) * LDS] * prev_inv;
+    for (int kb = 0; kb < NB / DB; kb++) {
+        const int k0 = kb * DB;
+        if (warp == 0) {
+            T a[DB], x[DB];
+#pragma unroll
+            for (int j = 0; j < DB; j++) a[j] = (lane < DB && j <= lane) ? S[(k0 + lane) + (k0 + j) * LDS] : (T)0;
+            double pm = 1e300;
+            const int f = chol_inv16<T>(a, x, lane, nb - k0, pm);
+            if (f >= 0) {
+                if (lane == 0) s_fail = k0 + f;
+            } else if (lane < DB) {
+#pragma unroll
+                for (int j = 0; j < DB; j++)
+                    if (j <= lane) {
+                        S[(k0 + lane) + (k0 + j) * LDS] = a[j];
+                        X[(k0 + lane) + (k0 + j) * LDS] = x[j];
+                    }
+            }
+            if (lane == 0 && pm < s_pm) s_pm = pm;
         }
-        for (int q = c + 1 + tx; q < nb; q += 16) {
-            const T sqc = S[q + c * LDS] * inv_d;
-            for (int r = q + ty; r < nb; r += 16) S[r + q * LDS] -= S[r + c * LDS] * sqc;
+        __syncthreads();
+        if (s_fail >= 0) break;
+        // rows below: L_ik = A_ik L_kk^-T, one thread a row (its 16 values first, then written)
+        const int rows = NB - k0 - DB;
+        if (tid < rows) {
+            const int r = k0 + DB + tid;
+            T v[DB];
+#pragma unroll
+            for (int k = 0; k < DB; k++) v[k] = S[r + (k0 + k) * LDS];
+#pragma unroll
+            for (int j = 0; j < DB; j++) {   // L_rj = sum_{k <= j} v_k X_kk[j][k] (v read whole first)
+                T s = (T)0;
+#pragma unroll
+                for (int k = 0; k <= j; k++) s += v[k] * X[(k0 + j) + (k0 + k) * LDS];
+                S[r + (k0 + j) * LDS] = s;
+            }
         }
-        prev_piv = sqrt(d);
-        prev_inv = (T)1 / prev_piv;
+        __syncthreads();
+        // the trailing lower triangle: S[i][j] -= sum_k L[i][k] L[j][k], i >= j > k0 + 15
+        const int t0 = k0 + DB, tn = NB - t0;
+        for (int idx = tid; idx < tn * tn; idx += 256) {
+            const int i = t0 + idx % tn, jj = t0 + idx / tn;
+            if (i < jj) continue;
+            T s = (T)0;
+#pragma unroll
+            for (int k = 0; k < DB; k++) s += S[i + (k0 + k) * LDS] * S[jj + (k0 + k) * LDS];
+            S[i + jj * LDS] -= s;
+        }
         __syncthreads();
     }
-    if (!fail && nb > 0) {   // scale the last column
-        for (int r = nb - 1 + tid; r < nb; r += 256)
-            S[r + (nb - 1) * LDS] = (r == nb - 1) ? prev_piv : S[r + (nb - 1) * LDS] * prev_inv;
-        __syncthreads();
-    }
-    if (fail) {
-        if (tid == 0) atomicCAS(info, 0, fail);
+    if (s_fail >= 0) {
+        if (tid == 0 && s_fail < nb) atomicCAS(info, 0, j0 + s_fail + 1);
         return;
     }
-    if (tid == 0) atomicMin((unsigned long long *)pmin, (unsigned long long)__double_as_longlong(pm));
-    // X = L^-1, one barrier a row: row k of X is final after its division by L(k,k); the rows below
-    // subtract L(r,k)/L(k,k) times the undivided row k, and row k is divided one phase later.
-    T prev_dinv = (T)0;
-    for (int k = 0; k < nb; k++) {
-        const T rk = (T)1 / S[k + k * LDS];
-        if (k > 0)
-            for (int j = tid; j <= k - 1; j += 256) X[(k - 1) + j * LDS] *= prev_dinv;
-        for (int j = tx; j <= k; j += 16) {
-            const T xkj = X[k + j * LDS] * rk;
-            for (int r = k + 1 + ty; r < nb; r += 16) X[r + j * LDS] -= S[r + k * LDS] * xkj;
+    if (tid == 0) atomicMin((unsigned long long *)pmin, (unsigned long long)__double_as_longlong(s_pm));
+    // the off-diagonal blocks of X, one block diagonal at a time
+    for (int d = 1; d < NB / DB; d++) {
+        const int nblk = NB / DB - d;
+        for (int idx = tid; idx < nblk * DB * DB; idx += 256) {   // P = sum_{k=j}^{i-1} L_ik X_kj
+            const int bj = idx / (DB * DB), e = idx % (DB * DB), r = e % DB, c = e / DB, bi = bj + d;
+            T s = (T)0;
+            for (int k = bj * DB; k < bi * DB; k++) s += S[(bi * DB + r) + k * LDS] * X[k + (bj * DB + c) * LDS];
+            P[bj][r][c] = s;
         }
-        prev_dinv = rk;
+        __syncthreads();
+        for (int idx = tid; idx < nblk * DB * DB; idx += 256) {   // X_ij = -X_ii P
+            const int bj = idx / (DB * DB), e = idx % (DB * DB), r = e % DB, c = e / DB, bi = bj + d;
+            T s = (T)0;
+#pragma unroll
+            for (int k = 0; k < DB; k++) s += X[(bi * DB + r) + (bi * DB + k) * LDS] * P[bj][k][c];
+            X[(bi * DB + r) + (bj * DB + c) * LDS] = -s;
+        }
         __syncthreads();
     }
-    if (nb > 0) {
-        for (int j = tid; j <= nb - 1; j += 256) X[(nb - 1) + j * LDS] *= prev_dinv;
-        __syncthreads();
+    for (int idx = tid; idx < NB * NB; idx += 256) {
+        const int r = idx & (NB - 1), c = idx >> 6;
+        if (r < nb && c < nb && r >= c) Ad[r + (long long)c * lda] = S[r + c * LDS];
+        dinv[r + c * NB] = (r >= c) ? X[r + c * LDS] : (T)0;   // identity past the block's order
     }
-    for (int c = ty; c < NB; c += 16)
-        for (int r = tx; r < NB; r += 16) {
-            if (r < nb && c < nb && r >= c) Ad[r + (long long)c * lda] = S[r + c * LDS];
-            // identity beyond nb so a partial last block acts as a full one in the solves
-            dinv[r + c * NB] = (r < nb && c < nb) ? ((r >= c) ? X[r + c * LDS] : (T)0) : (T)(r == c ? 1 : 0);
-        }
 }
 
 __global__ void init_info_kernel(int *info, double *pmin) {
@@ -131,99 +205,134 @@ __global__ void __launch_bounds__(256) trsm_panel_f32(int rows, int nb, float *A
     }
 }
 
-// C(i, j) -= sum_k A(i, k) A(j, k), lower triangle, K <= 64: 64 x 64 output tiles.
-__global__ void __launch_bounds__(256) syrk_f32(int n2, int K, const float *A, long long lda, float *C, long long ldc) {
+// C(i, j) -= sum_k A(i, k) A(j, k) for i >= j, i < M, j < N (the lower part of an M x N block whose
+// diagonal starts at its top left, N <= M): 64 x 64 output tiles, K in steps of 64.
+__global__ void __launch_bounds__(256) syrk_f32(int M, int N, int K, const float *A, long long lda, float *C,
+                                                long long ldc) {
     const int bi = blockIdx.x, bj = blockIdx.y;
     if (bi < bj) return;
     __shared__ float As[64 * LDS], Bs[64 * LDS];
     const int tid = threadIdx.x;
-    for (int idx = tid; idx < 64 * 64; idx += 256) {
-        const int r = idx % 64, k = idx / 64;
-        As[r + k * LDS] = (bi * 64 + r < n2 && k < K) ? A[(bi * 64 + r) + (long long)k * lda] : 0.f;
-        Bs[r + k * LDS] = (bj * 64 + r < n2 && k < K) ? A[(bj * 64 + r) + (long long)k * lda] : 0.f;
-    }
-    __syncthreads();
     const int tr = tid % 16, tc = tid / 16;   // 4 x 4 outputs per thread
     float acc[4][4] = {};
-    for (int k = 0; k < K; k++) {
-        float a[4], b[4];
+    for (int k0 = 0; k0 < K; k0 += 64) {
+        __syncthreads();   // the previous step's tiles are consumed
+        for (int idx = tid; idx < 64 * 64; idx += 256) {
+            const int r = idx % 64, k = idx / 64;
+            As[r + k * LDS] = (bi * 64 + r < M && k0 + k < K) ? A[(bi * 64 + r) + (long long)(k0 + k) * lda] : 0.f;
+            Bs[r + k * LDS] = (bj * 64 + r < N && k0 + k < K) ? A[(bj * 64 + r) + (long long)(k0 + k) * lda] : 0.f;
+        }
+        __syncthreads();
+        for (int k = 0; k < 64; k++) {
+            float a[4], b[4];
 #pragma unroll
-        for (int u = 0; u < 4; u++) { a[u] = As[tr + 16 * u + k * LDS]; b[u] = Bs[tc + 16 * u + k * LDS]; }
+            for (int u = 0; u < 4; u++) { a[u] = As[tr + 16 * u + k * LDS]; b[u] = Bs[tc + 16 * u + k * LDS]; }
 #pragma unroll
-        for (int u = 0; u < 4; u++)
+            for (int u = 0; u < 4; u++)
 #pragma unroll
-            for (int v = 0; v < 4; v++) acc[u][v] += a[u] * b[v];
+                for (int v = 0; v < 4; v++) acc[u][v] += a[u] * b[v];
+        }
     }
 #pragma unroll
     for (int u = 0; u < 4; u++)
 #pragma unroll
         for (int v = 0; v < 4; v++) {
             const int i = bi * 64 + tr + 16 * u, j = bj * 64 + tc + 16 * v;
-            if (i < n2 && j < n2 && i >= j) C[i + (long long)j * ldc] -= acc[u][v];
+            if (i < M && j < N && i >= j) C[i + (long long)j * ldc] -= acc[u][v];
         }
 }
 
 // ---- persistent triangular solve -----------------------------------------------------------
 // trans = 0: solve L x = b (block rows top-down); trans = 1: solve L' x = b (bottom-up).
-// One CTA per block row (all co-resident: a cooperative launch); the CTA of block row r waits
-// for the flags of the rows it depends on, at most `limit` polls each, then publishes its own.
+// One CTA per block row (all co-resident: a cooperative launch).  Thread (row, q) of the CTA of
+// block row r keeps, in a register, the sum over the blocks c that row r depends on of
+// L(r, c)[row, 16 q .. 16 q + 15] x_c; each warp waits by itself (its lane 0, at most `limit`
+// polls) for block c's flag before it reads x_c, so the waits cost no CTA barrier.  Once every
+// dependency is in, x_r = Dinv_r (b_r - sum) and the flag of r is published.  The critical path
+// is the chain of these last steps: with PRE, the block of the last dependency (c = r - 1, or
+// r + 1 for trans = 1) and Dinv_r are loaded into shared memory while the earlier rows solve, so
+// that step reads nothing but x_c from global memory.
 // hold >= 0 (failure-path tests only): the CTA of that block row computes its rows but does
 // not publish its flag, so the rows after it give up waiting and report through *err.
-template <typename T>
-__global__ void __launch_bounds__(256) trsv_kernel(int n, const T *L, long long lda, const T *dinv, T *x, int trans,
-                                                   int *flags, int epoch, int *err, unsigned limit, int hold) {
-    __shared__ T acc[NB];
+template <typename T, bool PRE>
+__global__ void __launch_bounds__(256, PRE ? 1 : 8) trsv_kernel(int n, const T *L, long long lda, const T *dinv, T *x,
+                                                                int trans, int *flags, int epoch, int *err,
+                                                                unsigned limit, int hold) {
+    extern __shared__ __align__(16) unsigned char tsm_raw[];   // PRE: Bs[NB * NB], Ds[NB * NB]
     __shared__ T part[4][NB];
-    __shared__ T xc[NB];
+    __shared__ T acc[NB];
     __shared__ int bad;
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31;
     const int nblk = (n + NB - 1) / NB;
     const int r = trans ? (nblk - 1 - blockIdx.x) : blockIdx.x;   // the block row this CTA owns
     const int r0 = r * NB, nr = min(NB, n - r0);
-    if (tid < NB) acc[tid] = (tid < nr) ? x[r0 + tid] : (T)0;
-    if (tid == 0) bad = 0;
-    __syncthreads();
     const int row = tid & 63, q = tid >> 6;   // 4 threads per row, 16 columns each
     const int ndep = trans ? (nblk - 1 - r) : r;
+    const T *D = dinv + (size_t)r * NB * NB;
+    T *Bs = reinterpret_cast<T *>(tsm_raw), *Ds = Bs + NB * NB;
+    if (tid < NB) acc[tid] = (tid < nr) ? x[r0 + tid] : (T)0;
+    if (tid == 0) bad = 0;
+    if (PRE) {
+        // Ds[i + k NB] = the (i, k) coefficient of x_r = Ds acc; Bs[i + k NB] the one of the last
+        // dependency's block (0 past the order)
+        for (int idx = tid; idx < NB * NB; idx += 256) {
+            const int a = idx & 63, b = idx >> 6;   // a: the index that is contiguous in memory
+            if (!trans) Ds[a + b * NB] = D[a + b * NB];
+            else Ds[b + a * NB] = D[a + b * NB];
+        }
+        if (ndep > 0) {
+            const int c = trans ? r + 1 : r - 1, c0 = c * NB, nc = min(NB, n - c0);
+            for (int idx = tid; idx < NB * NB; idx += 256) {
+                const int a = idx & 63, b = idx >> 6;
+                if (!trans)   // L(r0 + a, c0 + b): rows a contiguous
+                    Bs[a + b * NB] = (a < nr && b < nc) ? L[(r0 + a) + (long long)(c0 + b) * lda] : (T)0;
+                else          // L(c0 + a, r0 + b), the coefficient of row b, column a
+                    Bs[b + a * NB] = (b < nr && a < nc) ? L[(c0 + a) + (long long)(r0 + b) * lda] : (T)0;
+            }
+        }
+    }
+    __syncthreads();
+    T s = (T)0;
+    bool ok = true;
     for (int d = 0; d < ndep; d++) {
         const int c = trans ? (nblk - 1 - d) : d;   // dependencies in the order they finish
-        if (tid == 0) {
+        if (lane == 0) {
             unsigned spins = 0;
             while (ld_acquire(&flags[c]) != epoch) {
-                if (++spins > limit) { bad = 1; break; }
+                if (++spins > limit) { ok = false; break; }
                 __nanosleep(64);
             }
         }
-        __syncthreads();
-        if (bad) break;
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        if (!ok) break;
         const int c0 = c * NB, nc = min(NB, n - c0);
-        if (tid < NB) xc[tid] = (tid < nc) ? ((volatile T *)x)[c0 + tid] : (T)0;
-        __syncthreads();
-        T s = (T)0;
-        if (!trans) {   // acc(row) -= sum_col L(r0+row, c0+col) xc(col)
-            if (row < nr)
-                for (int k = q * 16; k < q * 16 + 16 && k < nc; k++) s += L[(r0 + row) + (long long)(c0 + k) * lda] * xc[k];
-        } else {        // acc(row) -= sum_col L(c0+col, r0+row) xc(col)
-            if (row < nr) {
-                const T *col = L + (long long)(r0 + row) * lda + c0;
-                for (int k = q * 16; k < q * 16 + 16 && k < nc; k++) s += col[k] * xc[k];
+        const bool last = PRE && d == ndep - 1;
+        if (row < nr) {
+#pragma unroll 4
+            for (int k = q * 16; k < q * 16 + 16; k++) {
+                if (k >= nc) break;
+                const T xv = ((volatile T *)x)[c0 + k];
+                const T lv = last ? Bs[row + k * NB]
+                                  : (trans ? L[(c0 + k) + (long long)(r0 + row) * lda] : L[(r0 + row) + (long long)(c0 + k) * lda]);
+                s += lv * xv;
             }
         }
-        part[q][row] = s;
-        __syncthreads();
-        if (tid < NB) acc[tid] -= (part[0][tid] + part[1][tid]) + (part[2][tid] + part[3][tid]);
-        __syncthreads();
     }
+    if (!ok) bad = 1;
+    part[q][row] = s;
+    __syncthreads();
     if (bad) {
         if (tid == 0) atomicExch(err, 1);
         return;
     }
+    if (tid < NB) acc[tid] -= (part[0][tid] + part[1][tid]) + (part[2][tid] + part[3][tid]);
+    __syncthreads();
     // x_r = Dinv_r acc (trans = 0) or Dinv_r' acc (trans = 1)
-    const T *D = dinv + (size_t)r * NB * NB;
-    T s = (T)0;
-    if (!trans) { for (int k = q * 16; k < q * 16 + 16; k++) s += D[row + k * NB] * acc[k]; }
-    else        { for (int k = q * 16; k < q * 16 + 16; k++) s += D[k + row * NB] * acc[k]; }
-    part[q][row] = s;
+    T t = (T)0;
+    if (PRE) { for (int k = q * 16; k < q * 16 + 16; k++) t += Ds[row + k * NB] * acc[k]; }
+    else if (!trans) { for (int k = q * 16; k < q * 16 + 16; k++) t += D[row + k * NB] * acc[k]; }
+    else             { for (int k = q * 16; k < q * 16 + 16; k++) t += D[k + row * NB] * acc[k]; }
+    part[q][row] = t;
     __syncthreads();
     if (tid < nr) x[r0 + tid] = (part[0][tid] + part[1][tid]) + (part[2][tid] + part[3][tid]);
     __threadfence();
@@ -231,21 +340,28 @@ __global__ void __launch_bounds__(256) trsv_kernel(int n, const T *L, long long 
     if (tid == 0 && r != hold) st_release(&flags[r], epoch);
 }
 
+template <typename T> constexpr size_t trsv_pre_smem() { return 2 * (size_t)NB * NB * sizeof(T); }
+
 // The largest number of block rows one solve can take on the current device: every CTA of the
-// cooperative launch must be resident at once (SMs x resident CTAs per SM).
-std::atomic<int> g_trsv_cap[2][64];
-template <typename T>
+// cooperative launch must be resident at once (SMs x resident CTAs per SM), for the kernel
+// without (PRE = false) or with the shared-memory preload.
+std::atomic<int> g_trsv_cap[2][2][64];
+template <typename T, bool PRE = false>
 int trsv_max_blocks(int *cap) {
     int dev = 0;
     BGPU_CHECK(cudaGetDevice(&dev));
-    std::atomic<int> *slot = (dev >= 0 && dev < 64) ? &g_trsv_cap[sizeof(T) == 8][dev] : nullptr;
+    std::atomic<int> *slot = (dev >= 0 && dev < 64) ? &g_trsv_cap[sizeof(T) == 8][PRE][dev] : nullptr;
     if (slot && slot->load(std::memory_order_relaxed) > 0) {
         *cap = slot->load(std::memory_order_relaxed);
         return BGPU_OK;
     }
     int nsm = 0, per = 0;
     BGPU_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    BGPU_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, trsv_kernel<T>, 256, 0));
+    if (PRE)
+        BGPU_CHECK(cudaFuncSetAttribute(trsv_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)trsv_pre_smem<T>()));
+    BGPU_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, trsv_kernel<T, PRE>, 256,
+                                                             PRE ? trsv_pre_smem<T>() : 0));
     *cap = nsm * per;
     if (slot) slot->store(*cap, std::memory_order_relaxed);
     return BGPU_OK;
@@ -256,14 +372,19 @@ int trsv_launch(cudaStream_t st, int n, const T *L, long long lda, const T *dinv
                 int epoch, int *d_err) {
     if (n <= 0) return BGPU_OK;
     const int nblk = (n + NB - 1) / NB;
-    int cap = 0;
+    int cap = 0, cap_pre = 0;
     if (int rc = trsv_max_blocks<T>(&cap)) return rc;
     if (nblk > cap) return BGPU_ERR_TOOBIG;
+    if (int rc = trsv_max_blocks<T, true>(&cap_pre)) return rc;
     unsigned limit = wait_limit();
     int hold = trsv_hold_row();
     void *args[] = {(void *)&n, (void *)&L, (void *)&lda, (void *)&dinv, (void *)&x, (void *)&trans,
                     (void *)&flags, (void *)&epoch, (void *)&d_err, (void *)&limit, (void *)&hold};
-    BGPU_CHECK(cudaLaunchCooperativeKernel((void *)trsv_kernel<T>, dim3(nblk), dim3(256), args, 0, st));
+    if (nblk <= cap_pre)
+        BGPU_CHECK(cudaLaunchCooperativeKernel((void *)trsv_kernel<T, true>, dim3(nblk), dim3(256), args,
+                                               trsv_pre_smem<T>(), st));
+    else
+        BGPU_CHECK(cudaLaunchCooperativeKernel((void *)trsv_kernel<T, false>, dim3(nblk), dim3(256), args, 0, st));
     BGPU_LAUNCH_CHECK();
     return BGPU_OK;
 }
@@ -364,24 +485,44 @@ int diag_smem_attr() {
     return BGPU_OK;
 }
 
+// The blocked factor in outer panels of PANEL columns: within a panel, each 64-column block is
+// factored (potrf_diag_kernel), the whole column below it solved against its inverse, and the
+// panel's later columns updated (rank 64); the columns right of the panel then take one rank-PANEL
+// update, which reads and writes the trailing triangle once per panel (not once per 64 columns)
+// and gives the tensor-core GEMM a depth of PANEL.
+constexpr int PANEL = 256;
+
 int potrf_f64(cudaStream_t st, int n, double *A, long long lda, double *dinv, int *d_info, double *d_pmin) {
     if (int rc = diag_smem_attr<double>()) return rc;
     init_info_kernel<<<1, 1, 0, st>>>(d_info, d_pmin);
     BGPU_LAUNCH_CHECK();
-    for (int j0 = 0; j0 < n; j0 += NB) {
-        const int nb = (n - j0 < NB) ? n - j0 : NB;
-        potrf_diag_kernel<double><<<1, 256, 2 * NB * LDS * sizeof(double), st>>>(n, A, lda, j0, dinv + (size_t)(j0 / NB) * NB * NB, d_info, d_pmin);
-        BGPU_LAUNCH_CHECK();
-        const int rest = n - j0 - nb;
+    for (int J0 = 0; J0 < n; J0 += PANEL) {
+        const int JB = std::min(PANEL, n - J0);
+        for (int j0 = J0; j0 < J0 + JB; j0 += NB) {
+            const int nb = std::min(NB, n - j0);
+            const double *Di = dinv + (size_t)(j0 / NB) * NB * NB;
+            potrf_diag_kernel<double><<<1, 256, 2 * NB * LDS * sizeof(double), st>>>(n, A, lda, j0, (double *)Di, d_info, d_pmin);
+            BGPU_LAUNCH_CHECK();
+            const int rest = n - j0 - nb;
+            if (rest <= 0) break;
+            double *A21 = A + (j0 + nb) + (long long)j0 * lda;
+            // A21 <- A21 Di'  (B(k, j) = Di(j, k) = Di[j + k*NB]: N-major); in place, N = nb <= 64
+            int rc = gemm_f64(st, 0, 0, rest, nb, nb, 1.0, A21, lda, 0, Di, NB, 0, 0.0, A21, lda, 0, 1, 0);
+            if (rc) return rc;
+            // the panel's later columns: A[j0+nb.., j0+nb .. J0+JB) -= A21 A21(top pc rows)', lower
+            const int pc = J0 + JB - (j0 + nb);
+            if (pc > 0) {
+                rc = gemm_f64(st, 0, 0, rest, pc, nb, -1.0, A21, lda, 0, A21, lda, 0, 1.0,
+                              A + (j0 + nb) + (long long)(j0 + nb) * lda, lda, 0, 1, 1);
+                if (rc) return rc;
+            }
+        }
+        const int rest = n - J0 - JB;
         if (rest <= 0) break;
-        double *A21 = A + (j0 + nb) + (long long)j0 * lda;
-        double *A22 = A + (j0 + nb) + (long long)(j0 + nb) * lda;
-        const double *Di = dinv + (size_t)(j0 / NB) * NB * NB;
-        // A21 <- A21 Di'  (B(k, j) = Di(j, k) = Di[j + k*NB]: N-major); in place, N = nb <= 64
-        int rc = gemm_f64(st, 0, 0, rest, nb, nb, 1.0, A21, lda, 0, Di, NB, 0, 0.0, A21, lda, 0, 1, 0);
-        if (rc) return rc;
-        // A22 <- A22 - A21 A21'  (lower)
-        rc = gemm_f64(st, 0, 0, rest, rest, nb, -1.0, A21, lda, 0, A21, lda, 0, 1.0, A22, lda, 0, 1, 1);
+        // A22 <- A22 - P P' (lower), P the rows below the panel (rest x JB)
+        const double *P = A + (J0 + JB) + (long long)J0 * lda;
+        double *A22 = A + (J0 + JB) + (long long)(J0 + JB) * lda;
+        int rc = gemm_f64(st, 0, 0, rest, rest, JB, -1.0, P, lda, 0, P, lda, 0, 1.0, A22, lda, 0, 1, 1);
         if (rc) return rc;
     }
     return BGPU_OK;
@@ -391,18 +532,30 @@ int potrf_f32(cudaStream_t st, int n, float *A, long long lda, float *dinv, int 
     if (int rc = diag_smem_attr<float>()) return rc;
     init_info_kernel<<<1, 1, 0, st>>>(d_info, d_pmin);
     BGPU_LAUNCH_CHECK();
-    for (int j0 = 0; j0 < n; j0 += NB) {
-        const int nb = (n - j0 < NB) ? n - j0 : NB;
-        potrf_diag_kernel<float><<<1, 256, 2 * NB * LDS * sizeof(float), st>>>(n, A, lda, j0, dinv + (size_t)(j0 / NB) * NB * NB, d_info, d_pmin);
-        BGPU_LAUNCH_CHECK();
-        const int rest = n - j0 - nb;
+    for (int J0 = 0; J0 < n; J0 += PANEL) {
+        const int JB = std::min(PANEL, n - J0);
+        for (int j0 = J0; j0 < J0 + JB; j0 += NB) {
+            const int nb = std::min(NB, n - j0);
+            float *Di = dinv + (size_t)(j0 / NB) * NB * NB;
+            potrf_diag_kernel<float><<<1, 256, 2 * NB * LDS * sizeof(float), st>>>(n, A, lda, j0, Di, d_info, d_pmin);
+            BGPU_LAUNCH_CHECK();
+            const int rest = n - j0 - nb;
+            if (rest <= 0) break;
+            float *A21 = A + (j0 + nb) + (long long)j0 * lda;
+            trsm_panel_f32<<<ceil_div(rest, 64), 256, 0, st>>>(rest, nb, A21, lda, Di);
+            BGPU_LAUNCH_CHECK();
+            const int pc = J0 + JB - (j0 + nb);
+            if (pc > 0) {
+                syrk_f32<<<dim3(ceil_div(rest, 64), ceil_div(pc, 64)), 256, 0, st>>>(
+                    rest, pc, nb, A21, lda, A + (j0 + nb) + (long long)(j0 + nb) * lda, lda);
+                BGPU_LAUNCH_CHECK();
+            }
+        }
+        const int rest = n - J0 - JB;
         if (rest <= 0) break;
-        float *A21 = A + (j0 + nb) + (long long)j0 * lda;
-        float *A22 = A + (j0 + nb) + (long long)(j0 + nb) * lda;
-        trsm_panel_f32<<<ceil_div(rest, 64), 256, 0, st>>>(rest, nb, A21, lda, dinv + (size_t)(j0 / NB) * NB * NB);
-        BGPU_LAUNCH_CHECK();
+        const float *P = A + (J0 + JB) + (long long)J0 * lda;
         const int t = ceil_div(rest, 64);
-        syrk_f32<<<dim3(t, t), 256, 0, st>>>(rest, nb, A21, lda, A22, lda);
+        syrk_f32<<<dim3(t, t), 256, 0, st>>>(rest, rest, JB, P, lda, A + (J0 + JB) + (long long)(J0 + JB) * lda, lda);
         BGPU_LAUNCH_CHECK();
     }
     return BGPU_OK;

@@ -25,11 +25,14 @@ constexpr int TP_Q = 128, TP_K = 32, TP_LD = TP_K + 1;   // CTA tile: 128 rows q
 // Zi[q + p' n]).  Warp w owns columns k0 + w, k0 + w + 8, ...; a lane owns rows q0 + lane + 32 u.
 // The column's entries come from the per-constraint column pointers ccol, so no entry is read
 // by a warp that does not use it and the sums stay in registers in a fixed order.
-template <typename OutT>
+// ZT: the type Zi is read in.  The 3xTF32 form reads an FP32 copy of Zi: half the L2 traffic of
+// this L2-bound kernel (each entry reads a 128-value segment of a Zi column), and T keeps the
+// accuracy its tf32 hi + lo split can carry (2^-24 relative per term against 2^-22).
+template <typename OutT, typename ZT = double>
 __global__ void __launch_bounds__(256) tprod_kernel(int n, int ldt, int K, int a0, int ncon,
                                                    const long long *__restrict__ cptr, const int *__restrict__ ccol,
                                                    const int *__restrict__ cpos, const double *__restrict__ cval,
-                                                   const double *__restrict__ Zi, OutT *__restrict__ T,
+                                                   const ZT *__restrict__ Zi, OutT *__restrict__ T,
                                                    OutT *__restrict__ Tlo) {
     __shared__ double tile[TP_Q * TP_LD];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -45,10 +48,10 @@ __global__ void __launch_bounds__(256) tprod_kernel(int n, int ldt, int K, int a
             for (long long e = e0; e < e1; e++) {
                 const int pp = cpos[e] - k * n;   // the row p' of the entry (p', k)
                 const double v = cval[e];
-                const double *z = Zi + (long long)pp * n + q0 + lane;
+                const ZT *z = Zi + (long long)pp * n + q0 + lane;
 #pragma unroll
                 for (int u = 0; u < 4; u++)
-                    if (q0 + lane + 32 * u < n) acc[u] += v * z[32 * u];
+                    if (q0 + lane + 32 * u < n) acc[u] += v * (double)z[32 * u];
             }
         }
 #pragma unroll
@@ -411,6 +414,11 @@ int gather_launch(cudaStream_t st, int K, int a0, int ncon, int m, const DevBloc
     return BGPU_OK;
 }
 
+__global__ void to_f32_kernel(long long count, const double *__restrict__ src, float *__restrict__ dst) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count) dst[i] = (float)src[i];
+}
+
 // hi/lo tf32 parts of a column-major n x n double matrix into rows of stride ld (ld >= n)
 __global__ void split2d_kernel(int n, const double *__restrict__ X, int ld, float *__restrict__ hi, float *__restrict__ lo) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
@@ -542,8 +550,9 @@ size_t schur_ws_bytes(int n, int chunk, int precision) {
         return 2 * nn * sizeof(double) + ozaki_operand_bytes((long long)n * chunk, n, S) + ozaki_operand_bytes(n, n, S);
     }
     const size_t ld = tf32_ld(n);
-    // T hi/lo (n K rows of ld), G (float, n K x n), X hi/lo (n rows of ld), plus 256 B alignment slack each
-    return (2 * (size_t)n * chunk * ld + nn + 2 * (size_t)n * ld) * sizeof(float) + 5 * 256;
+    // T hi/lo (n K rows of ld), G (float, n K x n), X hi/lo (n rows of ld), Zi in FP32 (n x n), plus
+    // 256 B alignment slack each
+    return (2 * (size_t)n * chunk * ld + nn + 2 * (size_t)n * ld + (size_t)n * n) * sizeof(float) + 6 * 256;
 }
 
 int schur_assemble(cudaStream_t st, const DevBlock &B, const double *X, const double *Zi, double *M, int m,
@@ -595,11 +604,13 @@ int schur_assemble(cudaStream_t st, const DevBlock &B, const double *X, const do
         return r;
     };
     float *Th = carve((size_t)n * K * ld), *Tl = carve((size_t)n * K * ld), *G = carve(nnK);
-    float *Xh = carve((size_t)n * ld), *Xl = carve((size_t)n * ld);
+    float *Xh = carve((size_t)n * ld), *Xl = carve((size_t)n * ld), *Zf = carve((size_t)n * n);
     split2d_kernel<<<dim3(ceil_div(ld, 256), n), 256, 0, st>>>(n, X, ld, Xh, Xl);
     BGPU_LAUNCH_CHECK();
+    to_f32_kernel<<<ceil_div((long long)n * n, 256), 256, 0, st>>>((long long)n * n, Zi, Zf);
+    BGPU_LAUNCH_CHECK();
     for (int a0 = 0; a0 < B.ncon; a0 += K) {
-        tprod_kernel<float><<<tgrid, 256, 0, st>>>(n, ld, K, a0, B.ncon, B.cptr, B.ccol, B.cpos, B.cval, Zi, Th, Tl);
+        tprod_kernel<float, float><<<tgrid, 256, 0, st>>>(n, ld, K, a0, B.ncon, B.cptr, B.ccol, B.cpos, B.cval, Zf, Th, Tl);
         BGPU_LAUNCH_CHECK();
         int rc = gemm_tf32x3(st, n * K, n, n, Th, Tl, ld, Xh, Xl, ld, G, (long long)n * K);
         if (rc) return rc;

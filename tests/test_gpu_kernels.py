@@ -279,6 +279,37 @@ def test_schur_sym_gather_matches_oracle(cuda, name, kw, chunk):
     assert np.abs(got[1] - got[0]).max() / np.abs(got[0]).max() <= 1e-5
 
 
+def test_schur_large_block_gather_staged_by_cp_async(cuda):
+    """A block of order 820: the chunk's packed sum S outgrows 32 MB at 64 constraints (86 MB in
+    FP32, 172 MB in FP64), so the gather stages S rows through shared memory with cp.async; at 8
+    constraints S stays small and the register gather runs.  Both give the same M (FP64: 1e-12),
+    the 3xTF32 one within 1e-5, and the FP64 one matches the sparse restatement M_ab = <A_b, X A_a Zi>."""
+    d = problems.random_sdp(n=820, m=96, density=0.005, seed=11)
+    S, n, a = block_arrays(d, cuda)
+    u = upper_arrays(a, n, cuda)
+    X = spd(n, 5, cond=100)
+    Zi = spd(n, 6, cond=100)
+    dX, dZi = colmajor(X, cuda), colmajor(Zi, cuda)
+    got = {}
+    for prec, chunk in ((0, 64), (0, 8), (1, 64)):
+        M = torch.zeros(d.m * d.m, dtype=torch.float64, device=cuda)
+        ws = torch.empty(step.ws_bytes(n, chunk, prec), dtype=torch.uint8, device=cuda)
+        step.call("schur_assemble_sym", n, d.m, int(a["con"].numel()), a["con"].data_ptr(), a["cptr"].data_ptr(),
+                  a["ccol"].data_ptr(), a["cpos"].data_ptr(), a["cval"].data_ptr(), u["uptr"].data_ptr(),
+                  u["upos"].data_ptr(), u["uval"].data_ptr(), dX.data_ptr(), dZi.data_ptr(), M.data_ptr(), prec,
+                  chunk, ws.data_ptr(), ws.numel(), None)
+        step.call("sync", None)
+        got[(prec, chunk)] = M.cpu().numpy().reshape(d.m, d.m).T
+    ref = got[(0, 8)]
+    scale = np.abs(ref).max()
+    assert np.abs(got[(0, 64)] - ref).max() <= 1e-12 * scale
+    assert np.abs(got[(1, 64)] - ref).max() <= 1e-5 * scale
+    A = S.A[0]
+    G = np.stack([X @ A[t] @ Zi for t in range(d.m)])
+    want = np.einsum("ipq,jpq->ij", A, G)
+    np.testing.assert_allclose(got[(0, 64)], want, rtol=1e-10, atol=1e-12 * np.abs(want).max())
+
+
 @pytest.mark.parametrize("kw", [dict(n=60, m=200, density=0.05, seed=2), dict(n=100, m=300, density=0.02, seed=3)])
 def test_gram_matches_numpy(cuda, kw):
     """bgpu_schur_gram: <A_a, A_b> of the scaled constraints, to 1e-13 relative."""
