@@ -215,16 +215,28 @@ __global__ void slice_kernel(int rows, int K, int S, const double *__restrict__ 
     for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
     const int e = mx > 0.0 ? ilogb(mx) + 1 : 0;   // max |x| 2^-e < 1
     if (lane == 0) exps[r] = e;
+    // 8 consecutive columns a lane (ldk is a multiple of 64): each slice's 8 digits go out as
+    // one 8-byte store
     int8_t *out = dst + (long long)r * ldk;
-    for (long long k = lane; k < ldk; k += 32) {
-        double a = k < K ? ldexp(x[k], -e) : 0.0;
+    for (long long k8 = lane; k8 < ldk / 8; k8 += 32) {
+        double a[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            const long long k = k8 * 8 + i;
+            a[i] = k < K ? ldexp(x[k], -e) : 0.0;
+        }
 #pragma unroll
         for (int p = 0; p < OZ_SMAX; p++) {
             if (p >= S) break;
-            a *= 128.0;
-            const double t = trunc(a);
-            a -= t;
-            out[p * slice_bytes + k] = (int8_t)(int)t;
+            unsigned long long w = 0;
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                a[i] *= 128.0;
+                const double t = trunc(a[i]);
+                a[i] -= t;
+                w |= (unsigned long long)(uint8_t)(int8_t)(int)t << (8 * i);
+            }
+            *reinterpret_cast<unsigned long long *>(out + p * slice_bytes + k8 * 8) = w;
         }
     }
 }

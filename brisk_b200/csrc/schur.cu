@@ -214,9 +214,25 @@ __global__ void __launch_bounds__(GW * 32) gather_sym_kernel(int a0, int ncon, i
     const long long len = e0 - s0, per_w = (len + GW - 1) / GW;
     const long long s = s0 + warp * per_w, e = min(e0, s + per_w);
     long long base = s;
+    // S rows are K sizeof(GT) bytes at random positions of an S as large as L2: the loads below
+    // wait on memory.  With FP32 rows (the 3xTF32 assembly), each lane asks L2 ahead of time for
+    // the row of its entry in the next group of 32 (prefetch.global.L2: no register is held while
+    // it is in flight), so that group's loads find their rows in L2 (measured on B200, rand1000:
+    // the assembly 175 -> 164 ms; with the FP64 rows, twice as long, the prefetches cost more than
+    // they save: 669 -> 709 ms, so they are left out there).
+    constexpr int RB = K * (int)sizeof(GT);
+    auto prefetch_row = [&](long long at) {
+        if (sizeof(GT) == 4 && at < e) {
+            const char *row = reinterpret_cast<const char *>(S + (long long)upos[at] * K);
+#pragma unroll
+            for (int o = 0; o < RB; o += 128) asm volatile("prefetch.global.L2 [%0];" ::"l"(row + o));
+        }
+    };
+    prefetch_row(base + lane);
     for (; base + 32 <= e; base += 32) {
         const int pos = upos[base + lane];
         const double v = uval[base + lane];
+        prefetch_row(base + 32 + lane);
 #pragma unroll
         for (int j = 0; j < 32; j += GPW) {
             const int pj = __shfl_sync(0xffffffffu, pos, j + sub);
