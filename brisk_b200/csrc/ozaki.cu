@@ -26,11 +26,16 @@
 // multiply-adds; 128 x 96 x 32 reads 7 KB for 393 k) as well as issuing fewer MMAs: S = 5 issues
 // 15 per 32-deep k-step and 96 columns, S = 8 36 per 64 columns.
 //
-// One CTA per 128 x BN tile, as tf32x3.cu: warp 0 / lane 0 the TMA producer (the S slices of A and
-// of B for a 64-byte k-block, 64-byte swizzle, a 2- or 3-deep ring), warp 1 / lane 0 the MMA
-// issuer (kind::i8, M = 128, N = BN, K = 32 per instruction), all 4 warps the epilogue (16
-// columns at a time over all S accumulators).  Every mbarrier wait is bounded; a wait that runs
-// out sets *err and the CTA winds down.  No cluster, no multicast.
+// Persistent and warp-specialised, as tf32x3.cu: one CTA per SM walks the 128 x BN tiles (N tiles
+// fastest).  Warp 0 / lane 0 is the TMA producer (the S slices of A and of B for a 64-byte
+// k-block, 64-byte swizzle, a 2- or 3-deep ring that runs on across tiles), warp 1 / lane 0 the
+// MMA issuer (kind::i8, M = 128, N = BN, K = 32 per instruction), warps 2-5 the epilogue (16
+// columns at a time over all S accumulators, the tile's column exponents staged in shared
+// memory, the scale 2^(e_i + f_j) built exactly as a power of two).  The S accumulators fill
+// TMEM, so the MMAs of the next tile wait for this tile's epilogue; the next tile's loads do not.
+// Every mbarrier wait is bounded; a role that gives up stops the others, the producer waits
+// (bounded) for its copies in flight, the MMA warp for its last MMAs, and *err records the
+// failure.  No cluster, no multicast.
 #include "common.cuh"
 #include "kernels.h"
 #include "tcgen05.cuh"
@@ -38,7 +43,7 @@
 namespace {
 using namespace tc;
 constexpr int OZ_SMAX = 8;               // most slices per operand (56 bits)
-constexpr int BM = 128, BK = 64, NTHREADS = 128;
+constexpr int BM = 128, BK = 64, NTHREADS = 192;
 constexpr int A_TILE = BM * BK;          // bytes of one slice's A tile
 constexpr int TMEM_COLS = 512;           // S accumulators of BN columns
 
@@ -52,7 +57,7 @@ template <int S> struct OzShape {
     static constexpr int BN = OzCfg<S>::BN, STAGES = OzCfg<S>::STAGES;
     static constexpr int B_TILE = BN * BK;
     static constexpr int STAGE = S * (A_TILE + B_TILE);
-    static constexpr size_t SMEM = (size_t)STAGES * STAGE + 1024 /*align*/ + 256 /*barriers*/;
+    static constexpr size_t SMEM = (size_t)STAGES * STAGE + 1024 /*align*/ + 256 /*barriers*/ + BN * sizeof(int);
     static_assert(S * BN <= TMEM_COLS, "accumulators must fit in TMEM");
     static_assert(STAGE % 1024 == 0, "stages keep the 1024-byte alignment of the swizzled tiles");
     static_assert(SMEM <= 232448, "shared memory of one CTA");
@@ -81,6 +86,12 @@ __device__ __forceinline__ void umma_i8(uint32_t tmem_d, uint64_t a, uint64_t b,
         ::"r"(tmem_d), "l"(a), "l"(b), "r"(idesc), "r"(acc));
 }
 
+// 2^e as a double, exactly, for e in the normal range (ldexp otherwise)
+__device__ __forceinline__ double pow2(int e) {
+    if (e >= -1022 && e <= 1023) return __longlong_as_double((long long)(e + 1023) << 52);
+    return ldexp(1.0, e);
+}
+
 template <int S>
 __global__ void __launch_bounds__(NTHREADS, 1)
     ozaki_kernel(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorMap tB, long long a_slice_rows,
@@ -92,11 +103,14 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     uint64_t *full = (uint64_t *)(smem + STAGES * STAGE);
     uint64_t *empty = full + STAGES;
-    uint64_t *done = empty + STAGES;
-    uint32_t *tslot = (uint32_t *)(done + 1);
-    int *bad = (int *)(tslot + 1);
+    uint64_t *tfull = empty + STAGES;     // the accumulators are ready for the epilogue
+    uint64_t *tempty = tfull + 1;         // ... drained (4 epilogue warps arrive)
+    uint64_t *mdone = tempty + 1;         // the MMA warp's last MMAs
+    uint32_t *tslot = (uint32_t *)(mdone + 1);
+    volatile int *bad = (volatile int *)(tslot + 1);
+    int *ebs = (int *)(smem + STAGES * STAGE + 256);   // the tile's column exponents
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+    const int ntn = (N + BN - 1) / BN, ntm = (M + BM - 1) / BM, ntiles = ntn * ntm;
     const int nkb = (K + BK - 1) / BK;
 
     if (threadIdx.x == 0) {
@@ -104,7 +118,9 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], 1);
         }
-        mbar_init(done, 1);
+        mbar_init(tfull, 1);
+        mbar_init(tempty, 4);
+        mbar_init(mdone, 1);
         *bad = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -119,84 +135,115 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     tc_fence_after();
     const uint32_t tmem = *tslot;
 
-    if (warp == 0 && lane == 0) {
-        // ---- TMA producer: the S slices of A (rows m0..) and of B (rows n0..) of a k-block ----
-        int issued = 0;
-        for (int kb = 0; kb < nkb; kb++) {
-            const int s = kb % STAGES, use = kb / STAGES;
-            if (use > 0 && !mbar_wait(&empty[s], (use - 1) & 1)) { atomicExch(bad, 1); break; }
-            uint8_t *st = smem + s * STAGE;
-            mbar_expect_tx(&full[s], STAGE);
-            const int x = kb * BK;
-            for (int p = 0; p < S; p++) {
-                tma_load_2d(st + p * A_TILE, &tA, &full[s], x, (int)(p * a_slice_rows + m0));
-                tma_load_2d(st + S * A_TILE + p * B_TILE, &tB, &full[s], x, (int)(p * b_slice_rows + n0));
-            }
-            issued++;
-        }
-        for (int kb = (issued > STAGES ? issued - STAGES : 0); kb < issued; kb++)
-            mbar_wait(&full[kb % STAGES], (kb / STAGES) & 1);
-    } else if (warp == 1 && lane == 0) {
-        // ---- MMA issuer: every slice pair p + q <= S + 1 into the accumulator of its diagonal ----
-        constexpr uint32_t idesc = idesc_i8(BM, BN);
-        for (int kb = 0; kb < nkb; kb++) {
-            const int s = kb % STAGES;
-            if (!mbar_wait(&full[s], (kb / STAGES) & 1)) { atomicExch(bad, 1); break; }
-            tc_fence_after();
-            const uint32_t base = smem_u32(smem + s * STAGE);
-#pragma unroll
-            for (int ks = 0; ks < BK / 32; ks++) {   // K-step of 32 int8 = 32 bytes inside the swizzle atom
-                const uint32_t off = ks * 32;
-#pragma unroll
-                for (int d = 0; d < S; d++) {          // diagonal p + q = d + 2 (0-based slices: p + q = d)
-#pragma unroll
-                    for (int p = 0; p <= d; p++) {
-                        const int q = d - p;
-                        const uint64_t a = smem_desc64(base + p * A_TILE + off);
-                        const uint64_t b = smem_desc64(base + S * A_TILE + q * B_TILE + off);
-                        umma_i8(tmem + (uint32_t)(d * BN), a, b, idesc, (kb | ks | p) != 0);
+    if (warp == 0) {
+        if (lane == 0) {
+            // ---- TMA producer: the S slices of A (rows m0..) and of B (rows n0..) of a k-block ----
+            long long it = 0;
+            for (int t = blockIdx.x; t < ntiles && !*bad; t += gridDim.x) {
+                const int m0 = (t / ntn) * BM, n0 = (t % ntn) * BN;
+                for (int kb = 0; kb < nkb; kb++, it++) {
+                    const int s = (int)(it % STAGES);
+                    const long long use = it / STAGES;
+                    if (use > 0 && !mbar_wait_or_stop(&empty[s], (uint32_t)((use - 1) & 1), bad)) { *bad = 1; break; }
+                    uint8_t *st = smem + s * STAGE;
+                    mbar_expect_tx(&full[s], STAGE);
+                    const int x = kb * BK;
+                    for (int p = 0; p < S; p++) {
+                        tma_load_2d(st + p * A_TILE, &tA, &full[s], x, (int)(p * a_slice_rows + m0));
+                        tma_load_2d(st + S * A_TILE + p * B_TILE, &tB, &full[s], x, (int)(p * b_slice_rows + n0));
                     }
                 }
             }
-            umma_commit(&empty[s]);
+            for (long long k = (it > STAGES ? it - STAGES : 0); k < it; k++)
+                mbar_wait(&full[k % STAGES], (uint32_t)((k / STAGES) & 1));
         }
-        umma_commit(done);
-    }
-    __syncwarp();
-    // ---- epilogue: the S accumulators -> FP64, smallest terms first, scaled by 2^(e_i + f_j) ----
-    const bool ok = mbar_wait(done, 0);
-    tc_fence_after();
-    const bool good = __all_sync(0xffffffffu, ok && !*(volatile int *)bad);
-    if (good) {
-        // 16 columns at a time: their S accumulators, smallest diagonal terms first
-        const int row = m0 + warp * 32 + lane;
-        const int e = row < M ? ea[row] : 0;
-#pragma unroll 1
-        for (int c0 = 0; c0 < BN; c0 += 16) {
-            double acc[16];
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // ---- MMA issuer: every slice pair p + q <= S + 1 into the accumulator of its diagonal ----
+            constexpr uint32_t idesc = idesc_i8(BM, BN);
+            long long it = 0;
+            int lt = 0;
+            for (int t = blockIdx.x; t < ntiles && !*bad; t += gridDim.x, lt++) {
+                if (lt > 0 && !mbar_wait_or_stop(tempty, (uint32_t)((lt - 1) & 1), bad)) { *bad = 1; break; }
+                tc_fence_after();
+                bool ok = true;
+                for (int kb = 0; kb < nkb; kb++, it++) {
+                    const int s = (int)(it % STAGES);
+                    if (!mbar_wait_or_stop(&full[s], (uint32_t)((it / STAGES) & 1), bad)) { ok = false; break; }
+                    tc_fence_after();
+                    const uint32_t base = smem_u32(smem + s * STAGE);
 #pragma unroll
-            for (int j = 0; j < 16; j++) acc[j] = 0.0;
+                    for (int ks = 0; ks < BK / 32; ks++) {   // K-step of 32 int8 = 32 bytes inside the swizzle atom
+                        const uint32_t off = ks * 32;
 #pragma unroll
-            for (int d = S - 1; d >= 0; d--) {
-                const double w = ldexp(1.0, -7 * (d + 2));
-                uint32_t r[16];
-                tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(d * BN + c0), r);
+                        for (int d = 0; d < S; d++) {          // diagonal p + q = d + 2 (0-based slices: p + q = d)
 #pragma unroll
-                for (int j = 0; j < 16; j++) acc[j] += w * (double)(int)r[j];
+                            for (int p = 0; p <= d; p++) {
+                                const int q = d - p;
+                                const uint64_t a = smem_desc64(base + p * A_TILE + off);
+                                const uint64_t b = smem_desc64(base + S * A_TILE + q * B_TILE + off);
+                                umma_i8(tmem + (uint32_t)(d * BN), a, b, idesc, (kb | ks | p) != 0);
+                            }
+                        }
+                    }
+                    umma_commit(&empty[s]);
+                }
+                if (!ok) { *bad = 1; break; }
+                umma_commit(tfull);
             }
-            if (row < M) {
+            umma_commit(mdone);
+            mbar_wait(mdone, 0);
+        }
+    } else {
+        // ---- epilogue: the S accumulators -> FP64, smallest terms first, scaled by 2^(e_i + f_j) ----
+        const int q = warp & 3;               // the TMEM lane quarter this warp may read
+        const int et = threadIdx.x - 64;      // 0..127 over the 4 epilogue warps
+        int lt = 0;
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x, lt++) {
+            const int m0 = (t / ntn) * BM, n0 = (t % ntn) * BN;
+            // the tile's column exponents (the previous tile's have been read: every epilogue
+            // thread passed the barrier below after its last read of them)
+            asm volatile("bar.sync 1, 128;" ::: "memory");
+            for (int c = et; c < BN; c += 128) ebs[c] = n0 + c < N ? eb[n0 + c] : 0;
+            const bool ok = mbar_wait_or_stop(tfull, (uint32_t)(lt & 1), bad);
+            // one decision for the 4 warps (a barrier reduction: the next iteration's barrier must
+            // see all 128 threads or none), which also publishes ebs
+            unsigned stop;
+            asm volatile("{\n .reg .pred p, r;\n setp.ne.u32 p, %1, 0;\n bar.red.or.pred r, 1, 128, p;\n selp.u32 %0, 1, 0, r;\n}\n"
+                         : "=r"(stop) : "r"((unsigned)(!ok)) : "memory");
+            if (stop) { if (et == 0) *bad = 1; break; }
+            tc_fence_after();
+            const int row = m0 + q * 32 + lane;
+            const int e = row < M ? ea[row] : 0;
+#pragma unroll 1
+            for (int c0 = 0; c0 < BN; c0 += 16) {
+                double acc[16];
 #pragma unroll
-                for (int j = 0; j < 16; j++) {
-                    const int col = n0 + c0 + j;
-                    if (col < N) C[(long long)row + (long long)col * ldc] = ldexp(acc[j], e + eb[col]);
+                for (int j = 0; j < 16; j++) acc[j] = 0.0;
+#pragma unroll
+                for (int d = S - 1; d >= 0; d--) {
+                    const double w = pow2(-7 * (d + 2));
+                    uint32_t r[16];
+                    tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(d * BN + c0), r);
+#pragma unroll
+                    for (int j = 0; j < 16; j++) acc[j] += w * (double)(int)r[j];
+                }
+                if (row < M) {
+#pragma unroll
+                    for (int j = 0; j < 16; j++) {
+                        const int col = n0 + c0 + j;
+                        if (col < N) C[(long long)row + (long long)col * ldc] = acc[j] * pow2(e + ebs[c0 + j]);
+                    }
                 }
             }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(tempty);
         }
-    } else if (threadIdx.x == 0) {
-        atomicExch(err, 1);
     }
-    tc_fence_before();
     __syncthreads();
+    if (threadIdx.x == 0 && *bad) atomicExch(err, 1);
+    tc_fence_after();
     if (warp == 0) {
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
     }
@@ -310,8 +357,12 @@ int ozaki_launch(cudaStream_t st, const OzakiOperand &A, const OzakiOperand &B, 
                                                    (int)Sh::SMEM)));
     void *d = nullptr;
     BGPU_CHECK(cudaGetSymbolAddress(&d, g_ozaki_err));
-    if (ceil_div(M, BM) > 65535) return BGPU_ERR_TOOBIG;
-    dim3 grid(ceil_div(N, Sh::BN), ceil_div(M, BM));
+    int dev = 0, nsm = 0;
+    BGPU_CHECK(cudaGetDevice(&dev));
+    BGPU_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    const long long ntiles = (long long)ceil_div(N, Sh::BN) * ceil_div(M, BM);
+    if (ntiles > 0x7fffffffLL) return BGPU_ERR_TOOBIG;
+    const int grid = (int)(ntiles < nsm ? ntiles : nsm);   // persistent: one CTA per SM
     ozaki_kernel<S><<<grid, NTHREADS, Sh::SMEM, st>>>(mA, mB, A.srows, B.srows, A.e, B.e, C, ldc, M, N, K, (int *)d);
     BGPU_LAUNCH_CHECK();
     return BGPU_OK;

@@ -35,6 +35,30 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
     }
     return false;
 }
+// a plain arrive (count 1) on an mbarrier
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+// bounded wait that also gives up once *stop is set (another role of the CTA gave up)
+__device__ __forceinline__ bool mbar_wait_or_stop(uint64_t *bar, uint32_t parity, const volatile int *stop) {
+    for (uint32_t i = 0; i < BGPU_SPIN_LIMIT; i++) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if ((i & 63) == 63 && *stop) return false;
+        if (i > 128) __nanosleep(64);
+    }
+    return false;
+}
+// tcgen05 shared-memory matrix descriptor: K-major rows of 64 bytes, 64-byte swizzle, 8-row groups
+// 512 B apart (the layout TMA writes with CU_TENSOR_MAP_SWIZZLE_64B)
+__device__ __forceinline__ uint64_t smem_desc_sw64(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr & 0x3FFFFu) >> 4);        // start address
+    d |= (uint64_t)(16u >> 4) << 16;                  // leading byte offset (unused with this swizzle)
+    d |= (uint64_t)(512u >> 4) << 32;                 // stride byte offset: 8 rows x 64 B
+    d |= (uint64_t)1 << 46;                           // descriptor version
+    d |= (uint64_t)4 << 61;                           // swizzle: 64 B
+    return d;
+}
 __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, uint64_t *bar, int x, int y) {
     asm volatile(
         "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];"

@@ -4,40 +4,38 @@
 // Ah Bh + Ah Bl + Al Bh with FP32 accumulation in tensor memory: FP32-level accuracy at
 // three tf32 MMAs per product (the dropped Al Bl term is below FP32 rounding).
 //
-// One CTA per 128 x BN output tile (cta_group::1):
-//   warp 0 / lane 0  TMA producer: 4 operand tiles (Ah, Al, Bh, Bl: 32 fp32 of K x 128 or BN
-//                    rows, 128-byte swizzle) per k-block into a STAGES-deep ring, one mbarrier
-//                    with the transaction count per stage
-//   warp 1 / lane 0  MMA issuer: 4 K-steps of 8 x 3 products per k-block (tcgen05.mma kind::tf32,
-//                    M = 128, N = BN), tcgen05.commit releases the stage, a last commit the tile
-//   all 4 warps      epilogue: tcgen05.ld 32x32b (warp w reads TMEM lanes 32w..32w+31 = rows),
-//                    column-major stores (consecutive lanes = consecutive rows: coalesced)
-// Every mbarrier wait is bounded; a wait that runs out sets *err and the CTA winds down.
-// No cluster, no multicast: each CTA loads its own tiles from this GPU's memory.
+// Persistent and warp-specialised: one CTA per SM walks the 128 x BN output tiles t = blockIdx.x,
+// blockIdx.x + gridDim.x, ... (N tiles fastest, so the CTAs that share an A row panel run
+// together and reuse it from L2).
+//   warp 0 / lane 0  TMA producer: the 4 operand tiles of a 16-column k-block (Ah, Al: 128 rows;
+//                    Bh, Bl: BN rows; 64-byte rows, 64-byte swizzle) into a STAGES-deep ring that
+//                    runs on across tile boundaries, one mbarrier with the transaction count a stage
+//   warp 1 / lane 0  MMA issuer: 2 K-steps of 3 products a k-block (tcgen05.mma kind::tf32,
+//                    M = 128, N = BN) into one of two TMEM accumulators (2 x BN <= 512 columns);
+//                    tcgen05.commit frees a stage, and at a tile's end hands its accumulator over
+//   warps 2-5        epilogue: tcgen05.ld 32x32b (warp w reads TMEM lanes 32 (w % 4) .. +31 =
+//                    rows), column-major stores (consecutive lanes = consecutive rows: coalesced),
+//                    then the accumulator goes back to the MMA warp
+// So one tile's epilogue runs under the next tile's MMAs, and the next tile's loads under both.
+// Every mbarrier wait is bounded; a role that gives up sets a flag that stops the others, the
+// producer waits (bounded) for its copies in flight, the MMA warp for its last MMAs, and *err
+// records the failure.  No cluster, no multicast: each CTA loads its own tiles from this GPU's
+// memory.
 #include "common.cuh"
 #include "kernels.h"
 #include "tf32x3.h"
 #include "tcgen05.cuh"
 
 #include <cuda.h>
+#include <algorithm>
 #include <mutex>
 #include <unordered_map>
 
 namespace {
 using namespace tc;
-constexpr int BM = 128, BK = 32, STAGES = 2, NTHREADS = 128;
-constexpr int A_BYTES = BM * BK * 4;   // 16 KB
+constexpr int BM = 128, BK = 16, STAGES = 4, NTHREADS = 192;
+constexpr int A_BYTES = BM * BK * 4;   // 8 KB
 
-// tcgen05 shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups 1024 B apart
-__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr) {
-    uint64_t d = 0;
-    d |= (uint64_t)((saddr & 0x3FFFFu) >> 4);        // start address
-    d |= (uint64_t)(16u >> 4) << 16;                  // leading byte offset (unused with this swizzle)
-    d |= (uint64_t)(1024u >> 4) << 32;                // stride byte offset: 8 rows x 128 B
-    d |= (uint64_t)1 << 46;                           // descriptor version
-    d |= (uint64_t)2 << 61;                           // swizzle: 128 B
-    return d;
-}
 // instruction descriptor: D f32, A/B tf32, both K-major, N and M
 __host__ __device__ constexpr uint32_t idesc_tf32(int M, int N) {
     return (1u << 4)                       // D format f32
@@ -54,8 +52,11 @@ template <int BN>
 struct Cfg {
     static constexpr int B_BYTES = BN * BK * 4;
     static constexpr int STAGE = 2 * A_BYTES + 2 * B_BYTES;
-    static constexpr int TMEM_COLS = BN <= 32 ? 32 : BN <= 64 ? 64 : BN <= 128 ? 128 : 256;
+    static constexpr int ACC_COLS = BN <= 32 ? 32 : BN <= 64 ? 64 : BN <= 128 ? 128 : 256;   // one accumulator
+    static constexpr int TMEM_COLS = 2 * ACC_COLS;
     static constexpr size_t SMEM = (size_t)STAGES * STAGE + 1024 /*align*/ + 256 /*barriers*/;
+    static_assert(TMEM_COLS <= 512, "two accumulators in TMEM");
+    static_assert(STAGE % 1024 == 0, "stages keep the alignment of the swizzled tiles");
 };
 
 template <int BN>
@@ -68,12 +69,13 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     uint64_t *full = (uint64_t *)(smem + STAGES * C::STAGE);
     uint64_t *empty = full + STAGES;
-    uint64_t *done = empty + STAGES;
-    uint32_t *tslot = (uint32_t *)(done + 1);
-    int *bad = (int *)(tslot + 1);
+    uint64_t *tfull = empty + STAGES;     // [2] accumulator ready for the epilogue
+    uint64_t *tempty = tfull + 2;         // [2] accumulator drained (4 epilogue warps arrive)
+    uint64_t *mdone = tempty + 2;         // the MMA warp's last MMAs
+    uint32_t *tslot = (uint32_t *)(mdone + 1);
+    volatile int *bad = (volatile int *)(tslot + 1);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    // N tiles vary fastest: the CTAs that share an A row panel run together and reuse it from L2
-    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+    const int ntn = (N + BN - 1) / BN, ntm = (M + BM - 1) / BM, ntiles = ntn * ntm;
     const int nkb = (K + BK - 1) / BK;
 
     if (threadIdx.x == 0) {
@@ -81,7 +83,11 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], 1);
         }
-        mbar_init(done, 1);
+        for (int a = 0; a < 2; a++) {
+            mbar_init(&tfull[a], 1);
+            mbar_init(&tempty[a], 4);
+        }
+        mbar_init(mdone, 1);
         *bad = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -96,71 +102,96 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     tc_fence_after();
     const uint32_t tmem = *tslot;
 
-    if (warp == 0 && lane == 0) {
-        // ---- TMA producer ----
-        int issued = 0;
-        for (int kb = 0; kb < nkb; kb++) {
-            const int s = kb % STAGES, use = kb / STAGES;
-            if (use > 0 && !mbar_wait(&empty[s], (use - 1) & 1)) { atomicExch(bad, 1); break; }
-            uint8_t *st = smem + s * C::STAGE;
-            mbar_expect_tx(&full[s], C::STAGE);
-            const int x = kb * BK;
-            tma_load_2d(st, &tAh, &full[s], x, m0);
-            tma_load_2d(st + A_BYTES, &tAl, &full[s], x, m0);
-            tma_load_2d(st + 2 * A_BYTES, &tBh, &full[s], x, n0);
-            tma_load_2d(st + 2 * A_BYTES + C::B_BYTES, &tBl, &full[s], x, n0);
-            issued++;
-        }
-        // copies still in flight are waited for before the CTA ends (bounded)
-        for (int kb = (issued > STAGES ? issued - STAGES : 0); kb < issued; kb++)
-            mbar_wait(&full[kb % STAGES], (kb / STAGES) & 1);
-    } else if (warp == 1 && lane == 0) {
-        // ---- MMA issuer ----
-        constexpr uint32_t idesc = idesc_tf32(BM, BN);
-        for (int kb = 0; kb < nkb; kb++) {
-            const int s = kb % STAGES;
-            if (!mbar_wait(&full[s], (kb / STAGES) & 1)) { atomicExch(bad, 1); break; }
-            tc_fence_after();
-            const uint32_t base = smem_u32(smem + s * C::STAGE);
-#pragma unroll
-            for (int ks = 0; ks < BK / 8; ks++) {   // K-step of 8 tf32 = 32 bytes inside the swizzle atom
-                const uint32_t off = ks * 32;
-                const uint64_t ah = smem_desc(base + off), al = smem_desc(base + A_BYTES + off);
-                const uint64_t bh = smem_desc(base + 2 * A_BYTES + off);
-                const uint64_t bl = smem_desc(base + 2 * A_BYTES + C::B_BYTES + off);
-                umma_tf32(tmem, al, bh, idesc, (kb | ks) != 0);   // small terms first
-                umma_tf32(tmem, ah, bl, idesc, 1);
-                umma_tf32(tmem, ah, bh, idesc, 1);
-            }
-            umma_commit(&empty[s]);   // the stage is free once these MMAs have read it
-        }
-        umma_commit(done);
-    }
-    __syncwarp();
-    // ---- epilogue: TMEM -> registers -> global (column-major) ----
-    const bool ok = mbar_wait(done, 0);
-    tc_fence_after();
-    // tcgen05.ld is warp-collective: the decision must be uniform across the warp
-    const bool good = __all_sync(0xffffffffu, ok && !*(volatile int *)bad);
-    if (good) {
-        const int row = m0 + warp * 32 + lane;
-#pragma unroll 1
-        for (int c0 = 0; c0 < BN; c0 += 16) {
-            uint32_t r[16];
-            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, r);
-            if (row < M) {
-#pragma unroll
-                for (int j = 0; j < 16; j++) {
-                    const int col = n0 + c0 + j;
-                    if (col < N) G[(long long)row + (long long)col * ldg] = __uint_as_float(r[j]);
+    if (warp == 0) {
+        if (lane == 0) {
+            // ---- TMA producer ----
+            long long it = 0;
+            for (int t = blockIdx.x; t < ntiles && !*bad; t += gridDim.x) {
+                const int m0 = (t / ntn) * BM, n0 = (t % ntn) * BN;
+                for (int kb = 0; kb < nkb; kb++, it++) {
+                    const int s = (int)(it % STAGES);
+                    const long long use = it / STAGES;
+                    if (use > 0 && !mbar_wait_or_stop(&empty[s], (uint32_t)((use - 1) & 1), bad)) { *bad = 1; break; }
+                    uint8_t *st = smem + s * C::STAGE;
+                    mbar_expect_tx(&full[s], C::STAGE);
+                    const int x = kb * BK;
+                    tma_load_2d(st, &tAh, &full[s], x, m0);
+                    tma_load_2d(st + A_BYTES, &tAl, &full[s], x, m0);
+                    tma_load_2d(st + 2 * A_BYTES, &tBh, &full[s], x, n0);
+                    tma_load_2d(st + 2 * A_BYTES + C::B_BYTES, &tBl, &full[s], x, n0);
                 }
             }
+            // copies still in flight are waited for before the CTA ends (bounded)
+            for (long long k = (it > STAGES ? it - STAGES : 0); k < it; k++)
+                mbar_wait(&full[k % STAGES], (uint32_t)((k / STAGES) & 1));
         }
-    } else if (threadIdx.x == 0) {
-        atomicExch(err, 1);
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // ---- MMA issuer ----
+            constexpr uint32_t idesc = idesc_tf32(BM, BN);
+            long long it = 0;
+            int lt = 0;
+            for (int t = blockIdx.x; t < ntiles && !*bad; t += gridDim.x, lt++) {
+                const int a = lt & 1, use = lt >> 1;
+                if (use > 0 && !mbar_wait_or_stop(&tempty[a], (uint32_t)((use - 1) & 1), bad)) { *bad = 1; break; }
+                tc_fence_after();
+                const uint32_t d = tmem + (uint32_t)(a * C::ACC_COLS);
+                bool ok = true;
+                for (int kb = 0; kb < nkb; kb++, it++) {
+                    const int s = (int)(it % STAGES);
+                    if (!mbar_wait_or_stop(&full[s], (uint32_t)((it / STAGES) & 1), bad)) { ok = false; break; }
+                    tc_fence_after();
+                    const uint32_t base = smem_u32(smem + s * C::STAGE);
+#pragma unroll
+                    for (int ks = 0; ks < BK / 8; ks++) {   // K-step of 8 tf32 = 32 bytes inside the swizzle atom
+                        const uint32_t off = ks * 32;
+                        const uint64_t ah = smem_desc_sw64(base + off), al = smem_desc_sw64(base + A_BYTES + off);
+                        const uint64_t bh = smem_desc_sw64(base + 2 * A_BYTES + off);
+                        const uint64_t bl = smem_desc_sw64(base + 2 * A_BYTES + C::B_BYTES + off);
+                        umma_tf32(d, al, bh, idesc, (kb | ks) != 0);   // small terms first
+                        umma_tf32(d, ah, bl, idesc, 1);
+                        umma_tf32(d, ah, bh, idesc, 1);
+                    }
+                    umma_commit(&empty[s]);   // the stage is free once these MMAs have read it
+                }
+                if (!ok) { *bad = 1; break; }
+                umma_commit(&tfull[a]);       // the accumulator is complete once these MMAs are
+            }
+            umma_commit(mdone);
+            mbar_wait(mdone, 0);              // every MMA of this CTA has completed (bounded)
+        }
+    } else {
+        // ---- epilogue: TMEM -> registers -> global (column-major) ----
+        const int q = warp & 3;               // the TMEM lane quarter this warp may read
+        int lt = 0;
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x, lt++) {
+            const int a = lt & 1, use = lt >> 1;
+            const bool ok = mbar_wait_or_stop(&tfull[a], (uint32_t)(use & 1), bad);
+            // tcgen05.ld is warp-collective: the decision must be uniform across the warp
+            if (!__all_sync(0xffffffffu, ok)) { if (lane == 0) *bad = 1; break; }
+            tc_fence_after();
+            const int m0 = (t / ntn) * BM, n0 = (t % ntn) * BN;
+            const int row = m0 + q * 32 + lane;
+#pragma unroll 1
+            for (int c0 = 0; c0 < BN; c0 += 16) {
+                uint32_t r[16];
+                tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(a * C::ACC_COLS + c0), r);
+                if (row < M) {
+#pragma unroll
+                    for (int j = 0; j < 16; j++) {
+                        const int col = n0 + c0 + j;
+                        if (col < N) G[(long long)row + (long long)col * ldg] = __uint_as_float(r[j]);
+                    }
+                }
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&tempty[a]);
+        }
     }
-    tc_fence_before();
     __syncthreads();
+    if (threadIdx.x == 0 && *bad) atomicExch(err, 1);
+    tc_fence_after();
     if (warp == 0) {
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(C::TMEM_COLS)
                      : "memory");
@@ -176,7 +207,7 @@ __global__ void split_kernel(long long n, const double *x, float *hi, float *lo)
     lo[i] = tf32_round((float)(v - (double)h));
 }
 
-// rows x K fp32, row stride ld elements, box 32 (K) x box_rows, 128-byte swizzle
+// rows x K fp32, row stride ld elements, box BK = 16 (K: 64 bytes) x box_rows, 64-byte swizzle
 int make_map(CUtensorMap *map, const float *ptr, long long rows, long long K, long long ld, int box_rows) {
     EncodeTiledFn fn = encode_fn();
     if (!fn) return BGPU_ERR_CUDA;
@@ -186,7 +217,7 @@ int make_map(CUtensorMap *map, const float *ptr, long long rows, long long K, lo
     cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)box_rows};
     cuuint32_t estr[2] = {1, 1};
     CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, (void *)ptr, dims, strides, box, estr,
-                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS ? BGPU_OK : BGPU_ERR_ARG;
 }
@@ -213,7 +244,12 @@ int launch(cudaStream_t st, int M, int N, int K, const float *Ah, const float *A
                                                    (int)Cfg<BN>::SMEM)));
     int *err = err_flag();
     if (!err) return BGPU_ERR_NOMEM;
-    dim3 grid(ceil_div(N, BN), ceil_div(M, BM));
+    int dev = 0, nsm = 0;
+    BGPU_CHECK(cudaGetDevice(&dev));
+    BGPU_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    const long long ntiles = (long long)ceil_div(N, BN) * ceil_div(M, BM);
+    if (ntiles > 0x7fffffffLL) return BGPU_ERR_TOOBIG;
+    const int grid = (int)std::min<long long>(ntiles, nsm);   // persistent: one CTA per SM
     tf32x3_kernel<BN><<<grid, NTHREADS, Cfg<BN>::SMEM, st>>>(mAh, mAl, mBh, mBl, G, ldg, M, N, K, err);
     BGPU_LAUNCH_CHECK();
     return BGPU_OK;

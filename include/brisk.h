@@ -64,9 +64,10 @@ BRISK_API int brisk_interrupted(void);
 BRISK_API void brisk_clear_interrupt(void);
 BRISK_API void brisk_set_interrupt_owner(int caller);
 
-/* Solve the SDPA problem given by its numbers: block sizes bs (LP blocks are not supported
- * by this build and return 2), c (m), entries (mat, blk, i, j, v), 1-based as in the file,
- * mat 0 = F0.  Options are command-line strings.  Returns the exit code: 0 optimal, 10
+/* Solve the SDPA problem given by its numbers: block sizes bs (an LP block is a negative size:
+ * its variables are solved as blocks of order 1, and brisk_result_X / brisk_result_Z return it
+ * as its vector of values, as the reference does), c (m), entries (mat, blk, i, j, v), 1-based as
+ * in the file, mat 0 = F0.  Options are command-line strings.  Returns the exit code: 0 optimal, 10
  * reduced accuracy, 11/12 primal/dual infeasible, 13 iteration limit, 14 numerical
  * difficulties, 15 time limit, 1 bad options, 2 unreadable problem, < 0 abort.
  * Replaces capi.c:175 brisk_solve_data. */

@@ -7,7 +7,8 @@ problem as given, and records per run: status, iterations, objectives, the six D
 the iteration table of -v (pobj, dobj, pinf, dinf, gap, mu per iteration) and the time.
 
 Runs per instance: "init0" and "default" (HKM direction, SDPT3 and least-squares start), "nt"
-and "nt_init0" (NT direction, least-squares and SDPT3 start).
+and "nt_init0" (NT direction, least-squares and SDPT3 start), "hsd_auto" (no -nohsd: the
+reference's automatic choice, the self-dual embedding first on most problems).
 
 usage: python tests/golden/make_golden.py [--big] [--huge] [--runs r1,r2] [names]
        (--big adds rand400 and mom700; --huge adds rand1000, the n = 1000, m = 8000 instance, with
@@ -57,7 +58,10 @@ HUGE = {"rand1000": (random_sdp, dict(n=1000, m=8000, density=0.005, seed=0))}
 
 HKM = ["-nohsd", "-dir", "hkm", "-mixed", "0", "-tol", "1e-7"] + AS_GIVEN
 NTD = ["-nohsd", "-dir", "nt", "-mixed", "0", "-tol", "1e-7"] + AS_GIVEN
-RUNS = {"init0": HKM + ["-init", "0"], "default": HKM, "nt": NTD, "nt_init0": NTD + ["-init", "0"]}
+# "hsd_auto": the reference's own choice of method (no -nohsd: its automatic rule runs the self-dual
+# embedding first on most problems), the solve a caller gets with its default options
+RUNS = {"init0": HKM + ["-init", "0"], "default": HKM, "nt": NTD, "nt_init0": NTD + ["-init", "0"],
+        "hsd_auto": ["-dir", "hkm", "-mixed", "0", "-tol", "1e-7"] + AS_GIVEN}
 HUGE_RUNS = {"default": HKM, "mixed": ["-nohsd", "-dir", "hkm", "-tol", "1e-7"] + AS_GIVEN}
 
 ROW = re.compile(r"^\s*(\d+)\s+([+-]\S+)\s+([+-]\S+)\s+(\S+)\s+(\S+)\s+(\S+)\s+(\S+)\s+(\S+)\s+(\S+)\s+(\S+)\s+(\S+)\s*$")
