@@ -59,24 +59,31 @@ __device__ __forceinline__ int chol_inv16(T (&a)[DB], T (&x)[DB], int lane, int 
     for (int j = 0; j < DB; j++)
         if (lane == j) diag = a[j];
     const T rd = (T)1 / diag;
+    // X = L^-1 row by row: row k is final once the rows above have been subtracted (acc), so step
+    // k finishes it in lane k and broadcasts it; the 16 shuffles of a step are independent, and
+    // the chain is 16 steps long: X[r][j] = -(sum_{k<r} L[r][k] X[k][j]) / L[r][r], X[r][r] = 1/L[r][r]
+    T acc[DB];
 #pragma unroll
-    for (int j = 0; j < DB; j++) x[j] = (T)0;
+    for (int j = 0; j < DB; j++) acc[j] = (T)0;
 #pragma unroll
-    for (int j = 0; j < DB; j++) {   // column j of X: X[k][j] = -(sum_{i=j}^{k-1} L[k][i] X[i][j]) / L[k][k]
-        T acc = (T)0;
+    for (int k = 0; k < DB; k++) {
+        if (lane == k) {
 #pragma unroll
-        for (int k = 0; k < DB; k++) {
-            if (k < j) continue;
-            if (lane == k) x[j] = (k == j) ? rd : -acc * rd;
-            const T xk = __shfl_sync(0xffffffffu, x[j], k);
-            if (lane > k) acc += a[k] * xk;
+            for (int j = 0; j < DB; j++) x[j] = (j < k) ? -acc[j] * rd : (j == k ? rd : (T)0);
+        }
+        const T lrk = a[k];   // L[r][k] of this lane's row r
+#pragma unroll
+        for (int j = 0; j < DB; j++) {
+            if (j > k) continue;
+            const T xkj = __shfl_sync(0xffffffffu, x[j], k);
+            if (lane > k) acc[j] += lrk * xkj;
         }
     }
     return fail;
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) potrf_diag_kernel(int n, T *A, long long lda, int j0, T *dinv, int *info,
+__global__ void __launch_bounds__(256, 1) potrf_diag_kernel(int n, T *A, long long lda, int j0, T *dinv, int *info,
                                                          double *pmin) {
     extern __shared__ __align__(16) unsigned char dsm_raw[];
     T *S = reinterpret_cast<T *>(dsm_raw);   // S[r + c*LDS]: the block, then L
@@ -206,39 +213,55 @@ __global__ void __launch_bounds__(256) trsm_panel_f32(int rows, int nb, float *A
 }
 
 // C(i, j) -= sum_k A(i, k) A(j, k) for i >= j, i < M, j < N (the lower part of an M x N block whose
-// diagonal starts at its top left, N <= M): 64 x 64 output tiles, K in steps of 64.
+// diagonal starts at its top left, N <= M): 128 x 128 output tiles (tiles wholly above the
+// diagonal return at once), 8 x 8 outputs a thread, K in steps of 16 through shared memory (a
+// quarter of a shared-memory load per FMA).
+constexpr int SY_T = 128, SY_K = 16;
 __global__ void __launch_bounds__(256) syrk_f32(int M, int N, int K, const float *A, long long lda, float *C,
                                                 long long ldc) {
     const int bi = blockIdx.x, bj = blockIdx.y;
     if (bi < bj) return;
-    __shared__ float As[64 * LDS], Bs[64 * LDS];
+    __shared__ __align__(16) float As[SY_K][SY_T + 4], Bs[SY_K][SY_T + 4];
     const int tid = threadIdx.x;
-    const int tr = tid % 16, tc = tid / 16;   // 4 x 4 outputs per thread
-    float acc[4][4] = {};
-    for (int k0 = 0; k0 < K; k0 += 64) {
+    // rows tr*4 .. +3 and 64 + tr*4 .. +3, columns likewise from tc: a quarter-warp's float4 reads
+    // of a shared-memory row are 128 contiguous bytes (no bank conflict)
+    const int tr = tid % 16, tc = tid / 16;
+    float acc[8][8];
+#pragma unroll
+    for (int u = 0; u < 8; u++)
+#pragma unroll
+        for (int v = 0; v < 8; v++) acc[u][v] = 0.f;
+    const long long ri0 = (long long)bi * SY_T, rj0 = (long long)bj * SY_T;
+    for (int k0 = 0; k0 < K; k0 += SY_K) {
         __syncthreads();   // the previous step's tiles are consumed
-        for (int idx = tid; idx < 64 * 64; idx += 256) {
-            const int r = idx % 64, k = idx / 64;
-            As[r + k * LDS] = (bi * 64 + r < M && k0 + k < K) ? A[(bi * 64 + r) + (long long)(k0 + k) * lda] : 0.f;
-            Bs[r + k * LDS] = (bj * 64 + r < N && k0 + k < K) ? A[(bj * 64 + r) + (long long)(k0 + k) * lda] : 0.f;
+        for (int idx = tid; idx < SY_T * SY_K; idx += 256) {
+            const int r = idx % SY_T, k = idx / SY_T;   // rows contiguous in A (column-major)
+            const bool kin = k0 + k < K;
+            As[k][r] = (ri0 + r < M && kin) ? A[(ri0 + r) + (long long)(k0 + k) * lda] : 0.f;
+            Bs[k][r] = (rj0 + r < N && kin) ? A[(rj0 + r) + (long long)(k0 + k) * lda] : 0.f;
         }
         __syncthreads();
-        for (int k = 0; k < 64; k++) {
-            float a[4], b[4];
+#pragma unroll 4
+        for (int k = 0; k < SY_K; k++) {
+            const float4 a0 = *reinterpret_cast<const float4 *>(&As[k][tr * 4]);
+            const float4 a1 = *reinterpret_cast<const float4 *>(&As[k][SY_T / 2 + tr * 4]);
+            const float4 b0 = *reinterpret_cast<const float4 *>(&Bs[k][tc * 4]);
+            const float4 b1 = *reinterpret_cast<const float4 *>(&Bs[k][SY_T / 2 + tc * 4]);
+            const float a[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+            const float b[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
 #pragma unroll
-            for (int u = 0; u < 4; u++) { a[u] = As[tr + 16 * u + k * LDS]; b[u] = Bs[tc + 16 * u + k * LDS]; }
+            for (int u = 0; u < 8; u++)
 #pragma unroll
-            for (int u = 0; u < 4; u++)
-#pragma unroll
-                for (int v = 0; v < 4; v++) acc[u][v] += a[u] * b[v];
+                for (int v = 0; v < 8; v++) acc[u][v] += a[u] * b[v];
         }
     }
 #pragma unroll
-    for (int u = 0; u < 4; u++)
+    for (int u = 0; u < 8; u++)
 #pragma unroll
-        for (int v = 0; v < 4; v++) {
-            const int i = bi * 64 + tr + 16 * u, j = bj * 64 + tc + 16 * v;
-            if (i < M && j < N && i >= j) C[i + (long long)j * ldc] -= acc[u][v];
+        for (int v = 0; v < 8; v++) {
+            const long long i = ri0 + (u < 4 ? tr * 4 + u : SY_T / 2 + tr * 4 + u - 4);
+            const long long j = rj0 + (v < 4 ? tc * 4 + v : SY_T / 2 + tc * 4 + v - 4);
+            if (i < M && j < N && i >= j) C[i + j * ldc] -= acc[u][v];
         }
 }
 
@@ -546,7 +569,7 @@ int potrf_f32(cudaStream_t st, int n, float *A, long long lda, float *dinv, int 
             BGPU_LAUNCH_CHECK();
             const int pc = J0 + JB - (j0 + nb);
             if (pc > 0) {
-                syrk_f32<<<dim3(ceil_div(rest, 64), ceil_div(pc, 64)), 256, 0, st>>>(
+                syrk_f32<<<dim3(ceil_div(rest, SY_T), ceil_div(pc, SY_T)), 256, 0, st>>>(
                     rest, pc, nb, A21, lda, A + (j0 + nb) + (long long)(j0 + nb) * lda, lda);
                 BGPU_LAUNCH_CHECK();
             }
@@ -554,7 +577,7 @@ int potrf_f32(cudaStream_t st, int n, float *A, long long lda, float *dinv, int 
         const int rest = n - J0 - JB;
         if (rest <= 0) break;
         const float *P = A + (J0 + JB) + (long long)J0 * lda;
-        const int t = ceil_div(rest, 64);
+        const int t = ceil_div(rest, SY_T);
         syrk_f32<<<dim3(t, t), 256, 0, st>>>(rest, rest, JB, P, lda, A + (J0 + JB) + (long long)(J0 + JB) * lda, lda);
         BGPU_LAUNCH_CHECK();
     }
