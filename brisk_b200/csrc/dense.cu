@@ -508,80 +508,178 @@ int diag_smem_attr() {
     return BGPU_OK;
 }
 
-// The blocked factor in outer panels of PANEL columns: within a panel, each 64-column block is
+// The blocked factor in outer panels of PANEL columns.  Within a panel, each 64-column block is
 // factored (potrf_diag_kernel), the whole column below it solved against its inverse, and the
-// panel's later columns updated (rank 64); the columns right of the panel then take one rank-PANEL
-// update, which reads and writes the trailing triangle once per panel (not once per 64 columns)
-// and gives the tensor-core GEMM a depth of PANEL.
+// panel's later columns updated (rank 64).  The columns right of the panel then take one
+// rank-PANEL update, which reads and writes the trailing triangle once per panel (not once per 64
+// columns) and gives the tensor-core GEMM a depth of PANEL.
 constexpr int PANEL = 256;
 
-int potrf_f64(cudaStream_t st, int n, double *A, long long lda, double *dinv, int *d_info, double *d_pmin) {
-    if (int rc = diag_smem_attr<double>()) return rc;
-    init_info_kernel<<<1, 1, 0, st>>>(d_info, d_pmin);
-    BGPU_LAUNCH_CHECK();
-    for (int J0 = 0; J0 < n; J0 += PANEL) {
-        const int JB = std::min(PANEL, n - J0);
-        for (int j0 = J0; j0 < J0 + JB; j0 += NB) {
-            const int nb = std::min(NB, n - j0);
-            const double *Di = dinv + (size_t)(j0 / NB) * NB * NB;
-            potrf_diag_kernel<double><<<1, 256, 2 * NB * LDS * sizeof(double), st>>>(n, A, lda, j0, (double *)Di, d_info, d_pmin);
-            BGPU_LAUNCH_CHECK();
-            const int rest = n - j0 - nb;
-            if (rest <= 0) break;
-            double *A21 = A + (j0 + nb) + (long long)j0 * lda;
-            // A21 <- A21 Di'  (B(k, j) = Di(j, k) = Di[j + k*NB]: N-major); in place, N = nb <= 64
-            int rc = gemm_f64(st, 0, 0, rest, nb, nb, 1.0, A21, lda, 0, Di, NB, 0, 0.0, A21, lda, 0, 1, 0);
-            if (rc) return rc;
-            // the panel's later columns: A[j0+nb.., j0+nb .. J0+JB) -= A21 A21(top pc rows)', lower
-            const int pc = J0 + JB - (j0 + nb);
-            if (pc > 0) {
-                rc = gemm_f64(st, 0, 0, rest, pc, nb, -1.0, A21, lda, 0, A21, lda, 0, 1.0,
-                              A + (j0 + nb) + (long long)(j0 + nb) * lda, lda, 0, 1, 1);
-                if (rc) return rc;
-            }
-        }
-        const int rest = n - J0 - JB;
+namespace {
+// factor the panel of columns [J0, J0 + JB) (all its updates from earlier panels applied)
+template <typename T>
+int factor_panel(cudaStream_t st, int n, T *A, long long lda, T *dinv, int J0, int JB, int *d_info, double *d_pmin);
+
+template <>
+int factor_panel<double>(cudaStream_t st, int n, double *A, long long lda, double *dinv, int J0, int JB, int *d_info,
+                         double *d_pmin) {
+    for (int j0 = J0; j0 < J0 + JB; j0 += NB) {
+        const int nb = std::min(NB, n - j0);
+        double *Di = dinv + (size_t)(j0 / NB) * NB * NB;
+        potrf_diag_kernel<double><<<1, 256, 2 * NB * LDS * sizeof(double), st>>>(n, A, lda, j0, Di, d_info, d_pmin);
+        BGPU_LAUNCH_CHECK();
+        const int rest = n - j0 - nb;
         if (rest <= 0) break;
-        // A22 <- A22 - P P' (lower), P the rows below the panel (rest x JB)
-        const double *P = A + (J0 + JB) + (long long)J0 * lda;
-        double *A22 = A + (J0 + JB) + (long long)(J0 + JB) * lda;
-        int rc = gemm_f64(st, 0, 0, rest, rest, JB, -1.0, P, lda, 0, P, lda, 0, 1.0, A22, lda, 0, 1, 1);
+        double *A21 = A + (j0 + nb) + (long long)j0 * lda;
+        // A21 <- A21 Di'  (B(k, j) = Di(j, k) = Di[j + k*NB]: N-major); in place, N = nb <= 64
+        int rc = gemm_f64(st, 0, 0, rest, nb, nb, 1.0, A21, lda, 0, Di, NB, 0, 0.0, A21, lda, 0, 1, 0);
         if (rc) return rc;
+        // the panel's later columns: A[j0+nb.., j0+nb .. J0+JB) -= A21 A21(top pc rows)', lower
+        const int pc = J0 + JB - (j0 + nb);
+        if (pc > 0) {
+            rc = gemm_f64(st, 0, 0, rest, pc, nb, -1.0, A21, lda, 0, A21, lda, 0, 1.0,
+                          A + (j0 + nb) + (long long)(j0 + nb) * lda, lda, 0, 1, 1);
+            if (rc) return rc;
+        }
     }
     return BGPU_OK;
 }
 
-int potrf_f32(cudaStream_t st, int n, float *A, long long lda, float *dinv, int *d_info, double *d_pmin) {
-    if (int rc = diag_smem_attr<float>()) return rc;
-    init_info_kernel<<<1, 1, 0, st>>>(d_info, d_pmin);
-    BGPU_LAUNCH_CHECK();
-    for (int J0 = 0; J0 < n; J0 += PANEL) {
-        const int JB = std::min(PANEL, n - J0);
-        for (int j0 = J0; j0 < J0 + JB; j0 += NB) {
-            const int nb = std::min(NB, n - j0);
-            float *Di = dinv + (size_t)(j0 / NB) * NB * NB;
-            potrf_diag_kernel<float><<<1, 256, 2 * NB * LDS * sizeof(float), st>>>(n, A, lda, j0, Di, d_info, d_pmin);
-            BGPU_LAUNCH_CHECK();
-            const int rest = n - j0 - nb;
-            if (rest <= 0) break;
-            float *A21 = A + (j0 + nb) + (long long)j0 * lda;
-            trsm_panel_f32<<<ceil_div(rest, 64), 256, 0, st>>>(rest, nb, A21, lda, Di);
-            BGPU_LAUNCH_CHECK();
-            const int pc = J0 + JB - (j0 + nb);
-            if (pc > 0) {
-                syrk_f32<<<dim3(ceil_div(rest, SY_T), ceil_div(pc, SY_T)), 256, 0, st>>>(
-                    rest, pc, nb, A21, lda, A + (j0 + nb) + (long long)(j0 + nb) * lda, lda);
-                BGPU_LAUNCH_CHECK();
-            }
-        }
-        const int rest = n - J0 - JB;
-        if (rest <= 0) break;
-        const float *P = A + (J0 + JB) + (long long)J0 * lda;
-        const int t = ceil_div(rest, SY_T);
-        syrk_f32<<<dim3(t, t), 256, 0, st>>>(rest, rest, JB, P, lda, A + (J0 + JB) + (long long)(J0 + JB) * lda, lda);
+template <>
+int factor_panel<float>(cudaStream_t st, int n, float *A, long long lda, float *dinv, int J0, int JB, int *d_info,
+                        double *d_pmin) {
+    for (int j0 = J0; j0 < J0 + JB; j0 += NB) {
+        const int nb = std::min(NB, n - j0);
+        float *Di = dinv + (size_t)(j0 / NB) * NB * NB;
+        potrf_diag_kernel<float><<<1, 256, 2 * NB * LDS * sizeof(float), st>>>(n, A, lda, j0, Di, d_info, d_pmin);
         BGPU_LAUNCH_CHECK();
+        const int rest = n - j0 - nb;
+        if (rest <= 0) break;
+        float *A21 = A + (j0 + nb) + (long long)j0 * lda;
+        trsm_panel_f32<<<ceil_div(rest, 64), 256, 0, st>>>(rest, nb, A21, lda, Di);
+        BGPU_LAUNCH_CHECK();
+        const int pc = J0 + JB - (j0 + nb);
+        if (pc > 0) {
+            syrk_f32<<<dim3(ceil_div(rest, SY_T), ceil_div(pc, SY_T)), 256, 0, st>>>(
+                rest, pc, nb, A21, lda, A + (j0 + nb) + (long long)(j0 + nb) * lda, lda);
+            BGPU_LAUNCH_CHECK();
+        }
     }
     return BGPU_OK;
+}
+
+// A[C0.., C0 .. C0 + cols) -= P P' (lower part), P = A[C0.., P0 .. P0 + PB): the update of the
+// columns from C0 on by the factored panel at P0
+template <typename T>
+int update_lower(cudaStream_t st, int n, T *A, long long lda, int C0, int cols, int P0, int PB);
+
+template <>
+int update_lower<double>(cudaStream_t st, int n, double *A, long long lda, int C0, int cols, int P0, int PB) {
+    const double *P = A + C0 + (long long)P0 * lda;
+    return gemm_f64(st, 0, 0, n - C0, cols, PB, -1.0, P, lda, 0, P, lda, 0, 1.0, A + C0 + (long long)C0 * lda, lda,
+                    0, 1, 1);
+}
+
+template <>
+int update_lower<float>(cudaStream_t st, int n, float *A, long long lda, int C0, int cols, int P0, int PB) {
+    const float *P = A + C0 + (long long)P0 * lda;
+    syrk_f32<<<dim3(ceil_div(n - C0, SY_T), ceil_div(cols, SY_T)), 256, 0, st>>>(n - C0, cols, PB, P, lda,
+                                                                                 A + C0 + (long long)C0 * lda, lda);
+    BGPU_LAUNCH_CHECK();
+    return BGPU_OK;
+}
+
+// Two streams of this host thread on this device for the look-ahead factor: `crit` (the highest
+// priority: its CTAs go ahead of the waiting CTAs of the trailing update as SMs free up) and
+// `bulk`, with the events that order them.  Created once per thread and device, kept for the
+// life of the thread.
+struct FactorStreams {
+    cudaStream_t crit = nullptr, bulk = nullptr;
+    cudaEvent_t fork = nullptr, panel = nullptr, trail = nullptr, done = nullptr;
+    ~FactorStreams() {
+        for (cudaEvent_t e : {fork, panel, trail, done})
+            if (e) cudaEventDestroy(e);
+        if (crit) cudaStreamDestroy(crit);
+        if (bulk) cudaStreamDestroy(bulk);
+    }
+};
+
+int factor_streams(FactorStreams **out) {
+    int dev = 0;
+    BGPU_CHECK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return BGPU_ERR_ARG;
+    thread_local FactorStreams fs[64];
+    FactorStreams &f = fs[dev];
+    if (!f.crit) {
+        int lo = 0, hi = 0;
+        BGPU_CHECK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+        BGPU_CHECK(cudaStreamCreateWithPriority(&f.crit, cudaStreamNonBlocking, hi));
+        BGPU_CHECK(cudaStreamCreateWithPriority(&f.bulk, cudaStreamNonBlocking, lo));
+        for (cudaEvent_t *e : {&f.fork, &f.panel, &f.trail, &f.done})
+            BGPU_CHECK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    }
+    *out = &f;
+    return BGPU_OK;
+}
+
+// The factor with a look-ahead of one panel.  On `crit`: factor panel k, update panel k+1's
+// columns by it (U_next), factor panel k+1, ...; on `bulk`: update the columns from panel k+2 on
+// by panel k (U_rest, the big rank-PANEL GEMM), while `crit` factors panel k+1.  Order: U_rest(k)
+// waits for panel k's factor; U_next(k+1) writes panel k+2's columns, as U_rest(k) does, so it
+// waits for U_rest(k).  The chain of diagonal-block factors then runs under the trailing updates
+// instead of between them.  Small orders (three panels or fewer) run the plain order on `st`.
+template <typename T>
+int potrf_blocked(cudaStream_t st, int n, T *A, long long lda, T *dinv, int *d_info, double *d_pmin) {
+    if (int rc = diag_smem_attr<T>()) return rc;
+    init_info_kernel<<<1, 1, 0, st>>>(d_info, d_pmin);
+    BGPU_LAUNCH_CHECK();
+    const int np = ceil_div(n, PANEL);
+    if (np <= 3) {
+        for (int J0 = 0; J0 < n; J0 += PANEL) {
+            const int JB = std::min(PANEL, n - J0);
+            if (int rc = factor_panel<T>(st, n, A, lda, dinv, J0, JB, d_info, d_pmin)) return rc;
+            if (J0 + JB < n)
+                if (int rc = update_lower<T>(st, n, A, lda, J0 + JB, n - J0 - JB, J0, JB)) return rc;
+        }
+        return BGPU_OK;
+    }
+    FactorStreams *f = nullptr;
+    if (int rc = factor_streams(&f)) return rc;
+    BGPU_CHECK(cudaEventRecord(f->fork, st));
+    BGPU_CHECK(cudaStreamWaitEvent(f->crit, f->fork, 0));
+    BGPU_CHECK(cudaStreamWaitEvent(f->bulk, f->fork, 0));
+    int rc = factor_panel<T>(f->crit, n, A, lda, dinv, 0, std::min(PANEL, n), d_info, d_pmin);
+    for (int k = 0; rc == 0 && k + 1 < np; k++) {
+        const int J0 = k * PANEL, JB = PANEL;            // panel k (not the last: full width)
+        const int J1 = J0 + JB, JB1 = std::min(PANEL, n - J1);
+        const int J2 = J1 + JB1;
+        BGPU_CHECK(cudaEventRecord(f->panel, f->crit));
+        if (J2 < n) {   // U_rest(k) on bulk, after panel k's factor
+            BGPU_CHECK(cudaStreamWaitEvent(f->bulk, f->panel, 0));
+            if ((rc = update_lower<T>(f->bulk, n, A, lda, J2, n - J2, J0, JB))) break;
+            BGPU_CHECK(cudaEventRecord(f->trail, f->bulk));
+        }
+        // U_next(k) (panel k+1's columns by panel k), then panel k+1's factor, on crit.  Panel
+        // k+1's columns took U_rest(k-1) before: crit waited for it ahead of U_next(k) below.
+        if ((rc = update_lower<T>(f->crit, n, A, lda, J1, JB1, J0, JB))) break;
+        if ((rc = factor_panel<T>(f->crit, n, A, lda, dinv, J1, JB1, d_info, d_pmin))) break;
+        if (J2 < n) BGPU_CHECK(cudaStreamWaitEvent(f->crit, f->trail, 0));   // before U_next(k+1)
+    }
+    // join (also on an error: nothing is left running ahead of st)
+    BGPU_CHECK(cudaEventRecord(f->done, f->bulk));
+    BGPU_CHECK(cudaStreamWaitEvent(st, f->done, 0));
+    BGPU_CHECK(cudaEventRecord(f->done, f->crit));
+    BGPU_CHECK(cudaStreamWaitEvent(st, f->done, 0));
+    return rc;
+}
+}  // namespace
+
+int potrf_f64(cudaStream_t st, int n, double *A, long long lda, double *dinv, int *d_info, double *d_pmin) {
+    return potrf_blocked<double>(st, n, A, lda, dinv, d_info, d_pmin);
+}
+
+int potrf_f32(cudaStream_t st, int n, float *A, long long lda, float *dinv, int *d_info, double *d_pmin) {
+    return potrf_blocked<float>(st, n, A, lda, dinv, d_info, d_pmin);
 }
 
 int trsv_f64(cudaStream_t st, int n, const double *L, long long lda, const double *dinv, double *x, int trans,

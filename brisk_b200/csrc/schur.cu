@@ -25,33 +25,35 @@ constexpr int TP_Q = 128, TP_K = 32, TP_LD = TP_K + 1;   // CTA tile: 128 rows q
 // Zi[q + p' n]).  Warp w owns columns k0 + w, k0 + w + 8, ...; a lane owns rows q0 + lane + 32 u.
 // The column's entries come from the per-constraint column pointers ccol, so no entry is read
 // by a warp that does not use it and the sums stay in registers in a fixed order.
-// ZT: the type Zi is read in.  The 3xTF32 form reads an FP32 copy of Zi: half the L2 traffic of
-// this L2-bound kernel (each entry reads a 128-value segment of a Zi column), and T keeps the
-// accuracy its tf32 hi + lo split can carry (2^-24 relative per term against 2^-22).
+// ZT: the type Zi is read in, and the type of the sums.  The 3xTF32 form reads an FP32 copy of
+// Zi and sums in FP32: half the L2 traffic of this L2-bound kernel (each entry reads a 128-value
+// segment of a Zi column), no conversions, half the tile, and T keeps the accuracy its tf32
+// hi + lo split can carry (2^-24 relative per term against the split's 2^-22).
 template <typename OutT, typename ZT = double>
 __global__ void __launch_bounds__(256) tprod_kernel(int n, int ldt, int K, int a0, int ncon,
                                                    const long long *__restrict__ cptr, const int *__restrict__ ccol,
                                                    const int *__restrict__ cpos, const double *__restrict__ cval,
                                                    const ZT *__restrict__ Zi, OutT *__restrict__ T,
                                                    OutT *__restrict__ Tlo) {
-    __shared__ double tile[TP_Q * TP_LD];
+    using AccT = ZT;
+    __shared__ AccT tile[TP_Q * TP_LD];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int q0 = blockIdx.x * TP_Q, k0 = blockIdx.y * TP_K, t = blockIdx.z;
     const int a = a0 + t;
     for (int kk = warp; kk < TP_K; kk += 8) {
         const int k = k0 + kk;
-        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        AccT acc[4] = {(AccT)0, (AccT)0, (AccT)0, (AccT)0};
         if (a < ncon && k < n) {
             const long long base = cptr[a];
             const int *cc = ccol + (long long)a * (n + 1);
             const long long e0 = base + cc[k], e1 = base + cc[k + 1];
             for (long long e = e0; e < e1; e++) {
                 const int pp = cpos[e] - k * n;   // the row p' of the entry (p', k)
-                const double v = cval[e];
+                const AccT v = (AccT)cval[e];
                 const ZT *z = Zi + (long long)pp * n + q0 + lane;
 #pragma unroll
                 for (int u = 0; u < 4; u++)
-                    if (q0 + lane + 32 * u < n) acc[u] += v * (double)z[32 * u];
+                    if (q0 + lane + 32 * u < n) acc[u] += v * z[32 * u];
             }
         }
 #pragma unroll
@@ -63,14 +65,14 @@ __global__ void __launch_bounds__(256) tprod_kernel(int n, int ldt, int K, int a
     for (int r = warp; r < TP_Q; r += 8) {
         const int q = q0 + r;
         if (q >= n || lane >= kw) continue;
-        const double v = tile[r * TP_LD + lane];
+        const AccT v = tile[r * TP_LD + lane];
         const long long o = ((long long)q * K + t) * ldt + k0 + lane;
         if (sizeof(OutT) == 8) {
             T[o] = (OutT)v;
         } else {
             const float hi_ = tf32_round((float)v);
             T[o] = (OutT)hi_;
-            Tlo[o] = (OutT)tf32_round((float)(v - (double)hi_));
+            Tlo[o] = (OutT)tf32_round((float)((double)v - (double)hi_));
         }
     }
 }
