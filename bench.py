@@ -525,6 +525,11 @@ def load_peaks():
         return 1590.0, 6650.0, "fallback"
 
 
+# DRAM bytes (read + write) of one launch of the n = 1000, K = 64 chunk GEMM, from
+# `ncu --set full` (profiles/tf32x3_kernel_rand1000_chunk.md): 536.1 MB + 227.5 MB
+TF32X3_TRAFFIC = 763.58e6
+
+
 def tf32x3_roofline(torch, step, n, chunk, launches=10):
     """The dominant kernel of the mixed path (the 3xTF32 row-product GEMM of the Schur assembly,
     (n K) x n x n per launch, three tf32 MMAs per product on tcgen05) timed alone with CUDA events
@@ -554,7 +559,10 @@ def tf32x3_roofline(torch, step, n, chunk, launches=10):
     ach = flops / t / 1e12
     return {"bound": "tensor", "kernel": "tf32x3_kernel (3xTF32, tcgen05.mma kind::tf32, TMEM accumulator)",
             "achieved": round(ach, 2), "peak": round(peak, 2), "unit": "TFLOP/s", "frac": round(ach / peak, 4),
-            "traffic": None, "flops_per_launch": flops, "launch_ms": round(t * 1e3, 4),
+            "traffic": TF32X3_TRAFFIC if (n, chunk) == (1000, 64) else None,
+            "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of this launch "
+                              "(profiles/tf32x3_kernel_rand1000_chunk.md); algorithmic bytes 7.76e8",
+            "flops_per_launch": flops, "launch_ms": round(t * 1e3, 4),
             "peak_source": f"{src} bf16 {bf16:.1f} TF/s (burst) / 2 for TF32 / 3 MMAs per useful product "
                            f"({'of measured' if src == 'measured' else 'of fallback'})"}
 
@@ -727,6 +735,61 @@ def run_ours(args):
         torch.distributed.destroy_process_group()
 
 
+PROFILE_CASES = ("tf32x3", "ozaki5", "potrf_f64", "potrf_f32")
+
+
+def profile_case(name, launches=3):
+    """A few launches of one kernel on its rand1000 shape, for ncu captures (no timing printed):
+    tf32x3 / ozaki5 the chunk GEMM of the Schur assembly ((n K) x n x n, n = 1000, K = 64: 1.3 GB
+    on the device at most), potrf_f64 / potrf_f32 the factor of an m = 8000 SPD matrix (the Schur
+    complement's order)."""
+    import torch
+    from brisk_b200 import step
+    torch.cuda.set_device(0)
+    cuda = torch.device("cuda:0")
+    sp = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    torch.manual_seed(0)
+    if name in ("tf32x3", "ozaki5"):
+        n, K = 1000, 64
+        M = n * K
+        if name == "tf32x3":
+            ld = (n + 3) // 4 * 4
+            f32 = torch.float32
+            Ah, Al = torch.randn(M * ld, dtype=f32, device=cuda), torch.randn(M * ld, dtype=f32, device=cuda) * 1e-4
+            Bh, Bl = torch.randn(n * ld, dtype=f32, device=cuda), torch.randn(n * ld, dtype=f32, device=cuda) * 1e-4
+            G = torch.empty(M * n, dtype=f32, device=cuda)
+            for _ in range(launches):
+                step.call("gemm_tf32x3", M, n, n, Ah.data_ptr(), Al.data_ptr(), ld, Bh.data_ptr(), Bl.data_ptr(), ld,
+                          G.data_ptr(), M, sp)
+        else:
+            T = torch.randn(M * n, dtype=torch.float64, device=cuda)
+            X = torch.randn(n * n, dtype=torch.float64, device=cuda)
+            G = torch.empty(M * n, dtype=torch.float64, device=cuda)
+            nws = int(step.lib().bgpu_ozaki_ws_bytes(M, n, n))
+            ws = torch.empty(nws, dtype=torch.uint8, device=cuda)
+            for _ in range(launches):
+                step.call("gemm_ozaki_slices", 5, M, n, n, T.data_ptr(), n, X.data_ptr(), n, G.data_ptr(), M,
+                          ws.data_ptr(), nws, sp)
+    else:
+        m = 8000
+        dt = torch.float64 if name == "potrf_f64" else torch.float32
+        R = torch.randn(m, m, dtype=torch.float64, device=cuda)
+        A = (R @ R.T / m + torch.eye(m, dtype=torch.float64, device=cuda)).to(dt)
+        L = torch.empty_like(A)
+        nb = (m + 63) // 64
+        dinv = torch.zeros(nb * 4096, dtype=dt, device=cuda)
+        info = torch.zeros(1, dtype=torch.int32, device=cuda)
+        pmin = torch.zeros(1, dtype=torch.float64, device=cuda)
+        for _ in range(launches):
+            L.copy_(A)
+            step.call(name.replace("_f64", ""), m, L.data_ptr(), m, dinv.data_ptr(), info.data_ptr(),
+                      pmin.data_ptr(), sp)
+        torch.cuda.synchronize()
+        if int(info.item()) != 0:
+            raise SystemExit(f"{name}: factor failed at column {int(info.item())}")
+    torch.cuda.synchronize()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -737,7 +800,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-count", type=int, default=4096, help="instances of the batch workload")
     ap.add_argument("--batch-sample", type=int, default=64, help="instances the reference solves for its sample")
+    ap.add_argument("--profile-case", choices=PROFILE_CASES,
+                    help="run three launches of one kernel on its rand1000 shape and exit (for ncu captures)")
     args = ap.parse_args()
+    if args.profile_case:
+        profile_case(args.profile_case)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:
