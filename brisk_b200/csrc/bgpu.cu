@@ -365,8 +365,8 @@ BGPU_API int bgpu_schol_supernodes(const bgpu_schol *h, int *sfirst, int *parent
     return BGPU_OK;
 }
 
-BGPU_API int bgpu_schol_factor(bgpu_schol *h, const double *d_M, int64_t ldm, const double *d_D, double reg,
-                               int *info, double *pmin, void *stream) {
+static int schol_factor_any(bgpu_schol *h, const double *d_M, int64_t ldm, const double *d_D, double reg, int *info,
+                            double *pmin, void *stream, bool fp32) {
     if (!h || !d_M || !d_D || ldm < h->A.m) return BGPU_ERR_ARG;
     if (!h->bound) {
         const size_t b = schol::factor_bytes(h->A);
@@ -375,7 +375,7 @@ BGPU_API int bgpu_schol_factor(bgpu_schol *h, const double *d_M, int64_t ldm, co
         if (rc) return rc;
         h->bound = true;
     }
-    int rc = schol::factor(S(stream), h->F, d_M, ldm, d_D, reg);
+    int rc = schol::factor(S(stream), h->F, d_M, ldm, d_D, reg, fp32);
     if (rc) return rc;
     if (info || pmin) {
         int i = 0;
@@ -387,6 +387,16 @@ BGPU_API int bgpu_schol_factor(bgpu_schol *h, const double *d_M, int64_t ldm, co
         if (pmin) *pmin = p;
     }
     return BGPU_OK;
+}
+
+BGPU_API int bgpu_schol_factor(bgpu_schol *h, const double *d_M, int64_t ldm, const double *d_D, double reg,
+                               int *info, double *pmin, void *stream) {
+    return schol_factor_any(h, d_M, ldm, d_D, reg, info, pmin, stream, false);
+}
+
+BGPU_API int bgpu_schol_factor_f32(bgpu_schol *h, const double *d_M, int64_t ldm, const double *d_D, double reg,
+                                   int *info, double *pmin, void *stream) {
+    return schol_factor_any(h, d_M, ldm, d_D, reg, info, pmin, stream, true);
 }
 
 BGPU_API int bgpu_schol_solve(bgpu_schol *h, const double *d_D, double *d_x, void *stream) {

@@ -433,6 +433,27 @@ __global__ void symv_full_kernel(int n, double alpha, const double *M, long long
     if (lane == 0) y[col] = (beta == 0.0) ? alpha * s : alpha * s + beta * y[col];
 }
 
+// y = M x over a known pattern: row a holds the columns cols[rowptr[a] .. rowptr[a+1]) (ascending),
+// read from column a of the symmetric dense M (contiguous in memory); one warp a row, lanes
+// strided over the row's entries and summed by a fixed reduction.  Entries off the pattern are
+// zero in M, so this is M x with a fraction of the reads.
+__global__ void pattern_symv_kernel(int n, const long long *__restrict__ rowptr, const int *__restrict__ cols,
+                                    const double *__restrict__ M, long long ldm, const double *__restrict__ x,
+                                    double *y) {
+    const int warps = blockDim.x >> 5;
+    const int a = blockIdx.x * warps + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (a >= n) return;
+    const double *c = M + (long long)a * ldm;
+    double s = 0.0;
+    for (long long t = rowptr[a] + lane; t < rowptr[a + 1]; t += 32) {
+        const int b = cols[t];
+        s += c[b] * x[b];
+    }
+    s = warp_sum(s);
+    if (lane == 0) y[a] = s;
+}
+
 __global__ void diag_scale_kernel(int m, const double *M, long long ldm, double *D) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m) return;
@@ -717,6 +738,14 @@ int trtri_f64(cudaStream_t st, int n, const double *L, long long lda, const doub
 int symv_full_f64(cudaStream_t st, int n, double alpha, const double *M, long long ldm, const double *x, double beta,
                   double *y) {
     symv_full_kernel<<<ceil_div(n, 8), 256, 0, st>>>(n, alpha, M, ldm, x, beta, y);
+    BGPU_LAUNCH_CHECK();
+    return BGPU_OK;
+}
+
+int pattern_symv_f64(cudaStream_t st, int n, const long long *rowptr, const int *cols, const double *M, long long ldm,
+                     const double *x, double *y) {
+    if (n <= 0) return BGPU_OK;
+    pattern_symv_kernel<<<ceil_div(n, 8), 256, 0, st>>>(n, rowptr, cols, M, ldm, x, y);
     BGPU_LAUNCH_CHECK();
     return BGPU_OK;
 }

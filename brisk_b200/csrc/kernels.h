@@ -69,6 +69,10 @@ int trtri_f64(cudaStream_t st, int n, const double *L, long long lda, const doub
 // y = alpha M x + beta y, M symmetric and stored in full (column-major, ldm).
 int symv_full_f64(cudaStream_t st, int n, double alpha, const double *M, long long ldm, const double *x, double beta,
                   double *y);
+// y = M x reading only the pattern's entries (rowptr/cols: each row's columns, both triangles and
+// the diagonal, ascending; entries of M off the pattern must be zero)
+int pattern_symv_f64(cudaStream_t st, int n, const long long *rowptr, const int *cols, const double *M, long long ldm,
+                     const double *x, double *y);
 
 // Equilibrated copy for the factor: L = D M D + reg I (lower triangle; D = diag(M)^{-1/2},
 // computed here into d_D), and the float variant writing Mf.
@@ -139,10 +143,11 @@ int schur_assemble_dense(cudaStream_t st, const DevBlock &B, const double *X, co
 // Many small blocks (n <= SB_NMAX) at once: M += each listed block's contribution (FP64), one CTA
 // per block.  The listed blocks must share no constraint.  Per-block data by block id: order d_n,
 // constraint count d_ncon, and device pointer tables of con / cptr / cpos / cval (the full
-// expansion); X and Zi are the concatenations (block k at d_boff[k]); nmax = the largest listed n.
+// expansion); X and Zi are the concatenations (block k at d_boff[k]); nmax = the largest listed n,
+// ncon_max = the largest listed constraint count (it sets how many CTAs share a block).
 constexpr int SB_NMAX = 32;
 size_t schur_small_smem(int nmax);
-int schur_assemble_small(cudaStream_t st, int count, const int *d_blocks, int nmax, const int *d_n,
+int schur_assemble_small(cudaStream_t st, int count, const int *d_blocks, int nmax, int ncon_max, const int *d_n,
                          const int *d_ncon, const int *const *con_tab, const long long *const *cptr_tab,
                          const int *const *cpos_tab, const double *const *cval_tab, const long long *d_boff,
                          const double *Xcat, const double *Zicat, double *M, int m);

@@ -682,11 +682,12 @@ int schur_assemble_gram(cudaStream_t st, const DevBlock &B, double *M, int m, vo
 }
 
 // ---- many small blocks at once ----------------------------------------------------------------
-// One CTA per block (n <= SB_NMAX), one warp per constraint a of the block: W = A_a Zi row by row
-// from a's entries (W[p, :] += v Zi[q, :]), G = X W over the rows A_a touches, then
-// M[a, b] = <A_b, G> for the block's b >= a, a warp sum per b.  The blocks of one launch share no
-// constraint (the caller colours them), so every M entry has one writer per launch and the
-// launches add in a fixed order.
+// gridDim.y CTAs per block (n <= SB_NMAX), one warp per constraint a of the block (the block's
+// constraints dealt round-robin to the CTAs' warps): W = A_a Zi row by row from a's entries
+// (W[p, :] += v Zi[q, :]), G = X W over the rows A_a touches, then M[a, b] = <A_b, G> for the
+// block's b >= a, a warp sum per b.  The blocks of one launch share no constraint (the caller
+// colours them), so every M entry has one writer per launch and the launches add in a fixed
+// order; how many CTAs share a block changes no sum.
 namespace {
 constexpr int SB_W = 8;   // warps per CTA
 __global__ void __launch_bounds__(SB_W * 32) small_schur_kernel(
@@ -698,6 +699,7 @@ __global__ void __launch_bounds__(SB_W * 32) small_schur_kernel(
     extern __shared__ __align__(16) double sb_sm[];
     const int k = blocks[blockIdx.x];
     const int n = bn[k], ncon = bncon[k], nn = n * n;
+    if ((int)blockIdx.y * SB_W >= ncon) return;   // no constraint of this block for this CTA
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     double *Xs = sb_sm, *Zs = sb_sm + nn;
     double *W = sb_sm + 2 * nn + (size_t)warp * 2 * nn, *G = W + nn;
@@ -708,7 +710,7 @@ __global__ void __launch_bounds__(SB_W * 32) small_schur_kernel(
     const long long *cptr = cptr_tab[k];
     const int *cpos = cpos_tab[k];
     const double *cval = cval_tab[k];
-    for (int a = warp; a < ncon; a += SB_W) {
+    for (int a = (int)blockIdx.y * SB_W + warp; a < ncon; a += SB_W * (int)gridDim.y) {
         for (int i = lane; i < nn; i += 32) W[i] = 0.0;
         __syncwarp();
         unsigned long long rows = 0;
@@ -747,7 +749,7 @@ __global__ void __launch_bounds__(SB_W * 32) small_schur_kernel(
 
 size_t schur_small_smem(int nmax) { return (size_t)(2 + 2 * SB_W) * nmax * nmax * sizeof(double); }
 
-int schur_assemble_small(cudaStream_t st, int count, const int *d_blocks, int nmax, const int *d_n,
+int schur_assemble_small(cudaStream_t st, int count, const int *d_blocks, int nmax, int ncon_max, const int *d_n,
                          const int *d_ncon, const int *const *con_tab, const long long *const *cptr_tab,
                          const int *const *cpos_tab, const double *const *cval_tab, const long long *d_boff,
                          const double *Xcat, const double *Zicat, double *M, int m) {
@@ -755,8 +757,13 @@ int schur_assemble_small(cudaStream_t st, int count, const int *d_blocks, int nm
     if (nmax <= 0 || nmax > SB_NMAX) return BGPU_ERR_ARG;
     BGPU_ATTR_ONCE(BGPU_CHECK(cudaFuncSetAttribute(small_schur_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                    (int)schur_small_smem(SB_NMAX))));
-    small_schur_kernel<<<count, SB_W * 32, schur_small_smem(nmax), st>>>(d_blocks, d_n, d_ncon, con_tab, cptr_tab,
-                                                                         cpos_tab, cval_tab, d_boff, Xcat, Zicat, M, m);
+    // enough CTAs per block that the launch fills the SMs twice over, one warp per constraint at most
+    int dev = 0, nsm = 0;
+    BGPU_CHECK(cudaGetDevice(&dev));
+    BGPU_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    const int per_block = std::max(1, std::min(ceil_div(std::max(ncon_max, 1), SB_W), ceil_div(2 * nsm, count)));
+    small_schur_kernel<<<dim3(count, per_block), SB_W * 32, schur_small_smem(nmax), st>>>(
+        d_blocks, d_n, d_ncon, con_tab, cptr_tab, cpos_tab, cval_tab, d_boff, Xcat, Zicat, M, m);
     BGPU_LAUNCH_CHECK();
     return BGPU_OK;
 }

@@ -870,6 +870,7 @@ class Solver {
     int run(ResultData &res);     // one solve from the resident data
     void set_options(const Options &o) { opt = o; }
     ~Solver() {
+        schol::release(sp_f);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (evs0) cudaEventDestroy(evs0);
@@ -932,6 +933,12 @@ class Solver {
     int epoch = 0;
     // factor state (Schur in solver.c:4511-4568)
     bool allow_float = false, want_double = false, is_float = false, reg_hint = false;
+    // the sparse factor in FP32 while mu >= mu_switch (-mixed as for the dense factor)
+    bool sparse_float = false;
+    // the pattern of the sparse M (both triangles and the diagonal, rows ascending): the FP64
+    // residual product reads only these entries of the dense copy
+    long long *d_prow = nullptr;
+    int *d_pcol = nullptr;
     double reg = 0, reg_ok = 0, min_pivot = 1;
     int nfloat = 0, nfactor = 0, pcg_iters = 0;
     double mu_now = 1e300;
@@ -963,6 +970,7 @@ class Solver {
     // blocks that share no constraint
     std::vector<char> in_sb;
     std::vector<int> sb_coff, sb_nmax;   // colour c: d_sb_list[sb_coff[c] .. sb_coff[c+1]), its largest n
+    std::vector<int> sb_cmax;            // ... and its largest constraint count
     int *d_sb_list = nullptr, *d_sb_ncon = nullptr;
     const int **d_sb_con = nullptr, **d_sb_cpos = nullptr;
     const long long **d_sb_cptr = nullptr;
@@ -1297,6 +1305,10 @@ void Solver::setup() {
     if (!h_dots) throw GpuFail{BGPU_ERR_NOMEM, __LINE__};
     choose_sparse();
     allow_float = !use_sparse && (opt.mixed > 0 || (opt.mixed < 0 && m >= 1000));
+    // FP32 fronts only when asked for (-mixed 1): the fronts of these problems are small and
+    // latency-bound, so FP32 saves no factor time and costs PCG steps (mom700: 0.153 s FP64,
+    // 0.175 s with FP32 fronts early)
+    sparse_float = use_sparse && opt.mixed > 0;
     asm_prec = opt.asm_prec < 0 ? 0 : opt.asm_prec;
     if (asm_prec == 1 && !use_sparse) allow_float = true;   // the 3xTF32 path factors in FP32 until mu_switch
     if (allow_float) {
@@ -1350,6 +1362,28 @@ void Solver::choose_sparse() {
     RC(schol::factor_bind(g.st, sp_an, buf, sp_f));
     CU(cudaStreamSynchronize(g.st));
     use_sparse = true;
+    {   // the pattern's rows for the residual product: row a is the union of the constraint lists
+        // of the blocks that hold a (a marker per row, then each row sorted)
+        std::vector<std::vector<int>> blocks_of(m);
+        for (int k = 0; k < nb; k++)
+            for (int c : P.blk[k].con) blocks_of[c].push_back(k);
+        std::vector<long long> rp(m + 1, 0);
+        std::vector<int> cols, mark(m, -1);
+        for (int a = 0; a < m; a++) {
+            const size_t s0 = cols.size();
+            for (int k : blocks_of[a])
+                for (int b : P.blk[k].con)
+                    if (mark[b] != a) { mark[b] = a; cols.push_back(b); }
+            std::sort(cols.begin() + s0, cols.end());
+            rp[a + 1] = (long long)cols.size();
+        }
+        d_prow = g.alloc<long long>(m + 1);
+        d_pcol = g.alloc<int>(std::max<size_t>(cols.size(), 1));
+        if (!d_prow || !d_pcol) throw GpuFail{BGPU_ERR_NOMEM, __LINE__};
+        CU(cudaMemcpyAsync(d_prow, rp.data(), sizeof(long long) * (m + 1), cudaMemcpyHostToDevice, g.st));
+        if (!cols.empty()) CU(cudaMemcpyAsync(d_pcol, cols.data(), sizeof(int) * cols.size(), cudaMemcpyHostToDevice, g.st));
+        CU(cudaStreamSynchronize(g.st));
+    }
     if (opt.verbose > 1)
         log_printf(0, "   [Schur pattern: sparse Cholesky, %.0f nonzeros in L, %.1e flops, %d supernodes, largest front %d, "
                    "%d levels (%.3fs)]\n", sp_an.nnz, sp_an.flops, sp_an.nsup, sp_an.fmax,
@@ -1435,11 +1469,13 @@ void Solver::setup_small_schur() {
     std::vector<int> list;
     sb_coff.assign(1, 0);
     sb_nmax.clear();
+    sb_cmax.clear();
     for (auto &cl : cls) {
-        int nm = 1;
-        for (int k : cl) { list.push_back(k); nm = std::max(nm, db[k].n); }
+        int nm = 1, cm = 1;
+        for (int k : cl) { list.push_back(k); nm = std::max(nm, db[k].n); cm = std::max(cm, db[k].ncon); }
         sb_coff.push_back((int)list.size());
         sb_nmax.push_back(nm);
+        sb_cmax.push_back(cm);
     }
     std::vector<int> ncon(nb, 0);
     std::vector<const int *> con(nb, nullptr), cpos(nb, nullptr);
@@ -1475,8 +1511,8 @@ void Solver::setup_small_schur() {
 
 void Solver::assemble_small(const double *Xc, const double *Zc) {
     for (size_t c = 0; c + 1 < sb_coff.size(); c++)
-        RC(schur_assemble_small(g.st, sb_coff[c + 1] - sb_coff[c], d_sb_list + sb_coff[c], sb_nmax[c], d_bn, d_sb_ncon,
-                                d_sb_con, d_sb_cptr, d_sb_cpos, d_sb_cval, d_boff, Xc, Zc, M, m));
+        RC(schur_assemble_small(g.st, sb_coff[c + 1] - sb_coff[c], d_sb_list + sb_coff[c], sb_nmax[c], sb_cmax[c], d_bn,
+                                d_sb_ncon, d_sb_con, d_sb_cptr, d_sb_cpos, d_sb_cval, d_boff, Xc, Zc, M, m));
 }
 
 void Solver::aop_cat(const double *D, std::vector<double> &out) {
@@ -1690,10 +1726,28 @@ int Solver::factor() {
     is_float = false;
     if (use_sparse) {
         RC(schur_diag_scale(g.st, m, M, m, Dsc));
+        if (sparse_float && !want_double && mu_now >= opt.mu_switch) {
+            // FP32 fronts early: PCG refines against the FP64 M, and the first factor that needs a
+            // shift or a PCG that struggles turns the rest of the solve to FP64 (want_double)
+            RC(schol::factor(g.st, sp_f, M, m, Dsc, 0.0, true));
+            int info = 0;
+            double pmin = 0;
+            CU(cudaMemcpyAsync(&info, sp_f.info, sizeof(int), cudaMemcpyDeviceToHost, g.st));
+            CU(cudaMemcpyAsync(&pmin, sp_f.pmin, sizeof(double), cudaMemcpyDeviceToHost, g.st));
+            CU(cudaStreamSynchronize(g.st));
+            if (info == 0 && pmin >= 1e-6) {
+                is_float = true;
+                reg = 0;
+                nfloat++;
+                min_pivot = std::min(pmin, 1.0);
+                return 0;
+            }
+            want_double = true;
+        }
         double r = reg_hint ? std::max(reg_floor, 0.01 * reg_ok) : 0.0;
         int info = 0;
         for (int attempt = 0; attempt < 10; attempt++) {
-            RC(schol::factor(g.st, sp_f, M, m, Dsc, r));
+            RC(schol::factor(g.st, sp_f, M, m, Dsc, r, false));
             double pmin = 0;
             CU(cudaMemcpyAsync(&info, sp_f.info, sizeof(int), cudaMemcpyDeviceToHost, g.st));
             CU(cudaMemcpyAsync(&pmin, sp_f.pmin, sizeof(double), cudaMemcpyDeviceToHost, g.st));
@@ -1745,11 +1799,19 @@ int Solver::factor() {
 
 void Solver::prec(const std::vector<double> &rv, std::vector<double> &z) {
     // z = D L^-T L^-1 D r (schur_prec_, solver.c:5424-5460)
+    z.resize(m);
+    if (use_sparse) {   // (FP32 or FP64 fronts: the solve takes the last factor's type; D is applied on
+                        // the device, and the sparse solve has no device waits to report)
+        CU(cudaMemcpyAsync(dv_in, rv.data(), sizeof(double) * m, cudaMemcpyHostToDevice, g.st));
+        RC(schol::solve(g.st, sp_f, Dsc, dv_in));
+        CU(cudaMemcpyAsync(z.data(), dv_in, sizeof(double) * m, cudaMemcpyDeviceToHost, g.st));
+        CU(cudaStreamSynchronize(g.st));
+        return;
+    }
     std::vector<double> h(m);
     std::vector<double> Dh(m);
     CU(cudaMemcpyAsync(Dh.data(), Dsc, sizeof(double) * m, cudaMemcpyDeviceToHost, g.st));
     CU(cudaStreamSynchronize(g.st));
-    z.resize(m);
     if (is_float) {
         std::vector<float> f(m);
         for (int i = 0; i < m; i++) f[i] = (float)(rv[i] * Dh[i]);
@@ -1759,11 +1821,6 @@ void Solver::prec(const std::vector<double> &rv, std::vector<double> &z) {
         CU(cudaMemcpyAsync(f.data(), fv, sizeof(float) * m, cudaMemcpyDeviceToHost, g.st));
         CU(cudaStreamSynchronize(g.st));
         for (int i = 0; i < m; i++) z[i] = (double)f[i] * Dh[i];
-    } else if (use_sparse) {
-        CU(cudaMemcpyAsync(dv_in, rv.data(), sizeof(double) * m, cudaMemcpyHostToDevice, g.st));
-        RC(schol::solve(g.st, sp_f, Dsc, dv_in));
-        CU(cudaMemcpyAsync(z.data(), dv_in, sizeof(double) * m, cudaMemcpyDeviceToHost, g.st));
-        CU(cudaStreamSynchronize(g.st));
     } else {
         for (int i = 0; i < m; i++) h[i] = rv[i] * Dh[i];
         CU(cudaMemcpyAsync(dv_in, h.data(), sizeof(double) * m, cudaMemcpyHostToDevice, g.st));
@@ -1781,7 +1838,8 @@ void Solver::prec(const std::vector<double> &rv, std::vector<double> &z) {
 
 void Solver::schur_mv(const std::vector<double> &x, std::vector<double> &y) {
     CU(cudaMemcpyAsync(dv_in, x.data(), sizeof(double) * m, cudaMemcpyHostToDevice, g.st));
-    RC(symv_full_f64(g.st, m, 1.0, M, m, dv_in, 0.0, dv_out));
+    if (use_sparse && d_prow) RC(pattern_symv_f64(g.st, m, d_prow, d_pcol, M, m, dv_in, dv_out));
+    else RC(symv_full_f64(g.st, m, 1.0, M, m, dv_in, 0.0, dv_out));
     y.resize(m);
     CU(cudaMemcpyAsync(y.data(), dv_out, sizeof(double) * m, cudaMemcpyDeviceToHost, g.st));
     CU(cudaStreamSynchronize(g.st));

@@ -396,17 +396,20 @@ __global__ void sp_init_kernel(int *info, double *pmin) {
 // The front of supernode s (order f, ns own columns, rs = f - ns): element (i, j), i >= j, lives
 // in the panel P (f x ns, ld f) when j < ns, else in the update matrix Us (rs x rs, ld rs).  In
 // shared memory (SMEM) the whole lower front is held as F (ld = f | 1) and written back at the end.
+template <typename T>
 struct FrontRef {
-    double *P, *Us, *F;
+    T *P, *Us, *F;
     int f, ns, rs, ldf;
     bool smem;
-    __device__ __forceinline__ double &at(int i, int j) const {
+    __device__ __forceinline__ T &at(int i, int j) const {
         if (smem) return F[i + j * ldf];
         return j < ns ? P[i + (long long)j * f] : Us[(i - ns) + (long long)(j - ns) * rs];
     }
 };
 
-template <bool SMEM>
+// T: the type of the front, the panel and the update matrices (double; float for the early
+// iterations of the mixed path, whose PCG refines against the FP64 M).
+template <bool SMEM, typename T>
 __global__ void __launch_bounds__(FT) front_kernel(const int *__restrict__ sups, const int *__restrict__ fsz,
                                                    const int *__restrict__ nsz, const long long *__restrict__ rptr,
                                                    const int *__restrict__ rows, const int *__restrict__ perm,
@@ -414,20 +417,20 @@ __global__ void __launch_bounds__(FT) front_kernel(const int *__restrict__ sups,
                                                    const int *__restrict__ cptr, const int *__restrict__ child,
                                                    const long long *__restrict__ relptr, const int *__restrict__ rel,
                                                    const double *__restrict__ M, long long ldm,
-                                                   const double *__restrict__ D, double reg, double *L, double *U,
+                                                   const double *__restrict__ D, double reg, T *L, T *U,
                                                    int *info, double *pmin) {
     extern __shared__ __align__(16) unsigned char fs_raw[];
     const int s = sups[blockIdx.x];
     const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
     if (*(volatile int *)info != 0) return;   // an earlier level failed
-    FrontRef F;
+    FrontRef<T> F;
     F.f = fsz[s];
     F.ns = nsz[s];
     F.rs = F.f - F.ns;
     F.ldf = F.f | 1;
     F.P = L + lptr[s];
     F.Us = U + uptr[s];
-    F.F = reinterpret_cast<double *>(fs_raw);
+    F.F = reinterpret_cast<T *>(fs_raw);
     F.smem = SMEM;
     const int f = F.f, ns = F.ns;
     const int *rw = rows + rptr[s];
@@ -442,7 +445,7 @@ __global__ void __launch_bounds__(FT) front_kernel(const int *__restrict__ sups,
                 v = D[ci] * M[ci + (long long)cj * ldm] * dj;
                 if (i == j) v += reg;
             }
-            F.at(i, j) = v;
+            F.at(i, j) = (T)v;
         }
     }
     __syncthreads();
@@ -451,7 +454,7 @@ __global__ void __launch_bounds__(FT) front_kernel(const int *__restrict__ sups,
         const int k = child[c];
         const int rc = fsz[k] - nsz[k];
         const int *rl = rel + relptr[k];
-        const double *Uc = U + uptr[k];
+        const T *Uc = U + uptr[k];
         for (int b = ty; b < rc; b += 16) {
             const int jb = rl[b];
             for (int a = b + tx; a < rc; a += 16) F.at(rl[a], jb) += Uc[a + (long long)b * rc];
@@ -462,20 +465,20 @@ __global__ void __launch_bounds__(FT) front_kernel(const int *__restrict__ sups,
     //    while column k updates the trailing front with its unscaled values / d)
     double pm = 1e300;
     int fail = 0;
-    double prev_piv = 0.0, prev_inv = 0.0;
+    T prev_piv = 0, prev_inv = 0;
     for (int k = 0; k < ns; k++) {
-        const double d = F.at(k, k);
-        if (!(d > 0.0) || !isfinite(d)) { fail = rw[k] + 1; break; }
-        pm = fmin(pm, d);
-        const double inv_d = 1.0 / d;
+        const T d = F.at(k, k);
+        if (!(d > (T)0) || !isfinite((double)d)) { fail = rw[k] + 1; break; }
+        pm = fmin(pm, (double)d);
+        const T inv_d = (T)1 / d;
         if (k > 0)
             for (int r = k - 1 + tid; r < f; r += FT) F.at(r, k - 1) = (r == k - 1) ? prev_piv : F.at(r, k - 1) * prev_inv;
         for (int q = k + 1 + tx; q < f; q += 16) {
-            const double sqc = F.at(q, k) * inv_d;
+            const T sqc = F.at(q, k) * inv_d;
             for (int r = q + ty; r < f; r += 16) F.at(r, q) -= F.at(r, k) * sqc;
         }
         prev_piv = sqrt(d);
-        prev_inv = 1.0 / prev_piv;
+        prev_inv = (T)1 / prev_piv;
         __syncthreads();
     }
     if (!fail && ns > 0) {
@@ -490,13 +493,13 @@ __global__ void __launch_bounds__(FT) front_kernel(const int *__restrict__ sups,
     // 4. back to the panel (its strict upper part zeroed) and the update matrix
     if (SMEM) {
         for (int j = ty; j < ns; j += 16)
-            for (int i = tx; i < f; i += 16) F.P[i + (long long)j * f] = i >= j ? F.F[i + j * F.ldf] : 0.0;
+            for (int i = tx; i < f; i += 16) F.P[i + (long long)j * f] = i >= j ? F.F[i + j * F.ldf] : (T)0;
         const int rs = F.rs;
         for (int j = ty; j < rs; j += 16)
             for (int i = j + tx; i < rs; i += 16) F.Us[i + (long long)j * rs] = F.F[(i + ns) + (j + ns) * F.ldf];
     } else {
         for (int j = ty; j < ns; j += 16)
-            for (int i = tx; i < j; i += 16) F.P[i + (long long)j * f] = 0.0;
+            for (int i = tx; i < j; i += 16) F.P[i + (long long)j * f] = (T)0;
     }
 }
 
@@ -519,10 +522,11 @@ __global__ void perm_out_kernel(int m, const int *__restrict__ perm, const doubl
     if (k < m) { const int c = perm[k]; x[c] = D[c] * xe[k]; }
 }
 
+template <typename T>
 __global__ void __launch_bounds__(ST) fwd_kernel(const int *__restrict__ sups, const int *__restrict__ fsz,
                                                  const int *__restrict__ nsz, const long long *__restrict__ rptr,
                                                  const int *__restrict__ rows, const long long *__restrict__ lptr,
-                                                 const double *__restrict__ L, const int *__restrict__ cptr,
+                                                 const T *__restrict__ L, const int *__restrict__ cptr,
                                                  const int *__restrict__ child, const long long *__restrict__ relptr,
                                                  const int *__restrict__ rel, double *xe, double *V) {
     __shared__ double xs[SX];
@@ -530,7 +534,7 @@ __global__ void __launch_bounds__(ST) fwd_kernel(const int *__restrict__ sups, c
     const int s = sups[blockIdx.x], tid = threadIdx.x;
     const int f = fsz[s], ns = nsz[s], rs = f - ns;
     const int k0 = rows[rptr[s]];
-    const double *P = L + lptr[s];
+    const T *P = L + lptr[s];
     double *vo = V + relptr[s];   // rs values (none at a root)
     const bool sm = ns <= SX;
     double *y = sm ? xs : xe + k0;
@@ -549,46 +553,47 @@ __global__ void __launch_bounds__(ST) fwd_kernel(const int *__restrict__ sups, c
         __syncthreads();
     }
     for (int j = 0; j < ns; j++) {
-        if (tid == 0) { yj = y[j] / P[j + (long long)j * f]; y[j] = yj; }
+        if (tid == 0) { yj = y[j] / (double)P[j + (long long)j * f]; y[j] = yj; }
         __syncthreads();
         const double v = yj;
-        for (int i = j + 1 + tid; i < ns; i += ST) y[i] -= P[i + (long long)j * f] * v;
+        for (int i = j + 1 + tid; i < ns; i += ST) y[i] -= (double)P[i + (long long)j * f] * v;
         __syncthreads();
     }
     for (int i = tid; i < rs; i += ST) {
         double a = 0.0;
-        for (int j = 0; j < ns; j++) a += P[(ns + i) + (long long)j * f] * y[j];
+        for (int j = 0; j < ns; j++) a += (double)P[(ns + i) + (long long)j * f] * y[j];
         vo[i] += a;
     }
     if (sm) for (int j = tid; j < ns; j += ST) xe[k0 + j] = xs[j];
 }
 
+template <typename T>
 __global__ void __launch_bounds__(ST) bwd_kernel(const int *__restrict__ sups, const int *__restrict__ fsz,
                                                  const int *__restrict__ nsz, const long long *__restrict__ rptr,
                                                  const int *__restrict__ rows, const long long *__restrict__ lptr,
-                                                 const double *__restrict__ L, double *xe) {
+                                                 const T *__restrict__ L, double *xe) {
     __shared__ double xs[SX];
     __shared__ double xj_s;
     const int s = sups[blockIdx.x], tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int f = fsz[s], ns = nsz[s];
     const int *rw = rows + rptr[s];
     const int k0 = rw[0];
-    const double *P = L + lptr[s];
+    const T *P = L + lptr[s];
     const bool sm = ns <= SX;
     double *x = sm ? xs : xe + k0;
     // x_s = y_s - L_off,s' x_off: a warp per column
     for (int j = warp; j < ns; j += ST / 32) {
         double a = 0.0;
-        for (int i = ns + lane; i < f; i += 32) a += P[i + (long long)j * f] * xe[rw[i]];
+        for (int i = ns + lane; i < f; i += 32) a += (double)P[i + (long long)j * f] * xe[rw[i]];
         a = warp_sum(a);
         if (lane == 0) x[j] = xe[k0 + j] - a;
     }
     __syncthreads();
     for (int j = ns - 1; j >= 0; j--) {
-        if (tid == 0) { xj_s = x[j] / P[j + (long long)j * f]; x[j] = xj_s; }
+        if (tid == 0) { xj_s = x[j] / (double)P[j + (long long)j * f]; x[j] = xj_s; }
         __syncthreads();
         const double v = xj_s;
-        for (int i = tid; i < j; i += ST) x[i] -= P[j + (long long)i * f] * v;
+        for (int i = tid; i < j; i += ST) x[i] -= (double)P[j + (long long)i * f] * v;
         __syncthreads();
     }
     if (sm) for (int j = tid; j < ns; j += ST) xe[k0 + j] = xs[j];
@@ -616,6 +621,7 @@ size_t factor_bytes(const Analysis &A) {
 }
 
 int factor_bind(cudaStream_t st, const Analysis &A, void *buf, Factor &F) {
+    release(F);
     F = Factor();
     F.A = &A;
     const size_t n = A.nsup;
@@ -682,50 +688,104 @@ int factor_bind(cudaStream_t st, const Analysis &A, void *buf, Factor &F) {
     return BGPU_OK;
 }
 
-int factor(cudaStream_t st, Factor &F, const double *M, long long ldm, const double *d_D, double reg) {
+namespace {
+template <typename T>
+int factor_t(cudaStream_t st, Factor &F, const double *M, long long ldm, const double *d_D, double reg) {
     const Analysis &A = *F.A;
+    T *L = reinterpret_cast<T *>(F.L), *U = reinterpret_cast<T *>(F.U);
     sp_init_kernel<<<1, 1, 0, st>>>(F.info, F.pmin);
     BGPU_LAUNCH_CHECK();
-    BGPU_ATTR_ONCE(BGPU_CHECK(cudaFuncSetAttribute(front_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                   (int)((FS_MAX | 1) * FS_MAX * sizeof(double)))));
+    BGPU_ATTR_ONCE(BGPU_CHECK(cudaFuncSetAttribute(front_kernel<true, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)((FS_MAX | 1) * FS_MAX * sizeof(T)))));
     for (size_t l = 0; l + 1 < A.lvptr.size(); l++) {
         const int lo = A.lvptr[l], cnt = A.lvptr[l + 1] - lo, ns_ = F.lvsplit[l];
         if (ns_ > 0) {
-            const size_t smem = (size_t)(F.lvsmem[l] | 1) * F.lvsmem[l] * sizeof(double);
-            front_kernel<true><<<ns_, FT, smem, st>>>(F.lvsup + lo, F.f, F.ns, F.rptr, F.rows, F.perm, F.lptr, F.uptr,
-                                                      F.cptr, F.child, F.relptr, F.rel, M, ldm, d_D, reg, F.L, F.U,
-                                                      F.info, F.pmin);
+            const size_t smem = (size_t)(F.lvsmem[l] | 1) * F.lvsmem[l] * sizeof(T);
+            front_kernel<true, T><<<ns_, FT, smem, st>>>(F.lvsup + lo, F.f, F.ns, F.rptr, F.rows, F.perm, F.lptr,
+                                                         F.uptr, F.cptr, F.child, F.relptr, F.rel, M, ldm, d_D, reg, L,
+                                                         U, F.info, F.pmin);
             BGPU_LAUNCH_CHECK();
         }
         if (cnt - ns_ > 0) {
-            front_kernel<false><<<cnt - ns_, FT, 0, st>>>(F.lvsup + lo + ns_, F.f, F.ns, F.rptr, F.rows, F.perm, F.lptr,
-                                                          F.uptr, F.cptr, F.child, F.relptr, F.rel, M, ldm, d_D, reg,
-                                                          F.L, F.U, F.info, F.pmin);
+            front_kernel<false, T><<<cnt - ns_, FT, 0, st>>>(F.lvsup + lo + ns_, F.f, F.ns, F.rptr, F.rows, F.perm,
+                                                             F.lptr, F.uptr, F.cptr, F.child, F.relptr, F.rel, M, ldm,
+                                                             d_D, reg, L, U, F.info, F.pmin);
             BGPU_LAUNCH_CHECK();
         }
     }
     return BGPU_OK;
 }
 
-int solve(cudaStream_t st, Factor &F, const double *d_D, double *x) {
+template <typename T>
+int solve_t(cudaStream_t st, Factor &F, const double *d_D, double *x) {
     const Analysis &A = *F.A;
+    const T *L = reinterpret_cast<const T *>(F.L);
     const int m = A.m, nlev = (int)A.lvptr.size() - 1;
     perm_in_kernel<<<ceil_div(m, 256), 256, 0, st>>>(m, F.perm, d_D, x, F.x);
     BGPU_LAUNCH_CHECK();
     for (int l = 0; l < nlev; l++) {
         const int lo = A.lvptr[l], cnt = A.lvptr[l + 1] - lo;
-        fwd_kernel<<<cnt, ST, 0, st>>>(F.lvsup + lo, F.f, F.ns, F.rptr, F.rows, F.lptr, F.L, F.cptr, F.child, F.relptr,
-                                       F.rel, F.x, F.V);
+        fwd_kernel<T><<<cnt, ST, 0, st>>>(F.lvsup + lo, F.f, F.ns, F.rptr, F.rows, F.lptr, L, F.cptr, F.child,
+                                          F.relptr, F.rel, F.x, F.V);
         BGPU_LAUNCH_CHECK();
     }
     for (int l = nlev - 1; l >= 0; l--) {
         const int lo = A.lvptr[l], cnt = A.lvptr[l + 1] - lo;
-        bwd_kernel<<<cnt, ST, 0, st>>>(F.lvsup + lo, F.f, F.ns, F.rptr, F.rows, F.lptr, F.L, F.x);
+        bwd_kernel<T><<<cnt, ST, 0, st>>>(F.lvsup + lo, F.f, F.ns, F.rptr, F.rows, F.lptr, L, F.x);
         BGPU_LAUNCH_CHECK();
     }
     perm_out_kernel<<<ceil_div(m, 256), 256, 0, st>>>(m, F.perm, d_D, F.x, x);
     BGPU_LAUNCH_CHECK();
     return BGPU_OK;
+}
+}  // namespace
+
+int factor(cudaStream_t st, Factor &F, const double *M, long long ldm, const double *d_D, double reg, bool fp32) {
+    F.fp32 = fp32;
+    return fp32 ? factor_t<float>(st, F, M, ldm, d_D, reg) : factor_t<double>(st, F, M, ldm, d_D, reg);
+}
+
+int solve(cudaStream_t st, Factor &F, const double *d_D, double *x) {
+    auto direct = [&]() { return F.fp32 ? solve_t<float>(st, F, d_D, x) : solve_t<double>(st, F, d_D, x); };
+    const int t = F.fp32 ? 1 : 0;
+    if (F.solve_graph[t] && (F.graph_D[t] != d_D || F.graph_x[t] != x)) {
+        cudaGraphExecDestroy(F.solve_graph[t]);
+        F.solve_graph[t] = nullptr;
+    }
+    if (!F.solve_graph[t] && st != nullptr) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusNone &&
+            cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+            const long long before = __atomic_load_n(&g_bgpu_launches, __ATOMIC_RELAXED);
+            const int rc = direct();
+            cudaGraph_t graph = nullptr;
+            const cudaError_t ce = cudaStreamEndCapture(st, &graph);
+            cudaGraphExec_t exec = nullptr;
+            if (rc == 0 && ce == cudaSuccess && graph && cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess) {
+                F.solve_graph[t] = exec;
+                F.graph_D[t] = d_D;
+                F.graph_x[t] = x;
+                F.graph_launches = (int)(__atomic_load_n(&g_bgpu_launches, __ATOMIC_RELAXED) - before);
+                __atomic_add_fetch(&g_bgpu_launches, -(long long)F.graph_launches, __ATOMIC_RELAXED);
+            }
+            if (graph) cudaGraphDestroy(graph);
+            cudaGetLastError();
+        }
+    }
+    if (F.solve_graph[t]) {
+        BGPU_CHECK(cudaGraphLaunch(F.solve_graph[t], st));
+        __atomic_add_fetch(&g_bgpu_launches, (long long)F.graph_launches, __ATOMIC_RELAXED);
+        return BGPU_OK;
+    }
+    return direct();
+}
+
+void release(Factor &F) {
+    for (int t = 0; t < 2; t++)
+        if (F.solve_graph[t]) {
+            cudaGraphExecDestroy(F.solve_graph[t]);
+            F.solve_graph[t] = nullptr;
+        }
 }
 
 }  // namespace schol

@@ -47,6 +47,13 @@ struct Factor {
     int *info = nullptr;
     double *pmin = nullptr;
     size_t bytes = 0;
+    bool fp32 = false;   // the last factor's type (L and U then hold floats, in the first half of their bytes)
+    // the solve's launches captured as a CUDA graph, per factor type, for the (D, x) they were
+    // captured with (released by release())
+    cudaGraphExec_t solve_graph[2] = {nullptr, nullptr};
+    const double *graph_D[2] = {nullptr, nullptr};
+    double *graph_x[2] = {nullptr, nullptr};
+    int graph_launches = 0;
     // host: front orders, own columns, and per level the supernodes (shared-memory fronts first),
     // how many fit shared memory and the largest of those
     std::vector<int> fs, nss, lvs, lvsplit, lvsmem;
@@ -56,10 +63,17 @@ size_t factor_bytes(const Analysis &A);
 // Lays out the factor's arrays in buf (factor_bytes(A) bytes, 256-byte aligned) and uploads the
 // analysis (stream-ordered; the host vectors of A must outlive the copies: call cudaStreamSynchronize).
 int factor_bind(cudaStream_t st, const Analysis &A, void *buf, Factor &F);
-// L L' = D M D + reg I on the pattern (M: dense m x m, column-major, both triangles; D = d_D).
-// info: first failing elimination position + 1 or 0; pmin: the smallest pivot (scaled).
-int factor(cudaStream_t st, Factor &F, const double *M, long long ldm, const double *d_D, double reg);
-// x := D (L L')^-1 D x (x in constraint order, length m; D = d_D).
+// L L' = D M D + reg I on the pattern (M: dense m x m, column-major, both triangles; D = d_D),
+// in FP64, or in FP32 (fp32: the fronts, L and the update matrices in single precision; M, D
+// and the solve's vectors stay FP64).  info: first failing elimination position + 1 or 0;
+// pmin: the smallest pivot (scaled).
+int factor(cudaStream_t st, Factor &F, const double *M, long long ldm, const double *d_D, double reg,
+           bool fp32 = false);
+// x := D (L L')^-1 D x (x in constraint order, length m; D = d_D), with the last factor's type.
+// The launches (two per tree level and the permutations) run as one CUDA graph, captured on
+// the first solve with these (D, x) on a stream that can capture; otherwise launched directly.
 int solve(cudaStream_t st, Factor &F, const double *d_D, double *x);
+// Releases the factor's graphs (its device memory belongs to the caller's allocation).
+void release(Factor &F);
 
 }  // namespace schol

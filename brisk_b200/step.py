@@ -44,6 +44,7 @@ def lib():
         "bgpu_schol_perm": ([P, P], I),
         "bgpu_schol_supernodes": ([P, P, P, P, P], I),
         "bgpu_schol_factor": ([P, P, I64, P, D, P, P, P], I),
+        "bgpu_schol_factor_f32": ([P, P, I64, P, D, P, P, P], I),
         "bgpu_schol_solve": ([P, P, P, P], I),
         "bgpu_schol_destroy": ([P], None),
         "bgpu_schol_set_delta": ([D], None),

@@ -289,7 +289,9 @@ BGPU_API int bgpu_aop(int n, int ncon, const int *d_con, const long long *d_cptr
  * (m x m, both triangles, leading dimension ldm) and the scaling d_D (m), on the device; the
  * first call allocates the factor's memory.  *info: 0 or the failing elimination position + 1;
  * *pmin: the smallest pivot (either pointer may be NULL; the call then does not synchronise).
- * bgpu_schol_solve: d_x := D (L L')^-1 D d_x. */
+ * bgpu_schol_factor_f32: the same factor with the fronts, L and the update matrices in FP32
+ * (M, D and the solve's vectors stay FP64): the early iterations' factor, refined by PCG against
+ * the FP64 M.  bgpu_schol_solve: d_x := D (L L')^-1 D d_x with the last factor's type. */
 typedef struct bgpu_schol bgpu_schol;
 BGPU_API bgpu_schol *bgpu_schol_analyze(int m, int ncliques, const int64_t *clq_ptr, const int *clq_idx, int *rc);
 BGPU_API int bgpu_schol_info(const bgpu_schol *h, double *out8);
@@ -297,6 +299,8 @@ BGPU_API int bgpu_schol_perm(const bgpu_schol *h, int *perm);
 BGPU_API int bgpu_schol_supernodes(const bgpu_schol *h, int *sfirst, int *parent, int64_t *rptr, int *rows);
 BGPU_API int bgpu_schol_factor(bgpu_schol *h, const double *d_M, int64_t ldm, const double *d_D, double reg,
                                int *info, double *pmin, void *stream);
+BGPU_API int bgpu_schol_factor_f32(bgpu_schol *h, const double *d_M, int64_t ldm, const double *d_D, double reg,
+                                   int *info, double *pmin, void *stream);
 BGPU_API int bgpu_schol_solve(bgpu_schol *h, const double *d_D, double *d_x, void *stream);
 BGPU_API void bgpu_schol_destroy(bgpu_schol *h);
 /* The ordering's tolerance for later analyses: each minimum-degree round eliminates the

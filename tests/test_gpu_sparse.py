@@ -106,3 +106,58 @@ def test_large_moment_relaxation_sparse_matches_reference(golden):
     assert res.status_str == ref["status"]
     objectives_close(res.pobj, res.dobj, ref["pobj"], ref["dobj"], each=res.iterations == ref["iterations"])
     assert np.max(np.abs(res.dimacs)) <= 1e-7
+
+
+@pytest.mark.parametrize("name,nv", [("mom8", 8), ("mom60", 60)])
+def test_sparse_factor_f32_solves_like_dense(cuda, name, nv):
+    """bgpu_schol_factor_f32: the fronts, L and the update matrices in FP32.  The solve agrees with
+    numpy's FP64 solve within the FP32 factor's error (a few ulps of FP32 times the condition
+    number of the scaled matrix), and the smallest pivot with the FP64 factor's to FP32 rounding."""
+    d = problems.moment_relaxation(nvars=nv, clique=4, seed=1 if nv == 8 else 0)
+    cl = cliques_of(d)
+    S = step.SparseCholesky(d.m, cl)
+    M = pattern_spd(d.m, cl, 3)
+    _, _, D, info64, pmin64 = factor_solve(S, M, cuda)
+    assert info64 == 0
+    dM = torch.as_tensor(M.T.copy().ravel(), device=cuda)
+    dD = torch.as_tensor(D, device=cuda)
+    info, pmin = ctypes.c_int(0), ctypes.c_double(0)
+    step.call("schol_factor_f32", S.h, dM.data_ptr(), d.m, dD.data_ptr(), 0.0, ctypes.addressof(info),
+              ctypes.addressof(pmin), None)
+    assert info.value == 0
+    assert pmin.value == pytest.approx(pmin64, rel=1e-4)
+    b = np.random.default_rng(4).standard_normal(d.m)
+    x = torch.as_tensor(b, device=cuda)
+    step.call("schol_solve", S.h, dD.data_ptr(), x.data_ptr(), None)
+    step.call("sync", None)
+    want = np.linalg.solve(M, b)
+    cond_s = np.linalg.cond(D[:, None] * M * D[None, :])
+    err = np.linalg.norm(x.cpu().numpy() - want) / np.linalg.norm(want)
+    assert err <= 64 * 2.0 ** -24 * cond_s, (err, cond_s)
+    assert err > 1e-12   # it is the FP32 factor that solved
+    # the next FP64 factor on the same handle solves to FP64 accuracy again
+    _, dD2, _, info2, _ = factor_solve(S, M, cuda)
+    x = torch.as_tensor(b, device=cuda)
+    step.call("schol_solve", S.h, dD2.data_ptr(), x.data_ptr(), None)
+    step.call("sync", None)
+    assert info2 == 0
+    assert np.linalg.norm(x.cpu().numpy() - want) <= 1e-12 * np.linalg.cond(M) * np.linalg.norm(want)
+    S.close()
+
+
+@pytest.mark.parametrize("name", ["mom60", "mom700"])
+def test_moment_relaxation_fp32_early_sparse_factor_matches_reference(golden, name):
+    """The mixed form of the sparse path (-mixed 1; the default for m >= 1000): FP32 fronts while
+    mu >= 1e-4, FP64 after, PCG against the FP64 M throughout.  Against the reference's FP64
+    solve: the same status, objectives by the parity bar, DIMACS <= 1e-7; the log shows both
+    factor types."""
+    e = golden[name]
+    d = problems.moment_relaxation(**e["kwargs"])
+    opts = ["-nohsd", "-dir", "hkm", "-mixed", "1", "-tol", "1e-7", "-sparse", "1", "-vv"]
+    res = brisk_b200.solve_sdpa(*d.args(), options=opts, verbose=False)
+    assert "sparse Cholesky" in res.log
+    assert "factor fp32" in res.log and "factor fp64" in res.log, res.log
+    ref = e["runs"]["default"]
+    assert res.status_str == ref["status"]
+    objectives_close(res.pobj, res.dobj, ref["pobj"], ref["dobj"], each=res.iterations == ref["iterations"])
+    assert np.max(np.abs(res.dimacs)) <= 1e-7
