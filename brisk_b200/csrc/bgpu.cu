@@ -234,6 +234,76 @@ BGPU_API int bgpu_schur_assemble_dense(int n, int m, int ncon, const int *d_con,
     return schur_assemble_dense(S(stream), B, d_X, d_Zi, d_M, m, precision, chunk, d_ws, ws_bytes);
 }
 
+BGPU_API int bgpu_schur_lp(int m, int N, int nc, int64_t ne, const int *d_gcon, const int64_t *d_aptr,
+                           const int *d_avar, const double *d_aval, const int64_t *d_vptr, const int *d_vcon,
+                           const double *d_vval, const double *d_x, const double *d_zi, double *d_M, void *stream) {
+    if (m <= 0 || N < 0 || nc < 0 || nc > m || ne < 0) return BGPU_ERR_ARG;
+    LpGroupDev G;
+    G.N = N;
+    G.nc = nc;
+    G.ne = ne;
+    G.gcon = (int *)d_gcon;
+    G.aptr = (long long *)d_aptr;
+    G.avar = (int *)d_avar;
+    G.aval = (double *)d_aval;
+    G.vptr = (long long *)d_vptr;
+    G.vcon = (int *)d_vcon;
+    G.vval = (double *)d_vval;
+    return schur_assemble_lp(S(stream), G, d_x, d_zi, d_M, m);
+}
+
+BGPU_API int bgpu_lowrank_factor(int n, int ncon, const int64_t *h_cptr, const int *h_cpos, const double *h_cval,
+                                 int max_rank, int *off, double *W, double *sig) {
+    if (n <= 0 || ncon < 0 || max_rank < 0 || !h_cptr || !h_cpos || !h_cval || !off) return BGPU_ERR_ARG;
+    std::vector<int> o;
+    std::vector<double> w, s;
+    if (!lowrank_factor_block(n, ncon, (const long long *)h_cptr, h_cpos, h_cval, o, w, s, max_rank))
+        return BGPU_ERR_UNSUPPORTED;
+    const int R = o[ncon];
+    std::copy(o.begin(), o.end(), off);
+    if (W) std::copy(w.begin(), w.begin() + (size_t)n * R, W);
+    if (sig) std::copy(s.begin(), s.begin() + R, sig);
+    return R;
+}
+
+BGPU_API int bgpu_schur_lowrank(int n, int m, int ncon, const int *d_con, const int64_t *h_cptr, const int *h_cpos,
+                                const double *h_cval, const double *d_X, const double *d_Zi, double *d_M, int *rank,
+                                void *stream) {
+    if (n <= 0 || m <= 0 || ncon < 0 || ncon > m || !h_cptr || !h_cpos || !h_cval || !rank) return BGPU_ERR_ARG;
+    *rank = 0;
+    std::vector<int> off;
+    std::vector<double> W, sig;
+    if (!lowrank_factor_block(n, ncon, (const long long *)h_cptr, h_cpos, h_cval, off, W, sig, 1 << 15))
+        return BGPU_ERR_UNSUPPORTED;
+    const int R = ncon > 0 ? off[ncon] : 0;
+    *rank = R;
+    if (R == 0) return BGPU_OK;
+    cudaStream_t st = S(stream);
+    LowRankDev L;
+    L.n = n;
+    L.ncon = ncon;
+    L.R = R;
+    const size_t bytes = sizeof(double) * ((size_t)2 * n * R + (size_t)2 * R * R + R) + sizeof(int) * (ncon + 1);
+    unsigned char *buf = nullptr;
+    BGPU_CHECK(cudaMalloc(&buf, bytes + 256));
+    double *p = (double *)buf;
+    L.W = p; p += (size_t)n * R;
+    L.XW = p; p += (size_t)n * R;
+    L.P = p; p += (size_t)R * R;
+    L.Q = p; p += (size_t)R * R;
+    L.sig = p; p += R;
+    L.off = (int *)p;
+    int rc = BGPU_OK;
+    if (cudaMemcpyAsync(L.W, W.data(), sizeof(double) * (size_t)n * R, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(L.sig, sig.data(), sizeof(double) * R, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(L.off, off.data(), sizeof(int) * (ncon + 1), cudaMemcpyHostToDevice, st) != cudaSuccess)
+        rc = BGPU_ERR_CUDA;
+    if (!rc) rc = schur_assemble_lowrank(st, L, d_con, d_X, d_Zi, d_M, m);
+    if (cudaStreamSynchronize(st) != cudaSuccess && !rc) rc = BGPU_ERR_CUDA;
+    cudaFree(buf);
+    return rc;
+}
+
 BGPU_API int bgpu_potrf(int n, double *d_A, int lda, double *d_dinv, int *d_info, double *d_pmin, void *stream) {
     if (n <= 0 || lda < n) return BGPU_ERR_ARG;
     return potrf_f64(S(stream), n, d_A, lda, d_dinv, d_info, d_pmin);

@@ -3,6 +3,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <vector>
 
 // ---- GEMM (gemm_f64.cu) ----------------------------------------------------------------
 int gemm_f64(cudaStream_t st, int a_kmajor, int b_kmajor, int M, int N, int K, double alpha, const double *A,
@@ -151,6 +152,41 @@ int schur_assemble_small(cudaStream_t st, int count, const int *d_blocks, int nm
                          const int *d_ncon, const int *const *con_tab, const long long *const *cptr_tab,
                          const int *const *cpos_tab, const double *const *cval_tab, const long long *d_boff,
                          const double *Xcat, const double *Zicat, double *M, int m);
+// The LP route (schur_lp, solver.c:3233): M += A diag(x_p zi_p) A' for the N variables of one LP
+// block, A the block's nc x N constraint matrix.  Per local constraint t (global id gcon[t]): its
+// entries (variable, value) by ascending variable in aptr/avar/aval; per variable p: its entries
+// (local constraint, value) by ascending constraint in vptr/vcon/vval.  Xv[p], Zv[p] are the
+// variables' X and Z^-1 (their order-1 blocks, one after another).  One warp per constraint a
+// writes column gcon[a] (rows b >= a) and its mirror; each entry sums over ascending p, as the
+// reference does.
+struct LpGroupDev {
+    int N = 0, nc = 0;
+    long long ne = 0;
+    int *gcon = nullptr;
+    long long *aptr = nullptr;   // [nc+1]
+    int *avar = nullptr;         // [ne]
+    double *aval = nullptr;      // [ne]
+    long long *vptr = nullptr;   // [N+1]
+    int *vcon = nullptr;         // [ne]
+    double *vval = nullptr;      // [ne]
+};
+int schur_assemble_lp(cudaStream_t st, const LpGroupDev &G, const double *Xv, const double *Zv, double *M, int m);
+// The low-rank route (schur_lowrank, solver.c:1862-1934; lowrank.cu): a block whose every
+// constraint is A_t = sum_{k in t} sig_k w_k w_k' (columns off[t] .. off[t+1] of W, n x R,
+// column-major, unit columns).  XW (n x R), P and Q (R x R) are the route's workspace.
+struct LowRankDev {
+    int n = 0, ncon = 0, R = 0;
+    double *W = nullptr, *sig = nullptr, *XW = nullptr, *P = nullptr, *Q = nullptr;
+    int *off = nullptr;   // [ncon+1]
+};
+// Host: the factors of every constraint of a block from its full-expansion lists (cptr, cpos,
+// cval as in DevBlock, host memory); 1 when every constraint factors and R <= max_rank, else 0.
+int lowrank_factor_block(int n, int ncon, const long long *cptr, const int *cpos, const double *cval,
+                         std::vector<int> &off, std::vector<double> &W, std::vector<double> &sig, int max_rank);
+// M += the block's Schur complement: P = W' X W, Q = W' Zi W (DMMA), then M[con[u], con[t]] (and
+// its mirror) += sum_{k in t, l in u} sig_k sig_l P_lk Q_lk over the pairs u >= t.
+int schur_assemble_lowrank(cudaStream_t st, const LowRankDev &L, const int *con, const double *X, const double *Zi,
+                           double *M, int m);
 // Fills B.ccol (device, ncon*(n+1) ints) from cptr/cpos: the column pointers of each constraint.
 int schur_colptr(cudaStream_t st, const DevBlock &B);
 // Upper-triangle lists from the full ones: schur_upper_ptr fills B.uptr (ncon+1; uptr[ncon] is

@@ -768,6 +768,53 @@ int schur_assemble_small(cudaStream_t st, int count, const int *d_blocks, int nm
     return BGPU_OK;
 }
 
+// ---- the LP route ----------------------------------------------------------------------------
+namespace {
+constexpr int LP_WARPS = 8;
+// One warp per local constraint a: for each variable p of a (ascending), w = A[a,p] d_p, and the
+// lanes add w A[b,p] to M[b, a] and M[a, b] for the constraints b >= a of p.  Within one p every
+// b is distinct, and __syncwarp orders one p after the next, so each entry of column gcon[a] sums
+// its terms by ascending p with no atomics; no other warp writes that column or its mirror row.
+__global__ void __launch_bounds__(LP_WARPS * 32) lp_schur_kernel(
+    int nc, const int *__restrict__ gcon, const long long *__restrict__ aptr, const int *__restrict__ avar,
+    const double *__restrict__ aval, const long long *__restrict__ vptr, const int *__restrict__ vcon,
+    const double *__restrict__ vval, const double *__restrict__ Xv, const double *__restrict__ Zv, double *M,
+    int m) {
+    const int lane = threadIdx.x & 31;
+    const int ta = blockIdx.x * LP_WARPS + (threadIdx.x >> 5);
+    if (ta >= nc) return;
+    const long long ga = gcon[ta];
+    for (long long e = aptr[ta]; e < aptr[ta + 1]; e++) {
+        const int p = avar[e];
+        const double w = aval[e] * (Xv[p] * Zv[p]);
+        // the entries of p below a: p's list is sorted by constraint, so start at a's own entry
+        long long lo = vptr[p], hi = vptr[p + 1];
+        while (lo < hi) {
+            const long long mid = (lo + hi) >> 1;
+            if (vcon[mid] < ta) lo = mid + 1; else hi = mid;
+        }
+        for (long long f = lo + lane; f < vptr[p + 1]; f += 32) {
+            const int tb = vcon[f];
+            const long long gb = gcon[tb];
+            const double v = w * vval[f];
+            M[gb + ga * m] += v;
+            if (tb != ta) M[ga + gb * m] += v;
+        }
+        __syncwarp();
+    }
+}
+}  // namespace
+
+int schur_assemble_lp(cudaStream_t st, const LpGroupDev &G, const double *Xv, const double *Zv, double *M, int m) {
+    if (G.nc <= 0 || G.ne <= 0) return BGPU_OK;
+    if (!G.gcon || !G.aptr || !G.avar || !G.aval || !G.vptr || !G.vcon || !G.vval || !Xv || !Zv || !M)
+        return BGPU_ERR_ARG;
+    lp_schur_kernel<<<ceil_div(G.nc, LP_WARPS), LP_WARPS * 32, 0, st>>>(G.nc, G.gcon, G.aptr, G.avar, G.aval, G.vptr,
+                                                                         G.vcon, G.vval, Xv, Zv, M, m);
+    BGPU_LAUNCH_CHECK();
+    return BGPU_OK;
+}
+
 // ---- the dense route -------------------------------------------------------------------------
 namespace {
 __global__ void densify_kernel(int n, int ncon, const long long *__restrict__ cptr, const int *__restrict__ cpos,

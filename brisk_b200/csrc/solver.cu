@@ -886,6 +886,8 @@ class Solver {
     std::vector<DevBlock> db;
     std::vector<DevArrays> da;
     std::vector<char> dense_route;   // per block: the dense Schur route (Ad resident)
+    std::vector<LowRankDev> lowrank;    // per block: the low-rank route's factors (R > 0 when taken)
+    void setup_lowrank(int k);
     // Schur complement
     double *M = nullptr, *Lm = nullptr, *dinvM = nullptr, *Dsc = nullptr;
     // the supernodal sparse factor of M (use_sparse): symbolic analysis and device factor
@@ -975,6 +977,10 @@ class Solver {
     const int **d_sb_con = nullptr, **d_sb_cpos = nullptr;
     const long long **d_sb_cptr = nullptr;
     const double **d_sb_cval = nullptr;
+    // LP blocks as given: the LP route (one launch per LP block), their order-1 blocks marked in_sb
+    struct LpGroup { int q0 = 0; LpGroupDev dev; };
+    std::vector<LpGroup> lp_groups;
+    void setup_lp_groups();
     void setup_small_schur();
     void assemble_small(const double *Xc, const double *Zc);
     void aop_cat(const double *D, std::vector<double> &out);                                    // out = A(D)
@@ -1047,6 +1053,44 @@ void Solver::dots(int nq, const double *const *a, const double *const *b, long l
     for (int q = 0; q < nq; q++) out[q] = h_dots[q];
 }
 
+// The low-rank route for block k (lowrank_block, problem.c:972-1075, with this build's own
+// factorization and cost rule, lowrank.cu): blocks above the small-block size whose every
+// constraint has low rank, where P and Q (4 n^2 R + 4 n R^2 flops) cost under half of the
+// row-product route's 2 n^3 per constraint, and P and Q fit in 4 GB.
+void Solver::setup_lowrank(int k) {
+    const HBlock &B = P.blk[k];
+    const int n = B.n, nc = (int)B.con.size();
+    if (opt.lowrank == 0 || nc == 0 || n <= SMALL_N_MAX) return;
+    const double nd = n, route = 2.0 * nd * nd * nd * nc;
+    auto cost = [&](double R) { return 4.0 * nd * nd * R + 4.0 * nd * R * R; };
+    if (opt.lowrank < 0 && cost((double)nc) >= 0.5 * route) return;   // every constraint has rank >= 1
+    int max_rank = (int)std::min(16384.0, std::sqrt(4e9 / 16.0));
+    std::vector<int> off;
+    std::vector<double> W, sig;
+    if (!lowrank_factor_block(n, nc, B.cptr.data(), B.cpos.data(), B.cval.data(), off, W, sig, max_rank)) return;
+    const int R = off[nc];
+    if (R == 0 || (opt.lowrank < 0 && cost((double)R) >= 0.5 * route)) return;
+    LowRankDev &L = lowrank[k];
+    L.n = n;
+    L.ncon = nc;
+    L.W = g.alloc<double>((size_t)n * R);
+    L.sig = g.alloc<double>(R);
+    L.off = g.alloc<int>(nc + 1);
+    L.XW = g.alloc<double>((size_t)n * R);
+    L.P = g.alloc<double>((size_t)R * R);
+    L.Q = g.alloc<double>((size_t)R * R);
+    if (!L.W || !L.sig || !L.off || !L.XW || !L.P || !L.Q) throw GpuFail{BGPU_ERR_NOMEM, __LINE__};
+    CU(cudaMemcpyAsync(L.W, W.data(), sizeof(double) * (size_t)n * R, cudaMemcpyHostToDevice, g.st));
+    CU(cudaMemcpyAsync(L.sig, sig.data(), sizeof(double) * R, cudaMemcpyHostToDevice, g.st));
+    CU(cudaMemcpyAsync(L.off, off.data(), sizeof(int) * (nc + 1), cudaMemcpyHostToDevice, g.st));
+    CU(cudaStreamSynchronize(g.st));   // the host factors are freed on return
+    L.R = R;
+    upload_bytes += (double)n * R * 8 + (double)R * 8 + (double)(nc + 1) * 4;
+    if (opt.verbose > 1)
+        log_printf(0, "   [block %d: low-rank route, %d constraints of total rank %d (%.2e flops an assembly against "
+                      "%.2e)]\n", k + 1, nc, R, cost((double)R), route);
+}
+
 void Solver::upload_block(int k) {
     const HBlock &B = P.blk[k];
     DevBlock &d = db[k];
@@ -1094,6 +1138,8 @@ void Solver::upload_block(int k) {
         const double bytes = (double)d.ncon * n * n * sizeof(double);
         bool dense = opt.route == 1 || (opt.route < 0 && n >= 8 && avg >= 0.02 * (double)n * n);
         if (dense && bytes > 8e9) dense = false;
+        setup_lowrank(k);
+        if (lowrank[k].R > 0) dense = false;
         dense_route[k] = dense;
         if (dense && d.ncon > 0) {
             d.Ad = g.alloc<double>((size_t)d.ncon * n * n);
@@ -1194,6 +1240,7 @@ void Solver::setup() {
     db.resize(nb);
     da.resize(nb);
     dense_route.assign(nb, 0);
+    lowrank.assign(nb, LowRankDev{});
     int nmax = 1;
     const double t1 = wtime();
     boff.assign(nb + 1, 0);
@@ -1444,11 +1491,89 @@ void Solver::build_gall() {
     upload_bytes += (double)ne * 12 + (double)m * 12;
 }
 
+// The LP route's lists for every LP block as given (its variables are the order-1 blocks
+// in_first[k] .. in_first[k+1]): the constraints that touch it, their entries by variable, and
+// each variable's entries by constraint, as schur_lp reads them (solver.c:3233, B->lp_ptr/lp_con).
+void Solver::setup_lp_groups() {
+    lp_groups.clear();
+    const int nbin = (int)P.in_n.size();
+    std::vector<int> loc(m, -1);
+    for (int k = 0; k < nbin; k++) {
+        if (P.in_n[k] >= 0) continue;
+        const int q0 = P.in_first[k], N = P.in_first[k + 1] - q0;
+        std::vector<int> gcon;
+        for (int p = 0; p < N; p++)
+            for (int c : P.blk[q0 + p].con) gcon.push_back(c);
+        std::sort(gcon.begin(), gcon.end());
+        gcon.erase(std::unique(gcon.begin(), gcon.end()), gcon.end());
+        const int nc = (int)gcon.size();
+        if (nc == 0) continue;
+        for (int t = 0; t < nc; t++) loc[gcon[t]] = t;
+        std::vector<long long> vptr(N + 1, 0), aptr(nc + 1, 0);
+        std::vector<int> vcon;
+        std::vector<double> vval;
+        for (int p = 0; p < N; p++) {
+            const HBlock &B = P.blk[q0 + p];
+            for (size_t t = 0; t < B.con.size(); t++) {
+                double v = 0;   // the order-1 block's one entry per constraint (summed if repeated)
+                for (long long e = B.cptr[t]; e < B.cptr[t + 1]; e++) v += B.cval[e];
+                if (v == 0) continue;
+                vcon.push_back(loc[B.con[t]]);
+                vval.push_back(v);
+                aptr[loc[B.con[t]] + 1]++;
+            }
+            vptr[p + 1] = (long long)vcon.size();
+        }
+        for (int t = 0; t < nc; t++) aptr[t + 1] += aptr[t];
+        const long long ne = (long long)vcon.size();
+        std::vector<int> avar(ne);
+        std::vector<double> aval(ne);
+        std::vector<long long> fill(aptr.begin(), aptr.end() - 1);
+        for (int p = 0; p < N; p++)   // by ascending variable within each constraint
+            for (long long f = vptr[p]; f < vptr[p + 1]; f++) {
+                const long long o = fill[vcon[f]]++;
+                avar[o] = p;
+                aval[o] = vval[f];
+            }
+        for (int t = 0; t < nc; t++) loc[gcon[t]] = -1;
+        LpGroup G;
+        G.q0 = q0;
+        G.dev.N = N;
+        G.dev.nc = nc;
+        G.dev.ne = ne;
+        G.dev.gcon = g.alloc<int>(nc);
+        G.dev.aptr = g.alloc<long long>(nc + 1);
+        G.dev.vptr = g.alloc<long long>(N + 1);
+        G.dev.avar = g.alloc<int>(std::max(ne, 1LL));
+        G.dev.vcon = g.alloc<int>(std::max(ne, 1LL));
+        G.dev.aval = g.alloc<double>(std::max(ne, 1LL));
+        G.dev.vval = g.alloc<double>(std::max(ne, 1LL));
+        if (!G.dev.gcon || !G.dev.aptr || !G.dev.vptr || !G.dev.avar || !G.dev.vcon || !G.dev.aval || !G.dev.vval)
+            throw GpuFail{BGPU_ERR_NOMEM, __LINE__};
+        CU(cudaMemcpyAsync(G.dev.gcon, gcon.data(), sizeof(int) * nc, cudaMemcpyHostToDevice, g.st));
+        CU(cudaMemcpyAsync(G.dev.aptr, aptr.data(), sizeof(long long) * (nc + 1), cudaMemcpyHostToDevice, g.st));
+        CU(cudaMemcpyAsync(G.dev.vptr, vptr.data(), sizeof(long long) * (N + 1), cudaMemcpyHostToDevice, g.st));
+        if (ne > 0) {
+            CU(cudaMemcpyAsync(G.dev.avar, avar.data(), sizeof(int) * ne, cudaMemcpyHostToDevice, g.st));
+            CU(cudaMemcpyAsync(G.dev.vcon, vcon.data(), sizeof(int) * ne, cudaMemcpyHostToDevice, g.st));
+            CU(cudaMemcpyAsync(G.dev.aval, aval.data(), sizeof(double) * ne, cudaMemcpyHostToDevice, g.st));
+            CU(cudaMemcpyAsync(G.dev.vval, vval.data(), sizeof(double) * ne, cudaMemcpyHostToDevice, g.st));
+        }
+        CU(cudaStreamSynchronize(g.st));   // the host lists are freed on return
+        for (int p = 0; p < N; p++) in_sb[q0 + p] = 1;
+        upload_bytes += (double)ne * 24 + (double)(nc + N) * 8;
+        if (opt.verbose > 1)
+            log_printf(0, "   [LP block %d: %d variables over %d constraints by the LP route]\n", k + 1, N, nc);
+        lp_groups.push_back(std::move(G));
+    }
+}
+
 void Solver::setup_small_schur() {
     in_sb.assign(nb, 0);
+    setup_lp_groups();
     std::vector<int> ids;
     for (int k : small_ids)
-        if (db[k].n <= SB_NMAX && db[k].ncon > 0) ids.push_back(k);
+        if (db[k].n <= SB_NMAX && db[k].ncon > 0 && !in_sb[k]) ids.push_back(k);
     if (ids.size() < 2) return;
     // greedy colouring: the first colour none of whose blocks shares a constraint with k
     std::vector<std::vector<char>> used;
@@ -1510,6 +1635,7 @@ void Solver::setup_small_schur() {
 }
 
 void Solver::assemble_small(const double *Xc, const double *Zc) {
+    for (const LpGroup &G : lp_groups) RC(schur_assemble_lp(g.st, G.dev, Xc + boff[G.q0], Zc + boff[G.q0], M, m));
     for (size_t c = 0; c + 1 < sb_coff.size(); c++)
         RC(schur_assemble_small(g.st, sb_coff[c + 1] - sb_coff[c], d_sb_list + sb_coff[c], sb_nmax[c], sb_cmax[c], d_bn,
                                 d_sb_ncon, d_sb_con, d_sb_cptr, d_sb_cpos, d_sb_cval, d_boff, Xc, Zc, M, m));
@@ -1678,6 +1804,12 @@ void Solver::assemble(std::vector<double> &) {
             continue;
         }
         const double *Xa = da[k].*xmem();
+        if (lowrank[k].R > 0) {   // (FP64: the route's products are small)
+            RC(schur_assemble_lowrank(g.st, lowrank[k], db[k].con, Xa, da[k].Zi, M, m));
+            const double n = db[k].n, R = lowrank[k].R;
+            schur_flops += 4.0 * n * n * R + 4.0 * n * R * R;
+            continue;
+        }
         if (dense_route[k])   // (the dense route has no Ozaki form: FP64 there)
             RC(schur_assemble_dense(g.st, db[k], Xa, da[k].Zi, M, m, oz ? 0 : prec, prec == 1 ? chunk : chunk64,
                                     ws, ws_bytes));
@@ -2057,7 +2189,8 @@ void Solver::least_squares_start(std::vector<double> &y) {
     for (int k = 0; k < nb; k++) {
         if (in_sb[k]) continue;
         RC(ew_set_scaled_identity(g.st, db[k].n, da[k].T, 1.0));
-        if (dense_route[k]) RC(schur_assemble_dense(g.st, db[k], da[k].T, da[k].T, M, m, 0, chunk_fp64(k), ws, ws_bytes));
+        if (lowrank[k].R > 0) RC(schur_assemble_lowrank(g.st, lowrank[k], db[k].con, da[k].T, da[k].T, M, m));
+        else if (dense_route[k]) RC(schur_assemble_dense(g.st, db[k], da[k].T, da[k].T, M, m, 0, chunk_fp64(k), ws, ws_bytes));
         else RC(schur_assemble_gram(g.st, db[k], M, m, ws, ws_bytes));
     }
     const int frc = factor();

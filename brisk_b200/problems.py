@@ -159,13 +159,15 @@ def random_sdp(n: int = 400, m: int = 2000, density: float = 0.01, seed: int = 0
 
 
 def sdp_lp_problem(blocks=(30, -40, 6), m: int = 50, density: float = 0.1, lp_per_con: int = 4,
-                   seed: int = 0) -> SdpaData:
+                   seed: int = 0, dense_rows: int = 0) -> SdpaData:
     """A random problem with LP blocks (negative sizes) among SDP blocks.
 
     SDP block of order n: C = G G'/n + I, each A_i with round(density n(n+1)/2) N(0,1) upper
     entries at distinct positions.  LP block of size N: c ~ U(0.5, 1.5), each A_i with
-    min(lp_per_con, N) N(0,1) entries on distinct variables.  b = A(I, 1, ...), so X = I, x = 1
-    is feasible, and y = 0 gives Z = C > 0, z = c > 0: both sides strictly feasible.
+    min(lp_per_con, N) N(0,1) entries on distinct variables; the first dense_rows constraints
+    instead hold all N variables (rows that join every variable of the block).  b = A(I, 1, ...),
+    so X = I, x = 1 is feasible, and y = 0 gives Z = C > 0, z = c > 0: both sides strictly
+    feasible.
     """
     rng = np.random.default_rng(seed)
     mats, blks, ii, jj, vv = [], [], [], [], []
@@ -191,8 +193,8 @@ def sdp_lp_problem(blocks=(30, -40, 6), m: int = 50, density: float = 0.1, lp_pe
             idx = np.arange(1, N + 1)
             mats.append(np.zeros(N, np.int32)); blks.append(np.full(N, kb, np.int32))
             ii.append(idx); jj.append(idx); vv.append(-c)
-            q = min(lp_per_con, N)
             for t in range(m):
+                q = N if t < dense_rows else min(lp_per_con, N)
                 var = rng.choice(N, size=q, replace=False) + 1
                 val = rng.standard_normal(q)
                 mats.append(np.full(q, t + 1, np.int32)); blks.append(np.full(q, kb, np.int32))
@@ -201,7 +203,34 @@ def sdp_lp_problem(blocks=(30, -40, 6), m: int = 50, density: float = 0.1, lp_pe
     d = _normalise(np.concatenate(mats), np.concatenate(blks), np.concatenate(ii), np.concatenate(jj),
                    np.concatenate(vv))
     return SdpaData(np.array(blocks, np.int32), b, *d, name=f"sdp_lp_{'_'.join(map(str, blocks))}_m{m}_seed{seed}",
-                    meta=dict(kind="sdp_lp", blocks=list(blocks), m=m, seed=seed))
+                    meta=dict(kind="sdp_lp", blocks=list(blocks), m=m, seed=seed, dense_rows=dense_rows))
+
+
+def lowrank_sdp(n: int = 100, m: int = 300, max_rank: int = 3, support: int = 0, seed: int = 0) -> SdpaData:
+    """A random SDP whose constraints have low rank (one n x n block): A_i = sum_k s_k g_k g_k'
+    with 1..max_rank terms, s_k = +-1, g_k ~ N(0,1) on `support` random rows (0: all n rows,
+    dense data).  b = A(I), C = G G'/n + I: X = I and y = 0 are strictly feasible."""
+    rng = np.random.default_rng(seed)
+    G = rng.standard_normal((n, n))
+    C = G @ G.T / n + np.eye(n)
+    iu, ju = np.triu_indices(n)
+    mats, ii, jj, vv = [np.zeros(iu.size, np.int32)], [iu + 1], [ju + 1], [-C[iu, ju]]
+    b = np.zeros(m)
+    for t in range(m):
+        r = int(rng.integers(1, max_rank + 1))
+        A = np.zeros((n, n))
+        for _ in range(r):
+            g = np.zeros(n)
+            rows = np.arange(n) if support <= 0 else rng.choice(n, size=min(support, n), replace=False)
+            g[rows] = rng.standard_normal(rows.size)
+            A += (1.0 if rng.random() < 0.7 else -1.0) * np.outer(g, g)
+        nzr, nzc = np.nonzero(np.triu(A))
+        mats.append(np.full(nzr.size, t + 1, np.int32)); ii.append(nzr + 1); jj.append(nzc + 1); vv.append(A[nzr, nzc])
+        b[t] = np.trace(A)
+    mat = np.concatenate(mats)
+    d = _normalise(mat, np.ones(mat.size, np.int32), np.concatenate(ii), np.concatenate(jj), np.concatenate(vv))
+    return SdpaData(np.array([n], np.int32), b, *d, name=f"lowrank_sdp_n{n}_m{m}_r{max_rank}_s{support}_seed{seed}",
+                    meta=dict(kind="lowrank", n=n, m=m, max_rank=max_rank, support=support, seed=seed))
 
 
 def random_dense_instance(rng, n: int, m: int, name: str = "") -> SdpaData:

@@ -50,6 +50,9 @@ def lib():
         "bgpu_schol_set_delta": ([D], None),
         "bgpu_schur_densify": ([I, I, P, P, P, P, P], I),
         "bgpu_schur_assemble_dense": ([I, I, I, P, P, P, P, P, P, P, P, P, I, I, P, SZ, P], I),
+        "bgpu_schur_lp": ([I, I, I, I64, P, P, P, P, P, P, P, P, P, P, P], I),
+        "bgpu_lowrank_factor": ([I, I, P, P, P, I, P, P, P], I),
+        "bgpu_schur_lowrank": ([I, I, I, P, P, P, P, P, P, P, P, P], I),
         "bgpu_potrf": ([I, P, I, P, P, P, P], I),
         "bgpu_potrf_f32": ([I, P, I, P, P, P, P], I),
         "bgpu_trsv": ([I, P, I, P, P, I, P, I, P, P], I),

@@ -173,6 +173,36 @@ BGPU_API int bgpu_schur_assemble_dense(int n, int m, int ncon, const int *d_con,
                                        const double *d_X, const double *d_Zi, double *d_M, int precision, int chunk,
                                        void *d_ws, size_t ws_bytes, void *stream);
 
+/* The LP route (schur_lp, solver.c:3233): M += A diag(x_p zi_p) A' over the N variables of one LP
+ * block, A its nc x N constraint matrix, both triangles of M (column-major, m x m).  d_gcon[t]
+ * is local constraint t's row of M; per constraint, its entries (variable, value) by ascending
+ * variable in d_aptr (nc+1) / d_avar / d_aval; per variable, its entries (local constraint,
+ * value) by ascending constraint in d_vptr (N+1) / d_vcon / d_vval (ne entries each); d_x and
+ * d_zi the variables' x and 1/z.  Each entry of M sums its terms by ascending variable, as the
+ * reference does; no atomics. */
+BGPU_API int bgpu_schur_lp(int m, int N, int nc, int64_t ne, const int *d_gcon, const int64_t *d_aptr,
+                           const int *d_avar, const double *d_aval, const int64_t *d_vptr, const int *d_vcon,
+                           const double *d_vval, const double *d_x, const double *d_zi, double *d_M, void *stream);
+
+/* The low-rank route (schur_lowrank, solver.c:1862-1934) for one block of order n: every
+ * constraint's factor A_t = sum_k sig_k w_k w_k' is found on the host from the block's
+ * full-expansion lists (host memory, as bgpu_schur_assemble takes them on the device: h_cptr
+ * ncon+1 offsets, h_cpos positions p + q n, h_cval values), then M += the block's Schur
+ * complement from P = W' X W and Q = W' Zi W (DMMA) and one launch over the pairs of
+ * constraints; d_con[t] is constraint t's row of M (m x m, both triangles).  *rank receives the
+ * total rank R.  Returns BGPU_ERR_UNSUPPORTED, leaving M alone, when some constraint has no
+ * factor of rank below 28.  The device workspace (2 n R + 2 R^2 + 2 R doubles) is allocated and
+ * freed inside the call, which waits for the stream. */
+/* The host half of the low-rank route alone (no GPU): the factors of a block's constraints,
+ * off[t] .. off[t+1] the columns of constraint t (off: ncon+1 ints), W (n x max_rank, column-major,
+ * unit columns) and sig (max_rank) written when not NULL.  Returns R, or BGPU_ERR_UNSUPPORTED
+ * when a constraint has no factor of rank below 28 or R > max_rank. */
+BGPU_API int bgpu_lowrank_factor(int n, int ncon, const int64_t *h_cptr, const int *h_cpos, const double *h_cval,
+                                 int max_rank, int *off, double *W, double *sig);
+BGPU_API int bgpu_schur_lowrank(int n, int m, int ncon, const int *d_con, const int64_t *h_cptr, const int *h_cpos,
+                                const double *h_cval, const double *d_X, const double *d_Zi, double *d_M, int *rank,
+                                void *stream);
+
 /* In-place Cholesky L L' = A of the lower triangle (column-major, lda); d_dinv receives the
  * inverses of the 64 x 64 diagonal blocks (ceil(n/64)*4096 entries), *d_info the first failing
  * column (1-based) or 0, *d_pmin the smallest squared pivot.  Replaces brisk_dpotrf

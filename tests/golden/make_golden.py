@@ -26,8 +26,8 @@ import tempfile
 
 ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 sys.path.insert(0, ROOT)
-from brisk_b200.problems import (batch_instance, dense_instance, moment_relaxation, random_sdp, sdp_lp_problem,  # noqa: E402
-                                 theta_problem, write_sdpa)
+from brisk_b200.problems import (batch_instance, dense_instance, lowrank_sdp, moment_relaxation, random_sdp,  # noqa: E402
+                                 sdp_lp_problem, theta_problem, write_sdpa)
 
 REF = os.path.join(ROOT, "oracle", "_ref", "brisk_ref")
 OUT = os.path.join(ROOT, "tests", "golden", "ref_runs.json")
@@ -46,6 +46,11 @@ INSTANCES = {
     # LP blocks (negative sizes) among SDP blocks, and an LP alone
     "lp_mixed": (sdp_lp_problem, dict(blocks=(30, -40, 6), m=50, density=0.1, lp_per_con=4, seed=3)),
     "lp_only": (sdp_lp_problem, dict(blocks=(-60,), m=30, lp_per_con=6, seed=4)),
+    # an LP block of 300 variables with two rows over all of them, beside an SDP block
+    # constraints of rank 1-3: dense vectors (the reference's low-rank route), and on 20 of 80 rows
+    "lowrank80": (lowrank_sdp, dict(n=80, m=200, max_rank=3, support=0, seed=6)),
+    "lowrank80s": (lowrank_sdp, dict(n=80, m=150, max_rank=2, support=20, seed=7)),
+    "lp_dense": (sdp_lp_problem, dict(blocks=(20, -300), m=80, density=0.1, lp_per_con=5, seed=5, dense_rows=2)),
 }
 # instances of the 4096-instance uneven batch (n ~ U{8..64}, m ~ U{n..n(n+1)/4}, seed 0): the
 # first twelve and the largest (q = 3339: n = 64, m = 1038)
