@@ -174,6 +174,12 @@ int parse_options(int argc, const char *const *argv, Options &opt, std::string &
             else if (!strcmp(s, "row")) opt.route = 0;
             else if (!strcmp(s, "dense")) opt.route = 1;
             else { err = "bad -schurroute (auto, row or dense)"; return 1; }
+        } else if (a == "-batchtune") {   // this build: the lockstep batch's work-item autotuner
+            const char *s = need("0 or 1");
+            if (!s || !parse_int(s, opt.batch_tune) || opt.batch_tune < 0 || opt.batch_tune > 1) {
+                if (err.empty()) err = "bad -batchtune (0 or 1)";
+                return 1;
+            }
         } else if (a == "-lowrank") {   // the reference's option: -1 auto, 0 off, 1 force
             const char *s = need("-1, 0 or 1");
             if (!s || !parse_int(s, opt.lowrank) || opt.lowrank < -1 || opt.lowrank > 1) {

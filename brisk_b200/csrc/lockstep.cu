@@ -56,8 +56,8 @@ __device__ __forceinline__ void smem_gemm_n(int n, const double *A, const double
     else smem_gemm<4>(n, A, Bm, C);
 }
 
-// one work item: ITEM constraints of one instance; shared: X, Z, A, W (n x n each); 256 threads
-__global__ void __launch_bounds__(256) form_q_kernel(const int2 *__restrict__ items, const int *__restrict__ nv,
+// one work item: `item` constraints of one instance; shared: X, Z, A, W (n x n each); 256 threads
+__global__ void __launch_bounds__(256) form_q_kernel(int item, const int2 *__restrict__ items, const int *__restrict__ nv,
                                                      const int *__restrict__ mv, const long long *__restrict__ boff,
                                                      const long long *__restrict__ poff, const double *__restrict__ P,
                                                      const double *__restrict__ Xc, const double *__restrict__ Zc,
@@ -71,7 +71,7 @@ __global__ void __launch_bounds__(256) form_q_kernel(const int2 *__restrict__ it
     for (int i = threadIdx.x; i < nn; i += blockDim.x) { Xs[i] = X[i]; Zs[i] = Z[i]; }
     const double *Pk = P + poff[k];
     double *Qk = Q + poff[k];
-    const int a1 = min(m, a0 + ITEM);
+    const int a1 = min(m, a0 + item);
     for (int a = a0; a < a1; a++) {
         const double *prow = Pk + (long long)a * t;
         __syncthreads();   // the previous constraint's A (G) is no longer read
@@ -362,13 +362,13 @@ __global__ void __launch_bounds__(256) seg_dots_kernel(const long long *__restri
 
 size_t form_q_smem(int nmax) { return 4 * (size_t)nmax * nmax * sizeof(double); }
 
-int form_q(cudaStream_t st, const Layout &L, const int2 *items, int nitems, int nmax, const double *P,
+int form_q(cudaStream_t st, const Layout &L, const int2 *items, int nitems, int nmax, int item, const double *P,
            const double *Xc, const double *Zc, double *Q) {
     if (nitems <= 0) return BGPU_OK;
-    if (nmax <= 0 || nmax > NMAX) return BGPU_ERR_ARG;
+    if (nmax <= 0 || nmax > NMAX || item <= 0) return BGPU_ERR_ARG;
     BGPU_ATTR_ONCE(BGPU_CHECK(cudaFuncSetAttribute(form_q_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                    (int)form_q_smem(NMAX))));
-    form_q_kernel<<<nitems, 256, form_q_smem(nmax), st>>>(items, L.n, L.m, L.boff, L.poff, P, Xc, Zc, Q);
+    form_q_kernel<<<nitems, 256, form_q_smem(nmax), st>>>(item, items, L.n, L.m, L.boff, L.poff, P, Xc, Zc, Q);
     BGPU_LAUNCH_CHECK();
     return BGPU_OK;
 }

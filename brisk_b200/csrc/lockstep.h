@@ -21,9 +21,14 @@ struct Layout {
 // P row a of instance k: the upper entries of A_a (A[p, q], p <= q) at their packed index,
 // built on the host.
 // Q row a = packed (G_a + G_a') off the diagonal, G_a on it, G_a = X A_a Zi, for the work items
-// (instance, first constraint) in items (chunks of ITEM constraints); nmax: the largest n listed.
-constexpr int ITEM = 8;
-int form_q(cudaStream_t st, const Layout &L, const int2 *items, int nitems, int nmax, const double *P,
+// (instance, first constraint) in items (chunks of `item` constraints); nmax: the largest n
+// listed.  The chunk size is the batch's tuned work-item shape: ITEM_CANDIDATES are the sizes the
+// autotuner (lockstep_solver.cuh, Lockstep::tune_items) times on each block-order class; every
+// size gives the same Q (each constraint's row is computed alone).
+constexpr int ITEM = 8;   // before tuning, and with -batchtune 0
+constexpr int ITEM_MIN = 2;
+constexpr int ITEM_CANDIDATES[5] = {2, 4, 8, 16, 32};
+int form_q(cudaStream_t st, const Layout &L, const int2 *items, int nitems, int nmax, int item, const double *P,
            const double *Xc, const double *Zc, double *Q);
 // M: the lower triangle copied to the upper one, for the listed instances.
 int mirror(cudaStream_t st, const Layout &L, const int *list, int cnt, double *M);

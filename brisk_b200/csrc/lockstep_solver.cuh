@@ -40,6 +40,11 @@ class Lockstep {
     double *d_slam = nullptr;
     int2 *d_items = nullptr;
     int4 *d_tiles = nullptr;
+    // the Q form's work-item size per block-order class (n <= 16, 32, 48, 64), 0 until tuned
+    int class_item[4] = {0, 0, 0, 0};
+    void tune_items(const std::vector<int> &L, const double *X, const double *Zi);
+    static void class_items(const std::vector<int> &L, const std::vector<int> &n, const std::vector<int> &m, int c,
+                            int item, std::vector<int2> &items);
     GemmGroup *d_groups = nullptr;
     long long max_items = 0, max_tiles = 0;
     double *dv_a = nullptr, *dv_b = nullptr, *d_dots = nullptr;
@@ -177,7 +182,7 @@ void Lockstep::setup() {
     need(d_reg); need(d_pmin); need(d_info); need(d_list); need(d_all); need(d_flag); need(d_sinfo); need(d_slam); need(d_dots);
     need(d_pa); need(d_pb);
     for (int i = 0; i < 4; i++) { d_coef[i] = g.alloc<double>(B); need(d_coef[i]); }
-    for (int k = 0; k < B; k++) max_items += (m[k] + lockstep::ITEM - 1) / lockstep::ITEM;
+    for (int k = 0; k < B; k++) max_items += (m[k] + lockstep::ITEM_MIN - 1) / lockstep::ITEM_MIN;
     const int TR = gemm_grouped_tile_rows();
     for (int k = 0; k < B; k++) max_tiles += (long long)ceil_div(m[k], TR) * ceil_div(m[k], 64);
     {   // the work items of A(.) (RI rows) and A'(.) (256 packed entries) over all instances
@@ -368,21 +373,92 @@ void Lockstep::segdots(int nq, const double *const *a, const double *const *b, s
     out.assign(h_dots, h_dots + (size_t)B * nq);
 }
 
+// The block-order classes of the Q form (a launch's shared memory is sized by its largest n, so
+// the small classes run several CTAs per SM): class c holds the instances with cls_max[c-1] < n
+// <= cls_max[c].
+static const int cls_max[4] = {16, 32, 48, 64};
+
+void Lockstep::class_items(const std::vector<int> &L, const std::vector<int> &n, const std::vector<int> &m, int c,
+                           int item, std::vector<int2> &items) {
+    for (int k : L)
+        if (n[k] <= cls_max[c] && (c == 0 || n[k] > cls_max[c - 1]))
+            for (int a0 = 0; a0 < m[k]; a0 += item) items.push_back(make_int2(k, a0));
+}
+
+// The autotuner of the batch's work-item shape: for each block-order class, the number of
+// constraints one CTA of the Q form takes (its X and Zi loaded once for them) is timed on this
+// batch's own data, every candidate in turn (CUDA events on the solve's stream, after one
+// untimed launch of each), and the fastest kept.  Few constraints a CTA give more CTAs (small
+// classes, few instances); many amortise the loads of X and Zi (large classes).  The choice is
+// cached for the process by (device, class, the class's constraint count to a power of two), so
+// later batches of the same shape skip the timing.  Every candidate writes the same Q.
+void Lockstep::tune_items(const std::vector<int> &L, const double *X, const double *Zi) {
+    static std::mutex mu;
+    static std::map<std::tuple<int, int, int>, int> cache;
+    int dev = 0;
+    CU(cudaGetDevice(&dev));
+    cudaEvent_t e0, e1;
+    CU(cudaEventCreate(&e0));
+    CU(cudaEventCreate(&e1));
+    std::string note;
+    for (int c = 0; c < 4; c++) {
+        long long cons = 0;
+        for (int k : L)
+            if (n[k] <= cls_max[c] && (c == 0 || n[k] > cls_max[c - 1])) cons += m[k];
+        if (cons == 0) { class_item[c] = lockstep::ITEM; continue; }
+        int bucket = 0;
+        while ((1LL << bucket) < cons) bucket++;
+        const auto key = std::make_tuple(dev, c, bucket);
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            auto it = cache.find(key);
+            if (it != cache.end()) { class_item[c] = it->second; continue; }
+        }
+        int best = lockstep::ITEM;
+        float best_ms = 1e30f;
+        char buf[160];
+        int w = snprintf(buf, sizeof buf, " n<=%d:", cls_max[c]);
+        for (int item : lockstep::ITEM_CANDIDATES) {
+            std::vector<int2> items;
+            class_items(L, n, m, c, item, items);
+            CU(cudaMemcpyAsync(d_items, items.data(), sizeof(int2) * items.size(), cudaMemcpyHostToDevice, g.st));
+            float ms = 0;
+            for (int rep = 0; rep < 2; rep++) {   // the first launch untimed
+                CU(cudaEventRecord(e0, g.st));
+                RC(lockstep::form_q(g.st, Ld, d_items, (int)items.size(), cls_max[c], item, Pp, X, Zi, Qp));
+                CU(cudaEventRecord(e1, g.st));
+                CU(cudaEventSynchronize(e1));
+                CU(cudaEventElapsedTime(&ms, e0, e1));
+            }
+            if (w < (int)sizeof buf) w += snprintf(buf + w, sizeof buf - w, " %d %.3f ms", item, ms);
+            if (ms < best_ms) { best_ms = ms; best = item; }
+        }
+        class_item[c] = best;
+        note += buf;
+        std::lock_guard<std::mutex> lk(mu);
+        cache[key] = best;
+    }
+    CU(cudaEventDestroy(e0));
+    CU(cudaEventDestroy(e1));
+    if (opt.verbose > 1 && !note.empty())
+        log_printf(0, "   [batch work items tuned (constraints a CTA, Q form time):%s; taken: %d %d %d %d]\n", note.c_str(),
+                   class_item[0], class_item[1], class_item[2], class_item[3]);
+}
+
 void Lockstep::assemble(const std::vector<int> &L, const double *X, const double *Zi) {
     if (L.empty()) return;
     const double t0 = wtime();
-    // the Q form's work items by block-order class (the shared memory of a launch is sized by its
-    // largest n: the small classes run several CTAs per SM)
-    const int cls_max[4] = {16, 32, 48, 64};
+    if (class_item[0] == 0) {
+        if (opt.batch_tune) tune_items(L, X, Zi);
+        else for (int &c : class_item) c = lockstep::ITEM;
+    }
     std::vector<int2> items;
     std::vector<int> cls_start(5, 0);
     std::vector<int4> tiles;
     const int TR = gemm_grouped_tile_rows();
     for (int c = 0; c < 4; c++) {
         cls_start[c] = (int)items.size();
-        for (int k : L)
-            if (n[k] <= cls_max[c] && (c == 0 || n[k] > cls_max[c - 1]))
-                for (int a0 = 0; a0 < m[k]; a0 += lockstep::ITEM) items.push_back(make_int2(k, a0));
+        class_items(L, n, m, c, class_item[c], items);
     }
     cls_start[4] = (int)items.size();
     for (int k : L) {
@@ -394,8 +470,8 @@ void Lockstep::assemble(const std::vector<int> &L, const double *X, const double
     CU(cudaMemcpyAsync(d_items, items.data(), sizeof(int2) * items.size(), cudaMemcpyHostToDevice, g.st));
     CU(cudaMemcpyAsync(d_tiles, tiles.data(), sizeof(int4) * tiles.size(), cudaMemcpyHostToDevice, g.st));
     for (int c = 0; c < 4; c++)
-        RC(lockstep::form_q(g.st, Ld, d_items + cls_start[c], cls_start[c + 1] - cls_start[c], cls_max[c], Pp, X, Zi,
-                            Qp));
+        RC(lockstep::form_q(g.st, Ld, d_items + cls_start[c], cls_start[c + 1] - cls_start[c], cls_max[c],
+                            class_item[c], Pp, X, Zi, Qp));
     RC(gemm_f64_grouped(g.st, (int)tiles.size(), d_tiles, d_groups, 1.0, 0.0));
     upload_list(L);
     RC(lockstep::mirror(g.st, Ld, d_list, (int)L.size(), Mm));

@@ -38,6 +38,7 @@
 #include <numeric>
 #include <thread>
 #include <functional>
+#include <tuple>
 
 namespace bsolve {
 

@@ -101,6 +101,7 @@ struct Options {
     int direction = -1;         // -1 auto (solver.c:13585-13591), 0 HKM, 1 NT
     int route = -1;             // Schur route per block: -1 auto (dense when the constraints average >= 2 % of
                                 // n^2 entries, problem.c:1299), 0 row-product, 1 dense
+    int batch_tune = 1;         // the lockstep batch's work-item autotuner (-batchtune 0|1)
     int lowrank = -1;           // the low-rank Schur route (-lowrank, problem.c:972): -1 where it is cheaper
                                 // (every constraint of the block of low rank), 0 off, 1 wherever it applies
 };

@@ -139,3 +139,35 @@ def test_default_direction_batch_is_nt_in_lockstep():
     for a, b in zip(out, ref):
         assert a.status == b.status and a.iterations == b.iterations
         assert a.pobj == b.pobj and a.dobj == b.dobj
+
+
+def test_every_instance_of_the_4096_batch_matches_its_own_solve():
+    """The whole uneven batch, 4096 instances in one lockstep call, each checked against its own
+    stand-alone FP64 solve (the concurrent form, which gives brisk_solve_data's bits per instance):
+    the same status (all OPTIMAL), DIMACS errors <= 1e-7 in both, objectives within 1e-7 by the
+    lockstep bar (parity.objectives_close) and the iteration count within 2."""
+    full = problems.batch_arrays(4096)
+    lock = brisk_b200.solve_batch_arrays(**full, options=FP64)
+    own = brisk_b200.solve_batch_arrays(**full, options=FP64 + ["-batchmode", "concurrent"], workers=16)
+    assert len(lock) == len(own) == 4096
+    worst = 0.0
+    for q, (a, b) in enumerate(zip(lock, own)):
+        assert a.exit_code == b.exit_code == 0, (q, a.exit_code, b.exit_code)
+        assert a.status_str == b.status_str == "OPTIMAL", q
+        objectives_close(a.pobj, a.dobj, b.pobj, b.dobj, each=False)
+        worst = max(worst, float(np.max(np.abs(a.dimacs))), float(np.max(np.abs(b.dimacs))))
+        assert abs(a.iterations - b.iterations) <= 2, (q, a.iterations, b.iterations)
+    assert worst <= 1e-7, worst
+
+
+def test_batch_work_item_autotuner_keeps_the_bits():
+    """The lockstep batch's autotuner times the Q form's work-item sizes on the batch's own data and
+    keeps the fastest per block-order class; every size computes each constraint's row alone, so
+    the tuned batch gives the bits of the untuned one (-batchtune 0: 8 constraints a CTA)."""
+    insts = [problems.batch_instance(q) for q in range(200, 264)]
+    tuned = brisk_b200.solve_batch(insts, options=FP64 + ["-batchtune", "1"])
+    fixed = brisk_b200.solve_batch(insts, options=FP64 + ["-batchtune", "0"])
+    for a, b in zip(tuned, fixed):
+        assert a.exit_code == b.exit_code == 0
+        assert (a.pobj, a.dobj, a.iterations) == (b.pobj, b.dobj, b.iterations)
+        np.testing.assert_array_equal(a.y, b.y)
