@@ -194,11 +194,10 @@ int parse_options(int argc, const char *const *argv, Options &opt, std::string &
             opt.verbose = 3;
         } else if (a == "-nohsd" || a == "-nofr" || a == "-feasible") {
             if (a == "-feasible") opt.known_feasible = 1;
+            if (a == "-nohsd") opt.hsd = 0;
         } else if (a == "-hsd") {
             // a flag in the reference (OPTIONS.md: "-hsd | -nohsd"): the self-dual embedding
-            // (hsd_run, solver.c:9803) is not part of this build
-            log_printf(1, "brisk: note: -hsd asks for the self-dual embedding, which this build does not have: "
-                          "the infeasible-start method runs\n");
+            opt.hsd = 1;
         } else if (a == "-corr" || a == "-chordal" || a == "-sym" || a == "-symalg" || a == "-deprows" ||
                    a == "-mixedfrac") {
             // options of the reference that change its method; this build solves the problem as

@@ -869,6 +869,8 @@ class Solver {
     }
     void setup();                 // upload the scaled problem and allocate the device state
     int run(ResultData &res);     // one solve from the resident data
+    int run_hsd(ResultData &res); // the same by the self-dual embedding (HKM)
+    void start_sdpt3();
     void set_options(const Options &o) { opt = o; }
     ~Solver() {
         schol::release(sp_f);
@@ -1039,7 +1041,7 @@ class Solver {
     // step length
     double maxstep(int primal, int K);
     double lanczos(int n, const double *Bm, int K);
-    int try_step(int primal, double *alpha);
+    int try_step(int primal, double *alpha, double from = 0.0);
     void least_squares_start(std::vector<double> &y);
     // final measures
     void final_measures(const std::vector<double> &y, ResultData &res);
@@ -2141,10 +2143,11 @@ double Solver::maxstep(int primal, int K) {
     return a;
 }
 
-// try_step (solver.c:6393-6447): V += alpha dV with a Cholesky test, alpha *= 0.8 on failure
-int Solver::try_step(int primal, double *alpha) {
+// try_step (solver.c:6393-6447): V += alpha dV with a Cholesky test, alpha *= 0.8 on failure.
+// `from`: the step V already took along dV (V is moved from there to alpha).
+int Solver::try_step(int primal, double *alpha, double from) {
     double a = *alpha;
-    double stepped = 0.0;   // all blocks stay at the same step
+    double stepped = from;   // all blocks stay at the same step
     const int ns = (int)small_ids.size();
     for (int tries = 0; tries < 40; tries++) {
         bool ok = true;
@@ -2321,23 +2324,34 @@ void Solver::final_measures(const std::vector<double> &y, ResultData &res) {
                 if (h_sinfo[i]) neg = std::max(neg, -h_slam[i]);
         }
     }
+    // -lambda_min of V (block k) where its Cholesky test fails: the Lanczos estimate theta - res
+    // (conservative: an upper bound), or the smallest shift s = 10^j 1e-16 |V|_F below it for which
+    // V + s I passes a Cholesky test (also an upper bound), whichever is smaller.  The Lanczos
+    // bound alone can exceed a nearly singular V's true negative part by orders of magnitude.
+    auto neg_part = [&](int k, const double *V, double *dinv) {
+        const int n = db[k].n;
+        const long long nn = (long long)n * n;
+        DevArrays &d = da[k];
+        RC(ew_lincomb(g.st, nn, 1.0, V, 0.0, nullptr, 0.0, nullptr, d.Bm));
+        const double est = -lanczos(n, d.Bm, 30);
+        double f2 = 0;
+        const double *aa[1] = {V};
+        dots(1, aa, aa, nn, &f2);
+        for (double sft = 1e-16 * std::sqrt(f2); sft > 0 && sft < est; sft *= 10) {
+            RC(ew_lincomb(g.st, nn, 1.0, V, sft, Icat + boff[k], 0.0, nullptr, d.T));
+            if (chol(n, d.T, dinv) == 0) return sft;
+        }
+        return est;
+    };
     for (int k : big_ids) {
         const int n = db[k].n;
         const long long nn = (long long)n * n;
         DevArrays &d = da[k];
-        // cone errors: a Cholesky test, then lambda_min by Lanczos when it fails
+        // cone errors: a Cholesky test, then the bound of neg_part when it fails
         RC(ew_lincomb(g.st, nn, 1.0, d.W, 0.0, nullptr, 0.0, nullptr, d.T));
-        if (chol(n, d.T, d.dinvZ) != 0) {
-            RC(ew_lincomb(g.st, nn, 1.0, d.W, 0.0, nullptr, 0.0, nullptr, d.Bm));
-            const double lam = lanczos(n, d.Bm, 30);
-            lamz_neg = std::max(lamz_neg, -lam);
-        }
+        if (chol(n, d.T, d.dinvZ) != 0) lamz_neg = std::max(lamz_neg, neg_part(k, d.W, d.dinvZ));
         RC(ew_lincomb(g.st, nn, 1.0, d.G, 0.0, nullptr, 0.0, nullptr, d.T));
-        if (chol(n, d.T, d.dinvX) != 0) {
-            RC(ew_lincomb(g.st, nn, 1.0, d.G, 0.0, nullptr, 0.0, nullptr, d.Bm));
-            const double lam = lanczos(n, d.Bm, 30);
-            lamx_neg = std::max(lamx_neg, -lam);
-        }
+        if (chol(n, d.T, d.dinvX) != 0) lamx_neg = std::max(lamx_neg, neg_part(k, d.G, d.dinvX));
     }
     std::vector<double> AX;
     aop_cat(cat.G, AX);   // scaled A' = d A: A_o(X_o) = AX / d
@@ -2374,22 +2388,10 @@ static double dimacs_score(const IterRes &R) {
                     std::max(std::fabs(nan_inf(R.err[5])), std::fabs(nan_inf(R.err[6]))));
 }
 
-int Solver::run(ResultData &res) {
-    const double t0 = wtime();
-    tm = Timings();
-    want_double = is_float = reg_hint = false;
-    reg = reg_ok = 0;
-    min_pivot = 1;
-    nfloat = nfactor = pcg_iters = 0;
-    mu_now = 1e300;
-    m_exact = true;
-    asm_fp64 = late_exact = false;
-    schur_flops = schur_dev_time = 0;
-    CU(cudaEventRecord(evs0, g.st));
-    std::vector<double> y(m, 0.0), ybest(m, 0.0), dy, rp(m), a0, h(m, 0.0), rhs(m), qv, ev(m), wv;
-    std::vector<double> tmpv;
-    // start_sdpt3 (solver.c:6622-6661).  An LP block as given takes one xi and one eta, from its
-    // order N and the norms over all its variables, for each of its blocks of order 1.
+// start_sdpt3 (solver.c:6622-6661): X = xi I, Z = eta I per block, their factors, the factors'
+// diagonal-block inverses and the inverses of the factors.  An LP block as given takes one xi and
+// one eta, from its order N and the norms over all its variables, for each of its blocks of order 1.
+void Solver::start_sdpt3() {
     std::vector<std::vector<double>> sval(6, std::vector<double>(nb, 0.0));
     std::vector<double> lp_xi(nb, 0.0), lp_eta(nb, 0.0);
     for (size_t kin = 0; kin < P.in_n.size(); kin++) {
@@ -2469,6 +2471,23 @@ int Solver::run(ResultData &res) {
             CU(cudaStreamSynchronize(g.st));   // d_bval is reused by the next member
         }
     }
+}
+
+int Solver::run(ResultData &res) {
+    const double t0 = wtime();
+    tm = Timings();
+    want_double = is_float = reg_hint = false;
+    reg = reg_ok = 0;
+    min_pivot = 1;
+    nfloat = nfactor = pcg_iters = 0;
+    mu_now = 1e300;
+    m_exact = true;
+    asm_fp64 = late_exact = false;
+    schur_flops = schur_dev_time = 0;
+    CU(cudaEventRecord(evs0, g.st));
+    std::vector<double> y(m, 0.0), ybest(m, 0.0), dy, rp(m), a0, h(m, 0.0), rhs(m), qv, ev(m), wv;
+    std::vector<double> tmpv;
+    start_sdpt3();
     if (opt.init >= 1 && m > 0) least_squares_start(y);
     // R0 = C - Z - A'y, theta = 1 (solver.c:14317-14326)
     double theta = 1.0, r0norm = 0;
@@ -2783,6 +2802,7 @@ int Solver::run(ResultData &res) {
     }
     res.iters = it;
     res.direction = nt_mode ? 1 : 0;
+    res.embedding = 0;
     // fall back to the best iterate seen
     if (status != 0 && status != 1 && status != 2 && best_score < res_score(R)) {
         R = best;
@@ -2793,6 +2813,300 @@ int Solver::run(ResultData &res) {
     }
     final_measures(y, res);
     // the status of the returned point as measured on the data as given (main.c:2349-2362)
+    const double acc = std::max(std::max(res.err[1], res.err[2]),
+                                std::max(res.err[4], std::max(std::fabs(res.err[5]), std::fabs(res.err[6]))));
+    if (status == 0 || status == 5 || status == 3 || status == 4 || status == 6) {
+        if (acc <= opt.tol) status = 0;
+        else if (acc <= opt.red_acc) status = 5;
+        else if (status == 0 || status == 5) status = 4;
+    }
+    res.status = status;
+    res.exit_code = exit_code_of(status);
+    res.nfloat = nfloat;
+    res.nfactor = nfactor;
+    res.pcg_iters = pcg_iters;
+    res.schur_flops = schur_flops;
+    res.schur_time = schur_dev_time;
+    CU(cudaEventRecord(evs1, g.st));
+    CU(cudaEventSynchronize(evs1));
+    float dms = 0;
+    CU(cudaEventElapsedTime(&dms, evs0, evs1));
+    res.device_time = dms * 1e-3;
+    tm.total = wtime() - t0;
+    res.t = tm;
+    res.time = tm.total;
+    return res.exit_code;
+}
+
+// The self-dual embedding (the reference's hsd_run, solver.c:9803, which BRISK runs first on most
+// problems), as this build's own homogeneous self-dual predictor-corrector with the HKM direction
+// (the reference's direction in the embedding, solver.c:13566).  With tau, kappa >= 0 the scaled
+// problem is embedded as
+//     A(X) - b tau = 0,   A'y + Z - C tau = 0,   b'y - <C,X> - kappa = 0,
+//     X Z = mu I,  tau kappa = mu,  mu = (<X,Z> + tau kappa) / (N + 1),
+// and the residuals rp = b tau - A(X), Rd = C tau - A'y - Z, rg = kappa - b'y + <C,X> fall by
+// 1 - eta alpha a step (predictor: sigma 0, eta 1; corrector: Mehrotra's sigma, eta = 1 - sigma
+// and the second-order terms).  The Newton system reduces to the infeasible method's Schur
+// complement M:
+//     dZ = C dtau - A'dy + eta Rd,  dX = sigma mu Zi - X - sym(Zi dZ X + Q),  Q = Zi dZp dXp,
+//     dkappa = (sigma mu - tau kappa - dtau_p dkappa_p - kappa dtau) / tau,
+//     M dy - p dtau = eta rp - sigma mu A(Zi) + A(X) + eta A(Zi Rd X) + A(Q),   p = A(Zi C X) + b,
+//     (2b - p)'dy + (<C, Zi C X> + kappa / tau) dtau =
+//         eta rg + sigma mu <C, Zi> - <C, X> - eta <C, Zi Rd X> - <C, Q> + (sigma mu - tau kappa - dtau_p dkappa_p) / tau,
+// so dy = u + v dtau with M u = (the first right side) and M v = p: three Schur solves an
+// iteration, as the infeasible method takes.  One step length for every variable keeps the
+// residuals falling together.  The solution is X / tau, y / tau; kappa >> tau certifies
+// infeasibility (b'y > 0: primal, <C,X> < 0: dual).  The start is start_sdpt3's X and Z with
+// tau = 1 and kappa = <X,Z> / N (on the central path).
+int Solver::run_hsd(ResultData &res) {
+    const double t0 = wtime();
+    tm = Timings();
+    want_double = is_float = reg_hint = false;
+    reg = reg_ok = 0;
+    min_pivot = 1;
+    nfloat = nfactor = pcg_iters = 0;
+    mu_now = 1e300;
+    m_exact = true;
+    asm_fp64 = late_exact = false;
+    schur_flops = schur_dev_time = 0;
+    CU(cudaEventRecord(evs0, g.st));
+    const bool nt_saved = nt_mode;   // a session's solver keeps its own direction for run()
+    nt_mode = false;
+    std::vector<double> y(m, 0.0), ybest(m, 0.0), rp(m), a0, pv, hv, qv, rhs(m), u, v, dy(m), tmpv, AX;
+    start_sdpt3();
+    // C as an iterate-shaped array for the products Zi C X (R0, the infeasible method's residual
+    // base, is not used here)
+    CU(cudaMemcpyAsync(cat.R0, Ccat, sizeof(double) * Ntot2, cudaMemcpyDeviceToDevice, g.st));
+    const double Ntot = (double)P.Ntot;
+    double tau = 1.0, kap = 0.0;
+    {
+        const double *aa[1] = {cat.X}, *bb[1] = {cat.Z};
+        dots_cat(1, aa, bb, &kap);
+        kap /= Ntot;
+    }
+    int status = -1, it = 0, it_best = 0, stall = 0;
+    double alpha = 0, sigma = 0, best_score = INFINITY, tau_best = 1.0;
+    IterRes R, best;
+    if (opt.verbose > 0)
+        log_printf(0, " it   pobj            dobj            pinf     dinf     gap      mu       alp   ald   sigma  time\n");
+    for (it = 0; it <= opt.maxit; it++) {
+        double td = wtime();
+        for (int k : big_ids) zinv(k);
+        if (!small_ids.empty())
+            RC(small_gemm(g.st, (int)small_ids.size(), d_sns, 1, 0, 1.0, (const double *const *)tab(&DevArrays::LiZ),
+                          (const double *const *)tab(&DevArrays::LiZ), 0.0, tab(&DevArrays::Zi), 1));
+        // residuals of the embedding
+        aop_cat(cat.X, AX);
+        for (int i = 0; i < m; i++) rp[i] = P.b[i] * tau - AX[i];
+        atop_cat(y, 1.0, 0.0, cat.F);                                   // A'y
+        lincomb_cat(tau, Ccat, -1.0, cat.F, -1.0, cat.Z, cat.Fd);       // Rd = C tau - A'y - Z
+        double cx = 0, xz = 0, rd2 = 0;
+        {
+            double part[3];
+            const double *aa[3] = {Ccat, cat.X, cat.Fd}, *bb[3] = {cat.X, cat.Z, cat.Fd};
+            dots_cat(3, aa, bb, part);
+            cx = part[0]; xz = part[1]; rd2 = part[2];
+        }
+        const double by = dot(P.b, y);
+        const double rg = kap - by + cx;
+        const double mu = (xz + tau * kap) / (Ntot + 1);
+        // the measures of the solution X / tau, y / tau, Z / tau (as the infeasible method's)
+        const double sc = P.bs * P.cs;
+        mu_now = sc * xz / (tau * tau * Ntot);
+        double rpo = 0;
+        for (int i = 0; i < m; i++) { const double w = rp[i] * P.du[i]; rpo += w * w; }
+        rpo = std::sqrt(rpo) / tau;
+        const double rdo = P.cs * std::sqrt(rd2) / tau;
+        const double po = sc * cx / tau, dob = sc * by / tau;
+        R.pobj = po; R.dobj = dob;
+        R.pinf = rpo / (1 + P.normb2);
+        R.dinf = rdo / (1 + P.normC2);
+        const double oden = 1 + std::fabs(po) + std::fabs(dob);
+        R.relgap = std::fabs(po - dob) / oden;
+        R.relcomp = sc * xz / (tau * tau) / oden;
+        R.err[1] = rpo / (1 + P.normb1);
+        R.err[3] = rdo / (1 + P.normC1);
+        R.err[5] = (po - dob) / oden;
+        R.err[6] = R.relcomp;
+        tm.dense += wtime() - td;
+        if (opt.verbose > 0)
+            log_printf(0, "%3d %+.8e %+.8e %.2e %.2e %.2e %.2e %.3f %.3f %.3f %6.2f\n", it, -po, -dob, R.pinf, R.dinf,
+                       R.relgap, mu_now, alpha, alpha, sigma, wtime() - t0);
+        if (!std::isfinite(po) || !std::isfinite(dob) || !(tau > 0) || !(kap > 0)) { status = 4; break; }
+        const double score = res_score(R);
+        if (score < best_score) {
+            best_score = score;
+            it_best = it;
+            best = R;
+            ybest = y;
+            tau_best = tau;
+            CU(cudaMemcpyAsync(cat.Xb, cat.X, sizeof(double) * Ntot2, cudaMemcpyDeviceToDevice, g.st));
+            CU(cudaMemcpyAsync(cat.Zb, cat.Z, sizeof(double) * Ntot2, cudaMemcpyDeviceToDevice, g.st));
+        }
+        if (score < opt.tol) { status = 0; break; }
+        if (it > it_best && dimacs_score(best) <= 0.5 * opt.tol) { status = 4; break; }
+        if (opt.timelimit > 0 && wtime() - t0 > opt.timelimit) { status = 6; break; }
+        if (kap > 1e8 * tau) {   // the embedding's certificate: tau -> 0 with kappa > 0
+            if (by > 0 && !opt.known_feasible) { status = 1; break; }
+            if (cx < 0 && !opt.known_feasible) { status = 2; break; }
+            status = 4;
+            break;
+        }
+        if (it == opt.maxit) { status = 3; break; }
+        if (stall >= 3) { status = 4; break; }
+        if (it - it_best >= opt.stall_win && best_score < 1e-6) { status = 4; break; }
+        if (it - it_best >= 12) { status = 4; break; }
+        // ---- Schur complement (the infeasible method's, with its precision ladder) ----
+        const double ts_before = tm.schur, tstep_before = tm.step;
+        double ts = wtime();
+        assemble(tmpv);
+        double tc = wtime();
+        tm.schur += tc - ts;
+        int frc = factor();
+        if (!m_exact && (frc != 0 || reg > 0) && raise_precision()) {
+            reg_hint = false;
+            reg_ok = 0;
+            tm.chol += wtime() - tc;
+            ts = wtime();
+            assemble(tmpv);
+            tc = wtime();
+            tm.schur += tc - ts;
+            frc = factor();
+            if (!m_exact && (frc != 0 || reg > 0) && raise_precision()) {
+                reg_hint = false;
+                reg_ok = 0;
+                ts = wtime();
+                assemble(tmpv);
+                tc = wtime();
+                tm.schur += tc - ts;
+                frc = factor();
+            }
+        }
+        if (frc != 0) { status = 4; tm.chol += wtime() - tc; break; }
+        if (cur_prec == 1 && !asm_fp64 && min_pivot < 1e-4) asm_fp64 = true;
+        tm.chol += wtime() - tc;
+        // ---- the pieces both directions share ----
+        td = wtime();
+        aop_cat(cat.Zi, a0);                                             // A(Zi)
+        mul_all(1.0, &DevArrays::Zi, &DevArrays::R0, &DevArrays::T);     // Zi C
+        mul_all(1.0, &DevArrays::T, &DevArrays::X, &DevArrays::G);       // Zi C X
+        aop_cat(cat.G, pv);
+        for (int i = 0; i < m; i++) pv[i] += P.b[i];                     // p = A(Zi C X) + b
+        mul_all(1.0, &DevArrays::Zi, &DevArrays::Fd, &DevArrays::T);     // Zi Rd
+        mul_all(1.0, &DevArrays::T, &DevArrays::X, &DevArrays::W);       // Zi Rd X
+        aop_cat(cat.W, hv);
+        double c2 = 0, cz = 0, c3 = 0;
+        {
+            double part[3];
+            const double *aa[3] = {Ccat, Ccat, Ccat}, *bb[3] = {cat.G, cat.Zi, cat.W};
+            dots_cat(3, aa, bb, part);
+            c2 = part[0]; cz = part[1]; c3 = part[2];
+        }
+        tm.dense += wtime() - td;
+        tc = wtime();
+        schur_solve(pv, v, 0);
+        tm.chol += wtime() - tc;
+        std::vector<double> q2(m);
+        for (int i = 0; i < m; i++) q2[i] = 2.0 * P.b[i] - pv[i];
+        const double den = dot(q2, v) + c2 + kap / tau;
+        if (!(den > 0) || !std::isfinite(den)) { status = 4; break; }
+        // one direction: returns dtau, dkappa; dy, dZ, dX on the device / host
+        auto direction = [&](double smu, double eta, bool corr, double dtdk, double cq, double &dt, double &dk) {
+            for (int i = 0; i < m; i++)
+                rhs[i] = eta * rp[i] - smu * a0[i] + AX[i] + eta * hv[i] + (corr ? qv[i] : 0.0);
+            double t1 = wtime();
+            schur_solve(rhs, u, corr ? 0 : 1e-7);
+            tm.chol += wtime() - t1;
+            t1 = wtime();
+            const double rg_rhs = eta * rg + smu * cz - cx - eta * c3 - cq + (smu - tau * kap - dtdk) / tau;
+            dt = (rg_rhs - dot(q2, u)) / den;
+            for (int i = 0; i < m; i++) dy[i] = u[i] + v[i] * dt;
+            atop_cat(dy, -1.0, 0.0, cat.dZ);
+            lincomb_cat(dt, Ccat, 1.0, cat.dZ, eta, cat.Fd, cat.dZ);      // dZ = C dt - A'dy + eta Rd
+            mul_all(1.0, &DevArrays::Zi, &DevArrays::dZ, &DevArrays::T);
+            mul_all(1.0, &DevArrays::T, &DevArrays::X, &DevArrays::G);    // Zi dZ X
+            if (corr) lincomb_cat(1.0, cat.G, 1.0, cat.Q, 0.0, nullptr, cat.G);
+            sym_cat(cat.G, -1.0, smu, cat.Zi, -1.0, cat.X, cat.dX);       // -sym(.) + smu Zi - X
+            dk = (smu - tau * kap - dtdk - kap * dt) / tau;
+            tm.dense += wtime() - t1;
+        };
+        auto ratio = [](double x, double dx) { return dx < 0 ? -x / dx : 1e30; };
+        // ---- predictor ----
+        double dtp = 0, dkp = 0;
+        direction(0.0, 1.0, false, 0.0, 0.0, dtp, dkp);
+        double tst = wtime();
+        const double apx = maxstep(1, opt.lanczos_k), apz = maxstep(0, opt.lanczos_k);
+        tm.step += wtime() - tst;
+        const double ap = std::min(1.0, std::min(std::min(apx, apz), std::min(ratio(tau, dtp), ratio(kap, dkp))));
+        double xdz = 0, dxz = 0, dxdz = 0;
+        {
+            double t3[3];
+            const double *aa[3] = {cat.X, cat.dX, cat.dX}, *bb[3] = {cat.dZ, cat.Z, cat.dZ};
+            dots_cat(3, aa, bb, t3);
+            xdz = t3[0]; dxz = t3[1]; dxdz = t3[2];
+        }
+        const double mu_a = (xz + ap * (xdz + dxz) + ap * ap * dxdz + (tau + ap * dtp) * (kap + ap * dkp)) / (Ntot + 1);
+        const double expon = R.relgap > 1e-6 ? std::max(1.0, 3.0 * ap * ap) : 3.0;
+        sigma = std::min(1.0, std::pow(std::max(0.0, mu_a / mu), expon));
+        if (sigma < opt.sigma_min) sigma = opt.sigma_min;
+        // ---- corrector ----
+        td = wtime();
+        mul_all(1.0, &DevArrays::Zi, &DevArrays::dZ, &DevArrays::T);
+        mul_all(1.0, &DevArrays::T, &DevArrays::dX, &DevArrays::Q);       // Q = Zi dZp dXp
+        aop_cat(cat.Q, qv);
+        double cq = 0;
+        {
+            const double *aa[1] = {Ccat}, *bb[1] = {cat.Q};
+            dots_cat(1, aa, bb, &cq);
+        }
+        tm.dense += wtime() - td;
+        double dt = 0, dk = 0;
+        direction(sigma * mu, 1.0 - sigma, true, dtp * dkp, cq, dt, dk);
+        tst = wtime();
+        const double ax = maxstep(1, opt.lanczos_k), az = maxstep(0, opt.lanczos_k);
+        tm.step += wtime() - tst;
+        const double amax = std::min(std::min(ax, az), std::min(ratio(tau, dt), ratio(kap, dk)));
+        const double gamma = 0.9 + (opt.gamma_max - 0.9) * std::min(1.0, amax);
+        double a = std::min(1.0, gamma * amax);
+        // one step for every variable: Z first, then X; Z moved back if X needed a shorter one
+        tst = wtime();
+        int ok = try_step(0, &a);
+        const double a_z = a;
+        ok = ok && try_step(1, &a);
+        if (ok && a < a_z) {
+            const double a_x = a;
+            ok = try_step(0, &a, a_z);
+            if (ok && a < a_x) ok = try_step(1, &a, a_x);
+        }
+        for (int k : big_ids) inv_from_chol(db[k].n, da[k].LX, da[k].dinvX, da[k].LiX);
+        tm.step += wtime() - tst;
+        if (!ok) { status = 4; break; }
+        for (int i = 0; i < m; i++) y[i] += a * dy[i];
+        tau += a * dt;
+        kap += a * dk;
+        if (opt.verbose > 1)
+            log_printf(0, "     [schur %.3fs %s, factor %s reg %.0e pmin %.1e, pcg %d, step %.3fs, tau %.3e kappa %.3e]\n",
+                       tm.schur - ts_before, asm_label, is_float ? "fp32" : "fp64", reg, min_pivot, pcg_iters,
+                       tm.step - tstep_before, tau, kap);
+        alpha = a;
+        stall = a < 1e-6 ? stall + 1 : 0;
+    }
+    res.iters = it;
+    res.direction = 0;
+    res.embedding = 1;
+    nt_mode = nt_saved;
+    if (status != 0 && status != 1 && status != 2 && best_score < res_score(R)) {
+        R = best;
+        y = ybest;
+        tau = tau_best;
+        CU(cudaMemcpyAsync(cat.X, cat.Xb, sizeof(double) * Ntot2, cudaMemcpyDeviceToDevice, g.st));
+        CU(cudaMemcpyAsync(cat.Z, cat.Zb, sizeof(double) * Ntot2, cudaMemcpyDeviceToDevice, g.st));
+        if (opt.verbose > 1) log_printf(0, "   returning best iterate (iteration %d)\n", it_best);
+    }
+    // the solution of the embedding: X / tau, y / tau (final_measures takes Z as C - A'y)
+    lincomb_cat(1.0 / tau, cat.X, 0.0, nullptr, 0.0, nullptr, cat.X);
+    for (int i = 0; i < m; i++) y[i] /= tau;
+    final_measures(y, res);
     const double acc = std::max(std::max(res.err[1], res.err[2]),
                                 std::max(res.err[4], std::max(std::fabs(res.err[5]), std::fabs(res.err[6]))));
     if (status == 0 || status == 5 || status == 3 || status == 4 || status == 6) {
@@ -2862,21 +3176,53 @@ static int solve_impl(const InputView &in, const Options &opt, ResultData &res, 
         log_printf(0, "BRISK-B200 %s interior-point SDP solver (Newton step on the GPU)\n", "1.7");
         log_printf(0, "problem: m = %d, %d SDP blocks (max n = %d)\n", in.m, in.nblk, nmax);
     }
+    // the method (solver.c:13519-13560): the self-dual embedding with -hsd; without -hsd or
+    // -nohsd the reference's rule: the embedding first when its dense work (12 sum n^3 over the
+    // semidefinite blocks) is at most the Schur factor's m^3/3, or half of factor and assembly (the
+    // row-product route's 2 n^3 a constraint here), or the whole is under 1e7 flops; the
+    // infeasible-start method runs again from the start when the embedding stops short.  The
+    // embedding takes the HKM direction (solver.c:13566).
+    bool use_hsd = opt.hsd == 1;
+    if (opt.hsd < 0) {
+        double n3 = 0, asm_fl = 0;
+        for (size_t k = 0; k < P.in_n.size(); k++)
+            if (P.in_n[k] > 0) {
+                const double nk = P.in_n[k];
+                n3 += nk * nk * nk;
+                asm_fl += 2.0 * nk * nk * nk * (double)P.blk[P.in_first[k]].con.size();
+            }
+        const double fac = (double)in.m * in.m * in.m / 3.0, dense = 12.0 * n3;
+        use_hsd = dense <= fac || dense <= 0.5 * (fac + asm_fl) || fac + dense < 1e7;
+        if (use_hsd && opt.verbose > 0)
+            log_printf(0, "   self-dual embedding first (dense work %.1e, Schur factor %.1e, assembly %.1e)\n", dense, fac,
+                       asm_fl);
+    }
+    Options sopt = opt;
+    if (use_hsd) sopt.direction = 0;
     try {
-        Solver S(P, opt, arena);
+        Solver S(P, sopt, arena);
         const double tsu = wtime();
         S.setup();
         const double t1 = wtime();
         if (opt.verbose > 1) log_printf(0, "   [device setup and upload %.3fs]\n", t1 - tsu);
-        int rc = S.run(res);
+        int rc = use_hsd ? S.run_hsd(res) : S.run(res);
+        if (use_hsd && opt.hsd < 0 && res.status != 0 && res.status != 1 && res.status != 2 && res.status != 6) {
+            if (opt.verbose > 0)
+                log_printf(0, "   the embedding stopped short (%s): the infeasible-start method from the start\n",
+                           status_string(res.status));
+            const int it_hsd = res.iters;
+            rc = S.run(res);
+            res.iters += it_hsd;
+        }
         blocks_as_given(P, res);
         res.t.setup = t1 - t0;
         res.h2d_bytes = S.upload_bytes;
         res.time = wtime() - t0;
         if (opt.verbose > 0) {
             log_printf(0, "status: %s   iterations: %d\n", status_string(res.status), res.iters);
-            log_printf(0, "  Solve:             interior-point method: infeasible start, %s direction, %d iterations\n",
-                       res.direction == 1 ? "NT" : "HKM", res.iters);
+            log_printf(0, "  Solve:             interior-point method: %s, %s direction, %d iterations\n",
+                       res.embedding ? "self-dual embedding" : "infeasible start", res.direction == 1 ? "NT" : "HKM",
+                       res.iters);
             log_printf(0, "  primal obj <C,X> = %.10e   dual obj b'y = %.10e\n", res.pobj, res.dobj);
             log_printf(0, "  DIMACS errors: %.1e %.1e %.1e %.1e %.1e %.1e\n", res.err[1], res.err[2], res.err[3],
                        res.err[4], res.err[5], res.err[6]);
@@ -3150,7 +3496,7 @@ int session_solve(Session *s, const Options &opt, ResultData &res) {
     res.bs = s->bs;
     s->S->set_options(opt);
     try {
-        const int rc = s->S->run(res);
+        const int rc = opt.hsd == 1 ? s->S->run_hsd(res) : s->S->run(res);   // (-hsd only: no automatic rule here)
         blocks_as_given(s->P, res);
         return rc;
     } catch (const GpuFail &f) {

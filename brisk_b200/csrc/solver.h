@@ -101,6 +101,8 @@ struct Options {
     int direction = -1;         // -1 auto (solver.c:13585-13591), 0 HKM, 1 NT
     int route = -1;             // Schur route per block: -1 auto (dense when the constraints average >= 2 % of
                                 // n^2 entries, problem.c:1299), 0 row-product, 1 dense
+    int hsd = -1;               // the self-dual embedding: -hsd 1, -nohsd 0, -1 the reference's rule
+                                // (solver.c:13519-13560: the embedding first where its dense work is small)
     int batch_tune = 1;         // the lockstep batch's work-item autotuner (-batchtune 0|1)
     int lowrank = -1;           // the low-rank Schur route (-lowrank, problem.c:972): -1 where it is cheaper
                                 // (every constraint of the block of low rank), 0 off, 1 wherever it applies
@@ -116,6 +118,7 @@ struct ResultData {
     int exit_code = 0;
     int iters = 0;
     int direction = 0;          // the search direction taken: 0 HKM, 1 NT
+    int embedding = 0;          // 1: solved by the self-dual embedding (Solver::run_hsd)
     int have_x = 0;
     int m = 0, nblk = 0;
     std::vector<int> bs;

@@ -233,6 +233,42 @@ def lowrank_sdp(n: int = 100, m: int = 300, max_rank: int = 3, support: int = 0,
                     meta=dict(kind="lowrank", n=n, m=m, max_rank=max_rank, support=support, seed=seed))
 
 
+def infeasible_sdp(kind: str = "primal", n: int = 6, m: int = 8, seed: int = 0) -> SdpaData:
+    """A seeded infeasible SDP (one n x n block).  kind "primal": A_1 = I with b_1 = -1 (no X >= 0
+    has a negative trace) and m - 1 random sparse constraints b = A(I); the dual is unbounded.
+    kind "dual": C = -E_11 (minimize -X_11) with constraints that leave X_11 free to grow (m
+    random constraints on the other rows and columns, b = A(I)); the primal is unbounded, the dual
+    infeasible.  C otherwise G G'/n + I."""
+    rng = np.random.default_rng(seed)
+    G = rng.standard_normal((n, n))
+    C = G @ G.T / n + np.eye(n)
+    if kind == "dual":
+        C = np.zeros((n, n))
+        C[0, 0] = -1.0
+    iu, ju = np.triu_indices(n)
+    keep = C[iu, ju] != 0
+    mats, ii, jj, vv = [np.zeros(int(keep.sum()), np.int32)], [iu[keep] + 1], [ju[keep] + 1], [-C[iu, ju][keep]]
+    b = np.zeros(m)
+    for t in range(m):
+        A = np.zeros((n, n))
+        if kind == "primal" and t == 0:
+            A = np.eye(n)
+        else:
+            lo = 1 if kind == "dual" else 0
+            for _ in range(3):
+                p, q = rng.integers(lo, n, size=2)
+                v = rng.standard_normal()
+                A[p, q] += v
+                A[q, p] = A[p, q]
+        nzr, nzc = np.nonzero(np.triu(A))
+        mats.append(np.full(nzr.size, t + 1, np.int32)); ii.append(nzr + 1); jj.append(nzc + 1); vv.append(A[nzr, nzc])
+        b[t] = -1.0 if (kind == "primal" and t == 0) else np.trace(A)
+    mat = np.concatenate(mats)
+    d = _normalise(mat, np.ones(mat.size, np.int32), np.concatenate(ii), np.concatenate(jj), np.concatenate(vv))
+    return SdpaData(np.array([n], np.int32), b, *d, name=f"infeasible_{kind}_n{n}_m{m}_seed{seed}",
+                    meta=dict(kind="infeasible", which=kind, n=n, m=m, seed=seed))
+
+
 def random_dense_instance(rng, n: int, m: int, name: str = "") -> SdpaData:
     """One small dense instance: A_i dense N(0,1) symmetric, b = A(I), C = G G'/n + I."""
     iu, ju = np.triu_indices(n)

@@ -26,8 +26,8 @@ import tempfile
 
 ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 sys.path.insert(0, ROOT)
-from brisk_b200.problems import (batch_instance, dense_instance, lowrank_sdp, moment_relaxation, random_sdp,  # noqa: E402
-                                 sdp_lp_problem, theta_problem, write_sdpa)
+from brisk_b200.problems import (batch_instance, dense_instance, infeasible_sdp, lowrank_sdp,  # noqa: E402
+                                 moment_relaxation, random_sdp, sdp_lp_problem, theta_problem, write_sdpa)
 
 REF = os.path.join(ROOT, "oracle", "_ref", "brisk_ref")
 OUT = os.path.join(ROOT, "tests", "golden", "ref_runs.json")
@@ -50,6 +50,9 @@ INSTANCES = {
     # constraints of rank 1-3: dense vectors (the reference's low-rank route), and on 20 of 80 rows
     "lowrank80": (lowrank_sdp, dict(n=80, m=200, max_rank=3, support=0, seed=6)),
     "lowrank80s": (lowrank_sdp, dict(n=80, m=150, max_rank=2, support=20, seed=7)),
+    # infeasible problems: no X >= 0 with trace -1 (primal), an unbounded primal (dual)
+    "infeas_p": (infeasible_sdp, dict(kind="primal", n=6, m=8, seed=1)),
+    "infeas_d": (infeasible_sdp, dict(kind="dual", n=6, m=5, seed=2)),
     "lp_dense": (sdp_lp_problem, dict(blocks=(20, -300), m=80, density=0.1, lp_per_con=5, seed=5, dense_rows=2)),
 }
 # instances of the 4096-instance uneven batch (n ~ U{8..64}, m ~ U{n..n(n+1)/4}, seed 0): the

@@ -188,15 +188,17 @@ def test_lp_blocks_match_reference(golden, name, run, opts):
                                   "batch_q5"])
 def test_default_options_against_the_reference_automatic_method(golden, name):
     """Without -nohsd the reference chooses its method itself and runs the self-dual embedding
-    first on these problems (its recorded "hsd_auto" runs, presolves off); this build has no
-    embedding and runs the infeasible-start method (it notes -hsd when asked for it).  The two
-    reach the same optimum: the same status, (pobj + dobj) / 2 within 1e-7 relative, each
-    objective within 1e-7 of the DIMACS denominator, DIMACS <= 1e-7.  The iteration counts
-    differ, by design: the embedding took 5-7 iterations on these instances where the
-    infeasible-start method takes 10-13 (the reference's own -nohsd runs take the same 10-13)."""
+    first on these problems (its recorded "hsd_auto" runs, presolves off); this build takes the
+    same rule (solver.c:13519-13560) and runs its own embedding (Solver::run_hsd).  The two reach
+    the same optimum: the same status, (pobj + dobj) / 2 within 1e-7 relative, each objective
+    within 1e-7 of the DIMACS denominator, DIMACS <= 1e-7.  The iteration counts differ, by
+    design: the reference's embedding (correctors, end phases) took 5-7 iterations on these
+    instances, this one takes 10-13, as the infeasible-start method does."""
     e = golden[name]
     ref = e["runs"]["hsd_auto"]
-    res = brisk_b200.solve_sdpa(*make(e).args(), options=["-dir", "hkm", "-mixed", "0", "-tol", "1e-7"], verbose=False)
+    res = brisk_b200.solve_sdpa(*make(e).args(), options=["-dir", "hkm", "-mixed", "0", "-tol", "1e-7", "-v"],
+                                verbose=False)
+    assert "self-dual embedding first" in res.log
     assert res.status_str == ref["status"], res.log
     objectives_close(res.pobj, res.dobj, ref["pobj"], ref["dobj"])
     assert np.max(np.abs(res.dimacs)) <= 1e-7, res.dimacs
