@@ -19,6 +19,11 @@ WORKLOADS = {
     "rand1000": lambda: problems.random_sdp(n=1000, m=8000, density=0.005, seed=0),
     "mom60": lambda: problems.moment_relaxation(nvars=60, clique=4, seed=0),
     "mom700": lambda: problems.moment_relaxation(nvars=700, clique=4, seed=0),
+    # an SDP block of 20 and an LP block of 300 variables, two rows over all of them (the LP route)
+    "lp_dense": lambda: problems.sdp_lp_problem(blocks=(20, -300), m=80, density=0.1, lp_per_con=5, seed=5,
+                                                dense_rows=2),
+    # constraints of rank 1-3 with dense vectors (the low-rank route)
+    "lowrank80": lambda: problems.lowrank_sdp(n=80, m=200, max_rank=3, support=0, seed=6),
 }
 
 
