@@ -870,7 +870,7 @@ class Solver {
     void setup();                 // upload the scaled problem and allocate the device state
     int run(ResultData &res);     // one solve from the resident data
     int run_hsd(ResultData &res); // the same by the self-dual embedding (HKM)
-    void start_sdpt3();
+    void start_sdpt3(bool unit = false);   // unit: X = Z = I (the embedding's start)
     void set_options(const Options &o) { opt = o; }
     ~Solver() {
         schol::release(sp_f);
@@ -2391,7 +2391,7 @@ static double dimacs_score(const IterRes &R) {
 // start_sdpt3 (solver.c:6622-6661): X = xi I, Z = eta I per block, their factors, the factors'
 // diagonal-block inverses and the inverses of the factors.  An LP block as given takes one xi and
 // one eta, from its order N and the norms over all its variables, for each of its blocks of order 1.
-void Solver::start_sdpt3() {
+void Solver::start_sdpt3(bool unit) {
     std::vector<std::vector<double>> sval(6, std::vector<double>(nb, 0.0));
     std::vector<double> lp_xi(nb, 0.0), lp_eta(nb, 0.0);
     for (size_t kin = 0; kin < P.in_n.size(); kin++) {
@@ -2438,8 +2438,9 @@ void Solver::start_sdpt3() {
             ratio = std::max(ratio, (1 + std::fabs(P.b[B.con[t]])) / (1 + a));
         }
         const bool lp = lp_xi[k] > 0;
-        const double xi = lp ? lp_xi[k] : std::max(10.0, std::max(std::sqrt((double)n), n * ratio));
-        const double eta = lp ? lp_eta[k] : std::max(10.0, std::max(std::sqrt((double)n), std::max(maxA, nC)));
+        double xi = lp ? lp_xi[k] : std::max(10.0, std::max(std::sqrt((double)n), n * ratio));
+        double eta = lp ? lp_eta[k] : std::max(10.0, std::max(std::sqrt((double)n), std::max(maxA, nC)));
+        if (unit) xi = eta = 1.0;
         DevArrays &d = da[k];
         if (n <= SMALL_N_MAX) {   // set below for all small blocks at once (closed form)
             sval[0][k] = xi;
@@ -2853,11 +2854,14 @@ int Solver::run(ResultData &res) {
 //     M dy - p dtau = eta rp - sigma mu A(Zi) + A(X) + eta A(Zi Rd X) + A(Q),   p = A(Zi C X) + b,
 //     (2b - p)'dy + (<C, Zi C X> + kappa / tau) dtau =
 //         eta rg + sigma mu <C, Zi> - <C, X> - eta <C, Zi Rd X> - <C, Q> + (sigma mu - tau kappa - dtau_p dkappa_p) / tau,
-// so dy = u + v dtau with M u = (the first right side) and M v = p: three Schur solves an
-// iteration, as the infeasible method takes.  One step length for every variable keeps the
+// so dy = u + v dtau with M u = (the first right side) and M v = p; dtau's coefficient and right
+// side are evaluated in a cancellation-free form (below): four Schur solves an iteration, one
+// factor.  One step length for every variable keeps the
 // residuals falling together.  The solution is X / tau, y / tau; kappa >> tau certifies
-// infeasibility (b'y > 0: primal, <C,X> < 0: dual).  The start is start_sdpt3's X and Z with
-// tau = 1 and kappa = <X,Z> / N (on the central path).
+// infeasibility (b'y > 0: primal, <C,X> < 0: dual).  The start is X = Z = I on the equilibrated
+// problem (its rows and C scaled to norm 1), tau = 1 and kappa = <X,Z> / N = 1, on the central
+// path: in a dense prototype it took 1-3 iterations fewer than start_sdpt3's xi I, eta I on every
+// parity instance.
 int Solver::run_hsd(ResultData &res) {
     const double t0 = wtime();
     tm = Timings();
@@ -2873,10 +2877,7 @@ int Solver::run_hsd(ResultData &res) {
     const bool nt_saved = nt_mode;   // a session's solver keeps its own direction for run()
     nt_mode = false;
     std::vector<double> y(m, 0.0), ybest(m, 0.0), rp(m), a0, pv, hv, qv, rhs(m), u, v, dy(m), tmpv, AX;
-    start_sdpt3();
-    // C as an iterate-shaped array for the products Zi C X (R0, the infeasible method's residual
-    // base, is not used here)
-    CU(cudaMemcpyAsync(cat.R0, Ccat, sizeof(double) * Ntot2, cudaMemcpyDeviceToDevice, g.st));
+    start_sdpt3(true);
     const double Ntot = (double)P.Ntot;
     double tau = 1.0, kap = 0.0;
     {
@@ -2986,40 +2987,59 @@ int Solver::run_hsd(ResultData &res) {
         if (cur_prec == 1 && !asm_fp64 && min_pivot < 1e-4) asm_fp64 = true;
         tm.chol += wtime() - tc;
         // ---- the pieces both directions share ----
+        // dy = u + (v1 + w) dtau with M v1 = A(Zi C X), M w = b.  The third equation's coefficient
+        // of dtau, (2b - p)'v + <C, Zi C X> + kappa/tau, is the difference of two terms that grow
+        // like 1/mu; it equals the sum of three non-negative ones,
+        //     den = b'w + <R, Zi R X> + kappa/tau,   R = C - A'v1,
+        // and the right side likewise loses its 1/mu terms when written with R (below), so both
+        // keep their accuracy to the end of the solve whatever the solves' residuals.
+        // (scratch: the PCG's matrix-free operator, newton_mv, overwrites F, W and T, so what must
+        // outlive a solve sits in R0 (C, then R) and Fd (Rd))
         td = wtime();
+        CU(cudaMemcpyAsync(cat.R0, Ccat, sizeof(double) * Ntot2, cudaMemcpyDeviceToDevice, g.st));
         aop_cat(cat.Zi, a0);                                             // A(Zi)
         mul_all(1.0, &DevArrays::Zi, &DevArrays::R0, &DevArrays::T);     // Zi C
         mul_all(1.0, &DevArrays::T, &DevArrays::X, &DevArrays::G);       // Zi C X
-        aop_cat(cat.G, pv);
-        for (int i = 0; i < m; i++) pv[i] += P.b[i];                     // p = A(Zi C X) + b
+        aop_cat(cat.G, pv);                                              // A(Zi C X)
         mul_all(1.0, &DevArrays::Zi, &DevArrays::Fd, &DevArrays::T);     // Zi Rd
         mul_all(1.0, &DevArrays::T, &DevArrays::X, &DevArrays::W);       // Zi Rd X
         aop_cat(cat.W, hv);
-        double c2 = 0, cz = 0, c3 = 0;
-        {
-            double part[3];
-            const double *aa[3] = {Ccat, Ccat, Ccat}, *bb[3] = {cat.G, cat.Zi, cat.W};
-            dots_cat(3, aa, bb, part);
-            c2 = part[0]; cz = part[1]; c3 = part[2];
-        }
         tm.dense += wtime() - td;
         tc = wtime();
-        schur_solve(pv, v, 0);
+        schur_solve(pv, v, 0);                                           // v1
+        std::vector<double> wv;
+        schur_solve(P.b, wv, 0);                                         // w
         tm.chol += wtime() - tc;
-        std::vector<double> q2(m);
-        for (int i = 0; i < m; i++) q2[i] = 2.0 * P.b[i] - pv[i];
-        const double den = dot(q2, v) + c2 + kap / tau;
+        td = wtime();
+        atop_cat(v, -1.0, 0.0, cat.R0);
+        lincomb_cat(1.0, Ccat, 1.0, cat.R0, 0.0, nullptr, cat.R0);       // R = C - A'v1
+        mul_all(1.0, &DevArrays::Zi, &DevArrays::R0, &DevArrays::T);
+        mul_all(1.0, &DevArrays::T, &DevArrays::X, &DevArrays::G);       // Zi R X
+        double rwr = 0, rzi = 0, rx = 0, rw = 0;
+        {   // <R, Zi Rd X> as <Rd, Zi R X> (equal: tr(R Zi Rd X) = tr(Rd Zi R X))
+            double part[4];
+            const double *aa[4] = {cat.R0, cat.R0, cat.R0, cat.Fd}, *bb[4] = {cat.G, cat.Zi, cat.X, cat.G};
+            dots_cat(4, aa, bb, part);
+            rwr = part[0]; rzi = part[1]; rx = part[2]; rw = part[3];
+        }
+        tm.dense += wtime() - td;
+        const double den = dot(P.b, wv) + rwr + kap / tau;
         if (!(den > 0) || !std::isfinite(den)) { status = 4; break; }
-        // one direction: returns dtau, dkappa; dy, dZ, dX on the device / host
-        auto direction = [&](double smu, double eta, bool corr, double dtdk, double cq, double &dt, double &dk) {
+        const double v1rp = dot(v, rp);
+        for (int i = 0; i < m; i++) v[i] += wv[i];                       // v = v1 + w
+        // one direction: returns dtau, dkappa; dy, dZ, dX on the device / host.  rq = <R, Q>.
+        //   dtau = (eta rg + (smu - tau kappa - dtdk)/tau - b'u + eta v1'rp + smu <R,Zi> - <R,X>
+        //           - eta <R, Zi Rd X> - <R,Q>) / den
+        auto direction = [&](double smu, double eta, bool corr, double dtdk, double rq, double &dt, double &dk) {
             for (int i = 0; i < m; i++)
                 rhs[i] = eta * rp[i] - smu * a0[i] + AX[i] + eta * hv[i] + (corr ? qv[i] : 0.0);
             double t1 = wtime();
             schur_solve(rhs, u, corr ? 0 : 1e-7);
             tm.chol += wtime() - t1;
             t1 = wtime();
-            const double rg_rhs = eta * rg + smu * cz - cx - eta * c3 - cq + (smu - tau * kap - dtdk) / tau;
-            dt = (rg_rhs - dot(q2, u)) / den;
+            const double num = eta * rg + (smu - tau * kap - dtdk) / tau - dot(P.b, u) + eta * v1rp + smu * rzi - rx -
+                               eta * rw - rq;
+            dt = num / den;
             for (int i = 0; i < m; i++) dy[i] = u[i] + v[i] * dt;
             atop_cat(dy, -1.0, 0.0, cat.dZ);
             lincomb_cat(dt, Ccat, 1.0, cat.dZ, eta, cat.Fd, cat.dZ);      // dZ = C dt - A'dy + eta Rd
@@ -3054,9 +3074,9 @@ int Solver::run_hsd(ResultData &res) {
         mul_all(1.0, &DevArrays::Zi, &DevArrays::dZ, &DevArrays::T);
         mul_all(1.0, &DevArrays::T, &DevArrays::dX, &DevArrays::Q);       // Q = Zi dZp dXp
         aop_cat(cat.Q, qv);
-        double cq = 0;
+        double cq = 0;   // <R, Q>
         {
-            const double *aa[1] = {Ccat}, *bb[1] = {cat.Q};
+            const double *aa[1] = {cat.R0}, *bb[1] = {cat.Q};
             dots_cat(1, aa, bb, &cq);
         }
         tm.dense += wtime() - td;

@@ -5,7 +5,7 @@ against the reference's own runs of its embedding (tests/golden/ref_runs.json "h
 status and exit code, (pobj + dobj) / 2 within 1e-7 relative and each objective within 1e-7 of
 the DIMACS denominator (parity.objectives_close: the two embeddings stop at different iterates),
 DIMACS errors <= 1e-7.  The reference's embedding, with its correctors and end phases, takes 4-7
-iterations here; this one the infeasible method's 10-13."""
+iterations here; this one 8-12 (the infeasible method 9-14)."""
 import numpy as np
 import pytest
 

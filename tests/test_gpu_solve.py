@@ -193,7 +193,7 @@ def test_default_options_against_the_reference_automatic_method(golden, name):
     the same optimum: the same status, (pobj + dobj) / 2 within 1e-7 relative, each objective
     within 1e-7 of the DIMACS denominator, DIMACS <= 1e-7.  The iteration counts differ, by
     design: the reference's embedding (correctors, end phases) took 5-7 iterations on these
-    instances, this one takes 10-13, as the infeasible-start method does."""
+    instances, this one 8-12 (the infeasible-start method 9-14)."""
     e = golden[name]
     ref = e["runs"]["hsd_auto"]
     res = brisk_b200.solve_sdpa(*make(e).args(), options=["-dir", "hkm", "-mixed", "0", "-tol", "1e-7", "-v"],
