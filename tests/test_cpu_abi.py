@@ -192,3 +192,22 @@ def test_options_that_change_the_method_are_noted(libpath):
                              options=["-nohsd", "-sym", "none", "-symalg", "0", "-chordal", "0", "-deprows", "0",
                                       "-corr", "0", "-nofr", "-tol", "x"], verbose=False)
     assert quiet.exit_code == 1 and "note" not in quiet.log
+
+
+@pytest.mark.parametrize("opt,val,msg", [("-lowrank", "2", "bad -lowrank"), ("-batchtune", "x", "bad -batchtune"),
+                                         ("-lowrank", "abc", "bad -lowrank")])
+def test_new_options_refuse_bad_values(libpath, opt, val, msg):
+    """-lowrank (-1 auto, 0 off, 1 force: the reference's values) and -batchtune (0 or 1) refuse
+    other values with exit code 1 and a message, before any device work."""
+    from brisk_b200 import _core
+    res = _core.solve_sdpa([2], [1.0], [1], [1], [1], [1], [1.0], options=[opt, val], verbose=False)
+    assert res.exit_code == 1 and msg in res.log, res.log
+
+
+def test_method_flags_are_accepted_silently(libpath):
+    """-hsd and -nohsd choose the method (the embedding, the infeasible-start method) and print no
+    note; a bad -tol after them still stops the solve at the options."""
+    from brisk_b200 import _core
+    for flag in ("-hsd", "-nohsd"):
+        res = _core.solve_sdpa([2], [1.0], [1], [1], [1], [1], [1.0], options=[flag, "-tol", "x"], verbose=False)
+        assert res.exit_code == 1 and "bad -tol" in res.log and "note" not in res.log
