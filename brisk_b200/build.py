@@ -23,7 +23,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
          "--expt-relaxed-constexpr", "-I" + CSRC, "-I" + os.path.join(ROOT, "include")]
 
-SOURCES = ["gemm_f64.cu", "dense.cu", "schur.cu", "elementwise.cu", "tf32x3.cu", "small.cu", "sparse.cu", "lockstep.cu", "nt.cu", "ozaki.cu", "lowrank.cu", "solver.cu",
+SOURCES = ["gemm_f64.cu", "dense.cu", "schur.cu", "elementwise.cu", "tf32x3.cu", "small.cu", "sparse.cu", "lockstep.cu", "nt.cu", "ozaki.cu", "lowrank.cu", "lanczos.cu", "solver.cu",
            "bgpu.cu", "capi.cpp", "sdpa.cpp"]
 
 

@@ -70,6 +70,19 @@ int trtri_f64(cudaStream_t st, int n, const double *L, long long lda, const doub
 // y = alpha M x + beta y, M symmetric and stored in full (column-major, ldm).
 int symv_full_f64(cudaStream_t st, int n, double alpha, const double *M, long long ldm, const double *x, double beta,
                   double *y);
+// The step-length Lanczos on the device (lanczos.cu).  lanczos_start: Q[0] = q0 / |q0| (first n
+// entries of q0) and the state reset; lanczos_step j (0 <= j < K <= 30), after w = B Q[j]:
+// alpha_j, w orthogonalised twice against Q[0..j], beta_j, the stop test, Q[j+1] = w / beta_j;
+// once done, lam = theta - res of the last T (or -1e300 when no bound exists) and the later steps
+// are no-ops.  Q holds (K + 1) n doubles.
+struct LanczosState {
+    double alpha[32], beta[32];
+    double scale, lam;
+    int kk, done;
+};
+int lanczos_start(cudaStream_t st, int n, const double *q0, double *Q, LanczosState *s);
+int lanczos_step(cudaStream_t st, int n, int j, int K, double *Q, double *w, LanczosState *s);
+
 // y = M x reading only the pattern's entries (rowptr/cols: each row's columns, both triangles and
 // the diagonal, ascending; entries of M off the pattern must be zero)
 int pattern_symv_f64(cudaStream_t st, int n, const long long *rowptr, const int *cols, const double *M, long long ldm,

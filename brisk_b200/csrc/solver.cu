@@ -647,82 +647,6 @@ static int build_problem(const InputView &in, HProblem &P, std::string &err) {
     return 0;
 }
 
-// ---------------------------------------------------------------------------------------------
-// small host numerics: the Ritz bound of the Lanczos step length
-// ---------------------------------------------------------------------------------------------
-// Smallest eigenvalue theta of the symmetric tridiagonal T (alpha[0..k-1], beta[0..k-2]) by
-// Sturm-count bisection, and the residual bound |beta[k-1] z[k-1]| of its unit eigenvector z by
-// inverse iteration (the quantities ritz_bound, solver.c:6030-6039, takes from dstev).
-static double sturm_below(int k, const double *a, const double *b, double x) {
-    int cnt = 0;
-    double q = a[0] - x;
-    if (q < 0) cnt++;
-    for (int i = 1; i < k; i++) {
-        if (q == 0) q = 1e-300;
-        q = (a[i] - x) - b[i - 1] * b[i - 1] / q;
-        if (q < 0) cnt++;
-    }
-    return cnt;
-}
-static double ritz_bound(int k, const double *alpha, const double *beta, double *theta) {
-    double lo = 1e300, hi = -1e300;
-    for (int i = 0; i < k; i++) {
-        const double r = (i > 0 ? std::fabs(beta[i - 1]) : 0) + (i + 1 < k ? std::fabs(beta[i]) : 0);
-        lo = std::min(lo, alpha[i] - r);
-        hi = std::max(hi, alpha[i] + r);
-    }
-    if (!std::isfinite(lo) || !std::isfinite(hi)) { *theta = 0; return 1e300; }
-    for (int it = 0; it < 200; it++) {
-        const double mid = 0.5 * (lo + hi);
-        if (mid <= lo || mid >= hi) break;
-        if (sturm_below(k, alpha, beta, mid) >= 1) hi = mid; else lo = mid;
-    }
-    const double th = 0.5 * (lo + hi);
-    *theta = th;
-    const double scale = std::max(std::fabs(lo), std::fabs(hi));
-    if (!(scale > 1e-280)) return std::fabs(beta[k - 1]);   // a zero operator: theta = 0, |z_k| <= 1
-    // inverse iteration on T - (th - delta) I, dense Gaussian elimination with partial pivoting
-    const double sh = th - 1e-10 * scale;
-    double z[64], A[64 * 64], w[64];
-    for (int i = 0; i < k; i++) z[i] = 1.0 / std::sqrt((double)k) * (1.0 + 0.01 * i);
-    for (int pass = 0; pass < 3; pass++) {
-        for (int i = 0; i < k * k; i++) A[i] = 0;
-        for (int i = 0; i < k; i++) {
-            A[i + i * k] = alpha[i] - sh;
-            if (i + 1 < k) { A[i + (i + 1) * k] = beta[i]; A[(i + 1) + i * k] = beta[i]; }
-        }
-        for (int i = 0; i < k; i++) w[i] = z[i];
-        for (int c = 0; c < k; c++) {
-            int piv = c;
-            for (int r = c + 1; r < k; r++) if (std::fabs(A[r + c * k]) > std::fabs(A[piv + c * k])) piv = r;
-            if (piv != c) {
-                for (int j = 0; j < k; j++) std::swap(A[c + j * k], A[piv + j * k]);
-                std::swap(w[c], w[piv]);
-            }
-            double d = A[c + c * k];
-            if (d == 0) d = A[c + c * k] = 1e-300;
-            for (int r = c + 1; r < k; r++) {
-                const double f = A[r + c * k] / d;
-                if (f == 0) continue;
-                for (int j = c; j < k; j++) A[r + j * k] -= f * A[c + j * k];
-                w[r] -= f * w[c];
-            }
-        }
-        for (int c = k - 1; c >= 0; c--) {
-            double s = w[c];
-            for (int j = c + 1; j < k; j++) s -= A[c + j * k] * z[j];
-            z[c] = s / A[c + c * k];
-        }
-        double zmax = 0;
-        for (int i = 0; i < k; i++) zmax = std::max(zmax, std::fabs(z[i]));
-        if (!(zmax > 0) || !std::isfinite(zmax)) return std::fabs(beta[k - 1]);   // the trivial bound |z_k| <= 1
-        double nz = 0;
-        for (int i = 0; i < k; i++) { z[i] /= zmax; nz += z[i] * z[i]; }
-        nz = std::sqrt(nz);
-        for (int i = 0; i < k; i++) z[i] /= nz;
-    }
-    return std::fabs(beta[k - 1] * z[k - 1]);
-}
 
 // ---------------------------------------------------------------------------------------------
 // output
@@ -912,6 +836,11 @@ class Solver {
     std::vector<int> small_ids, big_ids;
     int *d_sns = nullptr, *d_sinfo = nullptr, *h_sinfo = nullptr;
     double *d_slam = nullptr, *h_slam = nullptr;
+    // the step-length Lanczos of the blocks of order > SMALL_N_MAX: the start vector (its first n
+    // entries for a block of order n), the Krylov basis and the state in device memory, and a
+    // pinned copy of the state for the checkpoints
+    double *lz_q0 = nullptr, *lz_Q = nullptr;
+    LanczosState *lz_st = nullptr, *h_lz = nullptr;
     std::vector<std::pair<double *DevArrays::*, double **>> stab;   // device pointer tables per array kind
     double **tab(double *DevArrays::*mem);
     // C = alpha A B (column-major n x n) on every block: per-block DMMA GEMMs for the large
@@ -1353,6 +1282,19 @@ void Solver::setup() {
     CU(cudaMemsetAsync(d_err, 0, sizeof(int), g.st));
     h_dots = g.host_alloc<double>(16);
     if (!h_dots) throw GpuFail{BGPU_ERR_NOMEM, __LINE__};
+    if (!big_ids.empty()) {
+        int nbig = 1;
+        for (int k : big_ids) nbig = std::max(nbig, P.blk[k].n);
+        std::vector<double> q0(nbig);
+        for (int i = 0; i < nbig; i++) q0[i] = 1.0 + 0.5 * std::sin(1.7 * i + 0.3);
+        lz_q0 = g.alloc<double>(nbig);
+        lz_Q = g.alloc<double>((size_t)31 * nbig);
+        lz_st = g.alloc<LanczosState>(1);
+        h_lz = g.host_alloc<LanczosState>(1);
+        if (!lz_q0 || !lz_Q || !lz_st || !h_lz) throw GpuFail{BGPU_ERR_NOMEM, __LINE__};
+        CU(cudaMemcpyAsync(lz_q0, q0.data(), sizeof(double) * nbig, cudaMemcpyHostToDevice, g.st));
+        CU(cudaStreamSynchronize(g.st));
+    }
     choose_sparse();
     allow_float = !use_sparse && (opt.mixed > 0 || (opt.mixed < 0 && m >= 1000));
     // FP32 fronts only when asked for (-mixed 1): the fronts of these problems are small and
@@ -2057,55 +1999,24 @@ double Solver::schur_solve(const std::vector<double> &rhs, std::vector<double> &
 
 // ---- step length ---------------------------------------------------------------------------
 // Lanczos on the explicit Bm = L^-1 D L^-T (sdp_maxstep_lam, solver.c:6083-6225, cold start):
-// returns lambda_min estimate theta - residual bound (conservative), or -1e300 on failure.
+// returns lambda_min estimate theta - residual bound (conservative), or -1e300 on failure.  The
+// steps run on the device (lanczos.cu); the host reads the state at the steps where the stop
+// test runs (from the sixth, every third, and the last), once each.
 double Solver::lanczos(int n, const double *Bm, int Kmax) {
     int K = std::min(n, Kmax);
     K = std::min(K, 30);
-    std::vector<double> Q((size_t)(K + 1) * n), w(n);
-    double alpha[32], beta[32];
-    double nrm0 = 0;
-    for (int i = 0; i < n; i++) { Q[i] = 1.0 + 0.5 * std::sin(1.7 * i + 0.3); nrm0 += Q[i] * Q[i]; }
-    nrm0 = 1.0 / std::sqrt(nrm0);
-    for (int i = 0; i < n; i++) Q[i] *= nrm0;
-    int kk = 0;
-    double scale = 0, theta = 0, res = 0;
-    const double lz_tol = 0.02;
+    RC(lanczos_start(g.st, n, lz_q0, lz_Q, lz_st));
     for (int j = 0; j < K; j++) {
-        double *qj = Q.data() + (size_t)j * n;
-        CU(cudaMemcpyAsync(dv_in, qj, sizeof(double) * n, cudaMemcpyHostToDevice, g.st));
-        RC(symv_full_f64(g.st, n, 1.0, Bm, n, dv_in, 0.0, dv_out));
-        CU(cudaMemcpyAsync(w.data(), dv_out, sizeof(double) * n, cudaMemcpyDeviceToHost, g.st));
-        CU(cudaStreamSynchronize(g.st));
-        double a = 0;
-        for (int i = 0; i < n; i++) a += qj[i] * w[i];
-        alpha[j] = a;
-        for (int pass = 0; pass < 2; pass++)
-            for (int i = 0; i <= j; i++) {
-                const double *qi = Q.data() + (size_t)i * n;
-                double c = 0;
-                for (int t = 0; t < n; t++) c += qi[t] * w[t];
-                for (int t = 0; t < n; t++) w[t] -= c * qi[t];
-            }
-        double b = 0;
-        for (int t = 0; t < n; t++) b += w[t] * w[t];
-        b = std::sqrt(b);
-        beta[j] = b;
-        kk = j + 1;
-        if (std::fabs(a) > scale) scale = std::fabs(a);
-        if (b <= 1e-12 * (scale + 1e-300)) { beta[j] = 0; break; }
-        if (kk >= 6 && kk % 3 == 0) {
-            res = ritz_bound(kk, alpha, beta, &theta);
-            if (res <= lz_tol * std::fabs(theta) + 1e-14 * scale) break;
-        }
-        if (j + 1 < K) {
-            double *qn = Q.data() + (size_t)(j + 1) * n;
-            const double inv = 1.0 / b;
-            for (int t = 0; t < n; t++) qn[t] = w[t] * inv;
+        RC(symv_full_f64(g.st, n, 1.0, Bm, n, lz_Q + (size_t)j * n, 0.0, dv_out));
+        RC(lanczos_step(g.st, n, j, K, lz_Q, dv_out, lz_st));
+        const int kk = j + 1;
+        if ((kk >= 6 && kk % 3 == 0) || kk == K) {
+            CU(cudaMemcpyAsync(h_lz, lz_st, sizeof(LanczosState), cudaMemcpyDeviceToHost, g.st));
+            CU(cudaStreamSynchronize(g.st));
+            if (h_lz->done) break;
         }
     }
-    res = ritz_bound(kk, alpha, beta, &theta);
-    if (res > 1e299) return -1e300;
-    return theta - res;
+    return h_lz->lam;   // (done: the last step sets it)
 }
 
 // maxstep (solver.c:6300-6390): the largest alpha with V + alpha dV >= 0 over all blocks
