@@ -36,6 +36,7 @@ from __future__ import annotations
 from dataclasses import dataclass, field
 
 import numpy as np
+from scipy.linalg import cho_factor, cho_solve
 
 
 @dataclass
@@ -408,10 +409,17 @@ def solve(data, tol=1e-8, maxit=100, gamma_max=0.99, red_acc=None, log=None, dir
         M = schur(S.A, Xp, Zi)
         if out["M0"] is None:
             out["M0"] = M.copy()
-        Minv = np.linalg.inv(M)
+        # M's Cholesky factor and triangular solves (schur_factor / schur_solve, solver.c:14671,
+        # 14796): an explicit inverse leaves A(dX) - rp at eps cond(M) |rp|, which held the late
+        # rows' primal residual near 1e-10 where the reference's reaches 1e-13
+        try:
+            Mc = cho_factor(M, lower=True)
+            msolve = lambda v: cho_solve(Mc, v)   # noqa: E731
+        except np.linalg.LinAlgError:   # numerically indefinite: partial-pivoting LU
+            msolve = lambda v: np.linalg.solve(M, v)   # noqa: E731
         a0 = aop(S.A, Zi)
         h = aop(S.A, [theta * Zk @ R @ Xk for Zk, R, Xk in zip(Zi, R0, Xp)]) if theta > 0 else np.zeros(m)
-        dy = Minv @ (S.b + h)
+        dy = msolve(S.b + h)
         dZ = [-a + theta * R for a, R in zip(atop(S.A, dy), R0)]
         dX = []
         if nt:
@@ -456,7 +464,7 @@ def solve(data, tol=1e-8, maxit=100, gamma_max=0.99, red_acc=None, log=None, dir
         else:
             Q = [Zk @ dZk @ dXk for Zk, dZk, dXk in zip(Zi, dZ, dX)]
             rhs = S.b - smu * a0 + aop(S.A, Q) + h
-        dy = Minv @ rhs
+        dy = msolve(rhs)
         dZ = [-a + theta * R for a, R in zip(atop(S.A, dy), R0)]
         dX = []
         if nt:
@@ -471,7 +479,7 @@ def solve(data, tol=1e-8, maxit=100, gamma_max=0.99, red_acc=None, log=None, dir
             ne, nrp = np.linalg.norm(ev), np.linalg.norm(rp)
             if not (ne > 1e-2 * nrp and ne > 1e-3 * tol * (1 + nbs)):
                 break
-            wv = Minv @ ev
+            wv = msolve(ev)
             Qd = atop(S.A, wv)
             Gs = []
             for Zk, Qk, Xk in zip(Zi, Qd, Xp):
