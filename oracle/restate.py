@@ -162,6 +162,7 @@ def atop(A_blocks, y):
 
 
 SMALL_BLOCK = 32     # solver.c:5944: exact eigenvalues up to this order
+SMALL_N_MAX = 64     # the CUDA path's small-block kernel (exact eigenvalues) up to this order
 LANCZOS_K = 30       # solver.c:81, and the default -lanczos (solver.c:122)
 LZ_TOL = 0.02        # solver.c:6041: the relative Ritz accuracy that ends the Lanczos steps
 
@@ -224,23 +225,24 @@ def lam_min_lanczos(L, D, kmax=LANCZOS_K):
     return theta - res
 
 
-def block_lam_min(L, D, lp=False):
+def block_lam_min(L, D, lp=False, exact_n=SMALL_BLOCK):
     """The reference's lambda_min of L^-1 D L^-T for one block: exact up to order SMALL_BLOCK
     (small_lammin) and for an LP block (the ratio test of lp_maxstep, solver.c:6227-6235, on its
-    diagonal), the Lanczos estimate above (sdp_maxstep_lam).  L None: of D itself."""
+    diagonal), the Lanczos estimate above (sdp_maxstep_lam).  L None: of D itself.  exact_n:
+    the largest order with exact eigenvalues (the CUDA path's small-block kernel takes 64)."""
     n = D.shape[0]
-    if n <= SMALL_BLOCK or lp:
+    if n <= exact_n or lp:
         if L is None:
             return float(np.linalg.eigvalsh(0.5 * (D + D.T))[0])
         return lam_min(L, D)
     return lam_min_lanczos(L, D)
 
 
-def maxstep(Ls, dVs, lp=None):
+def maxstep(Ls, dVs, lp=None, exact_n=SMALL_BLOCK):
     """maxstep (solver.c:6300-6390): 1e30 when unbounded.  lp[k]: block k is an LP block."""
     a = 1e30
     for k, (L, dV) in enumerate(zip(Ls, dVs)):
-        lam = block_lam_min(L, dV, bool(lp[k]) if lp is not None else False)
+        lam = block_lam_min(L, dV, bool(lp[k]) if lp is not None else False, exact_n)
         ak = 1e30 if lam >= 0 else -1.0 / lam
         a = min(a, ak)
     return a
@@ -524,4 +526,182 @@ def solve(data, tol=1e-8, maxit=100, gamma_max=0.99, red_acc=None, log=None, dir
             status = 4
     out.update(status=status, status_str=STATUS.get(status, "?"), iterations=it, pobj=pobj_o, dobj=dobj_o,
                dimacs=err, X=Xo, y=yo, Z=Zo, xi=xis, eta=etas, scaled=S)
+    return out
+
+
+def solve_hsd(data, tol=1e-8, maxit=100, gamma_max=0.99, red_acc=None, log=None, exact_n=SMALL_N_MAX):
+    """The homogeneous self-dual embedding as the CUDA path runs it (Solver::run_hsd, which stands
+    for the reference's hsd_run, solver.c:9803, as a method of its own: HKM direction, one
+    Mehrotra predictor-corrector step an iteration, no extra correctors or end phases), FP64,
+    dense.  With tau, kappa >= 0 the scaled problem is embedded as
+        A(X) - b tau = 0,   A'y + Z - C tau = 0,   b'y - <C,X> - kappa = 0,
+    X Z = mu I, tau kappa = mu, mu = (<X,Z> + tau kappa) / (N + 1), from X = Z = I, y = 0,
+    tau = kappa = 1 on the equilibrated problem.  The Newton system reduces to the infeasible
+    method's Schur complement M: dy = u + (v1 + w) dtau with M v1 = A(Zi C X), M w = b and M u
+    = eta rp - sigma mu A(Zi) + A(X) + eta A(Zi Rd X) + A(Q); dtau from the third equation in
+    its cancellation-free form, den = b'w + <R, Zi R X> + kappa / tau with R = C - A'v1.  One
+    step length for every variable (Z's Cholesky test first, then X's, Z moved back when X's is
+    shorter); the step lengths take exact eigenvalues up to order exact_n (the CUDA path's
+    small-block kernel: 64) and the Lanczos estimate above.  kappa > 1e8 tau ends the solve with a certificate: b'y > 0 primal infeasible,
+    <C,X> < 0 dual infeasible.  The solution is X / tau, y / tau.
+
+    The reference's own embedding takes 4-7 iterations on the parity instances where this one
+    takes 8-12 (its extra correctors), so the two agree in status and objectives, not row by
+    row.  Returns the dict of solve() (status, iterations, pobj, dobj, dimacs, the table with
+    tau and kappa per row)."""
+    if red_acc is None:
+        red_acc = max(1e-6, 100 * tol)
+    lp = [int(b) < 0 for b in data.bs]
+    S = scale_problem(data)
+    m = S.m
+    C, A, b = S.C, S.A, S.b
+    Xs = [np.eye(Ck.shape[0]) for Ck in C]
+    Zs = [np.eye(Ck.shape[0]) for Ck in C]
+    LX = [np.eye(Ck.shape[0]) for Ck in C]
+    LZ = [np.eye(Ck.shape[0]) for Ck in C]
+    y = np.zeros(m)
+    N = sum(Ck.shape[0] for Ck in C)
+    tau = 1.0
+    kap = sum(float(np.sum(X * Z)) for X, Z in zip(Xs, Zs)) / N
+
+    def ip(P_, Q_):
+        return sum(float(np.sum(p * q)) for p, q in zip(P_, Q_))
+
+    def prod(P_, Q_, R_):
+        return [p @ q @ r for p, q, r in zip(P_, Q_, R_)]
+
+    def ratio(x, dx):
+        return -x / dx if dx < 0 else 1e30
+
+    status, stall, it, it_best = -1, 0, 0, 0
+    best_score, best, saved = np.inf, None, None
+    sigma = alpha = 0.0
+    out = {"table": []}
+    for it in range(maxit + 1):
+        Zi = [np.linalg.inv(L).T @ np.linalg.inv(L) for L in LZ]
+        Zi = [0.5 * (Q + Q.T) for Q in Zi]
+        AX = aop(A, Xs)
+        rp = b * tau - AX
+        Rd = [Ck * tau - a - Zk for Ck, a, Zk in zip(C, atop(A, y), Zs)]
+        cx, xz, rd2 = ip(C, Xs), ip(Xs, Zs), ip(Rd, Rd)
+        by = float(b @ y)
+        rg = kap - by + cx
+        mu = (xz + tau * kap) / (N + 1)
+        sc = S.bs * S.cs
+        rpo = float(np.linalg.norm(rp * S.du)) / tau
+        rdo = S.cs * np.sqrt(rd2) / tau
+        po, dob = sc * cx / tau, sc * by / tau
+        pinf, dinf = rpo / (1 + S.normb2), rdo / (1 + S.normC2)
+        oden = 1 + abs(po) + abs(dob)
+        relgap = abs(po - dob) / oden
+        relcomp = sc * xz / (tau * tau) / oden
+        row = dict(it=it, pobj=-po, dobj=-dob, pinf=pinf, dinf=dinf, gap=relgap, mu=sc * xz / (tau * tau * N),
+                   tau=tau, kappa=kap)
+        out["table"].append(row)
+        if log:
+            log(f"{it:3d} {-po:+.8e} {-dob:+.8e} {pinf:.2e} {dinf:.2e} {relgap:.2e} {row['mu']:.2e} "
+                f"{alpha:.3f} {sigma:.3f} tau {tau:.3e} kappa {kap:.3e}")
+        if not (np.isfinite(po) and np.isfinite(dob) and tau > 0 and kap > 0):
+            status = 4
+            break
+        score = max(relgap, relcomp, pinf, dinf)
+        err_it = (rpo / (1 + S.normb1), rdo / (1 + S.normC1), (po - dob) / oden, relcomp)
+        if score < best_score:
+            best_score, it_best, best = score, it, err_it
+            saved = ([X.copy() for X in Xs], [Z.copy() for Z in Zs], y.copy(), tau)
+        if score < tol:
+            status = 0
+            break
+        if it > it_best and max(abs(e) for e in best) <= 0.5 * tol:
+            status = 4
+            break
+        if kap > 1e8 * tau:
+            status = 1 if by > 0 else (2 if cx < 0 else 4)
+            break
+        if it == maxit:
+            status = 3
+            break
+        if stall >= 3 or (it - it_best >= 5 and best_score < 1e-6) or it - it_best >= 12:
+            status = 4
+            break
+        M = schur(A, Xs, Zi)
+        try:
+            Mc = cho_factor(M, lower=True)
+        except np.linalg.LinAlgError:
+            status = 4
+            break
+        msolve = lambda v: cho_solve(Mc, v)   # noqa: E731
+        a0 = aop(A, Zi)
+        pv = aop(A, prod(Zi, C, Xs))
+        hv = aop(A, prod(Zi, Rd, Xs))
+        v1 = msolve(pv)
+        w = msolve(b)
+        Rm = [Ck - a for Ck, a in zip(C, atop(A, v1))]            # R = C - A'v1
+        G = prod(Zi, Rm, Xs)
+        rwr, rzi, rx, rw = ip(Rm, G), ip(Rm, Zi), ip(Rm, Xs), ip(Rd, G)
+        den = float(b @ w) + rwr + kap / tau
+        if not (den > 0 and np.isfinite(den)):
+            status = 4
+            break
+        v1rp = float(v1 @ rp)
+        v = v1 + w
+
+        def direction(smu, eta, Q, qv, rq, dtdk):
+            rhs = eta * rp - smu * a0 + AX + eta * hv + (qv if Q is not None else 0.0)
+            u = msolve(rhs)
+            num = eta * rg + (smu - tau * kap - dtdk) / tau - float(b @ u) + eta * v1rp + smu * rzi - rx \
+                - eta * rw - rq
+            dt = num / den
+            dy = u + v * dt
+            dZ = [Ck * dt - a + eta * R for Ck, a, R in zip(C, atop(A, dy), Rd)]
+            Gd = prod(Zi, dZ, Xs)
+            if Q is not None:
+                Gd = [g + q for g, q in zip(Gd, Q)]
+            dX = [-0.5 * (g + g.T) + smu * zi - x for g, zi, x in zip(Gd, Zi, Xs)]
+            dk = (smu - tau * kap - dtdk - kap * dt) / tau
+            return dX, dy, dZ, dt, dk
+
+        dXp, _, dZp, dtp, dkp = direction(0.0, 1.0, None, None, 0.0, 0.0)
+        ap = min(1.0, maxstep(LX, dXp, lp, exact_n), maxstep(LZ, dZp, lp, exact_n), ratio(tau, dtp), ratio(kap, dkp))
+        xdz, dxz, dxdz = ip(Xs, dZp), ip(dXp, Zs), ip(dXp, dZp)
+        mu_a = (xz + ap * (xdz + dxz) + ap * ap * dxdz + (tau + ap * dtp) * (kap + ap * dkp)) / (N + 1)
+        expon = max(1.0, 3.0 * ap * ap) if relgap > 1e-6 else 3.0
+        sigma = min(1.0, max(0.0, mu_a / mu) ** expon)
+        Q = prod(Zi, dZp, dXp)
+        dX, dy, dZ, dt, dk = direction(sigma * mu, 1.0 - sigma, Q, aop(A, Q), ip(Rm, Q), dtp * dkp)
+        amax = min(maxstep(LX, dX, lp, exact_n), maxstep(LZ, dZ, lp, exact_n), ratio(tau, dt), ratio(kap, dk))
+        gamma = 0.9 + (gamma_max - 0.9) * min(1.0, amax)
+        a = min(1.0, gamma * amax)
+        okz, a, Zn, LZn = try_step(Zs, dZ, a)
+        a_z = a
+        okx = False
+        if okz:
+            okx, a, Xn, LXn = try_step(Xs, dX, a)
+            if okx and a < a_z:
+                a_x = a
+                okz, a, Zn, LZn = try_step(Zs, dZ, a)
+                if okz and a < a_x:
+                    okx, a, Xn, LXn = try_step(Xs, dX, a)
+        if not (okz and okx):
+            status = 4
+            break
+        Xs, Zs, LX, LZ = Xn, Zn, LXn, LZn
+        y = y + a * dy
+        tau += a * dt
+        kap += a * dk
+        alpha = a
+        stall = stall + 1 if a < 1e-6 else 0
+    if status not in (0, 1, 2) and saved is not None and best_score < score:
+        Xs, Zs, y, tau = saved
+    err, pobj_o, dobj_o, Xo, yo, Zo = dimacs(S, [X / tau for X in Xs], y / tau)
+    acc = max(err[0], err[1], err[3], abs(err[4]), abs(err[5]))
+    if status in (0, 3, 4, 5, 6):
+        if acc <= tol:
+            status = 0
+        elif acc <= red_acc:
+            status = 5
+        elif status in (0, 5):
+            status = 4
+    out.update(status=status, status_str=STATUS.get(status, "?"), iterations=it, pobj=pobj_o, dobj=dobj_o,
+               dimacs=err, X=Xo, y=yo, Z=Zo, scaled=S, tau=tau, kappa=kap)
     return out

@@ -1,0 +1,56 @@
+"""The oracle's restatement of the self-dual embedding (oracle/restate.py: solve_hsd, the method
+of Solver::run_hsd) against the reference's own runs of its embedding (tests/golden/ref_runs.json
+"hsd_auto": without -nohsd the reference's rule, solver.c:13519-13560, picks the embedding on
+these problems).  The two embeddings take different iterates (the reference's adds correctors
+and end phases: 4-7 iterations against 8-12), so the bar is the outcome: the same status, the
+objectives by parity.objectives_close, DIMACS errors <= 1e-7, and for the infeasible instances
+the same certificate.  The CUDA path's runs are compared with this restatement in
+tests/test_gpu_hsd.py."""
+import numpy as np
+import pytest
+
+from oracle import restate
+from parity import objectives_close
+from test_cpu_oracle import make
+
+# the instances whose oracle solves take seconds (blocks of order <= 64, m <= 300)
+FAST = ["theta30", "rand30", "mom8", "dense24", "batch_q5", "lp_only"]
+
+
+@pytest.mark.parametrize("name", FAST)
+def test_oracle_embedding_matches_the_reference_embedding(golden, name):
+    e = golden[name]
+    ref = e["runs"]["hsd_auto"]
+    out = restate.solve_hsd(make(e), tol=1e-7)
+    assert out["status_str"] == ref["status"] == "OPTIMAL"
+    objectives_close(out["pobj"], out["dobj"], ref["pobj"], ref["dobj"])
+    assert np.max(np.abs(out["dimacs"])) <= 1e-7, out["dimacs"]
+    assert ref["iterations"] < out["iterations"] <= 12
+
+
+@pytest.mark.parametrize("name,status", [("infeas_p", "PRIMAL INFEASIBLE"), ("infeas_d", "DUAL INFEASIBLE")])
+def test_oracle_embedding_certifies_infeasibility(golden, name, status):
+    """tau -> 0 with kappa > 1e8 tau: b'y > 0 certifies primal infeasibility, <C,X> < 0 dual
+    infeasibility, the reference's embedding's status on the same problems."""
+    e = golden[name]
+    assert e["runs"]["hsd_auto"]["status"] == status
+    out = restate.solve_hsd(make(e), tol=1e-7)
+    assert out["status_str"] == status
+    assert out["kappa"] > 1e8 * out["tau"]
+    last = out["table"][-1]
+    if status == "PRIMAL INFEASIBLE":
+        assert last["dobj"] < 0          # the table's sign convention: -b'y / tau, b'y > 0
+    else:
+        assert last["pobj"] > 0          # -<C,X> / tau, <C,X> < 0
+
+
+def test_oracle_embedding_residuals_fall_together(golden):
+    """One step length for every variable: the embedding's residuals rp = b tau - A(X) and
+    Rd = C tau - A'y - Z fall by the same factor 1 - eta alpha an iteration (the Newton equations
+    A(dX) - b dtau = eta rp and A'dy + dZ - C dtau = eta Rd), so pinf / dinf, the ratio of their
+    norms, is constant along the solve (to rounding) until the last rows."""
+    e = golden["rand30"]
+    out = restate.solve_hsd(make(e), tol=1e-7)
+    rows = out["table"]
+    r = [row["pinf"] / row["dinf"] for row in rows[:6]]
+    assert max(r) / min(r) < 1 + 1e-6, r

@@ -46,6 +46,23 @@ def test_embedding_certifies_infeasibility(golden, name, status, code):
         assert "self-dual embedding" in res.log
 
 
+@pytest.mark.parametrize("name", ["theta30", "rand30", "mom8", "dense24", "batch_q5", "lp_only", "infeas_p",
+                                  "infeas_d"])
+def test_embedding_follows_the_oracle_restatement(golden, name):
+    """The CUDA path's embedding against its numpy FP64 restatement (oracle solve_hsd: the same
+    start, Newton system, step rule and stops): the same status and iteration count, and on the
+    solved instances the same objectives to 1e-8 relative (they agree to about ten digits)."""
+    from oracle import restate
+    e = golden[name]
+    out = restate.solve_hsd(make(e), tol=1e-7)
+    res = brisk_b200.solve_sdpa(*make(e).args(), options=HSD, verbose=False)
+    assert res.status_str == out["status_str"], res.log
+    assert res.iterations == out["iterations"]
+    if out["status_str"] == "OPTIMAL":
+        for got, want in ((res.pobj, out["pobj"]), (res.dobj, out["dobj"])):
+            assert abs(got - want) <= 1e-8 * max(1.0, abs(want)), (got, want)
+
+
 def test_default_rule_and_nohsd():
     """Without -hsd or -nohsd the reference's rule (solver.c:13519-13560) picks the embedding for
     problems whose dense work is small next to the Schur factor (a 30 x 30 block, m = 60);
