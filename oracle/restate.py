@@ -24,12 +24,15 @@ It restates, on dense matrices (small sizes: tests), the reference BRISK 1.7 alg
                          Mb = L_Z' L_X; lam descending)
 * DIMACS errors on the data as given                                  postsolve.c:2880-2897
 * the final status rule                                               main.c:2349-2362
+* solve_hsd: the CUDA path's self-dual embedding (its own method in the place of hsd_run,
+  solver.c:9803), which the reference's embedding does not follow row by row
 
 Pinned against the reference's own runs on the same seeded inputs (tests/golden/, made by
 tests/golden/make_golden.py from oracle/_ref/brisk_ref, the reference compiled by
 oracle/Makefile): their iteration tables are followed row by row, from both starts and in both
-directions (tests/test_cpu_oracle.py); and against the reference's published golden value for
-theta1 (INSTALL.md:44-45).
+directions (tests/test_cpu_oracle.py); solve_hsd by outcome (status, objectives, certificates:
+tests/test_cpu_oracle_hsd.py); and against the reference's published golden value for theta1
+(INSTALL.md:44-45).
 """
 from __future__ import annotations
 
