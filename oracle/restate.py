@@ -151,8 +151,8 @@ def schur(A_blocks, X_blocks, Zi_blocks):
     m = A_blocks[0].shape[0]
     M = np.zeros((m, m))
     for Ak, Xk, Zik in zip(A_blocks, X_blocks, Zi_blocks):
-        G = np.einsum("pq,tqr,rs->tps", Xk, Ak, Zik)        # G_j = X A_j Zi
-        M += np.einsum("ipq,jpq->ij", Ak, G)
+        G = Xk[None] @ Ak @ Zik[None]                       # G_j = X A_j Zi (batched products)
+        M += Ak.reshape(m, -1) @ G.reshape(m, -1).T
     return M
 
 

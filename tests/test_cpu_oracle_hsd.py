@@ -13,11 +13,11 @@ from oracle import restate
 from parity import objectives_close
 from test_cpu_oracle import make
 
-# the instances whose oracle solves take seconds (blocks of order <= 64, m <= 300)
-FAST = ["theta30", "rand30", "mom8", "dense24", "batch_q5", "lp_only"]
+SOLVED = ["theta30", "theta50", "rand30", "rand60", "rand100", "mom8", "dense24", "batch_q0", "batch_q5",
+          "lowrank80", "lowrank80s", "lp_dense", "lp_mixed", "lp_only"]
 
 
-@pytest.mark.parametrize("name", FAST)
+@pytest.mark.parametrize("name", SOLVED)
 def test_oracle_embedding_matches_the_reference_embedding(golden, name):
     e = golden[name]
     ref = e["runs"]["hsd_auto"]
