@@ -5,7 +5,9 @@ against the reference's own runs of its embedding (tests/golden/ref_runs.json "h
 status and exit code, (pobj + dobj) / 2 within 1e-7 relative and each objective within 1e-7 of
 the DIMACS denominator (parity.objectives_close: the two embeddings stop at different iterates),
 DIMACS errors <= 1e-7.  The reference's embedding, with its correctors and end phases, takes 4-7
-iterations here; this one 8-12 (the infeasible method 9-14)."""
+iterations here; this one 8-12 (the infeasible method 9-14).  Row by row, the CUDA path is
+compared with the oracle's restatement of its own method (oracle solve_hsd), which these
+instances pin against the reference's runs on CPU."""
 import numpy as np
 import pytest
 
