@@ -151,8 +151,13 @@ def schur(A_blocks, X_blocks, Zi_blocks):
     m = A_blocks[0].shape[0]
     M = np.zeros((m, m))
     for Ak, Xk, Zik in zip(A_blocks, X_blocks, Zi_blocks):
-        G = Xk[None] @ Ak @ Zik[None]                       # G_j = X A_j Zi (batched products)
-        M += Ak.reshape(m, -1) @ G.reshape(m, -1).T
+        # the constraints that touch the block (the others add exact zeros)
+        idx = np.flatnonzero(np.any(Ak.reshape(m, -1) != 0, axis=1))
+        if idx.size == 0:
+            continue
+        Ai = Ak[idx]
+        G = Xk[None] @ Ai @ Zik[None]                       # G_j = X A_j Zi (batched products)
+        M[np.ix_(idx, idx)] += Ai.reshape(idx.size, -1) @ G.reshape(idx.size, -1).T
     return M
 
 

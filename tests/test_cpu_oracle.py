@@ -146,9 +146,10 @@ def test_oracle_lp_blocks_match_reference(golden, name, run, direction):
         assert mine["dobj"] == pytest.approx(theirs["dobj"], rel=1e-8, abs=1e-8)
 
 
-ROW_BY_ROW = ["theta30", "theta50", "rand30", "rand60", "rand100", "mom8", "dense24", "dense48", "lp_mixed", "lp_only",
-              "lp_dense", "lowrank80", "lowrank80s", "batch_q0", "batch_q1", "batch_q2", "batch_q3", "batch_q4",
-              "batch_q5", "batch_q6", "batch_q7", "batch_q8", "batch_q9", "batch_q10", "batch_q11", "batch_q3339"]
+ROW_BY_ROW = ["theta30", "theta50", "rand30", "rand60", "rand100", "mom8", "mom60", "dense24", "dense48", "lp_mixed",
+              "lp_only", "lp_dense", "lowrank80", "lowrank80s", "batch_q0", "batch_q1", "batch_q2", "batch_q3",
+              "batch_q4", "batch_q5", "batch_q6", "batch_q7", "batch_q8", "batch_q9", "batch_q10", "batch_q11",
+              "batch_q3339"]
 
 
 @pytest.mark.parametrize("name", ROW_BY_ROW)
