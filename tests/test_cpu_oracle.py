@@ -160,8 +160,8 @@ def test_oracle_follows_reference_row_by_row(golden, name, run, direction, init)
     from both starts (the least-squares start, the reference's default, solver.c:13939-14198; the
     SDPT3 start, -init 0) and in both directions: the same status and iterations, pobj and dobj of
     every row to the printed digits, and its gap, mu, pinf and dinf to theirs (three significant
-    digits, to 1 %; in the last rows, at the rounding floor of the residuals, pinf to 5e-12 and
-    dinf to 1e-13 absolute: the largest differences over these runs are 1.5e-12 and 1.7e-14).
+    digits, to 1 %; in the last rows, at the rounding floor of the residuals, pinf to 1e-11 and
+    dinf to 1e-13 absolute: the largest differences over these 95 runs are 4.5e-12 and 3.2e-14).
     Row 0 of a least-squares start also allows pinf 1e-10 and gap 1e-11 absolute: the reference
     solves that start by CG to 1e-10 where the restatement solves it exactly (lowrank80s: pinf
     6.2e-11 against 4.6e-16).  Blocks of order <= 32 take exact eigenvalues, larger ones the
@@ -183,7 +183,7 @@ def test_oracle_follows_reference_row_by_row(golden, name, run, direction, init)
         assert mine["gap"] == pytest.approx(theirs["gap"], rel=1e-2, abs=1e-11 if start else 1e-14), ("gap", theirs["it"])
         assert mine["mu"] == pytest.approx(theirs["mu"], rel=1e-2, abs=1e-14), ("mu", theirs["it"])
         assert mine["dinf"] == pytest.approx(theirs["dinf"], rel=6e-3, abs=1e-13), ("dinf", theirs["it"])
-        assert mine["pinf"] == pytest.approx(theirs["pinf"], rel=6e-3, abs=1e-10 if start else 5e-12), \
+        assert mine["pinf"] == pytest.approx(theirs["pinf"], rel=6e-3, abs=1e-10 if start else 1e-11), \
             ("pinf", theirs["it"])
 
 
