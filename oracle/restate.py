@@ -537,7 +537,7 @@ def solve(data, tol=1e-8, maxit=100, gamma_max=0.99, red_acc=None, log=None, dir
     return out
 
 
-def solve_hsd(data, tol=1e-8, maxit=100, gamma_max=0.99, red_acc=None, log=None, exact_n=SMALL_N_MAX):
+def solve_hsd(data, tol=1e-8, maxit=100, gamma_max=0.99, red_acc=None, log=None, exact_n=SMALL_N_MAX, check=False):
     """The homogeneous self-dual embedding as the CUDA path runs it (Solver::run_hsd, which stands
     for the reference's hsd_run, solver.c:9803, as a method of its own: HKM direction, one
     Mehrotra predictor-corrector step an iteration, no extra correctors or end phases), FP64,
@@ -556,7 +556,10 @@ def solve_hsd(data, tol=1e-8, maxit=100, gamma_max=0.99, red_acc=None, log=None,
     The reference's own embedding takes 4-7 iterations on the parity instances where this one
     takes 8-12 (its extra correctors), so the two agree in status and objectives, not row by
     row.  Returns the dict of solve() (status, iterations, pobj, dobj, dimacs, the table with
-    tau and kappa per row)."""
+    tau and kappa per row); with check, also "newton": per direction the relative residuals of
+    the four linearised equations A(dX) - b dtau = eta rp, A'dy + dZ - C dtau = eta Rd,
+    b'dy - <C,dX> - dkappa = eta rg and kappa dtau + tau dkappa = sigma mu - tau kappa - dtau_p
+    dkappa_p (each over the sum of its terms' norms)."""
     if red_acc is None:
         red_acc = max(1e-6, 100 * tol)
     lp = [int(b) < 0 for b in data.bs]
@@ -584,7 +587,7 @@ def solve_hsd(data, tol=1e-8, maxit=100, gamma_max=0.99, red_acc=None, log=None,
     status, stall, it, it_best = -1, 0, 0, 0
     best_score, best, saved = np.inf, None, None
     sigma = alpha = 0.0
-    out = {"table": []}
+    out = {"table": [], "newton": []}
     for it in range(maxit + 1):
         Zi = [np.linalg.inv(L).T @ np.linalg.inv(L) for L in LZ]
         Zi = [0.5 * (Q + Q.T) for Q in Zi]
@@ -667,6 +670,18 @@ def solve_hsd(data, tol=1e-8, maxit=100, gamma_max=0.99, red_acc=None, log=None,
                 Gd = [g + q for g, q in zip(Gd, Q)]
             dX = [-0.5 * (g + g.T) + smu * zi - x for g, zi, x in zip(Gd, Zi, Xs)]
             dk = (smu - tau * kap - dtdk - kap * dt) / tau
+            if check:
+                nrm = lambda V: float(np.sqrt(ip(V, V)))   # noqa: E731
+                ad, aty, bd = aop(A, dX), atop(A, dy), b * dt
+                e1 = float(np.linalg.norm(ad - bd - eta * rp)) / (
+                    np.linalg.norm(ad) + np.linalg.norm(bd) + eta * np.linalg.norm(rp))
+                e2 = nrm([a + z - Ck * dt - eta * R for a, z, Ck, R in zip(aty, dZ, C, Rd)]) / (
+                    nrm(aty) + nrm(dZ) + abs(dt) * nrm(C) + eta * nrm(Rd))
+                t3 = (float(b @ dy), ip(C, dX), dk, eta * rg)
+                e3 = abs(t3[0] - t3[1] - t3[2] - t3[3]) / sum(abs(t) for t in t3)
+                t4 = (kap * dt, tau * dk, smu - tau * kap - dtdk)
+                e4 = abs(t4[0] + t4[1] - t4[2]) / max(sum(abs(t) for t in t4), 1e-300)
+                out["newton"].append((it, e1, e2, e3, e4))
             return dX, dy, dZ, dt, dk
 
         dXp, _, dZp, dtp, dkp = direction(0.0, 1.0, None, None, 0.0, 0.0)

@@ -54,3 +54,19 @@ def test_oracle_embedding_residuals_fall_together(golden):
     rows = out["table"]
     r = [row["pinf"] / row["dinf"] for row in rows[:6]]
     assert max(r) / min(r) < 1 + 1e-6, r
+
+
+@pytest.mark.parametrize("name", ["rand30", "theta50", "mom8", "lp_mixed"])
+def test_oracle_embedding_solves_its_newton_system(golden, name):
+    """Every direction the restatement takes satisfies the embedding's linearised equations
+    (solve_hsd's check).  The dual equation A'dy + dZ = C dtau + eta Rd and the tau-kappa one
+    hold to rounding by construction.  The primal one and the gap equation pass through the
+    Schur solves, whose residual is eps cond(M): 1e-16 to 1e-13 while mu >= 1e-2, growing like
+    1/mu^2 near the end (up to 3e-6 relative at mu ~ 1e-7 on lp_mixed)."""
+    out = restate.solve_hsd(make(golden[name]), tol=1e-7, check=True)
+    assert out["status_str"] == "OPTIMAL"
+    assert len(out["newton"]) == 2 * out["iterations"]          # a predictor and a corrector each
+    for it, e1, e2, e3, e4 in out["newton"]:
+        assert e2 <= 1e-14 and e4 <= 1e-14, (it, e2, e4)
+        bound = 1e-12 if out["table"][it]["mu"] >= 1e-2 else 1e-4
+        assert e1 <= bound and e3 <= bound, (it, e1, e3)
